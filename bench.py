@@ -1,0 +1,392 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 sort + group-by path.
+
+Workload (one "step"): the 100,000,000-row two-key frame -- key1 int64 over
+the full 64-bit range, key2 int32 Zipf(s=1.1) over 1,000,000 distinct values,
+payload f64 N(0,1), int32 uniform and a uint64 row id -- is stably sorted by
+(key1, key2), every payload column is gathered into sorted order, and the
+frame is grouped by (key1, key2) with count/sum/min/max/mean of the f64 and
+int32 payloads.  One vdf_sort_groupby call per step through the C-ABI.
+
+  value  rows/s with the inputs resident in HBM (device-timed, CUDA events).
+  e2e    the same call fed from pinned HOST buffers: every step copies the five
+         input columns host->device, runs the call, and copies the result
+         (permutation + the group table) device->host.
+  roofline   the dominant kernel's algorithmic bytes per launch / its average
+             launch time (CUDA events around each launch, inside the timed
+             region), against the measured HBM copy bandwidth.
+  cpu_baseline   the reference's own radix kernels (+ the hash group-by restated
+                 on the reference's map and hash) on the host cores, on a
+                 10,000,000-row sample of the same workload.
+
+--gpus N (launched by torchrun for N > 1) runs N independent replicas, one per
+GPU ("replicas only": the single-GPU path has no exchange step); value is all
+rows processed / the slowest rank's time.
+
+--impl reference times the reference CPU path alone (rank 0), each step a
+bounded sample of the workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "rows/s & %HBM peak, 100M-row sort+group-by; served p99 and rows/s vs per-call"
+UNIT = "rows/s"
+WORKLOAD = ("two-key stable radix sort (key1 int64 full range, key2 int32 Zipf s=1.1 over 1M values) "
+            "+ gather of 3 payload columns (f64, int32, uint64 row id) + group-by (key1, key2) "
+            "count/sum/min/max/mean of the f64 and int32 payloads")
+# Canonical algorithmic bytes per row (8-bit digits over full key widths,
+# u32 row ids; see DESIGN.md's byte model): sort 344 + group-by with G ~= N 108.
+SORT_BYTES_PER_ROW = 344
+GROUPBY_BYTES_PER_ROW_G_EQ_N = 108
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        rows = []
+        try:
+            for line in Path(self.path).read_text().splitlines():
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_info() -> str:
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name:"):
+                return line.split(":", 1)[1].strip()
+    except FileNotFoundError:
+        pass
+    return "unknown"
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_sample(n_sample: int, cores: int):
+    """One step of the reference CPU path on an n_sample-row frame; returns
+    (seconds, kind, cores_used)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_bind as ob
+    from visondf_b200 import datagen
+
+    f = datagen.frame_w1(n_sample)
+    keys = [f["key1"], f["key2"]]
+    pay = [f["f64"], f["i32"], f["rowid"]]
+    if ob.ref_available():
+        cores = max(1, min(cores, 32))  # the reference's tables hold MAX_THREADS = 32
+        t0 = time.perf_counter()
+        perm, pay_out = ob.ref_sort(keys, ob.ASC, cores=cores, payload=pay)
+        ob.ref_groupby(keys, [f["f64"], f["i32"]], cores=cores)
+        return time.perf_counter() - t0, "reference", cores
+    t0 = time.perf_counter()
+    perm = ob.argsort(keys)
+    for p in pay:
+        p[perm]
+    ob.groupby(keys, [f["f64"], f["i32"]], sorted_groups=False)
+    return time.perf_counter() - t0, "port", 1
+
+
+def reference_arm(args, rank: int, world: int):
+    if rank != 0:
+        return
+    cores = cpu_threads()
+    times = []
+    kind, used = "reference", cores
+    for step in range(args.warmup + args.steps):
+        dt, kind, used = run_reference_sample(args.ref_sample, cores)
+        if step >= args.warmup:
+            times.append(dt)
+    sec = statistics.median(times)
+    value = args.ref_sample / sec
+    sample = (f"{args.ref_sample:,} rows of the same two-key workload per step (same generators), "
+              f"sort + payload gather + group-by; host CPU: {cpu_info()}")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rows": args.ref_sample, "parallelism": f"{used} host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def our_arm(args, rank: int, world: int, local_rank: int):
+    import torch
+    import torch.distributed as dist
+
+    import visondf_b200 as vdf
+    from visondf_b200 import datagen
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    n = args.rows
+    t0 = time.time()
+    f = datagen.frame_w1(n)
+    log(f"[rank {rank}] generated {n:,} rows in {time.time() - t0:.1f}s")
+    names = ["key1", "key2", "f64", "i32", "rowid"]
+    host = {k: torch.from_numpy(f[k]).pin_memory() for k in names}
+    del f
+    d = {k: host[k].to(dev, non_blocking=True) for k in names}
+    torch.cuda.synchronize()
+    keys = [d["key1"], d["key2"]]
+    payload = [d["f64"], d["i32"], d["rowid"]]
+    agg_cols = [0, 1]
+    ctx = vdf.Context(local_rank)
+    stream = torch.cuda.current_stream()
+    outs = ctx.alloc_sort_groupby_outputs(keys, payload, agg_cols)
+    packed = ctx.pack_sort_groupby(keys, payload, agg_cols, vdf.ORDER_ASC, True, outs, host_count=False)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident timing ------------------------------------------------
+    for _ in range(args.warmup):
+        ctx.sort_groupby_packed(packed, stream)
+    ctx.check(stream)
+    ctx.profile(True)
+    ctx.profile_reset()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = ctx.kernel_launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clocks:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.sort_groupby_packed(packed, stream)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    launches = ctx.kernel_launches - launches0
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    ctx.check(stream)
+    n_groups = int(outs["ngroups_dev"].item())
+    clk = clocks.summary()
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n * world / (ms / 1e3)
+
+    # ---- roofline of the dominant kernel ------------------------------------------
+    peak, peak_kind = measured_peaks()
+    bytes_per_launch = {"onesweep32": 2 * (4 + 4) * n, "onesweep64": 2 * (8 + 4) * n,
+                        "hist": 12 * n, "gather": None, "segreduce": None}
+    dom = max(prof, key=lambda k: prof[k][0])
+    dom_ms, dom_cnt = prof[dom]
+    if bytes_per_launch.get(dom) is None:
+        dom = "onesweep64"
+        dom_ms, dom_cnt = prof[dom]
+    avg_ms = dom_ms / max(dom_cnt, 1)
+    achieved = bytes_per_launch[dom] / (avg_ms / 1e3) / 1e9
+    traffic = None
+    tfile = ROOT / "profiles" / "traffic.json"
+    if tfile.exists():
+        tj = json.loads(tfile.read_text())
+        ent = tj.get(dom)
+        if ent and ent.get("rows"):
+            traffic = ent["bytes_per_launch"] * n / ent["rows"]
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": bytes_per_launch[dom], "avg_launch_ms": avg_ms}
+    kernels = {k: {"ms_per_step": v[0] / args.steps, "launches_per_step": v[1] / args.steps}
+               for k, v in prof.items() if v[1]}
+    canonical = (SORT_BYTES_PER_ROW + GROUPBY_BYTES_PER_ROW_G_EQ_N) * n
+    step_frac = canonical / (ms / 1e3) / 1e9 / peak
+
+    # ---- end to end from host buffers -------------------------------------------
+    e2e = None
+    if not args.no_e2e:
+        h2d = sum(host[k].numel() * host[k].element_size() for k in names)
+        g = n_groups
+        res_host = {
+            "perm": torch.empty(n, dtype=torch.int32).pin_memory(),
+            "k1": torch.empty(n, dtype=torch.int64).pin_memory(),
+            "k2": torch.empty(n, dtype=torch.int32).pin_memory(),
+            "count": torch.empty(n, dtype=torch.int64).pin_memory(),
+        }
+        agg_host = []
+        for a in outs["aggs"]:
+            agg_host.append({fld: torch.empty(getattr(a, fld).numel(), dtype=getattr(a, fld).dtype).pin_memory()
+                             for fld in ("sum", "sum_hi", "min", "max", "mean") if getattr(a, fld) is not None})
+        outs_e = ctx.alloc_sort_groupby_outputs(keys, payload, agg_cols)
+        packed_e = ctx.pack_sort_groupby(keys, payload, agg_cols, vdf.ORDER_ASC, True, outs_e, host_count=True)
+
+        def e2e_step():
+            for k in names:
+                d[k].copy_(host[k], non_blocking=True)
+            ctx.sort_groupby_packed(packed_e, stream)
+            gg = int(outs_e["_ng"].value)
+            res_host["perm"].copy_(outs_e["perm"], non_blocking=True)
+            res_host["k1"][:gg].copy_(outs_e["gkeys"][0][:gg], non_blocking=True)
+            res_host["k2"][:gg].copy_(outs_e["gkeys"][1][:gg], non_blocking=True)
+            res_host["count"][:gg].copy_(outs_e["count"][:gg], non_blocking=True)
+            nbytes = 4 * n + gg * (8 + 4 + 8)
+            for a, ah in zip(outs_e["aggs"], agg_host):
+                for fld, t in ah.items():
+                    src = getattr(a, fld)
+                    t[:gg].copy_(src[:gg], non_blocking=True)
+                    nbytes += gg * src.element_size()
+            return nbytes
+
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        torch.cuda.synchronize()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        d2h = 0
+        for _ in range(args.steps):
+            d2h = e2e_step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ems = e0.elapsed_time(e1) / args.steps
+        if world > 1:
+            t = torch.tensor([ems], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        e2e = {"value": n * world / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+               "ms_per_step": ems}
+
+    # ---- CPU baseline (rank 0, one GPU only) -------------------------------------
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sec, kind, used = run_reference_sample(args.ref_sample, cpu_threads())
+        cpu = {"value": args.ref_sample / sec, "unit": UNIT, "cores": used, "kind": kind,
+               "sample": f"{args.ref_sample:,} rows of the same workload (same generators), one step of "
+                         f"sort + payload gather + group-by; host CPU: {cpu_info()}"}
+
+    ctx.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "rows": n, "n_groups": n_groups, "key_dtypes": ["int64", "int32"],
+                       "payload_dtypes": ["float64", "int32", "uint64"], "parallelism": f"replicas x{world}",
+                       "l2": "inputs (3.2 GB) larger than L2 (126 MB); no flush between steps"},
+            "roofline": roofline,
+            "hbm_frac_canonical": step_frac,
+            "canonical_bytes_per_row": SORT_BYTES_PER_ROW + GROUPBY_BYTES_PER_ROW_G_EQ_N,
+            "kernels": kernels,
+            "gpu_launches": launches,
+            "clocks": clk,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--rows", type=int, default=100_000_000)
+    ap.add_argument("--ref-sample", type=int, default=10_000_000)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("note: fewer than 3 warm-up steps; the timing rules ask for at least 3")
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local_rank))
+    try:
+        our_arm(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

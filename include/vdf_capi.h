@@ -1,0 +1,232 @@
+/*
+ * vdf_capi.h -- C-ABI of the B200 sort + group-by path (libvdf_b200.so).
+ *
+ * Plain pointers and sizes only.  Column data, permutations and outputs are
+ * DEVICE pointers on the context's GPU, owned by the caller; `stream` is a
+ * cudaStream_t passed as void* (NULL = the legacy default stream).  Every call
+ * returns a vdf_status and never aborts or throws.  Compute calls are
+ * asynchronous on `stream` unless they return a host value (n_groups_host),
+ * in which case they synchronise that stream before returning.
+ *
+ * A context owns one grow-only workspace, so calls on one context are
+ * serialised on the host and must not overlap on the GPU: use one context per
+ * concurrently used stream, or the *_ws variants with caller-owned workspace.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the VisonDF project, V/ = include/vison/).  The reference's own error
+ * convention (std::cerr message + early return, sort_by_mt.hpp:16-18,40-41,
+ * 68-69) is restored by the C++ layer in include/vison_b200/vison.hpp.
+ */
+#ifndef VDF_CAPI_H
+#define VDF_CAPI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VDF_ABI_VERSION 1u
+
+typedef enum vdf_status {
+    VDF_OK = 0,
+    VDF_ERR_INVALID_ARG = 1, /* bad pointer, dtype, count or alignment            */
+    VDF_ERR_OOM = 2,         /* workspace allocation failed                         */
+    VDF_ERR_TIMEOUT = 3,     /* a bounded device wait gave up (look-back)           */
+    VDF_ERR_DEVICE = 4,      /* CUDA runtime error                                  */
+    VDF_ERR_UNSUPPORTED = 5, /* valid request outside this build's limits           */
+    VDF_ERR_WORKSPACE = 6    /* caller-provided workspace too small                 */
+} vdf_status;
+
+/* Column element types.  The reference's DefaultTypes are IntT=int,
+ * UIntT=unsigned int, FloatT=double (V/types/inference_type.hpp:3-8); the
+ * 64-bit integer widths cover sort_integers' int64 branch
+ * (V/inlines/transform/sort_by/sort_integers.inl:121-133). */
+typedef enum vdf_dtype {
+    VDF_I32 = 0,
+    VDF_I64 = 1,
+    VDF_U32 = 2,
+    VDF_U64 = 3,
+    VDF_F64 = 4,
+    VDF_F32 = 5
+} vdf_dtype;
+
+/* Sort order.  ASC: stable ascending (ties keep row order).
+ * DESC_STABLE: stable descending, the order V/INTERNALS.doc:1610-1632 shows.
+ * DESC_REVERSE: the reference code's descending order, an ascending sort
+ * followed by std::reverse (sort_integers.inl:225-227), so ties come out in
+ * reverse row order. */
+typedef enum vdf_order {
+    VDF_ORDER_ASC = 0,
+    VDF_ORDER_DESC_STABLE = 1,
+    VDF_ORDER_DESC_REVERSE = 2
+} vdf_order;
+
+/* A device column: `data` points at n elements of `dtype`. */
+typedef struct vdf_col {
+    const void* data;
+    int32_t dtype;
+} vdf_col;
+
+/* Group-by outputs of one value column; device arrays with room for n
+ * groups (the group count is only known after the call).  Any may be NULL.
+ *   sum    : double for float columns; the low 64 bits (int64 wrap-around
+ *            view) of the exact 128-bit sum for integer columns
+ *   sum_hi : high 64 bits of the exact integer sum (integer columns)
+ *   min,max: in the column's own dtype
+ *   mean   : double, sum / count (the reference divides by the frame's row
+ *            count instead, V/inlines/transform/transform_group_by/
+ *            create_value_col.inl:46; that is a bug and is not reproduced) */
+typedef struct vdf_agg_out {
+    void* sum;
+    int64_t* sum_hi;
+    void* min;
+    void* max;
+    double* mean;
+} vdf_agg_out;
+
+typedef struct vdf_ctx vdf_ctx;
+
+/* ---- library / context --------------------------------------------------- */
+uint32_t vdf_abi_version(void);
+const char* vdf_status_string(vdf_status s);
+
+/* Creates a context on `device`.  Replaces init_openmp(cores)
+ * (V/vison.hpp:57-74), the reference's only runtime set-up. */
+vdf_status vdf_ctx_create(int device, vdf_ctx** out);
+vdf_status vdf_ctx_destroy(vdf_ctx* ctx);
+/* Last error message of this context (empty string when none). */
+const char* vdf_ctx_last_error(const vdf_ctx* ctx);
+/* Grows the context workspace to at least `bytes` now (optional). */
+vdf_status vdf_ctx_reserve(vdf_ctx* ctx, size_t bytes);
+/* Synchronises `stream`, then reads and clears the device error bits that
+ * bounded waits raise; returns VDF_ERR_TIMEOUT if any were set. */
+vdf_status vdf_ctx_check(vdf_ctx* ctx, void* stream);
+/* Number of kernels this context has launched so far (for benchmarks). */
+uint64_t vdf_ctx_kernel_launches(const vdf_ctx* ctx);
+
+/* Kernel classes for per-launch timing. */
+typedef enum vdf_kernel_class {
+    VDF_KC_HIST = 0,        /* all-digit histogram            */
+    VDF_KC_SCAN = 1,        /* digit offset scan              */
+    VDF_KC_ONESWEEP32 = 2,  /* radix pass, 4-byte keys        */
+    VDF_KC_ONESWEEP64 = 3,  /* radix pass, 8-byte keys        */
+    VDF_KC_GATHER = 4,      /* payload gather                 */
+    VDF_KC_SEGREDUCE = 5,   /* group-by segmented reduction   */
+    VDF_KC_BROADCAST = 6    /* transform broadcast            */
+} vdf_kernel_class;
+/* When enabled, every kernel the context launches is bracketed by CUDA
+ * events on its stream (no reference counterpart: the reference has no
+ * tracing beyond ad-hoc std::chrono in benchmarks/readf.cpp:20-25). */
+vdf_status vdf_ctx_profile(vdf_ctx* ctx, int enable);
+/* Waits for the recorded events; returns the summed device time (ms) and
+ * launch count of kernel class `cls` since the last reset. */
+vdf_status vdf_ctx_profile_read(vdf_ctx* ctx, int cls, double* total_ms, uint64_t* launches);
+vdf_status vdf_ctx_profile_reset(vdf_ctx* ctx);
+
+/* ---- workspace sizing (pure host functions) ------------------------------ */
+size_t vdf_sort_workspace_bytes(uint64_t n, const int32_t* key_dtypes, int nkeys);
+size_t vdf_groupby_workspace_bytes(uint64_t n, int nvals);
+/* Largest row count one call accepts (2^30 - 1 in this build). */
+uint64_t vdf_max_rows(void);
+
+/* ---- sort ----------------------------------------------------------------- */
+/* Stable LSD radix argsort over nkeys key columns; keys[0] is the most
+ * significant.  Writes perm_out[r] = source row of sorted row r (u32), and,
+ * for each k with sorted_keys_out != NULL && sorted_keys_out[k] != NULL, the
+ * raw key column k in sorted order.
+ * Replaces sort_integers / sort_uintegers / sort_flt
+ *   (V/inlines/transform/sort_by/sort_integers.inl:8-13 idx, col, nrow;
+ *    sort_uintegers.inl:8-13; sort_flt.inl:8-13)
+ * and the radix kernels they call, radix_sort_uint32[_mt] / radix_sort_uint64[_mt]
+ *   (V/inlines/radix_sorts/radix_sort_uint64.inl:5-7 tkeys, idx, n;
+ *    radix_sort_uint64_mt.inl:3-8), composed over several keys through the
+ * idx in/out parameter (the reference has no multi-key sort entry point). */
+vdf_status vdf_sort_argsort(vdf_ctx* ctx, uint64_t n, const vdf_col* keys, int nkeys, int order,
+                            uint32_t* perm_out, void* const* sorted_keys_out, void* stream);
+/* Same, with caller-owned workspace of at least vdf_sort_workspace_bytes(). */
+vdf_status vdf_sort_argsort_ws(vdf_ctx* ctx, uint64_t n, const vdf_col* keys, int nkeys, int order,
+                               uint32_t* perm_out, void* const* sorted_keys_out, void* workspace,
+                               size_t workspace_bytes, void* stream);
+
+/* ---- gather ---------------------------------------------------------------- */
+/* out[c][r] = in[c].data[perm[r]] for ncols (<= 8) columns in one launch.
+ * Replaces permute_block_mt (V/inlines/transform/sort_by/permute_block_mt.inl:3-47),
+ * no_inplace_permutation (V/inlines/no_inplace_permutation.inl:3-79) and the
+ * per-block loop of materialize_mt (V/materialize/materialize_mt.hpp:6-55). */
+vdf_status vdf_gather(vdf_ctx* ctx, uint64_t n, const uint32_t* perm, const vdf_col* in, int ncols,
+                      void* const* out, void* stream);
+
+/* ---- group-by over sorted rows -------------------------------------------- */
+/* Key and value columns are already in key order (e.g. the outputs of
+ * vdf_sort_argsort + vdf_gather).  Finds segment boundaries and writes, per
+ * group in ascending row order: group_keys_out[k][g], count_out[g] (int64),
+ * and the vdf_agg_out of each value column.  group_start_out[g] = first
+ * sorted row of group g; row_group_out[r] = group of sorted row r (both
+ * optional, u32).  The group count goes to *n_groups_dev (device, async)
+ * and/or *n_groups_host (host; the call then synchronises `stream`).
+ * Replaces the hash group-by loop of transform_group_by_onecol_mt
+ * (V/transform/transform_group_by/transform_group_by_onecol_mt.hpp:182-337,
+ * AddLookupOneCol / OccLookupOneCol V/inlines/transform/transform_group_by/
+ * onecol_functions.inl:4-86, MergeCurMap merge_functions.inl:3-36) and the
+ * multi-key variants (_sametype_mt / _difftype_mt via KeyBuildSameType /
+ * KeyBuildDiffType, key_build.inl:3-110). */
+vdf_status vdf_groupby_sorted(vdf_ctx* ctx, uint64_t n, const vdf_col* keys, int nkeys,
+                              const vdf_col* vals, int nvals, void* const* group_keys_out,
+                              int64_t* count_out, const vdf_agg_out* aggs, uint32_t* group_start_out,
+                              uint32_t* row_group_out, uint64_t* n_groups_dev, uint64_t* n_groups_host,
+                              void* stream);
+
+/* ---- fused sort + payload gather + group-by --------------------------------- */
+typedef struct vdf_sort_groupby_args {
+    uint64_t n;
+    const vdf_col* keys;      /* nkeys key columns, most significant first       */
+    int32_t nkeys;
+    int32_t order;            /* vdf_order                                       */
+    const vdf_col* payload;   /* npayload (<= 8) payload columns                 */
+    int32_t npayload;
+    /* sort outputs (each may be NULL) */
+    uint32_t* perm_out;            /* n row ids; NULL = internal buffer            */
+    void* const* sorted_keys_out;  /* nkeys entries (entries may be NULL)          */
+    void* const* payload_out;      /* npayload entries (entries may be NULL)       */
+    /* group-by (groupby == 0: sort + gather only) */
+    int32_t groupby;
+    const int32_t* agg_cols;       /* indices into payload of the aggregated columns */
+    int32_t nagg;                  /* <= 4                                           */
+    void* const* group_keys_out;   /* nkeys entries (entries may be NULL)          */
+    int64_t* group_count_out;
+    const vdf_agg_out* aggs;       /* nagg entries                                   */
+    uint32_t* group_start_out;
+    uint32_t* row_group_out;
+    uint64_t* n_groups_dev;
+    uint64_t* n_groups_host;       /* non-NULL: the call synchronises `stream`       */
+} vdf_sort_groupby_args;
+
+/* One call for the whole path: sort by the keys, gather every payload column
+ * by the permutation and aggregate the chosen payload columns per group; the
+ * payload gather is fused into the group-by pass.  Replaces the composition
+ * sort_by_mt (V/transform/sort_by/sort_by_mt.hpp:3-180, Soft=false:
+ * permute_block_mt over every type block :117-159) followed by
+ * transform_group_by_mt (V/transform/transform_group_by/
+ * transform_group_by_mt.hpp:12-114), in the segment layout of the "hard"
+ * variant (hard/transform_group_by_onecol_hard_mt.hpp:11-372). */
+vdf_status vdf_sort_groupby(vdf_ctx* ctx, const vdf_sort_groupby_args* args, void* stream);
+
+/* ---- transform output --------------------------------------------------------- */
+/* out[perm ? perm[r] : r] = group_vals[row_group[r]] (width 4 or 8 bytes,
+ * n_groups entries in group_vals): broadcasts a per-group aggregate back to
+ * every row, in sorted order or (perm != NULL) in the frame's original row
+ * order.  Out-of-range group or row ids are skipped and raise the context's
+ * error bits (see vdf_ctx_check).  Replaces
+ * CreateValueCol::apply (V/inlines/transform/transform_group_by/
+ * create_value_col.inl:36-61) and the segment fill of CreateValueColHard
+ * (hard/create_value_col_hard.inl:38-59). */
+vdf_status vdf_broadcast(vdf_ctx* ctx, uint64_t n, const uint32_t* row_group, const void* group_vals,
+                         uint64_t n_groups, int width, const uint32_t* perm, void* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VDF_CAPI_H */

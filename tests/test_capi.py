@@ -1,0 +1,76 @@
+"""The C-ABI library, without a GPU: it loads, exports every function
+include/vdf_capi.h declares, and its pure host functions (sizing, limits,
+status strings) behave.  No compute call is made here."""
+import ctypes as C
+import subprocess
+
+import numpy as np
+import pytest
+
+import visondf_b200 as vdf
+from visondf_b200 import _lib
+
+
+def test_library_exports_every_declared_symbol():
+    declared = _lib.header_functions()
+    assert len(declared) >= 15
+    out = subprocess.run(["nm", "-D", "--defined-only", str(vdf.LIB_PATH)], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if " T " in line}
+    missing = [f for f in declared if f not in exported]
+    assert not missing, missing
+    for f in declared:
+        assert hasattr(vdf.lib, f)
+
+
+def test_abi_version_and_limits():
+    assert vdf.lib.vdf_abi_version() == 1
+    assert vdf.lib.vdf_max_rows() == (1 << 30) - 1
+
+
+def test_status_strings():
+    for s in range(7):
+        assert vdf.lib.vdf_status_string(s)
+    assert vdf.lib.vdf_status_string(99) == b"unknown status"
+
+
+def test_sort_workspace_sizing():
+    dts = (C.c_int32 * 2)(vdf.I64, vdf.I32)
+    small = vdf.lib.vdf_sort_workspace_bytes(1000, dts, 2)
+    big = vdf.lib.vdf_sort_workspace_bytes(100_000_000, dts, 2)
+    assert 0 < small < big
+    # ping-pong keys (8 B) + row ids (4 B) dominate: about 24 B/row
+    assert 24 * 100_000_000 <= big <= 26 * 100_000_000
+    bad = (C.c_int32 * 1)(42)
+    assert vdf.lib.vdf_sort_workspace_bytes(10, bad, 1) == 0
+    assert vdf.lib.vdf_sort_workspace_bytes(10, dts, 0) == 0
+    assert vdf.lib.vdf_sort_workspace_bytes(10, dts, 5) == 0
+
+
+def test_groupby_workspace_sizing():
+    assert vdf.lib.vdf_groupby_workspace_bytes(0, 2) == 256
+    a = vdf.lib.vdf_groupby_workspace_bytes(1 << 20, 2)
+    b = vdf.lib.vdf_groupby_workspace_bytes(1 << 20, 4)
+    assert 256 < a < b
+    assert vdf.lib.vdf_groupby_workspace_bytes(10, 5) == 0
+
+
+def test_null_context_is_rejected():
+    assert vdf.lib.vdf_sort_argsort(None, 0, None, 1, 0, None, None, None) == _lib.ERR_INVALID_ARG
+    assert vdf.lib.vdf_ctx_destroy(None) == _lib.ERR_INVALID_ARG
+    assert vdf.lib.vdf_ctx_kernel_launches(None) == 0
+
+
+def test_ctx_create_without_gpu_fails_cleanly():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = C.c_void_p()
+    assert vdf.lib.vdf_ctx_create(0, C.byref(h)) == _lib.ERR_DEVICE
+    assert not h.value
+
+
+def test_dtype_maps_are_consistent():
+    import torch
+    for t, code in _lib.TORCH_TO_VDF.items():
+        assert _lib.WIDTH[code] == torch.empty(0, dtype=t).element_size()

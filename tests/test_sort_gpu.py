@@ -1,0 +1,134 @@
+"""GPU stable radix argsort through the C-ABI, bit-exact against the CPU
+oracle (and, through the golden fixtures, the reference's own kernels)."""
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+import torch
+
+import oracle_bind as ob
+import visondf_b200 as vdf
+from gpu_util import bits_equal, dev, host
+from visondf_b200 import datagen
+
+pytestmark = pytest.mark.gpu
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+# tile sizes are 4096 rows (4-byte keys) and 3072 rows (8-byte keys)
+SIZES = [0, 1, 2, 31, 32, 33, 255, 256, 257, 3071, 3072, 3073, 4095, 4096, 4097, 100_003]
+DTYPES = [np.int32, np.int64, np.uint32, np.uint64, np.float64, np.float32]
+ORDERS = [vdf.ORDER_ASC, vdf.ORDER_DESC_STABLE, vdf.ORDER_DESC_REVERSE]
+
+
+def check_sort(ctx, keys, order=vdf.ORDER_ASC):
+    n = keys[0].size
+    dk = [dev(k) for k in keys]
+    skeys = [torch.empty_like(k) for k in dk]
+    perm = ctx.argsort(dk, order=order, sorted_keys_out=skeys)
+    ctx.check()
+    exp = ob.argsort(keys, order)
+    got = host(perm).view(np.uint32)
+    assert got.shape == (n,)
+    assert (got == exp).all(), f"first mismatch at {np.argmax(got != exp)}"
+    for k, s in zip(keys, skeys):
+        assert bits_equal(host(s), k[exp])
+
+
+@pytest.mark.parametrize("n", SIZES)
+@pytest.mark.parametrize("dt", DTYPES)
+def test_single_key_sizes(ctx, n, dt):
+    rng = np.random.default_rng(n * 7 + 1)
+    check_sort(ctx, [datagen.keys_for("uniform", dt, n, rng)])
+
+
+@pytest.mark.parametrize("dist", ["uniform", "few", "equal", "sorted", "reversed", "zipf", "small"])
+@pytest.mark.parametrize("dt", [np.int32, np.int64, np.uint64, np.float64])
+@pytest.mark.parametrize("order", ORDERS)
+def test_single_key_distributions(ctx, dist, dt, order):
+    if dist in ("zipf", "small") and np.dtype(dt).kind == "f":
+        pytest.skip("integer-only distribution")
+    rng = np.random.default_rng(hash((dist, np.dtype(dt).name, order)) & 0xFFFF)
+    check_sort(ctx, [datagen.keys_for(dist, dt, 250_001, rng)], order)
+
+
+@pytest.mark.parametrize("order", ORDERS)
+@pytest.mark.parametrize("dts", [(np.int64, np.int32), (np.int32, np.int64, np.uint32), (np.float64, np.uint64),
+                                 (np.uint32, np.uint32, np.uint32, np.int64)])
+def test_multi_key(ctx, dts, order):
+    rng = np.random.default_rng(len(dts) * 100 + order)
+    n = 200_003
+    dists = ["few", "zipf", "small", "uniform"]
+    keys = [datagen.keys_for(dists[i] if np.dtype(t).kind != "f" else "few", t, n, rng) for i, t in enumerate(dts)]
+    check_sort(ctx, keys, order)
+
+
+def test_golden_reference_radix_fixtures(ctx):
+    z = np.load(GOLDEN / "ref_sort_cases.npz")
+    for c in range(int(z["n_cases"][0])):
+        keys, i = [], 0
+        while f"c{c}_k{i}" in z:
+            keys.append(z[f"c{c}_k{i}"])
+            i += 1
+        for order, name in [(vdf.ORDER_ASC, "asc"), (vdf.ORDER_DESC_REVERSE, "rev")]:
+            perm = ctx.argsort([dev(k) for k in keys], order=order)
+            assert (host(perm).view(np.uint32) == z[f"c{c}_{name}"]).all(), (c, name)
+
+
+def test_golden_internals_doc_example(ctx):
+    d = json.loads((GOLDEN / "internals_sort_by.json").read_text())
+    col = list(d["columns"])[d["sort_col_index"]]
+    key = np.array(d["columns"][col], dtype=np.uint32)
+    ids = np.array(d["columns"]["col1"])
+    perm = host(ctx.argsort([dev(key)], order=vdf.ORDER_ASC)).view(np.uint32)
+    assert list(ids[perm]) == d["asc_col1"]
+    perm = host(ctx.argsort([dev(key)], order=vdf.ORDER_DESC_STABLE)).view(np.uint32)
+    assert list(ids[perm]) == d["desc_col1"]
+
+
+def test_workspace_variant_and_too_small(ctx):
+    rng = np.random.default_rng(9)
+    k = datagen.keys_for("uniform", np.int64, 50_000, rng)
+    import ctypes as C
+    need = vdf.lib.vdf_sort_workspace_bytes(k.size, (C.c_int32 * 1)(vdf.I64), 1)
+    ws = torch.empty(need, dtype=torch.uint8, device="cuda")
+    perm = ctx.argsort([dev(k)], workspace=ws)
+    assert (host(perm).view(np.uint32) == ob.argsort([k])).all()
+    with pytest.raises(vdf.VdfError) as ei:
+        ctx.argsort([dev(k)], workspace=ws[: need // 2])
+    assert ei.value.status == vdf._lib.ERR_WORKSPACE
+
+
+def test_invalid_arguments(ctx):
+    k = dev(np.arange(10, dtype=np.int32))
+    with pytest.raises(vdf.VdfError):
+        ctx.argsort([k], order=7)
+    with pytest.raises(vdf.VdfError) as ei:
+        ctx.argsort([k] * 5)
+    assert ei.value.status == vdf._lib.ERR_INVALID_ARG
+
+
+def test_gather_widths_and_alignment(ctx):
+    rng = np.random.default_rng(4)
+    for n in (1, 3, 4, 5, 1001, 65_537):
+        perm = rng.permutation(n).astype(np.uint32)
+        cols = [rng.integers(-9, 9, n).astype(np.int32), rng.standard_normal(n),
+                rng.integers(0, 2**63, n, dtype=np.uint64), rng.standard_normal(n).astype(np.float32)]
+        out = ctx.gather(dev(perm).view(torch.int32), [dev(c) for c in cols])
+        for c, o in zip(cols, out):
+            assert bits_equal(host(o), c[perm])
+    # unaligned output views take the scalar path
+    n = 1003
+    perm = rng.permutation(n).astype(np.uint32)
+    src = rng.standard_normal(n)
+    big = torch.empty(n + 1, dtype=torch.float64, device="cuda")
+    ctx.gather(dev(perm).view(torch.int32), [dev(src)], out=[big[1:]])
+    assert bits_equal(host(big[1:]), src[perm])
+
+
+def test_repeated_calls_reuse_workspace(ctx):
+    rng = np.random.default_rng(21)
+    for n in (10_000, 1_000_000, 5_000, 2_000_000):
+        k = datagen.keys_for("zipf", np.int64, n, rng)
+        perm = ctx.argsort([dev(k)])
+        assert (host(perm).view(np.uint32) == ob.argsort([k])).all()

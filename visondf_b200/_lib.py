@@ -1,0 +1,363 @@
+"""ctypes binding of include/vdf_capi.h (libvdf_b200.so).
+
+Columns are contiguous CUDA torch tensors; torch only provides device memory
+and streams here.  Every operation runs in the CUDA library; if the library
+is missing the import fails loudly -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Optional, Sequence
+
+import torch
+
+LIB_PATH = Path(__file__).resolve().parent / "libvdf_b200.so"
+HEADER_PATH = Path(__file__).resolve().parent.parent / "include" / "vdf_capi.h"
+
+# vdf_status
+OK, ERR_INVALID_ARG, ERR_OOM, ERR_TIMEOUT, ERR_DEVICE, ERR_UNSUPPORTED, ERR_WORKSPACE = range(7)
+# vdf_dtype
+I32, I64, U32, U64, F64, F32 = range(6)
+# vdf_order
+ORDER_ASC, ORDER_DESC_STABLE, ORDER_DESC_REVERSE = range(3)
+
+KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast"]
+
+TORCH_TO_VDF = {
+    torch.int32: I32, torch.int64: I64, torch.uint32: U32, torch.uint64: U64,
+    torch.float64: F64, torch.float32: F32,
+}
+VDF_TO_TORCH = {v: k for k, v in TORCH_TO_VDF.items()}
+WIDTH = {I32: 4, I64: 8, U32: 4, U64: 8, F64: 8, F32: 4}
+
+
+class VdfError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"vdf status {status}: {message}")
+        self.status = status
+
+
+class vdf_col(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("dtype", C.c_int32)]
+
+
+class vdf_agg_out(C.Structure):
+    _fields_ = [("sum", C.c_void_p), ("sum_hi", C.c_void_p), ("min", C.c_void_p), ("max", C.c_void_p),
+                ("mean", C.c_void_p)]
+
+
+class vdf_sort_groupby_args(C.Structure):
+    _fields_ = [
+        ("n", C.c_uint64), ("keys", C.POINTER(vdf_col)), ("nkeys", C.c_int32), ("order", C.c_int32),
+        ("payload", C.POINTER(vdf_col)), ("npayload", C.c_int32),
+        ("perm_out", C.c_void_p), ("sorted_keys_out", C.POINTER(C.c_void_p)), ("payload_out", C.POINTER(C.c_void_p)),
+        ("groupby", C.c_int32), ("agg_cols", C.POINTER(C.c_int32)), ("nagg", C.c_int32),
+        ("group_keys_out", C.POINTER(C.c_void_p)), ("group_count_out", C.c_void_p),
+        ("aggs", C.POINTER(vdf_agg_out)), ("group_start_out", C.c_void_p), ("row_group_out", C.c_void_p),
+        ("n_groups_dev", C.c_void_p), ("n_groups_host", C.POINTER(C.c_uint64)),
+    ]
+
+
+def _load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is not built; run `python -m visondf_b200.build` (no CPU fallback exists)")
+    lib = C.CDLL(str(LIB_PATH))
+    vp, u64, i32, sz = C.c_void_p, C.c_uint64, C.c_int, C.c_size_t
+    st = C.c_int
+    sig = {
+        "vdf_abi_version": (C.c_uint32, []),
+        "vdf_status_string": (C.c_char_p, [st]),
+        "vdf_max_rows": (u64, []),
+        "vdf_ctx_create": (st, [i32, C.POINTER(vp)]),
+        "vdf_ctx_destroy": (st, [vp]),
+        "vdf_ctx_last_error": (C.c_char_p, [vp]),
+        "vdf_ctx_reserve": (st, [vp, sz]),
+        "vdf_ctx_check": (st, [vp, vp]),
+        "vdf_ctx_kernel_launches": (u64, [vp]),
+        "vdf_ctx_profile": (st, [vp, i32]),
+        "vdf_ctx_profile_read": (st, [vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+        "vdf_ctx_profile_reset": (st, [vp]),
+        "vdf_sort_workspace_bytes": (sz, [u64, C.POINTER(C.c_int32), i32]),
+        "vdf_groupby_workspace_bytes": (sz, [u64, i32]),
+        "vdf_sort_argsort": (st, [vp, u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp]),
+        "vdf_sort_argsort_ws": (st, [vp, u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp, sz, vp]),
+        "vdf_gather": (st, [vp, u64, vp, C.POINTER(vdf_col), i32, C.POINTER(vp), vp]),
+        "vdf_groupby_sorted": (st, [vp, u64, C.POINTER(vdf_col), i32, C.POINTER(vdf_col), i32, C.POINTER(vp), vp,
+                                    C.POINTER(vdf_agg_out), vp, vp, vp, C.POINTER(C.c_uint64), vp]),
+        "vdf_sort_groupby": (st, [vp, C.POINTER(vdf_sort_groupby_args), vp]),
+        "vdf_broadcast": (st, [vp, u64, vp, vp, u64, i32, vp, vp, vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+lib = _load()
+
+
+def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
+    return None if t is None else t.data_ptr()
+
+
+def _col(t: torch.Tensor) -> vdf_col:
+    if not t.is_cuda or not t.is_contiguous():
+        raise ValueError("columns must be contiguous CUDA tensors")
+    if t.dtype not in TORCH_TO_VDF:
+        raise TypeError(f"unsupported column dtype {t.dtype}")
+    return vdf_col(t.data_ptr(), TORCH_TO_VDF[t.dtype])
+
+
+def _cols(ts: Sequence[torch.Tensor]):
+    arr = (vdf_col * max(1, len(ts)))()
+    for i, t in enumerate(ts):
+        arr[i] = _col(t)
+    return arr
+
+
+def _ptrs(ts: Sequence[Optional[torch.Tensor]]):
+    arr = (C.c_void_p * max(1, len(ts)))()
+    for i, t in enumerate(ts):
+        arr[i] = _ptr(t)
+    return arr
+
+
+def _stream(stream) -> Optional[int]:
+    if stream is None:
+        stream = torch.cuda.current_stream()
+    return stream.cuda_stream
+
+
+@dataclass
+class AggResult:
+    sum: torch.Tensor
+    sum_hi: Optional[torch.Tensor]
+    min: torch.Tensor
+    max: torch.Tensor
+    mean: torch.Tensor
+
+
+@dataclass
+class GroupResult:
+    n_groups: int
+    keys: list
+    count: torch.Tensor
+    aggs: list
+    group_start: Optional[torch.Tensor] = None
+    row_group: Optional[torch.Tensor] = None
+    perm: Optional[torch.Tensor] = None
+    sorted_keys: list = field(default_factory=list)
+    payload: list = field(default_factory=list)
+
+    def trimmed(self) -> "GroupResult":
+        g = self.n_groups
+        aggs = [AggResult(a.sum[:g], None if a.sum_hi is None else a.sum_hi[:g], a.min[:g], a.max[:g], a.mean[:g])
+                for a in self.aggs]
+        return GroupResult(g, [k[:g] for k in self.keys], self.count[:g], aggs,
+                           None if self.group_start is None else self.group_start[:g], self.row_group, self.perm,
+                           self.sorted_keys, self.payload)
+
+
+def _alloc_aggs(vals: Sequence[torch.Tensor], n: int, device):
+    outs, structs = [], (vdf_agg_out * max(1, len(vals)))()
+    for i, v in enumerate(vals):
+        is_float = v.dtype in (torch.float64, torch.float32)
+        s = torch.empty(n, dtype=torch.float64 if is_float else torch.int64, device=device)
+        hi = None if is_float else torch.empty(n, dtype=torch.int64, device=device)
+        mn = torch.empty(n, dtype=v.dtype, device=device)
+        mx = torch.empty(n, dtype=v.dtype, device=device)
+        mean = torch.empty(n, dtype=torch.float64, device=device)
+        outs.append(AggResult(s, hi, mn, mx, mean))
+        structs[i] = vdf_agg_out(_ptr(s), _ptr(hi), _ptr(mn), _ptr(mx), _ptr(mean))
+    return outs, structs
+
+
+class Context:
+    """One vdf_ctx: a device, a grow-only workspace and an error word."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        h = C.c_void_p()
+        self._check(lib.vdf_ctx_create(device, C.byref(h)), "vdf_ctx_create", ctx=None)
+        self.handle = h
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.vdf_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, status: int, what: str, ctx="self"):
+        if status != OK:
+            msg = lib.vdf_status_string(status).decode()
+            if ctx == "self" and getattr(self, "handle", None):
+                detail = lib.vdf_ctx_last_error(self.handle).decode()
+                if detail:
+                    msg += f" ({detail})"
+            raise VdfError(status, f"{what}: {msg}")
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib.vdf_ctx_kernel_launches(self.handle))
+
+    def check(self, stream=None):
+        self._check(lib.vdf_ctx_check(self.handle, _stream(stream)), "vdf_ctx_check")
+
+    def profile(self, enable: bool = True):
+        self._check(lib.vdf_ctx_profile(self.handle, 1 if enable else 0), "vdf_ctx_profile")
+
+    def profile_reset(self):
+        self._check(lib.vdf_ctx_profile_reset(self.handle), "vdf_ctx_profile_reset")
+
+    def profile_read(self) -> dict:
+        """{kernel class name: (total device ms, launches)}"""
+        out = {}
+        for cls, name in enumerate(KERNEL_CLASSES):
+            ms, cnt = C.c_double(0), C.c_uint64(0)
+            self._check(lib.vdf_ctx_profile_read(self.handle, cls, C.byref(ms), C.byref(cnt)), "profile_read")
+            out[name] = (ms.value, int(cnt.value))
+        return out
+
+    def reserve(self, nbytes: int):
+        self._check(lib.vdf_ctx_reserve(self.handle, nbytes), "vdf_ctx_reserve")
+
+    # ---- sort ----------------------------------------------------------------
+    def argsort(self, keys: Sequence[torch.Tensor], order: int = ORDER_ASC, perm_out=None,
+                sorted_keys_out: Optional[Sequence[Optional[torch.Tensor]]] = None, stream=None,
+                workspace: Optional[torch.Tensor] = None) -> torch.Tensor:
+        n = keys[0].numel() if keys else 0
+        dev = keys[0].device if keys else torch.device("cuda", self.device)
+        if perm_out is None:
+            perm_out = torch.empty(n, dtype=torch.int32, device=dev)
+        sko = _ptrs(sorted_keys_out) if sorted_keys_out is not None else None
+        if workspace is None:
+            st = lib.vdf_sort_argsort(self.handle, n, _cols(keys), len(keys), order, _ptr(perm_out), sko,
+                                      _stream(stream))
+        else:
+            st = lib.vdf_sort_argsort_ws(self.handle, n, _cols(keys), len(keys), order, _ptr(perm_out), sko,
+                                         _ptr(workspace), workspace.numel() * workspace.element_size(),
+                                         _stream(stream))
+        self._check(st, "vdf_sort_argsort")
+        return perm_out
+
+    def gather(self, perm: torch.Tensor, cols: Sequence[torch.Tensor], out=None, stream=None):
+        n = perm.numel()
+        if out is None:
+            out = [torch.empty(n, dtype=c.dtype, device=c.device) for c in cols]
+        self._check(lib.vdf_gather(self.handle, n, _ptr(perm), _cols(cols), len(cols), _ptrs(out), _stream(stream)),
+                    "vdf_gather")
+        return out
+
+    # ---- group-by ------------------------------------------------------------
+    def groupby_sorted(self, keys: Sequence[torch.Tensor], vals: Sequence[torch.Tensor], want_row_group=False,
+                       want_group_start=False, stream=None) -> GroupResult:
+        n = keys[0].numel()
+        dev = keys[0].device
+        gk = [torch.empty(n, dtype=k.dtype, device=dev) for k in keys]
+        cnt = torch.empty(n, dtype=torch.int64, device=dev)
+        aggs, structs = _alloc_aggs(vals, n, dev)
+        gs = torch.empty(n, dtype=torch.int32, device=dev) if want_group_start else None
+        rg = torch.empty(n, dtype=torch.int32, device=dev) if want_row_group else None
+        ng = C.c_uint64(0)
+        st = lib.vdf_groupby_sorted(self.handle, n, _cols(keys), len(keys), _cols(vals), len(vals), _ptrs(gk),
+                                    _ptr(cnt), structs, _ptr(gs), _ptr(rg), None, C.byref(ng), _stream(stream))
+        self._check(st, "vdf_groupby_sorted")
+        return GroupResult(int(ng.value), gk, cnt, aggs, gs, rg).trimmed()
+
+    def sort_groupby(self, keys: Sequence[torch.Tensor], payload: Sequence[torch.Tensor] = (),
+                     agg_cols: Sequence[int] = (), order: int = ORDER_ASC, groupby: bool = True,
+                     want_perm=True, want_sorted_keys=True, want_payload=True, want_row_group=False,
+                     want_group_start=False, stream=None, outputs: Optional[dict] = None) -> GroupResult:
+        """Sort + payload gather + group-by in one call.  `outputs` may carry
+        preallocated tensors (keys as in the returned GroupResult fields) so a
+        benchmark loop allocates nothing."""
+        n = keys[0].numel()
+        dev = keys[0].device
+        o = outputs if outputs is not None else self.alloc_sort_groupby_outputs(
+            keys, payload, agg_cols, groupby, want_perm, want_sorted_keys, want_payload, want_row_group,
+            want_group_start)
+        args = self.pack_sort_groupby(keys, payload, agg_cols, order, groupby, o)
+        self._check(lib.vdf_sort_groupby(self.handle, C.byref(args), _stream(stream)), "vdf_sort_groupby")
+        g = int(o["_ng"].value) if groupby else 0
+        res = GroupResult(g, o["gkeys"], o["count"], o["aggs"], o["gstart"], o["rgroup"], o["perm"],
+                          o["skeys"], o["pay"])
+        return res.trimmed() if groupby else res
+
+    def alloc_sort_groupby_outputs(self, keys, payload, agg_cols, groupby=True, want_perm=True,
+                                   want_sorted_keys=True, want_payload=True, want_row_group=False,
+                                   want_group_start=False) -> dict:
+        n = keys[0].numel()
+        dev = keys[0].device
+        o = {
+            "perm": torch.empty(n, dtype=torch.int32, device=dev) if want_perm else None,
+            "skeys": [torch.empty(n, dtype=k.dtype, device=dev) for k in keys] if want_sorted_keys else [],
+            "pay": [torch.empty(n, dtype=p.dtype, device=dev) for p in payload] if want_payload else [],
+            "gkeys": [], "count": None, "aggs": [], "gstart": None, "rgroup": None,
+        }
+        if groupby:
+            o["gkeys"] = [torch.empty(n, dtype=k.dtype, device=dev) for k in keys]
+            o["count"] = torch.empty(n, dtype=torch.int64, device=dev)
+            o["aggs"], o["_structs"] = _alloc_aggs([payload[i] for i in agg_cols], n, dev)
+            o["gstart"] = torch.empty(n, dtype=torch.int32, device=dev) if want_group_start else None
+            o["rgroup"] = torch.empty(n, dtype=torch.int32, device=dev) if want_row_group else None
+        return o
+
+    def pack_sort_groupby(self, keys, payload, agg_cols, order, groupby, o, host_count=True):
+        n = keys[0].numel()
+        a = vdf_sort_groupby_args()
+        kc, pc = _cols(keys), _cols(payload)
+        o["_keep"] = [kc, pc]
+        a.n = n
+        a.keys, a.nkeys, a.order = kc, len(keys), order
+        a.payload, a.npayload = pc, len(payload)
+        a.perm_out = _ptr(o["perm"])
+        if o["skeys"]:
+            sk = _ptrs(o["skeys"]); o["_keep"].append(sk); a.sorted_keys_out = sk
+        if o["pay"]:
+            pp = _ptrs(o["pay"]); o["_keep"].append(pp); a.payload_out = pp
+        a.groupby = 1 if groupby else 0
+        if groupby:
+            ac = (C.c_int32 * max(1, len(agg_cols)))(*agg_cols)
+            gk = _ptrs(o["gkeys"])
+            o["_keep"] += [ac, gk]
+            a.agg_cols, a.nagg = ac, len(agg_cols)
+            a.group_keys_out = gk
+            a.group_count_out = _ptr(o["count"])
+            a.aggs = o["_structs"]
+            a.group_start_out = _ptr(o["gstart"])
+            a.row_group_out = _ptr(o["rgroup"])
+            o["_ng"] = C.c_uint64(0)
+            if host_count:
+                a.n_groups_host = C.pointer(o["_ng"])
+            else:
+                o["ngroups_dev"] = torch.zeros(1, dtype=torch.int64, device=keys[0].device)
+                a.n_groups_dev = o["ngroups_dev"].data_ptr()
+        return a
+
+    def sort_groupby_packed(self, args, stream=None):
+        self._check(lib.vdf_sort_groupby(self.handle, C.byref(args), _stream(stream)), "vdf_sort_groupby")
+
+    def broadcast(self, row_group: torch.Tensor, group_vals: torch.Tensor, perm=None, out=None, stream=None):
+        n = row_group.numel()
+        if out is None:
+            out = torch.empty(n, dtype=group_vals.dtype, device=group_vals.device)
+        self._check(lib.vdf_broadcast(self.handle, n, _ptr(row_group), _ptr(group_vals), group_vals.numel(),
+                                      group_vals.element_size(), _ptr(perm), _ptr(out), _stream(stream)),
+                    "vdf_broadcast")
+        return out
+
+
+def header_functions() -> list[str]:
+    """Names of the functions include/vdf_capi.h declares."""
+    import re
+    text = HEADER_PATH.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(vdf_[a-z0-9_]+)\s*\(", text)))

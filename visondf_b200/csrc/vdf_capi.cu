@@ -1,0 +1,589 @@
+// vdf_capi.cu -- the extern "C" boundary declared in include/vdf_capi.h:
+// argument checks, the context (device, grow-only workspace, device error
+// word, launch counter) and the composition of the sort, gather and
+// segmented-reduction kernels into the public operations.
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "vdf_capi.h"
+#include "vdf_common.cuh"
+#include "vdf_internal.h"
+
+// Per-launch CUDA-event timing, enabled by vdf_ctx_profile().  Events come
+// from a pool and are resolved (synchronised) only when read.
+struct EventProfiler final : vdf::Profiler {
+    std::vector<cudaEvent_t> pool;
+    size_t used = 0;
+    struct Pending { int cls; size_t b, e; };
+    std::vector<Pending> pending;
+    double total_ms[vdf::KC_COUNT] = {};
+    uint64_t count[vdf::KC_COUNT] = {};
+    int open_cls = -1;
+    size_t open_b = 0;
+
+    cudaEvent_t next() {
+        if (used == pool.size()) {
+            cudaEvent_t ev;
+            if (cudaEventCreate(&ev) != cudaSuccess) return nullptr;
+            pool.push_back(ev);
+        }
+        return pool[used++];
+    }
+    void begin(int cls, cudaStream_t s) override {
+        cudaEvent_t ev = next();
+        if (!ev) return;
+        cudaEventRecord(ev, s);
+        open_cls = cls;
+        open_b = used - 1;
+    }
+    void end(int cls, cudaStream_t s) override {
+        if (open_cls != cls) return;
+        cudaEvent_t ev = next();
+        if (!ev) return;
+        cudaEventRecord(ev, s);
+        pending.push_back({cls, open_b, used - 1});
+        open_cls = -1;
+    }
+    cudaError_t resolve() {
+        for (const Pending& p : pending) {
+            cudaError_t e = cudaEventSynchronize(pool[p.e]);
+            if (e != cudaSuccess) return e;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, pool[p.b], pool[p.e]);
+            total_ms[p.cls] += ms;
+            count[p.cls]++;
+        }
+        pending.clear();
+        used = 0;
+        return cudaSuccess;
+    }
+    ~EventProfiler() override {
+        for (cudaEvent_t ev : pool) cudaEventDestroy(ev);
+    }
+};
+
+struct vdf_ctx {
+    int device = 0;
+    bool profiling = false;
+    EventProfiler prof;
+    std::mutex mu;
+    unsigned char* ws = nullptr;
+    size_t ws_cap = 0;
+    unsigned char* dev_small = nullptr;  // [0,4): error bits; [8,16): group count scratch
+    uint64_t* host_pinned = nullptr;     // [0]: group count, [1]: error bits
+    std::atomic<uint64_t> launches{0};
+    std::string last_error;
+};
+
+namespace {
+
+constexpr uint64_t kMaxRows = (1ull << 30) - 1;
+
+vdf_status fail(vdf_ctx* c, vdf_status s, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (c) c->last_error = buf;
+    return s;
+}
+
+vdf_status from_cuda(vdf_ctx* c, cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return VDF_OK;
+    vdf_status s = (e == cudaErrorMemoryAllocation) ? VDF_ERR_OOM : VDF_ERR_DEVICE;
+    return fail(c, s, "%s: %s", what, cudaGetErrorString(e));
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int d) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != d) cudaSetDevice(d);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+bool valid_dtype(int32_t dt) { return dt >= VDF_I32 && dt <= VDF_F32; }
+
+inline size_t align256(size_t x) { return (x + 255) / 256 * 256; }
+
+vdf::Profiler* prof_of(vdf_ctx* c) { return c->profiling ? &c->prof : nullptr; }
+
+uint32_t* err_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->dev_small); }
+uint64_t* count_word(vdf_ctx* c) { return reinterpret_cast<uint64_t*>(c->dev_small + 8); }
+
+vdf_status ws_ensure(vdf_ctx* c, size_t bytes) {
+    if (bytes <= c->ws_cap) return VDF_OK;
+    if (c->ws) {
+        cudaError_t e = cudaFree(c->ws);  // waits for work still using the old buffer
+        c->ws = nullptr;
+        c->ws_cap = 0;
+        if (e != cudaSuccess) return from_cuda(c, e, "cudaFree(workspace)");
+    }
+    size_t cap = align256(bytes + bytes / 8);
+    cudaError_t e = cudaMalloc(&c->ws, cap);
+    if (e != cudaSuccess) {
+        c->ws = nullptr;
+        cudaGetLastError();
+        return fail(c, VDF_ERR_OOM, "workspace allocation of %zu bytes failed: %s", cap, cudaGetErrorString(e));
+    }
+    c->ws_cap = cap;
+    return VDF_OK;
+}
+
+// Reads and clears the device error bits after the stream has drained.
+vdf_status drain_and_check(vdf_ctx* c, cudaStream_t s) {
+    cudaError_t e = cudaMemcpyAsync(&c->host_pinned[1], err_word(c), sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, "stream synchronize");
+    uint32_t bits = (uint32_t)c->host_pinned[1];
+    if (bits) {
+        cudaMemsetAsync(err_word(c), 0, sizeof(uint32_t), s);
+        cudaStreamSynchronize(s);
+        return fail(c, VDF_ERR_TIMEOUT, "device error bits 0x%x (look-back wait gave up or bad index)", bits);
+    }
+    return VDF_OK;
+}
+
+vdf_status check_keys(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys) {
+    if (nkeys < 1 || nkeys > vdf::kMaxKeys) return fail(c, VDF_ERR_INVALID_ARG, "nkeys must be 1..%d", vdf::kMaxKeys);
+    if (!keys) return fail(c, VDF_ERR_INVALID_ARG, "keys is NULL");
+    for (int k = 0; k < nkeys; ++k) {
+        if (!valid_dtype(keys[k].dtype)) return fail(c, VDF_ERR_INVALID_ARG, "key %d: bad dtype %d", k, keys[k].dtype);
+        if (n && !keys[k].data) return fail(c, VDF_ERR_INVALID_ARG, "key %d: NULL data", k);
+    }
+    return VDF_OK;
+}
+
+vdf_status check_rows(vdf_ctx* c, uint64_t n) {
+    if (n > kMaxRows) return fail(c, VDF_ERR_UNSUPPORTED, "n=%llu exceeds the %llu-row limit", (unsigned long long)n,
+                                  (unsigned long long)kMaxRows);
+    return VDF_OK;
+}
+
+// Sorted copies of key columns 1..nkeys-1 (column 0 is written by the last
+// radix pass) by gathering through the permutation.
+vdf_status emit_other_keys(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, const uint32_t* perm,
+                           void* const* sorted_keys_out, cudaStream_t s) {
+    if (!sorted_keys_out) return VDF_OK;
+    vdf::GatherArgs g{};
+    g.perm = perm;
+    g.err = err_word(c);
+    g.n = n;
+    for (int k = 1; k < nkeys; ++k) {
+        if (!sorted_keys_out[k]) continue;
+        g.src[g.ncols] = keys[k].data;
+        g.dst[g.ncols] = sorted_keys_out[k];
+        g.width[g.ncols] = vdf::dtype_width(keys[k].dtype);
+        g.ncols++;
+    }
+    if (!g.ncols) return VDF_OK;
+    c->launches++;
+    return from_cuda(c, vdf::run_gather(g, s, prof_of(c)), "gather keys");
+}
+
+vdf_status sort_impl(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, int order, uint32_t* perm_out,
+                     void* const* sorted_keys_out, unsigned char* ws, size_t ws_bytes, cudaStream_t s) {
+    int32_t dts[vdf::kMaxKeys];
+    const void* cols[vdf::kMaxKeys];
+    for (int k = 0; k < nkeys; ++k) {
+        dts[k] = keys[k].dtype;
+        cols[k] = keys[k].data;
+    }
+    vdf::SortPlan p = vdf::make_sort_plan(n, dts, nkeys);
+    if (ws_bytes < p.ws_bytes)
+        return fail(c, VDF_ERR_WORKSPACE, "workspace of %zu bytes < %zu needed", ws_bytes, p.ws_bytes);
+    void* key0_out = sorted_keys_out ? sorted_keys_out[0] : nullptr;
+    cudaError_t e = vdf::run_sort(p, cols, order, perm_out, key0_out, ws, err_word(c), s, prof_of(c));
+    c->launches += 2 + (uint64_t)p.total_passes;
+    if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
+    return emit_other_keys(c, n, keys, nkeys, perm_out, sorted_keys_out, s);
+}
+
+vdf_status finish_groups(vdf_ctx* c, uint64_t* n_groups_dev, uint64_t* n_groups_host, cudaStream_t s) {
+    if (!n_groups_host) return VDF_OK;
+    const uint64_t* src = n_groups_dev ? n_groups_dev : count_word(c);
+    cudaError_t e = cudaMemcpyAsync(&c->host_pinned[0], src, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return from_cuda(c, e, "read group count");
+    vdf_status st = drain_and_check(c, s);
+    if (st != VDF_OK) return st;
+    *n_groups_host = c->host_pinned[0];
+    return VDF_OK;
+}
+
+std::mutex g_prep_mu;
+bool g_prepared[64];
+
+}  // namespace
+
+extern "C" {
+
+uint32_t vdf_abi_version(void) { return VDF_ABI_VERSION; }
+
+const char* vdf_status_string(vdf_status s) {
+    switch (s) {
+    case VDF_OK: return "ok";
+    case VDF_ERR_INVALID_ARG: return "invalid argument";
+    case VDF_ERR_OOM: return "out of device memory";
+    case VDF_ERR_TIMEOUT: return "device wait timed out";
+    case VDF_ERR_DEVICE: return "CUDA error";
+    case VDF_ERR_UNSUPPORTED: return "unsupported";
+    case VDF_ERR_WORKSPACE: return "workspace too small";
+    }
+    return "unknown status";
+}
+
+uint64_t vdf_max_rows(void) { return kMaxRows; }
+
+size_t vdf_sort_workspace_bytes(uint64_t n, const int32_t* key_dtypes, int nkeys) {
+    if (!key_dtypes || nkeys < 1 || nkeys > vdf::kMaxKeys) return 0;
+    for (int k = 0; k < nkeys; ++k)
+        if (!valid_dtype(key_dtypes[k])) return 0;
+    return vdf::make_sort_plan(n, key_dtypes, nkeys).ws_bytes;
+}
+
+size_t vdf_groupby_workspace_bytes(uint64_t n, int nvals) {
+    if (nvals < 0 || nvals > vdf::kMaxVals) return 0;
+    return vdf::segreduce_workspace_bytes(n, nvals);
+}
+
+vdf_status vdf_ctx_create(int device, vdf_ctx** out) {
+    if (!out) return VDF_ERR_INVALID_ARG;
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return VDF_ERR_DEVICE;
+    }
+    if (device < 0 || device >= count || device >= 64) return VDF_ERR_INVALID_ARG;
+    vdf_ctx* c = new vdf_ctx();
+    c->device = device;
+    DeviceGuard g(device);
+    {
+        std::lock_guard<std::mutex> lk(g_prep_mu);
+        if (!g_prepared[device]) {
+            e = vdf::prepare_sort_kernels();
+            if (e != cudaSuccess) {
+                delete c;
+                return VDF_ERR_DEVICE;
+            }
+            g_prepared[device] = true;
+        }
+    }
+    if (cudaMalloc(&c->dev_small, 256) != cudaSuccess || cudaMemset(c->dev_small, 0, 256) != cudaSuccess ||
+        cudaMallocHost(&c->host_pinned, 2 * sizeof(uint64_t)) != cudaSuccess) {
+        cudaGetLastError();
+        if (c->dev_small) cudaFree(c->dev_small);
+        delete c;
+        return VDF_ERR_OOM;
+    }
+    *out = c;
+    return VDF_OK;
+}
+
+vdf_status vdf_ctx_destroy(vdf_ctx* c) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    {
+        std::lock_guard<std::mutex> lk(c->mu);
+        DeviceGuard g(c->device);
+        c->prof.resolve();
+        if (c->ws) cudaFree(c->ws);
+        if (c->dev_small) cudaFree(c->dev_small);
+        if (c->host_pinned) cudaFreeHost(c->host_pinned);
+    }
+    delete c;
+    return VDF_OK;
+}
+
+const char* vdf_ctx_last_error(const vdf_ctx* c) { return c ? c->last_error.c_str() : "null context"; }
+
+uint64_t vdf_ctx_kernel_launches(const vdf_ctx* c) { return c ? c->launches.load() : 0; }
+
+vdf_status vdf_ctx_profile(vdf_ctx* c, int enable) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->profiling = enable != 0;
+    return VDF_OK;
+}
+
+vdf_status vdf_ctx_profile_read(vdf_ctx* c, int cls, double* total_ms, uint64_t* launches) {
+    if (!c || cls < 0 || cls >= vdf::KC_COUNT) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    cudaError_t e = c->prof.resolve();
+    if (e != cudaSuccess) return from_cuda(c, e, "profile events");
+    if (total_ms) *total_ms = c->prof.total_ms[cls];
+    if (launches) *launches = c->prof.count[cls];
+    return VDF_OK;
+}
+
+vdf_status vdf_ctx_profile_reset(vdf_ctx* c) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    cudaError_t e = c->prof.resolve();
+    for (int k = 0; k < vdf::KC_COUNT; ++k) {
+        c->prof.total_ms[k] = 0;
+        c->prof.count[k] = 0;
+    }
+    return from_cuda(c, e, "profile events");
+}
+
+vdf_status vdf_ctx_reserve(vdf_ctx* c, size_t bytes) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    return ws_ensure(c, bytes);
+}
+
+vdf_status vdf_ctx_check(vdf_ctx* c, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    return drain_and_check(c, static_cast<cudaStream_t>(stream));
+}
+
+vdf_status vdf_sort_argsort_ws(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, int order,
+                               uint32_t* perm_out, void* const* sorted_keys_out, void* workspace,
+                               size_t workspace_bytes, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if ((st = check_keys(c, n, keys, nkeys)) != VDF_OK) return st;
+    if (order < VDF_ORDER_ASC || order > VDF_ORDER_DESC_REVERSE) return fail(c, VDF_ERR_INVALID_ARG, "bad order %d", order);
+    if (n == 0) return VDF_OK;
+    if (!perm_out) return fail(c, VDF_ERR_INVALID_ARG, "perm_out is NULL");
+    if (!workspace) return fail(c, VDF_ERR_INVALID_ARG, "workspace is NULL");
+    DeviceGuard g(c->device);
+    return sort_impl(c, n, keys, nkeys, order, perm_out, sorted_keys_out, static_cast<unsigned char*>(workspace),
+                     workspace_bytes, static_cast<cudaStream_t>(stream));
+}
+
+vdf_status vdf_sort_argsort(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, int order, uint32_t* perm_out,
+                            void* const* sorted_keys_out, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if ((st = check_keys(c, n, keys, nkeys)) != VDF_OK) return st;
+    if (order < VDF_ORDER_ASC || order > VDF_ORDER_DESC_REVERSE) return fail(c, VDF_ERR_INVALID_ARG, "bad order %d", order);
+    if (n == 0) return VDF_OK;
+    if (!perm_out) return fail(c, VDF_ERR_INVALID_ARG, "perm_out is NULL");
+    DeviceGuard g(c->device);
+    int32_t dts[vdf::kMaxKeys];
+    for (int k = 0; k < nkeys; ++k) dts[k] = keys[k].dtype;
+    const size_t need = vdf::make_sort_plan(n, dts, nkeys).ws_bytes;
+    if ((st = ws_ensure(c, need)) != VDF_OK) return st;
+    return sort_impl(c, n, keys, nkeys, order, perm_out, sorted_keys_out, c->ws, c->ws_cap,
+                     static_cast<cudaStream_t>(stream));
+}
+
+vdf_status vdf_gather(vdf_ctx* c, uint64_t n, const uint32_t* perm, const vdf_col* in, int ncols, void* const* out,
+                      void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if (ncols < 0 || ncols > vdf::kMaxGather) return fail(c, VDF_ERR_INVALID_ARG, "ncols must be 0..%d", vdf::kMaxGather);
+    if (n == 0 || ncols == 0) return VDF_OK;
+    if (!perm || !in || !out) return fail(c, VDF_ERR_INVALID_ARG, "NULL perm, in or out");
+    vdf::GatherArgs g{};
+    g.perm = perm;
+    g.err = err_word(c);
+    g.n = n;
+    g.ncols = ncols;
+    for (int i = 0; i < ncols; ++i) {
+        if (!valid_dtype(in[i].dtype) || !in[i].data || !out[i])
+            return fail(c, VDF_ERR_INVALID_ARG, "column %d: bad dtype or NULL pointer", i);
+        g.src[i] = in[i].data;
+        g.dst[i] = out[i];
+        g.width[i] = vdf::dtype_width(in[i].dtype);
+    }
+    DeviceGuard gd(c->device);
+    c->launches++;
+    return from_cuda(c, vdf::run_gather(g, static_cast<cudaStream_t>(stream), prof_of(c)), "gather");
+}
+
+vdf_status vdf_groupby_sorted(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, const vdf_col* vals, int nvals,
+                              void* const* group_keys_out, int64_t* count_out, const vdf_agg_out* aggs,
+                              uint32_t* group_start_out, uint32_t* row_group_out, uint64_t* n_groups_dev,
+                              uint64_t* n_groups_host, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if ((st = check_keys(c, n, keys, nkeys)) != VDF_OK) return st;
+    if (nvals < 0 || nvals > vdf::kMaxVals) return fail(c, VDF_ERR_INVALID_ARG, "nvals must be 0..%d", vdf::kMaxVals);
+    if (nvals && (!vals || !aggs)) return fail(c, VDF_ERR_INVALID_ARG, "vals/aggs NULL with nvals > 0");
+    for (int v = 0; v < nvals; ++v)
+        if (!valid_dtype(vals[v].dtype) || (n && !vals[v].data))
+            return fail(c, VDF_ERR_INVALID_ARG, "value %d: bad dtype or NULL data", v);
+    DeviceGuard g(c->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    vdf::SegArgs a{};
+    a.n = n;
+    a.perm = nullptr;
+    a.nkeys = nkeys;
+    a.nvals = nvals;
+    for (int k = 0; k < nkeys; ++k) {
+        a.key[k] = vdf::SegCol{keys[k].data, nullptr, keys[k].dtype, 0};
+        a.key_out[k] = group_keys_out ? group_keys_out[k] : nullptr;
+    }
+    for (int v = 0; v < nvals; ++v) {
+        a.val[v] = vdf::SegCol{vals[v].data, nullptr, vals[v].dtype, 0};
+        a.agg[v] = vdf::SegAggOut{aggs[v].sum, aggs[v].sum_hi, aggs[v].min, aggs[v].max, aggs[v].mean};
+    }
+    a.count_out = count_out;
+    a.group_start = group_start_out;
+    a.row_group = row_group_out;
+    a.n_groups = n_groups_dev ? n_groups_dev : (n_groups_host ? count_word(c) : nullptr);
+    a.err = err_word(c);
+    if (n) {
+        if ((st = ws_ensure(c, vdf::segreduce_workspace_bytes(n, nvals))) != VDF_OK) return st;
+        c->launches++;
+    }
+    cudaError_t e = vdf::run_segreduce(a, c->ws, s, prof_of(c));
+    if (e != cudaSuccess) return from_cuda(c, e, "segmented reduction");
+    return finish_groups(c, a.n_groups, n_groups_host, s);
+}
+
+vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* stream) {
+    if (!c || !x) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    const uint64_t n = x->n;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if ((st = check_keys(c, n, x->keys, x->nkeys)) != VDF_OK) return st;
+    if (x->order < VDF_ORDER_ASC || x->order > VDF_ORDER_DESC_REVERSE)
+        return fail(c, VDF_ERR_INVALID_ARG, "bad order %d", x->order);
+    if (x->npayload < 0 || x->npayload > vdf::kMaxGather)
+        return fail(c, VDF_ERR_INVALID_ARG, "npayload must be 0..%d", vdf::kMaxGather);
+    if (x->npayload && !x->payload) return fail(c, VDF_ERR_INVALID_ARG, "payload is NULL");
+    for (int p = 0; p < x->npayload; ++p)
+        if (!valid_dtype(x->payload[p].dtype) || (n && !x->payload[p].data))
+            return fail(c, VDF_ERR_INVALID_ARG, "payload %d: bad dtype or NULL data", p);
+    if (x->groupby) {
+        if (x->nagg < 0 || x->nagg > vdf::kMaxVals) return fail(c, VDF_ERR_INVALID_ARG, "nagg must be 0..%d", vdf::kMaxVals);
+        if (x->nagg && (!x->agg_cols || !x->aggs)) return fail(c, VDF_ERR_INVALID_ARG, "agg_cols/aggs NULL");
+        for (int i = 0; i < x->nagg; ++i)
+            if (x->agg_cols[i] < 0 || x->agg_cols[i] >= x->npayload)
+                return fail(c, VDF_ERR_INVALID_ARG, "agg_cols[%d]=%d out of range", i, x->agg_cols[i]);
+    }
+    DeviceGuard g(c->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        if (x->groupby && x->n_groups_dev) cudaMemsetAsync(x->n_groups_dev, 0, sizeof(uint64_t), s);
+        if (x->groupby && x->n_groups_host) *x->n_groups_host = 0;
+        return VDF_OK;
+    }
+
+    int32_t dts[vdf::kMaxKeys];
+    const void* cols[vdf::kMaxKeys];
+    for (int k = 0; k < x->nkeys; ++k) {
+        dts[k] = x->keys[k].dtype;
+        cols[k] = x->keys[k].data;
+    }
+    const vdf::SortPlan plan = vdf::make_sort_plan(n, dts, x->nkeys);
+    // workspace: [perm (internal)] [sorted key 0 (internal)] [max(sort, group-by)]
+    const bool own_perm = (x->perm_out == nullptr);
+    void* user_key0 = x->sorted_keys_out ? x->sorted_keys_out[0] : nullptr;
+    const bool own_key0 = x->groupby && !user_key0;
+    const size_t perm_bytes = own_perm ? align256(n * 4) : 0;
+    const size_t key0_bytes = own_key0 ? align256(n * 8) : 0;
+    const size_t seg_bytes = x->groupby ? vdf::segreduce_workspace_bytes(n, x->nagg) : 0;
+    const size_t tail = std::max(plan.ws_bytes, seg_bytes);
+    if ((st = ws_ensure(c, perm_bytes + key0_bytes + tail)) != VDF_OK) return st;
+    uint32_t* perm = own_perm ? reinterpret_cast<uint32_t*>(c->ws) : x->perm_out;
+    void* key0 = own_key0 ? static_cast<void*>(c->ws + perm_bytes) : user_key0;
+    unsigned char* tws = c->ws + perm_bytes + key0_bytes;
+
+    cudaError_t e = vdf::run_sort(plan, cols, x->order, perm, key0, tws, err_word(c), s, prof_of(c));
+    c->launches += 2 + (uint64_t)plan.total_passes;
+    if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
+
+    if (!x->groupby) {
+        if ((st = emit_other_keys(c, n, x->keys, x->nkeys, perm, x->sorted_keys_out, s)) != VDF_OK) return st;
+        if (x->payload_out) {
+            vdf::GatherArgs ga{};
+            ga.perm = perm;
+            ga.err = err_word(c);
+            ga.n = n;
+            for (int p = 0; p < x->npayload; ++p) {
+                if (!x->payload_out[p]) continue;
+                ga.src[ga.ncols] = x->payload[p].data;
+                ga.dst[ga.ncols] = x->payload_out[p];
+                ga.width[ga.ncols] = vdf::dtype_width(x->payload[p].dtype);
+                ga.ncols++;
+            }
+            if (ga.ncols) {
+                c->launches++;
+                if ((e = vdf::run_gather(ga, s, prof_of(c))) != cudaSuccess) return from_cuda(c, e, "gather payload");
+            }
+        }
+        return VDF_OK;
+    }
+
+    vdf::SegArgs a{};
+    a.n = n;
+    a.perm = perm;
+    a.nkeys = x->nkeys;
+    a.nvals = x->nagg;
+    for (int k = 0; k < x->nkeys; ++k) {
+        if (k == 0) a.key[k] = vdf::SegCol{key0, nullptr, x->keys[0].dtype, 0};
+        else a.key[k] = vdf::SegCol{x->keys[k].data, x->sorted_keys_out ? x->sorted_keys_out[k] : nullptr,
+                                    x->keys[k].dtype, 1};
+        a.key_out[k] = x->group_keys_out ? x->group_keys_out[k] : nullptr;
+    }
+    bool emitted[vdf::kMaxGather] = {false};
+    for (int i = 0; i < x->nagg; ++i) {
+        const int p = x->agg_cols[i];
+        void* emit = (x->payload_out && !emitted[p]) ? x->payload_out[p] : nullptr;
+        if (emit) emitted[p] = true;
+        a.val[i] = vdf::SegCol{x->payload[p].data, emit, x->payload[p].dtype, 1};
+        const vdf_agg_out& o = x->aggs[i];
+        a.agg[i] = vdf::SegAggOut{o.sum, o.sum_hi, o.min, o.max, o.mean};
+    }
+    for (int p = 0; p < x->npayload; ++p) {
+        if (!x->payload_out || !x->payload_out[p] || emitted[p]) continue;
+        a.extra[a.nextra++] = vdf::SegCol{x->payload[p].data, x->payload_out[p], x->payload[p].dtype, 1};
+        emitted[p] = true;
+    }
+    a.count_out = x->group_count_out;
+    a.group_start = x->group_start_out;
+    a.row_group = x->row_group_out;
+    a.n_groups = x->n_groups_dev ? x->n_groups_dev : (x->n_groups_host ? count_word(c) : nullptr);
+    a.err = err_word(c);
+    c->launches++;
+    if ((e = vdf::run_segreduce(a, tws, s, prof_of(c))) != cudaSuccess) return from_cuda(c, e, "segmented reduction");
+    return finish_groups(c, a.n_groups, x->n_groups_host, s);
+}
+
+vdf_status vdf_broadcast(vdf_ctx* c, uint64_t n, const uint32_t* row_group, const void* group_vals,
+                         uint64_t n_groups, int width, const uint32_t* perm, void* out, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if (width != 4 && width != 8) return fail(c, VDF_ERR_INVALID_ARG, "width must be 4 or 8");
+    if (n == 0) return VDF_OK;
+    if (!row_group || !group_vals || !out) return fail(c, VDF_ERR_INVALID_ARG, "NULL row_group, group_vals or out");
+    DeviceGuard g(c->device);
+    c->launches++;
+    return from_cuda(c, vdf::run_broadcast(row_group, n, group_vals, n_groups, width, perm, out, err_word(c),
+                                           static_cast<cudaStream_t>(stream), prof_of(c)),
+                     "broadcast");
+}
+
+}  // extern "C"

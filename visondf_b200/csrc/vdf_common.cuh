@@ -1,0 +1,107 @@
+// vdf_common.cuh -- device helpers shared by the sort, gather and group-by
+// kernels: column dtypes, order-preserving key images, acquire/release
+// accesses for the decoupled look-back, and bounded waits.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vdf {
+
+// Column dtypes.  Codes match vdf_dtype in include/vdf_capi.h.
+enum Dtype : int { I32 = 0, I64 = 1, U32 = 2, U64 = 3, F64 = 4, F32 = 5 };
+
+__host__ __device__ inline int dtype_width(int dt) {
+    return (dt == I32 || dt == U32 || dt == F32) ? 4 : (dt == I64 || dt == U64 || dt == F64) ? 8 : 0;
+}
+
+// Order-preserving unsigned image of a raw key (sort_integers.inl:46 flips the
+// sign bit of signed integers; sort_uintegers copies; sort_flt.inl:123-129
+// maps IEEE doubles with bits ^ (mask(sign) | signbit)).  `invert` gives the
+// stable descending order (all bits flipped).
+__device__ __forceinline__ uint32_t order32(uint32_t raw, int dt, bool invert) {
+    uint32_t k;
+    if (dt == I32) k = raw ^ 0x80000000u;
+    else if (dt == F32) k = raw ^ ((0u - (raw >> 31)) | 0x80000000u);
+    else k = raw;
+    return invert ? ~k : k;
+}
+__device__ __forceinline__ uint64_t order64(uint64_t raw, int dt, bool invert) {
+    uint64_t k;
+    if (dt == I64) k = raw ^ 0x8000000000000000ull;
+    else if (dt == F64) k = raw ^ ((0ull - (raw >> 63)) | 0x8000000000000000ull);
+    else k = raw;
+    return invert ? ~k : k;
+}
+// Inverses of the above (used when the last radix pass writes raw sorted keys).
+__device__ __forceinline__ uint32_t unorder32(uint32_t k, int dt, bool invert) {
+    if (invert) k = ~k;
+    if (dt == I32) return k ^ 0x80000000u;
+    if (dt == F32) return (k & 0x80000000u) ? (k ^ 0x80000000u) : ~k;
+    return k;
+}
+__device__ __forceinline__ uint64_t unorder64(uint64_t k, int dt, bool invert) {
+    if (invert) k = ~k;
+    if (dt == I64) return k ^ 0x8000000000000000ull;
+    if (dt == F64) return (k & 0x8000000000000000ull) ? (k ^ 0x8000000000000000ull) : ~k;
+    return k;
+}
+
+template <typename K> struct KeyOps;
+template <> struct KeyOps<uint32_t> {
+    static __device__ __forceinline__ uint32_t order(uint32_t r, int dt, bool inv) { return order32(r, dt, inv); }
+    static __device__ __forceinline__ uint32_t unorder(uint32_t k, int dt, bool inv) { return unorder32(k, dt, inv); }
+};
+template <> struct KeyOps<uint64_t> {
+    static __device__ __forceinline__ uint64_t order(uint64_t r, int dt, bool inv) { return order64(r, dt, inv); }
+    static __device__ __forceinline__ uint64_t unorder(uint64_t k, int dt, bool inv) { return unorder64(k, dt, inv); }
+};
+
+// ---- memory-model helpers for the decoupled look-back ---------------------
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
+    uint32_t v;
+    asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
+    asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Streaming (evict-first) loads/stores for data touched exactly once.
+template <typename T> __device__ __forceinline__ T ldg_stream(const T* p) { return __ldcs(p); }
+template <typename T> __device__ __forceinline__ void stg_stream(T* p, T v) { __stcs(p, v); }
+
+// Bounded waits: every spin in these kernels gives up after this many polls
+// (each poll sleeps 32-128 ns, so about 0.1 s), records an error bit in the
+// context's error word and carries on, so a broken dependency ends the kernel
+// with an error status instead of hanging the GPU.  Legitimate waits on an
+// earlier tile last microseconds.
+constexpr uint32_t kSpinLimit = 1u << 20;
+enum ErrBits : uint32_t { ERR_LOOKBACK_TIMEOUT = 1u, ERR_BAD_INDEX = 2u };
+
+__device__ __forceinline__ void backoff(uint32_t it) {
+    __nanosleep(it < 16 ? 32 : 128);
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+}  // namespace vdf

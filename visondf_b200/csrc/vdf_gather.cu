@@ -1,0 +1,123 @@
+// vdf_gather.cu -- payload gather by a permutation, and the group-by
+// "transform" broadcast.
+//
+// k_gather replaces the reference's permute_block_mt
+// (V/inlines/transform/sort_by/permute_block_mt.inl:3-47) and
+// no_inplace_permutation (V/inlines/no_inplace_permutation.inl:3-79), which
+// apply the sort's idx to every column of a type block with AVX-512 gathers.
+// Here one launch serves up to kMaxGather columns of mixed width: each thread
+// owns 4 consecutive output rows, reads their 4 row ids with one 16-byte load
+// (the permutation is read once for all columns), issues the 4 random reads
+// per column back to back, and writes each column's 4 results with 16-byte
+// stores.
+//
+// k_broadcast produces the reference's transform output
+// (CreateValueCol::apply, V/inlines/transform/transform_group_by/
+// create_value_col.inl:36-61: v_col[i] = lookup.at(key_vec[i])): every row
+// receives its group's aggregate, in sorted order or scattered back to the
+// original row order through the permutation.
+#include "vdf_common.cuh"
+#include "vdf_internal.h"
+
+namespace vdf {
+
+template <bool VEC>
+__global__ void __launch_bounds__(256) k_gather(GatherArgs g) {
+    const uint64_t r0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    if (r0 >= g.n) return;
+    if (VEC && r0 + 4 <= g.n) {
+        uint4 p = ldg_stream(reinterpret_cast<const uint4*>(g.perm + r0));
+        if (p.x >= g.n || p.y >= g.n || p.z >= g.n || p.w >= g.n) {  // not a permutation of [0, n)
+            if (g.err) atomicOr(g.err, ERR_BAD_INDEX);
+            p.x = p.x < g.n ? p.x : 0;
+            p.y = p.y < g.n ? p.y : 0;
+            p.z = p.z < g.n ? p.z : 0;
+            p.w = p.w < g.n ? p.w : 0;
+        }
+#pragma unroll 1
+        for (int c = 0; c < g.ncols; ++c) {
+            if (g.width[c] == 8) {
+                const unsigned long long* s = static_cast<const unsigned long long*>(g.src[c]);
+                ulonglong2 a, b;
+                a.x = __ldg(s + p.x);
+                a.y = __ldg(s + p.y);
+                b.x = __ldg(s + p.z);
+                b.y = __ldg(s + p.w);
+                ulonglong2* d = reinterpret_cast<ulonglong2*>(static_cast<unsigned long long*>(g.dst[c]) + r0);
+                stg_stream(d, a);
+                stg_stream(d + 1, b);
+            } else {
+                const uint32_t* s = static_cast<const uint32_t*>(g.src[c]);
+                uint4 v;
+                v.x = __ldg(s + p.x);
+                v.y = __ldg(s + p.y);
+                v.z = __ldg(s + p.z);
+                v.w = __ldg(s + p.w);
+                stg_stream(reinterpret_cast<uint4*>(static_cast<uint32_t*>(g.dst[c]) + r0), v);
+            }
+        }
+        return;
+    }
+    const uint64_t r1 = r0 + 4 < g.n ? r0 + 4 : g.n;
+    for (uint64_t r = r0; r < r1; ++r) {
+        uint32_t p = g.perm[r];
+        if (p >= g.n) {
+            if (g.err) atomicOr(g.err, ERR_BAD_INDEX);
+            p = 0;
+        }
+        for (int c = 0; c < g.ncols; ++c) {
+            if (g.width[c] == 8)
+                static_cast<unsigned long long*>(g.dst[c])[r] = __ldg(static_cast<const unsigned long long*>(g.src[c]) + p);
+            else
+                static_cast<uint32_t*>(g.dst[c])[r] = __ldg(static_cast<const uint32_t*>(g.src[c]) + p);
+        }
+    }
+}
+
+cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof) {
+    if (g.n == 0 || g.ncols == 0) return cudaSuccess;
+    bool vec = (reinterpret_cast<uintptr_t>(g.perm) & 15) == 0;
+    for (int c = 0; c < g.ncols; ++c) vec = vec && (reinterpret_cast<uintptr_t>(g.dst[c]) & 15) == 0;
+    const uint64_t threads = (g.n + 3) / 4;
+    const uint32_t blocks = (uint32_t)((threads + 255) / 256);
+    if (prof) prof->begin(KC_GATHER, s);
+    if (vec) k_gather<true><<<blocks, 256, 0, s>>>(g);
+    else k_gather<false><<<blocks, 256, 0, s>>>(g);
+    if (prof) prof->end(KC_GATHER, s);
+    return cudaGetLastError();
+}
+
+template <int W>
+__global__ void __launch_bounds__(256) k_broadcast(const uint32_t* row_group, uint64_t n, const void* gvals,
+                                                   uint64_t n_groups, const uint32_t* perm, void* out,
+                                                   uint32_t* err) {
+    using T = typename std::conditional<W == 8, unsigned long long, uint32_t>::type;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; r < n; r += stride) {
+        const uint32_t g = row_group[r];
+        const uint64_t dst = perm ? perm[r] : r;
+        if (g >= n_groups || dst >= n) {
+            atomicOr(err, ERR_BAD_INDEX);
+            continue;
+        }
+        static_cast<T*>(out)[dst] = __ldg(static_cast<const T*>(gvals) + g);
+    }
+}
+
+cudaError_t run_broadcast(const uint32_t* row_group, uint64_t n, const void* group_vals, uint64_t n_groups,
+                          int width, const uint32_t* perm, void* out, uint32_t* err, cudaStream_t s,
+                          Profiler* prof) {
+    if (n == 0) return cudaSuccess;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    uint64_t want = (n + 255) / 256;
+    uint32_t blocks = (uint32_t)(want < (uint64_t)sms * 16 ? want : (uint64_t)sms * 16);
+    if (prof) prof->begin(KC_BROADCAST, s);
+    if (width == 8) k_broadcast<8><<<blocks, 256, 0, s>>>(row_group, n, group_vals, n_groups, perm, out, err);
+    else k_broadcast<4><<<blocks, 256, 0, s>>>(row_group, n, group_vals, n_groups, perm, out, err);
+    if (prof) prof->end(KC_BROADCAST, s);
+    return cudaGetLastError();
+}
+
+}  // namespace vdf

@@ -1,0 +1,142 @@
+// vdf_internal.h -- host/device structures shared by the .cu files of the
+// library.  Not part of the public C-ABI (that is include/vdf_capi.h).
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vdf {
+
+constexpr int kMaxKeys = 4;     // key columns per sort / group-by
+constexpr int kMaxVals = 4;     // aggregated value columns per group-by launch
+constexpr int kMaxGather = 8;   // columns per gather launch
+
+// Kernel classes for the optional per-launch timing (vdf_ctx_profile).
+enum KernelClass : int {
+    KC_HIST = 0, KC_SCAN = 1, KC_ONESWEEP32 = 2, KC_ONESWEEP64 = 3, KC_GATHER = 4, KC_SEGREDUCE = 5,
+    KC_BROADCAST = 6, KC_COUNT = 7
+};
+
+// Brackets kernel launches with CUDA events when profiling is enabled.
+struct Profiler {
+    virtual void begin(int cls, cudaStream_t s) = 0;
+    virtual void end(int cls, cudaStream_t s) = 0;
+    virtual ~Profiler() = default;
+};
+
+// ---- radix sort ------------------------------------------------------------
+enum InMode : int { IN_RAW = 0, IN_GATHER = 1, IN_BUF = 2 };
+
+struct HistCol {
+    const void* data;
+    int dtype;
+    int passes;
+    int pass_base;
+    int invert;
+};
+struct HistArgs {
+    HistCol col[kMaxKeys];
+    int ncols;
+    int total_passes;
+    uint64_t n;
+    uint32_t* hist;
+};
+
+struct PassArgs {
+    const void* keys_in;        // raw column (IN_RAW / IN_GATHER) or ordered-key buffer
+    const uint32_t* vals_in;    // row ids (IN_GATHER: current permutation; IN_BUF: buffer)
+    void* keys_out;             // ordered-key buffer, or raw sorted keys (final pass; may be null)
+    uint32_t* vals_out;         // row-id buffer, or the output permutation (final pass)
+    const uint32_t* bin_offsets;  // [RADIX] global exclusive bin starts for this digit
+    uint32_t* status;           // [tiles][RADIX] look-back words of this pass
+    uint32_t* status_next;      // the other status buffer, cleared for the next pass
+    uint32_t* tile_counter;     // tile ids in scheduling order
+    uint32_t* err;              // error bits (vdf::ErrBits)
+    uint64_t n;
+    uint32_t shift;
+    uint32_t status_rows;       // rows of status_next to clear
+    int dtype;
+    int invert;                 // stable descending: keys bit-inverted
+    int reverse;                // reference descending: output positions mirrored
+};
+
+struct SortPlan {
+    uint64_t n;
+    int nkeys;
+    int bits, radix;
+    int dtype[kMaxKeys], width[kMaxKeys], passes[kMaxKeys], pass_base[kMaxKeys];
+    int total_passes;
+    uint32_t max_tiles;
+    size_t off_keys[2], off_vals[2], off_offs, off_zero, off_hist, off_counters, off_status[2];
+    size_t zero_bytes;
+    size_t ws_bytes;
+};
+
+SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys);
+// Sorts; writes perm_out (and key0_out = raw sorted most-significant key, may
+// be null).  Bounded waits that give up OR their ErrBits into *err.
+cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
+                     void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof = nullptr);
+size_t sort_smem_bytes(int key_width);
+int sort_tile_rows(int key_width);
+cudaError_t prepare_sort_kernels();
+
+// ---- gather ----------------------------------------------------------------
+struct GatherArgs {
+    const uint32_t* perm;
+    uint32_t* err;     // error word for out-of-range row ids (may be null)
+    uint64_t n;
+    int ncols;
+    const void* src[kMaxGather];
+    void* dst[kMaxGather];
+    int width[kMaxGather];
+};
+cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof = nullptr);
+
+// ---- segmented reduction (group-by over sorted rows) -----------------------
+// A column of the sorted view.  Row r is src[perm[r]] when `gathered` is set
+// (the payload gather is fused into the reduction), else src[r].  When emit
+// is non-null the materialised sorted column is also written there.
+struct SegCol {
+    const void* src;
+    void* emit;
+    int dtype;
+    int gathered;
+};
+// Per value column outputs (device pointers, any may be null).
+struct SegAggOut {
+    void* sum;        // f64 (float columns) or int64 low word (integer columns)
+    int64_t* sum_hi;  // high word of the 128-bit integer sum
+    void* min;        // in the column's own dtype
+    void* max;
+    double* mean;
+};
+struct SegArgs {
+    uint64_t n;
+    const uint32_t* perm;      // sorted row -> source row, for gathered columns
+    int nkeys, nvals, nextra;
+    SegCol key[kMaxKeys];
+    SegCol val[kMaxVals];
+    SegCol extra[kMaxGather];  // emit-only payload columns
+    void* key_out[kMaxKeys];   // group key columns
+    int64_t* count_out;        // rows per group
+    SegAggOut agg[kMaxVals];
+    uint32_t* group_start;     // first sorted row of each group (may be null)
+    uint32_t* row_group;       // group index of each sorted row (may be null)
+    uint64_t* n_groups;        // device word: number of groups (may be null)
+    // workspace (filled by run_segreduce)
+    unsigned char* status;     // per-tile look-back records
+    uint32_t* tile_counter;
+    uint32_t* err;
+};
+size_t segreduce_workspace_bytes(uint64_t n, int nvals);
+// a.err must point at the caller's error word; the workspace fields of `a`
+// are filled here.
+cudaError_t run_segreduce(SegArgs a, unsigned char* ws, cudaStream_t s, Profiler* prof = nullptr);
+
+// ---- transform output (aggregate broadcast to rows) --------------------------
+cudaError_t run_broadcast(const uint32_t* row_group, uint64_t n, const void* group_vals, uint64_t n_groups,
+                          int width, const uint32_t* perm, void* out, uint32_t* err, cudaStream_t s,
+                          Profiler* prof = nullptr);
+
+}  // namespace vdf

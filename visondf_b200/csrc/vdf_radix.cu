@@ -1,0 +1,548 @@
+// vdf_radix.cu -- stable LSD radix argsort for sm_100a.
+//
+// Replaces the reference's radix_sort_uint{32,64}[_mt] family
+// (V/inlines/radix_sorts/radix_sort_uint64_mt.inl:6-166: per-pass histogram,
+// serial exclusive scan over 65,536 buckets, per-thread bucket offsets, stable
+// scatter of (key, size_t idx), swap + memcpy) with a single-pass-per-digit
+// ("onesweep") design:
+//
+//   1. k_digit_hist   one read of every key column computes the histograms of
+//                     ALL digit positions at once (a histogram does not depend
+//                     on row order, so the columns are read unpermuted).
+//   2. k_hist_scan    exclusive scan per digit position -> global bin offsets.
+//   3. k_onesweep     one launch per digit: each CTA ranks a tile of keys
+//                     (warp match/ballot, per-warp shared-memory counters),
+//                     publishes its per-bin counts early, resolves its global
+//                     per-bin base with a decoupled look-back over earlier
+//                     tiles, and scatters (key, u32 row id) through a
+//                     shared-memory reorder buffer so global writes are runs.
+//
+// Key transforms (sign flip / IEEE image / descending inversion) are applied
+// on the fly when a raw column is read, and undone when the last pass writes
+// raw sorted keys; no transformed copy of a column is ever materialised.
+// Multi-key sorts run least-significant key first; the first pass of each
+// later key reads its raw column through the current permutation.
+#include "vdf_common.cuh"
+#include "vdf_internal.h"
+
+namespace vdf {
+
+// ---------------------------------------------------------------------------
+// 1. all-digit histogram
+// ---------------------------------------------------------------------------
+template <int BITS>
+__global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
+    constexpr int RADIX = 1 << BITS;
+    constexpr uint32_t MASK = RADIX - 1;
+    extern __shared__ uint32_t sh_hist[];  // [total_passes][RADIX]
+    const int total = a.total_passes * RADIX;
+    for (int i = threadIdx.x; i < total; i += blockDim.x) sh_hist[i] = 0;
+    __syncthreads();
+
+    const uint64_t n = a.n;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (int c = 0; c < a.ncols; ++c) {
+        const HistCol col = a.col[c];
+        uint32_t* h = sh_hist + col.pass_base * RADIX;
+        const int w = dtype_width(col.dtype);
+        if (w == 4) {
+            const uint32_t* src = static_cast<const uint32_t*>(col.data);
+            for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+                uint32_t k = order32(ldg_stream(src + i), col.dtype, col.invert);
+#pragma unroll 4
+                for (int p = 0; p < col.passes; ++p) atomicAdd(&h[p * RADIX + ((k >> (p * BITS)) & MASK)], 1u);
+            }
+        } else {
+            const uint64_t* src = static_cast<const uint64_t*>(col.data);
+            for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+                uint64_t k = order64(ldg_stream(src + i), col.dtype, col.invert);
+#pragma unroll 8
+                for (int p = 0; p < col.passes; ++p)
+                    atomicAdd(&h[p * RADIX + (uint32_t)((k >> (p * BITS)) & MASK)], 1u);
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+        uint32_t v = sh_hist[i];
+        if (v) atomicAdd(&a.hist[i], v);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 2. exclusive scan of each digit position's histogram (one CTA per position)
+// ---------------------------------------------------------------------------
+template <int BITS>
+__global__ void __launch_bounds__(256) k_hist_scan(const uint32_t* hist, uint32_t* offs) {
+    constexpr int RADIX = 1 << BITS;
+    constexpr int PER = (RADIX + 255) / 256;
+    __shared__ uint32_t warp_tot[8];
+    const uint32_t* h = hist + (size_t)blockIdx.x * RADIX;
+    uint32_t* o = offs + (size_t)blockIdx.x * RADIX;
+    uint32_t v[PER];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        int b = threadIdx.x * PER + j;
+        v[j] = b < RADIX ? h[b] : 0;
+        sum += v[j];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += warp_tot[w];
+    uint32_t run = wbase + incl - sum;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        int b = threadIdx.x * PER + j;
+        if (b < RADIX) o[b] = run;
+        run += v[j];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3. onesweep pass
+// ---------------------------------------------------------------------------
+// Look-back status word: [31:30] flag, [29:0] count.  n < 2^30 is required.
+constexpr uint32_t ST_AGG = 1u << 30;
+constexpr uint32_t ST_INC = 2u << 30;
+constexpr uint32_t ST_CNT = (1u << 30) - 1;
+
+template <typename K, int BITS, int THREADS, int ITEMS>
+struct OnesweepCfg {
+    static constexpr int RADIX = 1 << BITS;
+    static constexpr int WARPS = THREADS / 32;
+    static constexpr int TILE = THREADS * ITEMS;
+    static constexpr int BPT = (RADIX + THREADS - 1) / THREADS;  // bins per thread
+    // shared memory: exchange buffer | per-warp counters | bin bases | misc
+    static constexpr size_t EX_BYTES = (size_t)TILE * (sizeof(K) > 4 ? sizeof(K) : 4);
+    static constexpr size_t CNT_BYTES = (size_t)WARPS * RADIX * 4;
+    static constexpr size_t GLOB_BYTES = (size_t)RADIX * 4;
+    static constexpr size_t SMEM = EX_BYTES + CNT_BYTES + GLOB_BYTES + 64 + WARPS * 4;
+};
+
+template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL>
+__global__ void __launch_bounds__(THREADS) k_onesweep(PassArgs a) {
+    using C = OnesweepCfg<K, BITS, THREADS, ITEMS>;
+    constexpr int RADIX = C::RADIX, WARPS = C::WARPS, TILE = C::TILE, BPT = C::BPT;
+    constexpr uint32_t MASK = RADIX - 1;
+    extern __shared__ __align__(16) unsigned char smem[];
+    K* ex_keys = reinterpret_cast<K*>(smem);
+    uint32_t* ex_vals = reinterpret_cast<uint32_t*>(smem);
+    uint32_t* wcnt = reinterpret_cast<uint32_t*>(smem + C::EX_BYTES);             // [WARPS][RADIX]
+    uint32_t* bglob = reinterpret_cast<uint32_t*>(smem + C::EX_BYTES + C::CNT_BYTES);  // [RADIX]
+    uint32_t* misc = bglob + RADIX;                                                   // [0]=tile
+    uint32_t* wsum = misc + 16;                                                       // [WARPS]
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) misc[0] = atomicAdd(a.tile_counter, 1u);
+    for (int i = tid; i < WARPS * RADIX; i += THREADS) wcnt[i] = 0;
+    __syncthreads();
+    const uint32_t tile = misc[0];
+    const uint64_t n = a.n;
+    const uint64_t tile_base = (uint64_t)tile * TILE;
+    const uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tile_base);
+
+    // Clear this tile's row of the other status buffer for the next pass
+    // (that buffer's previous user, the pass before this one, has finished).
+    // Rows tile, tile + gridDim.x, ... so that every row a later pass with
+    // more tiles could read is cleared too.
+    if (a.status_next)
+        for (uint32_t r = tile; r < a.status_rows; r += gridDim.x)
+            for (int b = tid; b < RADIX; b += THREADS) a.status_next[(size_t)r * RADIX + b] = 0;
+
+    // ---- load keys (warp-striped: item j of lane l is tile position
+    //      warp*ITEMS*32 + j*32 + l, so positions follow row order) ----------
+    K key[ITEMS];
+    uint32_t gval[ITEMS];  // IN_GATHER: the incoming permutation entries
+    const uint32_t wpos = (uint32_t)warp * ITEMS * 32;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = wpos + j * 32 + lane;
+        const uint64_t i = tile_base + pos;
+        key[j] = ~K(0);
+        gval[j] = 0;
+        if (pos < valid) {
+            if (IN_MODE == IN_RAW) {
+                key[j] = KeyOps<K>::order(ldg_stream(static_cast<const K*>(a.keys_in) + i), a.dtype, a.invert);
+            } else if (IN_MODE == IN_GATHER) {
+                uint32_t src = ldg_stream(a.vals_in + i);
+                if (src >= n) {  // never for a valid permutation
+                    atomicOr(a.err, ERR_BAD_INDEX);
+                    src = 0;
+                }
+                gval[j] = src;
+                key[j] = KeyOps<K>::order(__ldg(static_cast<const K*>(a.keys_in) + src), a.dtype, a.invert);
+            } else {
+                key[j] = ldg_stream(static_cast<const K*>(a.keys_in) + i);
+            }
+        }
+    }
+
+    // ---- warp-local ranks and per-warp digit counts (match/ballot) --------
+    uint32_t rank[ITEMS];
+    uint32_t* my_cnt = wcnt + warp * RADIX;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = wpos + j * 32 + lane;
+        const bool ok = pos < valid;
+        const uint32_t d = ok ? (uint32_t)((key[j] >> a.shift) & MASK) : (uint32_t)RADIX;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const int leader = __ffs(peers) - 1;
+        uint32_t base = 0;
+        if (lane == leader && ok) {
+            base = my_cnt[d];
+            my_cnt[d] = base + __popc(peers);
+        }
+        base = __shfl_sync(0xffffffffu, base, leader);
+        rank[j] = ok ? base + __popc(peers & lanemask_lt()) : pos;
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // ---- per-bin totals, early publish, tile-local bin starts --------------
+    uint32_t tot[BPT];
+    uint32_t tsum = 0;
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+        const int b = tid * BPT + k;
+        uint32_t run = 0;
+        if (b < RADIX) {
+#pragma unroll
+            for (int w = 0; w < WARPS; ++w) {
+                uint32_t c = wcnt[w * RADIX + b];
+                wcnt[w * RADIX + b] = run;
+                run += c;
+            }
+            uint32_t* st = a.status + (size_t)tile * RADIX + b;
+            st_relaxed_u32(st, (tile == 0 ? ST_INC : ST_AGG) | run);
+        }
+        tot[k] = run;
+        tsum += run;
+    }
+    // block exclusive scan of tsum over threads (bins are blocked per thread)
+    uint32_t incl = tsum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t wb = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) wb += (w < warp) ? wsum[w] : 0u;
+    uint32_t bstart[BPT];
+    {
+        uint32_t run = wb + incl - tsum;
+#pragma unroll
+        for (int k = 0; k < BPT; ++k) {
+            bstart[k] = run;
+            run += tot[k];
+            const int b = tid * BPT + k;
+            if (b < RADIX)
+#pragma unroll
+                for (int w = 0; w < WARPS; ++w) wcnt[w * RADIX + b] += bstart[k];
+        }
+    }
+
+    // ---- decoupled look-back per bin ---------------------------------------
+#pragma unroll
+    for (int k = 0; k < BPT; ++k) {
+        const int b = tid * BPT + k;
+        if (b >= RADIX) break;
+        uint32_t excl = 0;
+        if (tile > 0) {
+            int64_t p = (int64_t)tile - 1;
+            uint32_t spins = 0;
+            while (true) {
+                uint32_t s = ld_relaxed_u32(a.status + (size_t)p * RADIX + b);
+                if ((s & ~ST_CNT) == 0) {
+                    if (++spins > kSpinLimit) { atomicOr(a.err, ERR_LOOKBACK_TIMEOUT); break; }
+                    backoff(spins);
+                    continue;
+                }
+                excl += s & ST_CNT;
+                if ((s & ST_INC) || p == 0) break;
+                --p;
+            }
+            st_relaxed_u32(a.status + (size_t)tile * RADIX + b, ST_INC | (excl + tot[k]));
+        }
+        bglob[b] = a.bin_offsets[b] + excl - bstart[k];
+    }
+    __syncthreads();
+
+    // ---- key exchange through shared memory, then run-coalesced writes -----
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = wpos + j * 32 + lane;
+        const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
+        if (pos < valid) rank[j] += wcnt[warp * RADIX + d];
+        if (rank[j] >= (uint32_t)TILE) {  // never when the counts are consistent
+            atomicOr(a.err, ERR_BAD_INDEX);
+            rank[j] = pos;
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) ex_keys[rank[j]] = key[j];
+    __syncthreads();
+    uint32_t opos[ITEMS];
+    K* kout = static_cast<K*>(a.keys_out);
+#pragma unroll
+    for (int r = 0; r < ITEMS; ++r) {
+        const uint32_t i = r * THREADS + tid;
+        opos[r] = 0;
+        if (i < valid) {
+            const K k = ex_keys[i];
+            const uint32_t d = (uint32_t)((k >> a.shift) & MASK);
+            uint32_t p = bglob[d] + i;
+            if (p >= n) {  // only after a look-back timeout: never write out of bounds
+                atomicOr(a.err, ERR_BAD_INDEX);
+                p = 0xffffffffu;
+                opos[r] = p;
+                continue;
+            }
+            if (FINAL && a.reverse) p = (uint32_t)(n - 1) - p;
+            opos[r] = p;
+            if (FINAL) {
+                if (kout) stg_stream(kout + p, KeyOps<K>::unorder(k, a.dtype, a.invert));
+            } else {
+                stg_stream(kout + p, k);
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- value (row id) exchange -------------------------------------------
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = wpos + j * 32 + lane;
+        uint32_t v;
+        if (IN_MODE == IN_RAW) v = (uint32_t)(tile_base + pos);
+        else if (IN_MODE == IN_GATHER) v = gval[j];
+        else v = pos < valid ? ldg_stream(a.vals_in + tile_base + pos) : 0u;
+        ex_vals[rank[j]] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < ITEMS; ++r) {
+        const uint32_t i = r * THREADS + tid;
+        if (i < valid && opos[r] != 0xffffffffu) stg_stream(a.vals_out + opos[r], ex_vals[i]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kBits = 8;
+constexpr int kThreads32 = 256, kItems32 = 16;
+constexpr int kThreads64 = 256, kItems64 = 12;
+
+template <typename K, int THREADS, int ITEMS, int IN_MODE, bool FINAL>
+cudaError_t launch_pass(const PassArgs& a, uint32_t tiles, cudaStream_t s) {
+    using C = OnesweepCfg<K, kBits, THREADS, ITEMS>;
+    k_onesweep<K, kBits, THREADS, ITEMS, IN_MODE, FINAL><<<tiles, THREADS, C::SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <typename K, int THREADS, int ITEMS, int IN_MODE, bool FINAL>
+cudaError_t set_pass_attr() {
+    using C = OnesweepCfg<K, kBits, THREADS, ITEMS>;
+    return cudaFuncSetAttribute(k_onesweep<K, kBits, THREADS, ITEMS, IN_MODE, FINAL>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
+}
+
+template <typename K, int THREADS, int ITEMS>
+cudaError_t set_pass_attrs() {
+    cudaError_t e;
+    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_RAW, false>()) != cudaSuccess) return e;
+    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_GATHER, false>()) != cudaSuccess) return e;
+    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_BUF, false>()) != cudaSuccess) return e;
+    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_RAW, true>()) != cudaSuccess) return e;
+    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_GATHER, true>()) != cudaSuccess) return e;
+    return set_pass_attr<K, THREADS, ITEMS, IN_BUF, true>();
+}
+
+template <typename K, int THREADS, int ITEMS>
+cudaError_t dispatch_pass(const PassArgs& a, int in_mode, bool final_pass, uint32_t tiles, cudaStream_t s) {
+    if (final_pass) {
+        if (in_mode == IN_RAW) return launch_pass<K, THREADS, ITEMS, IN_RAW, true>(a, tiles, s);
+        if (in_mode == IN_GATHER) return launch_pass<K, THREADS, ITEMS, IN_GATHER, true>(a, tiles, s);
+        return launch_pass<K, THREADS, ITEMS, IN_BUF, true>(a, tiles, s);
+    }
+    if (in_mode == IN_RAW) return launch_pass<K, THREADS, ITEMS, IN_RAW, false>(a, tiles, s);
+    if (in_mode == IN_GATHER) return launch_pass<K, THREADS, ITEMS, IN_GATHER, false>(a, tiles, s);
+    return launch_pass<K, THREADS, ITEMS, IN_BUF, false>(a, tiles, s);
+}
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+}  // namespace
+
+int sort_tile_rows(int key_width) { return key_width == 4 ? kThreads32 * kItems32 : kThreads64 * kItems64; }
+
+SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys) {
+    SortPlan p{};
+    p.n = n;
+    p.nkeys = nkeys;
+    p.bits = kBits;
+    p.radix = 1 << kBits;
+    int maxw = 4;
+    int total = 0;
+    uint32_t max_tiles = 0;
+    for (int k = 0; k < nkeys; ++k) {
+        p.dtype[k] = dtypes[k];
+        p.width[k] = dtype_width(dtypes[k]);
+        p.passes[k] = (p.width[k] * 8 + kBits - 1) / kBits;
+        if (p.width[k] > maxw) maxw = p.width[k];
+        uint32_t t = (uint32_t)((n + sort_tile_rows(p.width[k]) - 1) / sort_tile_rows(p.width[k]));
+        if (t > max_tiles) max_tiles = t;
+    }
+    // passes are numbered in processing order (least-significant key first)
+    for (int k = nkeys - 1; k >= 0; --k) {
+        p.pass_base[k] = total;
+        total += p.passes[k];
+    }
+    p.total_passes = total;
+    p.max_tiles = max_tiles;
+    size_t off = 0;
+    const size_t A = 256;
+    p.off_keys[0] = off; off = align_up(off + n * (size_t)maxw, A);
+    p.off_keys[1] = off; off = align_up(off + n * (size_t)maxw, A);
+    p.off_vals[0] = off; off = align_up(off + n * 4, A);
+    p.off_vals[1] = off; off = align_up(off + n * 4, A);
+    p.off_offs = off; off = align_up(off + (size_t)total * p.radix * 4, A);
+    // zeroed region: hist | counters+err | status[0]
+    p.off_zero = off;
+    p.off_hist = off; off = align_up(off + (size_t)total * p.radix * 4, A);
+    p.off_counters = off; off = align_up(off + (size_t)(total + 1) * 4, A);
+    p.off_status[0] = off; off = align_up(off + (size_t)max_tiles * p.radix * 4, A);
+    p.zero_bytes = off - p.off_zero;
+    p.off_status[1] = off; off = align_up(off + (size_t)max_tiles * p.radix * 4, A);
+    p.ws_bytes = off;
+    return p;
+}
+
+cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
+                     void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof) {
+    const uint64_t n = p.n;
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(ws + p.off_zero, 0, p.zero_bytes, s);
+    if (e != cudaSuccess) return e;
+    uint32_t* hist = reinterpret_cast<uint32_t*>(ws + p.off_hist);
+    uint32_t* offs = reinterpret_cast<uint32_t*>(ws + p.off_offs);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(ws + p.off_counters);
+    uint32_t* status[2] = {reinterpret_cast<uint32_t*>(ws + p.off_status[0]),
+                           reinterpret_cast<uint32_t*>(ws + p.off_status[1])};
+    void* kbuf[2] = {ws + p.off_keys[0], ws + p.off_keys[1]};
+    uint32_t* vbuf[2] = {reinterpret_cast<uint32_t*>(ws + p.off_vals[0]),
+                         reinterpret_cast<uint32_t*>(ws + p.off_vals[1])};
+    const bool invert = (order == 1);
+    const bool reverse = (order == 2);
+
+    HistArgs h{};
+    h.n = n;
+    h.hist = hist;
+    h.ncols = p.nkeys;
+    h.total_passes = p.total_passes;
+    for (int k = 0; k < p.nkeys; ++k) {
+        h.col[k].data = key_cols[k];
+        h.col[k].dtype = p.dtype[k];
+        h.col[k].passes = p.passes[k];
+        h.col[k].pass_base = p.pass_base[k];
+        h.col[k].invert = invert;
+    }
+    {
+        size_t smem = (size_t)p.total_passes * p.radix * 4;
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        uint64_t want = (n + 511) / 512;
+        uint32_t grid = (uint32_t)(want < (uint64_t)sms * 4 ? want : (uint64_t)sms * 4);
+        if (grid == 0) grid = 1;
+        if (prof) prof->begin(KC_HIST, s);
+        k_digit_hist<kBits><<<grid, 512, smem, s>>>(h);
+        if (prof) prof->end(KC_HIST, s);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        if (prof) prof->begin(KC_SCAN, s);
+        k_hist_scan<kBits><<<p.total_passes, 256, 0, s>>>(hist, offs);
+        if (prof) prof->end(KC_SCAN, s);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
+
+    int kcur = -1, vcur = -1;
+    int g = 0;  // global pass counter (processing order)
+    for (int k = p.nkeys - 1; k >= 0; --k) {
+        const int w = p.width[k];
+        const uint32_t tiles = (uint32_t)((n + sort_tile_rows(w) - 1) / sort_tile_rows(w));
+        for (int q = 0; q < p.passes[k]; ++q, ++g) {
+            PassArgs a{};
+            a.n = n;
+            a.shift = (uint32_t)(q * p.bits);
+            a.dtype = p.dtype[k];
+            a.invert = invert;
+            a.reverse = reverse;
+            a.bin_offsets = offs + (size_t)g * p.radix;
+            a.status = status[g & 1];
+            a.status_next = (g + 1 < p.total_passes) ? status[(g + 1) & 1] : nullptr;
+            a.status_rows = p.max_tiles;
+            a.tile_counter = counters + g;
+            a.err = err;
+            int mode;
+            if (q == 0 && k == p.nkeys - 1) {
+                mode = IN_RAW;
+                a.keys_in = key_cols[k];
+                a.vals_in = nullptr;
+            } else if (q == 0) {
+                mode = IN_GATHER;
+                a.keys_in = key_cols[k];
+                a.vals_in = vbuf[vcur];
+            } else {
+                mode = IN_BUF;
+                a.keys_in = kbuf[kcur];
+                a.vals_in = vbuf[vcur];
+            }
+            const bool fin = (k == 0 && q == p.passes[k] - 1);
+            const int kn = (kcur < 0) ? 0 : kcur ^ 1;
+            const int vn = (vcur < 0) ? 0 : vcur ^ 1;
+            if (fin) {
+                a.keys_out = key0_out;
+                a.vals_out = perm_out;
+            } else {
+                a.keys_out = kbuf[kn];
+                a.vals_out = vbuf[vn];
+            }
+            if (prof) prof->begin(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
+            e = (w == 4) ? dispatch_pass<uint32_t, kThreads32, kItems32>(a, mode, fin, tiles, s)
+                         : dispatch_pass<uint64_t, kThreads64, kItems64>(a, mode, fin, tiles, s);
+            if (prof) prof->end(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
+            if (e != cudaSuccess) return e;
+            kcur = kn;
+            vcur = vn;
+        }
+    }
+    return cudaSuccess;
+}
+
+// Raises the dynamic shared-memory limit of every sort kernel on the current
+// device; called once per device before the first sort.
+cudaError_t prepare_sort_kernels() {
+    cudaError_t e = set_pass_attrs<uint32_t, kThreads32, kItems32>();
+    if (e != cudaSuccess) return e;
+    if ((e = set_pass_attrs<uint64_t, kThreads64, kItems64>()) != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_digit_hist<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+}
+
+size_t sort_smem_bytes(int key_width) {
+    return key_width == 4 ? OnesweepCfg<uint32_t, kBits, kThreads32, kItems32>::SMEM
+                          : OnesweepCfg<uint64_t, kBits, kThreads64, kItems64>::SMEM;
+}
+
+}  // namespace vdf

@@ -1,0 +1,540 @@
+// vdf_segreduce.cu -- sort-based group-by: segment boundaries + segmented
+// count / sum / min / max / mean over rows already in key order.
+//
+// The reference group-by is hash based (transform_group_by_onecol_mt.hpp:
+// 182-337 with AddLookupOneCol / OccLookupOneCol, onecol_functions.inl:4-86:
+// one ankerl map probe per row, per-thread maps merged serially,
+// merge_functions.inl:3-36; output via CreateValueCol, create_value_col.inl:
+// 36-61).  On the GPU the rows are first sorted, so each group is a contiguous
+// segment and the whole aggregation is one streaming pass ("reduce by key"):
+//
+//   * a row is a segment head when any key differs from the previous row;
+//   * each thread folds its ITEMS rows into an aggregate
+//       (heads, open-segment partial {count, per column sum/min/max}),
+//     combined with the associative reduce-by-key operator
+//       A (+) B = (A.heads + B.heads, B.heads ? B.partial : A.partial (+) B.partial);
+//   * a block scan gives each thread its in-tile prefix, and a decoupled
+//     look-back over earlier tiles' published aggregates (32 predecessors
+//     per warp step) gives the tile's global prefix: the number of groups
+//     before it and the partial of the segment that runs into it;
+//   * each thread then walks its rows once more and writes every segment
+//     that ends inside its rows (keys, count, sum, min, max, mean).
+//
+// Exactness: integer sums are 128-bit (lo, hi words); float sums are carried
+// as (sum, compensation) with an error-free TwoSum at every combine, so a
+// group's f64 sum is accurate to about one rounding of the exact value,
+// independent of how the rows were split over threads and tiles.
+//
+// Value columns, the second and later key columns and emit-only payload
+// columns may be read through the sort permutation (the payload gather is
+// fused here), and written out as materialised sorted columns on the way.
+#include "vdf_common.cuh"
+#include "vdf_internal.h"
+
+namespace vdf {
+
+namespace {
+
+enum VClass : int { VC_FLOAT = 0, VC_SINT = 1, VC_UINT = 2 };
+__device__ __forceinline__ int vclass(int dt) {
+    return (dt == F64 || dt == F32) ? VC_FLOAT : (dt == I32 || dt == I64) ? VC_SINT : VC_UINT;
+}
+__device__ __forceinline__ double as_f(uint64_t b) { return __longlong_as_double((long long)b); }
+__device__ __forceinline__ uint64_t as_b(double d) { return (uint64_t)__double_as_longlong(d); }
+
+// Canonical 64-bit image of a value: double bits for float columns, the
+// sign- or zero-extended integer otherwise.
+__device__ __forceinline__ uint64_t load_val(const void* src, int dt, uint64_t i) {
+    switch (dt) {
+    case I32: return (uint64_t)(int64_t)__ldg(static_cast<const int32_t*>(src) + i);
+    case U32: return (uint64_t)__ldg(static_cast<const uint32_t*>(src) + i);
+    case F32: return as_b((double)__ldg(static_cast<const float*>(src) + i));
+    default: return (uint64_t)__ldg(static_cast<const unsigned long long*>(src) + i);
+    }
+}
+// Raw bits of a key / emitted element (zero-extended).
+__device__ __forceinline__ uint64_t load_raw(const void* src, int w, uint64_t i) {
+    return w == 4 ? (uint64_t)__ldg(static_cast<const uint32_t*>(src) + i)
+                  : (uint64_t)__ldg(static_cast<const unsigned long long*>(src) + i);
+}
+__device__ __forceinline__ void store_raw(void* dst, int w, uint64_t i, uint64_t v) {
+    if (w == 4) static_cast<uint32_t*>(dst)[i] = (uint32_t)v;
+    else static_cast<unsigned long long*>(dst)[i] = v;
+}
+
+// Per value column accumulator words:
+//   float : w0 sum, w1 compensation, w2 min, w3 max   (double bits)
+//   int   : w0 sum low, w1 sum high (128-bit two's complement), w2 min, w3 max
+__device__ __forceinline__ void col_init(uint64_t* w, uint64_t x, int vc) {
+    w[0] = x;
+    w[1] = (vc == VC_SINT && (int64_t)x < 0) ? ~0ull : 0ull;  // 0.0 for floats
+    w[2] = x;
+    w[3] = x;
+}
+__device__ __forceinline__ void col_merge(uint64_t* a, const uint64_t* b, int vc) {
+    if (vc == VC_FLOAT) {
+        const double x = as_f(a[0]), y = as_f(b[0]);
+        const double s = __dadd_rn(x, y);
+        const double bp = __dsub_rn(s, x);
+        const double e = __dadd_rn(__dsub_rn(x, __dsub_rn(s, bp)), __dsub_rn(y, bp));  // TwoSum error
+        a[0] = as_b(s);
+        a[1] = as_b(__dadd_rn(__dadd_rn(as_f(a[1]), as_f(b[1])), e));
+        a[2] = as_b(fmin(as_f(a[2]), as_f(b[2])));
+        a[3] = as_b(fmax(as_f(a[3]), as_f(b[3])));
+    } else {
+        const uint64_t lo = a[0] + b[0];
+        a[1] = a[1] + b[1] + (lo < a[0] ? 1ull : 0ull);
+        a[0] = lo;
+        if (vc == VC_SINT) {
+            a[2] = (uint64_t)min((long long)a[2], (long long)b[2]);
+            a[3] = (uint64_t)max((long long)a[3], (long long)b[3]);
+        } else {
+            a[2] = min((unsigned long long)a[2], (unsigned long long)b[2]);
+            a[3] = max((unsigned long long)a[3], (unsigned long long)b[3]);
+        }
+    }
+}
+
+template <int NV>
+struct Agg {
+    uint32_t heads;  // segment heads in the covered rows
+    uint32_t cnt;    // rows of the open (last) segment inside the covered rows
+    uint64_t w[NV > 0 ? NV : 1][4];
+};
+
+template <int NV>
+__device__ __forceinline__ Agg<NV> agg_identity() {
+    Agg<NV> r;
+    r.heads = 0;
+    r.cnt = 0;
+#pragma unroll
+    for (int v = 0; v < (NV > 0 ? NV : 1); ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r.w[v][q] = 0;
+    return r;
+}
+
+// A is earlier in row order than B.
+template <int NV>
+__device__ __forceinline__ Agg<NV> agg_combine(const Agg<NV>& A, const Agg<NV>& B, const int* vc) {
+    Agg<NV> r;
+    r.heads = A.heads + B.heads;
+    if (B.heads > 0 || A.cnt == 0) {
+        r.cnt = B.cnt;
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) r.w[v][q] = B.w[v][q];
+    } else if (B.cnt == 0) {
+        r.cnt = A.cnt;
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) r.w[v][q] = A.w[v][q];
+    } else {
+        r.cnt = A.cnt + B.cnt;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) r.w[v][q] = A.w[v][q];
+            col_merge(r.w[v], B.w[v], vc[v]);
+        }
+    }
+    if (NV == 0) r.w[0][0] = 0;
+    return r;
+}
+
+template <int NV>
+__device__ __forceinline__ Agg<NV> agg_shfl_up(const Agg<NV>& a, int d) {
+    Agg<NV> r;
+    r.heads = __shfl_up_sync(0xffffffffu, a.heads, d);
+    r.cnt = __shfl_up_sync(0xffffffffu, a.cnt, d);
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r.w[v][q] = __shfl_up_sync(0xffffffffu, a.w[v][q], d);
+    return r;
+}
+template <int NV>
+__device__ __forceinline__ Agg<NV> agg_shfl_down(const Agg<NV>& a, int d) {
+    Agg<NV> r;
+    r.heads = __shfl_down_sync(0xffffffffu, a.heads, d);
+    r.cnt = __shfl_down_sync(0xffffffffu, a.cnt, d);
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r.w[v][q] = __shfl_down_sync(0xffffffffu, a.w[v][q], d);
+    return r;
+}
+template <int NV>
+__device__ __forceinline__ Agg<NV> agg_shfl(const Agg<NV>& a, int src) {
+    Agg<NV> r;
+    r.heads = __shfl_sync(0xffffffffu, a.heads, src);
+    r.cnt = __shfl_sync(0xffffffffu, a.cnt, src);
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) r.w[v][q] = __shfl_sync(0xffffffffu, a.w[v][q], src);
+    return r;
+}
+
+// Look-back record of one tile.  The aggregate and the inclusive prefix live
+// in separate slots, each written once before its flag is raised, so a
+// reader never sees a slot being overwritten.
+constexpr uint32_t REC_AGG = 1, REC_INC = 2;
+template <int NV>
+struct Rec {
+    uint32_t flag;
+    uint32_t pad;
+    Agg<NV> slot[2];  // [0] aggregate, [1] inclusive prefix
+};
+
+template <int NV>
+__device__ __forceinline__ void rec_write(Rec<NV>* r, const Agg<NV>& a, uint32_t flag) {
+    Agg<NV>* dst = &r->slot[flag == REC_INC ? 1 : 0];
+    st_relaxed_u32(&dst->heads, a.heads);
+    st_relaxed_u32(&dst->cnt, a.cnt);
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) st_relaxed_u64(&dst->w[v][q], a.w[v][q]);
+    __threadfence();
+    st_release_u32(&r->flag, flag);
+}
+template <int NV>
+__device__ __forceinline__ Agg<NV> rec_read(const Rec<NV>* r, uint32_t flag) {
+    const Agg<NV>* src = &r->slot[flag == REC_INC ? 1 : 0];
+    Agg<NV> a;
+    a.heads = ld_relaxed_u32(&src->heads);
+    a.cnt = ld_relaxed_u32(&src->cnt);
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) a.w[v][q] = ld_relaxed_u64(&src->w[v][q]);
+    if (NV == 0) a.w[0][0] = 0;
+    return a;
+}
+
+__device__ __forceinline__ double i128_to_double(uint64_t lo, uint64_t hi, bool is_signed) {
+    if (is_signed) {
+        if ((int64_t)hi == ((int64_t)lo >> 63)) return (double)(int64_t)lo;
+        return ldexp((double)(int64_t)hi, 64) + (double)lo;
+    }
+    if (hi == 0) return (double)lo;
+    return ldexp((double)hi, 64) + (double)lo;
+}
+
+template <int NV>
+__device__ __forceinline__ void emit_group(const SegArgs& a, uint32_t g, uint32_t cnt, const uint64_t (*w)[4],
+                                           const int* vc) {
+    if (a.count_out) a.count_out[g] = (int64_t)cnt;
+#pragma unroll
+    for (int v = 0; v < NV; ++v) {
+        const SegAggOut& o = a.agg[v];
+        const int dt = a.val[v].dtype;
+        if (vc[v] == VC_FLOAT) {
+            const double s = __dadd_rn(as_f(w[v][0]), as_f(w[v][1]));
+            if (o.sum) static_cast<double*>(o.sum)[g] = s;
+            if (o.mean) o.mean[g] = s / (double)cnt;
+            if (dt == F64) {
+                if (o.min) static_cast<double*>(o.min)[g] = as_f(w[v][2]);
+                if (o.max) static_cast<double*>(o.max)[g] = as_f(w[v][3]);
+            } else {
+                if (o.min) static_cast<float*>(o.min)[g] = (float)as_f(w[v][2]);
+                if (o.max) static_cast<float*>(o.max)[g] = (float)as_f(w[v][3]);
+            }
+        } else {
+            if (o.sum) static_cast<int64_t*>(o.sum)[g] = (int64_t)w[v][0];
+            if (o.sum_hi) o.sum_hi[g] = (int64_t)w[v][1];
+            if (o.mean) o.mean[g] = i128_to_double(w[v][0], w[v][1], vc[v] == VC_SINT) / (double)cnt;
+            const int wd = dtype_width(dt);
+            if (o.min) store_raw(o.min, wd, g, w[v][2]);
+            if (o.max) store_raw(o.max, wd, g, w[v][3]);
+        }
+    }
+}
+
+// Source row of sorted row r for gathered columns (bounds-checked: an entry
+// >= n can only come from a failed sort and is replaced by row 0).
+__device__ __forceinline__ uint64_t perm_row(const SegArgs& a, uint64_t r) {
+    if (!a.perm) return r;
+    const uint32_t s = __ldg(a.perm + r);
+    if (s >= a.n) {
+        atomicOr(a.err, ERR_BAD_INDEX);
+        return 0;
+    }
+    return s;
+}
+
+constexpr int kSegThreads = 256;
+constexpr int kSegItems = 4;
+
+template <int NK, int NV, int THREADS, int ITEMS>
+__global__ void __launch_bounds__(THREADS) k_segreduce(SegArgs a) {
+    constexpr int WARPS = THREADS / 32;
+    constexpr int TILE = THREADS * ITEMS;
+    __shared__ Agg<NV> s_warp[WARPS];
+    __shared__ Agg<NV> s_prefix;
+    __shared__ uint32_t s_tile;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t n = a.n;
+    const uint64_t row0 = (uint64_t)tile * TILE + (uint64_t)tid * ITEMS;
+    Rec<NV>* recs = reinterpret_cast<Rec<NV>*>(a.status);
+
+    int vc[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) vc[v] = vclass(a.val[v].dtype);
+    int kw[NK];
+#pragma unroll
+    for (int k = 0; k < NK; ++k) kw[k] = dtype_width(a.key[k].dtype);
+
+    // ---- phase A: load this thread's rows, emit fused gathers, find segment
+    //      heads and fold the rows into the thread aggregate.  Row data is not
+    //      kept live across the scan below (phase B reloads it from L1/L2). ---
+    uint32_t hmask = 0;
+    Agg<NV> t = agg_identity<NV>();
+    {
+        uint64_t key[ITEMS][NK];
+        uint64_t val[ITEMS][NV > 0 ? NV : 1];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint64_t r = row0 + j;
+#pragma unroll
+            for (int k = 0; k < NK; ++k) key[j][k] = 0;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) val[j][v] = 0;
+            if (r < n) {
+                const uint64_t src = perm_row(a, r);
+#pragma unroll
+                for (int k = 0; k < NK; ++k) {
+                    const SegCol& c = a.key[k];
+                    key[j][k] = load_raw(c.src, kw[k], c.gathered ? src : r);
+                    if (c.emit) store_raw(c.emit, kw[k], r, key[j][k]);
+                }
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    const SegCol& c = a.val[v];
+                    const uint64_t i = c.gathered ? src : r;
+                    val[j][v] = load_val(c.src, c.dtype, i);
+                    if (c.emit) {
+                        const int w = dtype_width(c.dtype);
+                        store_raw(c.emit, w, r, load_raw(c.src, w, i));
+                    }
+                }
+                for (int x = 0; x < a.nextra; ++x) {
+                    const SegCol& c = a.extra[x];
+                    const int w = dtype_width(c.dtype);
+                    store_raw(c.emit, w, r, load_raw(c.src, w, c.gathered ? src : r));
+                }
+            }
+        }
+        uint64_t prev[NK];
+#pragma unroll
+        for (int k = 0; k < NK; ++k) prev[k] = __shfl_up_sync(0xffffffffu, key[ITEMS - 1][k], 1);
+        if (lane == 0 && row0 > 0 && row0 < n) {
+            const uint64_t r = row0 - 1;
+            const uint64_t src = perm_row(a, r);
+#pragma unroll
+            for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], a.key[k].gathered ? src : r);
+        }
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint64_t r = row0 + j;
+            bool h = (r == 0);
+#pragma unroll
+            for (int k = 0; k < NK; ++k) h |= (j == 0 ? prev[k] : key[j - 1][k]) != key[j][k];
+            if (r < n && h) hmask |= 1u << j;
+        }
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (row0 + j >= n) break;
+            if ((hmask >> j) & 1u) {
+                t.heads++;
+                t.cnt = 1;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) col_init(t.w[v], val[j][v], vc[v]);
+            } else if (t.cnt == 0) {
+                t.cnt = 1;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) col_init(t.w[v], val[j][v], vc[v]);
+            } else {
+                t.cnt++;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    uint64_t one[4];
+                    col_init(one, val[j][v], vc[v]);
+                    col_merge(t.w[v], one, vc[v]);
+                }
+            }
+        }
+    }
+
+    // ---- block scan ---------------------------------------------------------
+    Agg<NV> incl = t;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        Agg<NV> o = agg_shfl_up(incl, d);
+        if (lane >= d) incl = agg_combine(o, incl, vc);
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    Agg<NV> lane_excl = agg_shfl_up(incl, 1);
+    if (lane == 0) lane_excl = agg_identity<NV>();
+    __syncthreads();
+    Agg<NV> wpre = agg_identity<NV>();
+    for (int w = 0; w < warp; ++w) wpre = agg_combine(wpre, s_warp[w], vc);
+    const Agg<NV> thr_excl = agg_combine(wpre, lane_excl, vc);
+
+    // ---- decoupled look-back (warp 0) ---------------------------------------
+    if (warp == 0) {
+        Agg<NV> total = agg_identity<NV>();
+        for (int w = 0; w < WARPS; ++w) total = agg_combine(total, s_warp[w], vc);
+        Agg<NV> X = agg_identity<NV>();
+        if (tile == 0) {
+            if (lane == 0) rec_write(&recs[0], total, REC_INC);
+        } else {
+            if (lane == 0) rec_write(&recs[tile], total, REC_AGG);
+            int64_t base = (int64_t)tile - 1;
+            while (true) {
+                const int64_t p = base - lane;
+                uint32_t f = REC_INC;
+                if (p >= 0) {
+                    uint32_t spins = 0;
+                    while ((f = ld_acquire_u32(&recs[p].flag)) == 0) {
+                        if (++spins > kSpinLimit) { atomicOr(a.err, ERR_LOOKBACK_TIMEOUT); f = REC_INC; break; }
+                        backoff(spins);
+                    }
+                }
+                const uint32_t incmask = __ballot_sync(0xffffffffu, f == REC_INC);
+                const int stop = incmask ? __ffs(incmask) - 1 : 31;
+                Agg<NV> r = agg_identity<NV>();
+                if (p >= 0 && lane <= stop) r = rec_read(&recs[p], f);
+                // chronological fold: higher lanes are older tiles
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    Agg<NV> o = agg_shfl_down(r, d);
+                    if (lane + d < 32) r = agg_combine(o, r, vc);
+                }
+                const Agg<NV> win = agg_shfl(r, 0);
+                X = agg_combine(win, X, vc);
+                if (incmask) break;
+                base -= 32;
+            }
+            if (lane == 0) rec_write(&recs[tile], agg_combine(X, total, vc), REC_INC);
+        }
+        if (lane == 0) s_prefix = X;
+    }
+    __syncthreads();
+
+    // ---- emit completed segments --------------------------------------------
+    const Agg<NV> pre = agg_combine(s_prefix, thr_excl, vc);
+    // Every row contributes at most one head, so a prefix claiming more heads
+    // (or a longer open segment) than rows before row0 can only come from a
+    // timed-out look-back: record it and write nothing rather than out of bounds.
+    if (row0 < n && (pre.heads > row0 || pre.cnt > row0 || (row0 > 0 && pre.heads == 0))) {
+        atomicOr(a.err, ERR_BAD_INDEX);
+        return;
+    }
+    uint32_t gid = pre.heads;
+    uint32_t cnt = pre.cnt;
+    uint64_t w[NV > 0 ? NV : 1][4];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[v][q] = pre.w[v][q];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint64_t r = row0 + j;
+        if (r >= n) break;
+        const uint64_t src = perm_row(a, r);
+        uint64_t val[NV > 0 ? NV : 1];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) val[v] = load_val(a.val[v].src, a.val[v].dtype, a.val[v].gathered ? src : r);
+        if ((hmask >> j) & 1u) {
+            if (gid > 0) emit_group<NV>(a, gid - 1, cnt, w, vc);
+            ++gid;
+#pragma unroll
+            for (int k = 0; k < NK; ++k)
+                if (a.key_out[k])
+                    store_raw(a.key_out[k], kw[k], gid - 1, load_raw(a.key[k].src, kw[k], a.key[k].gathered ? src : r));
+            if (a.group_start) a.group_start[gid - 1] = (uint32_t)r;
+            cnt = 1;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) col_init(w[v], val[v], vc[v]);
+        } else {
+            ++cnt;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                uint64_t one[4];
+                col_init(one, val[v], vc[v]);
+                col_merge(w[v], one, vc[v]);
+            }
+        }
+        if (a.row_group) a.row_group[r] = gid - 1;
+        if (r == n - 1) {
+            emit_group<NV>(a, gid - 1, cnt, w, vc);
+            if (a.n_groups) *a.n_groups = gid;
+        }
+    }
+}
+
+template <int NK, int NV>
+cudaError_t launch_seg(const SegArgs& a, uint32_t tiles, cudaStream_t s) {
+    k_segreduce<NK, NV, kSegThreads, kSegItems><<<tiles, kSegThreads, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+template <int NK>
+cudaError_t launch_seg_nv(const SegArgs& a, uint32_t tiles, cudaStream_t s) {
+    switch (a.nvals) {
+    case 0: return launch_seg<NK, 0>(a, tiles, s);
+    case 1: return launch_seg<NK, 1>(a, tiles, s);
+    case 2: return launch_seg<NK, 2>(a, tiles, s);
+    case 3: return launch_seg<NK, 3>(a, tiles, s);
+    default: return launch_seg<NK, 4>(a, tiles, s);
+    }
+}
+
+size_t rec_bytes(int nvals) {
+    switch (nvals) {
+    case 0: return sizeof(Rec<0>);
+    case 1: return sizeof(Rec<1>);
+    case 2: return sizeof(Rec<2>);
+    case 3: return sizeof(Rec<3>);
+    default: return sizeof(Rec<4>);
+    }
+}
+
+}  // namespace
+
+size_t segreduce_workspace_bytes(uint64_t n, int nvals) {
+    const uint64_t tiles = (n + kSegThreads * kSegItems - 1) / (kSegThreads * kSegItems);
+    return 256 + (size_t)tiles * rec_bytes(nvals);
+}
+
+cudaError_t run_segreduce(SegArgs a, unsigned char* ws, cudaStream_t s, Profiler* prof) {
+    cudaError_t e;
+    if (a.n == 0) {
+        if (a.n_groups) return cudaMemsetAsync(a.n_groups, 0, sizeof(uint64_t), s);
+        return cudaSuccess;
+    }
+    const size_t bytes = segreduce_workspace_bytes(a.n, a.nvals);
+    if ((e = cudaMemsetAsync(ws, 0, bytes, s)) != cudaSuccess) return e;
+    a.tile_counter = reinterpret_cast<uint32_t*>(ws);
+    a.status = ws + 256;
+    const uint32_t tiles = (uint32_t)((a.n + kSegThreads * kSegItems - 1) / (kSegThreads * kSegItems));
+    if (prof) prof->begin(KC_SEGREDUCE, s);
+    switch (a.nkeys) {
+    case 1: e = launch_seg_nv<1>(a, tiles, s); break;
+    case 2: e = launch_seg_nv<2>(a, tiles, s); break;
+    case 3: e = launch_seg_nv<3>(a, tiles, s); break;
+    default: e = launch_seg_nv<4>(a, tiles, s); break;
+    }
+    if (prof) prof->end(KC_SEGREDUCE, s);
+    return e;
+}
+
+}  // namespace vdf

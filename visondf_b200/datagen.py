@@ -1,0 +1,124 @@
+"""Seeded synthetic frames for the sort + group-by workloads.
+
+There is no public dataset for this path; every input is synthetic.  The
+seed of column c of workload w is 0xB200 + 16*w + c.  All generators return
+numpy arrays on the host (the benchmark pins and uploads them; tests compare
+GPU results with the CPU oracle on the same arrays).
+
+  w0  small frame: N=1,000,000; int32 key uniform over 10,000 distinct random
+      int32 (negatives included); f64 value N(0,1); int64 value U[-1e9, 1e9].
+  w1  two-key frame: N=100,000,000; key1 int64 = 64 random bits; key2 int32
+      Zipf(s=1.1) over 1,000,000 ranks (inverse-CDF table), rank r mapped to a
+      fixed random distinct int32; payload f64 N(0,1), int32 uniform, uint64
+      row id (= original row index).
+  w2a group-by frame: N=200,000,000; int64 key uniform over a pool of
+      50,000,000 distinct random int64; f64 lognormal(0,1); int64 U[0, 2^40).
+  w2b same values; int32 key from 16 distinct random int32 with a 90/10 skew:
+      2 hot keys take 45% of the rows each, the other 14 share 10%.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+SEED_BASE = 0xB200
+
+
+def seed(workload: int, column: int) -> int:
+    return SEED_BASE + 16 * workload + column
+
+
+def distinct_pool(rng: np.random.Generator, size: int, dtype) -> np.ndarray:
+    """`size` distinct random values of an integer dtype (full range)."""
+    info = np.iinfo(dtype)
+    out = np.empty(0, dtype=dtype)
+    while out.size < size:
+        extra = rng.integers(info.min, info.max, size=int((size - out.size) * 1.1) + 16, dtype=dtype,
+                             endpoint=True)
+        out = np.unique(np.concatenate([out, extra]))
+    rng.shuffle(out)
+    return out[:size]
+
+
+def zipf_ranks(rng: np.random.Generator, n: int, ranks: int, s: float) -> np.ndarray:
+    """n draws of a Zipf(s) rank in [0, ranks) by inverse-CDF table lookup."""
+    w = np.arange(1, ranks + 1, dtype=np.float64) ** (-s)
+    cdf = np.cumsum(w)
+    cdf /= cdf[-1]
+    u = rng.random(n)
+    r = np.searchsorted(cdf, u, side="right")
+    return np.minimum(r, ranks - 1).astype(np.int64)
+
+
+def frame_w0(n: int = 1_000_000, distinct: int = 10_000):
+    rng = np.random.default_rng(seed(0, 0))
+    pool = distinct_pool(rng, distinct, np.int32)
+    key = pool[rng.integers(0, distinct, size=n)]
+    v1 = np.random.default_rng(seed(0, 1)).standard_normal(n)
+    v2 = np.random.default_rng(seed(0, 2)).integers(-10**9, 10**9, size=n, dtype=np.int64, endpoint=True)
+    return {"key": key, "v1": v1, "v2": v2}
+
+
+def frame_w1(n: int = 100_000_000, ranks: int = 1_000_000, s: float = 1.1):
+    k1 = np.random.default_rng(seed(1, 0)).integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, size=n,
+                                                    dtype=np.int64, endpoint=True)
+    rng2 = np.random.default_rng(seed(1, 1))
+    pool = distinct_pool(rng2, ranks, np.int32)
+    k2 = pool[zipf_ranks(rng2, n, ranks, s)]
+    f = np.random.default_rng(seed(1, 2)).standard_normal(n)
+    i = np.random.default_rng(seed(1, 3)).integers(np.iinfo(np.int32).min, np.iinfo(np.int32).max, size=n,
+                                                   dtype=np.int32, endpoint=True)
+    rowid = np.arange(n, dtype=np.uint64)
+    return {"key1": k1, "key2": k2, "f64": f, "i32": i, "rowid": rowid}
+
+
+def values_w2(n: int):
+    v1 = np.exp(np.random.default_rng(seed(2, 1)).standard_normal(n))
+    v2 = np.random.default_rng(seed(2, 2)).integers(0, 1 << 40, size=n, dtype=np.int64)
+    return v1, v2
+
+
+def frame_w2a(n: int = 200_000_000, distinct: int = 50_000_000):
+    rng = np.random.default_rng(seed(2, 0))
+    pool = distinct_pool(rng, distinct, np.int64)
+    key = pool[rng.integers(0, distinct, size=n)]
+    v1, v2 = values_w2(n)
+    return {"key": key, "v1": v1, "v2": v2}
+
+
+def frame_w2b(n: int = 200_000_000):
+    rng = np.random.default_rng(seed(2, 3))
+    pool = distinct_pool(rng, 16, np.int32)
+    p = np.full(16, 0.10 / 14)
+    p[:2] = 0.45
+    key = pool[rng.choice(16, size=n, p=p)]
+    v1, v2 = values_w2(n)
+    return {"key": key, "v1": v1, "v2": v2}
+
+
+def keys_for(dist: str, dtype, n: int, rng: np.random.Generator) -> np.ndarray:
+    """Key columns for parity tests: uniform, few, equal, sorted, reversed, zipf, small."""
+    if np.dtype(dtype).kind == "f":
+        base = rng.standard_normal(n).astype(dtype)
+        if dist == "few":
+            base = np.array([-0.0, 0.0, -1.5, 2.25, np.inf, -np.inf], dtype=dtype)[rng.integers(0, 6, size=n)]
+        elif dist == "equal":
+            base = np.full(n, 3.5, dtype=dtype)
+    else:
+        info = np.iinfo(dtype)
+        if dist in ("uniform", "sorted", "reversed"):
+            base = rng.integers(info.min, info.max, size=n, dtype=dtype, endpoint=True)
+        elif dist == "few":
+            base = distinct_pool(rng, 7, dtype)[rng.integers(0, 7, size=n)]
+        elif dist == "equal":
+            base = np.full(n, info.max // 3, dtype=dtype)
+        elif dist == "zipf":
+            base = distinct_pool(rng, 1000, dtype)[zipf_ranks(rng, n, 1000, 1.1)]
+        elif dist == "small":
+            base = rng.integers(0, 300, size=n).astype(dtype)
+        else:
+            raise ValueError(dist)
+    if dist == "sorted":
+        base = np.sort(base, kind="stable")
+    elif dist == "reversed":
+        base = np.sort(base, kind="stable")[::-1].copy()
+    return base
