@@ -195,27 +195,38 @@ struct RefAgg {
     int64_t imin[4], imax[4];
 };
 
-// Restated reference group-by (see file header).  Keys: up to 4 columns,
-// packed per row into a byte string (the reference concatenates key bytes,
-// key_build.inl:3-110).  Values: up to 4 columns of dtype i32/i64/f64.
-// Returns the number of groups (first-appearance order is not exported; the
-// tests compare sums over groups).  out_checksum receives sum(count) and the
-// sum over groups of each value column's sum, as a quick cross-check.
+// Restated reference group-by (see file header).  Keys: up to 4 columns.  A
+// single key column is hashed as its raw bytes (onecol_functions.inl:77-80);
+// several key columns are concatenated per row, each followed by the '\x1F'
+// separator, as KeyBuildDiffType / KeyBuildSameType do (key_build.inl:3-110).
+// The reference's simd_hash copies up to 16 bytes into an 8-byte local for
+// keys of 9..16 bytes (simd_hash.hpp:18-22 called from :35-36), which
+// overflows the stack; such composite keys are zero-padded to 17 bytes so the
+// hash takes its well-defined long-key path.  Values: up to 4 columns of
+// dtype i32/i64/f64.  Returns the number of groups; out_checksum receives
+// sum(count) and the sum over groups of each value column's sum.
 int64_t ref_groupby(const void* const* keys, const int* kdt, int nkeys,
                     const void* const* vals, const int* vdt, int nvals,
                     size_t n, int cores, double* out_checksum) {
     if (nkeys < 1 || nkeys > 4 || nvals < 0 || nvals > 4 || cores < 1) return -1;
     size_t kw = 0;
     int off[4];
-    for (int k = 0; k < nkeys; ++k) { off[k] = int(kw); int w = width_of(kdt[k]); if (!w) return -1; kw += size_t(w); }
+    const bool composite = nkeys > 1;
+    for (int k = 0; k < nkeys; ++k) {
+        off[k] = int(kw);
+        int w = width_of(kdt[k]);
+        if (!w) return -1;
+        kw += size_t(w) + (composite ? 1 : 0);
+    }
+    if (kw > 8 && kw <= 16) kw = 17;
     for (int v = 0; v < nvals; ++v) if (vdt[v] != 0 && vdt[v] != 1 && vdt[v] != 4) return -1;
-    // Composite key bytes per row (KeyBuildDiffType builds one key string per row).
-    std::vector<unsigned char> kbuf(n * kw);
+    std::vector<unsigned char> kbuf(n * kw, 0);
     #pragma omp parallel for num_threads(cores)
     for (size_t i = 0; i < n; ++i)
         for (int k = 0; k < nkeys; ++k) {
             size_t w = size_t(width_of(kdt[k]));
             std::memcpy(&kbuf[i * kw + size_t(off[k])], static_cast<const unsigned char*>(keys[k]) + i * w, w);
+            if (composite) kbuf[i * kw + size_t(off[k]) + w] = 0x1F;
         }
     using Map = ankerl::unordered_dense::map<std::string_view, RefAgg, simd_hash>;
     std::vector<Map> maps(static_cast<size_t>(cores));

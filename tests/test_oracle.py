@@ -159,3 +159,21 @@ def test_oracle_first_appearance_order():
     assert list(og.keys[0]) == [5, 3, 9, 1]  # the ankerl map's insertion order
     og = ob.groupby([key], [], sorted_groups=True)
     assert list(og.keys[0]) == [1, 3, 5, 9]
+
+
+@pytest.mark.skipif(not ob.ref_available(), reason="reference shim not built (needs the reference tree)")
+@pytest.mark.parametrize("cores", [1, 5])
+def test_live_reference_groupby_multikey_checksums(cores):
+    # composite (int64, int32) keys: 14 bytes with the reference's separators
+    rng = np.random.default_rng(31)
+    n = 60_000
+    k1 = rng.integers(-3, 3, n).astype(np.int64)
+    k2 = rng.integers(0, 1000, n).astype(np.int32)
+    v1 = np.round(rng.standard_normal(n) * 1000) / 8.0
+    v2 = rng.integers(-10**6, 10**6, n).astype(np.int32)
+    g, chk = ob.ref_groupby([k1, k2], [v1, v2], cores=cores)
+    og = ob.groupby([k1, k2], [v1, v2])
+    assert g == og.n_groups
+    assert chk[0] == og.count.sum()
+    assert chk[1] == pytest.approx(og.sum[0].sum(), rel=1e-12)
+    assert chk[2] == float(og.sum[1].sum())

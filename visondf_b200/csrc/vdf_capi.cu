@@ -434,15 +434,14 @@ vdf_status vdf_groupby_sorted(vdf_ctx* c, uint64_t n, const vdf_col* keys, int n
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     vdf::SegArgs a{};
     a.n = n;
-    a.perm = nullptr;
     a.nkeys = nkeys;
     a.nvals = nvals;
     for (int k = 0; k < nkeys; ++k) {
-        a.key[k] = vdf::SegCol{keys[k].data, nullptr, keys[k].dtype, 0};
+        a.key[k] = vdf::SegCol{keys[k].data, keys[k].dtype};
         a.key_out[k] = group_keys_out ? group_keys_out[k] : nullptr;
     }
     for (int v = 0; v < nvals; ++v) {
-        a.val[v] = vdf::SegCol{vals[v].data, nullptr, vals[v].dtype, 0};
+        a.val[v] = vdf::SegCol{vals[v].data, vals[v].dtype};
         a.agg[v] = vdf::SegAggOut{aggs[v].sum, aggs[v].sum_hi, aggs[v].min, aggs[v].max, aggs[v].mean};
     }
     a.count_out = count_out;
@@ -496,69 +495,91 @@ vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* st
         cols[k] = x->keys[k].data;
     }
     const vdf::SortPlan plan = vdf::make_sort_plan(n, dts, x->nkeys);
-    // workspace: [perm (internal)] [sorted key 0 (internal)] [max(sort, group-by)]
+    // Sorted copies needed by the group-by that the caller did not ask for
+    // live in the workspace: [perm][key 0][keys 1..][aggregated payload][tail]
+    // where tail = max(sort workspace, group-by workspace).
     const bool own_perm = (x->perm_out == nullptr);
-    void* user_key0 = x->sorted_keys_out ? x->sorted_keys_out[0] : nullptr;
-    const bool own_key0 = x->groupby && !user_key0;
     const size_t perm_bytes = own_perm ? align256(n * 4) : 0;
-    const size_t key0_bytes = own_key0 ? align256(n * 8) : 0;
+    void* skey[vdf::kMaxKeys] = {};
+    void* spay[vdf::kMaxGather] = {};
+    size_t off = perm_bytes;
+    size_t key_off[vdf::kMaxKeys] = {}, pay_off[vdf::kMaxGather] = {};
+    bool key_own[vdf::kMaxKeys] = {}, pay_own[vdf::kMaxGather] = {};
+    for (int k = 0; k < x->nkeys; ++k) {
+        skey[k] = x->sorted_keys_out ? x->sorted_keys_out[k] : nullptr;
+        if (!skey[k] && x->groupby) {
+            key_own[k] = true;
+            key_off[k] = off;
+            off += align256(n * (size_t)vdf::dtype_width(x->keys[k].dtype));
+        }
+    }
+    bool aggregated[vdf::kMaxGather] = {};
+    if (x->groupby)
+        for (int i = 0; i < x->nagg; ++i) aggregated[x->agg_cols[i]] = true;
+    for (int p = 0; p < x->npayload; ++p) {
+        spay[p] = x->payload_out ? x->payload_out[p] : nullptr;
+        if (!spay[p] && aggregated[p]) {
+            pay_own[p] = true;
+            pay_off[p] = off;
+            off += align256(n * (size_t)vdf::dtype_width(x->payload[p].dtype));
+        }
+    }
     const size_t seg_bytes = x->groupby ? vdf::segreduce_workspace_bytes(n, x->nagg) : 0;
     const size_t tail = std::max(plan.ws_bytes, seg_bytes);
-    if ((st = ws_ensure(c, perm_bytes + key0_bytes + tail)) != VDF_OK) return st;
+    if ((st = ws_ensure(c, off + tail)) != VDF_OK) return st;
     uint32_t* perm = own_perm ? reinterpret_cast<uint32_t*>(c->ws) : x->perm_out;
-    void* key0 = own_key0 ? static_cast<void*>(c->ws + perm_bytes) : user_key0;
-    unsigned char* tws = c->ws + perm_bytes + key0_bytes;
+    for (int k = 0; k < x->nkeys; ++k)
+        if (key_own[k]) skey[k] = c->ws + key_off[k];
+    for (int p = 0; p < x->npayload; ++p)
+        if (pay_own[p]) spay[p] = c->ws + pay_off[p];
+    unsigned char* tws = c->ws + off;
 
-    cudaError_t e = vdf::run_sort(plan, cols, x->order, perm, key0, tws, err_word(c), s, prof_of(c));
+    cudaError_t e = vdf::run_sort(plan, cols, x->order, perm, skey[0], tws, err_word(c), s, prof_of(c));
     c->launches += 2 + (uint64_t)plan.total_passes;
     if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
 
-    if (!x->groupby) {
-        if ((st = emit_other_keys(c, n, x->keys, x->nkeys, perm, x->sorted_keys_out, s)) != VDF_OK) return st;
-        if (x->payload_out) {
-            vdf::GatherArgs ga{};
-            ga.perm = perm;
-            ga.err = err_word(c);
-            ga.n = n;
-            for (int p = 0; p < x->npayload; ++p) {
-                if (!x->payload_out[p]) continue;
-                ga.src[ga.ncols] = x->payload[p].data;
-                ga.dst[ga.ncols] = x->payload_out[p];
-                ga.width[ga.ncols] = vdf::dtype_width(x->payload[p].dtype);
-                ga.ncols++;
-            }
-            if (ga.ncols) {
-                c->launches++;
-                if ((e = vdf::run_gather(ga, s, prof_of(c))) != cudaSuccess) return from_cuda(c, e, "gather payload");
-            }
-        }
-        return VDF_OK;
-    }
+    // Gather the other key columns and the payload into sorted order, up to
+    // kMaxGather columns per launch (the permutation is read once per launch).
+    vdf::GatherArgs ga{};
+    ga.perm = perm;
+    ga.err = err_word(c);
+    ga.n = n;
+    auto flush = [&]() -> cudaError_t {
+        if (!ga.ncols) return cudaSuccess;
+        c->launches++;
+        cudaError_t ge = vdf::run_gather(ga, s, prof_of(c));
+        ga.ncols = 0;
+        return ge;
+    };
+    auto add = [&](const void* src, void* dst, int dtype) -> cudaError_t {
+        ga.src[ga.ncols] = src;
+        ga.dst[ga.ncols] = dst;
+        ga.width[ga.ncols] = vdf::dtype_width(dtype);
+        if (++ga.ncols == vdf::kMaxGather) return flush();
+        return cudaSuccess;
+    };
+    for (int k = 1; k < x->nkeys; ++k)
+        if (skey[k] && (e = add(x->keys[k].data, skey[k], x->keys[k].dtype)) != cudaSuccess)
+            return from_cuda(c, e, "gather keys");
+    for (int p = 0; p < x->npayload; ++p)
+        if (spay[p] && (e = add(x->payload[p].data, spay[p], x->payload[p].dtype)) != cudaSuccess)
+            return from_cuda(c, e, "gather payload");
+    if ((e = flush()) != cudaSuccess) return from_cuda(c, e, "gather");
+    if (!x->groupby) return VDF_OK;
 
     vdf::SegArgs a{};
     a.n = n;
-    a.perm = perm;
     a.nkeys = x->nkeys;
     a.nvals = x->nagg;
     for (int k = 0; k < x->nkeys; ++k) {
-        if (k == 0) a.key[k] = vdf::SegCol{key0, nullptr, x->keys[0].dtype, 0};
-        else a.key[k] = vdf::SegCol{x->keys[k].data, x->sorted_keys_out ? x->sorted_keys_out[k] : nullptr,
-                                    x->keys[k].dtype, 1};
+        a.key[k] = vdf::SegCol{skey[k], x->keys[k].dtype};
         a.key_out[k] = x->group_keys_out ? x->group_keys_out[k] : nullptr;
     }
-    bool emitted[vdf::kMaxGather] = {false};
     for (int i = 0; i < x->nagg; ++i) {
         const int p = x->agg_cols[i];
-        void* emit = (x->payload_out && !emitted[p]) ? x->payload_out[p] : nullptr;
-        if (emit) emitted[p] = true;
-        a.val[i] = vdf::SegCol{x->payload[p].data, emit, x->payload[p].dtype, 1};
+        a.val[i] = vdf::SegCol{spay[p], x->payload[p].dtype};
         const vdf_agg_out& o = x->aggs[i];
         a.agg[i] = vdf::SegAggOut{o.sum, o.sum_hi, o.min, o.max, o.mean};
-    }
-    for (int p = 0; p < x->npayload; ++p) {
-        if (!x->payload_out || !x->payload_out[p] || emitted[p]) continue;
-        a.extra[a.nextra++] = vdf::SegCol{x->payload[p].data, x->payload_out[p], x->payload[p].dtype, 1};
-        emitted[p] = true;
     }
     a.count_out = x->group_count_out;
     a.group_start = x->group_start_out;

@@ -94,14 +94,10 @@ struct GatherArgs {
 cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof = nullptr);
 
 // ---- segmented reduction (group-by over sorted rows) -----------------------
-// A column of the sorted view.  Row r is src[perm[r]] when `gathered` is set
-// (the payload gather is fused into the reduction), else src[r].  When emit
-// is non-null the materialised sorted column is also written there.
+// A column of rows in key order.
 struct SegCol {
     const void* src;
-    void* emit;
     int dtype;
-    int gathered;
 };
 // Per value column outputs (device pointers, any may be null).
 struct SegAggOut {
@@ -113,11 +109,9 @@ struct SegAggOut {
 };
 struct SegArgs {
     uint64_t n;
-    const uint32_t* perm;      // sorted row -> source row, for gathered columns
-    int nkeys, nvals, nextra;
+    int nkeys, nvals;
     SegCol key[kMaxKeys];
     SegCol val[kMaxVals];
-    SegCol extra[kMaxGather];  // emit-only payload columns
     void* key_out[kMaxKeys];   // group key columns
     int64_t* count_out;        // rows per group
     SegAggOut agg[kMaxVals];

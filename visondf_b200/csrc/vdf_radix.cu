@@ -129,7 +129,7 @@ struct OnesweepCfg {
 };
 
 template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL>
-__global__ void __launch_bounds__(THREADS) k_onesweep(PassArgs a) {
+__global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
     using C = OnesweepCfg<K, BITS, THREADS, ITEMS>;
     constexpr int RADIX = C::RADIX, WARPS = C::WARPS, TILE = C::TILE, BPT = C::BPT;
     constexpr uint32_t MASK = RADIX - 1;
@@ -186,15 +186,25 @@ __global__ void __launch_bounds__(THREADS) k_onesweep(PassArgs a) {
         }
     }
 
-    // ---- warp-local ranks and per-warp digit counts (match/ballot) --------
+    // ---- warp-local ranks and per-warp digit counts --------------------------
+    // Lanes holding the same digit are found with one ballot per digit bit
+    // (plus one for validity) instead of match.any, which issues on the
+    // narrow XU pipe; the lowest such lane updates the warp's counter.
     uint32_t rank[ITEMS];
     uint32_t* my_cnt = wcnt + warp * RADIX;
+    const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const uint32_t pos = wpos + j * 32 + lane;
         const bool ok = pos < valid;
-        const uint32_t d = ok ? (uint32_t)((key[j] >> a.shift) & MASK) : (uint32_t)RADIX;
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
+        uint32_t peers = __ballot_sync(0xffffffffu, ok);
+        if (!ok) peers = ~peers;
+#pragma unroll
+        for (int b = 0; b < BITS; ++b) {
+            const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? bal : ~bal;
+        }
         const int leader = __ffs(peers) - 1;
         uint32_t base = 0;
         if (lane == leader && ok) {
@@ -202,7 +212,7 @@ __global__ void __launch_bounds__(THREADS) k_onesweep(PassArgs a) {
             my_cnt[d] = base + __popc(peers);
         }
         base = __shfl_sync(0xffffffffu, base, leader);
-        rank[j] = ok ? base + __popc(peers & lanemask_lt()) : pos;
+        rank[j] = ok ? base + __popc(peers & lt) : pos;
         __syncwarp();
     }
     __syncthreads();

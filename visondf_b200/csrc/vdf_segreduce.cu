@@ -25,9 +25,10 @@
 // group's f64 sum is accurate to about one rounding of the exact value,
 // independent of how the rows were split over threads and tiles.
 //
-// Value columns, the second and later key columns and emit-only payload
-// columns may be read through the sort permutation (the payload gather is
-// fused here), and written out as materialised sorted columns on the way.
+// All columns are read in sorted row order (the fused sort + group-by call
+// gathers them first with the high-occupancy gather kernel: a random read
+// costs a full DRAM access of 64 bytes, so each gathered value is read
+// randomly exactly once and everything here is sequential).
 #include "vdf_common.cuh"
 #include "vdf_internal.h"
 
@@ -60,6 +61,57 @@ __device__ __forceinline__ uint64_t load_raw(const void* src, int w, uint64_t i)
 __device__ __forceinline__ void store_raw(void* dst, int w, uint64_t i, uint64_t v) {
     if (w == 4) static_cast<uint32_t*>(dst)[i] = (uint32_t)v;
     else static_cast<unsigned long long*>(dst)[i] = v;
+}
+
+// Rows row0 .. row0+ITEMS-1 of a column into arr[j][c] (raw bits, zero-
+// extended), with 16-byte vector loads when the rows are in bounds and
+// aligned (row0 is a multiple of ITEMS; tile starts are multiples of it).
+template <int ITEMS, int W>
+__device__ __forceinline__ void load_rows(const void* src, int w, uint64_t row0, uint64_t n, uint64_t (&arr)[ITEMS][W],
+                                          int c) {
+    const bool full = row0 + ITEMS <= n;
+    if (w == 8) {
+        const unsigned long long* p = static_cast<const unsigned long long*>(src) + row0;
+        if (full && ITEMS % 2 == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+#pragma unroll
+            for (int j = 0; j < ITEMS; j += 2) {
+                const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p + j));
+                arr[j][c] = v.x;
+                arr[j + 1][c] = v.y;
+            }
+            return;
+        }
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) arr[j][c] = row0 + j < n ? __ldg(p + j) : 0ull;
+    } else {
+        const uint32_t* p = static_cast<const uint32_t*>(src) + row0;
+        if (full && ITEMS % 4 == 0 && (reinterpret_cast<uintptr_t>(p) & 15) == 0) {
+#pragma unroll
+            for (int j = 0; j < ITEMS; j += 4) {
+                const uint4 v = __ldg(reinterpret_cast<const uint4*>(p + j));
+                arr[j][c] = v.x;
+                arr[j + 1][c] = v.y;
+                arr[j + 2][c] = v.z;
+                arr[j + 3][c] = v.w;
+            }
+            return;
+        }
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) arr[j][c] = row0 + j < n ? (uint64_t)__ldg(p + j) : 0ull;
+    }
+}
+
+// Canonical images (see load_val) of rows row0 .. row0+ITEMS-1.
+template <int ITEMS, int W>
+__device__ __forceinline__ void load_vals(const void* src, int dt, uint64_t row0, uint64_t n, uint64_t (&arr)[ITEMS][W],
+                                          int c) {
+    load_rows<ITEMS>(src, dtype_width(dt), row0, n, arr, c);
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint64_t x = arr[j][c];
+        if (dt == I32) arr[j][c] = (uint64_t)(int64_t)(int32_t)(uint32_t)x;
+        else if (dt == F32) arr[j][c] = as_b((double)__uint_as_float((uint32_t)x));
+    }
 }
 
 // Per value column accumulator words:
@@ -254,26 +306,14 @@ __device__ __forceinline__ void emit_group(const SegArgs& a, uint32_t g, uint32_
     }
 }
 
-// Source row of sorted row r for gathered columns (bounds-checked: an entry
-// >= n can only come from a failed sort and is replaced by row 0).
-__device__ __forceinline__ uint64_t perm_row(const SegArgs& a, uint64_t r) {
-    if (!a.perm) return r;
-    const uint32_t s = __ldg(a.perm + r);
-    if (s >= a.n) {
-        atomicOr(a.err, ERR_BAD_INDEX);
-        return 0;
-    }
-    return s;
-}
-
 constexpr int kSegThreads = 256;
 constexpr int kSegItems = 4;
 
 template <int NK, int NV, int THREADS, int ITEMS>
-__global__ void __launch_bounds__(THREADS) k_segreduce(SegArgs a) {
+__global__ void __launch_bounds__(THREADS, (NV >= 3 ? 1 : 2)) k_segreduce(SegArgs a) {
     constexpr int WARPS = THREADS / 32;
     constexpr int TILE = THREADS * ITEMS;
-    __shared__ Agg<NV> s_warp[WARPS];
+    __shared__ Agg<NV> s_agg[THREADS];
     __shared__ Agg<NV> s_prefix;
     __shared__ uint32_t s_tile;
 
@@ -292,54 +332,24 @@ __global__ void __launch_bounds__(THREADS) k_segreduce(SegArgs a) {
 #pragma unroll
     for (int k = 0; k < NK; ++k) kw[k] = dtype_width(a.key[k].dtype);
 
-    // ---- phase A: load this thread's rows, emit fused gathers, find segment
-    //      heads and fold the rows into the thread aggregate.  Row data is not
-    //      kept live across the scan below (phase B reloads it from L1/L2). ---
+    // ---- phase A: load this thread's rows, find segment heads and fold the
+    //      rows into the thread aggregate.  Row data is not kept live across
+    //      the scan below (phase B reloads it, from L1/L2). -------------------
     uint32_t hmask = 0;
     Agg<NV> t = agg_identity<NV>();
     {
         uint64_t key[ITEMS][NK];
         uint64_t val[ITEMS][NV > 0 ? NV : 1];
 #pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            const uint64_t r = row0 + j;
+        for (int k = 0; k < NK; ++k) load_rows<ITEMS>(a.key[k].src, kw[k], row0, n, key, k);
 #pragma unroll
-            for (int k = 0; k < NK; ++k) key[j][k] = 0;
-#pragma unroll
-            for (int v = 0; v < NV; ++v) val[j][v] = 0;
-            if (r < n) {
-                const uint64_t src = perm_row(a, r);
-#pragma unroll
-                for (int k = 0; k < NK; ++k) {
-                    const SegCol& c = a.key[k];
-                    key[j][k] = load_raw(c.src, kw[k], c.gathered ? src : r);
-                    if (c.emit) store_raw(c.emit, kw[k], r, key[j][k]);
-                }
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    const SegCol& c = a.val[v];
-                    const uint64_t i = c.gathered ? src : r;
-                    val[j][v] = load_val(c.src, c.dtype, i);
-                    if (c.emit) {
-                        const int w = dtype_width(c.dtype);
-                        store_raw(c.emit, w, r, load_raw(c.src, w, i));
-                    }
-                }
-                for (int x = 0; x < a.nextra; ++x) {
-                    const SegCol& c = a.extra[x];
-                    const int w = dtype_width(c.dtype);
-                    store_raw(c.emit, w, r, load_raw(c.src, w, c.gathered ? src : r));
-                }
-            }
-        }
+        for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
         uint64_t prev[NK];
 #pragma unroll
         for (int k = 0; k < NK; ++k) prev[k] = __shfl_up_sync(0xffffffffu, key[ITEMS - 1][k], 1);
         if (lane == 0 && row0 > 0 && row0 < n) {
-            const uint64_t r = row0 - 1;
-            const uint64_t src = perm_row(a, r);
 #pragma unroll
-            for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], a.key[k].gathered ? src : r);
+            for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], row0 - 1);
         }
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
@@ -373,25 +383,34 @@ __global__ void __launch_bounds__(THREADS) k_segreduce(SegArgs a) {
         }
     }
 
-    // ---- block scan ---------------------------------------------------------
-    Agg<NV> incl = t;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        Agg<NV> o = agg_shfl_up(incl, d);
-        if (lane >= d) incl = agg_combine(o, incl, vc);
-    }
-    if (lane == 31) s_warp[warp] = incl;
-    Agg<NV> lane_excl = agg_shfl_up(incl, 1);
-    if (lane == 0) lane_excl = agg_identity<NV>();
+    // ---- block scan (raking, in shared memory) and decoupled look-back -------
+    // Thread aggregates go to shared memory; warp 0 folds 8 consecutive ones
+    // per lane, scans the 32 lane totals with shuffles, writes each thread's
+    // exclusive prefix back, then resolves the tile prefix against earlier
+    // tiles.  Keeping the scan in one warp keeps few aggregate copies live.
+    s_agg[tid] = t;
     __syncthreads();
-    Agg<NV> wpre = agg_identity<NV>();
-    for (int w = 0; w < warp; ++w) wpre = agg_combine(wpre, s_warp[w], vc);
-    const Agg<NV> thr_excl = agg_combine(wpre, lane_excl, vc);
-
-    // ---- decoupled look-back (warp 0) ---------------------------------------
     if (warp == 0) {
-        Agg<NV> total = agg_identity<NV>();
-        for (int w = 0; w < WARPS; ++w) total = agg_combine(total, s_warp[w], vc);
+        constexpr int R = THREADS / 32;
+        Agg<NV> acc = agg_identity<NV>();
+#pragma unroll
+        for (int i = 0; i < R; ++i) acc = agg_combine(acc, s_agg[lane * R + i], vc);
+        Agg<NV> incl = acc;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const Agg<NV> o = agg_shfl_up(incl, d);
+            if (lane >= d) incl = agg_combine(o, incl, vc);
+        }
+        const Agg<NV> total = agg_shfl(incl, 31);
+        Agg<NV> run = agg_shfl_up(incl, 1);
+        if (lane == 0) run = agg_identity<NV>();
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const Agg<NV> cur = s_agg[lane * R + i];
+            s_agg[lane * R + i] = run;
+            run = agg_combine(run, cur, vc);
+        }
+
         Agg<NV> X = agg_identity<NV>();
         if (tile == 0) {
             if (lane == 0) rec_write(&recs[0], total, REC_INC);
@@ -415,11 +434,10 @@ __global__ void __launch_bounds__(THREADS) k_segreduce(SegArgs a) {
                 // chronological fold: higher lanes are older tiles
 #pragma unroll
                 for (int d = 1; d < 32; d <<= 1) {
-                    Agg<NV> o = agg_shfl_down(r, d);
+                    const Agg<NV> o = agg_shfl_down(r, d);
                     if (lane + d < 32) r = agg_combine(o, r, vc);
                 }
-                const Agg<NV> win = agg_shfl(r, 0);
-                X = agg_combine(win, X, vc);
+                X = agg_combine(agg_shfl(r, 0), X, vc);
                 if (incmask) break;
                 base -= 32;
             }
@@ -428,6 +446,7 @@ __global__ void __launch_bounds__(THREADS) k_segreduce(SegArgs a) {
         if (lane == 0) s_prefix = X;
     }
     __syncthreads();
+    const Agg<NV> thr_excl = s_agg[tid];
 
     // ---- emit completed segments --------------------------------------------
     const Agg<NV> pre = agg_combine(s_prefix, thr_excl, vc);
@@ -449,17 +468,15 @@ __global__ void __launch_bounds__(THREADS) k_segreduce(SegArgs a) {
     for (int j = 0; j < ITEMS; ++j) {
         const uint64_t r = row0 + j;
         if (r >= n) break;
-        const uint64_t src = perm_row(a, r);
         uint64_t val[NV > 0 ? NV : 1];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) val[v] = load_val(a.val[v].src, a.val[v].dtype, a.val[v].gathered ? src : r);
+        for (int v = 0; v < NV; ++v) val[v] = load_val(a.val[v].src, a.val[v].dtype, r);
         if ((hmask >> j) & 1u) {
             if (gid > 0) emit_group<NV>(a, gid - 1, cnt, w, vc);
             ++gid;
 #pragma unroll
             for (int k = 0; k < NK; ++k)
-                if (a.key_out[k])
-                    store_raw(a.key_out[k], kw[k], gid - 1, load_raw(a.key[k].src, kw[k], a.key[k].gathered ? src : r));
+                if (a.key_out[k]) store_raw(a.key_out[k], kw[k], gid - 1, load_raw(a.key[k].src, kw[k], r));
             if (a.group_start) a.group_start[gid - 1] = (uint32_t)r;
             cnt = 1;
 #pragma unroll
