@@ -212,6 +212,11 @@ def our_arm(args, rank: int, world: int, local_rank: int):
         if world > 1:
             dist.barrier()
 
+    # ---- autotune the radix-pass variants on this shape (untimed) ------------------
+    from visondf_b200 import autotune
+    tuned = autotune.tune(ctx, lambda: ctx.sort_groupby_packed(packed, stream), reps=2)
+    log(f"[rank {rank}] autotune: {tuned}")
+
     # ---- device-resident timing ------------------------------------------------
     for _ in range(args.warmup):
         ctx.sort_groupby_packed(packed, stream)
@@ -344,6 +349,8 @@ def our_arm(args, rank: int, world: int, local_rank: int):
             "hbm_frac_canonical": step_frac,
             "canonical_bytes_per_row": SORT_BYTES_PER_ROW + GROUPBY_BYTES_PER_ROW_G_EQ_N,
             "kernels": kernels,
+            "tuning": {"variant32": tuned["variant32"], "variant64": tuned["variant64"],
+                       "variants": __import__("visondf_b200._lib", fromlist=["x"]).sort_variants()},
             "gpu_launches": launches,
             "clocks": clk,
             "e2e": e2e,

@@ -114,7 +114,8 @@ typedef enum vdf_kernel_class {
     VDF_KC_ONESWEEP64 = 3,  /* radix pass, 8-byte keys        */
     VDF_KC_GATHER = 4,      /* payload gather                 */
     VDF_KC_SEGREDUCE = 5,   /* group-by segmented reduction   */
-    VDF_KC_BROADCAST = 6    /* transform broadcast            */
+    VDF_KC_BROADCAST = 6,   /* transform broadcast            */
+    VDF_KC_PACK = 7         /* row-record packing for gathers */
 } vdf_kernel_class;
 /* When enabled, every kernel the context launches is bracketed by CUDA
  * events on its stream (no reference counterpart: the reference has no
@@ -125,7 +126,27 @@ vdf_status vdf_ctx_profile(vdf_ctx* ctx, int enable);
 vdf_status vdf_ctx_profile_read(vdf_ctx* ctx, int cls, double* total_ms, uint64_t* launches);
 vdf_status vdf_ctx_profile_reset(vdf_ctx* ctx);
 
+/* ---- tuning (the autotuner's search space) --------------------------------- */
+/* The radix pass is compiled in several variants (key width, threads per
+ * CTA, keys per thread, digit bits, warp digit-match method: 0 = ballots,
+ * 1 = match.any).  A context uses one variant per key width.  The reference
+ * fixes its digit width at 16 bits (RADIX_KI16, radix_sorts/details/
+ * constants.inl:4) and has no tuning; the digit width, tile size and match
+ * method here are chosen per size class by visondf_b200/autotune.py. */
+typedef struct vdf_sort_tuning {
+    int32_t pass_variant32; /* variant index used for 4-byte keys */
+    int32_t pass_variant64; /* variant index used for 8-byte keys */
+} vdf_sort_tuning;
+int vdf_sort_variant_count(void);
+vdf_status vdf_sort_variant_info(int index, int32_t* key_width, int32_t* threads, int32_t* items_per_thread,
+                                 int32_t* digit_bits, int32_t* match);
+vdf_status vdf_ctx_set_sort_tuning(vdf_ctx* ctx, const vdf_sort_tuning* tuning);
+vdf_status vdf_ctx_get_sort_tuning(vdf_ctx* ctx, vdf_sort_tuning* tuning);
+
 /* ---- workspace sizing (pure host functions) ------------------------------ */
+/* Enough for every tuning; vdf_sort_argsort_ws also packs the other sorted
+ * key columns into this buffer when it holds n * 16 * ceil((nkeys-1)/2)
+ * bytes, else gathers them column by column. */
 size_t vdf_sort_workspace_bytes(uint64_t n, const int32_t* key_dtypes, int nkeys);
 size_t vdf_groupby_workspace_bytes(uint64_t n, int nvals);
 /* Largest row count one call accepts (2^30 - 1 in this build). */

@@ -74,3 +74,21 @@ def test_dtype_maps_are_consistent():
     import torch
     for t, code in _lib.TORCH_TO_VDF.items():
         assert _lib.WIDTH[code] == torch.empty(0, dtype=t).element_size()
+
+
+def test_variant_table_is_consistent():
+    vs = _lib.sort_variants()
+    assert vs and {v["key_width"] for v in vs} == {4, 8}
+    for v in vs:
+        assert v["threads"] % 32 == 0 and v["items"] > 0 and v["digit_bits"] in (8, 11) and v["match"] in (0, 1)
+    assert vdf.lib.vdf_sort_variant_info(len(vs), None, None, None, None, None) == _lib.ERR_INVALID_ARG
+
+
+def test_autotune_size_classes():
+    from visondf_b200 import autotune
+    assert autotune.size_class(1) == 0
+    assert autotune.size_class(1024) == 10
+    assert autotune.size_class(1025) == 11
+    t = autotune.TuningTable({20: [1, 2, 0.1, 0.2]})
+    assert t.lookup(1 << 20) == (1, 2)
+    assert t.lookup(5) is None

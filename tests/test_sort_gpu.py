@@ -132,3 +132,39 @@ def test_repeated_calls_reuse_workspace(ctx):
         k = datagen.keys_for("zipf", np.int64, n, rng)
         perm = ctx.argsort([dev(k)])
         assert (host(perm).view(np.uint32) == ob.argsort([k])).all()
+
+
+def test_every_kernel_variant_gives_identical_results(ctx):
+    variants = vdf._lib.sort_variants()
+    v32 = [v["index"] for v in variants if v["key_width"] == 4]
+    v64 = [v["index"] for v in variants if v["key_width"] == 8]
+    rng = np.random.default_rng(17)
+    n = 300_007
+    keys = [datagen.keys_for("zipf", np.int64, n, rng), datagen.keys_for("few", np.int32, n, rng),
+            datagen.keys_for("uniform", np.uint32, n, rng)]
+    exp = ob.argsort(keys)
+    saved = ctx.get_sort_tuning()
+    try:
+        for a in v32:
+            for b in v64:
+                ctx.set_sort_tuning(a, b)
+                assert ctx.get_sort_tuning() == (a, b)
+                perm = ctx.argsort([dev(k) for k in keys])
+                assert (host(perm).view(np.uint32) == exp).all(), (a, b)
+        with pytest.raises(vdf.VdfError):
+            ctx.set_sort_tuning(v64[0], v32[0])  # widths swapped
+    finally:
+        ctx.set_sort_tuning(*saved)
+
+
+def test_autotune_picks_valid_variants(ctx):
+    from visondf_b200 import autotune
+    rng = np.random.default_rng(3)
+    k = [dev(datagen.keys_for("uniform", np.int64, 200_000, rng)), dev(datagen.keys_for("uniform", np.int32, 200_000, rng))]
+    saved = ctx.get_sort_tuning()
+    try:
+        res = autotune.tune(ctx, lambda: ctx.argsort(k), reps=1)
+        assert ctx.get_sort_tuning() == (res["variant32"], res["variant64"])
+        assert res["ms32"] and res["ms64"]
+    finally:
+        ctx.set_sort_tuning(*saved)

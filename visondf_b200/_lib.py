@@ -23,7 +23,7 @@ I32, I64, U32, U64, F64, F32 = range(6)
 # vdf_order
 ORDER_ASC, ORDER_DESC_STABLE, ORDER_DESC_REVERSE = range(3)
 
-KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast"]
+KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast", "pack"]
 
 TORCH_TO_VDF = {
     torch.int32: I32, torch.int64: I64, torch.uint32: U32, torch.uint64: U64,
@@ -46,6 +46,10 @@ class vdf_col(C.Structure):
 class vdf_agg_out(C.Structure):
     _fields_ = [("sum", C.c_void_p), ("sum_hi", C.c_void_p), ("min", C.c_void_p), ("max", C.c_void_p),
                 ("mean", C.c_void_p)]
+
+
+class vdf_sort_tuning(C.Structure):
+    _fields_ = [("pass_variant32", C.c_int32), ("pass_variant64", C.c_int32)]
 
 
 class vdf_sort_groupby_args(C.Structure):
@@ -80,6 +84,10 @@ def _load() -> C.CDLL:
         "vdf_ctx_profile_read": (st, [vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
         "vdf_ctx_profile_reset": (st, [vp]),
         "vdf_sort_workspace_bytes": (sz, [u64, C.POINTER(C.c_int32), i32]),
+        "vdf_sort_variant_count": (i32, []),
+        "vdf_sort_variant_info": (st, [i32] + [C.POINTER(C.c_int32)] * 5),
+        "vdf_ctx_set_sort_tuning": (st, [vp, C.POINTER(vdf_sort_tuning)]),
+        "vdf_ctx_get_sort_tuning": (st, [vp, C.POINTER(vdf_sort_tuning)]),
         "vdf_groupby_workspace_bytes": (sz, [u64, i32]),
         "vdf_sort_argsort": (st, [vp, u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp]),
         "vdf_sort_argsort_ws": (st, [vp, u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp, sz, vp]),
@@ -226,6 +234,15 @@ class Context:
             out[name] = (ms.value, int(cnt.value))
         return out
 
+    def set_sort_tuning(self, variant32: int, variant64: int):
+        t = vdf_sort_tuning(variant32, variant64)
+        self._check(lib.vdf_ctx_set_sort_tuning(self.handle, C.byref(t)), "vdf_ctx_set_sort_tuning")
+
+    def get_sort_tuning(self) -> tuple:
+        t = vdf_sort_tuning()
+        self._check(lib.vdf_ctx_get_sort_tuning(self.handle, C.byref(t)), "vdf_ctx_get_sort_tuning")
+        return t.pass_variant32, t.pass_variant64
+
     def reserve(self, nbytes: int):
         self._check(lib.vdf_ctx_reserve(self.handle, nbytes), "vdf_ctx_reserve")
 
@@ -353,6 +370,17 @@ class Context:
                                       group_vals.element_size(), _ptr(perm), _ptr(out), _stream(stream)),
                     "vdf_broadcast")
         return out
+
+
+def sort_variants() -> list:
+    """[{index, key_width, threads, items, digit_bits, match}] of the compiled radix-pass variants."""
+    out = []
+    for i in range(lib.vdf_sort_variant_count()):
+        vals = [C.c_int32() for _ in range(5)]
+        if lib.vdf_sort_variant_info(i, *[C.byref(v) for v in vals]) == OK:
+            out.append(dict(index=i, key_width=vals[0].value, threads=vals[1].value, items=vals[2].value,
+                            digit_bits=vals[3].value, match=vals[4].value))
+    return out
 
 
 def header_functions() -> list[str]:

@@ -1,0 +1,79 @@
+"""Autotuner for the radix sort's kernel variants.
+
+The library compiles the radix pass in several variants (key width, threads
+per CTA, keys per thread, digit bits, warp digit-match method; see
+vdf_sort_variant_info).  A context uses one variant per key width.  This
+module times every variant on the caller's own workload shape and picks the
+fastest per key width, keyed by a size class (power-of-two bucket of the row
+count), so a serving loop can keep one choice per class.
+
+Timing uses the library's per-launch CUDA-event profiler (vdf_ctx_profile),
+so the 4-byte-key and 8-byte-key passes of one run are measured separately
+and each width is tuned independently.
+"""
+from __future__ import annotations
+
+import json
+import math
+from dataclasses import dataclass, field
+from pathlib import Path
+from typing import Callable, Optional
+
+from . import _lib
+
+
+def size_class(n: int) -> int:
+    """Power-of-two bucket of a row count (0 for n <= 1)."""
+    return 0 if n <= 1 else int(math.ceil(math.log2(n)))
+
+
+@dataclass
+class TuningTable:
+    """Best (variant32, variant64) per size class."""
+
+    entries: dict = field(default_factory=dict)  # size class -> [v32, v64, ms32, ms64]
+
+    def lookup(self, n: int) -> Optional[tuple]:
+        e = self.entries.get(size_class(n))
+        return None if e is None else (e[0], e[1])
+
+    def save(self, path: Path):
+        Path(path).write_text(json.dumps({str(k): v for k, v in self.entries.items()}, indent=1) + "\n")
+
+    @classmethod
+    def load(cls, path: Path) -> "TuningTable":
+        d = json.loads(Path(path).read_text())
+        return cls({int(k): v for k, v in d.items()})
+
+
+def tune(ctx: "_lib.Context", run: Callable[[], None], reps: int = 2) -> dict:
+    """Times `run` (one sort or sort + group-by on the context) under every
+    variant assignment and returns {"variant32": i, "variant64": j,
+    "ms32": {i: ms per pass}, "ms64": {j: ms per pass}}; leaves the best
+    tuning set on the context."""
+    variants = _lib.sort_variants()
+    v32 = [v["index"] for v in variants if v["key_width"] == 4]
+    v64 = [v["index"] for v in variants if v["key_width"] == 8]
+    ms32, ms64 = {}, {}
+    run()  # warm the workspace and the kernels
+    for i in range(max(len(v32), len(v64))):
+        a, b = v32[i % len(v32)], v64[i % len(v64)]
+        ctx.set_sort_tuning(a, b)
+        run()
+        ctx.profile(True)
+        ctx.profile_reset()
+        for _ in range(reps):
+            run()
+        prof = ctx.profile_read()
+        ctx.profile(False)
+        t32, c32 = prof["onesweep32"]
+        t64, c64 = prof["onesweep64"]
+        if c32:
+            ms32[a] = min(ms32.get(a, math.inf), t32 / c32)
+        if c64:
+            ms64[b] = min(ms64.get(b, math.inf), t64 / c64)
+    cur = ctx.get_sort_tuning()
+    best32 = min(ms32, key=ms32.get) if ms32 else cur[0]
+    best64 = min(ms64, key=ms64.get) if ms64 else cur[1]
+    ctx.set_sort_tuning(best32, best64)
+    return {"variant32": best32, "variant64": best64, "ms32": ms32, "ms64": ms64}

@@ -71,6 +71,7 @@ struct EventProfiler final : vdf::Profiler {
 struct vdf_ctx {
     int device = 0;
     bool profiling = false;
+    vdf::SortTuning tuning = vdf::default_sort_tuning();
     EventProfiler prof;
     std::mutex mu;
     unsigned char* ws = nullptr;
@@ -174,7 +175,7 @@ vdf_status check_rows(vdf_ctx* c, uint64_t n) {
 // Sorted copies of key columns 1..nkeys-1 (column 0 is written by the last
 // radix pass) by gathering through the permutation.
 vdf_status emit_other_keys(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, const uint32_t* perm,
-                           void* const* sorted_keys_out, cudaStream_t s) {
+                           void* const* sorted_keys_out, void* rec_ws, cudaStream_t s) {
     if (!sorted_keys_out) return VDF_OK;
     vdf::GatherArgs g{};
     g.perm = perm;
@@ -188,8 +189,18 @@ vdf_status emit_other_keys(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkey
         g.ncols++;
     }
     if (!g.ncols) return VDF_OK;
-    c->launches++;
-    return from_cuda(c, vdf::run_gather(g, s, prof_of(c)), "gather keys");
+    int launched = 0;
+    cudaError_t e = vdf::run_gather(g, s, prof_of(c), rec_ws, &launched);
+    c->launches += launched;
+    return from_cuda(c, e, "gather keys");
+}
+
+// Workspace a sort needs: the radix buffers, then (reusing them once the
+// sort is done) the packed records of the other sorted key columns.
+size_t sort_ws_need(const vdf::SortPlan& p, uint64_t n, int nkeys, void* const* sorted_keys_out) {
+    int other = 0;
+    for (int k = 1; k < nkeys; ++k) other += (sorted_keys_out && sorted_keys_out[k]) ? 1 : 0;
+    return std::max(p.ws_bytes, (size_t)n * vdf::gather_record_bytes(other));
 }
 
 vdf_status sort_impl(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, int order, uint32_t* perm_out,
@@ -200,14 +211,15 @@ vdf_status sort_impl(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, int
         dts[k] = keys[k].dtype;
         cols[k] = keys[k].data;
     }
-    vdf::SortPlan p = vdf::make_sort_plan(n, dts, nkeys);
+    vdf::SortPlan p = vdf::make_sort_plan(n, dts, nkeys, c->tuning);
     if (ws_bytes < p.ws_bytes)
         return fail(c, VDF_ERR_WORKSPACE, "workspace of %zu bytes < %zu needed", ws_bytes, p.ws_bytes);
     void* key0_out = sorted_keys_out ? sorted_keys_out[0] : nullptr;
     cudaError_t e = vdf::run_sort(p, cols, order, perm_out, key0_out, ws, err_word(c), s, prof_of(c));
     c->launches += 2 + (uint64_t)p.total_passes;
     if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
-    return emit_other_keys(c, n, keys, nkeys, perm_out, sorted_keys_out, s);
+    const bool packed = ws_bytes >= sort_ws_need(p, n, nkeys, sorted_keys_out);
+    return emit_other_keys(c, n, keys, nkeys, perm_out, sorted_keys_out, packed ? ws : nullptr, s);
 }
 
 vdf_status finish_groups(vdf_ctx* c, uint64_t* n_groups_dev, uint64_t* n_groups_host, cudaStream_t s) {
@@ -249,7 +261,46 @@ size_t vdf_sort_workspace_bytes(uint64_t n, const int32_t* key_dtypes, int nkeys
     if (!key_dtypes || nkeys < 1 || nkeys > vdf::kMaxKeys) return 0;
     for (int k = 0; k < nkeys; ++k)
         if (!valid_dtype(key_dtypes[k])) return 0;
-    return vdf::make_sort_plan(n, key_dtypes, nkeys).ws_bytes;
+    // the largest over every kernel-variant choice, so it fits any tuning
+    size_t best = 0;
+    const int nv = vdf::sort_variant_count();
+    for (int a = 0; a < nv; ++a)
+        for (int b = 0; b < nv; ++b) {
+            vdf::SortTuning t{a, b};
+            if (vdf::sort_tuning_valid(t)) best = std::max(best, vdf::make_sort_plan(n, key_dtypes, nkeys, t).ws_bytes);
+        }
+    return best;
+}
+
+int vdf_sort_variant_count(void) { return vdf::sort_variant_count(); }
+
+vdf_status vdf_sort_variant_info(int index, int32_t* key_width, int32_t* threads, int32_t* items_per_thread,
+                                 int32_t* digit_bits, int32_t* match) {
+    int w, t, i, b, m;
+    if (!vdf::sort_variant_info(index, &w, &t, &i, &b, &m)) return VDF_ERR_INVALID_ARG;
+    if (key_width) *key_width = w;
+    if (threads) *threads = t;
+    if (items_per_thread) *items_per_thread = i;
+    if (digit_bits) *digit_bits = b;
+    if (match) *match = m;
+    return VDF_OK;
+}
+
+vdf_status vdf_ctx_set_sort_tuning(vdf_ctx* c, const vdf_sort_tuning* t) {
+    if (!c || !t) return VDF_ERR_INVALID_ARG;
+    vdf::SortTuning st{t->pass_variant32, t->pass_variant64};
+    if (!vdf::sort_tuning_valid(st)) return fail(c, VDF_ERR_INVALID_ARG, "invalid sort tuning %d/%d", st.variant32, st.variant64);
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->tuning = st;
+    return VDF_OK;
+}
+
+vdf_status vdf_ctx_get_sort_tuning(vdf_ctx* c, vdf_sort_tuning* t) {
+    if (!c || !t) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    t->pass_variant32 = c->tuning.variant32;
+    t->pass_variant64 = c->tuning.variant64;
+    return VDF_OK;
 }
 
 size_t vdf_groupby_workspace_bytes(uint64_t n, int nvals) {
@@ -384,7 +435,7 @@ vdf_status vdf_sort_argsort(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nke
     DeviceGuard g(c->device);
     int32_t dts[vdf::kMaxKeys];
     for (int k = 0; k < nkeys; ++k) dts[k] = keys[k].dtype;
-    const size_t need = vdf::make_sort_plan(n, dts, nkeys).ws_bytes;
+    const size_t need = sort_ws_need(vdf::make_sort_plan(n, dts, nkeys, c->tuning), n, nkeys, sorted_keys_out);
     if ((st = ws_ensure(c, need)) != VDF_OK) return st;
     return sort_impl(c, n, keys, nkeys, order, perm_out, sorted_keys_out, c->ws, c->ws_cap,
                      static_cast<cudaStream_t>(stream));
@@ -412,8 +463,12 @@ vdf_status vdf_gather(vdf_ctx* c, uint64_t n, const uint32_t* perm, const vdf_co
         g.width[i] = vdf::dtype_width(in[i].dtype);
     }
     DeviceGuard gd(c->device);
-    c->launches++;
-    return from_cuda(c, vdf::run_gather(g, static_cast<cudaStream_t>(stream), prof_of(c)), "gather");
+    const size_t rec = vdf::gather_record_bytes(ncols);
+    if (rec && (st = ws_ensure(c, n * rec)) != VDF_OK) return st;
+    int launched = 0;
+    cudaError_t e = vdf::run_gather(g, static_cast<cudaStream_t>(stream), prof_of(c), rec ? c->ws : nullptr, &launched);
+    c->launches += launched;
+    return from_cuda(c, e, "gather");
 }
 
 vdf_status vdf_groupby_sorted(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, const vdf_col* vals, int nvals,
@@ -494,7 +549,7 @@ vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* st
         dts[k] = x->keys[k].dtype;
         cols[k] = x->keys[k].data;
     }
-    const vdf::SortPlan plan = vdf::make_sort_plan(n, dts, x->nkeys);
+    const vdf::SortPlan plan = vdf::make_sort_plan(n, dts, x->nkeys, c->tuning);
     // Sorted copies needed by the group-by that the caller did not ask for
     // live in the workspace: [perm][key 0][keys 1..][aggregated payload][tail]
     // where tail = max(sort workspace, group-by workspace).
@@ -524,8 +579,12 @@ vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* st
             off += align256(n * (size_t)vdf::dtype_width(x->payload[p].dtype));
         }
     }
+    int ngather = 0;
+    for (int k = 1; k < x->nkeys; ++k) ngather += skey[k] ? 1 : 0;
+    for (int p = 0; p < x->npayload; ++p) ngather += spay[p] ? 1 : 0;
+    const size_t rec_bytes = (size_t)n * vdf::gather_record_bytes(std::min(ngather, vdf::kMaxGather));
     const size_t seg_bytes = x->groupby ? vdf::segreduce_workspace_bytes(n, x->nagg) : 0;
-    const size_t tail = std::max(plan.ws_bytes, seg_bytes);
+    const size_t tail = std::max(std::max(plan.ws_bytes, seg_bytes), rec_bytes);
     if ((st = ws_ensure(c, off + tail)) != VDF_OK) return st;
     uint32_t* perm = own_perm ? reinterpret_cast<uint32_t*>(c->ws) : x->perm_out;
     for (int k = 0; k < x->nkeys; ++k)
@@ -546,8 +605,9 @@ vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* st
     ga.n = n;
     auto flush = [&]() -> cudaError_t {
         if (!ga.ncols) return cudaSuccess;
-        c->launches++;
-        cudaError_t ge = vdf::run_gather(ga, s, prof_of(c));
+        int launched = 0;
+        cudaError_t ge = vdf::run_gather(ga, s, prof_of(c), tws, &launched);
+        c->launches += launched;
         ga.ncols = 0;
         return ge;
     };

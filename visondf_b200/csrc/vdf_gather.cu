@@ -11,6 +11,13 @@
 // per column back to back, and writes each column's 4 results with 16-byte
 // stores.
 //
+// When a workspace is supplied and two or more columns are gathered, the
+// columns are first packed row-wise into records of 8-byte slots (16..64
+// bytes, one streaming pass), and the gather then reads ONE record per row:
+// a random read costs a full DRAM access (64 bytes on this part) however few
+// bytes it uses, so gathering k columns separately costs k such accesses per
+// row while the packed record costs one.
+//
 // k_broadcast produces the reference's transform output
 // (CreateValueCol::apply, V/inlines/transform/transform_group_by/
 // create_value_col.inl:36-61: v_col[i] = lookup.at(key_vec[i])): every row
@@ -74,8 +81,82 @@ __global__ void __launch_bounds__(256) k_gather(GatherArgs g) {
     }
 }
 
-cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof) {
+template <int REC>
+__global__ void __launch_bounds__(256) k_pack(GatherArgs g, unsigned char* recs) {
+    constexpr int SLOTS = REC / 8;
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.n) return;
+    unsigned long long slot[SLOTS];
+#pragma unroll
+    for (int c = 0; c < SLOTS; ++c) {
+        slot[c] = 0;
+        if (c < g.ncols)
+            slot[c] = g.width[c] == 8 ? ldg_stream(static_cast<const unsigned long long*>(g.src[c]) + r)
+                                      : (unsigned long long)ldg_stream(static_cast<const uint32_t*>(g.src[c]) + r);
+    }
+    ulonglong2* dst = reinterpret_cast<ulonglong2*>(recs + r * REC);
+#pragma unroll
+    for (int c = 0; c < SLOTS; c += 2) dst[c / 2] = make_ulonglong2(slot[c], slot[c + 1]);
+}
+
+template <int REC>
+__global__ void __launch_bounds__(256) k_gather_rec(GatherArgs g, const unsigned char* recs) {
+    constexpr int SLOTS = REC / 8;
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= g.n) return;
+    uint32_t p = ldg_stream(g.perm + r);
+    if (p >= g.n) {  // not a permutation of [0, n)
+        if (g.err) atomicOr(g.err, ERR_BAD_INDEX);
+        p = 0;
+    }
+    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(recs + (uint64_t)p * REC);
+    unsigned long long slot[SLOTS];
+#pragma unroll
+    for (int c = 0; c < SLOTS; c += 2) {
+        const ulonglong2 v = __ldg(src + c / 2);
+        slot[c] = v.x;
+        slot[c + 1] = v.y;
+    }
+#pragma unroll
+    for (int c = 0; c < SLOTS; ++c) {
+        if (c >= g.ncols) break;
+        if (g.width[c] == 8) stg_stream(static_cast<unsigned long long*>(g.dst[c]) + r, slot[c]);
+        else stg_stream(static_cast<uint32_t*>(g.dst[c]) + r, (uint32_t)slot[c]);
+    }
+}
+
+size_t gather_record_bytes(int ncols) {
+    return (ncols >= 2 && ncols <= kMaxGather) ? (size_t)16 * ((ncols + 1) / 2) : 0;
+}
+
+cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof, void* rec_ws, int* launches) {
     if (g.n == 0 || g.ncols == 0) return cudaSuccess;
+    const size_t rec = gather_record_bytes(g.ncols);
+    if (rec_ws && rec) {
+        unsigned char* recs = static_cast<unsigned char*>(rec_ws);
+        const uint32_t blocks = (uint32_t)((g.n + 255) / 256);
+        if (prof) prof->begin(KC_PACK, s);
+        switch (rec) {
+        case 16: k_pack<16><<<blocks, 256, 0, s>>>(g, recs); break;
+        case 32: k_pack<32><<<blocks, 256, 0, s>>>(g, recs); break;
+        case 48: k_pack<48><<<blocks, 256, 0, s>>>(g, recs); break;
+        default: k_pack<64><<<blocks, 256, 0, s>>>(g, recs); break;
+        }
+        if (prof) prof->end(KC_PACK, s);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (prof) prof->begin(KC_GATHER, s);
+        switch (rec) {
+        case 16: k_gather_rec<16><<<blocks, 256, 0, s>>>(g, recs); break;
+        case 32: k_gather_rec<32><<<blocks, 256, 0, s>>>(g, recs); break;
+        case 48: k_gather_rec<48><<<blocks, 256, 0, s>>>(g, recs); break;
+        default: k_gather_rec<64><<<blocks, 256, 0, s>>>(g, recs); break;
+        }
+        if (prof) prof->end(KC_GATHER, s);
+        if (launches) *launches += 2;
+        return cudaGetLastError();
+    }
+    if (launches) *launches += 1;
     bool vec = (reinterpret_cast<uintptr_t>(g.perm) & 15) == 0;
     for (int c = 0; c < g.ncols; ++c) vec = vec && (reinterpret_cast<uintptr_t>(g.dst[c]) & 15) == 0;
     const uint64_t threads = (g.n + 3) / 4;

@@ -14,7 +14,7 @@ constexpr int kMaxGather = 8;   // columns per gather launch
 // Kernel classes for the optional per-launch timing (vdf_ctx_profile).
 enum KernelClass : int {
     KC_HIST = 0, KC_SCAN = 1, KC_ONESWEEP32 = 2, KC_ONESWEEP64 = 3, KC_GATHER = 4, KC_SEGREDUCE = 5,
-    KC_BROADCAST = 6, KC_COUNT = 7
+    KC_BROADCAST = 6, KC_PACK = 7, KC_COUNT = 8
 };
 
 // Brackets kernel launches with CUDA events when profiling is enabled.
@@ -60,8 +60,20 @@ struct PassArgs {
     int reverse;                // reference descending: output positions mirrored
 };
 
+// Kernel-variant choice of the radix pass per key width (indices into the
+// variant table in vdf_radix.cu); the autotuner's search space.
+struct SortTuning {
+    int variant32;
+    int variant64;
+};
+SortTuning default_sort_tuning();
+bool sort_tuning_valid(const SortTuning& t);
+int sort_variant_count();
+bool sort_variant_info(int i, int* width, int* threads, int* items, int* bits, int* match);
+
 struct SortPlan {
     uint64_t n;
+    SortTuning tuning;
     int nkeys;
     int bits, radix;
     int dtype[kMaxKeys], width[kMaxKeys], passes[kMaxKeys], pass_base[kMaxKeys];
@@ -72,13 +84,11 @@ struct SortPlan {
     size_t ws_bytes;
 };
 
-SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys);
+SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const SortTuning& tuning);
 // Sorts; writes perm_out (and key0_out = raw sorted most-significant key, may
 // be null).  Bounded waits that give up OR their ErrBits into *err.
 cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
                      void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof = nullptr);
-size_t sort_smem_bytes(int key_width);
-int sort_tile_rows(int key_width);
 cudaError_t prepare_sort_kernels();
 
 // ---- gather ----------------------------------------------------------------
@@ -91,7 +101,13 @@ struct GatherArgs {
     void* dst[kMaxGather];
     int width[kMaxGather];
 };
-cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof = nullptr);
+// Bytes per row of the packed-record buffer a gather of ncols columns uses
+// (0: gathered column by column).
+size_t gather_record_bytes(int ncols);
+// rec_ws: n * gather_record_bytes(ncols) bytes of workspace, or null for the
+// column-by-column path.  *launches is increased by the kernels launched.
+cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof = nullptr, void* rec_ws = nullptr,
+                       int* launches = nullptr);
 
 // ---- segmented reduction (group-by over sorted rows) -----------------------
 // A column of rows in key order.

@@ -128,7 +128,9 @@ struct OnesweepCfg {
     static constexpr size_t SMEM = EX_BYTES + CNT_BYTES + GLOB_BYTES + 64 + WARPS * 4;
 };
 
-template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL>
+// MATCH selects how a warp finds the lanes holding the same digit:
+// 0 = one ballot per digit bit (ALU/vote pipes), 1 = match.any (XU pipe).
+template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL, int MATCH>
 __global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
     using C = OnesweepCfg<K, BITS, THREADS, ITEMS>;
     constexpr int RADIX = C::RADIX, WARPS = C::WARPS, TILE = C::TILE, BPT = C::BPT;
@@ -188,8 +190,8 @@ __global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
 
     // ---- warp-local ranks and per-warp digit counts --------------------------
     // Lanes holding the same digit are found with one ballot per digit bit
-    // (plus one for validity) instead of match.any, which issues on the
-    // narrow XU pipe; the lowest such lane updates the warp's counter.
+    // (plus one for validity), or with match.any; the lowest such lane
+    // updates the warp's counter.
     uint32_t rank[ITEMS];
     uint32_t* my_cnt = wcnt + warp * RADIX;
     const uint32_t lt = lanemask_lt();
@@ -198,12 +200,17 @@ __global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
         const uint32_t pos = wpos + j * 32 + lane;
         const bool ok = pos < valid;
         const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
-        uint32_t peers = __ballot_sync(0xffffffffu, ok);
-        if (!ok) peers = ~peers;
+        uint32_t peers;
+        if (MATCH == 1) {
+            peers = __match_any_sync(0xffffffffu, ok ? d : (uint32_t)RADIX);
+        } else {
+            peers = __ballot_sync(0xffffffffu, ok);
+            if (!ok) peers = ~peers;
 #pragma unroll
-        for (int b = 0; b < BITS; ++b) {
-            const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
-            peers &= ((d >> b) & 1u) ? bal : ~bal;
+            for (int b = 0; b < BITS; ++b) {
+                const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+                peers &= ((d >> b) & 1u) ? bal : ~bal;
+            }
         }
         const int leader = __ffs(peers) - 1;
         uint32_t base = 0;
@@ -353,55 +360,82 @@ __global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
 // ---------------------------------------------------------------------------
 namespace {
 constexpr int kBits = 8;
-constexpr int kThreads32 = 256, kItems32 = 16;
-constexpr int kThreads64 = 256, kItems64 = 12;
 
-template <typename K, int THREADS, int ITEMS, int IN_MODE, bool FINAL>
-cudaError_t launch_pass(const PassArgs& a, uint32_t tiles, cudaStream_t s) {
+using PassKernel = void (*)(PassArgs);
+
+// One compiled configuration of the radix pass.  The variant table is the
+// autotuner's search space; a context selects one variant per key width.
+struct PassVariant {
+    int width, threads, items, bits, match;
+    size_t smem;
+    PassKernel k[3][2];  // [IN_MODE][FINAL]
+};
+
+template <typename K, int THREADS, int ITEMS, int MATCH>
+PassVariant make_variant() {
     using C = OnesweepCfg<K, kBits, THREADS, ITEMS>;
-    k_onesweep<K, kBits, THREADS, ITEMS, IN_MODE, FINAL><<<tiles, THREADS, C::SMEM, s>>>(a);
-    return cudaGetLastError();
+    PassVariant v{};
+    v.width = (int)sizeof(K);
+    v.threads = THREADS;
+    v.items = ITEMS;
+    v.bits = kBits;
+    v.match = MATCH;
+    v.smem = C::SMEM;
+    v.k[IN_RAW][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_RAW, false, MATCH>;
+    v.k[IN_GATHER][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_GATHER, false, MATCH>;
+    v.k[IN_BUF][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_BUF, false, MATCH>;
+    v.k[IN_RAW][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_RAW, true, MATCH>;
+    v.k[IN_GATHER][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_GATHER, true, MATCH>;
+    v.k[IN_BUF][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_BUF, true, MATCH>;
+    return v;
 }
 
-template <typename K, int THREADS, int ITEMS, int IN_MODE, bool FINAL>
-cudaError_t set_pass_attr() {
-    using C = OnesweepCfg<K, kBits, THREADS, ITEMS>;
-    return cudaFuncSetAttribute(k_onesweep<K, kBits, THREADS, ITEMS, IN_MODE, FINAL>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C::SMEM);
-}
+const PassVariant kVariants[] = {
+    make_variant<uint32_t, 256, 16, 0>(),  // 0
+    make_variant<uint32_t, 256, 16, 1>(),  // 1
+    make_variant<uint64_t, 256, 12, 0>(),  // 2
+    make_variant<uint64_t, 256, 12, 1>(),  // 3
+};
+constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
-template <typename K, int THREADS, int ITEMS>
-cudaError_t set_pass_attrs() {
-    cudaError_t e;
-    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_RAW, false>()) != cudaSuccess) return e;
-    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_GATHER, false>()) != cudaSuccess) return e;
-    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_BUF, false>()) != cudaSuccess) return e;
-    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_RAW, true>()) != cudaSuccess) return e;
-    if ((e = set_pass_attr<K, THREADS, ITEMS, IN_GATHER, true>()) != cudaSuccess) return e;
-    return set_pass_attr<K, THREADS, ITEMS, IN_BUF, true>();
-}
-
-template <typename K, int THREADS, int ITEMS>
-cudaError_t dispatch_pass(const PassArgs& a, int in_mode, bool final_pass, uint32_t tiles, cudaStream_t s) {
-    if (final_pass) {
-        if (in_mode == IN_RAW) return launch_pass<K, THREADS, ITEMS, IN_RAW, true>(a, tiles, s);
-        if (in_mode == IN_GATHER) return launch_pass<K, THREADS, ITEMS, IN_GATHER, true>(a, tiles, s);
-        return launch_pass<K, THREADS, ITEMS, IN_BUF, true>(a, tiles, s);
-    }
-    if (in_mode == IN_RAW) return launch_pass<K, THREADS, ITEMS, IN_RAW, false>(a, tiles, s);
-    if (in_mode == IN_GATHER) return launch_pass<K, THREADS, ITEMS, IN_GATHER, false>(a, tiles, s);
-    return launch_pass<K, THREADS, ITEMS, IN_BUF, false>(a, tiles, s);
+const PassVariant& variant_for(const SortTuning& t, int width) {
+    const int v = (width == 4) ? t.variant32 : t.variant64;
+    return kVariants[v];
 }
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 }  // namespace
 
-int sort_tile_rows(int key_width) { return key_width == 4 ? kThreads32 * kItems32 : kThreads64 * kItems64; }
+int sort_variant_count() { return kNumVariants; }
 
-SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys) {
+bool sort_variant_info(int i, int* width, int* threads, int* items, int* bits, int* match) {
+    if (i < 0 || i >= kNumVariants) return false;
+    const PassVariant& v = kVariants[i];
+    *width = v.width;
+    *threads = v.threads;
+    *items = v.items;
+    *bits = v.bits;
+    *match = v.match;
+    return true;
+}
+
+bool sort_tuning_valid(const SortTuning& t) {
+    return t.variant32 >= 0 && t.variant32 < kNumVariants && kVariants[t.variant32].width == 4 &&
+           t.variant64 >= 0 && t.variant64 < kNumVariants && kVariants[t.variant64].width == 8;
+}
+
+SortTuning default_sort_tuning() { return SortTuning{1, 2}; }
+
+static int tile_rows(const SortTuning& t, int width) {
+    const PassVariant& v = variant_for(t, width);
+    return v.threads * v.items;
+}
+
+SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const SortTuning& tuning) {
     SortPlan p{};
     p.n = n;
     p.nkeys = nkeys;
+    p.tuning = tuning;
     p.bits = kBits;
     p.radix = 1 << kBits;
     int maxw = 4;
@@ -412,7 +446,8 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys) {
         p.width[k] = dtype_width(dtypes[k]);
         p.passes[k] = (p.width[k] * 8 + kBits - 1) / kBits;
         if (p.width[k] > maxw) maxw = p.width[k];
-        uint32_t t = (uint32_t)((n + sort_tile_rows(p.width[k]) - 1) / sort_tile_rows(p.width[k]));
+        const int rows = tile_rows(tuning, p.width[k]);
+        uint32_t t = (uint32_t)((n + rows - 1) / rows);
         if (t > max_tiles) max_tiles = t;
     }
     // passes are numbered in processing order (least-significant key first)
@@ -491,7 +526,8 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
     int g = 0;  // global pass counter (processing order)
     for (int k = p.nkeys - 1; k >= 0; --k) {
         const int w = p.width[k];
-        const uint32_t tiles = (uint32_t)((n + sort_tile_rows(w) - 1) / sort_tile_rows(w));
+        const PassVariant& var = variant_for(p.tuning, w);
+        const uint32_t tiles = (uint32_t)((n + var.threads * var.items - 1) / (var.threads * var.items));
         for (int q = 0; q < p.passes[k]; ++q, ++g) {
             PassArgs a{};
             a.n = n;
@@ -530,8 +566,8 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
                 a.vals_out = vbuf[vn];
             }
             if (prof) prof->begin(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
-            e = (w == 4) ? dispatch_pass<uint32_t, kThreads32, kItems32>(a, mode, fin, tiles, s)
-                         : dispatch_pass<uint64_t, kThreads64, kItems64>(a, mode, fin, tiles, s);
+            var.k[mode][fin ? 1 : 0]<<<tiles, var.threads, var.smem, s>>>(a);
+            e = cudaGetLastError();
             if (prof) prof->end(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
             if (e != cudaSuccess) return e;
             kcur = kn;
@@ -544,15 +580,13 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
 // Raises the dynamic shared-memory limit of every sort kernel on the current
 // device; called once per device before the first sort.
 cudaError_t prepare_sort_kernels() {
-    cudaError_t e = set_pass_attrs<uint32_t, kThreads32, kItems32>();
-    if (e != cudaSuccess) return e;
-    if ((e = set_pass_attrs<uint64_t, kThreads64, kItems64>()) != cudaSuccess) return e;
+    for (const PassVariant& v : kVariants)
+        for (int m = 0; m < 3; ++m)
+            for (int f = 0; f < 2; ++f) {
+                cudaError_t e = cudaFuncSetAttribute(v.k[m][f], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
+                if (e != cudaSuccess) return e;
+            }
     return cudaFuncSetAttribute(k_digit_hist<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-}
-
-size_t sort_smem_bytes(int key_width) {
-    return key_width == 4 ? OnesweepCfg<uint32_t, kBits, kThreads32, kItems32>::SMEM
-                          : OnesweepCfg<uint64_t, kBits, kThreads64, kItems64>::SMEM;
 }
 
 }  // namespace vdf
