@@ -214,7 +214,13 @@ def our_arm(args, rank: int, world: int, local_rank: int):
 
     # ---- autotune the radix-pass variants on this shape (untimed) ------------------
     from visondf_b200 import autotune
-    tuned = autotune.tune(ctx, lambda: ctx.sort_groupby_packed(packed, stream), reps=2)
+    if args.no_autotune:
+        if args.variants:
+            ctx.set_sort_tuning(*args.variants)
+        v32, v64 = ctx.get_sort_tuning()
+        tuned = {"variant32": v32, "variant64": v64, "ms32": {}, "ms64": {}}
+    else:
+        tuned = autotune.tune(ctx, lambda: ctx.sort_groupby_packed(packed, stream), reps=2)
     log(f"[rank {rank}] autotune: {tuned}")
 
     # ---- device-resident timing ------------------------------------------------
@@ -369,6 +375,9 @@ def main():
     ap.add_argument("--ref-sample", type=int, default=10_000_000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the library's default kernel variants")
+    ap.add_argument("--variants", type=int, nargs=2, metavar=("V32", "V64"),
+                    help="with --no-autotune: radix-pass variant indices for 4- and 8-byte keys")
     args = ap.parse_args()
     if args.warmup < 3:
         log("note: fewer than 3 warm-up steps; the timing rules ask for at least 3")

@@ -325,6 +325,7 @@ vdf_status vdf_ctx_create(int device, vdf_ctx** out) {
         std::lock_guard<std::mutex> lk(g_prep_mu);
         if (!g_prepared[device]) {
             e = vdf::prepare_sort_kernels();
+            if (e == cudaSuccess) e = vdf::prepare_segreduce_kernels();
             if (e != cudaSuccess) {
                 delete c;
                 return VDF_ERR_DEVICE;
@@ -504,11 +505,10 @@ vdf_status vdf_groupby_sorted(vdf_ctx* c, uint64_t n, const vdf_col* keys, int n
     a.row_group = row_group_out;
     a.n_groups = n_groups_dev ? n_groups_dev : (n_groups_host ? count_word(c) : nullptr);
     a.err = err_word(c);
-    if (n) {
-        if ((st = ws_ensure(c, vdf::segreduce_workspace_bytes(n, nvals))) != VDF_OK) return st;
-        c->launches++;
-    }
-    cudaError_t e = vdf::run_segreduce(a, c->ws, s, prof_of(c));
+    if (n && (st = ws_ensure(c, vdf::segreduce_workspace_bytes(n, nvals))) != VDF_OK) return st;
+    int launched = 0;
+    cudaError_t e = vdf::run_segreduce(a, c->ws, s, prof_of(c), &launched);
+    c->launches += launched;
     if (e != cudaSuccess) return from_cuda(c, e, "segmented reduction");
     return finish_groups(c, a.n_groups, n_groups_host, s);
 }
@@ -646,8 +646,10 @@ vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* st
     a.row_group = x->row_group_out;
     a.n_groups = x->n_groups_dev ? x->n_groups_dev : (x->n_groups_host ? count_word(c) : nullptr);
     a.err = err_word(c);
-    c->launches++;
-    if ((e = vdf::run_segreduce(a, tws, s, prof_of(c))) != cudaSuccess) return from_cuda(c, e, "segmented reduction");
+    int launched = 0;
+    e = vdf::run_segreduce(a, tws, s, prof_of(c), &launched);
+    c->launches += launched;
+    if (e != cudaSuccess) return from_cuda(c, e, "segmented reduction");
     return finish_groups(c, a.n_groups, x->n_groups_host, s);
 }
 

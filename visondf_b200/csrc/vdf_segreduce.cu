@@ -29,6 +29,8 @@
 // gathers them first with the high-occupancy gather kernel: a random read
 // costs a full DRAM access of 64 bytes, so each gathered value is read
 // randomly exactly once and everything here is sequential).
+#include <algorithm>
+
 #include "vdf_common.cuh"
 #include "vdf_internal.h"
 
@@ -306,68 +308,79 @@ __device__ __forceinline__ void emit_group(const SegArgs& a, uint32_t g, uint32_
     }
 }
 
-constexpr int kSegThreads = 256;
-constexpr int kSegItems = 4;
+// Rows per lane of a warp tile: more rows amortise the tile's look-back;
+// fewer keep registers free when many value columns are aggregated.
+// 8 rows per lane: one byte of the head bitmap per lane, 256 rows per tile.
+struct SegShape {
+    static constexpr int ITEMS = 8;
+    static constexpr int ROWS = 32 * ITEMS;  // rows per warp tile
+};
+constexpr int kSegThreads = 256;  // 8 independent warp tiles per CTA
 
-template <int NK, int NV, int THREADS, int ITEMS>
-__global__ void __launch_bounds__(THREADS, (NV >= 3 ? 1 : 2)) k_segreduce(SegArgs a) {
-    constexpr int WARPS = THREADS / 32;
-    constexpr int TILE = THREADS * ITEMS;
-    __shared__ Agg<NV> s_agg[THREADS];
-    __shared__ Agg<NV> s_prefix;
-    __shared__ uint32_t s_tile;
-
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (tid == 0) s_tile = atomicAdd(a.tile_counter, 1u);
-    __syncthreads();
-    const uint32_t tile = s_tile;
+// One WARP is one tile: it loads 32 x ITEMS consecutive rows (ITEMS per lane),
+// scans them with shuffles, resolves its prefix with a decoupled look-back
+// over earlier warp tiles and emits the groups that end in its rows.  There
+// is no CTA-wide barrier, so while one warp waits on a predecessor's record
+// the other resident warps keep the memory system busy.
+// NK > 0: segment heads are found by comparing the NK key columns of
+// adjacent rows (and written to a.heads_out, one bit per row, when set);
+// NK == 0: they are read from a.heads_in, so a value column can be reduced
+// in its own launch without re-reading the keys.
+template <int NK, int NV>
+__global__ void __launch_bounds__(kSegThreads, (NV > 0 || NK > 2) ? 3 : 4) k_segreduce(SegArgs a, uint32_t tiles) {
+    constexpr int ITEMS = SegShape::ITEMS;
+    constexpr int ROWS = SegShape::ROWS;
+    const int lane = threadIdx.x & 31;
+    uint32_t tile = 0;
+    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
+    tile = __shfl_sync(0xffffffffu, tile, 0);
+    if (tile >= tiles) return;  // whole warp
     const uint64_t n = a.n;
-    const uint64_t row0 = (uint64_t)tile * TILE + (uint64_t)tid * ITEMS;
+    const uint64_t row0 = (uint64_t)tile * ROWS + (uint64_t)lane * ITEMS;
     Rec<NV>* recs = reinterpret_cast<Rec<NV>*>(a.status);
 
     int vc[NV > 0 ? NV : 1];
 #pragma unroll
     for (int v = 0; v < NV; ++v) vc[v] = vclass(a.val[v].dtype);
-    int kw[NK];
+    int kw[NK > 0 ? NK : 1];
 #pragma unroll
     for (int k = 0; k < NK; ++k) kw[k] = dtype_width(a.key[k].dtype);
 
-    // ---- phase A: load this thread's rows, find segment heads and fold the
-    //      rows into the thread aggregate.  Row data is not kept live across
-    //      the scan below (phase B reloads it, from L1/L2). -------------------
+    // ---- phase A: load this lane's rows, find segment heads, fold ----------
     uint32_t hmask = 0;
     Agg<NV> t = agg_identity<NV>();
     {
-        uint64_t key[ITEMS][NK];
         uint64_t val[ITEMS][NV > 0 ? NV : 1];
 #pragma unroll
-        for (int k = 0; k < NK; ++k) load_rows<ITEMS>(a.key[k].src, kw[k], row0, n, key, k);
-#pragma unroll
         for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
-        uint64_t prev[NK];
+        if (NK == 0) {
+            hmask = row0 < n ? a.heads_in[(uint64_t)tile * 32 + lane] : 0u;
+        } else {
+            uint64_t key[ITEMS][NK > 0 ? NK : 1];
 #pragma unroll
-        for (int k = 0; k < NK; ++k) prev[k] = __shfl_up_sync(0xffffffffu, key[ITEMS - 1][k], 1);
-        if (lane == 0 && row0 > 0 && row0 < n) {
+            for (int k = 0; k < NK; ++k) load_rows<ITEMS>(a.key[k].src, kw[k], row0, n, key, k);
+            uint64_t prev[NK > 0 ? NK : 1];
 #pragma unroll
-            for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], row0 - 1);
-        }
+            for (int k = 0; k < NK; ++k) prev[k] = __shfl_up_sync(0xffffffffu, key[ITEMS - 1][k], 1);
+            if (lane == 0 && row0 > 0 && row0 < n) {
 #pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            const uint64_t r = row0 + j;
-            bool h = (r == 0);
+                for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], row0 - 1);
+            }
 #pragma unroll
-            for (int k = 0; k < NK; ++k) h |= (j == 0 ? prev[k] : key[j - 1][k]) != key[j][k];
-            if (r < n && h) hmask |= 1u << j;
+            for (int j = 0; j < ITEMS; ++j) {
+                const uint64_t r = row0 + j;
+                bool h = (r == 0);
+#pragma unroll
+                for (int k = 0; k < NK; ++k) h |= (j == 0 ? prev[k] : key[j - 1][k]) != key[j][k];
+                if (r < n && h) hmask |= 1u << j;
+            }
+            if (a.heads_out) a.heads_out[(uint64_t)tile * 32 + lane] = (uint8_t)hmask;
         }
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
             if (row0 + j >= n) break;
-            if ((hmask >> j) & 1u) {
-                t.heads++;
-                t.cnt = 1;
-#pragma unroll
-                for (int v = 0; v < NV; ++v) col_init(t.w[v], val[j][v], vc[v]);
-            } else if (t.cnt == 0) {
+            if (((hmask >> j) & 1u) || t.cnt == 0) {
+                if ((hmask >> j) & 1u) t.heads++;
                 t.cnt = 1;
 #pragma unroll
                 for (int v = 0; v < NV; ++v) col_init(t.w[v], val[j][v], vc[v]);
@@ -383,35 +396,16 @@ __global__ void __launch_bounds__(THREADS, (NV >= 3 ? 1 : 2)) k_segreduce(SegArg
         }
     }
 
-    // ---- block scan (raking, in shared memory) and decoupled look-back -------
-    // Thread aggregates go to shared memory; warp 0 folds 8 consecutive ones
-    // per lane, scans the 32 lane totals with shuffles, writes each thread's
-    // exclusive prefix back, then resolves the tile prefix against earlier
-    // tiles.  Keeping the scan in one warp keeps few aggregate copies live.
-    s_agg[tid] = t;
-    __syncthreads();
-    if (warp == 0) {
-        constexpr int R = THREADS / 32;
-        Agg<NV> acc = agg_identity<NV>();
+    // ---- warp scan and decoupled look-back -------------------------------
+    Agg<NV> incl = t;
 #pragma unroll
-        for (int i = 0; i < R; ++i) acc = agg_combine(acc, s_agg[lane * R + i], vc);
-        Agg<NV> incl = acc;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const Agg<NV> o = agg_shfl_up(incl, d);
-            if (lane >= d) incl = agg_combine(o, incl, vc);
-        }
+    for (int d = 1; d < 32; d <<= 1) {
+        const Agg<NV> o = agg_shfl_up(incl, d);
+        if (lane >= d) incl = agg_combine(o, incl, vc);
+    }
+    Agg<NV> X = agg_identity<NV>();
+    {
         const Agg<NV> total = agg_shfl(incl, 31);
-        Agg<NV> run = agg_shfl_up(incl, 1);
-        if (lane == 0) run = agg_identity<NV>();
-#pragma unroll
-        for (int i = 0; i < R; ++i) {
-            const Agg<NV> cur = s_agg[lane * R + i];
-            s_agg[lane * R + i] = run;
-            run = agg_combine(run, cur, vc);
-        }
-
-        Agg<NV> X = agg_identity<NV>();
         if (tile == 0) {
             if (lane == 0) rec_write(&recs[0], total, REC_INC);
         } else {
@@ -443,13 +437,12 @@ __global__ void __launch_bounds__(THREADS, (NV >= 3 ? 1 : 2)) k_segreduce(SegArg
             }
             if (lane == 0) rec_write(&recs[tile], agg_combine(X, total, vc), REC_INC);
         }
-        if (lane == 0) s_prefix = X;
     }
-    __syncthreads();
-    const Agg<NV> thr_excl = s_agg[tid];
+    Agg<NV> lane_excl = agg_shfl_up(incl, 1);
+    if (lane == 0) lane_excl = agg_identity<NV>();
+    const Agg<NV> pre = agg_combine(X, lane_excl, vc);
 
-    // ---- emit completed segments --------------------------------------------
-    const Agg<NV> pre = agg_combine(s_prefix, thr_excl, vc);
+    // ---- phase B: emit the segments that end in this lane's rows -------------
     // Every row contributes at most one head, so a prefix claiming more heads
     // (or a longer open segment) than rows before row0 can only come from a
     // timed-out look-back: record it and write nothing rather than out of bounds.
@@ -500,18 +493,17 @@ __global__ void __launch_bounds__(THREADS, (NV >= 3 ? 1 : 2)) k_segreduce(SegArg
 
 template <int NK, int NV>
 cudaError_t launch_seg(const SegArgs& a, uint32_t tiles, cudaStream_t s) {
-    k_segreduce<NK, NV, kSegThreads, kSegItems><<<tiles, kSegThreads, 0, s>>>(a);
+    const uint32_t blocks = (tiles + kSegThreads / 32 - 1) / (kSegThreads / 32);
+    k_segreduce<NK, NV><<<blocks, kSegThreads, 0, s>>>(a, tiles);
     return cudaGetLastError();
 }
 
-template <int NK>
-cudaError_t launch_seg_nv(const SegArgs& a, uint32_t tiles, cudaStream_t s) {
-    switch (a.nvals) {
-    case 0: return launch_seg<NK, 0>(a, tiles, s);
-    case 1: return launch_seg<NK, 1>(a, tiles, s);
-    case 2: return launch_seg<NK, 2>(a, tiles, s);
-    case 3: return launch_seg<NK, 3>(a, tiles, s);
-    default: return launch_seg<NK, 4>(a, tiles, s);
+cudaError_t launch_heads(const SegArgs& a, uint32_t tiles, cudaStream_t s) {
+    switch (a.nkeys) {
+    case 1: return launch_seg<1, 0>(a, tiles, s);
+    case 2: return launch_seg<2, 0>(a, tiles, s);
+    case 3: return launch_seg<3, 0>(a, tiles, s);
+    default: return launch_seg<4, 0>(a, tiles, s);
     }
 }
 
@@ -527,31 +519,63 @@ size_t rec_bytes(int nvals) {
 
 }  // namespace
 
+cudaError_t prepare_segreduce_kernels() { return cudaSuccess; }
+
+uint32_t seg_tiles(uint64_t n) { return (uint32_t)((n + SegShape::ROWS - 1) / SegShape::ROWS); }
+
+// [counter+err 256 B][head bitmap: 32 B per tile][look-back records]
 size_t segreduce_workspace_bytes(uint64_t n, int nvals) {
-    const uint64_t tiles = (n + kSegThreads * kSegItems - 1) / (kSegThreads * kSegItems);
-    return 256 + (size_t)tiles * rec_bytes(nvals);
+    (void)nvals;
+    const size_t tiles = seg_tiles(n);
+    return 256 + tiles * 32 + tiles * std::max(rec_bytes(0), rec_bytes(1));
 }
 
-cudaError_t run_segreduce(SegArgs a, unsigned char* ws, cudaStream_t s, Profiler* prof) {
+// The keys pass (group boundaries, keys, counts, group starts, row groups,
+// head bitmap) runs first; then one launch per value column reads the head
+// bitmap and that column.  Each launch carries only its own small scan state.
+cudaError_t run_segreduce(SegArgs a, unsigned char* ws, cudaStream_t s, Profiler* prof, int* launches) {
     cudaError_t e;
     if (a.n == 0) {
         if (a.n_groups) return cudaMemsetAsync(a.n_groups, 0, sizeof(uint64_t), s);
         return cudaSuccess;
     }
-    const size_t bytes = segreduce_workspace_bytes(a.n, a.nvals);
-    if ((e = cudaMemsetAsync(ws, 0, bytes, s)) != cudaSuccess) return e;
+    const uint32_t tiles = seg_tiles(a.n);
+    uint8_t* bitmap = ws + 256;
+    unsigned char* recs = bitmap + (size_t)tiles * 32;
     a.tile_counter = reinterpret_cast<uint32_t*>(ws);
-    a.status = ws + 256;
-    const uint32_t tiles = (uint32_t)((a.n + kSegThreads * kSegItems - 1) / (kSegThreads * kSegItems));
+    a.status = recs;
+    a.heads_out = bitmap;
+    a.heads_in = bitmap;
+    const size_t rb0 = rec_bytes(0), rb1 = rec_bytes(1);
+    if ((e = cudaMemsetAsync(ws, 0, 256, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(recs, 0, (size_t)tiles * rb0, s)) != cudaSuccess) return e;
+    SegArgs k1 = a;
+    k1.nvals = 0;
     if (prof) prof->begin(KC_SEGREDUCE, s);
-    switch (a.nkeys) {
-    case 1: e = launch_seg_nv<1>(a, tiles, s); break;
-    case 2: e = launch_seg_nv<2>(a, tiles, s); break;
-    case 3: e = launch_seg_nv<3>(a, tiles, s); break;
-    default: e = launch_seg_nv<4>(a, tiles, s); break;
-    }
+    e = launch_heads(k1, tiles, s);
     if (prof) prof->end(KC_SEGREDUCE, s);
-    return e;
+    if (launches) ++*launches;
+    if (e != cudaSuccess) return e;
+    for (int v = 0; v < a.nvals; ++v) {
+        if ((e = cudaMemsetAsync(ws, 0, 4, s)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(recs, 0, (size_t)tiles * rb1, s)) != cudaSuccess) return e;
+        SegArgs k2{};
+        k2.n = a.n;
+        k2.nkeys = 0;
+        k2.nvals = 1;
+        k2.val[0] = a.val[v];
+        k2.agg[0] = a.agg[v];
+        k2.heads_in = bitmap;
+        k2.tile_counter = a.tile_counter;
+        k2.status = recs;
+        k2.err = a.err;
+        if (prof) prof->begin(KC_SEGREDUCE, s);
+        e = launch_seg<0, 1>(k2, tiles, s);
+        if (prof) prof->end(KC_SEGREDUCE, s);
+        if (launches) ++*launches;
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 }  // namespace vdf
