@@ -134,17 +134,12 @@ struct SegArgs {
     uint32_t* group_start;     // first sorted row of each group (may be null)
     uint32_t* row_group;       // group index of each sorted row (may be null)
     uint64_t* n_groups;        // device word: number of groups (may be null)
-    // workspace (filled by run_segreduce)
-    uint8_t* heads_out;        // head bitmap written by the keys pass
-    const uint8_t* heads_in;   // head bitmap read by the value passes
-    unsigned char* status;     // per-tile look-back records
-    uint32_t* tile_counter;
-    uint32_t* err;
+    uint32_t* err;             // error word
 };
 size_t segreduce_workspace_bytes(uint64_t n, int nvals);
 cudaError_t prepare_segreduce_kernels();
-// a.err must point at the caller's error word; the workspace fields of `a`
-// are filled here.
+// Three launches: tile aggregates, their scan (one CTA), then the emit pass.
+// The workspace holds the tile aggregates (segreduce_workspace_bytes).
 cudaError_t run_segreduce(SegArgs a, unsigned char* ws, cudaStream_t s, Profiler* prof = nullptr,
                           int* launches = nullptr);
 

@@ -13,12 +13,17 @@
 //       (heads, open-segment partial {count, per column sum/min/max}),
 //     combined with the associative reduce-by-key operator
 //       A (+) B = (A.heads + B.heads, B.heads ? B.partial : A.partial (+) B.partial);
-//   * a block scan gives each thread its in-tile prefix, and a decoupled
-//     look-back over earlier tiles' published aggregates (32 predecessors
-//     per warp step) gives the tile's global prefix: the number of groups
-//     before it and the partial of the segment that runs into it;
-//   * each thread then walks its rows once more and writes every segment
-//     that ends inside its rows (keys, count, sum, min, max, mean).
+//   * k_seg_tiles reduces every tile of rows to one aggregate (all tiles in
+//     parallel, no waiting on other tiles);
+//   * k_seg_scan (one CTA) turns the tile aggregates into exclusive tile
+//     prefixes: the number of groups before each tile and the partial of the
+//     segment that runs into it;
+//   * k_seg_emit re-reads each tile, block-scans it seeded with its prefix,
+//     and writes every segment that ends inside it (keys, count, sum, min,
+//     max, mean), staged per warp in shared memory so that each output
+//     column is written by consecutive lanes at consecutive group ids.
+// Nothing spins on another CTA, so there is no look-back latency chain: the
+// price is one extra sequential read of the key and value columns.
 //
 // Exactness: integer sums are 128-bit (lo, hi words); float sums are carried
 // as (sum, compensation) with an error-free TwoSum at every combine, so a
@@ -232,43 +237,6 @@ __device__ __forceinline__ Agg<NV> agg_shfl(const Agg<NV>& a, int src) {
     return r;
 }
 
-// Look-back record of one tile.  The aggregate and the inclusive prefix live
-// in separate slots, each written once before its flag is raised, so a
-// reader never sees a slot being overwritten.
-constexpr uint32_t REC_AGG = 1, REC_INC = 2;
-template <int NV>
-struct Rec {
-    uint32_t flag;
-    uint32_t pad;
-    Agg<NV> slot[2];  // [0] aggregate, [1] inclusive prefix
-};
-
-template <int NV>
-__device__ __forceinline__ void rec_write(Rec<NV>* r, const Agg<NV>& a, uint32_t flag) {
-    Agg<NV>* dst = &r->slot[flag == REC_INC ? 1 : 0];
-    st_relaxed_u32(&dst->heads, a.heads);
-    st_relaxed_u32(&dst->cnt, a.cnt);
-#pragma unroll
-    for (int v = 0; v < NV; ++v)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) st_relaxed_u64(&dst->w[v][q], a.w[v][q]);
-    __threadfence();
-    st_release_u32(&r->flag, flag);
-}
-template <int NV>
-__device__ __forceinline__ Agg<NV> rec_read(const Rec<NV>* r, uint32_t flag) {
-    const Agg<NV>* src = &r->slot[flag == REC_INC ? 1 : 0];
-    Agg<NV> a;
-    a.heads = ld_relaxed_u32(&src->heads);
-    a.cnt = ld_relaxed_u32(&src->cnt);
-#pragma unroll
-    for (int v = 0; v < NV; ++v)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) a.w[v][q] = ld_relaxed_u64(&src->w[v][q]);
-    if (NV == 0) a.w[0][0] = 0;
-    return a;
-}
-
 __device__ __forceinline__ double i128_to_double(uint64_t lo, uint64_t hi, bool is_signed) {
     if (is_signed) {
         if ((int64_t)hi == ((int64_t)lo >> 63)) return (double)(int64_t)lo;
@@ -310,146 +278,211 @@ __device__ __forceinline__ void emit_group(const SegArgs& a, uint32_t g, uint32_
 
 // Rows per lane of a warp tile: more rows amortise the tile's look-back;
 // fewer keep registers free when many value columns are aggregated.
-// 8 rows per lane: one byte of the head bitmap per lane, 256 rows per tile.
-struct SegShape {
-    static constexpr int ITEMS = 8;
-    static constexpr int ROWS = 32 * ITEMS;  // rows per warp tile
+
+// Per-warp staging of completed groups (records) and new groups (keys).
+template <int NK, int NV, int ITEMS>
+struct WarpStage {
+    static constexpr int ROWS = ITEMS * 32;
+    uint64_t w[ROWS + 1][NV > 0 ? NV : 1][4];
+    uint64_t key[ROWS][NK];
+    uint32_t cnt[ROWS + 1];
+    uint32_t start[ROWS];
+    __device__ __forceinline__ void put(uint32_t i, uint32_t c, const uint64_t (*src)[4]) {
+        cnt[i] = c;
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) w[i][v][q] = src[v][q];
+    }
 };
-constexpr int kSegThreads = 256;  // 8 independent warp tiles per CTA
 
-// One WARP is one tile: it loads 32 x ITEMS consecutive rows (ITEMS per lane),
-// scans them with shuffles, resolves its prefix with a decoupled look-back
-// over earlier warp tiles and emits the groups that end in its rows.  There
-// is no CTA-wide barrier, so while one warp waits on a predecessor's record
-// the other resident warps keep the memory system busy.
-// NK > 0: segment heads are found by comparing the NK key columns of
-// adjacent rows (and written to a.heads_out, one bit per row, when set);
-// NK == 0: they are read from a.heads_in, so a value column can be reduced
-// in its own launch without re-reading the keys.
+constexpr int kSegThreads = 256;
+constexpr int kSegItems = 4;
+constexpr int kSegTile = kSegThreads * kSegItems;  // rows per tile
+
+extern __shared__ __align__(16) unsigned char seg_smem[];
+
 template <int NK, int NV>
-__global__ void __launch_bounds__(kSegThreads, (NV > 0 || NK > 2) ? 3 : 4) k_segreduce(SegArgs a, uint32_t tiles) {
-    constexpr int ITEMS = SegShape::ITEMS;
-    constexpr int ROWS = SegShape::ROWS;
-    const int lane = threadIdx.x & 31;
-    uint32_t tile = 0;
-    if (lane == 0) tile = atomicAdd(a.tile_counter, 1u);
-    tile = __shfl_sync(0xffffffffu, tile, 0);
-    if (tile >= tiles) return;  // whole warp
+__host__ __device__ constexpr size_t stage_offset() {
+    return ((sizeof(Agg<NV>) * (kSegThreads + 1) + 15) / 16) * 16;
+}
+template <int NK, int NV>
+__host__ __device__ constexpr size_t emit_smem_bytes() {
+    return stage_offset<NK, NV>() + sizeof(WarpStage<NK, NV, kSegItems>) * (kSegThreads / 32);
+}
+
+// Head flags and the fold of this thread's rows into one aggregate.
+template <int NK, int NV>
+__device__ __forceinline__ Agg<NV> fold_rows(const SegArgs& a, uint64_t row0, int lane, const int* vc, const int* kw,
+                                             uint32_t& hmask) {
+    constexpr int ITEMS = kSegItems;
     const uint64_t n = a.n;
-    const uint64_t row0 = (uint64_t)tile * ROWS + (uint64_t)lane * ITEMS;
-    Rec<NV>* recs = reinterpret_cast<Rec<NV>*>(a.status);
-
-    int vc[NV > 0 ? NV : 1];
+    uint64_t key[ITEMS][NK];
+    uint64_t val[ITEMS][NV > 0 ? NV : 1];
 #pragma unroll
-    for (int v = 0; v < NV; ++v) vc[v] = vclass(a.val[v].dtype);
-    int kw[NK > 0 ? NK : 1];
+    for (int k = 0; k < NK; ++k) load_rows<ITEMS>(a.key[k].src, kw[k], row0, n, key, k);
 #pragma unroll
-    for (int k = 0; k < NK; ++k) kw[k] = dtype_width(a.key[k].dtype);
-
-    // ---- phase A: load this lane's rows, find segment heads, fold ----------
-    uint32_t hmask = 0;
+    for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
+    uint64_t prev[NK];
+#pragma unroll
+    for (int k = 0; k < NK; ++k) prev[k] = __shfl_up_sync(0xffffffffu, key[ITEMS - 1][k], 1);
+    if (lane == 0 && row0 > 0 && row0 < n) {
+#pragma unroll
+        for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], row0 - 1);
+    }
+    hmask = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint64_t r = row0 + j;
+        bool h = (r == 0);
+#pragma unroll
+        for (int k = 0; k < NK; ++k) h |= (j == 0 ? prev[k] : key[j - 1][k]) != key[j][k];
+        if (r < n && h) hmask |= 1u << j;
+    }
     Agg<NV> t = agg_identity<NV>();
-    {
-        uint64_t val[ITEMS][NV > 0 ? NV : 1];
 #pragma unroll
-        for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
-        if (NK == 0) {
-            hmask = row0 < n ? a.heads_in[(uint64_t)tile * 32 + lane] : 0u;
+    for (int j = 0; j < ITEMS; ++j) {
+        if (row0 + j >= n) break;
+        if (((hmask >> j) & 1u) || t.cnt == 0) {
+            if ((hmask >> j) & 1u) t.heads++;
+            t.cnt = 1;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) col_init(t.w[v], val[j][v], vc[v]);
         } else {
-            uint64_t key[ITEMS][NK > 0 ? NK : 1];
+            t.cnt++;
 #pragma unroll
-            for (int k = 0; k < NK; ++k) load_rows<ITEMS>(a.key[k].src, kw[k], row0, n, key, k);
-            uint64_t prev[NK > 0 ? NK : 1];
-#pragma unroll
-            for (int k = 0; k < NK; ++k) prev[k] = __shfl_up_sync(0xffffffffu, key[ITEMS - 1][k], 1);
-            if (lane == 0 && row0 > 0 && row0 < n) {
-#pragma unroll
-                for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], row0 - 1);
-            }
-#pragma unroll
-            for (int j = 0; j < ITEMS; ++j) {
-                const uint64_t r = row0 + j;
-                bool h = (r == 0);
-#pragma unroll
-                for (int k = 0; k < NK; ++k) h |= (j == 0 ? prev[k] : key[j - 1][k]) != key[j][k];
-                if (r < n && h) hmask |= 1u << j;
-            }
-            if (a.heads_out) a.heads_out[(uint64_t)tile * 32 + lane] = (uint8_t)hmask;
-        }
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            if (row0 + j >= n) break;
-            if (((hmask >> j) & 1u) || t.cnt == 0) {
-                if ((hmask >> j) & 1u) t.heads++;
-                t.cnt = 1;
-#pragma unroll
-                for (int v = 0; v < NV; ++v) col_init(t.w[v], val[j][v], vc[v]);
-            } else {
-                t.cnt++;
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    uint64_t one[4];
-                    col_init(one, val[j][v], vc[v]);
-                    col_merge(t.w[v], one, vc[v]);
-                }
+            for (int v = 0; v < NV; ++v) {
+                uint64_t one[4];
+                col_init(one, val[j][v], vc[v]);
+                col_merge(t.w[v], one, vc[v]);
             }
         }
     }
+    return t;
+}
 
-    // ---- warp scan and decoupled look-back -------------------------------
-    Agg<NV> incl = t;
+template <int NK, int NV>
+__device__ __forceinline__ void seg_setup(const SegArgs& a, int* vc, int* kw) {
+#pragma unroll
+    for (int v = 0; v < NV; ++v) vc[v] = vclass(a.val[v].dtype);
+#pragma unroll
+    for (int k = 0; k < NK; ++k) kw[k] = dtype_width(a.key[k].dtype);
+}
+
+// ---- phase 1: one aggregate per tile ----------------------------------------
+template <int NK, int NV>
+__global__ void __launch_bounds__(kSegThreads) k_seg_tiles(SegArgs a, Agg<NV>* tile_agg) {
+    __shared__ Agg<NV> s_warp[kSegThreads / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t row0 = (uint64_t)blockIdx.x * kSegTile + (uint64_t)tid * kSegItems;
+    int vc[NV > 0 ? NV : 1], kw[NK];
+    seg_setup<NK, NV>(a, vc, kw);
+    uint32_t hmask;
+    Agg<NV> r = fold_rows<NK, NV>(a, row0, lane, vc, kw, hmask);
+    // ordered tree reduction: lower lanes are earlier rows
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const Agg<NV> o = agg_shfl_down(r, d);
+        if (lane + d < 32) r = agg_combine(r, o, vc);
+    }
+    if (lane == 0) s_warp[warp] = r;
+    __syncthreads();
+    if (tid == 0) {
+        Agg<NV> t = s_warp[0];
+        for (int w = 1; w < kSegThreads / 32; ++w) t = agg_combine(t, s_warp[w], vc);
+        tile_agg[blockIdx.x] = t;
+    }
+}
+
+// ---- phase 2: exclusive prefixes of the tile aggregates (one CTA) -------------
+template <int NV>
+struct ScanShape {
+    static constexpr int THREADS = NV <= 2 ? 1024 : 256;  // fewer threads when the aggregate is large
+};
+
+template <int NV>
+__global__ void __launch_bounds__(ScanShape<NV>::THREADS) k_seg_scan(const SegArgs a, Agg<NV>* tile_agg,
+                                                                     uint32_t tiles) {
+    constexpr int THREADS = ScanShape<NV>::THREADS;
+    __shared__ Agg<NV> s_warp[THREADS / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int vc[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) vc[v] = vclass(a.val[v].dtype);
+    const uint32_t per = (tiles + THREADS - 1) / THREADS;
+    const uint32_t t0 = min(tiles, (uint32_t)tid * per), t1 = min(tiles, t0 + per);
+    Agg<NV> acc = agg_identity<NV>();
+#pragma unroll 4
+    for (uint32_t t = t0; t < t1; ++t) acc = agg_combine(acc, tile_agg[t], vc);
+    Agg<NV> incl = acc;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const Agg<NV> o = agg_shfl_up(incl, d);
         if (lane >= d) incl = agg_combine(o, incl, vc);
     }
-    Agg<NV> X = agg_identity<NV>();
-    {
-        const Agg<NV> total = agg_shfl(incl, 31);
-        if (tile == 0) {
-            if (lane == 0) rec_write(&recs[0], total, REC_INC);
-        } else {
-            if (lane == 0) rec_write(&recs[tile], total, REC_AGG);
-            int64_t base = (int64_t)tile - 1;
-            while (true) {
-                const int64_t p = base - lane;
-                uint32_t f = REC_INC;
-                if (p >= 0) {
-                    uint32_t spins = 0;
-                    while ((f = ld_acquire_u32(&recs[p].flag)) == 0) {
-                        if (++spins > kSpinLimit) { atomicOr(a.err, ERR_LOOKBACK_TIMEOUT); f = REC_INC; break; }
-                        backoff(spins);
-                    }
-                }
-                const uint32_t incmask = __ballot_sync(0xffffffffu, f == REC_INC);
-                const int stop = incmask ? __ffs(incmask) - 1 : 31;
-                Agg<NV> r = agg_identity<NV>();
-                if (p >= 0 && lane <= stop) r = rec_read(&recs[p], f);
-                // chronological fold: higher lanes are older tiles
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    Agg<NV> run = agg_identity<NV>();
+    for (int w = 0; w < warp; ++w) run = agg_combine(run, s_warp[w], vc);
+    Agg<NV> lx = agg_shfl_up(incl, 1);
+    if (lane == 0) lx = agg_identity<NV>();
+    run = agg_combine(run, lx, vc);
+#pragma unroll 4
+    for (uint32_t t = t0; t < t1; ++t) {
+        const Agg<NV> cur = tile_agg[t];
+        tile_agg[t] = run;
+        run = agg_combine(run, cur, vc);
+    }
+}
+
+// ---- phase 3: scan each tile from its prefix and emit the groups -------------
+template <int NK, int NV>
+__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2)) k_seg_emit(SegArgs a, const Agg<NV>* tile_prefix) {
+    constexpr int ITEMS = kSegItems;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint64_t n = a.n;
+    const uint64_t row0 = (uint64_t)blockIdx.x * kSegTile + (uint64_t)tid * ITEMS;
+    Agg<NV>* s_agg = reinterpret_cast<Agg<NV>*>(seg_smem);
+    int vc[NV > 0 ? NV : 1], kw[NK];
+    seg_setup<NK, NV>(a, vc, kw);
+    uint32_t hmask;
+    s_agg[tid] = fold_rows<NK, NV>(a, row0, lane, vc, kw, hmask);
+    if (tid == 0) s_agg[kSegThreads] = tile_prefix[blockIdx.x];
+    __syncthreads();
+    // raking scan: warp 0 folds 8 consecutive thread aggregates per lane
+    if (warp == 0) {
+        constexpr int R = kSegThreads / 32;
+        Agg<NV> acc = agg_identity<NV>();
 #pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const Agg<NV> o = agg_shfl_down(r, d);
-                    if (lane + d < 32) r = agg_combine(o, r, vc);
-                }
-                X = agg_combine(agg_shfl(r, 0), X, vc);
-                if (incmask) break;
-                base -= 32;
-            }
-            if (lane == 0) rec_write(&recs[tile], agg_combine(X, total, vc), REC_INC);
+        for (int i = 0; i < R; ++i) acc = agg_combine(acc, s_agg[lane * R + i], vc);
+        Agg<NV> incl = acc;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const Agg<NV> o = agg_shfl_up(incl, d);
+            if (lane >= d) incl = agg_combine(o, incl, vc);
+        }
+        Agg<NV> run = agg_shfl_up(incl, 1);
+        if (lane == 0) run = agg_identity<NV>();
+        run = agg_combine(s_agg[kSegThreads], run, vc);
+#pragma unroll
+        for (int i = 0; i < R; ++i) {
+            const Agg<NV> cur = s_agg[lane * R + i];
+            s_agg[lane * R + i] = run;
+            run = agg_combine(run, cur, vc);
         }
     }
-    Agg<NV> lane_excl = agg_shfl_up(incl, 1);
-    if (lane == 0) lane_excl = agg_identity<NV>();
-    const Agg<NV> pre = agg_combine(X, lane_excl, vc);
+    __syncthreads();
+    const Agg<NV> pre = s_agg[tid];
 
-    // ---- phase B: emit the segments that end in this lane's rows -------------
-    // Every row contributes at most one head, so a prefix claiming more heads
-    // (or a longer open segment) than rows before row0 can only come from a
-    // timed-out look-back: record it and write nothing rather than out of bounds.
-    if (row0 < n && (pre.heads > row0 || pre.cnt > row0 || (row0 > 0 && pre.heads == 0))) {
-        atomicOr(a.err, ERR_BAD_INDEX);
-        return;
-    }
+    // A segment is complete when the next head (or the last row) is reached;
+    // the thread that reaches it produces the group's record.  The groups a
+    // warp completes, and the groups whose heads lie in its rows, have
+    // consecutive ids, so records and keys are staged in the warp's shared
+    // memory and every output column is then written by consecutive lanes.
+    using Stage = WarpStage<NK, NV, ITEMS>;
+    Stage& st = reinterpret_cast<Stage*>(seg_smem + stage_offset<NK, NV>())[warp];
+    const uint32_t H_w = __shfl_sync(0xffffffffu, pre.heads, 0);  // heads before the warp's first row
+    const uint32_t g0 = H_w > 0 ? H_w - 1 : 0;                     // first group the warp completes
     uint32_t gid = pre.heads;
     uint32_t cnt = pre.cnt;
     uint64_t w[NV > 0 ? NV : 1][4];
@@ -457,20 +490,26 @@ __global__ void __launch_bounds__(kSegThreads, (NV > 0 || NK > 2) ? 3 : 4) k_seg
     for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[v][q] = pre.w[v][q];
+    uint32_t rg[ITEMS];
+    uint32_t emitted = 0;
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const uint64_t r = row0 + j;
+        rg[j] = 0;
         if (r >= n) break;
         uint64_t val[NV > 0 ? NV : 1];
 #pragma unroll
         for (int v = 0; v < NV; ++v) val[v] = load_val(a.val[v].src, a.val[v].dtype, r);
         if ((hmask >> j) & 1u) {
-            if (gid > 0) emit_group<NV>(a, gid - 1, cnt, w, vc);
+            if (gid > 0) {
+                st.put(gid - 1 - g0, cnt, w);
+                ++emitted;
+            }
             ++gid;
+            const uint32_t ki = gid - 1 - H_w;
 #pragma unroll
-            for (int k = 0; k < NK; ++k)
-                if (a.key_out[k]) store_raw(a.key_out[k], kw[k], gid - 1, load_raw(a.key[k].src, kw[k], r));
-            if (a.group_start) a.group_start[gid - 1] = (uint32_t)r;
+            for (int k = 0; k < NK; ++k) st.key[ki][k] = load_raw(a.key[k].src, kw[k], r);
+            st.start[ki] = (uint32_t)r;
             cnt = 1;
 #pragma unroll
             for (int v = 0; v < NV; ++v) col_init(w[v], val[v], vc[v]);
@@ -483,99 +522,129 @@ __global__ void __launch_bounds__(kSegThreads, (NV > 0 || NK > 2) ? 3 : 4) k_seg
                 col_merge(w[v], one, vc[v]);
             }
         }
-        if (a.row_group) a.row_group[r] = gid - 1;
+        rg[j] = gid - 1;
         if (r == n - 1) {
-            emit_group<NV>(a, gid - 1, cnt, w, vc);
+            st.put(gid - 1 - g0, cnt, w);
+            ++emitted;
             if (a.n_groups) *a.n_groups = gid;
         }
+    }
+    if (a.row_group && row0 < n) {
+        if (row0 + ITEMS <= n && (reinterpret_cast<uintptr_t>(a.row_group + row0) & 15) == 0) {
+            *reinterpret_cast<uint4*>(a.row_group + row0) = make_uint4(rg[0], rg[1], rg[2], rg[3]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j)
+                if (row0 + j < n) a.row_group[row0 + j] = rg[j];
+        }
+    }
+    uint32_t E = emitted;
+    uint32_t K = __popc(hmask);
+#pragma unroll
+    for (int d = 16; d > 0; d >>= 1) {
+        E += __shfl_xor_sync(0xffffffffu, E, d);
+        K += __shfl_xor_sync(0xffffffffu, K, d);
+    }
+    __syncwarp();
+    for (uint32_t i = lane; i < E; i += 32) {
+        uint64_t gw[NV > 0 ? NV : 1][4];
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) gw[v][q] = st.w[i][v][q];
+        emit_group<NV>(a, g0 + i, st.cnt[i], gw, vc);
+    }
+    for (uint32_t i = lane; i < K; i += 32) {
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+            if (a.key_out[k]) store_raw(a.key_out[k], kw[k], H_w + i, st.key[i][k]);
+        if (a.group_start) a.group_start[H_w + i] = st.start[i];
     }
 }
 
 template <int NK, int NV>
-cudaError_t launch_seg(const SegArgs& a, uint32_t tiles, cudaStream_t s) {
-    const uint32_t blocks = (tiles + kSegThreads / 32 - 1) / (kSegThreads / 32);
-    k_segreduce<NK, NV><<<blocks, kSegThreads, 0, s>>>(a, tiles);
+cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaStream_t s) {
+    Agg<NV>* ta = reinterpret_cast<Agg<NV>*>(aggs);
+    k_seg_tiles<NK, NV><<<tiles, kSegThreads, 0, s>>>(a, ta);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_seg_scan<NV><<<1, ScanShape<NV>::THREADS, 0, s>>>(a, ta, tiles);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_seg_emit<NK, NV><<<tiles, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta);
     return cudaGetLastError();
 }
 
-cudaError_t launch_heads(const SegArgs& a, uint32_t tiles, cudaStream_t s) {
-    switch (a.nkeys) {
-    case 1: return launch_seg<1, 0>(a, tiles, s);
-    case 2: return launch_seg<2, 0>(a, tiles, s);
-    case 3: return launch_seg<3, 0>(a, tiles, s);
-    default: return launch_seg<4, 0>(a, tiles, s);
+template <int NK, int NV>
+cudaError_t seg_attr() {
+    constexpr size_t smem = emit_smem_bytes<NK, NV>();
+    static_assert(smem <= 227 * 1024, "group-by shared memory exceeds the per-CTA limit");
+    return cudaFuncSetAttribute(k_seg_emit<NK, NV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+template <int NK>
+cudaError_t seg_attrs() {
+    cudaError_t e;
+    if ((e = seg_attr<NK, 0>()) != cudaSuccess) return e;
+    if ((e = seg_attr<NK, 1>()) != cudaSuccess) return e;
+    if ((e = seg_attr<NK, 2>()) != cudaSuccess) return e;
+    if ((e = seg_attr<NK, 3>()) != cudaSuccess) return e;
+    return seg_attr<NK, 4>();
+}
+
+template <int NK>
+cudaError_t seg_run_nv(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaStream_t s) {
+    switch (a.nvals) {
+    case 0: return seg_run<NK, 0>(a, aggs, tiles, s);
+    case 1: return seg_run<NK, 1>(a, aggs, tiles, s);
+    case 2: return seg_run<NK, 2>(a, aggs, tiles, s);
+    case 3: return seg_run<NK, 3>(a, aggs, tiles, s);
+    default: return seg_run<NK, 4>(a, aggs, tiles, s);
     }
 }
 
-size_t rec_bytes(int nvals) {
+size_t agg_bytes(int nvals) {
     switch (nvals) {
-    case 0: return sizeof(Rec<0>);
-    case 1: return sizeof(Rec<1>);
-    case 2: return sizeof(Rec<2>);
-    case 3: return sizeof(Rec<3>);
-    default: return sizeof(Rec<4>);
+    case 0: return sizeof(Agg<0>);
+    case 1: return sizeof(Agg<1>);
+    case 2: return sizeof(Agg<2>);
+    case 3: return sizeof(Agg<3>);
+    default: return sizeof(Agg<4>);
     }
 }
+
+uint32_t seg_tiles(uint64_t n) { return (uint32_t)((n + kSegTile - 1) / kSegTile); }
 
 }  // namespace
 
-cudaError_t prepare_segreduce_kernels() { return cudaSuccess; }
-
-uint32_t seg_tiles(uint64_t n) { return (uint32_t)((n + SegShape::ROWS - 1) / SegShape::ROWS); }
-
-// [counter+err 256 B][head bitmap: 32 B per tile][look-back records]
-size_t segreduce_workspace_bytes(uint64_t n, int nvals) {
-    (void)nvals;
-    const size_t tiles = seg_tiles(n);
-    return 256 + tiles * 32 + tiles * std::max(rec_bytes(0), rec_bytes(1));
+cudaError_t prepare_segreduce_kernels() {
+    cudaError_t e;
+    if ((e = seg_attrs<1>()) != cudaSuccess) return e;
+    if ((e = seg_attrs<2>()) != cudaSuccess) return e;
+    if ((e = seg_attrs<3>()) != cudaSuccess) return e;
+    return seg_attrs<4>();
 }
 
-// The keys pass (group boundaries, keys, counts, group starts, row groups,
-// head bitmap) runs first; then one launch per value column reads the head
-// bitmap and that column.  Each launch carries only its own small scan state.
+size_t segreduce_workspace_bytes(uint64_t n, int nvals) {
+    return 256 + (size_t)seg_tiles(n) * agg_bytes(nvals);
+}
+
 cudaError_t run_segreduce(SegArgs a, unsigned char* ws, cudaStream_t s, Profiler* prof, int* launches) {
-    cudaError_t e;
     if (a.n == 0) {
         if (a.n_groups) return cudaMemsetAsync(a.n_groups, 0, sizeof(uint64_t), s);
         return cudaSuccess;
     }
     const uint32_t tiles = seg_tiles(a.n);
-    uint8_t* bitmap = ws + 256;
-    unsigned char* recs = bitmap + (size_t)tiles * 32;
-    a.tile_counter = reinterpret_cast<uint32_t*>(ws);
-    a.status = recs;
-    a.heads_out = bitmap;
-    a.heads_in = bitmap;
-    const size_t rb0 = rec_bytes(0), rb1 = rec_bytes(1);
-    if ((e = cudaMemsetAsync(ws, 0, 256, s)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(recs, 0, (size_t)tiles * rb0, s)) != cudaSuccess) return e;
-    SegArgs k1 = a;
-    k1.nvals = 0;
     if (prof) prof->begin(KC_SEGREDUCE, s);
-    e = launch_heads(k1, tiles, s);
-    if (prof) prof->end(KC_SEGREDUCE, s);
-    if (launches) ++*launches;
-    if (e != cudaSuccess) return e;
-    for (int v = 0; v < a.nvals; ++v) {
-        if ((e = cudaMemsetAsync(ws, 0, 4, s)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(recs, 0, (size_t)tiles * rb1, s)) != cudaSuccess) return e;
-        SegArgs k2{};
-        k2.n = a.n;
-        k2.nkeys = 0;
-        k2.nvals = 1;
-        k2.val[0] = a.val[v];
-        k2.agg[0] = a.agg[v];
-        k2.heads_in = bitmap;
-        k2.tile_counter = a.tile_counter;
-        k2.status = recs;
-        k2.err = a.err;
-        if (prof) prof->begin(KC_SEGREDUCE, s);
-        e = launch_seg<0, 1>(k2, tiles, s);
-        if (prof) prof->end(KC_SEGREDUCE, s);
-        if (launches) ++*launches;
-        if (e != cudaSuccess) return e;
+    cudaError_t e;
+    switch (a.nkeys) {
+    case 1: e = seg_run_nv<1>(a, ws + 256, tiles, s); break;
+    case 2: e = seg_run_nv<2>(a, ws + 256, tiles, s); break;
+    case 3: e = seg_run_nv<3>(a, ws + 256, tiles, s); break;
+    default: e = seg_run_nv<4>(a, ws + 256, tiles, s); break;
     }
-    return cudaSuccess;
+    if (prof) prof->end(KC_SEGREDUCE, s);
+    if (launches) *launches += 3;
+    return e;
 }
 
 }  // namespace vdf
