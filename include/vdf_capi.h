@@ -113,9 +113,11 @@ typedef enum vdf_kernel_class {
     VDF_KC_ONESWEEP32 = 2,  /* radix pass, 4-byte keys        */
     VDF_KC_ONESWEEP64 = 3,  /* radix pass, 8-byte keys        */
     VDF_KC_GATHER = 4,      /* payload gather                 */
-    VDF_KC_SEGREDUCE = 5,   /* group-by segmented reduction   */
+    VDF_KC_SEGREDUCE = 5,   /* group-by: per-tile aggregates  */
     VDF_KC_BROADCAST = 6,   /* transform broadcast            */
-    VDF_KC_PACK = 7         /* row-record packing for gathers */
+    VDF_KC_PACK = 7,        /* row-record packing for gathers */
+    VDF_KC_SEGSCAN = 8,     /* group-by: tile prefix scan     */
+    VDF_KC_SEGEMIT = 9      /* group-by: scan + emit groups   */
 } vdf_kernel_class;
 /* When enabled, every kernel the context launches is bracketed by CUDA
  * events on its stream (no reference counterpart: the reference has no

@@ -23,7 +23,8 @@ I32, I64, U32, U64, F64, F32 = range(6)
 # vdf_order
 ORDER_ASC, ORDER_DESC_STABLE, ORDER_DESC_REVERSE = range(3)
 
-KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast", "pack"]
+KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast", "pack",
+                  "segscan", "segemit"]
 
 TORCH_TO_VDF = {
     torch.int32: I32, torch.int64: I64, torch.uint32: U32, torch.uint64: U64,

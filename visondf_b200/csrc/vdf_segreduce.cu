@@ -279,20 +279,26 @@ __device__ __forceinline__ void emit_group(const SegArgs& a, uint32_t g, uint32_
 // Rows per lane of a warp tile: more rows amortise the tile's look-back;
 // fewer keep registers free when many value columns are aggregated.
 
-// Per-warp staging of completed groups (records) and new groups (keys).
+// Per-warp staging of completed groups (records) and new groups (keys),
+// column-major with one padding slot per 32 entries: a thread fills entries
+// 4t..4t+3 and the write-out reads consecutive entries across lanes, and the
+// skew keeps both patterns free of shared-memory bank conflicts.
 template <int NK, int NV, int ITEMS>
 struct WarpStage {
     static constexpr int ROWS = ITEMS * 32;
-    uint64_t w[ROWS + 1][NV > 0 ? NV : 1][4];
-    uint64_t key[ROWS][NK];
-    uint32_t cnt[ROWS + 1];
-    uint32_t start[ROWS];
+    static constexpr int SLOTS = ROWS + 1 + (ROWS + 1) / 32 + 1;
+    static __device__ __forceinline__ int at(uint32_t i) { return (int)(i + (i >> 5)); }
+    uint64_t w[NV > 0 ? NV : 1][4][SLOTS];
+    uint64_t key[NK][SLOTS];
+    uint32_t cnt[SLOTS];
+    uint32_t start[SLOTS];
     __device__ __forceinline__ void put(uint32_t i, uint32_t c, const uint64_t (*src)[4]) {
-        cnt[i] = c;
+        const int x = at(i);
+        cnt[x] = c;
 #pragma unroll
         for (int v = 0; v < NV; ++v)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) w[i][v][q] = src[v][q];
+            for (int q = 0; q < 4; ++q) w[v][q][x] = src[v][q];
     }
 };
 
@@ -304,7 +310,7 @@ extern __shared__ __align__(16) unsigned char seg_smem[];
 
 template <int NK, int NV>
 __host__ __device__ constexpr size_t stage_offset() {
-    return ((sizeof(Agg<NV>) * (kSegThreads + 1) + 15) / 16) * 16;
+    return ((sizeof(Agg<NV>) * (kSegThreads / 32 + 1) + 15) / 16) * 16;
 }
 template <int NK, int NV>
 __host__ __device__ constexpr size_t emit_smem_bytes() {
@@ -442,37 +448,28 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2)) k_seg_emit(Seg
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t n = a.n;
     const uint64_t row0 = (uint64_t)blockIdx.x * kSegTile + (uint64_t)tid * ITEMS;
-    Agg<NV>* s_agg = reinterpret_cast<Agg<NV>*>(seg_smem);
+    Agg<NV>* s_warp = reinterpret_cast<Agg<NV>*>(seg_smem);  // [8] warp totals, [8] tile prefix
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
     uint32_t hmask;
-    s_agg[tid] = fold_rows<NK, NV>(a, row0, lane, vc, kw, hmask);
-    if (tid == 0) s_agg[kSegThreads] = tile_prefix[blockIdx.x];
-    __syncthreads();
-    // raking scan: warp 0 folds 8 consecutive thread aggregates per lane
-    if (warp == 0) {
-        constexpr int R = kSegThreads / 32;
-        Agg<NV> acc = agg_identity<NV>();
+    const Agg<NV> t = fold_rows<NK, NV>(a, row0, lane, vc, kw, hmask);
+    // per-warp inclusive scan with shuffles, then the warp totals in order
+    Agg<NV> incl = t;
 #pragma unroll
-        for (int i = 0; i < R; ++i) acc = agg_combine(acc, s_agg[lane * R + i], vc);
-        Agg<NV> incl = acc;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const Agg<NV> o = agg_shfl_up(incl, d);
-            if (lane >= d) incl = agg_combine(o, incl, vc);
-        }
-        Agg<NV> run = agg_shfl_up(incl, 1);
-        if (lane == 0) run = agg_identity<NV>();
-        run = agg_combine(s_agg[kSegThreads], run, vc);
-#pragma unroll
-        for (int i = 0; i < R; ++i) {
-            const Agg<NV> cur = s_agg[lane * R + i];
-            s_agg[lane * R + i] = run;
-            run = agg_combine(run, cur, vc);
-        }
+    for (int d = 1; d < 32; d <<= 1) {
+        const Agg<NV> o = agg_shfl_up(incl, d);
+        if (lane >= d) incl = agg_combine(o, incl, vc);
     }
+    if (lane == 31) s_warp[warp] = incl;
+    if (tid == 0) s_warp[kSegThreads / 32] = tile_prefix[blockIdx.x];
     __syncthreads();
-    const Agg<NV> pre = s_agg[tid];
+    Agg<NV> pre = s_warp[kSegThreads / 32];
+    for (int w2 = 0; w2 < warp; ++w2) pre = agg_combine(pre, s_warp[w2], vc);
+    {
+        Agg<NV> lx = agg_shfl_up(incl, 1);
+        if (lane == 0) lx = agg_identity<NV>();
+        pre = agg_combine(pre, lx, vc);
+    }
 
     // A segment is complete when the next head (or the last row) is reached;
     // the thread that reaches it produces the group's record.  The groups a
@@ -506,9 +503,9 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2)) k_seg_emit(Seg
                 ++emitted;
             }
             ++gid;
-            const uint32_t ki = gid - 1 - H_w;
+            const int ki = Stage::at(gid - 1 - H_w);
 #pragma unroll
-            for (int k = 0; k < NK; ++k) st.key[ki][k] = load_raw(a.key[k].src, kw[k], r);
+            for (int k = 0; k < NK; ++k) st.key[k][ki] = load_raw(a.key[k].src, kw[k], r);
             st.start[ki] = (uint32_t)r;
             cnt = 1;
 #pragma unroll
@@ -547,30 +544,38 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2)) k_seg_emit(Seg
     }
     __syncwarp();
     for (uint32_t i = lane; i < E; i += 32) {
+        const int x = Stage::at(i);
         uint64_t gw[NV > 0 ? NV : 1][4];
 #pragma unroll
         for (int v = 0; v < NV; ++v)
 #pragma unroll
-            for (int q = 0; q < 4; ++q) gw[v][q] = st.w[i][v][q];
-        emit_group<NV>(a, g0 + i, st.cnt[i], gw, vc);
+            for (int q = 0; q < 4; ++q) gw[v][q] = st.w[v][q][x];
+        emit_group<NV>(a, g0 + i, st.cnt[x], gw, vc);
     }
     for (uint32_t i = lane; i < K; i += 32) {
+        const int x = Stage::at(i);
 #pragma unroll
         for (int k = 0; k < NK; ++k)
-            if (a.key_out[k]) store_raw(a.key_out[k], kw[k], H_w + i, st.key[i][k]);
-        if (a.group_start) a.group_start[H_w + i] = st.start[i];
+            if (a.key_out[k]) store_raw(a.key_out[k], kw[k], H_w + i, st.key[k][x]);
+        if (a.group_start) a.group_start[H_w + i] = st.start[x];
     }
 }
 
 template <int NK, int NV>
-cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaStream_t s) {
+cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaStream_t s, Profiler* prof) {
     Agg<NV>* ta = reinterpret_cast<Agg<NV>*>(aggs);
+    if (prof) prof->begin(KC_SEGREDUCE, s);
     k_seg_tiles<NK, NV><<<tiles, kSegThreads, 0, s>>>(a, ta);
+    if (prof) prof->end(KC_SEGREDUCE, s);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (prof) prof->begin(KC_SEGSCAN, s);
     k_seg_scan<NV><<<1, ScanShape<NV>::THREADS, 0, s>>>(a, ta, tiles);
+    if (prof) prof->end(KC_SEGSCAN, s);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (prof) prof->begin(KC_SEGEMIT, s);
     k_seg_emit<NK, NV><<<tiles, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta);
+    if (prof) prof->end(KC_SEGEMIT, s);
     return cudaGetLastError();
 }
 
@@ -592,13 +597,13 @@ cudaError_t seg_attrs() {
 }
 
 template <int NK>
-cudaError_t seg_run_nv(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaStream_t s) {
+cudaError_t seg_run_nv(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaStream_t s, Profiler* prof) {
     switch (a.nvals) {
-    case 0: return seg_run<NK, 0>(a, aggs, tiles, s);
-    case 1: return seg_run<NK, 1>(a, aggs, tiles, s);
-    case 2: return seg_run<NK, 2>(a, aggs, tiles, s);
-    case 3: return seg_run<NK, 3>(a, aggs, tiles, s);
-    default: return seg_run<NK, 4>(a, aggs, tiles, s);
+    case 0: return seg_run<NK, 0>(a, aggs, tiles, s, prof);
+    case 1: return seg_run<NK, 1>(a, aggs, tiles, s, prof);
+    case 2: return seg_run<NK, 2>(a, aggs, tiles, s, prof);
+    case 3: return seg_run<NK, 3>(a, aggs, tiles, s, prof);
+    default: return seg_run<NK, 4>(a, aggs, tiles, s, prof);
     }
 }
 
@@ -634,15 +639,13 @@ cudaError_t run_segreduce(SegArgs a, unsigned char* ws, cudaStream_t s, Profiler
         return cudaSuccess;
     }
     const uint32_t tiles = seg_tiles(a.n);
-    if (prof) prof->begin(KC_SEGREDUCE, s);
     cudaError_t e;
     switch (a.nkeys) {
-    case 1: e = seg_run_nv<1>(a, ws + 256, tiles, s); break;
-    case 2: e = seg_run_nv<2>(a, ws + 256, tiles, s); break;
-    case 3: e = seg_run_nv<3>(a, ws + 256, tiles, s); break;
-    default: e = seg_run_nv<4>(a, ws + 256, tiles, s); break;
+    case 1: e = seg_run_nv<1>(a, ws + 256, tiles, s, prof); break;
+    case 2: e = seg_run_nv<2>(a, ws + 256, tiles, s, prof); break;
+    case 3: e = seg_run_nv<3>(a, ws + 256, tiles, s, prof); break;
+    default: e = seg_run_nv<4>(a, ws + 256, tiles, s, prof); break;
     }
-    if (prof) prof->end(KC_SEGREDUCE, s);
     if (launches) *launches += 3;
     return e;
 }
