@@ -46,20 +46,20 @@ __global__ void __launch_bounds__(256) k_gather(GatherArgs g) {
             if (g.width[c] == 8) {
                 const unsigned long long* s = static_cast<const unsigned long long*>(g.src[c]);
                 ulonglong2 a, b;
-                a.x = __ldg(s + p.x);
-                a.y = __ldg(s + p.y);
-                b.x = __ldg(s + p.z);
-                b.y = __ldg(s + p.w);
+                a.x = __ldcg(s + p.x);
+                a.y = __ldcg(s + p.y);
+                b.x = __ldcg(s + p.z);
+                b.y = __ldcg(s + p.w);
                 ulonglong2* d = reinterpret_cast<ulonglong2*>(static_cast<unsigned long long*>(g.dst[c]) + r0);
                 stg_stream(d, a);
                 stg_stream(d + 1, b);
             } else {
                 const uint32_t* s = static_cast<const uint32_t*>(g.src[c]);
                 uint4 v;
-                v.x = __ldg(s + p.x);
-                v.y = __ldg(s + p.y);
-                v.z = __ldg(s + p.z);
-                v.w = __ldg(s + p.w);
+                v.x = __ldcg(s + p.x);
+                v.y = __ldcg(s + p.y);
+                v.z = __ldcg(s + p.z);
+                v.w = __ldcg(s + p.w);
                 stg_stream(reinterpret_cast<uint4*>(static_cast<uint32_t*>(g.dst[c]) + r0), v);
             }
         }
@@ -74,9 +74,9 @@ __global__ void __launch_bounds__(256) k_gather(GatherArgs g) {
         }
         for (int c = 0; c < g.ncols; ++c) {
             if (g.width[c] == 8)
-                static_cast<unsigned long long*>(g.dst[c])[r] = __ldg(static_cast<const unsigned long long*>(g.src[c]) + p);
+                static_cast<unsigned long long*>(g.dst[c])[r] = __ldcg(static_cast<const unsigned long long*>(g.src[c]) + p);
             else
-                static_cast<uint32_t*>(g.dst[c])[r] = __ldg(static_cast<const uint32_t*>(g.src[c]) + p);
+                static_cast<uint32_t*>(g.dst[c])[r] = __ldcg(static_cast<const uint32_t*>(g.src[c]) + p);
         }
     }
 }
@@ -109,11 +109,13 @@ __global__ void __launch_bounds__(256) k_gather_rec(GatherArgs g, const unsigned
         if (g.err) atomicOr(g.err, ERR_BAD_INDEX);
         p = 0;
     }
+    // L2-only loads: a non-coherent (L1) load of one record would fetch its
+    // whole 128-byte line from DRAM.
     const ulonglong2* src = reinterpret_cast<const ulonglong2*>(recs + (uint64_t)p * REC);
     unsigned long long slot[SLOTS];
 #pragma unroll
     for (int c = 0; c < SLOTS; c += 2) {
-        const ulonglong2 v = __ldg(src + c / 2);
+        const ulonglong2 v = __ldcg(src + c / 2);
         slot[c] = v.x;
         slot[c + 1] = v.y;
     }
@@ -181,7 +183,7 @@ __global__ void __launch_bounds__(256) k_broadcast(const uint32_t* row_group, ui
             atomicOr(err, ERR_BAD_INDEX);
             continue;
         }
-        static_cast<T*>(out)[dst] = __ldg(static_cast<const T*>(gvals) + g);
+        static_cast<T*>(out)[dst] = __ldcg(static_cast<const T*>(gvals) + g);
     }
 }
 

@@ -181,7 +181,8 @@ __global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
                     src = 0;
                 }
                 gval[j] = src;
-                key[j] = KeyOps<K>::order(__ldg(static_cast<const K*>(a.keys_in) + src), a.dtype, a.invert);
+                // L2-only: a random 4/8-byte read through L1 would fetch a 128-byte line
+                key[j] = KeyOps<K>::order(__ldcg(static_cast<const K*>(a.keys_in) + src), a.dtype, a.invert);
             } else {
                 key[j] = ldg_stream(static_cast<const K*>(a.keys_in) + i);
             }

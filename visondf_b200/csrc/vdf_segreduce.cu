@@ -280,14 +280,14 @@ __device__ __forceinline__ void emit_group(const SegArgs& a, uint32_t g, uint32_
 // fewer keep registers free when many value columns are aggregated.
 
 // Per-warp staging of completed groups (records) and new groups (keys),
-// column-major with one padding slot per 32 entries: a thread fills entries
-// 4t..4t+3 and the write-out reads consecutive entries across lanes, and the
-// skew keeps both patterns free of shared-memory bank conflicts.
+// column-major with one padding slot per 4 entries: a thread fills entries
+// ITEMS*t .. ITEMS*t+ITEMS-1 and the write-out reads consecutive entries
+// across lanes; the skew keeps both patterns (nearly) bank-conflict free.
 template <int NK, int NV, int ITEMS>
 struct WarpStage {
     static constexpr int ROWS = ITEMS * 32;
-    static constexpr int SLOTS = ROWS + 1 + (ROWS + 1) / 32 + 1;
-    static __device__ __forceinline__ int at(uint32_t i) { return (int)(i + (i >> 5)); }
+    static constexpr int SLOTS = ROWS + 1 + (ROWS + 1) / 4 + 1;
+    static __device__ __forceinline__ int at(uint32_t i) { return (int)(i + (i >> 2)); }
     uint64_t w[NV > 0 ? NV : 1][4][SLOTS];
     uint64_t key[NK][SLOTS];
     uint32_t cnt[SLOTS];
@@ -303,7 +303,7 @@ struct WarpStage {
 };
 
 constexpr int kSegThreads = 256;
-constexpr int kSegItems = 4;
+constexpr int kSegItems = 2;
 constexpr int kSegTile = kSegThreads * kSegItems;  // rows per tile
 
 extern __shared__ __align__(16) unsigned char seg_smem[];
@@ -400,27 +400,17 @@ __global__ void __launch_bounds__(kSegThreads) k_seg_tiles(SegArgs a, Agg<NV>* t
     }
 }
 
-// ---- phase 2: exclusive prefixes of the tile aggregates (one CTA) -------------
-template <int NV>
-struct ScanShape {
-    static constexpr int THREADS = NV <= 2 ? 1024 : 256;  // fewer threads when the aggregate is large
-};
+// ---- phase 2: exclusive prefixes of the tile aggregates ----------------------
+// Level 1: each CTA scans kScanTiles consecutive tile aggregates in place
+// (exclusive, within the CTA) and writes the CTA total; level 2: one CTA
+// turns the CTA totals into exclusive prefixes.  The emit pass combines the
+// two.
+constexpr int kScanTiles = 256;
 
 template <int NV>
-__global__ void __launch_bounds__(ScanShape<NV>::THREADS) k_seg_scan(const SegArgs a, Agg<NV>* tile_agg,
-                                                                     uint32_t tiles) {
-    constexpr int THREADS = ScanShape<NV>::THREADS;
-    __shared__ Agg<NV> s_warp[THREADS / 32];
+__device__ __forceinline__ Agg<NV> block_exclusive_scan(Agg<NV> x, Agg<NV>* s_warp, const int* vc, Agg<NV>& total) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    int vc[NV > 0 ? NV : 1];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) vc[v] = vclass(a.val[v].dtype);
-    const uint32_t per = (tiles + THREADS - 1) / THREADS;
-    const uint32_t t0 = min(tiles, (uint32_t)tid * per), t1 = min(tiles, t0 + per);
-    Agg<NV> acc = agg_identity<NV>();
-#pragma unroll 4
-    for (uint32_t t = t0; t < t1; ++t) acc = agg_combine(acc, tile_agg[t], vc);
-    Agg<NV> incl = acc;
+    Agg<NV> incl = x;
 #pragma unroll
     for (int d = 1; d < 32; d <<= 1) {
         const Agg<NV> o = agg_shfl_up(incl, d);
@@ -428,22 +418,53 @@ __global__ void __launch_bounds__(ScanShape<NV>::THREADS) k_seg_scan(const SegAr
     }
     if (lane == 31) s_warp[warp] = incl;
     __syncthreads();
-    Agg<NV> run = agg_identity<NV>();
-    for (int w = 0; w < warp; ++w) run = agg_combine(run, s_warp[w], vc);
+    Agg<NV> pre = agg_identity<NV>();
+    for (int w = 0; w < warp; ++w) pre = agg_combine(pre, s_warp[w], vc);
     Agg<NV> lx = agg_shfl_up(incl, 1);
     if (lane == 0) lx = agg_identity<NV>();
-    run = agg_combine(run, lx, vc);
-#pragma unroll 4
-    for (uint32_t t = t0; t < t1; ++t) {
-        const Agg<NV> cur = tile_agg[t];
-        tile_agg[t] = run;
+    total = agg_identity<NV>();
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) total = agg_combine(total, s_warp[w], vc);
+    return agg_combine(pre, lx, vc);
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kScanTiles) k_seg_scan1(const SegArgs a, Agg<NV>* tile_agg, Agg<NV>* block_tot,
+                                                          uint32_t tiles) {
+    __shared__ Agg<NV> s_warp[kScanTiles / 32];
+    int vc[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) vc[v] = vclass(a.val[v].dtype);
+    const uint32_t t = blockIdx.x * kScanTiles + threadIdx.x;
+    const Agg<NV> x = t < tiles ? tile_agg[t] : agg_identity<NV>();
+    Agg<NV> total;
+    const Agg<NV> ex = block_exclusive_scan(x, s_warp, vc, total);
+    if (t < tiles) tile_agg[t] = ex;
+    if (threadIdx.x == 0) block_tot[blockIdx.x] = total;
+}
+
+template <int NV>
+__global__ void __launch_bounds__(kScanTiles) k_seg_scan2(const SegArgs a, Agg<NV>* block_tot, uint32_t blocks) {
+    __shared__ Agg<NV> s_warp[kScanTiles / 32];
+    int vc[NV > 0 ? NV : 1];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) vc[v] = vclass(a.val[v].dtype);
+    const uint32_t per = (blocks + kScanTiles - 1) / kScanTiles;
+    const uint32_t b0 = min(blocks, threadIdx.x * per), b1 = min(blocks, b0 + per);
+    Agg<NV> acc = agg_identity<NV>();
+    for (uint32_t b = b0; b < b1; ++b) acc = agg_combine(acc, block_tot[b], vc);
+    Agg<NV> total;
+    Agg<NV> run = block_exclusive_scan(acc, s_warp, vc, total);
+    for (uint32_t b = b0; b < b1; ++b) {
+        const Agg<NV> cur = block_tot[b];
+        block_tot[b] = run;
         run = agg_combine(run, cur, vc);
     }
 }
 
 // ---- phase 3: scan each tile from its prefix and emit the groups -------------
 template <int NK, int NV>
-__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2)) k_seg_emit(SegArgs a, const Agg<NV>* tile_prefix) {
+__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3)) k_seg_emit(SegArgs a, const Agg<NV>* tile_prefix,
+                                                                          const Agg<NV>* block_prefix) {
     constexpr int ITEMS = kSegItems;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t n = a.n;
@@ -461,7 +482,8 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2)) k_seg_emit(Seg
         if (lane >= d) incl = agg_combine(o, incl, vc);
     }
     if (lane == 31) s_warp[warp] = incl;
-    if (tid == 0) s_warp[kSegThreads / 32] = tile_prefix[blockIdx.x];
+    if (tid == 0)
+        s_warp[kSegThreads / 32] = agg_combine(block_prefix[blockIdx.x / kScanTiles], tile_prefix[blockIdx.x], vc);
     __syncthreads();
     Agg<NV> pre = s_warp[kSegThreads / 32];
     for (int w2 = 0; w2 < warp; ++w2) pre = agg_combine(pre, s_warp[w2], vc);
@@ -527,8 +549,8 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2)) k_seg_emit(Seg
         }
     }
     if (a.row_group && row0 < n) {
-        if (row0 + ITEMS <= n && (reinterpret_cast<uintptr_t>(a.row_group + row0) & 15) == 0) {
-            *reinterpret_cast<uint4*>(a.row_group + row0) = make_uint4(rg[0], rg[1], rg[2], rg[3]);
+        if (row0 + ITEMS <= n && (reinterpret_cast<uintptr_t>(a.row_group + row0) & 7) == 0) {
+            *reinterpret_cast<uint2*>(a.row_group + row0) = make_uint2(rg[0], rg[1]);
         } else {
 #pragma unroll
             for (int j = 0; j < ITEMS; ++j)
@@ -564,17 +586,20 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2)) k_seg_emit(Seg
 template <int NK, int NV>
 cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaStream_t s, Profiler* prof) {
     Agg<NV>* ta = reinterpret_cast<Agg<NV>*>(aggs);
+    const uint32_t blocks = (tiles + kScanTiles - 1) / kScanTiles;
+    Agg<NV>* bt = ta + tiles;
     if (prof) prof->begin(KC_SEGREDUCE, s);
     k_seg_tiles<NK, NV><<<tiles, kSegThreads, 0, s>>>(a, ta);
     if (prof) prof->end(KC_SEGREDUCE, s);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (prof) prof->begin(KC_SEGSCAN, s);
-    k_seg_scan<NV><<<1, ScanShape<NV>::THREADS, 0, s>>>(a, ta, tiles);
+    k_seg_scan1<NV><<<blocks, kScanTiles, 0, s>>>(a, ta, bt, tiles);
+    k_seg_scan2<NV><<<1, kScanTiles, 0, s>>>(a, bt, blocks);
     if (prof) prof->end(KC_SEGSCAN, s);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (prof) prof->begin(KC_SEGEMIT, s);
-    k_seg_emit<NK, NV><<<tiles, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta);
+    k_seg_emit<NK, NV><<<tiles, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta, bt);
     if (prof) prof->end(KC_SEGEMIT, s);
     return cudaGetLastError();
 }
@@ -629,8 +654,10 @@ cudaError_t prepare_segreduce_kernels() {
     return seg_attrs<4>();
 }
 
+// [256 B][tile aggregates][CTA totals of the level-1 scan]
 size_t segreduce_workspace_bytes(uint64_t n, int nvals) {
-    return 256 + (size_t)seg_tiles(n) * agg_bytes(nvals);
+    const size_t tiles = seg_tiles(n);
+    return 256 + (tiles + (tiles + kScanTiles - 1) / kScanTiles) * agg_bytes(nvals);
 }
 
 cudaError_t run_segreduce(SegArgs a, unsigned char* ws, cudaStream_t s, Profiler* prof, int* launches) {
@@ -646,7 +673,7 @@ cudaError_t run_segreduce(SegArgs a, unsigned char* ws, cudaStream_t s, Profiler
     case 3: e = seg_run_nv<3>(a, ws + 256, tiles, s, prof); break;
     default: e = seg_run_nv<4>(a, ws + 256, tiles, s, prof); break;
     }
-    if (launches) *launches += 3;
+    if (launches) *launches += 4;
     return e;
 }
 
