@@ -121,27 +121,29 @@ struct OnesweepCfg {
     static constexpr int WARPS = THREADS / 32;
     static constexpr int TILE = THREADS * ITEMS;
     static constexpr int BPT = (RADIX + THREADS - 1) / THREADS;  // bins per thread
-    // shared memory: exchange buffer | per-warp counters | bin bases | misc
-    static constexpr size_t EX_BYTES = (size_t)TILE * (sizeof(K) > 4 ? sizeof(K) : 4);
+    // shared memory: keys | row ids | per-warp counters | bin bases | misc
+    static constexpr size_t KEY_BYTES = (size_t)TILE * sizeof(K);
+    static constexpr size_t VAL_BYTES = (size_t)TILE * 4;
     static constexpr size_t CNT_BYTES = (size_t)WARPS * RADIX * 4;
     static constexpr size_t GLOB_BYTES = (size_t)RADIX * 4;
-    static constexpr size_t SMEM = EX_BYTES + CNT_BYTES + GLOB_BYTES + 64 + WARPS * 4;
+    static constexpr size_t SMEM = KEY_BYTES + VAL_BYTES + CNT_BYTES + GLOB_BYTES + 64 + WARPS * 4;
 };
 
 // MATCH selects how a warp finds the lanes holding the same digit:
 // 0 = one ballot per digit bit (ALU/vote pipes), 1 = match.any (XU pipe).
-template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL, int MATCH>
-__global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
+// MINB: CTAs per SM the register allocation is sized for.
+template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL, int MATCH, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     using C = OnesweepCfg<K, BITS, THREADS, ITEMS>;
     constexpr int RADIX = C::RADIX, WARPS = C::WARPS, TILE = C::TILE, BPT = C::BPT;
     constexpr uint32_t MASK = RADIX - 1;
     extern __shared__ __align__(16) unsigned char smem[];
     K* ex_keys = reinterpret_cast<K*>(smem);
-    uint32_t* ex_vals = reinterpret_cast<uint32_t*>(smem);
-    uint32_t* wcnt = reinterpret_cast<uint32_t*>(smem + C::EX_BYTES);             // [WARPS][RADIX]
-    uint32_t* bglob = reinterpret_cast<uint32_t*>(smem + C::EX_BYTES + C::CNT_BYTES);  // [RADIX]
-    uint32_t* misc = bglob + RADIX;                                                   // [0]=tile
-    uint32_t* wsum = misc + 16;                                                       // [WARPS]
+    uint32_t* ex_vals = reinterpret_cast<uint32_t*>(smem + C::KEY_BYTES);
+    uint32_t* wcnt = reinterpret_cast<uint32_t*>(smem + C::KEY_BYTES + C::VAL_BYTES);  // [WARPS][RADIX]
+    uint32_t* bglob = wcnt + WARPS * RADIX;                                            // [RADIX]
+    uint32_t* misc = bglob + RADIX;                                                    // [0]=tile
+    uint32_t* wsum = misc + 16;                                                        // [WARPS]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) misc[0] = atomicAdd(a.tile_counter, 1u);
@@ -152,25 +154,17 @@ __global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
     const uint64_t tile_base = (uint64_t)tile * TILE;
     const uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tile_base);
 
-    // Clear this tile's row of the other status buffer for the next pass
-    // (that buffer's previous user, the pass before this one, has finished).
-    // Rows tile, tile + gridDim.x, ... so that every row a later pass with
-    // more tiles could read is cleared too.
-    if (a.status_next)
-        for (uint32_t r = tile; r < a.status_rows; r += gridDim.x)
-            for (int b = tid; b < RADIX; b += THREADS) a.status_next[(size_t)r * RADIX + b] = 0;
-
-    // ---- load keys (warp-striped: item j of lane l is tile position
-    //      warp*ITEMS*32 + j*32 + l, so positions follow row order) ----------
+    // ---- load keys and row ids (warp-striped: item j of lane l is tile
+    //      position warp*ITEMS*32 + j*32 + l, so positions follow row order) --
     K key[ITEMS];
-    uint32_t gval[ITEMS];  // IN_GATHER: the incoming permutation entries
+    uint32_t val[ITEMS];
     const uint32_t wpos = (uint32_t)warp * ITEMS * 32;
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const uint32_t pos = wpos + j * 32 + lane;
         const uint64_t i = tile_base + pos;
         key[j] = ~K(0);
-        gval[j] = 0;
+        val[j] = (uint32_t)i;  // IN_RAW: the row itself
         if (pos < valid) {
             if (IN_MODE == IN_RAW) {
                 key[j] = KeyOps<K>::order(ldg_stream(static_cast<const K*>(a.keys_in) + i), a.dtype, a.invert);
@@ -180,14 +174,23 @@ __global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
                     atomicOr(a.err, ERR_BAD_INDEX);
                     src = 0;
                 }
-                gval[j] = src;
-                // L2-only: a random 4/8-byte read through L1 would fetch a 128-byte line
+                val[j] = src;
+                // L2-only: a random read through L1 would allocate a whole line
                 key[j] = KeyOps<K>::order(__ldcg(static_cast<const K*>(a.keys_in) + src), a.dtype, a.invert);
             } else {
                 key[j] = ldg_stream(static_cast<const K*>(a.keys_in) + i);
+                val[j] = ldg_stream(a.vals_in + i);
             }
         }
     }
+
+    // Clear this tile's row of the other status buffer for the next pass
+    // (that buffer's previous user, the pass before this one, has finished).
+    // Rows tile, tile + gridDim.x, ... so that every row a later pass with
+    // more tiles could read is cleared too.
+    if (a.status_next)
+        for (uint32_t r = tile; r < a.status_rows; r += gridDim.x)
+            for (int b = tid; b < RADIX; b += THREADS) a.status_next[(size_t)r * RADIX + b] = 0;
 
     // ---- warp-local ranks and per-warp digit counts --------------------------
     // Lanes holding the same digit are found with one ballot per digit bit
@@ -270,6 +273,23 @@ __global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
                 for (int w = 0; w < WARPS; ++w) wcnt[w * RADIX + b] += bstart[k];
         }
     }
+    __syncthreads();
+
+    // ---- tile-local ranks; keys and row ids into shared memory --------------
+    // (overlaps the look-back below: other warps' global writes wait on it)
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = wpos + j * 32 + lane;
+        const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
+        uint32_t r = rank[j];
+        if (pos < valid) r += wcnt[warp * RADIX + d];
+        if (r >= (uint32_t)TILE) {  // never when the counts are consistent
+            atomicOr(a.err, ERR_BAD_INDEX);
+            r = pos;
+        }
+        ex_keys[r] = key[j];
+        ex_vals[r] = val[j];
+    }
 
     // ---- decoupled look-back per bin ---------------------------------------
 #pragma unroll
@@ -297,62 +317,28 @@ __global__ void __launch_bounds__(THREADS, 3) k_onesweep(PassArgs a) {
     }
     __syncthreads();
 
-    // ---- key exchange through shared memory, then run-coalesced writes -----
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t pos = wpos + j * 32 + lane;
-        const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
-        if (pos < valid) rank[j] += wcnt[warp * RADIX + d];
-        if (rank[j] >= (uint32_t)TILE) {  // never when the counts are consistent
-            atomicOr(a.err, ERR_BAD_INDEX);
-            rank[j] = pos;
-        }
-    }
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) ex_keys[rank[j]] = key[j];
-    __syncthreads();
-    uint32_t opos[ITEMS];
+    // ---- run-coalesced writes of keys and row ids ----------------------------
     K* kout = static_cast<K*>(a.keys_out);
 #pragma unroll
     for (int r = 0; r < ITEMS; ++r) {
         const uint32_t i = r * THREADS + tid;
-        opos[r] = 0;
         if (i < valid) {
             const K k = ex_keys[i];
+            const uint32_t v = ex_vals[i];
             const uint32_t d = (uint32_t)((k >> a.shift) & MASK);
             uint32_t p = bglob[d] + i;
             if (p >= n) {  // only after a look-back timeout: never write out of bounds
                 atomicOr(a.err, ERR_BAD_INDEX);
-                p = 0xffffffffu;
-                opos[r] = p;
                 continue;
             }
             if (FINAL && a.reverse) p = (uint32_t)(n - 1) - p;
-            opos[r] = p;
             if (FINAL) {
                 if (kout) stg_stream(kout + p, KeyOps<K>::unorder(k, a.dtype, a.invert));
             } else {
                 stg_stream(kout + p, k);
             }
+            stg_stream(a.vals_out + p, v);
         }
-    }
-    __syncthreads();
-
-    // ---- value (row id) exchange -------------------------------------------
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t pos = wpos + j * 32 + lane;
-        uint32_t v;
-        if (IN_MODE == IN_RAW) v = (uint32_t)(tile_base + pos);
-        else if (IN_MODE == IN_GATHER) v = gval[j];
-        else v = pos < valid ? ldg_stream(a.vals_in + tile_base + pos) : 0u;
-        ex_vals[rank[j]] = v;
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < ITEMS; ++r) {
-        const uint32_t i = r * THREADS + tid;
-        if (i < valid && opos[r] != 0xffffffffu) stg_stream(a.vals_out + opos[r], ex_vals[i]);
     }
 }
 
@@ -367,12 +353,12 @@ using PassKernel = void (*)(PassArgs);
 // One compiled configuration of the radix pass.  The variant table is the
 // autotuner's search space; a context selects one variant per key width.
 struct PassVariant {
-    int width, threads, items, bits, match;
+    int width, threads, items, bits, match, minb;
     size_t smem;
     PassKernel k[3][2];  // [IN_MODE][FINAL]
 };
 
-template <typename K, int THREADS, int ITEMS, int MATCH>
+template <typename K, int THREADS, int ITEMS, int MATCH, int MINB>
 PassVariant make_variant() {
     using C = OnesweepCfg<K, kBits, THREADS, ITEMS>;
     PassVariant v{};
@@ -381,21 +367,29 @@ PassVariant make_variant() {
     v.items = ITEMS;
     v.bits = kBits;
     v.match = MATCH;
+    v.minb = MINB;
     v.smem = C::SMEM;
-    v.k[IN_RAW][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_RAW, false, MATCH>;
-    v.k[IN_GATHER][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_GATHER, false, MATCH>;
-    v.k[IN_BUF][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_BUF, false, MATCH>;
-    v.k[IN_RAW][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_RAW, true, MATCH>;
-    v.k[IN_GATHER][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_GATHER, true, MATCH>;
-    v.k[IN_BUF][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_BUF, true, MATCH>;
+    v.k[IN_RAW][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_RAW, false, MATCH, MINB>;
+    v.k[IN_GATHER][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_GATHER, false, MATCH, MINB>;
+    v.k[IN_BUF][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_BUF, false, MATCH, MINB>;
+    v.k[IN_RAW][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_RAW, true, MATCH, MINB>;
+    v.k[IN_GATHER][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_GATHER, true, MATCH, MINB>;
+    v.k[IN_BUF][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_BUF, true, MATCH, MINB>;
     return v;
 }
 
+// key width, threads per CTA, keys per thread, match method, CTAs per SM
 const PassVariant kVariants[] = {
-    make_variant<uint32_t, 256, 16, 0>(),  // 0
-    make_variant<uint32_t, 256, 16, 1>(),  // 1
-    make_variant<uint64_t, 256, 12, 0>(),  // 2
-    make_variant<uint64_t, 256, 12, 1>(),  // 3
+    make_variant<uint32_t, 256, 16, 0, 3>(),  // 0
+    make_variant<uint32_t, 256, 16, 1, 3>(),  // 1
+    make_variant<uint64_t, 256, 12, 0, 3>(),  // 2
+    make_variant<uint64_t, 256, 12, 1, 3>(),  // 3
+    make_variant<uint32_t, 256, 16, 1, 2>(),  // 4
+    make_variant<uint64_t, 256, 12, 0, 2>(),  // 5
+    make_variant<uint32_t, 256, 12, 1, 4>(),  // 6
+    make_variant<uint64_t, 256, 8, 0, 4>(),   // 7
+    make_variant<uint64_t, 256, 16, 0, 2>(),  // 8
+    make_variant<uint32_t, 256, 24, 1, 2>(),  // 9
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 

@@ -280,14 +280,14 @@ __device__ __forceinline__ void emit_group(const SegArgs& a, uint32_t g, uint32_
 // fewer keep registers free when many value columns are aggregated.
 
 // Per-warp staging of completed groups (records) and new groups (keys),
-// column-major with one padding slot per 4 entries: a thread fills entries
+// column-major with one padding slot per 32 entries: a thread fills entries
 // ITEMS*t .. ITEMS*t+ITEMS-1 and the write-out reads consecutive entries
 // across lanes; the skew keeps both patterns (nearly) bank-conflict free.
 template <int NK, int NV, int ITEMS>
 struct WarpStage {
     static constexpr int ROWS = ITEMS * 32;
-    static constexpr int SLOTS = ROWS + 1 + (ROWS + 1) / 4 + 1;
-    static __device__ __forceinline__ int at(uint32_t i) { return (int)(i + (i >> 2)); }
+    static constexpr int SLOTS = ROWS + 1 + (ROWS + 1) / 32 + 1;
+    static __device__ __forceinline__ int at(uint32_t i) { return (int)(i + (i >> 5)); }
     uint64_t w[NV > 0 ? NV : 1][4][SLOTS];
     uint64_t key[NK][SLOTS];
     uint32_t cnt[SLOTS];
