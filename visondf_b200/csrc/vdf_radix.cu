@@ -130,7 +130,8 @@ struct OnesweepCfg {
 };
 
 // MATCH selects how a warp finds the lanes holding the same digit:
-// 0 = one ballot per digit bit (ALU/vote pipes), 1 = match.any (XU pipe).
+// 0 = one ballot per digit bit (ALU/vote pipes), 1 = match.any (XU pipe),
+// 2 = alternate the two by item, so both pipes work at once.
 // MINB: CTAs per SM the register allocation is sized for.
 template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL, int MATCH, int MINB>
 __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
@@ -193,10 +194,13 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
             for (int b = tid; b < RADIX; b += THREADS) a.status_next[(size_t)r * RADIX + b] = 0;
 
     // ---- warp-local ranks and per-warp digit counts --------------------------
-    // Lanes holding the same digit are found with one ballot per digit bit
-    // (plus one for validity), or with match.any; the lowest such lane
-    // updates the warp's counter.
+    // First the lanes holding the same digit are found for every item (one
+    // ballot per digit bit plus one for validity, or match.any); these are
+    // independent and overlap.  Then the warp's per-digit counters advance
+    // item by item (the lowest lane of each peer group updates it), which is
+    // the only serial part.
     uint32_t rank[ITEMS];
+    uint32_t peers[ITEMS];
     uint32_t* my_cnt = wcnt + warp * RADIX;
     const uint32_t lt = lanemask_lt();
 #pragma unroll
@@ -204,27 +208,33 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
         const uint32_t pos = wpos + j * 32 + lane;
         const bool ok = pos < valid;
         const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
-        uint32_t peers;
-        if (MATCH == 1) {
-            peers = __match_any_sync(0xffffffffu, ok ? d : (uint32_t)RADIX);
+        if (MATCH == 1 || (MATCH == 2 && (j & 1) == 0)) {
+            peers[j] = __match_any_sync(0xffffffffu, ok ? d : (uint32_t)RADIX);
         } else {
-            peers = __ballot_sync(0xffffffffu, ok);
-            if (!ok) peers = ~peers;
+            uint32_t pm = __ballot_sync(0xffffffffu, ok);
+            if (!ok) pm = ~pm;
 #pragma unroll
             for (int b = 0; b < BITS; ++b) {
                 const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
-                peers &= ((d >> b) & 1u) ? bal : ~bal;
+                pm &= ((d >> b) & 1u) ? bal : ~bal;
             }
+            peers[j] = pm;
         }
-        const int leader = __ffs(peers) - 1;
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = wpos + j * 32 + lane;
+        const bool ok = pos < valid;
+        const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
+        const int leader = __ffs(peers[j]) - 1;
         uint32_t base = 0;
         if (lane == leader && ok) {
             base = my_cnt[d];
-            my_cnt[d] = base + __popc(peers);
+            my_cnt[d] = base + __popc(peers[j]);
         }
-        base = __shfl_sync(0xffffffffu, base, leader);
-        rank[j] = ok ? base + __popc(peers & lt) : pos;
         __syncwarp();
+        base = __shfl_sync(0xffffffffu, base, leader);
+        rank[j] = ok ? base + __popc(peers[j] & lt) : pos;
     }
     __syncthreads();
 
@@ -292,6 +302,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     }
 
     // ---- decoupled look-back per bin ---------------------------------------
+    // Each bin's thread reads the status words of LB predecessors at once (one
+    // round trip per window), adds counts from the nearest one backwards and
+    // stops at the first inclusive prefix.
+    constexpr int LB = 8;
 #pragma unroll
     for (int k = 0; k < BPT; ++k) {
         const int b = tid * BPT + k;
@@ -300,16 +314,30 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
         if (tile > 0) {
             int64_t p = (int64_t)tile - 1;
             uint32_t spins = 0;
-            while (true) {
-                uint32_t s = ld_relaxed_u32(a.status + (size_t)p * RADIX + b);
-                if ((s & ~ST_CNT) == 0) {
-                    if (++spins > kSpinLimit) { atomicOr(a.err, ERR_LOOKBACK_TIMEOUT); break; }
-                    backoff(spins);
-                    continue;
+            bool done = false;
+            while (!done) {
+                uint32_t sw[LB];
+#pragma unroll
+                for (int w = 0; w < LB; ++w)
+                    sw[w] = (p - w >= 0) ? ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b) : ST_INC;
+#pragma unroll
+                for (int w = 0; w < LB; ++w) {
+                    if (done) break;
+                    uint32_t st = sw[w];
+                    while ((st & ~ST_CNT) == 0) {  // not yet published: wait for this one
+                        if (++spins > kSpinLimit) {
+                            atomicOr(a.err, ERR_LOOKBACK_TIMEOUT);
+                            st = ST_INC;
+                            break;
+                        }
+                        backoff(spins);
+                        st = ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b);
+                    }
+                    excl += st & ST_CNT;
+                    if (st & ST_INC) done = true;
                 }
-                excl += s & ST_CNT;
-                if ((s & ST_INC) || p == 0) break;
-                --p;
+                p -= LB;
+                if (p < 0) done = true;
             }
             st_relaxed_u32(a.status + (size_t)tile * RADIX + b, ST_INC | (excl + tot[k]));
         }
@@ -390,6 +418,10 @@ const PassVariant kVariants[] = {
     make_variant<uint64_t, 256, 8, 0, 4>(),   // 7
     make_variant<uint64_t, 256, 16, 0, 2>(),  // 8
     make_variant<uint32_t, 256, 24, 1, 2>(),  // 9
+    make_variant<uint32_t, 256, 12, 2, 4>(),  // 10
+    make_variant<uint64_t, 256, 12, 2, 3>(),  // 11
+    make_variant<uint64_t, 256, 8, 2, 4>(),   // 12
+    make_variant<uint32_t, 256, 16, 2, 3>(),  // 13
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
