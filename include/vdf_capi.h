@@ -173,6 +173,28 @@ vdf_status vdf_sort_argsort_ws(vdf_ctx* ctx, uint64_t n, const vdf_col* keys, in
                                uint32_t* perm_out, void* const* sorted_keys_out, void* workspace,
                                size_t workspace_bytes, void* stream);
 
+/* ---- sort without any allocation ------------------------------------------ */
+/* Largest row count vdf_sort_argsort_noalloc accepts. */
+#define VDF_NOALLOC_MAX_ROWS (1u << 20)
+/* The same stable argsort as vdf_sort_argsort for callers that cannot
+ * allocate device memory when they sort (inside another allocator's
+ * callback, under a host framework that forbids run-time allocations, or on
+ * a latency-critical path that must not trigger the synchronisation
+ * cudaMalloc/cudaFree can imply).  It takes no context and calls no
+ * cudaMalloc, cudaFree or other allocating routine: its scratch is a fixed
+ * 28 MiB device array inside the library, held on every GPU where the
+ * library's module holding it is loaded (the first call on that GPU) until the
+ * process exits.  The first call on a device looks up the array's device
+ * address and prepares the kernels, so make it before any stream capture.
+ * n above VDF_NOALLOC_MAX_ROWS returns VDF_ERR_UNSUPPORTED.  All calls on a
+ * device share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and corrupt each other's results; serialise them.
+ * The call is asynchronous on `stream` and does not report device-side wait
+ * timeouts.  No counterpart in the reference: the reference's radix sort
+ * always allocates its buffers (radix_sort_uint64.inl:23-24). */
+vdf_status vdf_sort_argsort_noalloc(uint64_t n, const vdf_col* keys, int nkeys, int order, uint32_t* perm_out,
+                                    void* const* sorted_keys_out, void* stream);
+
 /* ---- gather ---------------------------------------------------------------- */
 /* out[c][r] = in[c].data[perm[r]] for ncols (<= 8) columns in one launch.
  * Replaces permute_block_mt (V/inlines/transform/sort_by/permute_block_mt.inl:3-47),

@@ -92,6 +92,7 @@ def _load() -> C.CDLL:
         "vdf_groupby_workspace_bytes": (sz, [u64, i32]),
         "vdf_sort_argsort": (st, [vp, u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp]),
         "vdf_sort_argsort_ws": (st, [vp, u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp, sz, vp]),
+        "vdf_sort_argsort_noalloc": (st, [u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp]),
         "vdf_gather": (st, [vp, u64, vp, C.POINTER(vdf_col), i32, C.POINTER(vp), vp]),
         "vdf_groupby_sorted": (st, [vp, u64, C.POINTER(vdf_col), i32, C.POINTER(vdf_col), i32, C.POINTER(vp), vp,
                                     C.POINTER(vdf_agg_out), vp, vp, vp, C.POINTER(C.c_uint64), vp]),
