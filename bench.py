@@ -280,39 +280,39 @@ def our_arm(args, rank: int, world: int, local_rank: int):
     step_frac = canonical / (ms / 1e3) / 1e9 / peak
 
     # ---- end to end from host buffers -------------------------------------------
+    # One vdf_sort_groupby_host call per step: the five input columns are copied
+    # from pinned host memory to the device, the path runs, and the permutation
+    # plus the group table come back to pinned host memory.
     e2e = None
     if not args.no_e2e:
+        import ctypes as C
+        from visondf_b200 import _lib
         h2d = sum(host[k].numel() * host[k].element_size() for k in names)
-        g = n_groups
-        res_host = {
-            "perm": torch.empty(n, dtype=torch.int32).pin_memory(),
-            "k1": torch.empty(n, dtype=torch.int64).pin_memory(),
-            "k2": torch.empty(n, dtype=torch.int32).pin_memory(),
-            "count": torch.empty(n, dtype=torch.int64).pin_memory(),
-        }
-        agg_host = []
-        for a in outs["aggs"]:
-            agg_host.append({fld: torch.empty(getattr(a, fld).numel(), dtype=getattr(a, fld).dtype).pin_memory()
-                             for fld in ("sum", "sum_hi", "min", "max", "mean") if getattr(a, fld) is not None})
-        outs_e = ctx.alloc_sort_groupby_outputs(keys, payload, agg_cols)
-        packed_e = ctx.pack_sort_groupby(keys, payload, agg_cols, vdf.ORDER_ASC, True, outs_e, host_count=True)
+        pin = lambda dtype: torch.empty(n, dtype=dtype).pin_memory()  # noqa: E731
+        hp = {"perm": pin(torch.int32), "gk1": pin(torch.int64), "gk2": pin(torch.int32), "cnt": pin(torch.int64),
+              "f_sum": pin(torch.float64), "f_min": pin(torch.float64), "f_max": pin(torch.float64),
+              "f_mean": pin(torch.float64), "i_sum": pin(torch.int64), "i_hi": pin(torch.int64),
+              "i_min": pin(torch.int32), "i_max": pin(torch.int32), "i_mean": pin(torch.float64)}
+        hk = (_lib.vdf_col * 2)(_lib.vdf_col(host["key1"].data_ptr(), vdf.I64), _lib.vdf_col(host["key2"].data_ptr(), vdf.I32))
+        hpay = (_lib.vdf_col * 3)(_lib.vdf_col(host["f64"].data_ptr(), vdf.F64), _lib.vdf_col(host["i32"].data_ptr(), vdf.I32),
+                                  _lib.vdf_col(host["rowid"].data_ptr(), vdf.U64))
+        hagg = (_lib.vdf_agg_out * 2)(
+            _lib.vdf_agg_out(hp["f_sum"].data_ptr(), None, hp["f_min"].data_ptr(), hp["f_max"].data_ptr(), hp["f_mean"].data_ptr()),
+            _lib.vdf_agg_out(hp["i_sum"].data_ptr(), hp["i_hi"].data_ptr(), hp["i_min"].data_ptr(), hp["i_max"].data_ptr(),
+                             hp["i_mean"].data_ptr()))
+        hgk = (C.c_void_p * 2)(hp["gk1"].data_ptr(), hp["gk2"].data_ptr())
+        hac = (C.c_int32 * 2)(0, 1)
+        ng = C.c_uint64(0)
+        ha = _lib.vdf_sort_groupby_args()
+        ha.n, ha.keys, ha.nkeys, ha.order = n, hk, 2, vdf.ORDER_ASC
+        ha.payload, ha.npayload = hpay, 3
+        ha.perm_out = hp["perm"].data_ptr()
+        ha.groupby, ha.agg_cols, ha.nagg, ha.aggs = 1, hac, 2, hagg
+        ha.group_keys_out, ha.group_count_out = hgk, hp["cnt"].data_ptr()
+        ha.n_groups_host = C.pointer(ng)
 
         def e2e_step():
-            for k in names:
-                d[k].copy_(host[k], non_blocking=True)
-            ctx.sort_groupby_packed(packed_e, stream)
-            gg = int(outs_e["_ng"].value)
-            res_host["perm"].copy_(outs_e["perm"], non_blocking=True)
-            res_host["k1"][:gg].copy_(outs_e["gkeys"][0][:gg], non_blocking=True)
-            res_host["k2"][:gg].copy_(outs_e["gkeys"][1][:gg], non_blocking=True)
-            res_host["count"][:gg].copy_(outs_e["count"][:gg], non_blocking=True)
-            nbytes = 4 * n + gg * (8 + 4 + 8)
-            for a, ah in zip(outs_e["aggs"], agg_host):
-                for fld, t in ah.items():
-                    src = getattr(a, fld)
-                    t[:gg].copy_(src[:gg], non_blocking=True)
-                    nbytes += gg * src.element_size()
-            return nbytes
+            ctx._check(vdf.lib.vdf_sort_groupby_host(ctx.handle, C.byref(ha), stream.cuda_stream), "vdf_sort_groupby_host")
 
         for _ in range(max(1, args.warmup)):
             e2e_step()
@@ -320,19 +320,20 @@ def our_arm(args, rank: int, world: int, local_rank: int):
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        d2h = 0
         for _ in range(args.steps):
-            d2h = e2e_step()
+            e2e_step()
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
         ems = e0.elapsed_time(e1) / args.steps
+        g = int(ng.value)
+        d2h = 4 * n + g * (8 + 4 + 8 + 4 * 8 + (8 + 8 + 4 + 4 + 8))
         if world > 1:
             t = torch.tensor([ems], device=dev, dtype=torch.float64)
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             ems = float(t.item())
         e2e = {"value": n * world / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": ems}
+               "ms_per_step": ems, "call": "vdf_sort_groupby_host (pinned host buffers)"}
 
     # ---- CPU baseline (rank 0, one GPU only) -------------------------------------
     cpu = None

@@ -246,6 +246,11 @@ typedef struct vdf_sort_groupby_args {
     uint32_t* row_group_out;
     uint64_t* n_groups_dev;
     uint64_t* n_groups_host;       /* non-NULL: the call synchronises `stream`       */
+    /* optional permutation of [0, n) through which the rows are seen (a row
+     * view): the sort orders rows[perm_in[i]] and perm_out is composed with it,
+     * like the in/out idx of the reference's radix_sort_uint64
+     * (V/inlines/radix_sorts/radix_sort_uint64.inl:5-7).  NULL = identity. */
+    const uint32_t* perm_in;
 } vdf_sort_groupby_args;
 
 /* One call for the whole path: sort by the keys, gather every payload column
@@ -257,6 +262,43 @@ typedef struct vdf_sort_groupby_args {
  * transform_group_by_mt.hpp:12-114), in the segment layout of the "hard"
  * variant (hard/transform_group_by_onecol_hard_mt.hpp:11-372). */
 vdf_status vdf_sort_groupby(vdf_ctx* ctx, const vdf_sort_groupby_args* args, void* stream);
+
+/* The same call on HOST memory: every column, output and n_groups_host
+ * pointer in `args` is a host pointer (n_groups_dev is ignored).  The inputs
+ * are copied to the device, the path runs there, the outputs come back (the
+ * sorted frame as n rows, the group table as n_groups rows) and the call
+ * returns after synchronising `stream`.  Page-locked host buffers make the
+ * copies asynchronous and fast; ordinary ones work too.  This is the entry
+ * point behind the header-only dataframe layer (include/vison_b200/vison.hpp),
+ * replacing the same reference calls as vdf_sort_groupby on the reference's
+ * own host-resident columns (V/vison.hpp:207-212). */
+vdf_status vdf_sort_groupby_host(vdf_ctx* ctx, const vdf_sort_groupby_args* args, void* stream);
+
+/* Host-memory gather: out[c][r] = in[c].data[perm[r]] with perm, in and out
+ * in host memory (synchronises `stream`).  Replaces materialize_mt
+ * (V/materialize/materialize_mt.hpp:6-55) on host-resident columns. */
+vdf_status vdf_gather_host(vdf_ctx* ctx, uint64_t n, const uint32_t* perm, const vdf_col* in, int ncols,
+                           void* const* out, void* stream);
+
+/* Aggregate functions of the transform-style group-by. */
+typedef enum vdf_agg_fn {
+    VDF_AGG_COUNT = 0, /* int64 rows in the group (GroupFunction::Occurence)        */
+    VDF_AGG_SUM = 1,   /* double for float values, int64 low word of the exact sum */
+    VDF_AGG_MEAN = 2,  /* double sum / count                                        */
+    VDF_AGG_MIN = 3,   /* value dtype (extension: the reference has no min)         */
+    VDF_AGG_MAX = 4    /* value dtype (extension: the reference has no max)         */
+} vdf_agg_fn;
+
+/* The reference's transform group-by on host memory: groups the n rows by the
+ * key columns, aggregates `val` with `function`, and writes to `out` (host, n
+ * elements) every row's group value in the frame's row order, as
+ * transform_group_by does (V/transform/transform_group_by/
+ * transform_group_by.hpp:3-113, CreateValueCol::apply create_value_col.inl:
+ * 36-61).  perm_in (host, optional) is the frame's row view.  The group
+ * count goes to *n_groups_host.  Synchronises `stream`. */
+vdf_status vdf_transform_groupby_host(vdf_ctx* ctx, uint64_t n, const vdf_col* keys, int nkeys, vdf_col val,
+                                      int32_t function, const uint32_t* perm_in, void* out, uint64_t* n_groups_host,
+                                      void* stream);
 
 /* ---- transform output --------------------------------------------------------- */
 /* out[perm ? perm[r] : r] = group_vals[row_group[r]] (width 4 or 8 bytes,

@@ -1,0 +1,417 @@
+// vison_b200/vison.hpp -- header-only C++ dataframe layer over libvdf_b200.
+//
+// It keeps the reference's sort and group-by entry points (VisonDF's
+// vison::Dataframe, include/vison/vison.hpp:187-616) with their template
+// signatures, so code written against them compiles unchanged, while the work
+// runs on the GPU through the C-ABI in vdf_capi.h:
+//
+//   sort_by / sort_by_mt          transform/sort_by/sort_by.hpp:3-19, sort_by_mt.hpp:3-180
+//   sort_by_external[_mt]         transform/sort_by/sort_by_external_mt.hpp:3-130
+//   materialize / materialize_mt  materialize/materialize_mt.hpp:3-55
+//   transform_group_by[_mt]       transform/transform_group_by/transform_group_by.hpp:3-113,
+//                                 transform_group_by_mt.hpp:3-114
+//
+// Storage follows the reference: column-major type blocks (here int_v, uint_v,
+// dbl_v plus 64-bit integer blocks lint_v / luint_v, which the reference lacks:
+// it has one signed width per frame, so an int32 key and an int64 value cannot
+// share a frame), a per-column type char, and a lazy row view (row_view_idx +
+// in_view) that Soft sorts set and materialize() applies.  String, char and
+// bool columns are not part of this path.
+//
+// Template parameters that tune the reference's CPU code (CORES, Simd,
+// SortType, comparator factories, SimdHash, MapCol, NPerGroup) are accepted
+// and ignored: the GPU path has one implementation.  Errors follow the
+// reference's convention (a message on std::cerr and an early return,
+// sort_by_mt.hpp:16-18,40-41,68-69).
+//
+// Semantics defined by this layer (documented deviations):
+//   * descending sorts reproduce the reference CODE (ascending + std::reverse,
+//     sort_integers.inl:225-227: ties in reverse row order); define
+//     VISON_B200_STABLE_DESCENDING for the stable order INTERNALS.doc shows;
+//   * a Soft sort while in view sorts the rows as currently viewed (the
+//     reference re-sorts the raw column, sort_by_mt.hpp:99,111,169-176);
+//   * GroupFunction::Mean is sum / group count (the reference divides by the
+//     frame's row count, create_value_col.inl:46); Min and Max are added;
+//     Gather (a user lambda over the group's values) is not supported on the
+//     GPU path and reports an error.
+#pragma once
+
+#include <cstdint>
+#include <iostream>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "../vdf_capi.h"
+
+namespace vison_b200 {
+
+enum class SortType { Standard, Radix };  // supported_sorting_methods.inl:1-4 (both: the stable GPU radix sort)
+
+// supported_group_methods.inl:1-7, plus Min and Max
+enum class GroupFunction { Occurence, Sum, Mean, Gather, None, Min, Max };
+
+struct DefaultTypes {  // types/inference_type.hpp:3-8 (CharT omitted: no char columns here)
+    using IntT = int;
+    using UIntT = unsigned int;
+    using FloatT = double;
+};
+
+struct DefaultComparatorFactory {};  // types/comparator.inl:1-11; accepted, unused
+
+inline void default_groupfn_impl() {}
+
+// One library context per device, created on first use (the reference's
+// init_openmp, vison.hpp:57-74, is likewise process-wide state).
+inline vdf_ctx* context(int device = 0) {
+    static std::mutex mu;
+    static std::map<int, std::unique_ptr<vdf_ctx, vdf_status (*)(vdf_ctx*)>> ctxs;
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = ctxs.find(device);
+    if (it != ctxs.end()) return it->second.get();
+    vdf_ctx* c = nullptr;
+    if (vdf_ctx_create(device, &c) != VDF_OK) return nullptr;
+    ctxs.emplace(device, std::unique_ptr<vdf_ctx, vdf_status (*)(vdf_ctx*)>(c, vdf_ctx_destroy));
+    return c;
+}
+
+namespace detail {
+template <typename T> constexpr int32_t dtype_of() {
+    if constexpr (std::is_same_v<T, int32_t>) return VDF_I32;
+    else if constexpr (std::is_same_v<T, int64_t> || (std::is_same_v<T, long> && sizeof(long) == 8)) return VDF_I64;
+    else if constexpr (std::is_same_v<T, uint32_t>) return VDF_U32;
+    else if constexpr (std::is_same_v<T, uint64_t> || (std::is_same_v<T, unsigned long> && sizeof(long) == 8))
+        return VDF_U64;
+    else if constexpr (std::is_same_v<T, double>) return VDF_F64;
+    else if constexpr (std::is_same_v<T, float>) return VDF_F32;
+    else return -1;
+}
+inline bool report(vdf_status s, const char* what) {
+    if (s == VDF_OK) return true;
+    vdf_ctx* c = context();
+    std::cerr << what << ": " << vdf_status_string(s);
+    if (c && *vdf_ctx_last_error(c)) std::cerr << " (" << vdf_ctx_last_error(c) << ")";
+    std::cerr << "\n";
+    return false;
+}
+template <bool ASC>
+constexpr int32_t order() {
+#ifdef VISON_B200_STABLE_DESCENDING
+    return ASC ? VDF_ORDER_ASC : VDF_ORDER_DESC_STABLE;
+#else
+    return ASC ? VDF_ORDER_ASC : VDF_ORDER_DESC_REVERSE;
+#endif
+}
+}  // namespace detail
+
+template <typename Types = DefaultTypes>
+class Dataframe {
+  public:
+    using IntT = typename Types::IntT;
+    using UIntT = typename Types::UIntT;
+    using FloatT = typename Types::FloatT;
+    using LIntT = int64_t;
+    using LUIntT = uint64_t;
+
+    unsigned int nrow = 0;
+    unsigned int ncol = 0;
+    bool in_view = false;
+    std::vector<size_t> row_view_idx;
+
+    std::vector<std::vector<IntT>> int_v;      // 'i'
+    std::vector<std::vector<UIntT>> uint_v;    // 'u'
+    std::vector<std::vector<FloatT>> dbl_v;    // 'd'
+    std::vector<std::vector<LIntT>> lint_v;    // 'l' (extension)
+    std::vector<std::vector<LUIntT>> luint_v;  // 'L' (extension)
+    std::vector<char> type_refv;               // type char of each column
+    std::vector<unsigned int> slot_v;          // index of each column inside its type block
+    std::vector<std::string> name_v;
+
+    // ---- building and reading ------------------------------------------------
+    template <typename T>
+    void add_col(std::vector<T> v, std::string name = "") {
+        if (ncol == 0) nrow = (unsigned int)v.size();
+        if (v.size() != nrow) {
+            std::cerr << "add_col: column has " << v.size() << " rows, frame has " << nrow << "\n";
+            return;
+        }
+        if (in_view) materialize();
+        char t;
+        unsigned int slot;
+        if constexpr (std::is_same_v<T, IntT>) { t = 'i'; slot = (unsigned)int_v.size(); int_v.push_back(std::move(v)); }
+        else if constexpr (std::is_same_v<T, UIntT>) { t = 'u'; slot = (unsigned)uint_v.size(); uint_v.push_back(std::move(v)); }
+        else if constexpr (std::is_same_v<T, FloatT>) { t = 'd'; slot = (unsigned)dbl_v.size(); dbl_v.push_back(std::move(v)); }
+        else if constexpr (std::is_same_v<T, LIntT>) { t = 'l'; slot = (unsigned)lint_v.size(); lint_v.push_back(std::move(v)); }
+        else if constexpr (std::is_same_v<T, LUIntT>) { t = 'L'; slot = (unsigned)luint_v.size(); luint_v.push_back(std::move(v)); }
+        else { static_assert(!sizeof(T), "unsupported column type"); }
+        type_refv.push_back(t);
+        slot_v.push_back(slot);
+        name_v.push_back(name.empty() ? "col" + std::to_string(ncol + 1) : std::move(name));
+        ++ncol;
+    }
+
+    // Column n as currently viewed (through row_view_idx when in view).
+    template <typename T>
+    std::vector<T> get_col(unsigned int n) const {
+        const std::vector<T>* src = col_ptr<T>(n);
+        if (!src) return {};
+        if (!in_view) return *src;
+        std::vector<T> out(nrow);
+        for (unsigned int r = 0; r < nrow; ++r) out[r] = (*src)[row_view_idx[r]];
+        return out;
+    }
+
+    // ---- sort ------------------------------------------------------------------
+    template <bool ASC = 1, typename T = void, bool Simd = true, bool Soft = true, SortType S = SortType::Radix,
+              typename Cmp = DefaultComparatorFactory>
+    void sort_by(unsigned int& n) {
+        sort_by_mt<ASC, 1, T, Simd, Soft, S, Cmp>(n);
+    }
+
+    template <bool ASC = 1, unsigned int CORES = 4, typename T = void, bool Simd = true, bool Soft = true,
+              SortType S = SortType::Radix, typename Cmp = DefaultComparatorFactory>
+    void sort_by_mt(unsigned int& n) {
+        if (!Soft && in_view) {
+            std::cerr << "Can't use this operation while in `view` mode, consider applying `.materialize()`\n";
+            return;
+        }
+        if (n >= ncol) {
+            std::cerr << "Column not found\n";
+            return;
+        }
+        vdf_col key = col_desc(n);
+        sort_rows<ASC, Soft>(&key, 1);
+    }
+
+    // Several key columns, most significant first (no reference counterpart:
+    // the reference composes single-key sorts, see sort_by_mt.hpp:169-176).
+    template <bool ASC = 1, bool Soft = true>
+    void sort_by_cols(const std::vector<unsigned int>& cols) {
+        if (cols.empty() || cols.size() > 4) {
+            std::cerr << "sort_by_cols: 1 to 4 key columns\n";
+            return;
+        }
+        std::vector<vdf_col> keys;
+        for (unsigned int c : cols) {
+            if (c >= ncol) {
+                std::cerr << "Column not found\n";
+                return;
+            }
+            keys.push_back(col_desc(c));
+        }
+        sort_rows<ASC, Soft>(keys.data(), (int)keys.size());
+    }
+
+    template <typename T, bool ASC = true, unsigned int CORES = 4, bool Simd = true, bool Soft = true,
+              SortType S = SortType::Radix, bool BoolAsU8 = true, bool IsBoolCompressed = false>
+    void sort_by_external_mt(const std::vector<T>& nvec) {
+        if (nvec.size() != nrow) {
+            std::cerr << "sort vec must be same size as dataframe nrow\n";
+            return;
+        }
+        if (!Soft && in_view) {
+            std::cerr << "Can't use this operation while in `view` mode, consider applying `.materialize()`\n";
+            return;
+        }
+        static_assert(detail::dtype_of<T>() >= 0, "sort_by_external: unsupported key type on the GPU path");
+        // the external vector is indexed by storage row, like a frame column
+        vdf_col key{nvec.data(), detail::dtype_of<T>()};
+        sort_rows<ASC, Soft>(&key, 1);
+    }
+
+    template <typename T, bool ASC = true, bool Simd = true, bool Soft = true, SortType S = SortType::Radix,
+              bool BoolAsU8 = true, bool IsBoolCompressed = false>
+    void sort_by_external(const std::vector<T>& nvec) {
+        sort_by_external_mt<T, ASC, 1, Simd, Soft, S, BoolAsU8, IsBoolCompressed>(nvec);
+    }
+
+    // ---- materialize -------------------------------------------------------------
+    template <unsigned int CORES = 4, bool IsDense = true, bool MemClean = false>
+    void materialize_mt() {
+        if (!in_view) return;
+        std::vector<uint32_t> perm(row_view_idx.begin(), row_view_idx.end());
+        for (unsigned int c = 0; c < ncol; ++c) permute_col(c, perm);
+        in_view = false;
+        if (MemClean) std::vector<size_t>().swap(row_view_idx);
+        else row_view_idx.clear();
+    }
+
+    template <bool IsDense = true, bool MemClean = false>
+    void materialize() {
+        materialize_mt<1, IsDense, MemClean>();
+    }
+
+    // ---- group-by (transform semantics: one new column, a value per row) ------
+    template <typename TContainer = void, typename TColVal = void, GroupFunction Function = GroupFunction::Occurence,
+              bool SimdHash = true, bool MapCol = false, unsigned int NPerGroup = 4,
+              typename F = decltype(&default_groupfn_impl)>
+    void transform_group_by(const std::vector<unsigned int>& x, const unsigned int n_col,
+                            const std::string colname = "n", const F f = &default_groupfn_impl) {
+        transform_group_by_mt<TContainer, TColVal, 1, Function, SimdHash, MapCol, NPerGroup, F>(x, n_col, colname, f);
+    }
+
+    template <typename TContainer = void, typename TColVal = void, unsigned int CORES = 4,
+              GroupFunction Function = GroupFunction::Occurence, bool SimdHash = true, bool MapCol = false,
+              unsigned int NPerGroup = 4, typename F = decltype(&default_groupfn_impl)>
+    void transform_group_by_mt(const std::vector<unsigned int>& x, const unsigned int n_col,
+                               const std::string colname = "n", const F f = &default_groupfn_impl) {
+        (void)f;
+        if constexpr (Function == GroupFunction::Gather || Function == GroupFunction::None) {
+            std::cerr << "transform_group_by: GroupFunction::Gather/None is not supported on the GPU path\n";
+            return;
+        } else {
+            if (x.empty() || x.size() > 4 || n_col >= ncol) {
+                std::cerr << "transform_group_by: bad key or value column\n";
+                return;
+            }
+            std::vector<vdf_col> keys;
+            for (unsigned int c : x) {
+                if (c >= ncol) {
+                    std::cerr << "Column not found\n";
+                    return;
+                }
+                keys.push_back(col_desc(c));
+            }
+            const vdf_col val = col_desc(n_col);
+            int32_t fn = VDF_AGG_COUNT;
+            if (Function == GroupFunction::Sum) fn = VDF_AGG_SUM;
+            else if (Function == GroupFunction::Mean) fn = VDF_AGG_MEAN;
+            else if (Function == GroupFunction::Min) fn = VDF_AGG_MIN;
+            else if (Function == GroupFunction::Max) fn = VDF_AGG_MAX;
+            std::vector<uint32_t> view;
+            if (in_view) view.assign(row_view_idx.begin(), row_view_idx.end());
+            const char vt = type_refv[n_col];
+            const bool vfloat = (vt == 'd');
+            uint64_t groups = 0;
+            auto run = [&](void* out) {
+                return detail::report(vdf_transform_groupby_host(context(), nrow, keys.data(), (int)keys.size(), val, fn,
+                                                                 in_view ? view.data() : nullptr, out, &groups,
+                                                                 nullptr),
+                                      "transform_group_by");
+            };
+            // the new column is in storage order; when the frame is in view the
+            // view applies to it like to every other column
+            if (fn == VDF_AGG_COUNT) {
+                std::vector<int64_t> out(nrow);
+                if (!run(out.data())) return;
+                add_raw(std::vector<UIntT>(out.begin(), out.end()), colname);
+            } else if (fn == VDF_AGG_MEAN || (fn == VDF_AGG_SUM && vfloat)) {
+                std::vector<double> out(nrow);
+                if (!run(out.data())) return;
+                add_raw(std::vector<FloatT>(out.begin(), out.end()), colname);
+            } else if (fn == VDF_AGG_SUM) {
+                std::vector<int64_t> out(nrow);  // low 64 bits of the exact sum
+                if (!run(out.data())) return;
+                add_like(vt, out, colname);
+            } else {
+                dispatch_minmax(vt, run, colname);
+            }
+        }
+    }
+
+  private:
+    template <typename T>
+    const std::vector<T>* col_ptr(unsigned int n) const {
+        if (n >= ncol) return nullptr;
+        const unsigned s = slot_v[n];
+        switch (type_refv[n]) {
+        case 'i': if constexpr (std::is_same_v<T, IntT>) return &int_v[s]; break;
+        case 'u': if constexpr (std::is_same_v<T, UIntT>) return &uint_v[s]; break;
+        case 'd': if constexpr (std::is_same_v<T, FloatT>) return &dbl_v[s]; break;
+        case 'l': if constexpr (std::is_same_v<T, LIntT>) return &lint_v[s]; break;
+        case 'L': if constexpr (std::is_same_v<T, LUIntT>) return &luint_v[s]; break;
+        }
+        return nullptr;
+    }
+
+    vdf_col col_desc(unsigned int n) const {
+        const unsigned s = slot_v[n];
+        switch (type_refv[n]) {
+        case 'i': return vdf_col{int_v[s].data(), detail::dtype_of<IntT>()};
+        case 'u': return vdf_col{uint_v[s].data(), detail::dtype_of<UIntT>()};
+        case 'd': return vdf_col{dbl_v[s].data(), detail::dtype_of<FloatT>()};
+        case 'l': return vdf_col{lint_v[s].data(), VDF_I64};
+        default: return vdf_col{luint_v[s].data(), VDF_U64};
+        }
+    }
+
+    template <bool ASC, bool Soft>
+    void sort_rows(const vdf_col* keys, int nkeys) {
+        std::vector<uint32_t> perm(nrow);
+        std::vector<uint32_t> view;
+        if (in_view) view.assign(row_view_idx.begin(), row_view_idx.end());
+        vdf_sort_groupby_args a{};
+        a.n = nrow;
+        a.keys = keys;
+        a.nkeys = nkeys;
+        a.order = detail::order<ASC>();
+        a.perm_out = perm.data();
+        a.perm_in = in_view ? view.data() : nullptr;
+        if (!detail::report(vdf_sort_groupby_host(context(), &a, nullptr), "sort_by")) return;
+        if (Soft) {
+            row_view_idx.assign(perm.begin(), perm.end());
+            in_view = true;
+        } else {
+            for (unsigned int c = 0; c < ncol; ++c) permute_col(c, perm);
+        }
+    }
+
+    void permute_col(unsigned int c, const std::vector<uint32_t>& perm) {
+        vdf_col in = col_desc(c);
+        const unsigned s = slot_v[c];
+        auto go = [&](auto& vec) {
+            using V = typename std::decay_t<decltype(vec)>::value_type;
+            std::vector<V> out(nrow);
+            void* o = out.data();
+            if (detail::report(vdf_gather_host(context(), nrow, perm.data(), &in, 1, &o, nullptr), "materialize"))
+                vec.swap(out);
+        };
+        switch (type_refv[c]) {
+        case 'i': go(int_v[s]); break;
+        case 'u': go(uint_v[s]); break;
+        case 'd': go(dbl_v[s]); break;
+        case 'l': go(lint_v[s]); break;
+        default: go(luint_v[s]); break;
+        }
+    }
+
+    // Appends a column in storage order (transform outputs are computed per
+    // storage row), keeping the current view.
+    template <typename T>
+    void add_raw(std::vector<T> v, const std::string& name) {
+        const bool keep = in_view;
+        in_view = false;
+        add_col(std::move(v), name);
+        in_view = keep;
+    }
+
+    void add_like(char vt, const std::vector<int64_t>& v, const std::string& name) {
+        switch (vt) {
+        case 'i': add_raw(std::vector<IntT>(v.begin(), v.end()), name); break;
+        case 'u': add_raw(std::vector<UIntT>(v.begin(), v.end()), name); break;
+        case 'l': add_raw(std::vector<LIntT>(v.begin(), v.end()), name); break;
+        default: add_raw(std::vector<LUIntT>(v.begin(), v.end()), name); break;
+        }
+    }
+
+    template <typename Run>
+    void dispatch_minmax(char vt, Run& run, const std::string& name) {
+        switch (vt) {
+        case 'i': { std::vector<IntT> o(nrow); if (run(o.data())) add_raw(std::move(o), name); break; }
+        case 'u': { std::vector<UIntT> o(nrow); if (run(o.data())) add_raw(std::move(o), name); break; }
+        case 'd': { std::vector<FloatT> o(nrow); if (run(o.data())) add_raw(std::move(o), name); break; }
+        case 'l': { std::vector<LIntT> o(nrow); if (run(o.data())) add_raw(std::move(o), name); break; }
+        default: { std::vector<LUIntT> o(nrow); if (run(o.data())) add_raw(std::move(o), name); break; }
+        }
+    }
+};
+
+}  // namespace vison_b200
+
+#ifdef VISON_B200_AS_VISON
+namespace vison = vison_b200;  // drop-in: code written against vison::Dataframe compiles unchanged
+#endif

@@ -1,0 +1,162 @@
+// Exercises the header-only dataframe layer (include/vison_b200/vison.hpp) on
+// the GPU: the reference documentation's sort_by example, Soft/Hard sorts,
+// sorts while in view, materialize, sort_by_external, multi-key sorts and
+// the transform group-by, checked against plain CPU computations here.
+#include <algorithm>
+#include <cstdio>
+#include <map>
+#include <numeric>
+#include <random>
+#include <tuple>
+#include <vector>
+
+#include "vison_b200/vison.hpp"
+
+using DF = vison_b200::Dataframe<>;
+using vison_b200::GroupFunction;
+
+static int failures = 0;
+#define CHECK(cond)                                                                  \
+    do {                                                                             \
+        if (!(cond)) {                                                               \
+            std::fprintf(stderr, "CHECK failed at line %d: %s\n", __LINE__, #cond); \
+            ++failures;                                                              \
+        }                                                                            \
+    } while (0)
+
+// V/INTERNALS.doc:1554-1632: 15 rows, sorted by column n = 2
+static DF doc_frame() {
+    DF df;
+    std::vector<int> id(15);
+    std::iota(id.begin(), id.end(), 1);
+    df.add_col(id, "col1");
+    df.add_col(std::vector<unsigned>{1, 6, 1, 6, 1, 6, 1, 6, 6, 1, 6, 6, 6, 1, 16}, "col2");
+    df.add_col(std::vector<unsigned>{2, 7, 2, 7, 2, 7, 2, 7, 7, 2, 7, 7, 7, 2, 7}, "col3");
+    df.add_col(std::vector<unsigned>{3, 8, 3, 8, 3, 8, 3, 8, 8, 3, 8, 8, 8, 3, 8}, "col4");
+    return df;
+}
+
+static void test_doc_example() {
+    DF df = doc_frame();
+    unsigned n = 2;
+    df.sort_by(n);
+    CHECK(df.in_view);
+    const std::vector<int> asc = {1, 3, 5, 7, 10, 14, 2, 4, 6, 8, 9, 11, 12, 13, 15};
+    CHECK(df.get_col<int>(0) == asc);
+    df.materialize();
+    CHECK(!df.in_view);
+    CHECK(df.int_v[0] == asc);
+    CHECK((df.uint_v[0] == std::vector<unsigned>{1, 1, 1, 1, 1, 1, 6, 6, 6, 6, 6, 6, 6, 6, 16}));
+
+    DF d2 = doc_frame();
+    d2.sort_by<0>(n);  // the reference code: ascending, then std::reverse
+    std::vector<int> rev(asc.rbegin(), asc.rend());
+    CHECK(d2.get_col<int>(0) == rev);
+}
+
+static void test_hard_sort_and_view_composition() {
+    std::mt19937_64 rng(5);
+    const unsigned N = 200000;
+    std::vector<int> a(N), b(N), id(N);
+    std::vector<double> v(N);
+    for (unsigned i = 0; i < N; ++i) {
+        a[i] = (int)(rng() % 50) - 25;
+        b[i] = (int)(rng() % 7);
+        v[i] = (double)(rng() % 1000) / 8.0;
+        id[i] = (int)i;
+    }
+    // expected: stable by (a, b)
+    std::vector<unsigned> exp(N);
+    std::iota(exp.begin(), exp.end(), 0u);
+    std::stable_sort(exp.begin(), exp.end(), [&](unsigned x, unsigned y) { return std::tie(a[x], b[x]) < std::tie(a[y], b[y]); });
+
+    DF df;
+    df.add_col(a, "a");
+    df.add_col(b, "b");
+    df.add_col(v, "v");
+    df.add_col(id, "id");
+    // LSD composition through the view: sort by b, then (stably) by a
+    unsigned nb = 1, na = 0;
+    df.sort_by(nb);
+    df.sort_by(na);
+    std::vector<int> got = df.get_col<int>(3);
+    bool ok = true;
+    for (unsigned i = 0; i < N; ++i) ok &= (got[i] == (int)exp[i]);
+    CHECK(ok);
+
+    DF dh;
+    dh.add_col(a, "a");
+    dh.add_col(b, "b");
+    dh.add_col(id, "id");
+    dh.sort_by_cols<1, false>({0, 1});  // Hard: columns permuted in place
+    CHECK(!dh.in_view);
+    ok = true;
+    for (unsigned i = 0; i < N; ++i) ok &= (dh.int_v[2][i] == (int)exp[i]);
+    CHECK(ok);
+}
+
+static void test_sort_by_external() {
+    DF df = doc_frame();
+    std::vector<long> ext = {5, 4, 3, 2, 1, 0, -1, -2, -3, -4, -5, -6, -7, -8, -9};
+    df.sort_by_external<long>(ext);
+    std::vector<int> exp(15);
+    for (int i = 0; i < 15; ++i) exp[i] = 15 - i;
+    CHECK(df.get_col<int>(0) == exp);
+}
+
+static void test_transform_group_by() {
+    std::mt19937_64 rng(11);
+    const unsigned N = 100000;
+    std::vector<int> k1(N), iv(N);
+    std::vector<unsigned> k2(N);
+    std::vector<double> dv(N);
+    for (unsigned i = 0; i < N; ++i) {
+        k1[i] = (int)(rng() % 97) - 40;
+        k2[i] = (unsigned)(rng() % 3);
+        iv[i] = (int)(rng() % 2000001) - 1000000;
+        dv[i] = (double)((int64_t)(rng() % 4001) - 2000) / 16.0;  // exact sums
+    }
+    std::map<std::pair<int, unsigned>, std::tuple<long, long, double, int, int>> g;  // count, isum, dsum, imin, imax
+    for (unsigned i = 0; i < N; ++i) {
+        auto key = std::make_pair(k1[i], k2[i]);
+        auto it = g.find(key);
+        if (it == g.end()) g[key] = {1, iv[i], dv[i], iv[i], iv[i]};
+        else {
+            auto& [c, s, d, mn, mx] = it->second;
+            ++c; s += iv[i]; d += dv[i]; mn = std::min(mn, iv[i]); mx = std::max(mx, iv[i]);
+        }
+    }
+    DF df;
+    df.add_col(k1, "k1");
+    df.add_col(k2, "k2");
+    df.add_col(iv, "iv");
+    df.add_col(dv, "dv");
+    df.transform_group_by<void, void, GroupFunction::Occurence>({0, 1}, 2, "n");
+    df.transform_group_by<void, void, GroupFunction::Sum>({0, 1}, 2, "isum");
+    df.transform_group_by<void, void, GroupFunction::Mean>({0, 1}, 3, "dmean");
+    df.transform_group_by<void, void, GroupFunction::Min>({0, 1}, 2, "imin");
+    df.transform_group_by<void, void, GroupFunction::Max>({0, 1}, 2, "imax");
+    CHECK(df.ncol == 9);
+    bool ok = true;
+    for (unsigned i = 0; i < N; ++i) {
+        const auto& [c, s, d, mn, mx] = g[{k1[i], k2[i]}];
+        ok &= df.uint_v[1][i] == (unsigned)c;           // "n"
+        ok &= df.int_v[2][i] == (int)s;                  // "isum" (fits in int here)
+        ok &= df.dbl_v[1][i] == d / (double)c;           // "dmean"
+        ok &= df.int_v[3][i] == mn && df.int_v[4][i] == mx;
+    }
+    CHECK(ok);
+}
+
+int main() {
+    test_doc_example();
+    test_hard_sort_and_view_composition();
+    test_sort_by_external();
+    test_transform_group_by();
+    if (failures) {
+        std::fprintf(stderr, "%d checks failed\n", failures);
+        return 1;
+    }
+    std::printf("vison_b200 C++ layer: all checks passed\n");
+    return 0;
+}

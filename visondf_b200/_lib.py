@@ -62,6 +62,7 @@ class vdf_sort_groupby_args(C.Structure):
         ("group_keys_out", C.POINTER(C.c_void_p)), ("group_count_out", C.c_void_p),
         ("aggs", C.POINTER(vdf_agg_out)), ("group_start_out", C.c_void_p), ("row_group_out", C.c_void_p),
         ("n_groups_dev", C.c_void_p), ("n_groups_host", C.POINTER(C.c_uint64)),
+        ("perm_in", C.c_void_p),
     ]
 
 
@@ -97,7 +98,11 @@ def _load() -> C.CDLL:
         "vdf_groupby_sorted": (st, [vp, u64, C.POINTER(vdf_col), i32, C.POINTER(vdf_col), i32, C.POINTER(vp), vp,
                                     C.POINTER(vdf_agg_out), vp, vp, vp, C.POINTER(C.c_uint64), vp]),
         "vdf_sort_groupby": (st, [vp, C.POINTER(vdf_sort_groupby_args), vp]),
+        "vdf_sort_groupby_host": (st, [vp, C.POINTER(vdf_sort_groupby_args), vp]),
         "vdf_broadcast": (st, [vp, u64, vp, vp, u64, i32, vp, vp, vp]),
+        "vdf_gather_host": (st, [vp, u64, vp, C.POINTER(vdf_col), i32, C.POINTER(vp), vp]),
+        "vdf_transform_groupby_host": (st, [vp, u64, C.POINTER(vdf_col), i32, vdf_col, C.c_int32, vp, vp,
+                                            C.POINTER(C.c_uint64), vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

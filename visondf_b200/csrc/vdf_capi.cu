@@ -71,6 +71,8 @@ struct EventProfiler final : vdf::Profiler {
 struct vdf_ctx {
     int device = 0;
     bool profiling = false;
+    unsigned char* io = nullptr;  // staging for the host-memory entry points
+    size_t io_cap = 0;
     vdf::SortTuning tuning = vdf::default_sort_tuning();
     EventProfiler prof;
     std::mutex mu;
@@ -351,6 +353,7 @@ vdf_status vdf_ctx_destroy(vdf_ctx* c) {
         DeviceGuard g(c->device);
         c->prof.resolve();
         if (c->ws) cudaFree(c->ws);
+        if (c->io) cudaFree(c->io);
         if (c->dev_small) cudaFree(c->dev_small);
         if (c->host_pinned) cudaFreeHost(c->host_pinned);
     }
@@ -513,9 +516,12 @@ vdf_status vdf_groupby_sorted(vdf_ctx* c, uint64_t n, const vdf_col* keys, int n
     return finish_groups(c, a.n_groups, n_groups_host, s);
 }
 
-vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* stream) {
-    if (!c || !x) return VDF_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lk(c->mu);
+}  // extern "C"
+
+namespace {
+
+// vdf_sort_groupby with the context lock already held.
+vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaStream_t stream) {
     vdf_status st;
     const uint64_t n = x->n;
     if ((st = check_rows(c, n)) != VDF_OK) return st;
@@ -536,7 +542,7 @@ vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* st
                 return fail(c, VDF_ERR_INVALID_ARG, "agg_cols[%d]=%d out of range", i, x->agg_cols[i]);
     }
     DeviceGuard g(c->device);
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaStream_t s = stream;
     if (n == 0) {
         if (x->groupby && x->n_groups_dev) cudaMemsetAsync(x->n_groups_dev, 0, sizeof(uint64_t), s);
         if (x->groupby && x->n_groups_host) *x->n_groups_host = 0;
@@ -593,7 +599,7 @@ vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* st
         if (pay_own[p]) spay[p] = c->ws + pay_off[p];
     unsigned char* tws = c->ws + off;
 
-    cudaError_t e = vdf::run_sort(plan, cols, x->order, perm, skey[0], tws, err_word(c), s, prof_of(c));
+    cudaError_t e = vdf::run_sort(plan, cols, x->order, perm, skey[0], tws, err_word(c), s, prof_of(c), x->perm_in);
     c->launches += 2 + (uint64_t)plan.total_passes;
     if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
 
@@ -651,6 +657,300 @@ vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* st
     c->launches += launched;
     if (e != cudaSuccess) return from_cuda(c, e, "segmented reduction");
     return finish_groups(c, a.n_groups, x->n_groups_host, s);
+}
+
+// Device copy of a host vdf_sort_groupby_args: every input is staged into the
+// context's I/O buffer and every requested output gets a device slot there.
+struct HostStage {
+    vdf_col keys[vdf::kMaxKeys];
+    vdf_col pay[vdf::kMaxGather];
+    void* skeys[vdf::kMaxKeys];
+    void* spay[vdf::kMaxGather];
+    void* gkeys[vdf::kMaxKeys];
+    vdf_agg_out aggs[vdf::kMaxVals];
+    vdf_sort_groupby_args d;
+};
+
+vdf_status io_ensure(vdf_ctx* c, size_t bytes) {
+    if (bytes <= c->io_cap) return VDF_OK;
+    if (c->io) {
+        cudaFree(c->io);
+        c->io = nullptr;
+        c->io_cap = 0;
+    }
+    const size_t cap = align256(bytes + bytes / 8);
+    if (cudaMalloc(&c->io, cap) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, VDF_ERR_OOM, "I/O staging allocation of %zu bytes failed", cap);
+    }
+    c->io_cap = cap;
+    return VDF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vdf_status vdf_sort_groupby(vdf_ctx* c, const vdf_sort_groupby_args* x, void* stream) {
+    if (!c || !x) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    return sort_groupby_locked(c, x, static_cast<cudaStream_t>(stream));
+}
+
+vdf_status vdf_sort_groupby_host(vdf_ctx* c, const vdf_sort_groupby_args* x, void* stream) {
+    if (!c || !x) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    const uint64_t n = x->n;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if ((st = check_keys(c, n, x->keys, x->nkeys)) != VDF_OK) return st;
+    if (x->npayload < 0 || x->npayload > vdf::kMaxGather || (x->npayload && !x->payload))
+        return fail(c, VDF_ERR_INVALID_ARG, "bad payload columns");
+    for (int p = 0; p < x->npayload; ++p)
+        if (!valid_dtype(x->payload[p].dtype)) return fail(c, VDF_ERR_INVALID_ARG, "payload %d: bad dtype", p);
+    if (x->groupby && (x->nagg < 0 || x->nagg > vdf::kMaxVals || (x->nagg && (!x->agg_cols || !x->aggs))))
+        return fail(c, VDF_ERR_INVALID_ARG, "bad aggregation list");
+    for (int i = 0; x->groupby && i < x->nagg; ++i)
+        if (x->agg_cols[i] < 0 || x->agg_cols[i] >= x->npayload)
+            return fail(c, VDF_ERR_INVALID_ARG, "agg_cols[%d] out of range", i);
+    DeviceGuard g(c->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (n == 0) {
+        if (x->groupby && x->n_groups_host) *x->n_groups_host = 0;
+        return VDF_OK;
+    }
+    auto kw = [&](int k) { return (size_t)vdf::dtype_width(x->keys[k].dtype); };
+    auto pw = [&](int p) { return (size_t)vdf::dtype_width(x->payload[p].dtype); };
+    // layout of the staging buffer
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off = align256(off + bytes); return o; };
+    size_t o_keys[vdf::kMaxKeys], o_pay[vdf::kMaxGather], o_sk[vdf::kMaxKeys], o_sp[vdf::kMaxGather];
+    size_t o_gk[vdf::kMaxKeys], o_agg[vdf::kMaxVals][5], o_perm = 0, o_cnt = 0, o_gs = 0, o_rg = 0, o_ng = 0;
+    for (int k = 0; k < x->nkeys; ++k) o_keys[k] = take(n * kw(k));
+    for (int p = 0; p < x->npayload; ++p) o_pay[p] = take(n * pw(p));
+    const size_t o_pin = x->perm_in ? take(n * 4) : 0;
+    if (x->perm_out) o_perm = take(n * 4);
+    for (int k = 0; k < x->nkeys; ++k) o_sk[k] = (x->sorted_keys_out && x->sorted_keys_out[k]) ? take(n * kw(k)) : 0;
+    for (int p = 0; p < x->npayload; ++p) o_sp[p] = (x->payload_out && x->payload_out[p]) ? take(n * pw(p)) : 0;
+    if (x->groupby) {
+        for (int k = 0; k < x->nkeys; ++k) o_gk[k] = (x->group_keys_out && x->group_keys_out[k]) ? take(n * kw(k)) : 0;
+        if (x->group_count_out) o_cnt = take(n * 8);
+        for (int i = 0; i < x->nagg; ++i) {
+            const vdf_agg_out& a = x->aggs[i];
+            const size_t w = pw(x->agg_cols[i]);
+            o_agg[i][0] = a.sum ? take(n * 8) : 0;
+            o_agg[i][1] = a.sum_hi ? take(n * 8) : 0;
+            o_agg[i][2] = a.min ? take(n * w) : 0;
+            o_agg[i][3] = a.max ? take(n * w) : 0;
+            o_agg[i][4] = a.mean ? take(n * 8) : 0;
+        }
+        if (x->group_start_out) o_gs = take(n * 4);
+        if (x->row_group_out) o_rg = take(n * 4);
+        o_ng = take(8);
+    }
+    if ((st = io_ensure(c, off)) != VDF_OK) return st;
+    unsigned char* io = c->io;
+    auto at = [&](size_t o) -> void* { return io + o; };
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < x->nkeys && e == cudaSuccess; ++k)
+        e = cudaMemcpyAsync(at(o_keys[k]), x->keys[k].data, n * kw(k), cudaMemcpyHostToDevice, s);
+    for (int p = 0; p < x->npayload && e == cudaSuccess; ++p)
+        e = cudaMemcpyAsync(at(o_pay[p]), x->payload[p].data, n * pw(p), cudaMemcpyHostToDevice, s);
+    if (x->perm_in && e == cudaSuccess) e = cudaMemcpyAsync(at(o_pin), x->perm_in, n * 4, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return from_cuda(c, e, "copy inputs to the device");
+    HostStage h{};
+    vdf_sort_groupby_args& d = h.d;
+    d = *x;
+    for (int k = 0; k < x->nkeys; ++k) {
+        h.keys[k] = vdf_col{at(o_keys[k]), x->keys[k].dtype};
+        h.skeys[k] = o_sk[k] ? at(o_sk[k]) : nullptr;
+        h.gkeys[k] = (x->groupby && o_gk[k]) ? at(o_gk[k]) : nullptr;
+    }
+    for (int p = 0; p < x->npayload; ++p) {
+        h.pay[p] = vdf_col{at(o_pay[p]), x->payload[p].dtype};
+        h.spay[p] = o_sp[p] ? at(o_sp[p]) : nullptr;
+    }
+    d.keys = h.keys;
+    d.payload = h.pay;
+    d.perm_in = x->perm_in ? static_cast<const uint32_t*>(at(o_pin)) : nullptr;
+    d.perm_out = x->perm_out ? static_cast<uint32_t*>(at(o_perm)) : nullptr;
+    d.sorted_keys_out = x->sorted_keys_out ? h.skeys : nullptr;
+    d.payload_out = x->payload_out ? h.spay : nullptr;
+    uint64_t groups = 0;
+    if (x->groupby) {
+        for (int i = 0; i < x->nagg; ++i)
+            h.aggs[i] = vdf_agg_out{o_agg[i][0] ? at(o_agg[i][0]) : nullptr,
+                                    o_agg[i][1] ? static_cast<int64_t*>(at(o_agg[i][1])) : nullptr,
+                                    o_agg[i][2] ? at(o_agg[i][2]) : nullptr, o_agg[i][3] ? at(o_agg[i][3]) : nullptr,
+                                    o_agg[i][4] ? static_cast<double*>(at(o_agg[i][4])) : nullptr};
+        d.aggs = h.aggs;
+        d.group_keys_out = x->group_keys_out ? h.gkeys : nullptr;
+        d.group_count_out = o_cnt ? static_cast<int64_t*>(at(o_cnt)) : nullptr;
+        d.group_start_out = o_gs ? static_cast<uint32_t*>(at(o_gs)) : nullptr;
+        d.row_group_out = o_rg ? static_cast<uint32_t*>(at(o_rg)) : nullptr;
+        d.n_groups_dev = static_cast<uint64_t*>(at(o_ng));
+        d.n_groups_host = &groups;  // synchronises once the group count is known
+    }
+    if ((st = sort_groupby_locked(c, &d, s)) != VDF_OK) return st;
+    // results back to the host: rows (n) for the sorted frame, groups (G) for the group table
+    auto down = [&](void* dst, size_t o, size_t bytes) {
+        if (e == cudaSuccess && dst && bytes) e = cudaMemcpyAsync(dst, at(o), bytes, cudaMemcpyDeviceToHost, s);
+    };
+    down(x->perm_out, o_perm, n * 4);
+    for (int k = 0; k < x->nkeys; ++k)
+        if (o_sk[k]) down(x->sorted_keys_out[k], o_sk[k], n * kw(k));
+    for (int p = 0; p < x->npayload; ++p)
+        if (o_sp[p]) down(x->payload_out[p], o_sp[p], n * pw(p));
+    if (x->groupby) {
+        for (int k = 0; k < x->nkeys; ++k)
+            if (o_gk[k]) down(x->group_keys_out[k], o_gk[k], groups * kw(k));
+        if (o_cnt) down(x->group_count_out, o_cnt, groups * 8);
+        for (int i = 0; i < x->nagg; ++i) {
+            const vdf_agg_out& a = x->aggs[i];
+            const size_t w = pw(x->agg_cols[i]);
+            if (o_agg[i][0]) down(a.sum, o_agg[i][0], groups * 8);
+            if (o_agg[i][1]) down(a.sum_hi, o_agg[i][1], groups * 8);
+            if (o_agg[i][2]) down(a.min, o_agg[i][2], groups * w);
+            if (o_agg[i][3]) down(a.max, o_agg[i][3], groups * w);
+            if (o_agg[i][4]) down(a.mean, o_agg[i][4], groups * 8);
+        }
+        if (o_gs) down(x->group_start_out, o_gs, groups * 4);
+        if (o_rg) down(x->row_group_out, o_rg, n * 4);
+        if (x->n_groups_host) *x->n_groups_host = groups;
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, "copy results to the host");
+    return VDF_OK;
+}
+
+vdf_status vdf_gather_host(vdf_ctx* c, uint64_t n, const uint32_t* perm, const vdf_col* in, int ncols,
+                           void* const* out, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if (ncols < 0 || ncols > vdf::kMaxGather) return fail(c, VDF_ERR_INVALID_ARG, "ncols must be 0..%d", vdf::kMaxGather);
+    if (n == 0 || ncols == 0) return VDF_OK;
+    if (!perm || !in || !out) return fail(c, VDF_ERR_INVALID_ARG, "NULL perm, in or out");
+    for (int i = 0; i < ncols; ++i)
+        if (!valid_dtype(in[i].dtype) || !in[i].data || !out[i])
+            return fail(c, VDF_ERR_INVALID_ARG, "column %d: bad dtype or NULL pointer", i);
+    DeviceGuard g(c->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    size_t off = align256(n * 4);
+    size_t o_in[vdf::kMaxGather], o_out[vdf::kMaxGather];
+    for (int i = 0; i < ncols; ++i) {
+        o_in[i] = off;
+        off = align256(off + n * vdf::dtype_width(in[i].dtype));
+        o_out[i] = off;
+        off = align256(off + n * vdf::dtype_width(in[i].dtype));
+    }
+    if ((st = io_ensure(c, off)) != VDF_OK) return st;
+    const size_t rec = vdf::gather_record_bytes(ncols);
+    if (rec && (st = ws_ensure(c, n * rec)) != VDF_OK) return st;
+    cudaError_t e = cudaMemcpyAsync(c->io, perm, n * 4, cudaMemcpyHostToDevice, s);
+    vdf::GatherArgs ga{};
+    ga.perm = reinterpret_cast<const uint32_t*>(c->io);
+    ga.err = err_word(c);
+    ga.n = n;
+    ga.ncols = ncols;
+    for (int i = 0; i < ncols && e == cudaSuccess; ++i) {
+        const size_t w = (size_t)vdf::dtype_width(in[i].dtype);
+        e = cudaMemcpyAsync(c->io + o_in[i], in[i].data, n * w, cudaMemcpyHostToDevice, s);
+        ga.src[i] = c->io + o_in[i];
+        ga.dst[i] = c->io + o_out[i];
+        ga.width[i] = (int)w;
+    }
+    if (e != cudaSuccess) return from_cuda(c, e, "copy inputs to the device");
+    int launched = 0;
+    e = vdf::run_gather(ga, s, prof_of(c), rec ? c->ws : nullptr, &launched);
+    c->launches += launched;
+    for (int i = 0; i < ncols && e == cudaSuccess; ++i)
+        e = cudaMemcpyAsync(out[i], c->io + o_out[i], n * vdf::dtype_width(in[i].dtype), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, "gather");
+    return drain_and_check(c, s);
+}
+
+vdf_status vdf_transform_groupby_host(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, vdf_col val,
+                                      int32_t function, const uint32_t* perm_in, void* out, uint64_t* n_groups_host,
+                                      void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    vdf_status st;
+    if (function < VDF_AGG_COUNT || function > VDF_AGG_MAX) return fail(c, VDF_ERR_INVALID_ARG, "bad function %d", function);
+    if (!valid_dtype(val.dtype)) return fail(c, VDF_ERR_INVALID_ARG, "bad value dtype");
+    std::lock_guard<std::mutex> lk(c->mu);
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if ((st = check_keys(c, n, keys, nkeys)) != VDF_OK) return st;
+    if (n == 0) {
+        if (n_groups_host) *n_groups_host = 0;
+        return VDF_OK;
+    }
+    if (!out || (function != VDF_AGG_COUNT && !val.data)) return fail(c, VDF_ERR_INVALID_ARG, "NULL value or output");
+    DeviceGuard g(c->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const bool is_float = (val.dtype == VDF_F64 || val.dtype == VDF_F32);
+    const int vw = vdf::dtype_width(val.dtype);
+    // output element width: count and sum (integer low word / double) and mean are 8 bytes
+    const int ow = (function == VDF_AGG_MIN || function == VDF_AGG_MAX) ? vw : 8;
+    (void)is_float;
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off = align256(off + bytes); return o; };
+    size_t o_keys[vdf::kMaxKeys];
+    for (int k = 0; k < nkeys; ++k) o_keys[k] = take(n * vdf::dtype_width(keys[k].dtype));
+    const size_t o_val = (function != VDF_AGG_COUNT) ? take(n * vw) : 0;
+    const size_t o_pin = perm_in ? take(n * 4) : 0;
+    const size_t o_perm = take(n * 4), o_rg = take(n * 4), o_gv = take(n * 8), o_out = take(n * (size_t)ow);
+    const size_t o_ng = take(8);
+    if ((st = io_ensure(c, off)) != VDF_OK) return st;
+    unsigned char* io = c->io;
+    cudaError_t e = cudaSuccess;
+    vdf_col dkeys[vdf::kMaxKeys];
+    for (int k = 0; k < nkeys && e == cudaSuccess; ++k) {
+        e = cudaMemcpyAsync(io + o_keys[k], keys[k].data, n * vdf::dtype_width(keys[k].dtype), cudaMemcpyHostToDevice, s);
+        dkeys[k] = vdf_col{io + o_keys[k], keys[k].dtype};
+    }
+    if (o_val && e == cudaSuccess) e = cudaMemcpyAsync(io + o_val, val.data, n * vw, cudaMemcpyHostToDevice, s);
+    if (perm_in && e == cudaSuccess) e = cudaMemcpyAsync(io + o_pin, perm_in, n * 4, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return from_cuda(c, e, "copy inputs to the device");
+    vdf_col dval{o_val ? io + o_val : nullptr, val.dtype};
+    vdf_agg_out agg{};
+    int32_t agg_col = 0;
+    vdf_sort_groupby_args d{};
+    d.n = n;
+    d.keys = dkeys;
+    d.nkeys = nkeys;
+    d.order = VDF_ORDER_ASC;
+    d.perm_in = o_pin ? reinterpret_cast<const uint32_t*>(io + o_pin) : nullptr;
+    d.perm_out = reinterpret_cast<uint32_t*>(io + o_perm);
+    d.groupby = 1;
+    d.row_group_out = reinterpret_cast<uint32_t*>(io + o_rg);
+    void* gv = io + o_gv;
+    if (function == VDF_AGG_COUNT) {
+        d.group_count_out = static_cast<int64_t*>(gv);
+    } else {
+        d.payload = &dval;
+        d.npayload = 1;
+        d.agg_cols = &agg_col;
+        d.nagg = 1;
+        d.aggs = &agg;
+        if (function == VDF_AGG_SUM) agg.sum = gv;
+        else if (function == VDF_AGG_MEAN) agg.mean = static_cast<double*>(gv);
+        else if (function == VDF_AGG_MIN) agg.min = gv;
+        else agg.max = gv;
+    }
+    uint64_t groups = 0;
+    d.n_groups_dev = reinterpret_cast<uint64_t*>(io + o_ng);
+    d.n_groups_host = &groups;
+    if ((st = sort_groupby_locked(c, &d, s)) != VDF_OK) return st;
+    // every row receives its group's value, in the frame's row order
+    e = vdf::run_broadcast(d.row_group_out, n, gv, groups, ow, d.perm_out, io + o_out, err_word(c), s, prof_of(c));
+    c->launches++;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, io + o_out, n * (size_t)ow, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, "transform output");
+    if (n_groups_host) *n_groups_host = groups;
+    return drain_and_check(c, s);
 }
 
 vdf_status vdf_broadcast(vdf_ctx* c, uint64_t n, const uint32_t* row_group, const void* group_vals,

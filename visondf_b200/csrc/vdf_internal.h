@@ -86,9 +86,12 @@ struct SortPlan {
 
 SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const SortTuning& tuning);
 // Sorts; writes perm_out (and key0_out = raw sorted most-significant key, may
-// be null).  Bounded waits that give up OR their ErrBits into *err.
+// be null).  Bounded waits that give up OR their ErrBits into *err.  With
+// perm_in (a permutation of [0, n)) the rows are sorted as seen through it
+// and perm_out is the composed permutation.
 cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
-                     void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof = nullptr);
+                     void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof = nullptr,
+                     const uint32_t* perm_in = nullptr);
 cudaError_t prepare_sort_kernels();
 
 // ---- gather ----------------------------------------------------------------

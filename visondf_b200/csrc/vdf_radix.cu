@@ -503,7 +503,8 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
 }
 
 cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
-                     void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof) {
+                     void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof,
+                     const uint32_t* perm_in) {
     const uint64_t n = p.n;
     if (n == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(ws + p.off_zero, 0, p.zero_bytes, s);
@@ -570,9 +571,11 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
             a.err = err;
             int mode;
             if (q == 0 && k == p.nkeys - 1) {
-                mode = IN_RAW;
+                // first pass: the rows themselves, or the rows as seen through
+                // an input permutation (the reference radix sort's in/out idx)
+                mode = perm_in ? IN_GATHER : IN_RAW;
                 a.keys_in = key_cols[k];
-                a.vals_in = nullptr;
+                a.vals_in = perm_in;
             } else if (q == 0) {
                 mode = IN_GATHER;
                 a.keys_in = key_cols[k];
