@@ -147,3 +147,107 @@ def test_empty_input(ctx):
     e64 = torch.empty(0, dtype=torch.float64, device="cuda")
     gr = ctx.sort_groupby([e32], [e64], agg_cols=[0])
     assert gr.n_groups == 0
+
+
+def _host_args(keys, payload, agg_cols, n, perm_in=None):
+    """vdf_sort_groupby_args over numpy host arrays, with numpy output buffers."""
+    import ctypes as C
+    from visondf_b200 import _lib
+    out = {"perm": np.empty(n, np.uint32), "gk": [np.empty(n, k.dtype) for k in keys], "cnt": np.empty(n, np.int64),
+           "aggs": []}
+    a = _lib.vdf_sort_groupby_args()
+    kc = (_lib.vdf_col * len(keys))(*[_lib.vdf_col(k.ctypes.data, _lib_dt(k)) for k in keys])
+    pc = (_lib.vdf_col * max(1, len(payload)))(*[_lib.vdf_col(p.ctypes.data, _lib_dt(p)) for p in payload])
+    aggs = (_lib.vdf_agg_out * max(1, len(agg_cols)))()
+    for i, c in enumerate(agg_cols):
+        v = payload[c]
+        f = v.dtype.kind == "f"
+        o = {"sum": np.empty(n, np.float64 if f else np.int64), "hi": None if f else np.empty(n, np.int64),
+             "min": np.empty(n, v.dtype), "max": np.empty(n, v.dtype), "mean": np.empty(n, np.float64)}
+        out["aggs"].append(o)
+        aggs[i] = _lib.vdf_agg_out(o["sum"].ctypes.data, None if f else o["hi"].ctypes.data, o["min"].ctypes.data,
+                                   o["max"].ctypes.data, o["mean"].ctypes.data)
+    gk = (C.c_void_p * len(keys))(*[g.ctypes.data for g in out["gk"]])
+    ac = (C.c_int32 * max(1, len(agg_cols)))(*agg_cols)
+    ng = C.c_uint64(0)
+    a.n, a.keys, a.nkeys, a.order = n, kc, len(keys), 0
+    a.payload, a.npayload = pc, len(payload)
+    a.perm_out = out["perm"].ctypes.data
+    a.groupby, a.agg_cols, a.nagg, a.aggs = 1, ac, len(agg_cols), aggs
+    a.group_keys_out, a.group_count_out = gk, out["cnt"].ctypes.data
+    a.n_groups_host = C.pointer(ng)
+    if perm_in is not None:
+        a.perm_in = perm_in.ctypes.data
+    out["_keep"] = [kc, pc, aggs, gk, ac, keys, payload, perm_in]
+    out["_ng"] = ng
+    return a, out
+
+
+def _lib_dt(a):
+    from visondf_b200 import _lib
+    return {np.dtype(np.int32): _lib.I32, np.dtype(np.int64): _lib.I64, np.dtype(np.uint32): _lib.U32,
+            np.dtype(np.uint64): _lib.U64, np.dtype(np.float64): _lib.F64, np.dtype(np.float32): _lib.F32}[a.dtype]
+
+
+def test_host_entry_point_matches_oracle(ctx):
+    import ctypes as C
+    rng = np.random.default_rng(41)
+    keys, vals = frame(123_457, [np.int64, np.int32], 60, rng)
+    a, out = _host_args(keys, vals, [0, 1], keys[0].size)
+    st = vdf.lib.vdf_sort_groupby_host(ctx.handle, C.byref(a), None)
+    assert st == 0, vdf.lib.vdf_ctx_last_error(ctx.handle)
+    og = ob.groupby(keys, vals)
+    g = int(out["_ng"].value)
+    assert g == og.n_groups
+    assert (out["perm"] == ob.argsort(keys)).all()
+    for k, ok in zip(out["gk"], og.keys):
+        assert (k[:g] == ok).all()
+    assert (out["cnt"][:g] == og.count).all()
+    assert (out["aggs"][1]["sum"][:g] == og.sum[1]).all() and (out["aggs"][1]["hi"][:g] == og.sum_hi[1]).all()
+    assert (np.abs(out["aggs"][0]["sum"][:g] - og.sum[0]) <= 1e-12 * np.maximum(og.abs[0], 1e-300)).all()
+
+
+def test_host_entry_point_with_input_permutation(ctx):
+    # sorting through a row view composes the permutations (stable within the view)
+    import ctypes as C
+    rng = np.random.default_rng(42)
+    n = 50_000
+    k = rng.integers(0, 10, n).astype(np.int32)
+    view = rng.permutation(n).astype(np.uint32)
+    a, out = _host_args([k], [], [], n, perm_in=view)
+    a.groupby = 0
+    assert vdf.lib.vdf_sort_groupby_host(ctx.handle, C.byref(a), None) == 0
+    exp = view[np.argsort(k[view], kind="stable")]
+    assert (out["perm"] == exp).all()
+
+
+def test_gather_host_and_transform_groupby_host(ctx):
+    import ctypes as C
+    from visondf_b200 import _lib
+    rng = np.random.default_rng(43)
+    n = 70_001
+    perm = rng.permutation(n).astype(np.uint32)
+    cols = [rng.standard_normal(n), rng.integers(-5, 5, n).astype(np.int32)]
+    outs = [np.empty_like(c) for c in cols]
+    ic = (_lib.vdf_col * 2)(*[_lib.vdf_col(c.ctypes.data, _lib_dt(c)) for c in cols])
+    oc = (C.c_void_p * 2)(*[o.ctypes.data for o in outs])
+    assert vdf.lib.vdf_gather_host(ctx.handle, n, perm.ctypes.data, ic, 2, oc, None) == 0
+    for c, o in zip(cols, outs):
+        assert bits_equal(o, c[perm])
+    key = rng.integers(0, 300, n).astype(np.int64)
+    val = rng.integers(-1000, 1000, n).astype(np.int32)
+    og = ob.groupby([key], [val])
+    lookup = {int(k): i for i, k in enumerate(og.keys[0])}
+    gi = np.array([lookup[int(k)] for k in key])
+    kc = (_lib.vdf_col * 1)(_lib.vdf_col(key.ctypes.data, _lib.I64))
+    vc = _lib.vdf_col(val.ctypes.data, _lib.I32)
+    ng = C.c_uint64(0)
+    for fn, exp in [(0, og.count[gi]), (1, og.sum[0][gi]), (2, og.mean[0][gi]), (3, og.min[0][gi]), (4, og.max[0][gi])]:
+        out = np.empty(n, np.int32 if fn in (3, 4) else (np.float64 if fn == 2 else np.int64))
+        st = vdf.lib.vdf_transform_groupby_host(ctx.handle, n, kc, 1, vc, fn, None, out.ctypes.data, C.byref(ng), None)
+        assert st == 0
+        assert int(ng.value) == og.n_groups
+        if fn == 2:
+            np.testing.assert_allclose(out, exp, rtol=1e-12)
+        else:
+            assert (out == exp).all(), fn
