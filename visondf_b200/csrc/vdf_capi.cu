@@ -177,7 +177,7 @@ vdf_status check_rows(vdf_ctx* c, uint64_t n) {
 // Sorted copies of key columns 1..nkeys-1 (column 0 is written by the last
 // radix pass) by gathering through the permutation.
 vdf_status emit_other_keys(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, const uint32_t* perm,
-                           void* const* sorted_keys_out, void* rec_ws, cudaStream_t s) {
+                           void* const* sorted_keys_out, void* rec_ws, size_t rec_ws_bytes, cudaStream_t s) {
     if (!sorted_keys_out) return VDF_OK;
     vdf::GatherArgs g{};
     g.perm = perm;
@@ -192,7 +192,7 @@ vdf_status emit_other_keys(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkey
     }
     if (!g.ncols) return VDF_OK;
     int launched = 0;
-    cudaError_t e = vdf::run_gather(g, s, prof_of(c), rec_ws, &launched);
+    cudaError_t e = vdf::run_gather(g, s, prof_of(c), rec_ws, rec_ws_bytes, &launched);
     c->launches += launched;
     return from_cuda(c, e, "gather keys");
 }
@@ -220,8 +220,7 @@ vdf_status sort_impl(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, int
     cudaError_t e = vdf::run_sort(p, cols, order, perm_out, key0_out, ws, err_word(c), s, prof_of(c));
     c->launches += 2 + (uint64_t)p.total_passes;
     if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
-    const bool packed = ws_bytes >= sort_ws_need(p, n, nkeys, sorted_keys_out);
-    return emit_other_keys(c, n, keys, nkeys, perm_out, sorted_keys_out, packed ? ws : nullptr, s);
+    return emit_other_keys(c, n, keys, nkeys, perm_out, sorted_keys_out, ws, ws_bytes, s);
 }
 
 vdf_status finish_groups(vdf_ctx* c, uint64_t* n_groups_dev, uint64_t* n_groups_host, cudaStream_t s) {
@@ -470,7 +469,8 @@ vdf_status vdf_gather(vdf_ctx* c, uint64_t n, const uint32_t* perm, const vdf_co
     const size_t rec = vdf::gather_record_bytes(ncols);
     if (rec && (st = ws_ensure(c, n * rec)) != VDF_OK) return st;
     int launched = 0;
-    cudaError_t e = vdf::run_gather(g, static_cast<cudaStream_t>(stream), prof_of(c), rec ? c->ws : nullptr, &launched);
+    cudaError_t e = vdf::run_gather(g, static_cast<cudaStream_t>(stream), prof_of(c), rec ? c->ws : nullptr,
+                                    rec ? c->ws_cap : 0, &launched);
     c->launches += launched;
     return from_cuda(c, e, "gather");
 }
@@ -585,9 +585,11 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
             off += align256(n * (size_t)vdf::dtype_width(x->payload[p].dtype));
         }
     }
+    // columns the gather will produce: requested outputs and the sorted
+    // copies the group-by needs (owned buffers, assigned below)
     int ngather = 0;
-    for (int k = 1; k < x->nkeys; ++k) ngather += skey[k] ? 1 : 0;
-    for (int p = 0; p < x->npayload; ++p) ngather += spay[p] ? 1 : 0;
+    for (int k = 1; k < x->nkeys; ++k) ngather += (skey[k] || key_own[k]) ? 1 : 0;
+    for (int p = 0; p < x->npayload; ++p) ngather += (spay[p] || pay_own[p]) ? 1 : 0;
     const size_t rec_bytes = (size_t)n * vdf::gather_record_bytes(std::min(ngather, vdf::kMaxGather));
     const size_t seg_bytes = x->groupby ? vdf::segreduce_workspace_bytes(n, x->nagg) : 0;
     const size_t tail = std::max(std::max(plan.ws_bytes, seg_bytes), rec_bytes);
@@ -612,7 +614,7 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
     auto flush = [&]() -> cudaError_t {
         if (!ga.ncols) return cudaSuccess;
         int launched = 0;
-        cudaError_t ge = vdf::run_gather(ga, s, prof_of(c), tws, &launched);
+        cudaError_t ge = vdf::run_gather(ga, s, prof_of(c), tws, c->ws_cap - off, &launched);
         c->launches += launched;
         ga.ncols = 0;
         return ge;
@@ -863,7 +865,7 @@ vdf_status vdf_gather_host(vdf_ctx* c, uint64_t n, const uint32_t* perm, const v
     }
     if (e != cudaSuccess) return from_cuda(c, e, "copy inputs to the device");
     int launched = 0;
-    e = vdf::run_gather(ga, s, prof_of(c), rec ? c->ws : nullptr, &launched);
+    e = vdf::run_gather(ga, s, prof_of(c), rec ? c->ws : nullptr, rec ? c->ws_cap : 0, &launched);
     c->launches += launched;
     for (int i = 0; i < ncols && e == cudaSuccess; ++i)
         e = cudaMemcpyAsync(out[i], c->io + o_out[i], n * vdf::dtype_width(in[i].dtype), cudaMemcpyDeviceToHost, s);

@@ -131,10 +131,11 @@ size_t gather_record_bytes(int ncols) {
     return (ncols >= 2 && ncols <= kMaxGather) ? (size_t)16 * ((ncols + 1) / 2) : 0;
 }
 
-cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof, void* rec_ws, int* launches) {
+cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof, void* rec_ws, size_t rec_ws_bytes,
+                       int* launches) {
     if (g.n == 0 || g.ncols == 0) return cudaSuccess;
     const size_t rec = gather_record_bytes(g.ncols);
-    if (rec_ws && rec) {
+    if (rec_ws && rec && rec_ws_bytes / rec >= g.n) {
         unsigned char* recs = static_cast<unsigned char*>(rec_ws);
         const uint32_t blocks = (uint32_t)((g.n + 255) / 256);
         if (prof) prof->begin(KC_PACK, s);

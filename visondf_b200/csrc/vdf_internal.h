@@ -107,10 +107,12 @@ struct GatherArgs {
 // Bytes per row of the packed-record buffer a gather of ncols columns uses
 // (0: gathered column by column).
 size_t gather_record_bytes(int ncols);
-// rec_ws: n * gather_record_bytes(ncols) bytes of workspace, or null for the
-// column-by-column path.  *launches is increased by the kernels launched.
+// rec_ws: workspace of rec_ws_bytes for the packed records; the packed path
+// runs only when it holds n * gather_record_bytes(ncols) bytes, otherwise the
+// columns are gathered one by one.  *launches is increased by the kernels
+// launched.
 cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof = nullptr, void* rec_ws = nullptr,
-                       int* launches = nullptr);
+                       size_t rec_ws_bytes = 0, int* launches = nullptr);
 
 // ---- segmented reduction (group-by over sorted rows) -----------------------
 // A column of rows in key order.
