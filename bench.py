@@ -187,7 +187,7 @@ def our_arm(args, rank: int, world: int, local_rank: int):
     import torch.distributed as dist
 
     import visondf_b200 as vdf
-    from visondf_b200 import datagen
+    from visondf_b200 import datagen, replicas
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
@@ -247,11 +247,8 @@ def our_arm(args, rank: int, world: int, local_rank: int):
     ctx.check(stream)
     n_groups = int(outs["ngroups_dev"].item())
     clk = clocks.summary()
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = n * world / (ms / 1e3)
+    ms = replicas.max_over_ranks(ms, world, dev)
+    value = replicas.whole_job_rate(n, world, ms)
 
     # ---- roofline of the dominant kernel ------------------------------------------
     peak, peak_kind = measured_peaks()
@@ -328,11 +325,8 @@ def our_arm(args, rank: int, world: int, local_rank: int):
         ems = e0.elapsed_time(e1) / args.steps
         g = int(ng.value)
         d2h = 4 * n + g * (8 + 4 + 8 + 4 * 8 + (8 + 8 + 4 + 4 + 8))
-        if world > 1:
-            t = torch.tensor([ems], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ems = float(t.item())
-        e2e = {"value": n * world / (ems / 1e3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+        ems = replicas.max_over_ranks(ems, world, dev)
+        e2e = {"value": replicas.whole_job_rate(n, world, ems), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                "ms_per_step": ems, "call": "vdf_sort_groupby_host (pinned host buffers)"}
 
     # ---- CPU baseline (rank 0, one GPU only) -------------------------------------
