@@ -48,8 +48,10 @@ UNIT = "rows/s"
 WORKLOAD = ("two-key stable radix sort (key1 int64 full range, key2 int32 Zipf s=1.1 over 1M values) "
             "+ gather of 3 payload columns (f64, int32, uint64 row id) + group-by (key1, key2) "
             "count/sum/min/max/mean of the f64 and int32 payloads")
-# Canonical algorithmic bytes per row (8-bit digits over full key widths,
-# u32 row ids; see DESIGN.md's byte model): sort 344 + group-by with G ~= N 108.
+# Canonical algorithmic bytes per row (8-bit digits over the full key widths,
+# u32 row ids, each pass reading and writing key + row id once): sort 344
+# (key2 68, key1 220, key2 emit 12, payload gather 44) + group-by with G ~= N
+# 108 (sorted keys 12 + values 12 read, 84 written per group).
 SORT_BYTES_PER_ROW = 344
 GROUPBY_BYTES_PER_ROW_G_EQ_N = 108
 
