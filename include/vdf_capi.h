@@ -312,6 +312,85 @@ vdf_status vdf_transform_groupby_host(vdf_ctx* ctx, uint64_t n, const vdf_col* k
 vdf_status vdf_broadcast(vdf_ctx* ctx, uint64_t n, const uint32_t* row_group, const void* group_vals,
                          uint64_t n_groups, int width, const uint32_t* perm, void* out, void* stream);
 
+/* ---- batched queries ------------------------------------------------------
+ * Many independent sort + group-by queries (each: stable ascending sort of
+ * one key column, then count/sum/min/max/mean of every value column per
+ * key) planned once and run as one fixed sequence of launches.  The
+ * reference runs them one call each (sort_by_mt, V/transform/sort_by/
+ * sort_by_mt.hpp:3-180, then transform_group_by_onecol_mt,
+ * V/transform/transform_group_by/transform_group_by_onecol_mt.hpp:14-373). */
+#define VDF_BATCH_MAX_VALS 4
+
+/* One query: n rows of one key column and nvals value columns (device
+ * pointers; the value dtypes are the batch's). */
+typedef struct vdf_batch_query {
+    uint64_t n;
+    vdf_col key;
+    const void* vals[VDF_BATCH_MAX_VALS];
+} vdf_batch_query;
+
+/* Execution choices (vdf_batch_default_tuning; the Python autotuner searches
+ * them).  Queries of at most small_rows rows (<= 8192) are each sorted and
+ * grouped by one CTA in shared memory, with small_bits-bit digits (4 or 8);
+ * the others are sorted together by the segmented radix passes of variant
+ * seg_variant (vdf_batch_variant_info: digit bits, rows per tile). */
+typedef struct vdf_batch_tuning {
+    uint32_t small_rows;
+    int32_t small_bits;
+    int32_t seg_variant;
+} vdf_batch_tuning;
+
+/* Outputs are arenas of vdf_batch_rows(batch) = sum of n rows / group slots
+ * (device arrays, caller-owned):
+ *   perm_out[row_offset[q] + i]      i-th row (0-based within q) of q in key order
+ *   group slot group_offset[q] + g   q's g-th group (ascending key), g < n_groups[q]:
+ *       group_count_out[slot], aggs[j].sum/sum_hi/min/max/mean[slot]
+ *       (vdf_agg_out semantics); group keys are packed in q's own key
+ *       width from byte 8 * group_offset[q] of group_keys_out (8 bytes per slot)
+ *   row_offset_out, group_offset_out, n_groups_out: device [nqueries]
+ * A query of 0 rows has n_groups 0. */
+typedef struct vdf_batch_args {
+    uint32_t nqueries;
+    const vdf_batch_query* queries; /* host array, copied by vdf_batch_create */
+    int32_t nvals;
+    int32_t val_dtypes[VDF_BATCH_MAX_VALS];
+    uint32_t* perm_out;
+    void* group_keys_out;     /* may be NULL */
+    int64_t* group_count_out; /* may be NULL */
+    vdf_agg_out aggs[VDF_BATCH_MAX_VALS];
+    uint64_t* row_offset_out;
+    uint64_t* group_offset_out;
+    uint64_t* n_groups_out;
+} vdf_batch_args;
+
+typedef struct vdf_batch vdf_batch;
+
+int vdf_batch_variant_count(void);
+vdf_status vdf_batch_variant_info(int index, int32_t* digit_bits, int32_t* tile_rows);
+vdf_status vdf_batch_default_tuning(vdf_batch_tuning* tuning);
+
+/* Plans the batch (tuning NULL = default), sizes the context workspace for
+ * it and uploads its descriptor tables; synchronous.  Writes row_offset_out
+ * now.  The batch uses the context's workspace: a later call on the context
+ * that needs a larger workspace invalidates it (launch then fails with
+ * VDF_ERR_WORKSPACE), and its launches must not overlap other work of the
+ * context on the GPU. */
+vdf_status vdf_batch_create(vdf_ctx* ctx, const vdf_batch_args* args, const vdf_batch_tuning* tuning,
+                            vdf_batch** out);
+/* Rows (= group slots) of the batch's output arenas. */
+uint64_t vdf_batch_rows(const vdf_batch* batch);
+/* How the plan split the queries (any pointer may be NULL). */
+vdf_status vdf_batch_info(const vdf_batch* batch, uint32_t* small_queries, uint64_t* small_rows,
+                          uint32_t* large_queries, uint64_t* large_rows);
+/* Enqueues the batch on `stream`: no allocation, no host synchronisation,
+ * no host memory read, so it can be stream-captured.  Device-side wait
+ * timeouts are reported by vdf_ctx_check. */
+vdf_status vdf_batch_launch(vdf_batch* batch, void* stream);
+/* The same work as one CUDA graph: captured on the first call, replayed on
+ * every call (one graph launch). */
+vdf_status vdf_batch_launch_graph(vdf_batch* batch, void* stream);
+void vdf_batch_destroy(vdf_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,188 @@
+"""Batched queries (vdf_batch_*): every query of a mixed batch against the
+oracle, the same batch under every tuning (one-CTA path, segmented path,
+4/8/11-bit digits, tile sizes), graph replay, and each query alone versus in
+the mix.  Bit-exact for permutations, group keys, counts, integer sums and
+min/max; f64 sums and means within 1e-12 * sum|x| (f64 sums may differ in
+the last bits between a query run alone and in a mix, since the segmented
+reduction's tiles fall differently)."""
+import numpy as np
+import pytest
+import torch
+
+import oracle_bind as ob
+import visondf_b200 as vdf
+from gpu_util import assert_f64_close, bits_equal, dev, host
+from visondf_b200 import _lib, datagen
+
+pytestmark = pytest.mark.gpu
+
+KEY_TYPES = [np.int32, np.int64, np.uint32, np.uint64, np.float64, np.float32]
+
+
+def make_queries(specs):
+    out = []
+    for i, (n, dt, card) in enumerate(specs):
+        rng = np.random.default_rng(9000 + i)
+        if np.dtype(dt).kind == "f":
+            pool = rng.standard_normal(max(1, card)).astype(dt)
+            if card > 3:
+                pool[:3] = np.array([-0.0, np.inf, -np.inf], dtype=dt)
+        else:
+            pool = datagen.distinct_pool(rng, max(1, card), dt)
+        key = pool[rng.integers(0, len(pool), size=n)] if n else np.empty(0, dt)
+        v1 = rng.standard_normal(n)
+        v2 = rng.integers(-10**15, 10**15, size=n, dtype=np.int64)
+        out.append((key, v1, v2))
+    return out
+
+
+SPECS = [(0, np.int32, 1), (1, np.int64, 1), (7, np.uint32, 3), (1000, np.int32, 10), (4096, np.int64, 2048),
+         (4097, np.int32, 4), (8192, np.float64, 100), (2048, np.float32, 50), (20_000, np.uint64, 5000),
+         (150_001, np.int64, 40_000), (33_333, np.int32, 2), (70_000, np.float64, 1000), (3, np.int64, 3),
+         (500, np.uint64, 1), (90_000, np.int32, 45_000), (6000, np.uint32, 6000)]
+
+
+def to_batch(ctx, queries, tuning=None):
+    qs = [(dev(k), [dev(v1), dev(v2)]) for k, v1, v2 in queries]
+    return vdf.Batch(ctx, qs, tuning), qs
+
+
+def check_against_oracle(b, queries):
+    for q, (key, v1, v2) in enumerate(queries):
+        r = b.result(q)
+        n = key.size
+        if n == 0:
+            assert r.n_groups == 0 and r.perm.numel() == 0
+            continue
+        assert (host(r.perm).view(np.uint32) == ob.argsort([key])).all(), q
+        og = ob.groupby([key], [v1, v2])
+        assert r.n_groups == og.n_groups, q
+        assert bits_equal(host(r.keys), og.keys[0]), q
+        assert (host(r.count) == og.count).all(), q
+        a1, a2 = r.aggs
+        assert (host(a2.sum) == og.sum[1]).all() and (host(a2.sum_hi) == og.sum_hi[1]).all(), q
+        assert bits_equal(host(a2.min), og.min[1]) and bits_equal(host(a2.max), og.max[1]), q
+        assert bits_equal(host(a1.min), og.min[0]) and bits_equal(host(a1.max), og.max[0]), q
+        assert_f64_close(host(a1.sum), og.sum[0], og.abs[0], f"query {q} f64 sum")
+        assert_f64_close(host(a1.mean), og.mean[0], og.abs[0] / og.count, f"query {q} f64 mean")
+        assert_f64_close(host(a2.mean), og.mean[1], np.abs(og.mean[1]), f"query {q} int mean")
+
+
+def snapshot(b, nq):
+    out = []
+    for q in range(nq):
+        r = b.result(q)
+        out.append([host(r.perm), r.n_groups, host(r.keys), host(r.count)] +
+                   [host(x) for a in r.aggs for x in (a.sum, a.sum_hi, a.min, a.max, a.mean) if x is not None])
+    return out
+
+
+def test_mixed_batch_matches_the_oracle(ctx):
+    queries = make_queries(SPECS)
+    b, _ = to_batch(ctx, queries)
+    info = b.info()
+    assert info["small_queries"] > 0 and info["large_queries"] > 0
+    b.launch()
+    ctx.check()
+    check_against_oracle(b, queries)
+    b.close()
+
+
+@pytest.mark.parametrize("seg_variant", range(len(_lib.batch_variants())))
+@pytest.mark.parametrize("small", [(0, 8), (4096, 4), (8192, 8), (8192, 4)])
+def test_every_tuning_matches_the_oracle(ctx, seg_variant, small):
+    queries = make_queries(SPECS)
+    b, _ = to_batch(ctx, queries, dict(small_rows=small[0], small_bits=small[1], seg_variant=seg_variant))
+    b.launch()
+    ctx.check()
+    check_against_oracle(b, queries)
+    b.close()
+
+
+def test_graph_replay_gives_the_same_bits(ctx):
+    queries = make_queries(SPECS)
+    b, _ = to_batch(ctx, queries)
+    b.launch()
+    ctx.check()
+    ref = snapshot(b, len(queries))
+    for _ in range(3):
+        b.perm.fill_(-1)
+        b.count.fill_(-1)
+        b.launch_graph()
+        ctx.check()
+        got = snapshot(b, len(queries))
+        for x, y in zip(ref, got):
+            assert all(bits_equal(np.asarray(u), np.asarray(v)) for u, v in zip(x, y))
+    b.close()
+
+
+def test_each_query_alone_equals_the_mix(ctx):
+    queries = make_queries(SPECS)
+    b, _ = to_batch(ctx, queries)
+    b.launch()
+    ctx.check()
+    mixed = snapshot(b, len(queries))
+    for q, one in enumerate(queries):
+        a, _ = to_batch(ctx, [one])
+        a.launch()
+        ctx.check()
+        alone = snapshot(a, 1)[0]
+        m = mixed[q]
+        assert (alone[0] == m[0]).all() and alone[1] == m[1]
+        assert bits_equal(alone[2], m[2]) and (alone[3] == m[3]).all()
+        # f64 sum / mean: within tolerance; everything else bit-identical
+        f_sum, f_min, f_max, f_mean = alone[4:8]
+        assert bits_equal(f_min, m[5]) and bits_equal(f_max, m[6])
+        absum = np.abs(one[1]).sum() if one[1].size else 0.0
+        assert np.all(np.abs(f_sum - m[4]) <= 1e-12 * absum + 1e-300)
+        for u, v in zip(alone[8:], m[8:]):
+            if u.dtype == np.float64:
+                assert np.all(np.abs(u - v) <= 1e-12 * np.abs(v) + 1e-300)
+            else:
+                assert bits_equal(u, v)
+        a.close()
+    b.close()
+
+
+def test_generated_batch_shape_and_parity_sample(ctx):
+    """A scaled-down batch from the batched-workload generator (400 queries,
+    same distributions), every query checked."""
+    specs = datagen.batch_specs(nq=400, budget_bytes=64 << 20, min_rows=1000, seed_col=1)
+    queries = [datagen.batch_query(s) for s in specs]
+    b, _ = to_batch(ctx, queries)
+    b.launch_graph()
+    ctx.check()
+    check_against_oracle(b, queries)
+    b.close()
+
+
+def test_edge_batches(ctx):
+    # all queries empty
+    b, _ = to_batch(ctx, make_queries([(0, np.int32, 1), (0, np.int64, 1)]))
+    b.launch()
+    ctx.check()
+    assert b.result(0).n_groups == 0 and b.result(1).n_groups == 0
+    b.close()
+    # one row; all rows one key; a single query of exactly the one-CTA limit
+    for spec in [(1, np.float64, 1), (50_000, np.int64, 1), (8192, np.int32, 8192)]:
+        queries = make_queries([spec])
+        for small in (0, 8192):
+            b, _ = to_batch(ctx, queries, dict(small_rows=small, small_bits=8, seg_variant=0))
+            b.launch()
+            ctx.check()
+            check_against_oracle(b, queries)
+            b.close()
+
+
+def test_batch_rejects_bad_tuning_and_arguments(ctx):
+    queries = make_queries([(10, np.int32, 3)])
+    with pytest.raises(vdf.VdfError):
+        to_batch(ctx, queries, dict(small_rows=10_000, small_bits=8, seg_variant=0))
+    with pytest.raises(vdf.VdfError):
+        to_batch(ctx, queries, dict(small_rows=0, small_bits=6, seg_variant=0))
+    with pytest.raises(vdf.VdfError):
+        to_batch(ctx, queries, dict(small_rows=0, small_bits=8, seg_variant=99))
+    k = dev(queries[0][0])
+    with pytest.raises(ValueError):
+        vdf.Batch(ctx, [(k, [dev(queries[0][1]), dev(queries[0][2].astype(np.float64))]),
+                        (k, [dev(queries[0][1]), dev(queries[0][2])])])

@@ -168,3 +168,30 @@ def test_autotune_picks_valid_variants(ctx):
         assert res["ms32"] and res["ms64"]
     finally:
         ctx.set_sort_tuning(*saved)
+
+
+@pytest.mark.parametrize("order", [ob.ASC, ob.DESC_STABLE, ob.DESC_REVERSE])
+def test_eleven_bit_digits_with_every_key_type(ctx, order):
+    """Plans whose passes use 11-bit digits for one or both key widths
+    (3 passes per 4-byte key, 6 per 8-byte key) against the oracle, over
+    signed, unsigned and floating keys."""
+    variants = vdf._lib.sort_variants()
+    wide32 = [v["index"] for v in variants if v["key_width"] == 4 and v["digit_bits"] == 11]
+    wide64 = [v["index"] for v in variants if v["key_width"] == 8 and v["digit_bits"] == 11]
+    narrow32 = [v["index"] for v in variants if v["key_width"] == 4 and v["digit_bits"] == 8]
+    narrow64 = [v["index"] for v in variants if v["key_width"] == 8 and v["digit_bits"] == 8]
+    assert wide32 and wide64
+    rng = np.random.default_rng(1100 + order)
+    n = 2_000_003
+    keys = [datagen.keys_for("few", np.float64, n, rng), datagen.keys_for("zipf", np.int32, n, rng),
+            datagen.keys_for("uniform", np.uint64, n, rng), datagen.keys_for("uniform", np.float32, n, rng)]
+    exp = ob.argsort(keys, order)
+    saved = ctx.get_sort_tuning()
+    try:
+        for a, b in [(wide32[0], wide64[0]), (wide32[-1], wide64[-1]), (wide32[0], narrow64[0]),
+                     (narrow32[0], wide64[-1])]:
+            ctx.set_sort_tuning(a, b)
+            perm = ctx.argsort([dev(k) for k in keys], order=order)
+            assert (host(perm).view(np.uint32) == exp).all(), (a, b)
+    finally:
+        ctx.set_sort_tuning(*saved)

@@ -66,6 +66,26 @@ class vdf_sort_groupby_args(C.Structure):
     ]
 
 
+BATCH_MAX_VALS = 4
+
+
+class vdf_batch_query(C.Structure):
+    _fields_ = [("n", C.c_uint64), ("key", vdf_col), ("vals", C.c_void_p * BATCH_MAX_VALS)]
+
+
+class vdf_batch_tuning(C.Structure):
+    _fields_ = [("small_rows", C.c_uint32), ("small_bits", C.c_int32), ("seg_variant", C.c_int32)]
+
+
+class vdf_batch_args(C.Structure):
+    _fields_ = [
+        ("nqueries", C.c_uint32), ("queries", C.POINTER(vdf_batch_query)), ("nvals", C.c_int32),
+        ("val_dtypes", C.c_int32 * BATCH_MAX_VALS), ("perm_out", C.c_void_p), ("group_keys_out", C.c_void_p),
+        ("group_count_out", C.c_void_p), ("aggs", vdf_agg_out * BATCH_MAX_VALS), ("row_offset_out", C.c_void_p),
+        ("group_offset_out", C.c_void_p), ("n_groups_out", C.c_void_p),
+    ]
+
+
 def _load() -> C.CDLL:
     if not LIB_PATH.exists():
         raise ImportError(f"{LIB_PATH} is not built; run `python -m visondf_b200.build` (no CPU fallback exists)")
@@ -103,6 +123,16 @@ def _load() -> C.CDLL:
         "vdf_gather_host": (st, [vp, u64, vp, C.POINTER(vdf_col), i32, C.POINTER(vp), vp]),
         "vdf_transform_groupby_host": (st, [vp, u64, C.POINTER(vdf_col), i32, vdf_col, C.c_int32, vp, vp,
                                             C.POINTER(C.c_uint64), vp]),
+        "vdf_batch_variant_count": (i32, []),
+        "vdf_batch_variant_info": (st, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+        "vdf_batch_default_tuning": (st, [C.POINTER(vdf_batch_tuning)]),
+        "vdf_batch_create": (st, [vp, C.POINTER(vdf_batch_args), C.POINTER(vdf_batch_tuning), C.POINTER(vp)]),
+        "vdf_batch_rows": (u64, [vp]),
+        "vdf_batch_info": (st, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                C.POINTER(C.c_uint64)]),
+        "vdf_batch_launch": (st, [vp, vp]),
+        "vdf_batch_launch_graph": (st, [vp, vp]),
+        "vdf_batch_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -396,3 +426,142 @@ def header_functions() -> list[str]:
     text = HEADER_PATH.read_text()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     return sorted(set(re.findall(r"\b(vdf_[a-z0-9_]+)\s*\(", text)))
+
+
+def batch_variants() -> list:
+    """[{index, digit_bits, tile_rows}] of the segmented radix-pass variants."""
+    out = []
+    for i in range(lib.vdf_batch_variant_count()):
+        b, t = C.c_int32(), C.c_int32()
+        if lib.vdf_batch_variant_info(i, C.byref(b), C.byref(t)) == OK:
+            out.append(dict(index=i, digit_bits=b.value, tile_rows=t.value))
+    return out
+
+
+def default_batch_tuning() -> dict:
+    t = vdf_batch_tuning()
+    lib.vdf_batch_default_tuning(C.byref(t))
+    return dict(small_rows=t.small_rows, small_bits=t.small_bits, seg_variant=t.seg_variant)
+
+
+@dataclass
+class QueryResult:
+    """One query's results (device tensor views into the batch arenas)."""
+    perm: torch.Tensor
+    n_groups: int
+    keys: torch.Tensor
+    count: torch.Tensor
+    aggs: list
+
+
+class Batch:
+    """Many independent sort + group-by queries planned once (vdf_batch_*).
+
+    `queries` is a list of (key tensor, [value tensors]); every query has
+    the same value dtypes.  Outputs live in arenas owned by this object;
+    `result(q)` returns views of query q's part after a launch."""
+
+    def __init__(self, ctx: "Context", queries, tuning: Optional[dict] = None):
+        self.ctx = ctx
+        self.queries = [(k, list(vs)) for k, vs in queries]
+        nq = len(self.queries)
+        nvals = len(self.queries[0][1]) if nq else 0
+        if nvals > BATCH_MAX_VALS:
+            raise ValueError(f"at most {BATCH_MAX_VALS} value columns")
+        self.val_dtypes = [v.dtype for v in self.queries[0][1]] if nq else []
+        for k, vs in self.queries:
+            if [v.dtype for v in vs] != self.val_dtypes:
+                raise ValueError("every query must have the same value dtypes")
+        dev = torch.device("cuda", ctx.device)
+        self.n_total = sum(int(k.numel()) for k, _ in self.queries)
+        N = max(1, self.n_total)
+        self.perm = torch.empty(N, dtype=torch.int32, device=dev)
+        self.gkeys = torch.empty(N, dtype=torch.int64, device=dev)
+        self.count = torch.empty(N, dtype=torch.int64, device=dev)
+        self.aggs = []
+        structs = (vdf_agg_out * BATCH_MAX_VALS)()
+        for j, dt in enumerate(self.val_dtypes):
+            fl = dt in (torch.float64, torch.float32)
+            a = AggResult(torch.empty(N, dtype=torch.float64 if fl else torch.int64, device=dev),
+                          None if fl else torch.empty(N, dtype=torch.int64, device=dev),
+                          torch.empty(N, dtype=dt, device=dev), torch.empty(N, dtype=dt, device=dev),
+                          torch.empty(N, dtype=torch.float64, device=dev))
+            self.aggs.append(a)
+            structs[j] = vdf_agg_out(_ptr(a.sum), _ptr(a.sum_hi), _ptr(a.min), _ptr(a.max), _ptr(a.mean))
+        self.row_offset = torch.zeros(max(1, nq), dtype=torch.int64, device=dev)
+        self.group_offset = torch.zeros(max(1, nq), dtype=torch.int64, device=dev)
+        self.n_groups = torch.zeros(max(1, nq), dtype=torch.int64, device=dev)
+        qs = (vdf_batch_query * max(1, nq))()
+        for i, (k, vs) in enumerate(self.queries):
+            qs[i].n = k.numel()
+            qs[i].key = _col(k)
+            for j, v in enumerate(vs):
+                if not v.is_cuda or not v.is_contiguous() or v.numel() != k.numel():
+                    raise ValueError("value columns must be contiguous CUDA tensors of the key's length")
+                qs[i].vals[j] = v.data_ptr()
+        a = vdf_batch_args()
+        a.nqueries = nq
+        a.queries = qs
+        a.nvals = nvals
+        for j, dt in enumerate(self.val_dtypes):
+            a.val_dtypes[j] = TORCH_TO_VDF[dt]
+        a.perm_out = _ptr(self.perm)
+        a.group_keys_out = _ptr(self.gkeys)
+        a.group_count_out = _ptr(self.count)
+        a.aggs = structs
+        a.row_offset_out = _ptr(self.row_offset)
+        a.group_offset_out = _ptr(self.group_offset)
+        a.n_groups_out = _ptr(self.n_groups)
+        self._args = a
+        t = None
+        if tuning is not None:
+            t = vdf_batch_tuning(int(tuning["small_rows"]), int(tuning["small_bits"]), int(tuning["seg_variant"]))
+        h = C.c_void_p()
+        st = lib.vdf_batch_create(ctx.handle, C.byref(a), None if t is None else C.byref(t), C.byref(h))
+        ctx._check(st, "vdf_batch_create")
+        self.handle = h
+        self._host = None
+
+    def info(self) -> dict:
+        sq, lq = C.c_uint32(), C.c_uint32()
+        sr, lr = C.c_uint64(), C.c_uint64()
+        lib.vdf_batch_info(self.handle, C.byref(sq), C.byref(sr), C.byref(lq), C.byref(lr))
+        return dict(small_queries=sq.value, small_rows=sr.value, large_queries=lq.value, large_rows=lr.value,
+                    rows=lib.vdf_batch_rows(self.handle))
+
+    def launch(self, stream=None):
+        self._host = None
+        self.ctx._check(lib.vdf_batch_launch(self.handle, _stream(stream)), "vdf_batch_launch")
+
+    def launch_graph(self, stream=None):
+        self._host = None
+        self.ctx._check(lib.vdf_batch_launch_graph(self.handle, _stream(stream)), "vdf_batch_launch_graph")
+
+    def _offsets(self):
+        if self._host is None:
+            self._host = (self.row_offset.cpu().tolist(), self.group_offset.cpu().tolist(),
+                          self.n_groups.cpu().tolist())
+        return self._host
+
+    def result(self, q: int) -> QueryResult:
+        ro, go, ng = self._offsets()
+        k = self.queries[q][0]
+        n = k.numel()
+        G = int(ng[q])
+        r0, g0 = int(ro[q]), int(go[q])
+        kb = self.gkeys.view(torch.uint8)[8 * g0: 8 * g0 + k.element_size() * G]
+        keys = kb.view(k.dtype) if G else torch.empty(0, dtype=k.dtype, device=k.device)
+        aggs = [AggResult(a.sum[g0:g0 + G], None if a.sum_hi is None else a.sum_hi[g0:g0 + G], a.min[g0:g0 + G],
+                          a.max[g0:g0 + G], a.mean[g0:g0 + G]) for a in self.aggs]
+        return QueryResult(self.perm[r0:r0 + n], G, keys, self.count[g0:g0 + G], aggs)
+
+    def close(self):
+        if getattr(self, "handle", None):
+            lib.vdf_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -9,7 +9,9 @@ count), so a serving loop can keep one choice per class.
 
 Timing uses the library's per-launch CUDA-event profiler (vdf_ctx_profile),
 so the 4-byte-key and 8-byte-key passes of one run are measured separately
-and each width is tuned independently.
+and each width is tuned independently.  Variants differ in digit width (8 or
+11 bits: 4 or 3 passes over a 4-byte key, 8 or 6 over an 8-byte key), so the
+figure compared is the time of all of a width's passes in one run.
 """
 from __future__ import annotations
 
@@ -49,8 +51,9 @@ class TuningTable:
 def tune(ctx: "_lib.Context", run: Callable[[], None], reps: int = 2) -> dict:
     """Times `run` (one sort or sort + group-by on the context) under every
     variant assignment and returns {"variant32": i, "variant64": j,
-    "ms32": {i: ms per pass}, "ms64": {j: ms per pass}}; leaves the best
-    tuning set on the context."""
+    "ms32": {i: ms per run}, "ms64": {j: ms per run}} (time of all radix
+    passes over keys of that width in one run); leaves the best tuning set on
+    the context."""
     variants = _lib.sort_variants()
     v32 = [v["index"] for v in variants if v["key_width"] == 4]
     v64 = [v["index"] for v in variants if v["key_width"] == 8]
@@ -69,9 +72,9 @@ def tune(ctx: "_lib.Context", run: Callable[[], None], reps: int = 2) -> dict:
         t32, c32 = prof["onesweep32"]
         t64, c64 = prof["onesweep64"]
         if c32:
-            ms32[a] = min(ms32.get(a, math.inf), t32 / c32)
+            ms32[a] = min(ms32.get(a, math.inf), t32 / reps)
         if c64:
-            ms64[b] = min(ms64.get(b, math.inf), t64 / c64)
+            ms64[b] = min(ms64.get(b, math.inf), t64 / reps)
     cur = ctx.get_sort_tuning()
     best32 = min(ms32, key=ms32.get) if ms32 else cur[0]
     best64 = min(ms64, key=ms64.get) if ms64 else cur[1]

@@ -27,19 +27,43 @@ struct Profiler {
 // ---- radix sort ------------------------------------------------------------
 enum InMode : int { IN_RAW = 0, IN_GATHER = 1, IN_BUF = 2 };
 
+constexpr int kMaxBits = 11;                  // widest radix digit compiled
+constexpr int kMaxRadix = 1 << kMaxBits;
+constexpr int kMaxPasses = kMaxKeys * 8;      // 8-bit digits over four 8-byte keys
+
 struct HistCol {
     const void* data;
     int dtype;
     int passes;
-    int pass_base;
+    int bits;       // digit width of this column's passes
+    int hist_off;   // word offset of its first pass's histogram
     int invert;
 };
 struct HistArgs {
     HistCol col[kMaxKeys];
     int ncols;
-    int total_passes;
+    int hist_words;
     uint64_t n;
     uint32_t* hist;
+};
+// Histograms of every pass laid out back to back: pass g has radix[g] bins
+// starting at word off[g]; the scan writes exclusive starts at the same words.
+struct ScanArgs {
+    const uint32_t* hist;
+    uint32_t* offs;
+    uint32_t off[kMaxPasses];
+    uint32_t radix[kMaxPasses];
+};
+
+// One segment of a segmented sort: rows [row_start, row_start + rows) of the
+// arena, tiles [first_tile, first_tile + ceil(rows / tile)), sorted in
+// `passes` digit passes.
+struct SegDesc {
+    uint64_t row_start;
+    uint32_t rows;
+    uint32_t first_tile;
+    uint32_t passes;
+    uint32_t pad;
 };
 
 struct PassArgs {
@@ -55,9 +79,18 @@ struct PassArgs {
     uint64_t n;
     uint32_t shift;
     uint32_t status_rows;       // rows of status_next to clear
+    uint32_t status_row_words;  // words per status row (the plan's widest radix)
     int dtype;
     int invert;                 // stable descending: keys bit-inverted
     int reverse;                // reference descending: output positions mirrored
+    // segmented sorts only
+    const uint32_t* tile_seg;   // [tiles] segment of each tile
+    const SegDesc* segs;        // [segments]
+    const uint32_t* seg_offs;   // [segments][seg_stride]: per pass, exclusive digit starts in the segment
+    uint32_t seg_stride;        // words per segment in seg_offs (max passes x radix)
+    uint32_t pass;              // digit pass index
+    void* keys_final;           // where a segment's last pass writes its keys
+    uint32_t* vals_final;       // ... and its row ids
 };
 
 // Kernel-variant choice of the radix pass per key width (indices into the
@@ -75,9 +108,9 @@ struct SortPlan {
     uint64_t n;
     SortTuning tuning;
     int nkeys;
-    int bits, radix;
     int dtype[kMaxKeys], width[kMaxKeys], passes[kMaxKeys], pass_base[kMaxKeys];
-    int total_passes;
+    int bits[kMaxKeys], radix[kMaxKeys], hist_off[kMaxKeys];
+    int total_passes, hist_words, max_radix;
     uint32_t max_tiles;
     size_t off_keys[2], off_vals[2], off_offs, off_zero, off_hist, off_counters, off_status[2];
     size_t zero_bytes;
@@ -93,6 +126,35 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
                      void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof = nullptr,
                      const uint32_t* perm_in = nullptr);
 cudaError_t prepare_sort_kernels();
+
+// ---- segmented sort (many independent row ranges in one set of launches) ----
+// Keys are ordered 8-byte images (the batch packs them so); a segment whose
+// keys were 4 bytes wide has zero high halves and needs fewer passes.
+struct SegChunk {      // a histogram CTA's rows: part of one segment
+    uint64_t row_start;
+    uint32_t rows;
+    uint32_t seg;
+};
+struct SegSortArgs {
+    uint64_t n;                   // arena rows (< 2^30)
+    const uint64_t* keys;         // [n] ordered keys
+    const SegDesc* segs;          // device [nsegs]
+    uint32_t nsegs;
+    const uint32_t* tile_seg;     // device [ntiles]; segments with more passes first
+    uint32_t ntiles;
+    const SegChunk* chunks;       // device [nchunks]
+    uint32_t nchunks;
+    int max_passes;
+    uint32_t tiles_in_pass[16];   // launch width of pass g: tiles of segments with passes > g
+    int variant;                  // index into the segmented variant table
+    uint64_t* keys_out;           // [n] sorted ordered keys (each segment in place)
+    uint32_t* perm_out;           // [n] arena row ids in sorted order
+    uint32_t* err;
+};
+int seg_sort_variant_count();
+bool seg_sort_variant_info(int v, int* bits, int* tile_rows);
+size_t seg_sort_workspace_bytes(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes, int variant);
+cudaError_t run_seg_sort(const SegSortArgs& a, unsigned char* ws, cudaStream_t s, Profiler* prof = nullptr);
 
 // ---- gather ----------------------------------------------------------------
 struct GatherArgs {

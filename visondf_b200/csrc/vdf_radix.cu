@@ -30,27 +30,27 @@ namespace vdf {
 // ---------------------------------------------------------------------------
 // 1. all-digit histogram
 // ---------------------------------------------------------------------------
-template <int BITS>
+// Digit widths are per column (8 or 11 bits), so the shifts and masks are
+// runtime values; the histograms of all passes sit back to back in shared
+// memory.
 __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
-    constexpr int RADIX = 1 << BITS;
-    constexpr uint32_t MASK = RADIX - 1;
-    extern __shared__ uint32_t sh_hist[];  // [total_passes][RADIX]
-    const int total = a.total_passes * RADIX;
-    for (int i = threadIdx.x; i < total; i += blockDim.x) sh_hist[i] = 0;
+    extern __shared__ uint32_t sh_hist[];  // [hist_words]
+    for (int i = threadIdx.x; i < a.hist_words; i += blockDim.x) sh_hist[i] = 0;
     __syncthreads();
 
     const uint64_t n = a.n;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (int c = 0; c < a.ncols; ++c) {
         const HistCol col = a.col[c];
-        uint32_t* h = sh_hist + col.pass_base * RADIX;
+        uint32_t* h = sh_hist + col.hist_off;
         const int w = dtype_width(col.dtype);
+        const uint32_t bits = (uint32_t)col.bits, radix = 1u << bits, mask = radix - 1;
         if (w == 4) {
             const uint32_t* src = static_cast<const uint32_t*>(col.data);
             for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
                 uint32_t k = order32(ldg_stream(src + i), col.dtype, col.invert);
 #pragma unroll 4
-                for (int p = 0; p < col.passes; ++p) atomicAdd(&h[p * RADIX + ((k >> (p * BITS)) & MASK)], 1u);
+                for (int p = 0; p < col.passes; ++p) atomicAdd(&h[p * radix + ((k >> (p * bits)) & mask)], 1u);
             }
         } else {
             const uint64_t* src = static_cast<const uint64_t*>(col.data);
@@ -58,12 +58,12 @@ __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
                 uint64_t k = order64(ldg_stream(src + i), col.dtype, col.invert);
 #pragma unroll 8
                 for (int p = 0; p < col.passes; ++p)
-                    atomicAdd(&h[p * RADIX + (uint32_t)((k >> (p * BITS)) & MASK)], 1u);
+                    atomicAdd(&h[p * radix + (uint32_t)((k >> (p * bits)) & mask)], 1u);
             }
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < total; i += blockDim.x) {
+    for (int i = threadIdx.x; i < a.hist_words; i += blockDim.x) {
         uint32_t v = sh_hist[i];
         if (v) atomicAdd(&a.hist[i], v);
     }
@@ -72,19 +72,18 @@ __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
 // ---------------------------------------------------------------------------
 // 2. exclusive scan of each digit position's histogram (one CTA per position)
 // ---------------------------------------------------------------------------
-template <int BITS>
-__global__ void __launch_bounds__(256) k_hist_scan(const uint32_t* hist, uint32_t* offs) {
-    constexpr int RADIX = 1 << BITS;
-    constexpr int PER = (RADIX + 255) / 256;
+__global__ void __launch_bounds__(256) k_hist_scan(ScanArgs a) {
+    constexpr int PER = kMaxRadix / 256;
     __shared__ uint32_t warp_tot[8];
-    const uint32_t* h = hist + (size_t)blockIdx.x * RADIX;
-    uint32_t* o = offs + (size_t)blockIdx.x * RADIX;
+    const uint32_t radix = a.radix[blockIdx.x];
+    const uint32_t* h = a.hist + a.off[blockIdx.x];
+    uint32_t* o = a.offs + a.off[blockIdx.x];
     uint32_t v[PER];
     uint32_t sum = 0;
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-        int b = threadIdx.x * PER + j;
-        v[j] = b < RADIX ? h[b] : 0;
+        uint32_t b = threadIdx.x * PER + j;
+        v[j] = b < radix ? h[b] : 0;
         sum += v[j];
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -101,8 +100,78 @@ __global__ void __launch_bounds__(256) k_hist_scan(const uint32_t* hist, uint32_
     uint32_t run = wbase + incl - sum;
 #pragma unroll
     for (int j = 0; j < PER; ++j) {
-        int b = threadIdx.x * PER + j;
-        if (b < RADIX) o[b] = run;
+        uint32_t b = threadIdx.x * PER + j;
+        if (b < radix) o[b] = run;
+        run += v[j];
+    }
+}
+
+// Segmented histograms: one CTA per chunk of one segment, all of that
+// segment's passes at once, flushed into the segment's own rows
+// [seg][pass][radix] of the global histogram.
+struct SegHistArgs {
+    const uint64_t* keys;
+    const SegChunk* chunks;
+    const SegDesc* segs;
+    uint32_t* hist;
+    uint32_t stride;   // words per segment
+    uint32_t bits;
+    uint32_t nsegs;
+    uint64_t n;
+};
+__global__ void __launch_bounds__(512) k_seg_hist(SegHistArgs a) {
+    extern __shared__ uint32_t sh_hist[];
+    const SegChunk ch = a.chunks[blockIdx.x];
+    if (ch.seg >= a.nsegs || ch.row_start + ch.rows > a.n) return;  // host-built tables are consistent
+    const uint32_t passes = a.segs[ch.seg].passes;
+    const uint32_t radix = 1u << a.bits, mask = radix - 1;
+    const uint32_t words = passes * radix;
+    if (words > a.stride) return;
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) sh_hist[i] = 0;
+    __syncthreads();
+    for (uint32_t r = threadIdx.x; r < ch.rows; r += blockDim.x) {
+        const uint64_t k = ldg_stream(a.keys + ch.row_start + r);
+        for (uint32_t p = 0; p < passes; ++p)
+            atomicAdd(&sh_hist[p * radix + (uint32_t)((k >> (p * a.bits)) & mask)], 1u);
+    }
+    __syncthreads();
+    uint32_t* g = a.hist + (size_t)ch.seg * a.stride;
+    for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) {
+        const uint32_t v = sh_hist[i];
+        if (v) atomicAdd(&g[i], v);
+    }
+}
+
+// Exclusive scan of consecutive rows of `radix` words, one CTA per row.
+__global__ void __launch_bounds__(256) k_row_scan(const uint32_t* hist, uint32_t* offs, uint32_t radix) {
+    constexpr int PER = kMaxRadix / 256;
+    __shared__ uint32_t warp_tot[8];
+    const uint32_t* h = hist + (size_t)blockIdx.x * radix;
+    uint32_t* o = offs + (size_t)blockIdx.x * radix;
+    uint32_t v[PER];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        uint32_t b = threadIdx.x * PER + j;
+        v[j] = b < radix ? h[b] : 0;
+        sum += v[j];
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    uint32_t wbase = 0;
+    for (int w = 0; w < warp; ++w) wbase += warp_tot[w];
+    uint32_t run = wbase + incl - sum;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+        uint32_t b = threadIdx.x * PER + j;
+        if (b < radix) o[b] = run;
         run += v[j];
     }
 }
@@ -133,7 +202,13 @@ struct OnesweepCfg {
 // 0 = one ballot per digit bit (ALU/vote pipes), 1 = match.any (XU pipe),
 // 2 = alternate the two by item, so both pipes work at once.
 // MINB: CTAs per SM the register allocation is sized for.
-template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL, int MATCH, int MINB>
+// SEG: segmented sort of many independent row ranges (the queries of a
+// batch) in one launch.  Tiles never straddle a segment; a tile's bin bases
+// come from its segment's own histogram, its look-back stops at the
+// segment's first tile, and each segment has its own number of passes (the
+// last one writes to the final buffers, later passes skip its tiles).
+template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL, int MATCH, int MINB,
+          bool SEG = false>
 __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     using C = OnesweepCfg<K, BITS, THREADS, ITEMS>;
     constexpr int RADIX = C::RADIX, WARPS = C::WARPS, TILE = C::TILE, BPT = C::BPT;
@@ -152,8 +227,29 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     __syncthreads();
     const uint32_t tile = misc[0];
     const uint64_t n = a.n;
-    const uint64_t tile_base = (uint64_t)tile * TILE;
-    const uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tile_base);
+    uint64_t tile_base = (uint64_t)tile * TILE;
+    uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tile_base);
+    uint32_t first_tile = 0;   // look-back stops here
+    uint32_t seg = 0;
+    bool fin = FINAL;
+    if constexpr (SEG) {
+        valid = 0;
+        if (tile < a.status_rows) {
+            seg = a.tile_seg[tile];
+            const SegDesc sd = a.segs[seg];
+            if (tile < sd.first_tile || sd.row_start + sd.rows > n ||
+                (uint64_t)(tile - sd.first_tile) * TILE >= sd.rows) {
+                if (tid == 0) atomicOr(a.err, ERR_BAD_INDEX);  // inconsistent tile table
+            } else if (a.pass < sd.passes) {
+                first_tile = sd.first_tile;
+                tile_base = sd.row_start + (uint64_t)(tile - sd.first_tile) * TILE;
+                valid = (uint32_t)min((uint64_t)TILE, sd.row_start + sd.rows - tile_base);
+                fin = (a.pass + 1 == sd.passes);
+            }
+        } else if (tid == 0) {
+            atomicOr(a.err, ERR_BAD_INDEX);
+        }
+    }
 
     // ---- load keys and row ids (warp-striped: item j of lane l is tile
     //      position warp*ITEMS*32 + j*32 + l, so positions follow row order) --
@@ -191,7 +287,9 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     // more tiles could read is cleared too.
     if (a.status_next)
         for (uint32_t r = tile; r < a.status_rows; r += gridDim.x)
-            for (int b = tid; b < RADIX; b += THREADS) a.status_next[(size_t)r * RADIX + b] = 0;
+            for (uint32_t b = tid; b < a.status_row_words; b += THREADS)
+                a.status_next[(size_t)r * a.status_row_words + b] = 0;
+    if (SEG && valid == 0) return;  // segment finished in an earlier pass
 
     // ---- warp-local ranks and per-warp digit counts --------------------------
     // First the lanes holding the same digit are found for every item (one
@@ -253,7 +351,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
                 run += c;
             }
             uint32_t* st = a.status + (size_t)tile * RADIX + b;
-            st_relaxed_u32(st, (tile == 0 ? ST_INC : ST_AGG) | run);
+            st_relaxed_u32(st, (tile == first_tile ? ST_INC : ST_AGG) | run);
         }
         tot[k] = run;
         tsum += run;
@@ -304,26 +402,38 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     // ---- decoupled look-back per bin ---------------------------------------
     // Each bin's thread reads the status words of LB predecessors at once (one
     // round trip per window), adds counts from the nearest one backwards and
-    // stops at the first inclusive prefix.
-    constexpr int LB = 8;
+    // stops at the first inclusive prefix.  A thread owning several bins (wide
+    // digits) issues the windows of all its unfinished bins together.
+    constexpr int LB = (BPT >= 8) ? 2 : (BPT >= 4 ? 4 : 8);
+    {
+        uint32_t excl[BPT];
+        bool done[BPT];
 #pragma unroll
-    for (int k = 0; k < BPT; ++k) {
-        const int b = tid * BPT + k;
-        if (b >= RADIX) break;
-        uint32_t excl = 0;
-        if (tile > 0) {
-            int64_t p = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            bool done = false;
-            while (!done) {
-                uint32_t sw[LB];
+        for (int k = 0; k < BPT; ++k) {
+            excl[k] = 0;
+            done[k] = (tile == first_tile) || (tid * BPT + k >= RADIX);
+        }
+        const int64_t lo = first_tile;
+        int64_t p = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        bool all_done = false;
+        while (!all_done) {
+            uint32_t sw[BPT][LB];
+#pragma unroll
+            for (int k = 0; k < BPT; ++k)
 #pragma unroll
                 for (int w = 0; w < LB; ++w)
-                    sw[w] = (p - w >= 0) ? ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b) : ST_INC;
+                    sw[k][w] = (!done[k] && p - w >= lo)
+                                   ? ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + tid * BPT + k)
+                                   : ST_INC;
+            all_done = true;
+#pragma unroll
+            for (int k = 0; k < BPT; ++k) {
+                if (done[k]) continue;
 #pragma unroll
                 for (int w = 0; w < LB; ++w) {
-                    if (done) break;
-                    uint32_t st = sw[w];
+                    if (done[k]) break;
+                    uint32_t st = sw[k][w];
                     while ((st & ~ST_CNT) == 0) {  // not yet published: wait for this one
                         if (++spins > kSpinLimit) {
                             atomicOr(a.err, ERR_LOOKBACK_TIMEOUT);
@@ -331,22 +441,34 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
                             break;
                         }
                         backoff(spins);
-                        st = ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b);
+                        st = ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + tid * BPT + k);
                     }
-                    excl += st & ST_CNT;
-                    if (st & ST_INC) done = true;
+                    excl[k] += st & ST_CNT;
+                    if (st & ST_INC) done[k] = true;
                 }
-                p -= LB;
-                if (p < 0) done = true;
+                if (p - LB < lo) done[k] = true;
+                all_done = all_done && done[k];
             }
-            st_relaxed_u32(a.status + (size_t)tile * RADIX + b, ST_INC | (excl + tot[k]));
+            p -= LB;
         }
-        bglob[b] = a.bin_offsets[b] + excl - bstart[k];
+#pragma unroll
+        for (int k = 0; k < BPT; ++k) {
+            const int b = tid * BPT + k;
+            if (b >= RADIX) break;
+            if (tile > first_tile) st_relaxed_u32(a.status + (size_t)tile * RADIX + b, ST_INC | (excl[k] + tot[k]));
+            uint32_t base;
+            if constexpr (SEG)
+                base = (uint32_t)a.segs[seg].row_start + a.seg_offs[(size_t)seg * a.seg_stride + a.pass * RADIX + b];
+            else
+                base = a.bin_offsets[b];
+            bglob[b] = base + excl[k] - bstart[k];
+        }
     }
     __syncthreads();
 
     // ---- run-coalesced writes of keys and row ids ----------------------------
-    K* kout = static_cast<K*>(a.keys_out);
+    K* kout = static_cast<K*>((SEG && fin) ? a.keys_final : a.keys_out);
+    uint32_t* vout = (SEG && fin) ? a.vals_final : a.vals_out;
 #pragma unroll
     for (int r = 0; r < ITEMS; ++r) {
         const uint32_t i = r * THREADS + tid;
@@ -359,13 +481,13 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
                 atomicOr(a.err, ERR_BAD_INDEX);
                 continue;
             }
-            if (FINAL && a.reverse) p = (uint32_t)(n - 1) - p;
-            if (FINAL) {
+            if (fin && a.reverse) p = (uint32_t)(n - 1) - p;
+            if (fin) {
                 if (kout) stg_stream(kout + p, KeyOps<K>::unorder(k, a.dtype, a.invert));
             } else {
                 stg_stream(kout + p, k);
             }
-            stg_stream(a.vals_out + p, v);
+            stg_stream(vout + p, v);
         }
     }
 }
@@ -374,8 +496,6 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
 // host side
 // ---------------------------------------------------------------------------
 namespace {
-constexpr int kBits = 8;
-
 using PassKernel = void (*)(PassArgs);
 
 // One compiled configuration of the radix pass.  The variant table is the
@@ -386,44 +506,76 @@ struct PassVariant {
     PassKernel k[3][2];  // [IN_MODE][FINAL]
 };
 
-template <typename K, int THREADS, int ITEMS, int MATCH, int MINB>
+template <typename K, int BITS, int THREADS, int ITEMS, int MATCH, int MINB>
 PassVariant make_variant() {
-    using C = OnesweepCfg<K, kBits, THREADS, ITEMS>;
+    using C = OnesweepCfg<K, BITS, THREADS, ITEMS>;
+    static_assert(BITS <= kMaxBits, "digit wider than the histogram layout allows");
     PassVariant v{};
     v.width = (int)sizeof(K);
     v.threads = THREADS;
     v.items = ITEMS;
-    v.bits = kBits;
+    v.bits = BITS;
     v.match = MATCH;
     v.minb = MINB;
     v.smem = C::SMEM;
-    v.k[IN_RAW][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_RAW, false, MATCH, MINB>;
-    v.k[IN_GATHER][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_GATHER, false, MATCH, MINB>;
-    v.k[IN_BUF][0] = k_onesweep<K, kBits, THREADS, ITEMS, IN_BUF, false, MATCH, MINB>;
-    v.k[IN_RAW][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_RAW, true, MATCH, MINB>;
-    v.k[IN_GATHER][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_GATHER, true, MATCH, MINB>;
-    v.k[IN_BUF][1] = k_onesweep<K, kBits, THREADS, ITEMS, IN_BUF, true, MATCH, MINB>;
+    v.k[IN_RAW][0] = k_onesweep<K, BITS, THREADS, ITEMS, IN_RAW, false, MATCH, MINB>;
+    v.k[IN_GATHER][0] = k_onesweep<K, BITS, THREADS, ITEMS, IN_GATHER, false, MATCH, MINB>;
+    v.k[IN_BUF][0] = k_onesweep<K, BITS, THREADS, ITEMS, IN_BUF, false, MATCH, MINB>;
+    v.k[IN_RAW][1] = k_onesweep<K, BITS, THREADS, ITEMS, IN_RAW, true, MATCH, MINB>;
+    v.k[IN_GATHER][1] = k_onesweep<K, BITS, THREADS, ITEMS, IN_GATHER, true, MATCH, MINB>;
+    v.k[IN_BUF][1] = k_onesweep<K, BITS, THREADS, ITEMS, IN_BUF, true, MATCH, MINB>;
     return v;
 }
 
-// key width, threads per CTA, keys per thread, match method, CTAs per SM
+// key type, digit bits, threads per CTA, keys per thread, match method, CTAs per SM
 const PassVariant kVariants[] = {
-    make_variant<uint32_t, 256, 16, 0, 3>(),  // 0
-    make_variant<uint32_t, 256, 16, 1, 3>(),  // 1
-    make_variant<uint64_t, 256, 12, 0, 3>(),  // 2
-    make_variant<uint64_t, 256, 12, 1, 3>(),  // 3
-    make_variant<uint32_t, 256, 16, 1, 2>(),  // 4
-    make_variant<uint64_t, 256, 12, 0, 2>(),  // 5
-    make_variant<uint32_t, 256, 12, 1, 4>(),  // 6
-    make_variant<uint64_t, 256, 8, 0, 4>(),   // 7
-    make_variant<uint64_t, 256, 16, 0, 2>(),  // 8
-    make_variant<uint32_t, 256, 24, 1, 2>(),  // 9
-    make_variant<uint32_t, 256, 12, 2, 4>(),  // 10
-    make_variant<uint64_t, 256, 12, 2, 3>(),  // 11
-    make_variant<uint64_t, 256, 8, 2, 4>(),   // 12
-    make_variant<uint32_t, 256, 16, 2, 3>(),  // 13
+    make_variant<uint32_t, 8, 256, 16, 0, 3>(),  // 0
+    make_variant<uint32_t, 8, 256, 16, 1, 3>(),  // 1
+    make_variant<uint64_t, 8, 256, 12, 0, 3>(),  // 2
+    make_variant<uint64_t, 8, 256, 12, 1, 3>(),  // 3
+    make_variant<uint32_t, 8, 256, 16, 1, 2>(),  // 4
+    make_variant<uint64_t, 8, 256, 12, 0, 2>(),  // 5
+    make_variant<uint32_t, 8, 256, 12, 1, 4>(),  // 6
+    make_variant<uint64_t, 8, 256, 8, 0, 4>(),   // 7
+    make_variant<uint64_t, 8, 256, 16, 0, 2>(),  // 8
+    make_variant<uint32_t, 8, 256, 24, 1, 2>(),  // 9
+    make_variant<uint32_t, 8, 256, 12, 2, 4>(),  // 10
+    make_variant<uint64_t, 8, 256, 12, 2, 3>(),  // 11
+    make_variant<uint64_t, 8, 256, 8, 2, 4>(),   // 12
+    make_variant<uint32_t, 8, 256, 16, 2, 3>(),  // 13
+    // 11-bit digits: 3 passes for a 4-byte key, 6 for an 8-byte key
+    make_variant<uint32_t, 11, 256, 16, 1, 2>(),  // 14
+    make_variant<uint64_t, 11, 256, 8, 1, 2>(),   // 15
+    make_variant<uint32_t, 11, 256, 16, 2, 2>(),  // 16
+    make_variant<uint64_t, 11, 256, 12, 2, 2>(),  // 17
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
+
+// Segmented sorts run over ordered 8-byte keys; [0] = first pass (arena
+// rows), [1] = later passes (ping-pong buffers).
+struct SegVariant {
+    int bits, tile;
+    size_t smem;
+    PassKernel k[2];
+};
+template <int BITS, int THREADS, int ITEMS, int MATCH, int MINB>
+SegVariant make_seg_variant() {
+    using C = OnesweepCfg<uint64_t, BITS, THREADS, ITEMS>;
+    SegVariant v{};
+    v.bits = BITS;
+    v.tile = THREADS * ITEMS;
+    v.smem = C::SMEM;
+    v.k[0] = k_onesweep<uint64_t, BITS, THREADS, ITEMS, IN_RAW, false, MATCH, MINB, true>;
+    v.k[1] = k_onesweep<uint64_t, BITS, THREADS, ITEMS, IN_BUF, false, MATCH, MINB, true>;
+    return v;
+}
+const SegVariant kSegVariants[] = {
+    make_seg_variant<8, 256, 8, 2, 4>(),    // 0
+    make_seg_variant<8, 256, 12, 2, 2>(),   // 1
+    make_seg_variant<8, 256, 16, 0, 2>(),   // 2
+    make_seg_variant<11, 256, 8, 1, 2>(),   // 3
+};
+constexpr int kNumSegVariants = (int)(sizeof(kSegVariants) / sizeof(kSegVariants[0]));
 
 const PassVariant& variant_for(const SortTuning& t, int width) {
     const int v = (width == 4) ? t.variant32 : t.variant64;
@@ -463,41 +615,48 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
     p.n = n;
     p.nkeys = nkeys;
     p.tuning = tuning;
-    p.bits = kBits;
-    p.radix = 1 << kBits;
     int maxw = 4;
-    int total = 0;
     uint32_t max_tiles = 0;
+    p.max_radix = 0;
     for (int k = 0; k < nkeys; ++k) {
         p.dtype[k] = dtypes[k];
         p.width[k] = dtype_width(dtypes[k]);
-        p.passes[k] = (p.width[k] * 8 + kBits - 1) / kBits;
+        p.bits[k] = variant_for(tuning, p.width[k]).bits;
+        p.radix[k] = 1 << p.bits[k];
+        p.passes[k] = (p.width[k] * 8 + p.bits[k] - 1) / p.bits[k];
         if (p.width[k] > maxw) maxw = p.width[k];
+        if (p.radix[k] > p.max_radix) p.max_radix = p.radix[k];
         const int rows = tile_rows(tuning, p.width[k]);
         uint32_t t = (uint32_t)((n + rows - 1) / rows);
         if (t > max_tiles) max_tiles = t;
     }
-    // passes are numbered in processing order (least-significant key first)
+    // passes are numbered in processing order (least-significant key first);
+    // their histograms follow one another in that order
+    int total = 0, words = 0;
     for (int k = nkeys - 1; k >= 0; --k) {
         p.pass_base[k] = total;
+        p.hist_off[k] = words;
         total += p.passes[k];
+        words += p.passes[k] * p.radix[k];
     }
     p.total_passes = total;
+    p.hist_words = words;
     p.max_tiles = max_tiles;
     size_t off = 0;
     const size_t A = 256;
+    const size_t status_bytes = (size_t)max_tiles * p.max_radix * 4;
     p.off_keys[0] = off; off = align_up(off + n * (size_t)maxw, A);
     p.off_keys[1] = off; off = align_up(off + n * (size_t)maxw, A);
     p.off_vals[0] = off; off = align_up(off + n * 4, A);
     p.off_vals[1] = off; off = align_up(off + n * 4, A);
-    p.off_offs = off; off = align_up(off + (size_t)total * p.radix * 4, A);
+    p.off_offs = off; off = align_up(off + (size_t)words * 4, A);
     // zeroed region: hist | counters+err | status[0]
     p.off_zero = off;
-    p.off_hist = off; off = align_up(off + (size_t)total * p.radix * 4, A);
+    p.off_hist = off; off = align_up(off + (size_t)words * 4, A);
     p.off_counters = off; off = align_up(off + (size_t)(total + 1) * 4, A);
-    p.off_status[0] = off; off = align_up(off + (size_t)max_tiles * p.radix * 4, A);
+    p.off_status[0] = off; off = align_up(off + status_bytes, A);
     p.zero_bytes = off - p.off_zero;
-    p.off_status[1] = off; off = align_up(off + (size_t)max_tiles * p.radix * 4, A);
+    p.off_status[1] = off; off = align_up(off + status_bytes, A);
     p.ws_bytes = off;
     return p;
 }
@@ -524,16 +683,24 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
     h.n = n;
     h.hist = hist;
     h.ncols = p.nkeys;
-    h.total_passes = p.total_passes;
+    h.hist_words = p.hist_words;
+    ScanArgs sc{};
+    sc.hist = hist;
+    sc.offs = offs;
     for (int k = 0; k < p.nkeys; ++k) {
         h.col[k].data = key_cols[k];
         h.col[k].dtype = p.dtype[k];
         h.col[k].passes = p.passes[k];
-        h.col[k].pass_base = p.pass_base[k];
+        h.col[k].bits = p.bits[k];
+        h.col[k].hist_off = p.hist_off[k];
         h.col[k].invert = invert;
+        for (int q = 0; q < p.passes[k]; ++q) {
+            sc.off[p.pass_base[k] + q] = (uint32_t)(p.hist_off[k] + q * p.radix[k]);
+            sc.radix[p.pass_base[k] + q] = (uint32_t)p.radix[k];
+        }
     }
     {
-        size_t smem = (size_t)p.total_passes * p.radix * 4;
+        size_t smem = (size_t)p.hist_words * 4;
         int dev = 0, sms = 148;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -541,11 +708,11 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
         uint32_t grid = (uint32_t)(want < (uint64_t)sms * 4 ? want : (uint64_t)sms * 4);
         if (grid == 0) grid = 1;
         if (prof) prof->begin(KC_HIST, s);
-        k_digit_hist<kBits><<<grid, 512, smem, s>>>(h);
+        k_digit_hist<<<grid, 512, smem, s>>>(h);
         if (prof) prof->end(KC_HIST, s);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if (prof) prof->begin(KC_SCAN, s);
-        k_hist_scan<kBits><<<p.total_passes, 256, 0, s>>>(hist, offs);
+        k_hist_scan<<<p.total_passes, 256, 0, s>>>(sc);
         if (prof) prof->end(KC_SCAN, s);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
@@ -559,14 +726,15 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
         for (int q = 0; q < p.passes[k]; ++q, ++g) {
             PassArgs a{};
             a.n = n;
-            a.shift = (uint32_t)(q * p.bits);
+            a.shift = (uint32_t)(q * p.bits[k]);
             a.dtype = p.dtype[k];
             a.invert = invert;
             a.reverse = reverse;
-            a.bin_offsets = offs + (size_t)g * p.radix;
+            a.bin_offsets = offs + p.hist_off[k] + (size_t)q * p.radix[k];
             a.status = status[g & 1];
             a.status_next = (g + 1 < p.total_passes) ? status[(g + 1) & 1] : nullptr;
             a.status_rows = p.max_tiles;
+            a.status_row_words = (uint32_t)p.max_radix;
             a.tile_counter = counters + g;
             a.err = err;
             int mode;
@@ -607,6 +775,110 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
     return cudaSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// segmented sort (host side)
+// ---------------------------------------------------------------------------
+int seg_sort_variant_count() { return kNumSegVariants; }
+
+bool seg_sort_variant_info(int v, int* bits, int* tile_rows) {
+    if (v < 0 || v >= kNumSegVariants) return false;
+    *bits = kSegVariants[v].bits;
+    *tile_rows = kSegVariants[v].tile;
+    return true;
+}
+
+namespace {
+struct SegLayout {
+    size_t keys[2], vals[2], offs, zero, hist, counters, status[2], zero_bytes, total;
+    uint32_t stride, radix;
+};
+SegLayout seg_layout(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes, int variant) {
+    SegLayout L{};
+    const SegVariant& v = kSegVariants[variant];
+    L.radix = 1u << v.bits;
+    L.stride = (uint32_t)max_passes * L.radix;
+    const size_t A = 256;
+    size_t off = 0;
+    L.keys[0] = off; off = align_up(off + n * 8, A);
+    L.keys[1] = off; off = align_up(off + n * 8, A);
+    L.vals[0] = off; off = align_up(off + n * 4, A);
+    L.vals[1] = off; off = align_up(off + n * 4, A);
+    L.offs = off; off = align_up(off + (size_t)nsegs * L.stride * 4, A);
+    L.zero = off;
+    L.hist = off; off = align_up(off + (size_t)nsegs * L.stride * 4, A);
+    L.counters = off; off = align_up(off + (size_t)(max_passes + 1) * 4, A);
+    L.status[0] = off; off = align_up(off + (size_t)ntiles * L.radix * 4, A);
+    L.zero_bytes = off - L.zero;
+    L.status[1] = off; off = align_up(off + (size_t)ntiles * L.radix * 4, A);
+    L.total = off;
+    return L;
+}
+}  // namespace
+
+size_t seg_sort_workspace_bytes(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes, int variant) {
+    if (variant < 0 || variant >= kNumSegVariants) return 0;
+    return seg_layout(n, nsegs, ntiles, max_passes, variant).total;
+}
+
+cudaError_t run_seg_sort(const SegSortArgs& sa, unsigned char* ws, cudaStream_t s, Profiler* prof) {
+    if (sa.n == 0 || sa.ntiles == 0) return cudaSuccess;
+    if (sa.variant < 0 || sa.variant >= kNumSegVariants || sa.max_passes < 1 || sa.max_passes > 16)
+        return cudaErrorInvalidValue;
+    const SegVariant& var = kSegVariants[sa.variant];
+    const SegLayout L = seg_layout(sa.n, sa.nsegs, sa.ntiles, sa.max_passes, sa.variant);
+    cudaError_t e = cudaMemsetAsync(ws + L.zero, 0, L.zero_bytes, s);
+    if (e != cudaSuccess) return e;
+    uint32_t* hist = reinterpret_cast<uint32_t*>(ws + L.hist);
+    uint32_t* offs = reinterpret_cast<uint32_t*>(ws + L.offs);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(ws + L.counters);
+    uint32_t* status[2] = {reinterpret_cast<uint32_t*>(ws + L.status[0]),
+                           reinterpret_cast<uint32_t*>(ws + L.status[1])};
+    uint64_t* kbuf[2] = {reinterpret_cast<uint64_t*>(ws + L.keys[0]), reinterpret_cast<uint64_t*>(ws + L.keys[1])};
+    uint32_t* vbuf[2] = {reinterpret_cast<uint32_t*>(ws + L.vals[0]), reinterpret_cast<uint32_t*>(ws + L.vals[1])};
+
+    SegHistArgs h{sa.keys, sa.chunks, sa.segs, hist, L.stride, (uint32_t)var.bits, sa.nsegs, sa.n};
+    if (prof) prof->begin(KC_HIST, s);
+    k_seg_hist<<<sa.nchunks, 512, (size_t)L.stride * 4, s>>>(h);
+    if (prof) prof->end(KC_HIST, s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (prof) prof->begin(KC_SCAN, s);
+    k_row_scan<<<sa.nsegs * (uint32_t)sa.max_passes, 256, 0, s>>>(hist, offs, L.radix);
+    if (prof) prof->end(KC_SCAN, s);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+
+    for (int g = 0; g < sa.max_passes; ++g) {
+        const uint32_t grid = sa.tiles_in_pass[g];
+        if (grid == 0) break;
+        PassArgs a{};
+        a.n = sa.n;
+        a.shift = (uint32_t)(g * var.bits);
+        a.dtype = U64;
+        a.status = status[g & 1];
+        a.status_next = (g + 1 < sa.max_passes) ? status[(g + 1) & 1] : nullptr;
+        a.status_rows = sa.ntiles;
+        a.status_row_words = L.radix;
+        a.tile_counter = counters + g;
+        a.err = sa.err;
+        a.tile_seg = sa.tile_seg;
+        a.segs = sa.segs;
+        a.seg_offs = offs;
+        a.seg_stride = L.stride;
+        a.pass = (uint32_t)g;
+        a.keys_in = g == 0 ? static_cast<const void*>(sa.keys) : static_cast<const void*>(kbuf[(g - 1) & 1]);
+        a.vals_in = g == 0 ? nullptr : vbuf[(g - 1) & 1];
+        a.keys_out = kbuf[g & 1];
+        a.vals_out = vbuf[g & 1];
+        a.keys_final = sa.keys_out;
+        a.vals_final = sa.perm_out;
+        if (prof) prof->begin(KC_ONESWEEP64, s);
+        var.k[g == 0 ? 0 : 1]<<<grid, 256, var.smem, s>>>(a);
+        e = cudaGetLastError();
+        if (prof) prof->end(KC_ONESWEEP64, s);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 // Raises the dynamic shared-memory limit of every sort kernel on the current
 // device; called once per device before the first sort.
 cudaError_t prepare_sort_kernels() {
@@ -616,7 +888,20 @@ cudaError_t prepare_sort_kernels() {
                 cudaError_t e = cudaFuncSetAttribute(v.k[m][f], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
                 if (e != cudaSuccess) return e;
             }
-    return cudaFuncSetAttribute(k_digit_hist<kBits>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    for (const SegVariant& v : kSegVariants)
+        for (int m = 0; m < 2; ++m) {
+            cudaError_t e = cudaFuncSetAttribute(v.k[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
+            if (e != cudaSuccess) return e;
+        }
+    {
+        cudaError_t e = cudaFuncSetAttribute(k_seg_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             8 * kMaxRadix * 4);
+        if (e != cudaSuccess) return e;
+    }
+    // all histograms of a sort in shared memory: at most 4 keys x 6 passes x
+    // 2048 bins (11-bit digits) or 4 x 8 x 256 (8-bit)
+    return cudaFuncSetAttribute(k_digit_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                kMaxKeys * 6 * kMaxRadix * 4);
 }
 
 }  // namespace vdf

@@ -15,6 +15,14 @@ GPU results with the CPU oracle on the same arrays).
       50,000,000 distinct random int64; f64 lognormal(0,1); int64 U[0, 2^40).
   w2b same values; int32 key from 16 distinct random int32 with a 90/10 skew:
       2 hot keys take 45% of the rows each, the other 14 share 10%.
+  w3  batch of independent queries (the w0 schema): row counts log-uniform in
+      [1e3, 1e7], then all scaled by one factor so the batch holds a byte
+      budget (2 GiB of key + value bytes), floored at 1,000 rows; key int32 or
+      int64 (50/50); key cardinality log-uniform in [2, rows/2], drawn from a
+      per-query pool of distinct random values.
+  w4  served stream: Poisson arrivals; rows lognormal (median 1e6, sigma 1.0)
+      capped at 1e8; the w0 schema (int32 key over min(10,000, rows) distinct
+      values, f64 N(0,1) and int64 U[-1e9, 1e9] values).
 """
 from __future__ import annotations
 
@@ -122,3 +130,43 @@ def keys_for(dist: str, dtype, n: int, rng: np.random.Generator) -> np.ndarray:
     elif dist == "reversed":
         base = np.sort(base, kind="stable")[::-1].copy()
     return base
+
+
+def batch_specs(nq: int = 4096, rows_lo: float = 1e3, rows_hi: float = 1e7, budget_bytes: int = 2 << 30,
+                min_rows: int = 1000, seed_col: int = 0):
+    """Query shapes of a w3 batch: list of dicts {n, dtype, card, seed}."""
+    rng = np.random.default_rng(seed(3, seed_col))
+    n = np.floor(10 ** rng.uniform(np.log10(rows_lo), np.log10(rows_hi), size=nq)).astype(np.int64)
+    wide = rng.random(nq) < 0.5
+    nbytes = n * (np.where(wide, 8, 4) + 16)
+    s = min(1.0, budget_bytes / float(nbytes.sum()))
+    n = np.maximum(min_rows, np.floor(n * s)).astype(np.int64)
+    out = []
+    for i in range(nq):
+        hi = max(2.0, n[i] / 2)
+        card = int(np.floor(10 ** rng.uniform(np.log10(2.0), np.log10(hi)))) if hi > 2 else 2
+        out.append(dict(n=int(n[i]), dtype=np.int64 if wide[i] else np.int32, card=max(1, min(card, int(n[i]))),
+                        seed=int(rng.integers(0, 2**62))))
+    return out
+
+
+def batch_query(spec: dict):
+    """(key, v1 f64 N(0,1), v2 int64 U[-1e9, 1e9]) of one query shape."""
+    rng = np.random.default_rng(spec["seed"])
+    n, card = spec["n"], spec["card"]
+    pool = distinct_pool(rng, card, spec["dtype"])
+    key = pool[rng.integers(0, card, size=n)] if n else np.empty(0, spec["dtype"])
+    v1 = rng.standard_normal(n)
+    v2 = rng.integers(-10**9, 10**9, size=n, dtype=np.int64, endpoint=True)
+    return key, v1, v2
+
+
+def stream_specs(n_requests: int, rate_per_s: float, median_rows: float = 1e6, sigma: float = 1.0,
+                 cap_rows: int = 100_000_000, seed_col: int = 0):
+    """Request shapes of a w4 stream: list of dicts {t (arrival, s), n, dtype, card, seed}."""
+    rng = np.random.default_rng(seed(4, seed_col))
+    gaps = rng.exponential(1.0 / rate_per_s, size=n_requests)
+    t = np.cumsum(gaps) - gaps[0]
+    n = np.minimum(cap_rows, np.maximum(1, np.floor(rng.lognormal(np.log(median_rows), sigma, size=n_requests))))
+    return [dict(t=float(t[i]), n=int(n[i]), dtype=np.int32, card=int(min(10_000, n[i])),
+                 seed=int(rng.integers(0, 2**62))) for i in range(n_requests)]
