@@ -84,7 +84,7 @@ class ClockSampler:
         os.close(fd)
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.proc = None
@@ -182,6 +182,177 @@ def reference_arm(args, rank: int, world: int):
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def c0_canonical_bytes(n: int, key_width: int, n_groups: int) -> int:
+    """Canonical bytes of one one-key query (8-bit digits over the key, u32 row
+    ids, f64 + int64 values): sort w + w*2(w+4) + payload gather 4 + 2*16;
+    group-by reads keys + values once and writes per group key + count 8 +
+    f64 32 + int 40."""
+    w = key_width
+    return n * (w + w * 2 * (w + 4) + 4 + 32 + w + 16) + n_groups * (w + 8 + 32 + 40)
+
+
+def batched_section(args, local_rank: int) -> dict:
+    """Many independent queries as one graph-launched batch, against the same
+    queries run one library call each."""
+    import numpy as np
+    import torch
+
+    import visondf_b200 as vdf
+    from visondf_b200 import autotune, datagen
+
+    dev = torch.device("cuda", local_rank)
+    t0 = time.time()
+    specs = datagen.batch_specs(nq=args.batch_queries)
+    parts = [datagen.batch_query(s) for s in specs]
+    # one resident buffer per column kind; each query's columns are slices of it
+    cols = {}
+    for name, pick in (("k32", lambda p: p[0] if p[0].dtype == np.int32 else None),
+                       ("k64", lambda p: p[0] if p[0].dtype == np.int64 else None),
+                       ("v1", lambda p: p[1]), ("v2", lambda p: p[2])):
+        arrs = [a for a in (pick(p) for p in parts) if a is not None]
+        cols[name] = torch.from_numpy(np.concatenate(arrs)).to(dev)
+    off = {"k32": 0, "k64": 0, "v": 0}
+    queries = []
+    for key, v1, v2 in parts:
+        n = key.size
+        kk = "k32" if key.dtype == np.int32 else "k64"
+        k = cols[kk][off[kk]:off[kk] + n]
+        off[kk] += n
+        queries.append((k, [cols["v1"][off["v"]:off["v"] + n], cols["v2"][off["v"]:off["v"] + n]]))
+        off["v"] += n
+    del parts
+    rows = sum(int(k.numel()) for k, _ in queries)
+    log(f"[batched] {len(queries)} queries, {rows:,} rows, generated in {time.time() - t0:.1f}s")
+    ctx = vdf.Context(local_rank)
+    stream = torch.cuda.current_stream()
+    tuned = autotune.tune_batch(ctx, queries, reps=2)
+    log(f"[batched] tuning: {tuned['best']} ({tuned['best_ms']:.2f} ms)")
+    b = vdf.Batch(ctx, queries, tuned["best"])
+    for _ in range(args.warmup):
+        b.launch_graph(stream)
+    ctx.check(stream)
+    torch.cuda.synchronize()
+    l0 = ctx.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        b.launch_graph(stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.check(stream)
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = (ctx.kernel_launches - l0) / args.steps
+    ng = b.n_groups.cpu().tolist()
+    canonical = sum(c0_canonical_bytes(int(k.numel()), k.element_size(), int(g)) for (k, _), g in zip(queries, ng))
+    peak, _ = measured_peaks()
+    info = b.info()
+    b.close()
+
+    # one library call per query (vdf_sort_groupby, group count read back), one at a time
+    per_call_q = queries if args.per_call_queries <= 0 else queries[:args.per_call_queries]
+    for k, vs in per_call_q[:8]:
+        ctx.sort_groupby([k], vs, agg_cols=[0, 1])
+    torch.cuda.synchronize()
+    c0 = time.perf_counter()
+    for k, vs in per_call_q:
+        ctx.sort_groupby([k], vs, agg_cols=[0, 1])
+    torch.cuda.synchronize()
+    pc_sec = time.perf_counter() - c0
+    pc_rows = sum(int(k.numel()) for k, _ in per_call_q)
+    ctx.close()
+    del queries, cols
+    torch.cuda.empty_cache()
+    value = rows / (ms / 1e3)
+    per_call = pc_rows / pc_sec
+    return {
+        "workload": f"{len(specs)} independent sort + group-by queries, rows log-uniform 1e3..1e7 scaled to a "
+                    f"2 GiB batch (floor 1,000), int32/int64 keys 50/50, key cardinality log-uniform in "
+                    f"[2, rows/2], f64 + int64 values",
+        "queries": len(specs), "rows": rows, "value": value, "unit": UNIT, "ms_per_batch": ms,
+        "launch": "one CUDA graph per batch (captured once, replayed)", "gpu_launches_per_batch": launches,
+        "hbm_frac_canonical": canonical / (ms / 1e3) / 1e9 / peak, "canonical_bytes": canonical,
+        "split": info, "tuning": tuned["best"], "tuning_ms": tuned["table"],
+        "per_call": {"value": per_call, "unit": UNIT, "queries": len(per_call_q), "seconds": pc_sec,
+                     "call": "vdf_sort_groupby per query, group count read back (host sync) after each"},
+        "speedup_vs_per_call": value / per_call,
+    }
+
+
+def served_section(args, local_rank: int) -> dict:
+    """Poisson request stream over resident columns: continuous batching with
+    HBM-budget admission, against one library call per request."""
+    import numpy as np
+    import torch
+
+    from visondf_b200 import datagen, serve
+
+    dev = torch.device("cuda", local_rank)
+    table_rows = args.served_table_rows
+    f = datagen.frame_w0(n=table_rows, distinct=10_000)
+    key = torch.from_numpy(f["key"]).to(dev)
+    v1 = torch.from_numpy(f["v1"]).to(dev)
+    v2 = torch.from_numpy(f["v2"]).to(dev)
+    del f
+    resident = table_rows * (4 + 8 + 8)
+    budget = int(args.hbm_budget_gb * 1e9)
+    max_rows = 1 << 27
+    per_row_out = serve.out_bytes_per_row([True, False])
+    rng = np.random.default_rng(datagen.seed(4, 9))
+
+    def make_trace(rate, nreq, seed_col):
+        specs = datagen.stream_specs(nreq, rate, seed_col=seed_col)
+        reqs = []
+        for i, s in enumerate(specs):
+            n = min(s["n"], table_rows)
+            o = int(rng.integers(0, table_rows - n + 1))
+            reqs.append(serve.Request(rid=i, arrival=s["t"], rows=n, key=key[o:o + n],
+                                      vals=[v1[o:o + n], v2[o:o + n]], need_bytes=n * per_row_out))
+        return reqs
+
+    # both executors write into preallocated outputs (no allocation per batch or call)
+    vdts = [torch.float64, torch.int64]
+    batched_ex = serve.BatchExecutor(local_rank, slots=2, max_batch_rows=max_rows, val_dtypes=vdts)
+    per_call_ex = serve.PerCallExecutor(local_rank, reuse_outputs=(table_rows, torch.int32, vdts))
+    per_call_ex.ctx.reserve(serve.WS_BYTES_PER_ROW * table_rows)
+
+    def run(ex, reqs, single):
+        loop = serve.Loop(ex, budget, resident + ex.reserved_bytes, max_batch_rows=max_rows,
+                          max_batch_queries=1 if single else 4096)
+        st = loop.run(reqs)
+        for r in reqs:
+            r.result = None
+        return st
+
+    nreq = args.served_requests
+    # warm both paths (kernels, workspaces, allocator)
+    run(batched_ex, make_trace(1e9, 64, 7), False)
+    run(per_call_ex, make_trace(1e9, 16, 7), True)
+    torch.cuda.synchronize()
+    # capacity: every request waiting at t = 0
+    cap_b = run(batched_ex, make_trace(1e12, nreq, 0), False)
+    cap_p = run(per_call_ex, make_trace(1e12, nreq, 0), True)
+    mean_rows = cap_b.rows / cap_b.requests
+    rates = []
+    for frac in args.served_fractions:
+        rate = frac * cap_b.rows_per_s / mean_rows
+        sb = run(batched_ex, make_trace(rate, nreq, 1), False)
+        sp = run(per_call_ex, make_trace(rate, nreq, 1), True)
+        rates.append({"fraction_of_batched_capacity": frac, "requests_per_s": rate,
+                      "offered_rows_per_s": rate * mean_rows, "batched": sb.as_dict(), "per_call": sp.as_dict()})
+    del key, v1, v2
+    torch.cuda.empty_cache()
+    return {
+        "workload": f"Poisson arrivals, {nreq} requests per trace, rows lognormal (median 1e6, sigma 1.0, cap 1e8), "
+                    f"int32 key over min(10,000, rows) values + f64 + int64 values, slices of a resident "
+                    f"{table_rows:,}-row table; sort + group-by count/sum/min/max/mean per request",
+        "hbm_budget_bytes": budget, "resident_bytes": resident, "slots": 2,
+        "capacity": {"batched_rows_per_s": cap_b.rows_per_s, "per_call_rows_per_s": cap_p.rows_per_s,
+                     "speedup": cap_b.rows_per_s / cap_p.rows_per_s,
+                     "batched": cap_b.as_dict(), "per_call": cap_p.as_dict()},
+        "rates": rates,
+    }
 
 
 def our_arm(args, rank: int, world: int, local_rank: int):
@@ -340,6 +511,14 @@ def our_arm(args, rank: int, world: int, local_rank: int):
                          f"sort + payload gather + group-by; host CPU: {cpu_info()}"}
 
     ctx.close()
+    del d, outs, packed, keys, payload
+    torch.cuda.empty_cache()
+    sections = set(args.sections.split(","))
+    batched = served = None
+    if world == 1 and "batched" in sections:
+        batched = batched_section(args, local_rank)
+    if world == 1 and "served" in sections:
+        served = served_section(args, local_rank)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -358,6 +537,8 @@ def our_arm(args, rank: int, world: int, local_rank: int):
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "batched": batched,
+            "served": served,
         }
         print(json.dumps(line), flush=True)
 
@@ -375,6 +556,15 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default kernel variants")
     ap.add_argument("--variants", type=int, nargs=2, metavar=("V32", "V64"),
                     help="with --no-autotune: radix-pass variant indices for 4- and 8-byte keys")
+    ap.add_argument("--sections", default="batched,served",
+                    help="extra single-GPU measurements after the headline one: batched, served (comma list, "
+                         "'none' for neither)")
+    ap.add_argument("--batch-queries", type=int, default=4096)
+    ap.add_argument("--per-call-queries", type=int, default=0, help="queries of the per-call baseline (0 = all)")
+    ap.add_argument("--served-requests", type=int, default=400)
+    ap.add_argument("--served-table-rows", type=int, default=100_000_000)
+    ap.add_argument("--served-fractions", type=float, nargs="+", default=[0.5, 0.7, 0.9])
+    ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     args = ap.parse_args()
     if args.warmup < 3:
         log("note: fewer than 3 warm-up steps; the timing rules ask for at least 3")

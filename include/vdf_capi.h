@@ -6,7 +6,9 @@
  * cudaStream_t passed as void* (NULL = the legacy default stream).  Every call
  * returns a vdf_status and never aborts or throws.  Compute calls are
  * asynchronous on `stream` unless they return a host value (n_groups_host),
- * in which case they synchronise that stream before returning.
+ * in which case they synchronise that stream before returning, or sort by
+ * several keys in the default multi-key mode (vdf_ctx_set_multikey_mode),
+ * which synchronises the stream once to read one flag.
  *
  * A context owns one grow-only workspace, so calls on one context are
  * serialised on the host and must not overlap on the GPU: use one context per
@@ -117,7 +119,8 @@ typedef enum vdf_kernel_class {
     VDF_KC_BROADCAST = 6,   /* transform broadcast            */
     VDF_KC_PACK = 7,        /* row-record packing for gathers */
     VDF_KC_SEGSCAN = 8,     /* group-by: tile prefix scan     */
-    VDF_KC_SEGEMIT = 9      /* group-by: scan + emit groups   */
+    VDF_KC_SEGEMIT = 9,     /* group-by: scan + emit groups   */
+    VDF_KC_TIES = 10        /* equal-neighbour check (multi-key) */
 } vdf_kernel_class;
 /* When enabled, every kernel the context launches is bracketed by CUDA
  * events on its stream (no reference counterpart: the reference has no
@@ -144,6 +147,24 @@ vdf_status vdf_sort_variant_info(int index, int32_t* key_width, int32_t* threads
                                  int32_t* digit_bits, int32_t* match);
 vdf_status vdf_ctx_set_sort_tuning(vdf_ctx* ctx, const vdf_sort_tuning* tuning);
 vdf_status vdf_ctx_get_sort_tuning(vdf_ctx* ctx, vdf_sort_tuning* tuning);
+
+/* How a context sorts by several keys.
+ * VDF_MULTIKEY_PRIMARY_FIRST (default): sort by the most significant key
+ *   alone, then check its sorted copy for equal neighbours; with none, that
+ *   order already is the stable order over all keys (later keys only break
+ *   ties) and the remaining keys' passes are skipped; otherwise the LSD sort
+ *   over all keys follows.  The check reads one flag back: a multi-key call
+ *   synchronises its stream once (not under stream capture, where the LSD
+ *   sort runs).  Results are identical in both modes.
+ * VDF_MULTIKEY_LSD: always the LSD sort over all keys, least-significant key
+ *   first, fully asynchronous; the reference composes multi-key sorts the
+ *   same way through its in/out idx (sort_by_mt.hpp:3-180 per key). */
+typedef enum vdf_multikey_mode {
+    VDF_MULTIKEY_LSD = 0,
+    VDF_MULTIKEY_PRIMARY_FIRST = 1
+} vdf_multikey_mode;
+vdf_status vdf_ctx_set_multikey_mode(vdf_ctx* ctx, int mode);
+int vdf_ctx_get_multikey_mode(vdf_ctx* ctx); /* -1 for a NULL context */
 
 /* ---- workspace sizing (pure host functions) ------------------------------ */
 /* Enough for every tuning; vdf_sort_argsort_ws also packs the other sorted

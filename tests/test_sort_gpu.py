@@ -195,3 +195,74 @@ def test_eleven_bit_digits_with_every_key_type(ctx, order):
             assert (host(perm).view(np.uint32) == exp).all(), (a, b)
     finally:
         ctx.set_sort_tuning(*saved)
+
+
+def _primary_keys(case, n, rng):
+    if case == "distinct":
+        k0 = rng.integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, size=n, dtype=np.int64, endpoint=True)
+        assert np.unique(k0).size == n
+    elif case == "ties":
+        k0 = rng.integers(0, 1000, size=n).astype(np.int64)
+    elif case == "one_pair":  # distinct except the last row repeats the first
+        k0 = rng.permutation(n).astype(np.int64) * 3 - n
+        k0[-1] = k0[0]
+    else:  # all equal
+        k0 = np.full(n, -7, dtype=np.int64)
+    return k0
+
+
+@pytest.mark.parametrize("case", ["distinct", "ties", "one_pair", "all_equal"])
+@pytest.mark.parametrize("order", [ob.ASC, ob.DESC_STABLE, ob.DESC_REVERSE])
+def test_multikey_modes_give_the_oracle_order(ctx, case, order):
+    rng = np.random.default_rng(77 + order)
+    n = 400_003
+    k0 = _primary_keys(case, n, rng)
+    k1 = rng.integers(-5, 5, size=n).astype(np.int32)
+    v = rng.standard_normal(n)
+    exp = ob.argsort([k0, k1], order)
+    keys = [dev(k0), dev(k1)]
+    try:
+        for mode in (vdf._lib.MULTIKEY_LSD, vdf._lib.MULTIKEY_PRIMARY_FIRST):
+            ctx.set_multikey_mode(mode)
+            assert ctx.get_multikey_mode() == mode
+            perm = ctx.argsort(keys, order=order)
+            assert (host(perm).view(np.uint32) == exp).all(), (case, mode)
+            s0, s1 = torch.empty_like(keys[0]), torch.empty_like(keys[1])
+            perm = ctx.argsort(keys, order=order, sorted_keys_out=[s0, s1])
+            assert (host(perm).view(np.uint32) == exp).all()
+            assert bits_equal(host(s0), k0[exp]) and bits_equal(host(s1), k1[exp])
+            if order == ob.ASC:
+                gr = ctx.sort_groupby(keys, [dev(v)], agg_cols=[0])
+                assert (host(gr.perm).view(np.uint32) == exp).all()
+                og = ob.groupby([k0, k1], [v])
+                assert gr.n_groups == og.n_groups and (host(gr.count) == og.count).all()
+    finally:
+        ctx.set_multikey_mode(vdf._lib.MULTIKEY_PRIMARY_FIRST)
+
+
+def test_multikey_sort_under_graph_capture(ctx):
+    """Inside stream capture the primary-key check (a host read-back) is
+    skipped and the LSD sort over all keys is captured instead."""
+    rng = np.random.default_rng(5)
+    n = 300_000
+    k0 = rng.integers(0, 50, size=n).astype(np.int64)
+    k1 = rng.integers(0, 1 << 31, size=n).astype(np.int32)
+    keys = [dev(k0), dev(k1)]
+    exp = ob.argsort([k0, k1])
+    perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    ctx.reserve(1 << 28)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        ctx.argsort(keys, perm_out=perm, stream=s)  # warm
+    torch.cuda.current_stream().wait_stream(s)
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        ctx.argsort(keys, perm_out=perm)
+    perm.fill_(-1)
+    g.replay()
+    torch.cuda.synchronize()
+    ctx.check()
+    assert (host(perm).view(np.uint32) == exp).all()
+    del g

@@ -24,7 +24,9 @@ I32, I64, U32, U64, F64, F32 = range(6)
 ORDER_ASC, ORDER_DESC_STABLE, ORDER_DESC_REVERSE = range(3)
 
 KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast", "pack",
-                  "segscan", "segemit"]
+                  "segscan", "segemit", "ties"]
+# vdf_multikey_mode
+MULTIKEY_LSD, MULTIKEY_PRIMARY_FIRST = 0, 1
 
 TORCH_TO_VDF = {
     torch.int32: I32, torch.int64: I64, torch.uint32: U32, torch.uint64: U64,
@@ -123,6 +125,8 @@ def _load() -> C.CDLL:
         "vdf_gather_host": (st, [vp, u64, vp, C.POINTER(vdf_col), i32, C.POINTER(vp), vp]),
         "vdf_transform_groupby_host": (st, [vp, u64, C.POINTER(vdf_col), i32, vdf_col, C.c_int32, vp, vp,
                                             C.POINTER(C.c_uint64), vp]),
+        "vdf_ctx_set_multikey_mode": (st, [vp, i32]),
+        "vdf_ctx_get_multikey_mode": (i32, [vp]),
         "vdf_batch_variant_count": (i32, []),
         "vdf_batch_variant_info": (st, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         "vdf_batch_default_tuning": (st, [C.POINTER(vdf_batch_tuning)]),
@@ -274,6 +278,12 @@ class Context:
     def set_sort_tuning(self, variant32: int, variant64: int):
         t = vdf_sort_tuning(variant32, variant64)
         self._check(lib.vdf_ctx_set_sort_tuning(self.handle, C.byref(t)), "vdf_ctx_set_sort_tuning")
+
+    def set_multikey_mode(self, mode: int):
+        self._check(lib.vdf_ctx_set_multikey_mode(self.handle, mode), "vdf_ctx_set_multikey_mode")
+
+    def get_multikey_mode(self) -> int:
+        return lib.vdf_ctx_get_multikey_mode(self.handle)
 
     def get_sort_tuning(self) -> tuple:
         t = vdf_sort_tuning()
@@ -461,7 +471,24 @@ class Batch:
     the same value dtypes.  Outputs live in arenas owned by this object;
     `result(q)` returns views of query q's part after a launch."""
 
-    def __init__(self, ctx: "Context", queries, tuning: Optional[dict] = None):
+    @staticmethod
+    def alloc_outputs(capacity: int, val_dtypes, device) -> dict:
+        """Output arenas for batches of up to `capacity` rows, reusable by
+        successive batches (pass as `outputs=`)."""
+        N = max(1, int(capacity))
+        aggs = []
+        for dt in val_dtypes:
+            fl = dt in (torch.float64, torch.float32)
+            aggs.append(AggResult(torch.empty(N, dtype=torch.float64 if fl else torch.int64, device=device),
+                                  None if fl else torch.empty(N, dtype=torch.int64, device=device),
+                                  torch.empty(N, dtype=dt, device=device), torch.empty(N, dtype=dt, device=device),
+                                  torch.empty(N, dtype=torch.float64, device=device)))
+        return {"capacity": N, "perm": torch.empty(N, dtype=torch.int32, device=device),
+                "gkeys": torch.empty(N, dtype=torch.int64, device=device),
+                "count": torch.empty(N, dtype=torch.int64, device=device), "aggs": aggs,
+                "val_dtypes": list(val_dtypes)}
+
+    def __init__(self, ctx: "Context", queries, tuning: Optional[dict] = None, outputs: Optional[dict] = None):
         self.ctx = ctx
         self.queries = [(k, list(vs)) for k, vs in queries]
         nq = len(self.queries)
@@ -474,19 +501,13 @@ class Batch:
                 raise ValueError("every query must have the same value dtypes")
         dev = torch.device("cuda", ctx.device)
         self.n_total = sum(int(k.numel()) for k, _ in self.queries)
-        N = max(1, self.n_total)
-        self.perm = torch.empty(N, dtype=torch.int32, device=dev)
-        self.gkeys = torch.empty(N, dtype=torch.int64, device=dev)
-        self.count = torch.empty(N, dtype=torch.int64, device=dev)
-        self.aggs = []
+        if outputs is None:
+            outputs = Batch.alloc_outputs(self.n_total, self.val_dtypes, dev)
+        elif outputs["capacity"] < self.n_total or outputs["val_dtypes"] != self.val_dtypes:
+            raise ValueError("output arenas too small or of other value dtypes")
+        self.perm, self.gkeys, self.count, self.aggs = outputs["perm"], outputs["gkeys"], outputs["count"], outputs["aggs"]
         structs = (vdf_agg_out * BATCH_MAX_VALS)()
-        for j, dt in enumerate(self.val_dtypes):
-            fl = dt in (torch.float64, torch.float32)
-            a = AggResult(torch.empty(N, dtype=torch.float64 if fl else torch.int64, device=dev),
-                          None if fl else torch.empty(N, dtype=torch.int64, device=dev),
-                          torch.empty(N, dtype=dt, device=dev), torch.empty(N, dtype=dt, device=dev),
-                          torch.empty(N, dtype=torch.float64, device=dev))
-            self.aggs.append(a)
+        for j, a in enumerate(self.aggs):
             structs[j] = vdf_agg_out(_ptr(a.sum), _ptr(a.sum_hi), _ptr(a.min), _ptr(a.max), _ptr(a.mean))
         self.row_offset = torch.zeros(max(1, nq), dtype=torch.int64, device=dev)
         self.group_offset = torch.zeros(max(1, nq), dtype=torch.int64, device=dev)

@@ -80,3 +80,44 @@ def tune(ctx: "_lib.Context", run: Callable[[], None], reps: int = 2) -> dict:
     best64 = min(ms64, key=ms64.get) if ms64 else cur[1]
     ctx.set_sort_tuning(best32, best64)
     return {"variant32": best32, "variant64": best64, "ms32": ms32, "ms64": ms64}
+
+
+def batch_candidates() -> list:
+    """Tunings of the batched executor: the size-class boundary (largest
+    query run by one CTA in shared memory: none, 2048, 4096 or 8192 rows),
+    that kernel's digit width (4 or 8 bits) and the segmented radix-pass
+    variant (digit width 8 or 11, 2048-4096-row tiles) for the larger
+    queries."""
+    segs = [v["index"] for v in _lib.batch_variants()]
+    out = []
+    for seg in segs:
+        out.append({"small_rows": 0, "small_bits": 8, "seg_variant": seg})
+        for small in (2048, 4096, 8192):
+            for bits in (4, 8):
+                out.append({"small_rows": small, "small_bits": bits, "seg_variant": seg})
+    return out
+
+
+def tune_batch(ctx: "_lib.Context", queries, reps: int = 2, candidates: Optional[list] = None) -> dict:
+    """Times one batch of `queries` under every candidate tuning (graph
+    launches, CUDA events) and returns {"best": tuning, "best_ms": ms,
+    "table": [(tuning, ms), ...]}."""
+    import torch
+
+    stream = torch.cuda.current_stream()
+    table = []
+    for t in candidates or batch_candidates():
+        b = _lib.Batch(ctx, queries, t)
+        b.launch_graph(stream)  # capture + warm
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            b.launch_graph(stream)
+        e1.record(stream)
+        e1.synchronize()
+        ctx.check(stream)
+        table.append((dict(t), e0.elapsed_time(e1) / reps))
+        b.close()
+        del b
+    best, best_ms = min(table, key=lambda x: x[1])
+    return {"best": best, "best_ms": best_ms, "table": table}

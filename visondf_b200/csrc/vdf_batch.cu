@@ -57,11 +57,22 @@ __global__ void __launch_bounds__(256) k_batch_pack(BatchDev b) {
         const uint64_t local = i - sd.row_start;   // row within the query
         b.arena_keys[i] = ordered_image(q.key, local, q.key_dtype);
         b.arena_seg[i] = ch.seg;
-        for (int j = 0; j < b.nvals; ++j) {
-            if (b.val_width[j] == 8)
-                static_cast<uint64_t*>(b.arena_vals[j])[i] = __ldg(static_cast<const uint64_t*>(q.vals[j]) + local);
-            else
-                static_cast<uint32_t*>(b.arena_vals[j])[i] = __ldg(static_cast<const uint32_t*>(q.vals[j]) + local);
+        if (b.rec_bytes) {
+            // the packed gather's record: 8-byte slots, zero-extended
+            unsigned long long slot[VDF_BATCH_MAX_VALS] = {0, 0, 0, 0};
+            for (int j = 0; j < b.nvals; ++j)
+                slot[j] = b.val_width[j] == 8 ? __ldg(static_cast<const unsigned long long*>(q.vals[j]) + local)
+                                              : (unsigned long long)__ldg(static_cast<const uint32_t*>(q.vals[j]) + local);
+            ulonglong2* dst = reinterpret_cast<ulonglong2*>(b.arena_recs + i * (uint64_t)b.rec_bytes);
+            dst[0] = make_ulonglong2(slot[0], slot[1]);
+            if (b.rec_bytes == 32) dst[1] = make_ulonglong2(slot[2], slot[3]);
+        } else {
+            for (int j = 0; j < b.nvals; ++j) {
+                if (b.val_width[j] == 8)
+                    static_cast<uint64_t*>(b.arena_vals[j])[i] = __ldg(static_cast<const uint64_t*>(q.vals[j]) + local);
+                else
+                    static_cast<uint32_t*>(b.arena_vals[j])[i] = __ldg(static_cast<const uint32_t*>(q.vals[j]) + local);
+            }
         }
     }
 }
@@ -234,16 +245,20 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
     P.o_seg_first = o; o = align_up(o + 4 * std::max<size_t>(1, P.segs.size()), A);
     P.o_arena_keys = o; o = align_up(o + 8 * nl, A);
     P.o_arena_seg = o; o = align_up(o + 4 * nl, A);
-    for (int j = 0; j < a.nvals; ++j) { P.o_arena_vals[j] = o; o = align_up(o + (size_t)P.val_width[j] * nl, A); }
+    P.rec_bytes = gather_record_bytes(a.nvals);  // 0 for fewer than two value columns
+    if (P.rec_bytes) {
+        P.o_arena_recs = o;
+        o = align_up(o + P.rec_bytes * nl, A);
+    } else {
+        for (int j = 0; j < a.nvals; ++j) { P.o_arena_vals[j] = o; o = align_up(o + (size_t)P.val_width[j] * nl, A); }
+    }
     P.o_sorted_keys = o; o = align_up(o + 8 * nl, A);
     for (int j = 0; j < a.nvals; ++j) { P.o_sorted_vals[j] = o; o = align_up(o + (size_t)P.val_width[j] * nl, A); }
     P.o_group_seg = o; o = align_up(o + 4 * nl, A);
     P.o_group_key = o; o = align_up(o + 8 * nl, A);
     P.o_tail = o;
-    int rec_cols = a.nvals;
     size_t tail = seg_sort_workspace_bytes(nl, (uint32_t)P.segs.size(), (uint32_t)P.tile_seg.size(),
                                            std::max(1, maxp), t.seg_variant);
-    tail = std::max(tail, (size_t)nl * gather_record_bytes(rec_cols));
     tail = std::max(tail, segreduce_workspace_bytes(nl, a.nvals));
     P.ws_bytes = o + tail;
     return true;
@@ -266,9 +281,11 @@ BatchDev batch_dev_view(const BatchPlan& P, const vdf_batch_args& a, unsigned ch
     for (int j = 0; j < P.nvals; ++j) {
         b.val_width[j] = P.val_width[j];
         b.val_dtype[j] = a.val_dtypes[j];
-        b.arena_vals[j] = ws + P.o_arena_vals[j];
+        b.arena_vals[j] = P.rec_bytes ? nullptr : ws + P.o_arena_vals[j];
         b.aggs[j] = a.aggs[j];
     }
+    b.arena_recs = P.rec_bytes ? ws + P.o_arena_recs : nullptr;
+    b.rec_bytes = (int)P.rec_bytes;
     b.arena_keys = reinterpret_cast<uint64_t*>(ws + P.o_arena_keys);
     b.arena_seg = reinterpret_cast<uint32_t*>(ws + P.o_arena_seg);
     b.group_seg = reinterpret_cast<uint32_t*>(ws + P.o_group_seg);
@@ -339,12 +356,16 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
             g.n = P.n_large;
             g.ncols = P.nvals;
             for (int j = 0; j < P.nvals; ++j) {
-                g.src[j] = ws + P.o_arena_vals[j];
+                g.src[j] = P.rec_bytes ? nullptr : ws + P.o_arena_vals[j];
                 g.dst[j] = ws + P.o_sorted_vals[j];
                 g.width[j] = P.val_width[j];
             }
             int gl = 0;
-            if ((e = run_gather(g, s, prof, tail, P.ws_bytes - P.o_tail, &gl)) != cudaSuccess) return e;
+            if (P.rec_bytes)
+                e = run_gather_records(g, b.arena_recs, P.rec_bytes, s, prof, &gl);
+            else
+                e = run_gather(g, s, prof, nullptr, 0, &gl);
+            if (e != cudaSuccess) return e;
             n += gl;
         }
 
@@ -508,16 +529,21 @@ vdf_status vdf_batch_create(vdf_ctx* c, const vdf_batch_args* a, const vdf_batch
         std::memcpy(host.data() + P.o_chunks, P.chunks.data(), sizeof(vdf::SegChunk) * P.chunks.size());
     if (!P.small_queries.empty())
         std::memcpy(host.data() + P.o_small, P.small_queries.data(), 4 * P.small_queries.size());
-    // per-query outputs known on the host: row offsets; empty queries' ranges
+    // per-query outputs known on the host: row offsets; empty queries' ranges.
+    // Uploaded on the batch's own non-blocking stream, so creating a batch
+    // does not wait for other work on the device (only for these copies).
     std::vector<uint64_t> zeros(std::max<uint32_t>(1, a->nqueries), 0);
-    cudaError_t e = cudaMemcpy(b->ws, host.data(), P.desc_bytes, cudaMemcpyHostToDevice);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->ws, host.data(), P.desc_bytes, cudaMemcpyHostToDevice, b->side);
     if (e == cudaSuccess && a->nqueries) {
-        e = cudaMemcpy(a->row_offset_out, P.row_offset.data(), 8 * a->nqueries, cudaMemcpyHostToDevice);
+        e = cudaMemcpyAsync(a->row_offset_out, P.row_offset.data(), 8 * a->nqueries, cudaMemcpyHostToDevice, b->side);
         if (e == cudaSuccess)
-            e = cudaMemcpy(a->group_offset_out, P.row_offset.data(), 8 * a->nqueries, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess) e = cudaMemcpy(a->n_groups_out, zeros.data(), 8 * a->nqueries, cudaMemcpyHostToDevice);
+            e = cudaMemcpyAsync(a->group_offset_out, P.row_offset.data(), 8 * a->nqueries, cudaMemcpyHostToDevice,
+                                b->side);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(a->n_groups_out, zeros.data(), 8 * a->nqueries, cudaMemcpyHostToDevice, b->side);
     }
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->side);  // the host vectors die here
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->join, cudaEventDisableTiming);
     if (e != cudaSuccess) {

@@ -49,7 +49,9 @@ struct BatchDev {
     int small_bits;
     int val_width[VDF_BATCH_MAX_VALS];
     int val_dtype[VDF_BATCH_MAX_VALS];
-    void* arena_vals[VDF_BATCH_MAX_VALS];
+    void* arena_vals[VDF_BATCH_MAX_VALS];  // one value column each (fewer than two columns)
+    unsigned char* arena_recs;             // or one record per row (two or more)
+    int rec_bytes;
     vdf_agg_out aggs[VDF_BATCH_MAX_VALS];
     uint64_t* arena_keys;        // [n_large] ordered key images
     uint32_t* arena_seg;         // [n_large] segment of each arena row
@@ -83,6 +85,7 @@ struct BatchPlan {
     // workspace layout (byte offsets)
     size_t o_queries = 0, o_segs = 0, o_seg_query = 0, o_tile_seg = 0, o_chunks = 0, o_small = 0, desc_bytes = 0;
     size_t o_counters = 0, o_seg_first = 0, o_arena_keys = 0, o_arena_seg = 0, o_arena_vals[VDF_BATCH_MAX_VALS] = {};
+    size_t o_arena_recs = 0, rec_bytes = 0;
     size_t o_sorted_keys = 0, o_sorted_vals[VDF_BATCH_MAX_VALS] = {}, o_group_seg = 0, o_group_key = 0, o_tail = 0;
     size_t ws_bytes = 0;
     int graph_launches = 0;

@@ -56,6 +56,54 @@ size_t sort_ws_need(const vdf::SortPlan& p, uint64_t n, int nkeys, void* const* 
     for (int k = 1; k < nkeys; ++k) other += (sorted_keys_out && sorted_keys_out[k]) ? 1 : 0;
     return std::max(p.ws_bytes, (size_t)n * vdf::gather_record_bytes(other));
 }
+// ... plus, for a multi-key sort tried primary key first without a sorted
+// output for that key, room for its sorted copy beside its own sort.
+size_t primary_first_need(vdf_ctx* c, uint64_t n, const int32_t* dts, int nkeys, void* const* sorted_keys_out) {
+    if (nkeys < 2 || c->multikey_mode != VDF_MULTIKEY_PRIMARY_FIRST || (sorted_keys_out && sorted_keys_out[0]))
+        return 0;
+    const vdf::SortPlan p0 = vdf::make_sort_plan(n, dts, 1, c->tuning);
+    return align256(p0.ws_bytes) + (size_t)n * vdf::dtype_width(dts[0]);
+}
+
+// Multi-key sorts, primary key first: sort by the most significant key alone,
+// then look for equal neighbours in its sorted copy.  With none, no two rows
+// share the primary key, so that order already is the stable order over all
+// keys (later keys only break ties) and the sort is done; otherwise the caller
+// runs the LSD sort over all keys, overwriting perm and key0.  The check reads
+// one flag back, so it synchronises the stream once; under stream capture, or
+// with VDF_MULTIKEY_LSD, it is skipped.  key0_out may be null, in which case
+// the primary key's sorted copy goes to scratch after the sort's workspace.
+// Returns VDF_OK with *done telling which case happened.
+vdf_status primary_first(vdf_ctx* c, uint64_t n, const int32_t* dts, const void* const* cols, int nkeys, int order,
+                         uint32_t* perm, void* key0_out, unsigned char* ws, size_t ws_bytes, cudaStream_t s,
+                         const uint32_t* perm_in, bool* done) {
+    *done = false;
+    if (nkeys < 2 || c->multikey_mode != VDF_MULTIKEY_PRIMARY_FIRST || n < 2) return VDF_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return VDF_OK;
+    }
+    const vdf::SortPlan p0 = vdf::make_sort_plan(n, dts, 1, c->tuning);
+    size_t need = p0.ws_bytes;
+    void* k0 = key0_out;
+    if (!k0) {
+        k0 = ws + align256(p0.ws_bytes);
+        need = align256(p0.ws_bytes) + (size_t)n * vdf::dtype_width(dts[0]);
+    }
+    if (need > ws_bytes) return VDF_OK;  // no room: the LSD sort over all keys
+    cudaError_t e = vdf::run_sort(p0, cols, order, perm, k0, ws, err_word(c), s, prof_of(c), perm_in);
+    c->launches += 2 + (uint64_t)p0.total_passes;
+    if (e == cudaSuccess) e = cudaMemsetAsync(tie_word(c), 0, sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = vdf::flag_adjacent_ties(k0, vdf::dtype_width(dts[0]), n, tie_word(c), s, prof_of(c));
+    c->launches += 1;
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(&c->host_pinned[2], tie_word(c), sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, "primary-key sort");
+    *done = (static_cast<uint32_t>(c->host_pinned[2]) == 0);
+    return VDF_OK;
+}
 
 vdf_status sort_impl(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, int order, uint32_t* perm_out,
                      void* const* sorted_keys_out, unsigned char* ws, size_t ws_bytes, cudaStream_t s) {
@@ -69,9 +117,14 @@ vdf_status sort_impl(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, int
     if (ws_bytes < p.ws_bytes)
         return fail(c, VDF_ERR_WORKSPACE, "workspace of %zu bytes < %zu needed", ws_bytes, p.ws_bytes);
     void* key0_out = sorted_keys_out ? sorted_keys_out[0] : nullptr;
-    cudaError_t e = vdf::run_sort(p, cols, order, perm_out, key0_out, ws, err_word(c), s, prof_of(c));
-    c->launches += 2 + (uint64_t)p.total_passes;
-    if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
+    bool done = false;
+    vdf_status pst = primary_first(c, n, dts, cols, nkeys, order, perm_out, key0_out, ws, ws_bytes, s, nullptr, &done);
+    if (pst != VDF_OK) return pst;
+    if (!done) {
+        cudaError_t e = vdf::run_sort(p, cols, order, perm_out, key0_out, ws, err_word(c), s, prof_of(c));
+        c->launches += 2 + (uint64_t)p.total_passes;
+        if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
+    }
     return emit_other_keys(c, n, keys, nkeys, perm_out, sorted_keys_out, ws, ws_bytes, s);
 }
 
@@ -156,6 +209,21 @@ vdf_status vdf_ctx_get_sort_tuning(vdf_ctx* c, vdf_sort_tuning* t) {
     return VDF_OK;
 }
 
+vdf_status vdf_ctx_set_multikey_mode(vdf_ctx* c, int mode) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    if (mode != VDF_MULTIKEY_LSD && mode != VDF_MULTIKEY_PRIMARY_FIRST)
+        return fail(c, VDF_ERR_INVALID_ARG, "bad multi-key mode %d", mode);
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->multikey_mode = mode;
+    return VDF_OK;
+}
+
+int vdf_ctx_get_multikey_mode(vdf_ctx* c) {
+    if (!c) return -1;
+    std::lock_guard<std::mutex> lk(c->mu);
+    return c->multikey_mode;
+}
+
 size_t vdf_groupby_workspace_bytes(uint64_t n, int nvals) {
     if (nvals < 0 || nvals > vdf::kMaxVals) return 0;
     return vdf::segreduce_workspace_bytes(n, nvals);
@@ -188,7 +256,7 @@ vdf_status vdf_ctx_create(int device, vdf_ctx** out) {
         }
     }
     if (cudaMalloc(&c->dev_small, 256) != cudaSuccess || cudaMemset(c->dev_small, 0, 256) != cudaSuccess ||
-        cudaMallocHost(&c->host_pinned, 2 * sizeof(uint64_t)) != cudaSuccess) {
+        cudaMallocHost(&c->host_pinned, 4 * sizeof(uint64_t)) != cudaSuccess) {
         cudaGetLastError();
         if (c->dev_small) cudaFree(c->dev_small);
         delete c;
@@ -291,7 +359,8 @@ vdf_status vdf_sort_argsort(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nke
     DeviceGuard g(c->device);
     int32_t dts[vdf::kMaxKeys];
     for (int k = 0; k < nkeys; ++k) dts[k] = keys[k].dtype;
-    const size_t need = sort_ws_need(vdf::make_sort_plan(n, dts, nkeys, c->tuning), n, nkeys, sorted_keys_out);
+    const size_t need = std::max(sort_ws_need(vdf::make_sort_plan(n, dts, nkeys, c->tuning), n, nkeys, sorted_keys_out),
+                                 primary_first_need(c, n, dts, nkeys, sorted_keys_out));
     if ((st = ws_ensure(c, need)) != VDF_OK) return st;
     return sort_impl(c, n, keys, nkeys, order, perm_out, sorted_keys_out, c->ws, c->ws_cap,
                      static_cast<cudaStream_t>(stream));
@@ -445,7 +514,12 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
     for (int p = 0; p < x->npayload; ++p) ngather += (spay[p] || pay_own[p]) ? 1 : 0;
     const size_t rec_bytes = (size_t)n * vdf::gather_record_bytes(std::min(ngather, vdf::kMaxGather));
     const size_t seg_bytes = x->groupby ? vdf::segreduce_workspace_bytes(n, x->nagg) : 0;
-    const size_t tail = std::max(std::max(plan.ws_bytes, seg_bytes), rec_bytes);
+    size_t tail = std::max(std::max(plan.ws_bytes, seg_bytes), rec_bytes);
+    if (x->nkeys >= 2 && c->multikey_mode == VDF_MULTIKEY_PRIMARY_FIRST && !skey[0]) {
+        // room for the primary key's sorted copy next to its sort's workspace
+        const vdf::SortPlan p0 = vdf::make_sort_plan(n, dts, 1, c->tuning);
+        tail = std::max(tail, align256(p0.ws_bytes) + (size_t)n * vdf::dtype_width(dts[0]));
+    }
     if ((st = ws_ensure(c, off + tail)) != VDF_OK) return st;
     uint32_t* perm = own_perm ? reinterpret_cast<uint32_t*>(c->ws) : x->perm_out;
     for (int k = 0; k < x->nkeys; ++k)
@@ -454,9 +528,16 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
         if (pay_own[p]) spay[p] = c->ws + pay_off[p];
     unsigned char* tws = c->ws + off;
 
-    cudaError_t e = vdf::run_sort(plan, cols, x->order, perm, skey[0], tws, err_word(c), s, prof_of(c), x->perm_in);
-    c->launches += 2 + (uint64_t)plan.total_passes;
-    if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
+    bool done = false;
+    if ((st = primary_first(c, n, dts, cols, x->nkeys, x->order, perm, skey[0], tws, c->ws_cap - off, s, x->perm_in,
+                            &done)) != VDF_OK)
+        return st;
+    cudaError_t e = cudaSuccess;
+    if (!done) {
+        e = vdf::run_sort(plan, cols, x->order, perm, skey[0], tws, err_word(c), s, prof_of(c), x->perm_in);
+        c->launches += 2 + (uint64_t)plan.total_passes;
+        if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
+    }
 
     // Gather the other key columns and the payload into sorted order, up to
     // kMaxGather columns per launch (the permutation is read once per launch).

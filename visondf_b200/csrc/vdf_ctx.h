@@ -78,7 +78,8 @@ struct vdf_ctx {
     unsigned char* ws = nullptr;
     size_t ws_cap = 0;
     unsigned char* dev_small = nullptr;  // [0,4): error bits; [8,16): group count scratch
-    uint64_t* host_pinned = nullptr;     // [0]: group count, [1]: error bits
+    uint64_t* host_pinned = nullptr;     // [0]: group count, [1]: error bits, [2]: tie flag
+    int multikey_mode = VDF_MULTIKEY_PRIMARY_FIRST;
     std::atomic<uint64_t> launches{0};
     std::string last_error;
 };
@@ -124,6 +125,7 @@ inline vdf::Profiler* prof_of(vdf_ctx* c) { return c->profiling ? &c->prof : nul
 
 inline uint32_t* err_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->dev_small); }
 inline uint64_t* count_word(vdf_ctx* c) { return reinterpret_cast<uint64_t*>(c->dev_small + 8); }
+inline uint32_t* tie_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->dev_small + 16); }
 
 inline vdf_status ws_ensure(vdf_ctx* c, size_t bytes) {
     if (bytes <= c->ws_cap) return VDF_OK;

@@ -171,6 +171,24 @@ cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof, void
     return cudaGetLastError();
 }
 
+cudaError_t run_gather_records(const GatherArgs& g, const void* recs, size_t rec_bytes, cudaStream_t s, Profiler* prof,
+                               int* launches) {
+    if (g.n == 0 || g.ncols == 0) return cudaSuccess;
+    if (rec_bytes != gather_record_bytes(g.ncols)) return cudaErrorInvalidValue;
+    const unsigned char* r = static_cast<const unsigned char*>(recs);
+    const uint32_t blocks = (uint32_t)((g.n + 255) / 256);
+    if (prof) prof->begin(KC_GATHER, s);
+    switch (rec_bytes) {
+    case 16: k_gather_rec<16><<<blocks, 256, 0, s>>>(g, r); break;
+    case 32: k_gather_rec<32><<<blocks, 256, 0, s>>>(g, r); break;
+    case 48: k_gather_rec<48><<<blocks, 256, 0, s>>>(g, r); break;
+    default: k_gather_rec<64><<<blocks, 256, 0, s>>>(g, r); break;
+    }
+    if (prof) prof->end(KC_GATHER, s);
+    if (launches) *launches += 1;
+    return cudaGetLastError();
+}
+
 template <int W>
 __global__ void __launch_bounds__(256) k_broadcast(const uint32_t* row_group, uint64_t n, const void* gvals,
                                                    uint64_t n_groups, const uint32_t* perm, void* out,

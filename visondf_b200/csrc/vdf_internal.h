@@ -14,7 +14,7 @@ constexpr int kMaxGather = 8;   // columns per gather launch
 // Kernel classes for the optional per-launch timing (vdf_ctx_profile).
 enum KernelClass : int {
     KC_HIST = 0, KC_SCAN = 1, KC_ONESWEEP32 = 2, KC_ONESWEEP64 = 3, KC_GATHER = 4, KC_SEGREDUCE = 5,
-    KC_BROADCAST = 6, KC_PACK = 7, KC_SEGSCAN = 8, KC_SEGEMIT = 9, KC_COUNT = 10
+    KC_BROADCAST = 6, KC_PACK = 7, KC_SEGSCAN = 8, KC_SEGEMIT = 9, KC_TIES = 10, KC_COUNT = 11
 };
 
 // Brackets kernel launches with CUDA events when profiling is enabled.
@@ -126,6 +126,10 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
                      void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof = nullptr,
                      const uint32_t* perm_in = nullptr);
 cudaError_t prepare_sort_kernels();
+// *flag |= 1 when two neighbouring elements of a sorted key column (4- or
+// 8-byte elements) have the same bits.
+cudaError_t flag_adjacent_ties(const void* sorted_keys, int width, uint64_t n, uint32_t* flag, cudaStream_t s,
+                               Profiler* prof = nullptr);
 
 // ---- segmented sort (many independent row ranges in one set of launches) ----
 // Keys are ordered 8-byte images (the batch packs them so); a segment whose
@@ -175,6 +179,11 @@ size_t gather_record_bytes(int ncols);
 // launched.
 cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof = nullptr, void* rec_ws = nullptr,
                        size_t rec_ws_bytes = 0, int* launches = nullptr);
+// The second half of the packed gather, for callers that wrote the records
+// themselves: recs holds g.n records of gather_record_bytes(g.ncols) bytes
+// (8-byte slots in column order, 4-byte values zero-extended); g.src unused.
+cudaError_t run_gather_records(const GatherArgs& g, const void* recs, size_t rec_bytes, cudaStream_t s,
+                               Profiler* prof = nullptr, int* launches = nullptr);
 
 // ---- segmented reduction (group-by over sorted rows) -----------------------
 // A column of rows in key order.

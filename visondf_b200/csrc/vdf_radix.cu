@@ -22,6 +22,8 @@
 // raw sorted keys; no transformed copy of a column is ever materialised.
 // Multi-key sorts run least-significant key first; the first pass of each
 // later key reads its raw column through the current permutation.
+#include <algorithm>
+
 #include "vdf_common.cuh"
 #include "vdf_internal.h"
 
@@ -30,9 +32,11 @@ namespace vdf {
 // ---------------------------------------------------------------------------
 // 1. all-digit histogram
 // ---------------------------------------------------------------------------
-// Digit widths are per column (8 or 11 bits), so the shifts and masks are
-// runtime values; the histograms of all passes sit back to back in shared
-// memory.
+// Digit widths are per column (8 or 11 bits).  FIXED_BITS = 8 compiles the
+// shifts and masks for plans whose keys all use 8-bit digits; 0 reads each
+// column's width at run time.  The histograms of all passes sit back to back
+// in shared memory.
+template <int FIXED_BITS>
 __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
     extern __shared__ uint32_t sh_hist[];  // [hist_words]
     for (int i = threadIdx.x; i < a.hist_words; i += blockDim.x) sh_hist[i] = 0;
@@ -44,7 +48,8 @@ __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
         const HistCol col = a.col[c];
         uint32_t* h = sh_hist + col.hist_off;
         const int w = dtype_width(col.dtype);
-        const uint32_t bits = (uint32_t)col.bits, radix = 1u << bits, mask = radix - 1;
+        const uint32_t bits = FIXED_BITS ? (uint32_t)FIXED_BITS : (uint32_t)col.bits;
+        const uint32_t radix = 1u << bits, mask = radix - 1;
         if (w == 4) {
             const uint32_t* src = static_cast<const uint32_t*>(col.data);
             for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
@@ -285,10 +290,16 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     // (that buffer's previous user, the pass before this one, has finished).
     // Rows tile, tile + gridDim.x, ... so that every row a later pass with
     // more tiles could read is cleared too.
-    if (a.status_next)
-        for (uint32_t r = tile; r < a.status_rows; r += gridDim.x)
-            for (uint32_t b = tid; b < a.status_row_words; b += THREADS)
-                a.status_next[(size_t)r * a.status_row_words + b] = 0;
+    if (a.status_next) {
+        if (a.status_row_words == RADIX) {  // every pass of the plan has this radix
+            for (uint32_t r = tile; r < a.status_rows; r += gridDim.x)
+                for (int b = tid; b < RADIX; b += THREADS) a.status_next[(size_t)r * RADIX + b] = 0;
+        } else {
+            for (uint32_t r = tile; r < a.status_rows; r += gridDim.x)
+                for (uint32_t b = tid; b < a.status_row_words; b += THREADS)
+                    a.status_next[(size_t)r * a.status_row_words + b] = 0;
+        }
+    }
     if (SEG && valid == 0) return;  // segment finished in an earlier pass
 
     // ---- warp-local ranks and per-warp digit counts --------------------------
@@ -404,8 +415,51 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     // round trip per window), adds counts from the nearest one backwards and
     // stops at the first inclusive prefix.  A thread owning several bins (wide
     // digits) issues the windows of all its unfinished bins together.
-    constexpr int LB = (BPT >= 8) ? 2 : (BPT >= 4 ? 4 : 8);
-    {
+    const int64_t lo = first_tile;
+    if constexpr (BPT == 1) {
+        constexpr int LB = 8;
+        const int b = tid;
+        if (b < RADIX) {
+            uint32_t excl = 0;
+            if (tile > first_tile) {
+                int64_t p = (int64_t)tile - 1;
+                uint32_t spins = 0;
+                bool done = false;
+                while (!done) {
+                    uint32_t sw[LB];
+#pragma unroll
+                    for (int w = 0; w < LB; ++w)
+                        sw[w] = (p - w >= lo) ? ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b) : ST_INC;
+#pragma unroll
+                    for (int w = 0; w < LB; ++w) {
+                        if (done) break;
+                        uint32_t st = sw[w];
+                        while ((st & ~ST_CNT) == 0) {  // not yet published: wait for this one
+                            if (++spins > kSpinLimit) {
+                                atomicOr(a.err, ERR_LOOKBACK_TIMEOUT);
+                                st = ST_INC;
+                                break;
+                            }
+                            backoff(spins);
+                            st = ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b);
+                        }
+                        excl += st & ST_CNT;
+                        if (st & ST_INC) done = true;
+                    }
+                    p -= LB;
+                    if (p < lo) done = true;
+                }
+                st_relaxed_u32(a.status + (size_t)tile * RADIX + b, ST_INC | (excl + tot[0]));
+            }
+            uint32_t base;
+            if constexpr (SEG)
+                base = (uint32_t)a.segs[seg].row_start + a.seg_offs[(size_t)seg * a.seg_stride + a.pass * RADIX + b];
+            else
+                base = a.bin_offsets[b];
+            bglob[b] = base + excl - bstart[0];
+        }
+    } else {
+        constexpr int LB = (BPT >= 8) ? 2 : 4;
         uint32_t excl[BPT];
         bool done[BPT];
 #pragma unroll
@@ -413,7 +467,6 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
             excl[k] = 0;
             done[k] = (tile == first_tile) || (tid * BPT + k >= RADIX);
         }
-        const int64_t lo = first_tile;
         int64_t p = (int64_t)tile - 1;
         uint32_t spins = 0;
         bool all_done = false;
@@ -708,7 +761,10 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
         uint32_t grid = (uint32_t)(want < (uint64_t)sms * 4 ? want : (uint64_t)sms * 4);
         if (grid == 0) grid = 1;
         if (prof) prof->begin(KC_HIST, s);
-        k_digit_hist<<<grid, 512, smem, s>>>(h);
+        bool all8 = true;
+        for (int k = 0; k < p.nkeys; ++k) all8 = all8 && p.bits[k] == 8;
+        if (all8) k_digit_hist<8><<<grid, 512, smem, s>>>(h);
+        else k_digit_hist<0><<<grid, 512, smem, s>>>(h);
         if (prof) prof->end(KC_HIST, s);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         if (prof) prof->begin(KC_SCAN, s);
@@ -879,6 +935,36 @@ cudaError_t run_seg_sort(const SegSortArgs& sa, unsigned char* ws, cudaStream_t 
     return cudaSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// equal neighbours in a sorted column
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256) k_adjacent_ties(const T* keys, uint64_t n, uint32_t* flag) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    bool eq = false;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += stride)
+        eq = eq || (__ldg(keys + i) == __ldg(keys + i - 1));
+    if (__any_sync(0xffffffffu, eq) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
+cudaError_t flag_adjacent_ties(const void* sorted_keys, int width, uint64_t n, uint32_t* flag, cudaStream_t s,
+                               Profiler* prof) {
+    if (n < 2) return cudaSuccess;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint64_t want = (n + 255) / 256;
+    const uint32_t grid = (uint32_t)std::min<uint64_t>(want, (uint64_t)sms * 16);
+    if (prof) prof->begin(KC_TIES, s);
+    if (width == 8)
+        k_adjacent_ties<unsigned long long><<<grid, 256, 0, s>>>(static_cast<const unsigned long long*>(sorted_keys),
+                                                                 n, flag);
+    else
+        k_adjacent_ties<uint32_t><<<grid, 256, 0, s>>>(static_cast<const uint32_t*>(sorted_keys), n, flag);
+    if (prof) prof->end(KC_TIES, s);
+    return cudaGetLastError();
+}
+
 // Raises the dynamic shared-memory limit of every sort kernel on the current
 // device; called once per device before the first sort.
 cudaError_t prepare_sort_kernels() {
@@ -900,7 +986,10 @@ cudaError_t prepare_sort_kernels() {
     }
     // all histograms of a sort in shared memory: at most 4 keys x 6 passes x
     // 2048 bins (11-bit digits) or 4 x 8 x 256 (8-bit)
-    return cudaFuncSetAttribute(k_digit_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(k_digit_hist<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         kMaxKeys * 8 * 256 * 4);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_digit_hist<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 kMaxKeys * 6 * kMaxRadix * 4);
 }
 
