@@ -311,36 +311,44 @@ def served_section(args, local_rank: int) -> dict:
                                       vals=[v1[o:o + n], v2[o:o + n]], need_bytes=n * per_row_out))
         return reqs
 
-    # both executors write into preallocated outputs (no allocation per batch or call)
+    # batched: the library's request loop (C++ scheduler thread, two batches
+    # in flight); per call: one vdf_sort_groupby per request, one at a time,
+    # into preallocated outputs
     vdts = [torch.float64, torch.int64]
-    batched_ex = serve.BatchExecutor(local_rank, slots=2, max_batch_rows=max_rows, val_dtypes=vdts)
+    server = serve.Server(local_rank, budget_bytes=budget, resident_bytes=resident, slots=2,
+                          max_batch_rows=max_rows, val_dtypes=vdts)
     per_call_ex = serve.PerCallExecutor(local_rank, reuse_outputs=(table_rows, torch.int32, vdts))
     per_call_ex.ctx.reserve(serve.WS_BYTES_PER_ROW * table_rows)
 
-    def run(ex, reqs, single):
-        loop = serve.Loop(ex, budget, resident + ex.reserved_bytes, max_batch_rows=max_rows,
-                          max_batch_queries=1 if single else 4096)
-        st = loop.run(reqs)
+    def run(which, reqs):
+        if which == "batched":
+            st = serve.serve_trace(server, reqs)
+        else:
+            loop = serve.Loop(per_call_ex, budget, resident + per_call_ex.reserved_bytes, max_batch_rows=max_rows,
+                              max_batch_queries=1)
+            st = loop.run(reqs)
         for r in reqs:
             r.result = None
         return st
 
     nreq = args.served_requests
-    # warm both paths (kernels, workspaces, allocator)
-    run(batched_ex, make_trace(1e9, 64, 7), False)
-    run(per_call_ex, make_trace(1e9, 16, 7), True)
+    # warm both paths (kernels, workspaces, allocator pools)
+    run("batched", make_trace(1e9, 64, 7))
+    run("per_call", make_trace(1e9, 16, 7))
     torch.cuda.synchronize()
     # capacity: every request waiting at t = 0
-    cap_b = run(batched_ex, make_trace(1e12, nreq, 0), False)
-    cap_p = run(per_call_ex, make_trace(1e12, nreq, 0), True)
+    cap_b = run("batched", make_trace(1e12, nreq, 0))
+    cap_p = run("per_call", make_trace(1e12, nreq, 0))
     mean_rows = cap_b.rows / cap_b.requests
     rates = []
     for frac in args.served_fractions:
         rate = frac * cap_b.rows_per_s / mean_rows
-        sb = run(batched_ex, make_trace(rate, nreq, 1), False)
-        sp = run(per_call_ex, make_trace(rate, nreq, 1), True)
+        sb = run("batched", make_trace(rate, nreq, 1))
+        sp = run("per_call", make_trace(rate, nreq, 1))
         rates.append({"fraction_of_batched_capacity": frac, "requests_per_s": rate,
                       "offered_rows_per_s": rate * mean_rows, "batched": sb.as_dict(), "per_call": sp.as_dict()})
+    server_stats = server.stats()
+    server.close()
     del key, v1, v2
     torch.cuda.empty_cache()
     return {
@@ -348,6 +356,10 @@ def served_section(args, local_rank: int) -> dict:
                     f"int32 key over min(10,000, rows) values + f64 + int64 values, slices of a resident "
                     f"{table_rows:,}-row table; sort + group-by count/sum/min/max/mean per request",
         "hbm_budget_bytes": budget, "resident_bytes": resident, "slots": 2,
+        "batched_impl": "vdf_server_* (C++ scheduler thread: admission by HBM budget, continuous batching, "
+                        "2 batches in flight)",
+        "per_call_impl": "one vdf_sort_groupby call per request, one at a time, group count read back",
+        "server_stats": server_stats,
         "capacity": {"batched_rows_per_s": cap_b.rows_per_s, "per_call_rows_per_s": cap_p.rows_per_s,
                      "speedup": cap_b.rows_per_s / cap_p.rows_per_s,
                      "batched": cap_b.as_dict(), "per_call": cap_p.as_dict()},

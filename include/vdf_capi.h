@@ -412,6 +412,73 @@ vdf_status vdf_batch_launch(vdf_batch* batch, void* stream);
 vdf_status vdf_batch_launch_graph(vdf_batch* batch, void* stream);
 void vdf_batch_destroy(vdf_batch* batch);
 
+/* ---- request loop (serving) -------------------------------------------------
+ * Sort + group-by requests over device-resident columns, submitted and polled
+ * by id.  A scheduler thread admits requests first-come first-served while the
+ * device memory they hold (their output arenas) fits the HBM budget, and runs
+ * them with continuous batching: whenever one of `slots` execution slots (a
+ * context with its own stream and a workspace reserved for max_batch_rows
+ * rows) is free, every admitted waiting request, up to the batch limits, joins
+ * one batch (vdf_batch_*); batches of different slots overlap on the device.
+ * A request's columns must stay valid until it is done; its results (device
+ * pointers into the batch's outputs) stay valid until vdf_server_release.
+ * No counterpart in the reference (one sort_by_mt + transform_group_by call per
+ * query). */
+typedef struct vdf_server_config {
+    int32_t device;
+    uint64_t hbm_budget_bytes;  /* everything the server holds + resident_bytes */
+    uint64_t resident_bytes;    /* the caller's resident columns, counted against the budget */
+    uint32_t slots;             /* batches in flight (1..8) */
+    uint64_t max_batch_rows;
+    uint32_t max_batch_queries;
+    int32_t nvals;              /* value columns per request, same dtypes for all */
+    int32_t val_dtypes[VDF_BATCH_MAX_VALS];
+    int32_t use_default_tuning; /* else the three fields below (vdf_batch_tuning) */
+    uint32_t small_rows;
+    int32_t small_bits;
+    int32_t seg_variant;
+    int32_t use_graph;          /* launch each batch as a captured CUDA graph */
+} vdf_server_config;
+
+typedef struct vdf_server_result {
+    uint64_t n, n_groups;
+    const uint32_t* perm;       /* n sorted row ids */
+    const void* group_keys;     /* n_groups keys, the request's key dtype */
+    const int64_t* group_count; /* n_groups */
+    vdf_agg_out aggs[VDF_BATCH_MAX_VALS];
+    double t_submit, t_start, t_done; /* seconds since the server was created */
+} vdf_server_result;
+
+typedef struct vdf_server_stats {
+    uint64_t batches, completed, queued;
+    uint64_t in_use_bytes, max_in_use_bytes, fixed_bytes;
+} vdf_server_stats;
+
+typedef struct vdf_server vdf_server;
+
+/* States reported by vdf_server_poll. */
+#define VDF_REQ_QUEUED 0
+#define VDF_REQ_RUNNING 1
+#define VDF_REQ_DONE 2
+#define VDF_REQ_FAILED 3
+
+vdf_status vdf_server_default_config(vdf_server_config* cfg);
+vdf_status vdf_server_create(const vdf_server_config* cfg, vdf_server** out);
+/* Queues a request; VDF_ERR_OOM if it could never fit the budget,
+ * VDF_ERR_UNSUPPORTED above max_batch_rows rows. */
+vdf_status vdf_server_submit(vdf_server* srv, const vdf_batch_query* query, uint64_t* request_id);
+/* Current state; with out, the result once done (timestamps always). */
+vdf_status vdf_server_poll(vdf_server* srv, uint64_t request_id, int32_t* state, vdf_server_result* out);
+/* Blocks until the request is done or failed (VDF_ERR_TIMEOUT after timeout_s). */
+vdf_status vdf_server_wait(vdf_server* srv, uint64_t request_id, double timeout_s, vdf_server_result* out);
+/* Gives the request's result memory back (once every request of its batch
+ * is released, the batch's outputs return to the allocator). */
+vdf_status vdf_server_release(vdf_server* srv, uint64_t request_id);
+vdf_status vdf_server_read_stats(vdf_server* srv, vdf_server_stats* out);
+const char* vdf_server_last_error(vdf_server* srv);
+/* Stops the scheduler after the batches in flight and frees everything. */
+void vdf_server_destroy(vdf_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

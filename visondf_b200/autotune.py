@@ -58,26 +58,33 @@ def tune(ctx: "_lib.Context", run: Callable[[], None], reps: int = 2) -> dict:
     v32 = [v["index"] for v in variants if v["key_width"] == 4]
     v64 = [v["index"] for v in variants if v["key_width"] == 8]
     ms32, ms64 = {}, {}
-    run()  # warm the workspace and the kernels
-    for i in range(max(len(v32), len(v64))):
-        a, b = v32[i % len(v32)], v64[i % len(v64)]
-        ctx.set_sort_tuning(a, b)
-        run()
-        ctx.profile(True)
-        ctx.profile_reset()
-        for _ in range(reps):
+    saved = ctx.get_sort_tuning()
+    # every key's passes run in the LSD mode, so both widths get timed (the
+    # primary-key-first mode may skip the other keys' passes)
+    mode = ctx.get_multikey_mode()
+    ctx.set_multikey_mode(_lib.MULTIKEY_LSD)
+    try:
+        run()  # warm the workspace and the kernels
+        for i in range(max(len(v32), len(v64))):
+            a, b = v32[i % len(v32)], v64[i % len(v64)]
+            ctx.set_sort_tuning(a, b)
             run()
-        prof = ctx.profile_read()
-        ctx.profile(False)
-        t32, c32 = prof["onesweep32"]
-        t64, c64 = prof["onesweep64"]
-        if c32:
-            ms32[a] = min(ms32.get(a, math.inf), t32 / reps)
-        if c64:
-            ms64[b] = min(ms64.get(b, math.inf), t64 / reps)
-    cur = ctx.get_sort_tuning()
-    best32 = min(ms32, key=ms32.get) if ms32 else cur[0]
-    best64 = min(ms64, key=ms64.get) if ms64 else cur[1]
+            ctx.profile(True)
+            ctx.profile_reset()
+            for _ in range(reps):
+                run()
+            prof = ctx.profile_read()
+            ctx.profile(False)
+            t32, c32 = prof["onesweep32"]
+            t64, c64 = prof["onesweep64"]
+            if c32:
+                ms32[a] = min(ms32.get(a, math.inf), t32 / reps)
+            if c64:
+                ms64[b] = min(ms64.get(b, math.inf), t64 / reps)
+    finally:
+        ctx.set_multikey_mode(mode)
+    best32 = min(ms32, key=ms32.get) if ms32 else saved[0]  # a width not timed keeps its choice
+    best64 = min(ms64, key=ms64.get) if ms64 else saved[1]
     ctx.set_sort_tuning(best32, best64)
     return {"variant32": best32, "variant64": best64, "ms32": ms32, "ms64": ms64}
 

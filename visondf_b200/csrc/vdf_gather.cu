@@ -127,6 +127,103 @@ __global__ void __launch_bounds__(256) k_gather_rec(GatherArgs g, const unsigned
     }
 }
 
+// Four consecutive output rows per thread: one 16-byte load of their row ids,
+// then all their record reads issued back to back (four times the random
+// reads in flight per thread of k_gather_rec: the reads are latency-bound
+// when the records span gigabytes), then 16/32-byte stores per column.
+// Needs perm and every output column 16-byte aligned.
+template <int REC>
+__global__ void __launch_bounds__(256) k_gather_rec4(GatherArgs g, const unsigned char* recs) {
+    constexpr int SLOTS = REC / 8;
+    const uint64_t r0 = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;
+    if (r0 >= g.n) return;
+    if (r0 + 4 <= g.n) {
+        uint4 p4 = ldg_stream(reinterpret_cast<const uint4*>(g.perm + r0));
+        uint32_t p[4] = {p4.x, p4.y, p4.z, p4.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (p[k] >= g.n) {  // not a permutation of [0, n)
+                if (g.err) atomicOr(g.err, ERR_BAD_INDEX);
+                p[k] = 0;
+            }
+        unsigned long long slot[4][SLOTS];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const ulonglong2* src = reinterpret_cast<const ulonglong2*>(recs + (uint64_t)p[k] * REC);
+#pragma unroll
+            for (int c = 0; c < SLOTS; c += 2) {
+                const ulonglong2 v = __ldcg(src + c / 2);
+                slot[k][c] = v.x;
+                slot[k][c + 1] = v.y;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < SLOTS; ++c) {
+            if (c >= g.ncols) break;
+            if (g.width[c] == 8) {
+                ulonglong2* d = reinterpret_cast<ulonglong2*>(static_cast<unsigned long long*>(g.dst[c]) + r0);
+                stg_stream(d, make_ulonglong2(slot[0][c], slot[1][c]));
+                stg_stream(d + 1, make_ulonglong2(slot[2][c], slot[3][c]));
+            } else {
+                uint4 v = make_uint4((uint32_t)slot[0][c], (uint32_t)slot[1][c], (uint32_t)slot[2][c],
+                                     (uint32_t)slot[3][c]);
+                stg_stream(reinterpret_cast<uint4*>(static_cast<uint32_t*>(g.dst[c]) + r0), v);
+            }
+        }
+        return;
+    }
+    for (uint64_t r = r0; r < g.n; ++r) {
+        uint32_t p = ldg_stream(g.perm + r);
+        if (p >= g.n) {
+            if (g.err) atomicOr(g.err, ERR_BAD_INDEX);
+            p = 0;
+        }
+        const ulonglong2* src = reinterpret_cast<const ulonglong2*>(recs + (uint64_t)p * REC);
+        unsigned long long slot[SLOTS];
+#pragma unroll
+        for (int c = 0; c < SLOTS; c += 2) {
+            const ulonglong2 v = __ldcg(src + c / 2);
+            slot[c] = v.x;
+            slot[c + 1] = v.y;
+        }
+#pragma unroll
+        for (int c = 0; c < SLOTS; ++c) {
+            if (c >= g.ncols) break;
+            if (g.width[c] == 8) stg_stream(static_cast<unsigned long long*>(g.dst[c]) + r, slot[c]);
+            else stg_stream(static_cast<uint32_t*>(g.dst[c]) + r, (uint32_t)slot[c]);
+        }
+    }
+}
+
+namespace {
+bool aligned16(const GatherArgs& g) {
+    bool ok = (reinterpret_cast<uintptr_t>(g.perm) & 15) == 0;
+    for (int c = 0; c < g.ncols; ++c) ok = ok && (reinterpret_cast<uintptr_t>(g.dst[c]) & 15) == 0;
+    return ok;
+}
+
+cudaError_t launch_gather_rec(const GatherArgs& g, const unsigned char* recs, size_t rec, cudaStream_t s) {
+    if (aligned16(g)) {
+        const uint32_t blocks = (uint32_t)(((g.n + 3) / 4 + 255) / 256);
+        switch (rec) {
+        case 16: k_gather_rec4<16><<<blocks, 256, 0, s>>>(g, recs); break;
+        case 32: k_gather_rec4<32><<<blocks, 256, 0, s>>>(g, recs); break;
+        case 48: k_gather_rec4<48><<<blocks, 256, 0, s>>>(g, recs); break;
+        default: k_gather_rec4<64><<<blocks, 256, 0, s>>>(g, recs); break;
+        }
+    } else {
+        const uint32_t blocks = (uint32_t)((g.n + 255) / 256);
+        switch (rec) {
+        case 16: k_gather_rec<16><<<blocks, 256, 0, s>>>(g, recs); break;
+        case 32: k_gather_rec<32><<<blocks, 256, 0, s>>>(g, recs); break;
+        case 48: k_gather_rec<48><<<blocks, 256, 0, s>>>(g, recs); break;
+        default: k_gather_rec<64><<<blocks, 256, 0, s>>>(g, recs); break;
+        }
+    }
+    return cudaGetLastError();
+}
+}  // namespace
+
 size_t gather_record_bytes(int ncols) {
     return (ncols >= 2 && ncols <= kMaxGather) ? (size_t)16 * ((ncols + 1) / 2) : 0;
 }
@@ -149,15 +246,10 @@ cudaError_t run_gather(const GatherArgs& g, cudaStream_t s, Profiler* prof, void
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         if (prof) prof->begin(KC_GATHER, s);
-        switch (rec) {
-        case 16: k_gather_rec<16><<<blocks, 256, 0, s>>>(g, recs); break;
-        case 32: k_gather_rec<32><<<blocks, 256, 0, s>>>(g, recs); break;
-        case 48: k_gather_rec<48><<<blocks, 256, 0, s>>>(g, recs); break;
-        default: k_gather_rec<64><<<blocks, 256, 0, s>>>(g, recs); break;
-        }
+        e = launch_gather_rec(g, recs, rec, s);
         if (prof) prof->end(KC_GATHER, s);
         if (launches) *launches += 2;
-        return cudaGetLastError();
+        return e;
     }
     if (launches) *launches += 1;
     bool vec = (reinterpret_cast<uintptr_t>(g.perm) & 15) == 0;
@@ -176,17 +268,11 @@ cudaError_t run_gather_records(const GatherArgs& g, const void* recs, size_t rec
     if (g.n == 0 || g.ncols == 0) return cudaSuccess;
     if (rec_bytes != gather_record_bytes(g.ncols)) return cudaErrorInvalidValue;
     const unsigned char* r = static_cast<const unsigned char*>(recs);
-    const uint32_t blocks = (uint32_t)((g.n + 255) / 256);
     if (prof) prof->begin(KC_GATHER, s);
-    switch (rec_bytes) {
-    case 16: k_gather_rec<16><<<blocks, 256, 0, s>>>(g, r); break;
-    case 32: k_gather_rec<32><<<blocks, 256, 0, s>>>(g, r); break;
-    case 48: k_gather_rec<48><<<blocks, 256, 0, s>>>(g, r); break;
-    default: k_gather_rec<64><<<blocks, 256, 0, s>>>(g, r); break;
-    }
+    cudaError_t e = launch_gather_rec(g, r, rec_bytes, s);
     if (prof) prof->end(KC_GATHER, s);
     if (launches) *launches += 1;
-    return cudaGetLastError();
+    return e;
 }
 
 template <int W>

@@ -189,6 +189,19 @@ constexpr uint32_t ST_AGG = 1u << 30;
 constexpr uint32_t ST_INC = 2u << 30;
 constexpr uint32_t ST_CNT = (1u << 30) - 1;
 
+// Digit of a key at bit `shift`.  8-bit digits of 8-byte keys never straddle
+// the two 32-bit halves, so the digit comes from the half that holds it.
+template <typename K, int BITS>
+__device__ __forceinline__ uint32_t digit_of(K key, uint32_t shift) {
+    constexpr uint32_t MASK = (1u << BITS) - 1;
+    if constexpr (sizeof(K) == 8 && BITS == 8) {
+        const uint32_t w = (shift >= 32) ? (uint32_t)(key >> 32) : (uint32_t)key;
+        return (w >> (shift & 31)) & MASK;
+    } else {
+        return (uint32_t)(key >> shift) & MASK;
+    }
+}
+
 template <typename K, int BITS, int THREADS, int ITEMS>
 struct OnesweepCfg {
     static constexpr int RADIX = 1 << BITS;
@@ -217,7 +230,6 @@ template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL,
 __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     using C = OnesweepCfg<K, BITS, THREADS, ITEMS>;
     constexpr int RADIX = C::RADIX, WARPS = C::WARPS, TILE = C::TILE, BPT = C::BPT;
-    constexpr uint32_t MASK = RADIX - 1;
     extern __shared__ __align__(16) unsigned char smem[];
     K* ex_keys = reinterpret_cast<K*>(smem);
     uint32_t* ex_vals = reinterpret_cast<uint32_t*>(smem + C::KEY_BYTES);
@@ -304,24 +316,24 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
 
     // ---- warp-local ranks and per-warp digit counts --------------------------
     // First the lanes holding the same digit are found for every item (one
-    // ballot per digit bit plus one for validity, or match.any); these are
-    // independent and overlap.  Then the warp's per-digit counters advance
-    // item by item (the lowest lane of each peer group updates it), which is
-    // the only serial part.
+    // ballot per digit bit, or match.any); these are independent and
+    // overlap.  Then the warp's per-digit counters advance item by item (the
+    // lowest lane of each peer group adds the group's size), which is the
+    // only serial part.  Slots past the end of the last tile hold all-ones
+    // keys, whose digit is the largest in every pass: ranked like any key,
+    // they come after every real key of that digit (their positions are
+    // last), so they fill the tile's last slots and are never written out.
     uint32_t rank[ITEMS];
     uint32_t peers[ITEMS];
     uint32_t* my_cnt = wcnt + warp * RADIX;
     const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t pos = wpos + j * 32 + lane;
-        const bool ok = pos < valid;
-        const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
+        const uint32_t d = digit_of<K, BITS>(key[j], a.shift);
         if (MATCH == 1 || (MATCH == 2 && (j & 1) == 0)) {
-            peers[j] = __match_any_sync(0xffffffffu, ok ? d : (uint32_t)RADIX);
+            peers[j] = __match_any_sync(0xffffffffu, d);
         } else {
-            uint32_t pm = __ballot_sync(0xffffffffu, ok);
-            if (!ok) pm = ~pm;
+            uint32_t pm = 0xffffffffu;
 #pragma unroll
             for (int b = 0; b < BITS; ++b) {
                 const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
@@ -332,18 +344,13 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     }
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t pos = wpos + j * 32 + lane;
-        const bool ok = pos < valid;
-        const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
+        const uint32_t d = digit_of<K, BITS>(key[j], a.shift);
         const int leader = __ffs(peers[j]) - 1;
         uint32_t base = 0;
-        if (lane == leader && ok) {
-            base = my_cnt[d];
-            my_cnt[d] = base + __popc(peers[j]);
-        }
-        __syncwarp();
+        if (lane == leader) base = atomicAdd(&my_cnt[d], (uint32_t)__popc(peers[j]));
+        __syncwarp();  // the next item's leaders see this item's counts
         base = __shfl_sync(0xffffffffu, base, leader);
-        rank[j] = ok ? base + __popc(peers[j] & lt) : pos;
+        rank[j] = base + __popc(peers[j] & lt);
     }
     __syncthreads();
 
@@ -398,13 +405,11 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     // (overlaps the look-back below: other warps' global writes wait on it)
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t pos = wpos + j * 32 + lane;
-        const uint32_t d = (uint32_t)((key[j] >> a.shift) & MASK);
-        uint32_t r = rank[j];
-        if (pos < valid) r += wcnt[warp * RADIX + d];
+        const uint32_t d = digit_of<K, BITS>(key[j], a.shift);
+        uint32_t r = rank[j] + wcnt[warp * RADIX + d];
         if (r >= (uint32_t)TILE) {  // never when the counts are consistent
             atomicOr(a.err, ERR_BAD_INDEX);
-            r = pos;
+            r = wpos + j * 32 + lane;
         }
         ex_keys[r] = key[j];
         ex_vals[r] = val[j];
@@ -528,7 +533,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
         if (i < valid) {
             const K k = ex_keys[i];
             const uint32_t v = ex_vals[i];
-            const uint32_t d = (uint32_t)((k >> a.shift) & MASK);
+            const uint32_t d = digit_of<K, BITS>(k, a.shift);
             uint32_t p = bglob[d] + i;
             if (p >= n) {  // only after a look-back timeout: never write out of bounds
                 atomicOr(a.err, ERR_BAD_INDEX);

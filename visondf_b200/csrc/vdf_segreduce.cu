@@ -318,27 +318,108 @@ __device__ __forceinline__ void seg_setup(const SegArgs& a, int* vc, int* kw) {
 }
 
 // ---- phase 1: one aggregate per tile ----------------------------------------
+// A tile's aggregate is its head count plus the aggregate of its trailing
+// open segment (the rows from its last head, or all its rows if it has none).
+// So the keys are read to find the heads and the last head, and only the
+// threads whose rows lie in the trailing segment read values and fold them;
+// only warps overlapping it reduce.  With many groups (one per few rows)
+// almost no values are read here.
 template <int NK, int NV>
 __global__ void __launch_bounds__(kSegThreads) k_seg_tiles(SegArgs a, Agg<NV>* tile_agg) {
-    __shared__ Agg<NV> s_warp[kSegThreads / 32];
+    constexpr int ITEMS = kSegItems, WARPS = kSegThreads / 32;
+    __shared__ Agg<NV> s_warp[WARPS];
+    __shared__ uint32_t s_heads[WARPS];
+    __shared__ int s_last[WARPS];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const uint64_t row0 = (uint64_t)blockIdx.x * kSegTile + (uint64_t)tid * kSegItems;
+    const uint64_t n = a.n;
+    const uint64_t tile0 = (uint64_t)blockIdx.x * kSegTile;
+    const uint64_t row0 = tile0 + (uint64_t)tid * ITEMS;
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
-    uint32_t hmask;
-    Agg<NV> r = fold_rows<NK, NV>(a, row0, lane, vc, kw, hmask);
-    // ordered tree reduction: lower lanes are earlier rows
+
+    // keys and head flags
+    uint64_t key[ITEMS][NK];
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const Agg<NV> o = agg_shfl_down(r, d);
-        if (lane + d < 32) r = agg_combine(r, o, vc);
+    for (int k = 0; k < NK; ++k) load_rows<ITEMS>(a.key[k].src, kw[k], row0, n, key, k);
+    uint64_t prev[NK];
+#pragma unroll
+    for (int k = 0; k < NK; ++k) prev[k] = __shfl_up_sync(0xffffffffu, key[ITEMS - 1][k], 1);
+    if (lane == 0 && row0 > 0 && row0 < n) {
+#pragma unroll
+        for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], row0 - 1);
     }
-    if (lane == 0) s_warp[warp] = r;
+    uint32_t hmask = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint64_t r = row0 + j;
+        bool h = (r == 0);
+#pragma unroll
+        for (int k = 0; k < NK; ++k) h |= (j == 0 ? prev[k] : key[j - 1][k]) != key[j][k];
+        if (r < n && h) hmask |= 1u << j;
+    }
+    // head count and the last head (row within the tile, -1 for none)
+    uint32_t heads = __popc(hmask);
+    int last = hmask ? tid * ITEMS + (31 - __clz(hmask)) : -1;
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+        heads += __shfl_down_sync(0xffffffffu, heads, d);
+        last = max(last, __shfl_down_sync(0xffffffffu, last, d));
+    }
+    if (lane == 0) {
+        s_heads[warp] = heads;
+        s_last[warp] = last;
+    }
+    __syncthreads();
+    uint32_t tile_heads = 0;
+    int tile_last = -1;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+        tile_heads += s_heads[w];
+        tile_last = max(tile_last, s_last[w]);
+    }
+    const int from = tile_last >= 0 ? tile_last : 0;  // first row of the trailing segment
+
+    // fold this thread's rows of the trailing segment
+    Agg<NV> t = agg_identity<NV>();
+    if (tid * ITEMS + ITEMS - 1 >= from && row0 < n) {
+        uint64_t val[ITEMS][NV > 0 ? NV : 1];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (row0 + j >= n || tid * ITEMS + j < from) continue;
+            if (t.cnt == 0) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) col_init(t.w[v], val[j][v], vc[v]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    uint64_t one[4];
+                    col_init(one, val[j][v], vc[v]);
+                    col_merge(t.w[v], one, vc[v]);
+                }
+            }
+            t.cnt++;
+        }
+    }
+    // ordered reduction over the warps that hold trailing rows (lower lanes
+    // are earlier rows; heads stay 0, so the combine merges)
+    const bool active = (warp + 1) * 32 * ITEMS - 1 >= from;
+    if (active) {
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const Agg<NV> o = agg_shfl_down(t, d);
+            if (lane + d < 32) t = agg_combine(t, o, vc);
+        }
+        if (lane == 0) s_warp[warp] = t;
+    }
     __syncthreads();
     if (tid == 0) {
-        Agg<NV> t = s_warp[0];
-        for (int w = 1; w < kSegThreads / 32; ++w) t = agg_combine(t, s_warp[w], vc);
-        tile_agg[blockIdx.x] = t;
+        Agg<NV> r = agg_identity<NV>();
+        for (int w = 0; w < WARPS; ++w)
+            if ((w + 1) * 32 * ITEMS - 1 >= from) r = agg_combine(r, s_warp[w], vc);
+        r.heads = tile_heads;
+        tile_agg[blockIdx.x] = r;
     }
 }
 

@@ -285,3 +285,237 @@ class PerCallExecutor:
 
 def request_bytes(rows: int, val_is_float: Sequence[bool]) -> int:
     return rows * out_bytes_per_row(val_is_float)
+
+
+# ---------------------------------------------------------------------------
+# The library's own request loop (vdf_server_*): the scheduler thread runs in
+# C++; this is its Python view and a trace client for it.
+# ---------------------------------------------------------------------------
+def _server_lib():
+    import ctypes as C
+
+    from . import _lib
+
+    lib = _lib.lib
+    if getattr(lib, "_server_bound", False):
+        return lib, _lib
+
+    class Config(C.Structure):
+        _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_uint64), ("resident_bytes", C.c_uint64),
+                    ("slots", C.c_uint32), ("max_batch_rows", C.c_uint64), ("max_batch_queries", C.c_uint32),
+                    ("nvals", C.c_int32), ("val_dtypes", C.c_int32 * _lib.BATCH_MAX_VALS),
+                    ("use_default_tuning", C.c_int32), ("small_rows", C.c_uint32), ("small_bits", C.c_int32),
+                    ("seg_variant", C.c_int32), ("use_graph", C.c_int32)]
+
+    class Result(C.Structure):
+        _fields_ = [("n", C.c_uint64), ("n_groups", C.c_uint64), ("perm", C.c_void_p), ("group_keys", C.c_void_p),
+                    ("group_count", C.c_void_p), ("aggs", _lib.vdf_agg_out * _lib.BATCH_MAX_VALS),
+                    ("t_submit", C.c_double), ("t_start", C.c_double), ("t_done", C.c_double)]
+
+    class Stats(C.Structure):
+        _fields_ = [("batches", C.c_uint64), ("completed", C.c_uint64), ("queued", C.c_uint64),
+                    ("in_use_bytes", C.c_uint64), ("max_in_use_bytes", C.c_uint64), ("fixed_bytes", C.c_uint64)]
+
+    vp, st = C.c_void_p, C.c_int
+    for name, res, args in [
+        ("vdf_server_default_config", st, [C.POINTER(Config)]),
+        ("vdf_server_create", st, [C.POINTER(Config), C.POINTER(vp)]),
+        ("vdf_server_submit", st, [vp, C.POINTER(_lib.vdf_batch_query), C.POINTER(C.c_uint64)]),
+        ("vdf_server_poll", st, [vp, C.c_uint64, C.POINTER(C.c_int32), C.POINTER(Result)]),
+        ("vdf_server_wait", st, [vp, C.c_uint64, C.c_double, C.POINTER(Result)]),
+        ("vdf_server_release", st, [vp, C.c_uint64]),
+        ("vdf_server_read_stats", st, [vp, C.POINTER(Stats)]),
+        ("vdf_server_last_error", C.c_char_p, [vp]),
+        ("vdf_server_destroy", None, [vp]),
+    ]:
+        f = getattr(lib, name)
+        f.restype, f.argtypes = res, args
+    lib._server_types = (Config, Result, Stats)
+    lib._server_bound = True
+    return lib, _lib
+
+
+class _DevArray:
+    """A device buffer seen through __cuda_array_interface__ (so torch can wrap it)."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": typestr, "data": (int(ptr or 0), False),
+                                         "version": 3, "strides": None}
+
+
+def _tensor(ptr, n, dtype):
+    import numpy as np
+    import torch
+    typestr = np.dtype(str(dtype).replace("torch.", "")).str
+    if n == 0 or not ptr:
+        return torch.empty(0, dtype=dtype, device="cuda")
+    return torch.as_tensor(_DevArray(ptr, n, typestr), device="cuda")
+
+
+@dataclass
+class ServedResult:
+    perm: object
+    n_groups: int
+    keys: object
+    count: object
+    aggs: list
+    t_submit: float
+    t_start: float
+    t_done: float
+
+
+class Server:
+    """vdf_server_*: the library's request loop (admission by HBM budget,
+    continuous batching over `slots` in-flight batches)."""
+
+    def __init__(self, device: int = 0, budget_bytes: float = 150e9, resident_bytes: int = 0, slots: int = 2,
+                 max_batch_rows: int = 1 << 27, max_batch_queries: int = 4096, val_dtypes=(),
+                 tuning: Optional[dict] = None, use_graph: bool = False):
+        import ctypes as C
+
+        import torch
+        lib, _lib = _server_lib()
+        Config, _, _ = lib._server_types
+        self.lib, self._lib, self.C = lib, _lib, C
+        c = Config()
+        lib.vdf_server_default_config(C.byref(c))
+        c.device = device
+        c.hbm_budget_bytes = int(budget_bytes)
+        c.resident_bytes = int(resident_bytes)
+        c.slots = slots
+        c.max_batch_rows = int(max_batch_rows)
+        c.max_batch_queries = int(max_batch_queries)
+        self.val_dtypes = list(val_dtypes)
+        c.nvals = len(self.val_dtypes)
+        for j, dt in enumerate(self.val_dtypes):
+            c.val_dtypes[j] = _lib.TORCH_TO_VDF[dt]
+        if tuning is not None:
+            c.use_default_tuning = 0
+            c.small_rows, c.small_bits, c.seg_variant = tuning["small_rows"], tuning["small_bits"], tuning["seg_variant"]
+        c.use_graph = 1 if use_graph else 0
+        h = C.c_void_p()
+        stt = lib.vdf_server_create(C.byref(c), C.byref(h))
+        if stt != _lib.OK:
+            raise _lib.VdfError(stt, "vdf_server_create failed")
+        self.handle = h
+        self.torch = torch
+        self._keys = {}
+
+    def submit(self, key, vals) -> int:
+        q = self._lib.vdf_batch_query()
+        q.n = key.numel()
+        q.key = self._lib._col(key)
+        for j, v in enumerate(vals):
+            q.vals[j] = v.data_ptr()
+        rid = self.C.c_uint64()
+        st = self.lib.vdf_server_submit(self.handle, self.C.byref(q), self.C.byref(rid))
+        if st != self._lib.OK:
+            raise self._lib.VdfError(st, "vdf_server_submit")
+        self._keys[rid.value] = key.dtype
+        return rid.value
+
+    def _result(self, rid, r) -> ServedResult:
+        kdt = self._keys[rid]
+        aggs = []
+        for j, dt in enumerate(self.val_dtypes):
+            a = r.aggs[j]
+            fl = dt in (self.torch.float64, self.torch.float32)
+            g = r.n_groups
+            aggs.append(self._lib.AggResult(_tensor(a.sum, g, self.torch.float64 if fl else self.torch.int64),
+                                            None if fl else _tensor(a.sum_hi, g, self.torch.int64),
+                                            _tensor(a.min, g, dt), _tensor(a.max, g, dt),
+                                            _tensor(a.mean, g, self.torch.float64)))
+        return ServedResult(_tensor(r.perm, r.n, self.torch.int32), int(r.n_groups), _tensor(r.group_keys, r.n_groups, kdt),
+                            _tensor(r.group_count, r.n_groups, self.torch.int64), aggs, r.t_submit, r.t_start,
+                            r.t_done)
+
+    def poll(self, rid: int, want_result: bool = True):
+        """(state, result): state 0 queued, 1 running, 2 done; the result
+        (device tensors) once done, or just its timestamps with
+        want_result=False."""
+        _, Result, _ = self.lib._server_types
+        state = self.C.c_int32()
+        r = Result()
+        st = self.lib.vdf_server_poll(self.handle, rid, self.C.byref(state), self.C.byref(r))
+        if st != self._lib.OK:
+            raise self._lib.VdfError(st, self.lib.vdf_server_last_error(self.handle).decode())
+        if state.value != 2:
+            return state.value, None
+        if not want_result:
+            return state.value, ServedResult(None, int(r.n_groups), None, None, [], r.t_submit, r.t_start, r.t_done)
+        return state.value, self._result(rid, r)
+
+    def wait(self, rid: int, timeout: float = 120.0) -> ServedResult:
+        _, Result, _ = self.lib._server_types
+        r = Result()
+        st = self.lib.vdf_server_wait(self.handle, rid, timeout, self.C.byref(r))
+        if st != self._lib.OK:
+            raise self._lib.VdfError(st, self.lib.vdf_server_last_error(self.handle).decode())
+        return self._result(rid, r)
+
+    def release(self, rid: int):
+        self._keys.pop(rid, None)
+        st = self.lib.vdf_server_release(self.handle, rid)
+        if st != self._lib.OK:
+            raise self._lib.VdfError(st, "vdf_server_release")
+
+    def stats(self) -> dict:
+        _, _, Stats = self.lib._server_types
+        s = Stats()
+        self.lib.vdf_server_read_stats(self.handle, self.C.byref(s))
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.vdf_server_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def serve_trace(server: Server, requests: Sequence[Request], keep_results: bool = False,
+                clock: Callable[[], float] = time.perf_counter) -> TraceStats:
+    """Submits each request at its arrival time (seconds from the start),
+    releases results as they complete (or keeps them in r.result), and
+    returns the trace statistics with latencies on the server's clock."""
+    reqs = sorted(requests, key=lambda r: (r.arrival, r.rid))
+    ids = {}
+    outstanding = []
+    batches0 = int(server.stats()["batches"])
+    t0 = clock()
+    nxt = 0
+    done = 0
+    while done < len(reqs):
+        now = clock() - t0
+        while nxt < len(reqs) and reqs[nxt].arrival <= now:
+            r = reqs[nxt]
+            ids[r.rid] = server.submit(r.key, r.vals)
+            outstanding.append(r)
+            nxt += 1
+        still = []
+        for r in outstanding:
+            state, res = server.poll(ids[r.rid], want_result=keep_results)
+            if state == 2:
+                r.started, r.completed = res.t_start, res.t_done
+                r.admitted = res.t_submit
+                if keep_results:
+                    r.result = res
+                else:
+                    server.release(ids[r.rid])
+                done += 1
+            else:
+                still.append(r)
+        outstanding = still
+        if nxt < len(reqs) and not outstanding:
+            time.sleep(max(0.0, min(reqs[nxt].arrival - (clock() - t0), 0.0005)))
+    lat = [r.completed - r.admitted for r in reqs]
+    rows = sum(r.rows for r in reqs)
+    span = max(r.completed for r in reqs) - min(r.admitted for r in reqs)
+    st = server.stats()
+    return TraceStats(len(reqs), rows, span, rows / span if span > 0 else float("inf"),
+                      percentile(lat, 50) * 1e3, percentile(lat, 99) * 1e3, statistics.fmean(lat) * 1e3,
+                      int(st["batches"]) - batches0, int(st["max_in_use_bytes"]))
