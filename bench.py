@@ -204,7 +204,7 @@ def batched_section(args, local_rank: int) -> dict:
 
     dev = torch.device("cuda", local_rank)
     t0 = time.time()
-    specs = datagen.batch_specs(nq=args.batch_queries)
+    specs = datagen.batch_specs(nq=args.batch_queries, budget_bytes=args.batch_bytes)
     parts = [datagen.batch_query(s) for s in specs]
     # one resident buffer per column kind; each query's columns are slices of it
     cols = {}
@@ -227,7 +227,10 @@ def batched_section(args, local_rank: int) -> dict:
     log(f"[batched] {len(queries)} queries, {rows:,} rows, generated in {time.time() - t0:.1f}s")
     ctx = vdf.Context(local_rank)
     stream = torch.cuda.current_stream()
-    tuned = autotune.tune_batch(ctx, queries, reps=2)
+    if args.no_batch_autotune:
+        tuned = {"best": vdf._lib.default_batch_tuning(), "best_ms": float("nan"), "table": []}
+    else:
+        tuned = autotune.tune_batch(ctx, queries, reps=2)
     log(f"[batched] tuning: {tuned['best']} ({tuned['best_ms']:.2f} ms)")
     b = vdf.Batch(ctx, queries, tuned["best"])
     for _ in range(args.warmup):
@@ -572,6 +575,8 @@ def main():
                     help="extra single-GPU measurements after the headline one: batched, served (comma list, "
                          "'none' for neither)")
     ap.add_argument("--batch-queries", type=int, default=4096)
+    ap.add_argument("--no-batch-autotune", action="store_true", help="batched section: the default tuning")
+    ap.add_argument("--batch-bytes", type=int, default=2 << 30, help="batched section: key + value bytes of the batch")
     ap.add_argument("--per-call-queries", type=int, default=0, help="queries of the per-call baseline (0 = all)")
     ap.add_argument("--served-requests", type=int, default=400)
     ap.add_argument("--served-table-rows", type=int, default=100_000_000)

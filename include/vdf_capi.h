@@ -421,7 +421,9 @@ void vdf_batch_destroy(vdf_batch* batch);
  * rows) is free, every admitted waiting request, up to the batch limits, joins
  * one batch (vdf_batch_*); batches of different slots overlap on the device.
  * A request's columns must stay valid until it is done; its results (device
- * pointers into the batch's outputs) stay valid until vdf_server_release.
+ * pointers into its slot's output arenas, allocated once per slot) stay valid
+ * until vdf_server_release, and a slot takes its next batch only when every
+ * result of its previous batch has been released.
  * No counterpart in the reference (one sort_by_mt + transform_group_by call per
  * query). */
 typedef struct vdf_server_config {
@@ -452,6 +454,7 @@ typedef struct vdf_server_result {
 typedef struct vdf_server_stats {
     uint64_t batches, completed, queued;
     uint64_t in_use_bytes, max_in_use_bytes, fixed_bytes;
+    double host_start_seconds, host_finish_seconds; /* scheduler time spent planning/launching and reading back batches */
 } vdf_server_stats;
 
 typedef struct vdf_server vdf_server;

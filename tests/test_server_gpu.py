@@ -85,12 +85,16 @@ def test_request_states_and_release(ctx, table):
     srv = serve.Server(0, budget_bytes=60e9, slots=1, max_batch_rows=1 << 22, val_dtypes=VDT)
     ids = [srv.submit(key[i * 1000:(i + 1) * 1000 + i], [v1[i * 1000:(i + 1) * 1000 + i],
                                                        v2[i * 1000:(i + 1) * 1000 + i]]) for i in range(20)]
-    results = [srv.wait(i) for i in ids]
-    for i, (rid, res) in enumerate(zip(ids, results)):
+    # a slot takes its next batch once its previous batch's results are all
+    # released, so results are checked and released one by one
+    for i, rid in enumerate(ids):
+        res = srv.wait(rid)
         state, again = srv.poll(rid)
         assert state == 2 and again.n_groups == res.n_groups
         assert res.perm.numel() == 1000 + i
-    for rid in ids:
+        alone = ctx.sort_groupby([key[i * 1000:(i + 1) * 1000 + i]],
+                                 [v1[i * 1000:(i + 1) * 1000 + i], v2[i * 1000:(i + 1) * 1000 + i]], agg_cols=[0, 1])
+        assert (host(res.perm) == host(alone.perm)).all()
         srv.release(rid)
     with pytest.raises(vdf.VdfError):
         srv.release(ids[0])  # already released

@@ -247,6 +247,7 @@ struct WarpStage {
 constexpr int kSegThreads = 256;
 constexpr int kSegItems = 2;
 constexpr int kSegTile = kSegThreads * kSegItems;  // rows per tile
+constexpr int kSegTilesPerCta = 4;                  // tiles each CTA of the reduce and emit passes takes
 
 extern __shared__ __align__(16) unsigned char seg_smem[];
 
@@ -324,15 +325,22 @@ __device__ __forceinline__ void seg_setup(const SegArgs& a, int* vc, int* kw) {
 // threads whose rows lie in the trailing segment read values and fold them;
 // only warps overlapping it reduce.  With many groups (one per few rows)
 // almost no values are read here.
+template <int NV>
+struct TileSmem {
+    Agg<NV> s_warp[kSegThreads / 32];
+    uint32_t s_heads[kSegThreads / 32];
+    int s_last[kSegThreads / 32];
+};
+
 template <int NK, int NV>
-__global__ void __launch_bounds__(kSegThreads) k_seg_tiles(SegArgs a, Agg<NV>* tile_agg) {
+__device__ __forceinline__ void seg_tile_body(const SegArgs& a, Agg<NV>* tile_agg, uint32_t tile, TileSmem<NV>& sm) {
     constexpr int ITEMS = kSegItems, WARPS = kSegThreads / 32;
-    __shared__ Agg<NV> s_warp[WARPS];
-    __shared__ uint32_t s_heads[WARPS];
-    __shared__ int s_last[WARPS];
+    Agg<NV>* s_warp = sm.s_warp;
+    uint32_t* s_heads = sm.s_heads;
+    int* s_last = sm.s_last;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t n = a.n;
-    const uint64_t tile0 = (uint64_t)blockIdx.x * kSegTile;
+    const uint64_t tile0 = (uint64_t)tile * kSegTile;
     const uint64_t row0 = tile0 + (uint64_t)tid * ITEMS;
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
@@ -419,7 +427,18 @@ __global__ void __launch_bounds__(kSegThreads) k_seg_tiles(SegArgs a, Agg<NV>* t
         for (int w = 0; w < WARPS; ++w)
             if ((w + 1) * 32 * ITEMS - 1 >= from) r = agg_combine(r, s_warp[w], vc);
         r.heads = tile_heads;
-        tile_agg[blockIdx.x] = r;
+        tile_agg[tile] = r;
+    }
+}
+
+// Each CTA reduces several tiles in turn: 512-row tiles are too short to
+// amortise a CTA's launch.
+template <int NK, int NV>
+__global__ void __launch_bounds__(kSegThreads) k_seg_tiles(SegArgs a, Agg<NV>* tile_agg, uint32_t tiles) {
+    __shared__ TileSmem<NV> sm;
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        seg_tile_body<NK, NV>(a, tile_agg, t, sm);
+        __syncthreads();  // shared memory is reused by the next tile
     }
 }
 
@@ -486,35 +505,54 @@ __global__ void __launch_bounds__(kScanTiles) k_seg_scan2(const SegArgs a, Agg<N
 
 // ---- phase 3: scan each tile from its prefix and emit the groups -------------
 template <int NK, int NV>
-__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3)) k_seg_emit(SegArgs a, const Agg<NV>* tile_prefix,
-                                                                          const Agg<NV>* block_prefix) {
+__device__ __forceinline__ void seg_emit_body(const SegArgs& a, const Agg<NV>* tile_prefix, const Agg<NV>* block_prefix,
+                                              uint32_t tile) {
     constexpr int ITEMS = kSegItems;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t n = a.n;
-    const uint64_t row0 = (uint64_t)blockIdx.x * kSegTile + (uint64_t)tid * ITEMS;
+    const uint64_t row0 = (uint64_t)tile * kSegTile + (uint64_t)tid * ITEMS;
     Agg<NV>* s_warp = reinterpret_cast<Agg<NV>*>(seg_smem);  // [8] warp totals, [8] tile prefix
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
     uint32_t hmask;
     const Agg<NV> t = fold_rows<NK, NV>(a, row0, lane, vc, kw, hmask);
-    // per-warp inclusive scan with shuffles, then the warp totals in order
-    Agg<NV> incl = t;
+    // Per warp: the aggregate of the lanes before each lane (lx) and the
+    // warp's total.  When every lane's first row starts a group (typical with
+    // many groups), no segment crosses into a lane, so a lane's carry is just
+    // the previous lane's trailing segment plus a count of heads: one shuffle
+    // of the aggregate and a 32-bit scan instead of a scan of aggregates.
+    Agg<NV> lx, wtot;
+    if (__all_sync(0xffffffffu, row0 >= n || (hmask & 1u))) {
+        const uint32_t h = __popc(hmask);
+        uint32_t ih = h;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const Agg<NV> o = agg_shfl_up(incl, d);
-        if (lane >= d) incl = agg_combine(o, incl, vc);
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, ih, d);
+            if (lane >= d) ih += o;
+        }
+        lx = agg_shfl_up(t, 1);  // previous lane's trailing segment
+        lx.heads = ih - h;
+        if (lane == 0) lx = agg_identity<NV>();
+        wtot = t;  // (read at lane 31) its trailing segment, and all heads
+        wtot.heads = ih;
+    } else {
+        Agg<NV> incl = t;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const Agg<NV> o = agg_shfl_up(incl, d);
+            if (lane >= d) incl = agg_combine(o, incl, vc);
+        }
+        lx = agg_shfl_up(incl, 1);
+        if (lane == 0) lx = agg_identity<NV>();
+        wtot = incl;
     }
-    if (lane == 31) s_warp[warp] = incl;
+    if (lane == 31) s_warp[warp] = wtot;
     if (tid == 0)
-        s_warp[kSegThreads / 32] = agg_combine(block_prefix[blockIdx.x / kScanTiles], tile_prefix[blockIdx.x], vc);
+        s_warp[kSegThreads / 32] = agg_combine(block_prefix[tile / kScanTiles], tile_prefix[tile], vc);
     __syncthreads();
     Agg<NV> pre = s_warp[kSegThreads / 32];
     for (int w2 = 0; w2 < warp; ++w2) pre = agg_combine(pre, s_warp[w2], vc);
-    {
-        Agg<NV> lx = agg_shfl_up(incl, 1);
-        if (lane == 0) lx = agg_identity<NV>();
-        pre = agg_combine(pre, lx, vc);
-    }
+    pre = agg_combine(pre, lx, vc);
 
     // A segment is complete when the next head (or the last row) is reached;
     // the thread that reaches it produces the group's record.  The groups a
@@ -607,12 +645,22 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3)) k_seg_emit(Seg
 }
 
 template <int NK, int NV>
+__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3)) k_seg_emit(SegArgs a, const Agg<NV>* tile_prefix,
+                                                                          const Agg<NV>* block_prefix, uint32_t tiles) {
+    for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        seg_emit_body<NK, NV>(a, tile_prefix, block_prefix, t);
+        __syncthreads();  // the warp totals and staging are reused by the next tile
+    }
+}
+
+template <int NK, int NV>
 cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaStream_t s, Profiler* prof) {
     Agg<NV>* ta = reinterpret_cast<Agg<NV>*>(aggs);
     const uint32_t blocks = (tiles + kScanTiles - 1) / kScanTiles;
     Agg<NV>* bt = ta + tiles;
     if (prof) prof->begin(KC_SEGREDUCE, s);
-    k_seg_tiles<NK, NV><<<tiles, kSegThreads, 0, s>>>(a, ta);
+    const uint32_t grid = (tiles + kSegTilesPerCta - 1) / kSegTilesPerCta;
+    k_seg_tiles<NK, NV><<<grid, kSegThreads, 0, s>>>(a, ta, tiles);
     if (prof) prof->end(KC_SEGREDUCE, s);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -622,7 +670,7 @@ cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaS
     if (prof) prof->end(KC_SEGSCAN, s);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (prof) prof->begin(KC_SEGEMIT, s);
-    k_seg_emit<NK, NV><<<tiles, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta, bt);
+    k_seg_emit<NK, NV><<<grid, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta, bt, tiles);
     if (prof) prof->end(KC_SEGEMIT, s);
     return cudaGetLastError();
 }

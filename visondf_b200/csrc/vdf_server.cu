@@ -8,9 +8,9 @@
 // workspace) is free, every admitted waiting request, up to the batch limits,
 // joins one batch (vdf_batch_*), so requests arriving while other batches run
 // are taken as soon as a slot and memory free up, and the batches of different
-// slots overlap on the device.  Output arenas come from the stream-ordered
-// allocator, one set per batch, and return to it when the batch's last request
-// is released.
+// slots overlap on the device.  Each slot owns output arenas for its largest
+// batch, allocated once; a slot takes a new batch when its previous batch's
+// results have all been released, so no batch allocates device memory.
 //
 // The reference has no serving layer: a host runs one sort_by_mt +
 // transform_group_by_onecol_mt pair per query (sort_by_mt.hpp:3-180,
@@ -47,7 +47,6 @@ struct ServerBatch {
     int slot = 0;
     vdf_batch* b = nullptr;
     std::vector<uint64_t> ids;
-    std::vector<void*> allocs;  // output arenas (stream-ordered allocations)
     vdf_batch_args args{};
     std::vector<vdf_batch_query> queries;
     std::vector<uint64_t> row_off, grp_off, ngroups;  // host copies once done
@@ -65,12 +64,27 @@ uint64_t out_bytes_per_row(int nvals, const int32_t* dts) {
 
 }  // namespace
 
+// Output arenas of one slot, allocated once for max_batch_rows rows (and
+// max_batch_queries queries); every batch on the slot writes into them.
+struct SlotArena {
+    std::vector<void*> allocs;
+    uint32_t* perm = nullptr;
+    void* gkeys = nullptr;
+    int64_t* count = nullptr;
+    vdf_agg_out aggs[VDF_BATCH_MAX_VALS] = {};
+    uint64_t *row_off = nullptr, *grp_off = nullptr, *ngroups = nullptr;
+    uint64_t bytes = 0;
+};
+
 struct vdf_server {
     vdf_server_config cfg{};
     int nslots = 0;
     std::vector<vdf_ctx*> ctx;
     std::vector<cudaStream_t> stream;
-    std::vector<std::shared_ptr<ServerBatch>> running;  // per slot, null when free
+    std::vector<SlotArena> arena;
+    std::vector<std::shared_ptr<ServerBatch>> running;  // per slot: batch in flight
+    std::vector<std::shared_ptr<ServerBatch>> holding;  // per slot: finished batch with unreleased results
+    double t_host_start = 0, t_host_finish = 0;         // host seconds spent starting / finishing batches
     std::mutex mu;
     std::condition_variable cv;       // wakes the scheduler (new work, releases)
     std::condition_variable done_cv;  // wakes waiters (completions)
@@ -90,8 +104,7 @@ struct vdf_server {
 namespace {
 
 void free_batch_outputs(vdf_server* S, ServerBatch& B) {
-    for (void* p : B.allocs) cudaFreeAsync(p, S->stream[B.slot]);
-    B.allocs.clear();
+    (void)S;
     if (B.b) vdf_batch_destroy(B.b);
     B.b = nullptr;
     if (B.done) cudaEventDestroy(B.done);
@@ -104,49 +117,25 @@ vdf_status start_batch(vdf_server* S, ServerBatch& B, std::string& why) {
     cudaStream_t s = S->stream[B.slot];
     uint64_t rows = 0;
     for (const vdf_batch_query& q : B.queries) rows += q.n;
-    const uint64_t N = rows ? rows : 1;
     const uint32_t nq = (uint32_t)B.queries.size();
-    auto alloc = [&](size_t bytes) -> void* {
-        void* p = nullptr;
-        if (cudaMallocAsync(&p, bytes ? bytes : 8, s) != cudaSuccess) {
-            cudaGetLastError();
-            return nullptr;
-        }
-        B.allocs.push_back(p);
-        return p;
-    };
+    (void)rows;
+    const SlotArena& A = S->arena[B.slot];
     vdf_batch_args& a = B.args;
     a = vdf_batch_args{};
     a.nqueries = nq;
     a.queries = B.queries.data();
     a.nvals = c.nvals;
-    for (int j = 0; j < c.nvals; ++j) a.val_dtypes[j] = c.val_dtypes[j];
-    a.perm_out = static_cast<uint32_t*>(alloc(4 * N));
-    a.group_keys_out = alloc(8 * N);
-    a.group_count_out = static_cast<int64_t*>(alloc(8 * N));
     for (int j = 0; j < c.nvals; ++j) {
-        const bool fl = (c.val_dtypes[j] == VDF_F64 || c.val_dtypes[j] == VDF_F32);
-        const size_t w = (size_t)vdf::dtype_width(c.val_dtypes[j]);
-        a.aggs[j].sum = alloc(8 * N);
-        a.aggs[j].sum_hi = fl ? nullptr : static_cast<int64_t*>(alloc(8 * N));
-        a.aggs[j].min = alloc(w * N);
-        a.aggs[j].max = alloc(w * N);
-        a.aggs[j].mean = static_cast<double*>(alloc(8 * N));
+        a.val_dtypes[j] = c.val_dtypes[j];
+        a.aggs[j] = A.aggs[j];
     }
-    a.row_offset_out = static_cast<uint64_t*>(alloc(8 * nq));
-    a.group_offset_out = static_cast<uint64_t*>(alloc(8 * nq));
-    a.n_groups_out = static_cast<uint64_t*>(alloc(8 * nq));
-    for (void* p : B.allocs)
-        if (!p) {
-            why = "output allocation failed";
-            return VDF_ERR_OOM;
-        }
-    // the batch's own copies run on another stream: let the allocations land first
-    cudaError_t e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-        why = cudaGetErrorString(e);
-        return VDF_ERR_DEVICE;
-    }
+    a.perm_out = A.perm;
+    a.group_keys_out = A.gkeys;
+    a.group_count_out = A.count;
+    a.row_offset_out = A.row_off;
+    a.group_offset_out = A.grp_off;
+    a.n_groups_out = A.ngroups;
+    cudaError_t e = cudaSuccess;
     vdf_batch_tuning t{c.small_rows, c.small_bits, c.seg_variant};
     vdf_status st = vdf_batch_create(S->ctx[B.slot], &a, c.use_default_tuning ? nullptr : &t, &B.b);
     if (st != VDF_OK) {
@@ -202,12 +191,15 @@ void scheduler(vdf_server* S) {
             std::shared_ptr<ServerBatch> B = S->running[slot];
             if (!B || cudaEventQuery(B->done) == cudaErrorNotReady) continue;
             cudaGetLastError();
+            const double t_fin0 = S->now();
             lk.unlock();
             std::string why;
             vdf_status st = finish_batch(S, *B, why);
             lk.lock();
             B->finished = true;
             S->running[slot] = nullptr;
+            S->holding[slot] = B;  // the slot's arenas hold its results until released
+            S->t_host_finish += S->now() - t_fin0;
             const double t = S->now();
             for (uint64_t id : B->ids) {
                 auto it = S->reqs.find(id);
@@ -224,7 +216,7 @@ void scheduler(vdf_server* S) {
         // admission: first come, first served, while memory, the batch limits
         // and a free slot allow
         for (int slot = 0; slot < S->nslots && !S->queue.empty(); ++slot) {
-            if (S->running[slot]) continue;
+            if (S->running[slot] || S->holding[slot]) continue;
             auto B = std::make_shared<ServerBatch>();
             B->slot = slot;
             uint64_t rows = 0, bytes = 0;
@@ -253,10 +245,12 @@ void scheduler(vdf_server* S) {
             S->max_in_use = std::max(S->max_in_use, S->in_use);
             S->running[slot] = B;
             S->batches++;
+            const double t_st0 = S->now();
             lk.unlock();
             std::string why;
             vdf_status st = start_batch(S, *B, why);
             lk.lock();
+            S->t_host_start += S->now() - t_st0;
             if (st != VDF_OK) {
                 S->running[slot] = nullptr;
                 B->finished = true;
@@ -322,13 +316,6 @@ vdf_status vdf_server_create(const vdf_server_config* cfg, vdf_server** out) {
     S->nslots = (int)cfg->slots;
     S->t0 = std::chrono::steady_clock::now();
     DeviceGuard g(cfg->device);
-    // keep freed output arenas in the stream-ordered pool for the next batches
-    cudaMemPool_t pool;
-    if (cudaDeviceGetDefaultMemPool(&pool, cfg->device) == cudaSuccess) {
-        uint64_t thr = UINT64_MAX;
-        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
-    }
-    cudaGetLastError();
     for (int i = 0; i < S->nslots; ++i) {
         vdf_ctx* c = nullptr;
         vdf_status st = vdf_ctx_create(cfg->device, &c);
@@ -376,8 +363,51 @@ vdf_status vdf_server_create(const vdf_server_config* cfg, vdf_server** out) {
             S->fixed += P.ws_bytes + desc + (P.ws_bytes >> 4);
         }
     }
+    // output arenas, one set per slot
+    S->arena.resize(S->nslots);
+    for (int i = 0; i < S->nslots; ++i) {
+        SlotArena& A = S->arena[i];
+        const size_t R = cfg->max_batch_rows, Q = cfg->max_batch_queries;
+        bool ok = true;
+        auto alloc = [&](size_t bytes) -> void* {
+            void* p = nullptr;
+            if (cudaMalloc(&p, bytes) != cudaSuccess) {
+                cudaGetLastError();
+                ok = false;
+                return nullptr;
+            }
+            A.allocs.push_back(p);
+            A.bytes += bytes;
+            return p;
+        };
+        A.perm = static_cast<uint32_t*>(alloc(4 * R));
+        A.gkeys = alloc(8 * R);
+        A.count = static_cast<int64_t*>(alloc(8 * R));
+        for (int j = 0; j < cfg->nvals; ++j) {
+            const bool fl = (cfg->val_dtypes[j] == VDF_F64 || cfg->val_dtypes[j] == VDF_F32);
+            const size_t w = (size_t)vdf::dtype_width(cfg->val_dtypes[j]);
+            A.aggs[j].sum = alloc(8 * R);
+            A.aggs[j].sum_hi = fl ? nullptr : static_cast<int64_t*>(alloc(8 * R));
+            A.aggs[j].min = alloc(w * R);
+            A.aggs[j].max = alloc(w * R);
+            A.aggs[j].mean = static_cast<double*>(alloc(8 * R));
+        }
+        A.row_off = static_cast<uint64_t*>(alloc(8 * Q));
+        A.grp_off = static_cast<uint64_t*>(alloc(8 * Q));
+        A.ngroups = static_cast<uint64_t*>(alloc(8 * Q));
+        S->fixed += A.bytes;
+        if (!ok) {
+            for (SlotArena& X : S->arena)
+                for (void* p : X.allocs) cudaFree(p);
+            for (vdf_ctx* x : S->ctx) vdf_ctx_destroy(x);
+            for (cudaStream_t x : S->stream) cudaStreamDestroy(x);
+            return VDF_ERR_OOM;
+        }
+    }
     S->fixed += cfg->resident_bytes;
     if (S->fixed > cfg->hbm_budget_bytes) {
+        for (SlotArena& X : S->arena)
+            for (void* p : X.allocs) cudaFree(p);
         for (vdf_ctx* x : S->ctx) vdf_ctx_destroy(x);
         for (cudaStream_t x : S->stream) cudaStreamDestroy(x);
         return VDF_ERR_INVALID_ARG;
@@ -385,6 +415,7 @@ vdf_status vdf_server_create(const vdf_server_config* cfg, vdf_server** out) {
     S->in_use = S->fixed;
     S->max_in_use = S->fixed;
     S->running.assign(S->nslots, nullptr);
+    S->holding.assign(S->nslots, nullptr);
     vdf_server* raw = S.release();
     raw->th = std::thread(scheduler, raw);
     *out = raw;
@@ -475,6 +506,7 @@ vdf_status vdf_server_release(vdf_server* S, uint64_t id) {
         DeviceGuard g(S->cfg.device);
         free_batch_outputs(S, *B);
         S->in_use -= B->bytes;
+        if (S->holding[B->slot] == B) S->holding[B->slot] = nullptr;  // the slot's arenas are free again
         S->cv.notify_one();
     }
     return VDF_OK;
@@ -489,6 +521,8 @@ vdf_status vdf_server_read_stats(vdf_server* S, vdf_server_stats* out) {
     out->in_use_bytes = S->in_use;
     out->max_in_use_bytes = S->max_in_use;
     out->fixed_bytes = S->fixed;
+    out->host_start_seconds = S->t_host_start;
+    out->host_finish_seconds = S->t_host_finish;
     return VDF_OK;
 }
 
@@ -519,6 +553,8 @@ void vdf_server_destroy(vdf_server* S) {
         cudaStreamSynchronize(s);
         cudaStreamDestroy(s);
     }
+    for (SlotArena& A : S->arena)
+        for (void* p : A.allocs) cudaFree(p);
     for (vdf_ctx* c : S->ctx) vdf_ctx_destroy(c);
     delete S;
 }

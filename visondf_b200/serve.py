@@ -314,7 +314,8 @@ def _server_lib():
 
     class Stats(C.Structure):
         _fields_ = [("batches", C.c_uint64), ("completed", C.c_uint64), ("queued", C.c_uint64),
-                    ("in_use_bytes", C.c_uint64), ("max_in_use_bytes", C.c_uint64), ("fixed_bytes", C.c_uint64)]
+                    ("in_use_bytes", C.c_uint64), ("max_in_use_bytes", C.c_uint64), ("fixed_bytes", C.c_uint64),
+                    ("host_start_seconds", C.c_double), ("host_finish_seconds", C.c_double)]
 
     vp, st = C.c_void_p, C.c_int
     for name, res, args in [
@@ -480,8 +481,9 @@ class Server:
 def serve_trace(server: Server, requests: Sequence[Request], keep_results: bool = False,
                 clock: Callable[[], float] = time.perf_counter) -> TraceStats:
     """Submits each request at its arrival time (seconds from the start),
-    releases results as they complete (or keeps them in r.result), and
-    returns the trace statistics with latencies on the server's clock."""
+    releases results as they complete (keep_results: after copying them to
+    r.result), and returns the trace statistics with latencies on the
+    server's clock."""
     reqs = sorted(requests, key=lambda r: (r.arrival, r.rid))
     ids = {}
     outstanding = []
@@ -502,10 +504,12 @@ def serve_trace(server: Server, requests: Sequence[Request], keep_results: bool 
             if state == 2:
                 r.started, r.completed = res.t_start, res.t_done
                 r.admitted = res.t_submit
-                if keep_results:
-                    r.result = res
-                else:
-                    server.release(ids[r.rid])
+                if keep_results:  # copies: a slot's arenas are reused once released
+                    r.result = ServedResult(res.perm.clone(), res.n_groups, res.keys.clone(), res.count.clone(),
+                                            [server._lib.AggResult(*(None if x is None else x.clone()
+                                                                     for x in (a.sum, a.sum_hi, a.min, a.max, a.mean)))
+                                             for a in res.aggs], res.t_submit, res.t_start, res.t_done)
+                server.release(ids[r.rid])
                 done += 1
             else:
                 still.append(r)
