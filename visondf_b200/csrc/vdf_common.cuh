@@ -86,6 +86,33 @@ __device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
 template <typename T> __device__ __forceinline__ T ldg_stream(const T* p) { return __ldcs(p); }
 template <typename T> __device__ __forceinline__ void stg_stream(T* p, T v) { __stcs(p, v); }
 
+// Random reads of read-only data (gathers through a permutation): the
+// non-coherent path with the L2 fetch limited to 64 bytes.  Measured on B200
+// for 100M random 32-byte records: one 32-byte load of this form took 2.15 ms
+// and read 75 B of DRAM per record, against 4.1 ms and 137 B for two 16-byte
+// L2-only loads (the second half of a record then costs a second L2 request,
+// and a miss fetches 128 bytes by default).
+__device__ __forceinline__ void ld_rand32(const void* p, unsigned long long (&v)[4]) {  // 32-byte aligned
+    asm("ld.global.nc.L2::64B.v4.u64 {%0,%1,%2,%3}, [%4];"
+        : "=l"(v[0]), "=l"(v[1]), "=l"(v[2]), "=l"(v[3])
+        : "l"(p));
+}
+__device__ __forceinline__ ulonglong2 ld_rand16(const void* p) {  // 16-byte aligned
+    ulonglong2 v;
+    asm("ld.global.nc.L2::64B.v2.u64 {%0,%1}, [%2];" : "=l"(v.x), "=l"(v.y) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ unsigned long long ld_rand8(const void* p) {
+    unsigned long long v;
+    asm("ld.global.nc.L2::64B.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_rand4(const void* p) {
+    uint32_t v;
+    asm("ld.global.nc.L2::64B.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+
 // Bounded waits: every spin in these kernels gives up after this many polls
 // (each poll sleeps 32-128 ns, so about 0.1 s), records an error bit in the
 // context's error word and carries on, so a broken dependency ends the kernel

@@ -46,20 +46,20 @@ __global__ void __launch_bounds__(256) k_gather(GatherArgs g) {
             if (g.width[c] == 8) {
                 const unsigned long long* s = static_cast<const unsigned long long*>(g.src[c]);
                 ulonglong2 a, b;
-                a.x = __ldcg(s + p.x);
-                a.y = __ldcg(s + p.y);
-                b.x = __ldcg(s + p.z);
-                b.y = __ldcg(s + p.w);
+                a.x = ld_rand8(s + p.x);
+                a.y = ld_rand8(s + p.y);
+                b.x = ld_rand8(s + p.z);
+                b.y = ld_rand8(s + p.w);
                 ulonglong2* d = reinterpret_cast<ulonglong2*>(static_cast<unsigned long long*>(g.dst[c]) + r0);
                 stg_stream(d, a);
                 stg_stream(d + 1, b);
             } else {
                 const uint32_t* s = static_cast<const uint32_t*>(g.src[c]);
                 uint4 v;
-                v.x = __ldcg(s + p.x);
-                v.y = __ldcg(s + p.y);
-                v.z = __ldcg(s + p.z);
-                v.w = __ldcg(s + p.w);
+                v.x = ld_rand4(s + p.x);
+                v.y = ld_rand4(s + p.y);
+                v.z = ld_rand4(s + p.z);
+                v.w = ld_rand4(s + p.w);
                 stg_stream(reinterpret_cast<uint4*>(static_cast<uint32_t*>(g.dst[c]) + r0), v);
             }
         }
@@ -74,9 +74,9 @@ __global__ void __launch_bounds__(256) k_gather(GatherArgs g) {
         }
         for (int c = 0; c < g.ncols; ++c) {
             if (g.width[c] == 8)
-                static_cast<unsigned long long*>(g.dst[c])[r] = __ldcg(static_cast<const unsigned long long*>(g.src[c]) + p);
+                static_cast<unsigned long long*>(g.dst[c])[r] = ld_rand8(static_cast<const unsigned long long*>(g.src[c]) + p);
             else
-                static_cast<uint32_t*>(g.dst[c])[r] = __ldcg(static_cast<const uint32_t*>(g.src[c]) + p);
+                static_cast<uint32_t*>(g.dst[c])[r] = ld_rand4(static_cast<const uint32_t*>(g.src[c]) + p);
         }
     }
 }
@@ -99,6 +99,30 @@ __global__ void __launch_bounds__(256) k_pack(GatherArgs g, unsigned char* recs)
     for (int c = 0; c < SLOTS; c += 2) dst[c / 2] = make_ulonglong2(slot[c], slot[c + 1]);
 }
 
+// One record's 8-byte slots (records start at multiples of REC; 32- and
+// 64-byte records are 32-byte aligned, 16- and 48-byte ones 16-byte aligned).
+template <int REC>
+__device__ __forceinline__ void load_record(const unsigned char* rec, unsigned long long (&slot)[REC / 8]) {
+    if constexpr (REC % 32 == 0) {
+#pragma unroll
+        for (int c = 0; c < REC / 8; c += 4) {
+            unsigned long long v[4];
+            ld_rand32(rec + 8 * c, v);
+            slot[c] = v[0];
+            slot[c + 1] = v[1];
+            slot[c + 2] = v[2];
+            slot[c + 3] = v[3];
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < REC / 8; c += 2) {
+            const ulonglong2 v = ld_rand16(rec + 8 * c);
+            slot[c] = v.x;
+            slot[c + 1] = v.y;
+        }
+    }
+}
+
 template <int REC>
 __global__ void __launch_bounds__(256) k_gather_rec(GatherArgs g, const unsigned char* recs) {
     constexpr int SLOTS = REC / 8;
@@ -109,16 +133,8 @@ __global__ void __launch_bounds__(256) k_gather_rec(GatherArgs g, const unsigned
         if (g.err) atomicOr(g.err, ERR_BAD_INDEX);
         p = 0;
     }
-    // L2-only loads: a non-coherent (L1) load of one record would fetch its
-    // whole 128-byte line from DRAM.
-    const ulonglong2* src = reinterpret_cast<const ulonglong2*>(recs + (uint64_t)p * REC);
     unsigned long long slot[SLOTS];
-#pragma unroll
-    for (int c = 0; c < SLOTS; c += 2) {
-        const ulonglong2 v = __ldcg(src + c / 2);
-        slot[c] = v.x;
-        slot[c + 1] = v.y;
-    }
+    load_record<REC>(recs + (uint64_t)p * REC, slot);
 #pragma unroll
     for (int c = 0; c < SLOTS; ++c) {
         if (c >= g.ncols) break;
@@ -148,15 +164,7 @@ __global__ void __launch_bounds__(256) k_gather_rec4(GatherArgs g, const unsigne
             }
         unsigned long long slot[4][SLOTS];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const ulonglong2* src = reinterpret_cast<const ulonglong2*>(recs + (uint64_t)p[k] * REC);
-#pragma unroll
-            for (int c = 0; c < SLOTS; c += 2) {
-                const ulonglong2 v = __ldcg(src + c / 2);
-                slot[k][c] = v.x;
-                slot[k][c + 1] = v.y;
-            }
-        }
+        for (int k = 0; k < 4; ++k) load_record<REC>(recs + (uint64_t)p[k] * REC, slot[k]);
 #pragma unroll
         for (int c = 0; c < SLOTS; ++c) {
             if (c >= g.ncols) break;
@@ -178,14 +186,8 @@ __global__ void __launch_bounds__(256) k_gather_rec4(GatherArgs g, const unsigne
             if (g.err) atomicOr(g.err, ERR_BAD_INDEX);
             p = 0;
         }
-        const ulonglong2* src = reinterpret_cast<const ulonglong2*>(recs + (uint64_t)p * REC);
         unsigned long long slot[SLOTS];
-#pragma unroll
-        for (int c = 0; c < SLOTS; c += 2) {
-            const ulonglong2 v = __ldcg(src + c / 2);
-            slot[c] = v.x;
-            slot[c + 1] = v.y;
-        }
+        load_record<REC>(recs + (uint64_t)p * REC, slot);
 #pragma unroll
         for (int c = 0; c < SLOTS; ++c) {
             if (c >= g.ncols) break;

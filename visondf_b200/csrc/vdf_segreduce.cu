@@ -247,7 +247,7 @@ struct WarpStage {
 constexpr int kSegThreads = 256;
 constexpr int kSegItems = 2;
 constexpr int kSegTile = kSegThreads * kSegItems;  // rows per tile
-constexpr int kSegTilesPerCta = 4;                  // tiles each CTA of the reduce and emit passes takes
+constexpr int kSegTilesPerCta = 1;                  // tiles each CTA of the reduce and emit passes takes
 
 extern __shared__ __align__(16) unsigned char seg_smem[];
 
