@@ -76,7 +76,7 @@ size_t primary_first_need(vdf_ctx* c, uint64_t n, const int32_t* dts, int nkeys,
 // Returns VDF_OK with *done telling which case happened.
 vdf_status primary_first(vdf_ctx* c, uint64_t n, const int32_t* dts, const void* const* cols, int nkeys, int order,
                          uint32_t* perm, void* key0_out, unsigned char* ws, size_t ws_bytes, cudaStream_t s,
-                         const uint32_t* perm_in, bool* done, const vdf::PackArgs* pack = nullptr) {
+                         const uint32_t* perm_in, bool* done) {
     *done = false;
     if (nkeys < 2 || c->multikey_mode != VDF_MULTIKEY_PRIMARY_FIRST || n < 2) return VDF_OK;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
@@ -92,7 +92,7 @@ vdf_status primary_first(vdf_ctx* c, uint64_t n, const int32_t* dts, const void*
         need = align256(p0.ws_bytes) + (size_t)n * vdf::dtype_width(dts[0]);
     }
     if (need > ws_bytes) return VDF_OK;  // no room: the LSD sort over all keys
-    cudaError_t e = vdf::run_sort(p0, cols, order, perm, k0, ws, err_word(c), s, prof_of(c), perm_in, pack);
+    cudaError_t e = vdf::run_sort(p0, cols, order, perm, k0, ws, err_word(c), s, prof_of(c), perm_in);
     c->launches += 2 + (uint64_t)p0.total_passes;
     if (e == cudaSuccess) e = cudaMemsetAsync(tie_word(c), 0, sizeof(uint32_t), s);
     if (e == cudaSuccess) e = vdf::flag_adjacent_ties(k0, vdf::dtype_width(dts[0]), n, tie_word(c), s, prof_of(c));
@@ -513,18 +513,8 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
     for (int k = 1; k < x->nkeys; ++k) ngather += (skey[k] || key_own[k]) ? 1 : 0;
     for (int p = 0; p < x->npayload; ++p) ngather += (spay[p] || pay_own[p]) ? 1 : 0;
     const size_t rec_bytes = (size_t)n * vdf::gather_record_bytes(std::min(ngather, vdf::kMaxGather));
-    // With raw rows (no input permutation) and one record per row, the sort's
-    // first pass packs the records while it streams the rows, into their own
-    // region (the sort's workspace is busy then); the gather then only reads.
-    const bool fuse_pack = !x->perm_in && ngather >= 2 && ngather <= vdf::kMaxGather;
-    size_t rec_off = 0;
-    if (fuse_pack) {
-        rec_off = off;
-        off += align256(rec_bytes);
-    }
     const size_t seg_bytes = x->groupby ? vdf::segreduce_workspace_bytes(n, x->nagg) : 0;
-    size_t tail = std::max(plan.ws_bytes, seg_bytes);
-    if (!fuse_pack) tail = std::max(tail, rec_bytes);
+    size_t tail = std::max(std::max(plan.ws_bytes, seg_bytes), rec_bytes);
     if (x->nkeys >= 2 && c->multikey_mode == VDF_MULTIKEY_PRIMARY_FIRST && !skey[0]) {
         // room for the primary key's sorted copy next to its sort's workspace
         const vdf::SortPlan p0 = vdf::make_sort_plan(n, dts, 1, c->tuning);
@@ -545,25 +535,13 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
         if (skey[k]) gcols.push_back({x->keys[k].data, skey[k], x->keys[k].dtype});
     for (int p = 0; p < x->npayload; ++p)
         if (spay[p]) gcols.push_back({x->payload[p].data, spay[p], x->payload[p].dtype});
-    vdf::PackArgs pack{};
-    unsigned char* recs = c->ws + rec_off;
-    if (fuse_pack) {
-        pack.ncols = (int)gcols.size();
-        pack.rec = (int)vdf::gather_record_bytes(pack.ncols);
-        for (int i = 0; i < pack.ncols; ++i) {
-            pack.src[i] = gcols[i].src;
-            pack.width[i] = vdf::dtype_width(gcols[i].dtype);
-        }
-        pack.out = recs;
-    }
     bool done = false;
     if ((st = primary_first(c, n, dts, cols, x->nkeys, x->order, perm, skey[0], tws, c->ws_cap - off, s, x->perm_in,
-                            &done, fuse_pack ? &pack : nullptr)) != VDF_OK)
+                            &done)) != VDF_OK)
         return st;
     cudaError_t e = cudaSuccess;
     if (!done) {
-        e = vdf::run_sort(plan, cols, x->order, perm, skey[0], tws, err_word(c), s, prof_of(c), x->perm_in,
-                          fuse_pack ? &pack : nullptr);
+        e = vdf::run_sort(plan, cols, x->order, perm, skey[0], tws, err_word(c), s, prof_of(c), x->perm_in);
         c->launches += 2 + (uint64_t)plan.total_passes;
         if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
     }
@@ -589,22 +567,9 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
         if (++ga.ncols == vdf::kMaxGather) return flush();
         return cudaSuccess;
     };
-    if (fuse_pack) {
-        for (const GCol& gc : gcols) {
-            ga.src[ga.ncols] = gc.src;
-            ga.dst[ga.ncols] = gc.dst;
-            ga.width[ga.ncols] = vdf::dtype_width(gc.dtype);
-            ga.ncols++;
-        }
-        int launched = 0;
-        e = vdf::run_gather_records(ga, recs, (size_t)pack.rec, s, prof_of(c), &launched);
-        c->launches += launched;
-        if (e != cudaSuccess) return from_cuda(c, e, "gather");
-    } else {
-        for (const GCol& gc : gcols)
-            if ((e = add(gc.src, gc.dst, gc.dtype)) != cudaSuccess) return from_cuda(c, e, "gather");
-        if ((e = flush()) != cudaSuccess) return from_cuda(c, e, "gather");
-    }
+    for (const GCol& gc : gcols)
+        if ((e = add(gc.src, gc.dst, gc.dtype)) != cudaSuccess) return from_cuda(c, e, "gather");
+    if ((e = flush()) != cudaSuccess) return from_cuda(c, e, "gather");
     if (!x->groupby) return VDF_OK;
 
     vdf::SegArgs a{};

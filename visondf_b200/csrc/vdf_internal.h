@@ -91,24 +91,8 @@ struct PassArgs {
     uint32_t pass;              // digit pass index
     void* keys_final;           // where a segment's last pass writes its keys
     uint32_t* vals_final;       // ... and its row ids
-    // first pass over raw rows only: also copy pack_ncols columns into row
-    // records (the packed gather's layout: 8-byte slots, pack_rec bytes per
-    // row) at the rows' own positions, sparing the gather its packing pass
-    int pack_ncols;
-    int pack_rec;               // 0: no packing
-    const void* pack_src[kMaxGather];
-    int pack_width[kMaxGather];
-    unsigned char* pack_out;
 };
 
-// Columns the first pass of a sort packs into gather records (see PassArgs).
-struct PackArgs {
-    int ncols;
-    int rec;
-    const void* src[kMaxGather];
-    int width[kMaxGather];
-    unsigned char* out;
-};
 
 // Kernel-variant choice of the radix pass per key width (indices into the
 // variant table in vdf_radix.cu); the autotuner's search space.
@@ -141,7 +125,7 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
 // and perm_out is the composed permutation.
 cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
                      void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof = nullptr,
-                     const uint32_t* perm_in = nullptr, const PackArgs* pack = nullptr);
+                     const uint32_t* perm_in = nullptr);
 cudaError_t prepare_sort_kernels();
 // *flag |= 1 when two neighbouring elements of a sorted key column (4- or
 // 8-byte elements) have the same bits.

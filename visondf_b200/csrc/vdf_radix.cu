@@ -551,33 +551,6 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
             stg_stream(vout + p, v);
         }
     }
-
-    // ---- the gather's row records, packed while this tile's rows stream by --
-    if constexpr (IN_MODE == IN_RAW && !SEG) {
-        if (a.pack_rec) {
-            const int slots = a.pack_rec / 8;
-#pragma unroll 1
-            for (int j = 0; j < ITEMS; ++j) {
-                const uint32_t pos = wpos + j * 32 + lane;
-                if (pos >= valid) continue;
-                const uint64_t row = tile_base + pos;
-                ulonglong2* dst = reinterpret_cast<ulonglong2*>(a.pack_out + row * (uint64_t)a.pack_rec);
-#pragma unroll 1
-                for (int c = 0; c < slots; c += 2) {
-                    unsigned long long x = 0, y = 0;
-                    if (c < a.pack_ncols)
-                        x = a.pack_width[c] == 8
-                                ? ldg_stream(static_cast<const unsigned long long*>(a.pack_src[c]) + row)
-                                : (unsigned long long)ldg_stream(static_cast<const uint32_t*>(a.pack_src[c]) + row);
-                    if (c + 1 < a.pack_ncols)
-                        y = a.pack_width[c + 1] == 8
-                                ? ldg_stream(static_cast<const unsigned long long*>(a.pack_src[c + 1]) + row)
-                                : (unsigned long long)ldg_stream(static_cast<const uint32_t*>(a.pack_src[c + 1]) + row);
-                    stg_stream(dst + c / 2, make_ulonglong2(x, y));
-                }
-            }
-        }
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -751,7 +724,7 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
 
 cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
                      void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof,
-                     const uint32_t* perm_in, const PackArgs* pack) {
+                     const uint32_t* perm_in) {
     const uint64_t n = p.n;
     if (n == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(ws + p.off_zero, 0, p.zero_bytes, s);
@@ -835,15 +808,6 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
                 mode = perm_in ? IN_GATHER : IN_RAW;
                 a.keys_in = key_cols[k];
                 a.vals_in = perm_in;
-                if (mode == IN_RAW && pack && pack->rec) {
-                    a.pack_ncols = pack->ncols;
-                    a.pack_rec = pack->rec;
-                    for (int c = 0; c < pack->ncols; ++c) {
-                        a.pack_src[c] = pack->src[c];
-                        a.pack_width[c] = pack->width[c];
-                    }
-                    a.pack_out = pack->out;
-                }
             } else if (q == 0) {
                 mode = IN_GATHER;
                 a.keys_in = key_cols[k];

@@ -645,7 +645,7 @@ __device__ __forceinline__ void seg_emit_body(const SegArgs& a, const Agg<NV>* t
 }
 
 template <int NK, int NV>
-__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3)) k_seg_emit(SegArgs a, const Agg<NV>* tile_prefix,
+__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : (NV == 2 ? 4 : 3))) k_seg_emit(SegArgs a, const Agg<NV>* tile_prefix,
                                                                           const Agg<NV>* block_prefix, uint32_t tiles) {
     for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
         seg_emit_body<NK, NV>(a, tile_prefix, block_prefix, t);
