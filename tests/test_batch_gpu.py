@@ -186,3 +186,48 @@ def test_batch_rejects_bad_tuning_and_arguments(ctx):
     with pytest.raises(ValueError):
         vdf.Batch(ctx, [(k, [dev(queries[0][1]), dev(queries[0][2].astype(np.float64))]),
                         (k, [dev(queries[0][1]), dev(queries[0][2])])])
+
+
+@pytest.mark.parametrize("vals", [(), (np.float32,), (np.int32, np.uint64, np.float64),
+                                  (np.uint32, np.int64, np.float32, np.float64)])
+def test_value_column_sets(ctx, vals):
+    """No values, one value column (column gather), three and four columns
+    (32-byte records with zero-padded slots), every value dtype."""
+    rng = np.random.default_rng(4242 + len(vals))
+    specs = [(3000, np.int64, 40), (50_000, np.int32, 900), (0, np.int32, 1), (120_000, np.uint64, 7),
+             (7000, np.float64, 7000)]
+    queries = []
+    for n, kdt, card in specs:
+        pool = datagen.distinct_pool(rng, card, kdt) if np.dtype(kdt).kind != "f" else rng.standard_normal(card)
+        key = pool[rng.integers(0, card, size=n)].astype(kdt) if n else np.empty(0, kdt)
+        vs = []
+        for vdt in vals:
+            if np.dtype(vdt).kind == "f":
+                vs.append(rng.standard_normal(n).astype(vdt))
+            else:
+                info = np.iinfo(vdt)
+                lo, hi = max(info.min, -10**12), min(info.max, 10**12)
+                vs.append(rng.integers(lo, hi, size=n, dtype=vdt, endpoint=True))
+        queries.append((key, vs))
+    for small in (0, 4096):
+        b = vdf.Batch(ctx, [(dev(k), [dev(v) for v in vs]) for k, vs in queries],
+                      dict(small_rows=small, small_bits=8, seg_variant=0))
+        b.launch()
+        ctx.check()
+        for q, (key, vs) in enumerate(queries):
+            r = b.result(q)
+            if key.size == 0:
+                assert r.n_groups == 0
+                continue
+            assert (host(r.perm).view(np.uint32) == ob.argsort([key])).all()
+            og = ob.groupby([key], vs) if vs else ob.groupby([key], [np.zeros(key.size)])
+            assert r.n_groups == og.n_groups and bits_equal(host(r.keys), og.keys[0])
+            assert (host(r.count) == og.count).all()
+            for j, v in enumerate(vs):
+                a = r.aggs[j]
+                assert bits_equal(host(a.min), og.min[j]) and bits_equal(host(a.max), og.max[j]), (q, j)
+                if v.dtype.kind == "f":
+                    assert_f64_close(host(a.sum), og.sum[j], og.abs[j], f"query {q} col {j}")
+                else:
+                    assert (host(a.sum) == og.sum[j]).all() and (host(a.sum_hi) == og.sum_hi[j]).all(), (q, j)
+        b.close()
