@@ -52,26 +52,46 @@ __global__ void __launch_bounds__(256) k_batch_pack(BatchDev b) {
         if (threadIdx.x == 0) atomicOr(b.err, ERR_BAD_INDEX);
         return;
     }
-    for (uint32_t r = threadIdx.x; r < ch.rows; r += blockDim.x) {
-        const uint64_t i = ch.row_start + r;       // arena row
-        const uint64_t local = i - sd.row_start;   // row within the query
-        b.arena_keys[i] = ordered_image(q.key, local, q.key_dtype);
-        b.arena_seg[i] = ch.seg;
-        if (b.rec_bytes) {
-            // the packed gather's record: 8-byte slots, zero-extended
-            unsigned long long slot[VDF_BATCH_MAX_VALS] = {0, 0, 0, 0};
-            for (int j = 0; j < b.nvals; ++j)
-                slot[j] = b.val_width[j] == 8 ? __ldg(static_cast<const unsigned long long*>(q.vals[j]) + local)
-                                              : (unsigned long long)__ldg(static_cast<const uint32_t*>(q.vals[j]) + local);
-            ulonglong2* dst = reinterpret_cast<ulonglong2*>(b.arena_recs + i * (uint64_t)b.rec_bytes);
-            dst[0] = make_ulonglong2(slot[0], slot[1]);
-            if (b.rec_bytes == 32) dst[1] = make_ulonglong2(slot[2], slot[3]);
-        } else {
-            for (int j = 0; j < b.nvals; ++j) {
-                if (b.val_width[j] == 8)
-                    static_cast<uint64_t*>(b.arena_vals[j])[i] = __ldg(static_cast<const uint64_t*>(q.vals[j]) + local);
-                else
-                    static_cast<uint32_t*>(b.arena_vals[j])[i] = __ldg(static_cast<const uint32_t*>(q.vals[j]) + local);
+    // four rows per thread per round, all loads issued before the stores
+    constexpr int R = 4;
+    for (uint32_t r0 = threadIdx.x * R; r0 < ch.rows; r0 += blockDim.x * R) {
+        uint64_t kimg[R];
+        unsigned long long slot[R][VDF_BATCH_MAX_VALS];
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const uint32_t r = r0 + k;
+            kimg[k] = 0;
+#pragma unroll
+            for (int j = 0; j < VDF_BATCH_MAX_VALS; ++j) slot[k][j] = 0;
+            if (r >= ch.rows) continue;
+            const uint64_t local = ch.row_start + r - sd.row_start;  // row within the query
+            kimg[k] = ordered_image(q.key, local, q.key_dtype);
+#pragma unroll
+            for (int j = 0; j < VDF_BATCH_MAX_VALS; ++j)
+                if (j < b.nvals)
+                    slot[k][j] = b.val_width[j] == 8
+                                     ? __ldg(static_cast<const unsigned long long*>(q.vals[j]) + local)
+                                     : (unsigned long long)__ldg(static_cast<const uint32_t*>(q.vals[j]) + local);
+        }
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const uint32_t r = r0 + k;
+            if (r >= ch.rows) continue;
+            const uint64_t i = ch.row_start + r;  // arena row
+            b.arena_keys[i] = kimg[k];
+            b.arena_seg[i] = ch.seg;
+            if (b.rec_bytes) {
+                // the packed gather's record: 8-byte slots, zero-extended
+                ulonglong2* dst = reinterpret_cast<ulonglong2*>(b.arena_recs + i * (uint64_t)b.rec_bytes);
+                dst[0] = make_ulonglong2(slot[k][0], slot[k][1]);
+                if (b.rec_bytes == 32) dst[1] = make_ulonglong2(slot[k][2], slot[k][3]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < VDF_BATCH_MAX_VALS; ++j) {
+                    if (j >= b.nvals) break;
+                    if (b.val_width[j] == 8) static_cast<uint64_t*>(b.arena_vals[j])[i] = slot[k][j];
+                    else static_cast<uint32_t*>(b.arena_vals[j])[i] = (uint32_t)slot[k][j];
+                }
             }
         }
     }
