@@ -19,6 +19,17 @@ int32 payloads.  One vdf_sort_groupby call per step through the C-ABI.
                  on the reference's map and hash) on the host cores, on a
                  10,000,000-row sample of the same workload.
 
+  batched    4,096 independent sort + group-by queries (rows log-uniform
+             1e3..1e7 scaled to a 2 GiB batch, int32/int64 keys, f64 + int64
+             values) as one CUDA graph launch per batch (vdf_batch_*), autotuned,
+             against one vdf_sort_groupby call per query.
+  served     a Poisson request stream (rows lognormal, median 1e6) over a
+             resident 100M-row table through the library's request loop
+             (vdf_server_*: HBM-budget admission, continuous batching): capacity
+             and p50/p99 latency at 50/70/90 % of batched capacity, against one
+             vdf_sort_groupby call per request on the same traces.
+  (both single-GPU, after the headline measurement; --sections selects them)
+
 --gpus N (launched by torchrun for N > 1) runs N independent replicas, one per
 GPU ("replicas only": the single-GPU path has no exchange step); value is all
 rows processed / the slowest rank's time.

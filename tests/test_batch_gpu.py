@@ -99,6 +99,23 @@ def test_every_tuning_matches_the_oracle(ctx, seg_variant, small):
     b.close()
 
 
+SPECS_4BYTE_LARGE = [(3, np.int64, 3), (1000, np.uint64, 10), (70_000, np.int32, 1000), (150_001, np.float32, 40_000),
+                     (20_000, np.uint32, 20_000), (33_333, np.int32, 2), (5000, np.float64, 700)]
+
+
+@pytest.mark.parametrize("seg_variant", range(len(_lib.batch_variants())))
+def test_four_byte_key_arena_matches_the_oracle(ctx, seg_variant):
+    """Every large query has 4-byte keys, so the arena holds 4-byte key
+    images; small queries of 8-byte keys run on the one-CTA path beside it."""
+    queries = make_queries(SPECS_4BYTE_LARGE)
+    b, _ = to_batch(ctx, queries, dict(small_rows=8192, small_bits=8, seg_variant=seg_variant))
+    assert b.info()["large_queries"] == 4
+    b.launch()
+    ctx.check()
+    check_against_oracle(b, queries)
+    b.close()
+
+
 def test_graph_replay_gives_the_same_bits(ctx):
     queries = make_queries(SPECS)
     b, _ = to_batch(ctx, queries)

@@ -72,7 +72,10 @@ def test_budget_bounds_memory_in_flight(ctx, table):
     st = serve.serve_trace(srv, reqs, keep_results=False)
     s = srv.stats()
     assert s["max_in_use_bytes"] <= fixed + 3 * per_req
-    assert s["completed"] == 30 and st.batches >= 10  # about three requests per batch at most
+    # each batch holds at most 3 * per_req bytes of requests, whenever the
+    # scheduler admitted it, so the batch count has a size-only lower bound
+    need = sum(r.rows * serve.out_bytes_per_row([True, False]) + 256 for r in reqs)
+    assert s["completed"] == 30 and st.batches >= -(-need // (3 * per_req)) and st.batches >= 2
     # a request that can never fit is refused at submission
     key, v1, v2 = table
     with pytest.raises(vdf.VdfError):

@@ -31,6 +31,7 @@
 namespace vdf {
 namespace {
 
+// A 4-byte key's image has a zero high half, so it also fits a 4-byte arena.
 __device__ __forceinline__ uint64_t ordered_image(const void* col, uint64_t i, int dt) {
     switch (dt) {
     case I32: case U32: case F32:
@@ -40,8 +41,9 @@ __device__ __forceinline__ uint64_t ordered_image(const void* col, uint64_t i, i
     }
 }
 
-// Copies each large query's rows into the arena: ordered key image, segment
-// index, and the value columns; one CTA per chunk of one segment.
+// Copies each large query's rows into the arena: ordered key image (8 or 4
+// bytes), segment index, and the value columns; one CTA per chunk of one
+// segment.
 __global__ void __launch_bounds__(256) k_batch_pack(BatchDev b) {
     const SegChunk ch = b.chunks[blockIdx.x];
     if (ch.seg >= b.nsegs) return;
@@ -78,7 +80,8 @@ __global__ void __launch_bounds__(256) k_batch_pack(BatchDev b) {
             const uint32_t r = r0 + k;
             if (r >= ch.rows) continue;
             const uint64_t i = ch.row_start + r;  // arena row
-            b.arena_keys[i] = kimg[k];
+            if (b.key_width == 8) static_cast<uint64_t*>(b.arena_keys)[i] = kimg[k];
+            else static_cast<uint32_t*>(b.arena_keys)[i] = (uint32_t)kimg[k];
             b.arena_seg[i] = ch.seg;
             if (b.rec_bytes) {
                 // the packed gather's record: 8-byte slots, zero-extended
@@ -150,7 +153,8 @@ __global__ void __launch_bounds__(256) k_batch_group_keys(BatchDev b) {
         }
         const uint32_t first = b.seg_first_group[s];
         const int dt = b.queries[b.seg_query[s]].key_dtype;
-        const uint64_t img = b.group_key_img[g];
+        const uint64_t img = b.key_width == 8 ? static_cast<const uint64_t*>(b.group_key_img)[g]
+                                              : static_cast<const uint32_t*>(b.group_key_img)[g];
         unsigned char* base = out + 8 * (b.large_base + first);
         if (dtype_width(dt) == 4)
             reinterpret_cast<uint32_t*>(base)[g - first] = unorder32((uint32_t)img, dt, false);
@@ -187,6 +191,7 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
     int bits = 8, tile = 2048;
     seg_sort_variant_info(t.seg_variant, &bits, &tile);
     P.tile_rows = (uint32_t)tile;
+    P.key_width = 4;
     for (int j = 0; j < a.nvals; ++j) P.val_width[j] = dtype_width(a.val_dtypes[j]);
 
     // small queries first (in query order), then large ones with 8-byte keys,
@@ -199,6 +204,7 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
         else if (dtype_width(Q.key.dtype) == 8) large8.push_back(q);
         else large4.push_back(q);
     }
+    if (!large8.empty()) P.key_width = 8;  // one 8-byte key widens every image
     P.row_offset.assign(a.nqueries, 0);
     uint64_t off = 0;
     for (uint32_t q : small) { P.row_offset[q] = off; off += a.queries[q].n; }
@@ -263,7 +269,8 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
     P.desc_bytes = o;
     P.o_counters = o; o = align_up(o + 64, A);  // [0]: small-kernel work counter, [8]: large group count
     P.o_seg_first = o; o = align_up(o + 4 * std::max<size_t>(1, P.segs.size()), A);
-    P.o_arena_keys = o; o = align_up(o + 8 * nl, A);
+    const size_t kw = (size_t)P.key_width;
+    P.o_arena_keys = o; o = align_up(o + kw * nl, A);
     P.o_arena_seg = o; o = align_up(o + 4 * nl, A);
     P.rec_bytes = gather_record_bytes(a.nvals);  // 0 for fewer than two value columns
     if (P.rec_bytes) {
@@ -272,13 +279,13 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
     } else {
         for (int j = 0; j < a.nvals; ++j) { P.o_arena_vals[j] = o; o = align_up(o + (size_t)P.val_width[j] * nl, A); }
     }
-    P.o_sorted_keys = o; o = align_up(o + 8 * nl, A);
+    P.o_sorted_keys = o; o = align_up(o + kw * nl, A);
     for (int j = 0; j < a.nvals; ++j) { P.o_sorted_vals[j] = o; o = align_up(o + (size_t)P.val_width[j] * nl, A); }
     P.o_group_seg = o; o = align_up(o + 4 * nl, A);
-    P.o_group_key = o; o = align_up(o + 8 * nl, A);
+    P.o_group_key = o; o = align_up(o + kw * nl, A);
     P.o_tail = o;
     size_t tail = seg_sort_workspace_bytes(nl, (uint32_t)P.segs.size(), (uint32_t)P.tile_seg.size(),
-                                           std::max(1, maxp), t.seg_variant);
+                                           std::max(1, maxp), t.seg_variant, P.key_width);
     tail = std::max(tail, segreduce_workspace_bytes(nl, a.nvals));
     P.ws_bytes = o + tail;
     return true;
@@ -306,10 +313,11 @@ BatchDev batch_dev_view(const BatchPlan& P, const vdf_batch_args& a, unsigned ch
     }
     b.arena_recs = P.rec_bytes ? ws + P.o_arena_recs : nullptr;
     b.rec_bytes = (int)P.rec_bytes;
-    b.arena_keys = reinterpret_cast<uint64_t*>(ws + P.o_arena_keys);
+    b.arena_keys = ws + P.o_arena_keys;
+    b.key_width = P.key_width;
     b.arena_seg = reinterpret_cast<uint32_t*>(ws + P.o_arena_seg);
     b.group_seg = reinterpret_cast<uint32_t*>(ws + P.o_group_seg);
-    b.group_key_img = reinterpret_cast<uint64_t*>(ws + P.o_group_key);
+    b.group_key_img = ws + P.o_group_key;
     b.n_large = P.n_large;
     b.large_base = P.large_base;
     b.perm_out = a.perm_out;
@@ -351,6 +359,7 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
         SegSortArgs sa{};
         sa.n = P.n_large;
         sa.keys = b.arena_keys;
+        sa.key_width = P.key_width;
         sa.segs = b.segs;
         sa.nsegs = b.nsegs;
         sa.tile_seg = reinterpret_cast<const uint32_t*>(ws + P.o_tile_seg);
@@ -360,7 +369,7 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
         sa.max_passes = P.max_passes;
         for (int g = 0; g < 16; ++g) sa.tiles_in_pass[g] = P.tiles_in_pass[g];
         sa.variant = P.tuning.seg_variant;
-        sa.keys_out = reinterpret_cast<uint64_t*>(ws + P.o_sorted_keys);
+        sa.keys_out = ws + P.o_sorted_keys;
         sa.perm_out = a.perm_out + P.large_base;
         sa.err = err;
         unsigned char* tail = ws + P.o_tail;
@@ -396,7 +405,7 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
         r.nkeys = 2;
         r.nvals = P.nvals;
         r.key[0] = SegCol{b.arena_seg, U32};
-        r.key[1] = SegCol{sa.keys_out, U64};
+        r.key[1] = SegCol{sa.keys_out, P.key_width == 8 ? U64 : U32};
         r.key_out[0] = b.group_seg;
         r.key_out[1] = b.group_key_img;
         for (int j = 0; j < P.nvals; ++j) {

@@ -53,10 +53,11 @@ struct BatchDev {
     unsigned char* arena_recs;             // or one record per row (two or more)
     int rec_bytes;
     vdf_agg_out aggs[VDF_BATCH_MAX_VALS];
-    uint64_t* arena_keys;        // [n_large] ordered key images
+    void* arena_keys;            // [n_large] ordered key images, key_width bytes each
+    int key_width;               // 8, or 4 when every large query's keys are 4 bytes
     uint32_t* arena_seg;         // [n_large] segment of each arena row
     uint32_t* group_seg;         // [groups] segment of each large-query group
-    uint64_t* group_key_img;     // [groups] ordered key image of each group
+    void* group_key_img;         // [groups] ordered key image of each group (key_width bytes)
     uint64_t n_large;
     uint64_t large_base;         // first arena row of the large queries
     uint32_t* perm_out;
@@ -73,6 +74,7 @@ struct BatchPlan {
     int nvals = 0;
     int val_width[VDF_BATCH_MAX_VALS] = {};
     uint32_t tile_rows = 0;
+    int key_width = 8;  // arena key image width
     std::vector<uint64_t> row_offset;
     std::vector<uint32_t> small_queries;
     std::vector<SegDesc> segs;

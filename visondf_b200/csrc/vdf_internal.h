@@ -133,8 +133,9 @@ cudaError_t flag_adjacent_ties(const void* sorted_keys, int width, uint64_t n, u
                                Profiler* prof = nullptr);
 
 // ---- segmented sort (many independent row ranges in one set of launches) ----
-// Keys are ordered 8-byte images (the batch packs them so); a segment whose
-// keys were 4 bytes wide has zero high halves and needs fewer passes.
+// Keys are ordered images (the batch packs them so), 8 bytes wide, or 4 when
+// every segment's keys are; a 4-byte key in an 8-byte image has a zero high
+// half and needs fewer passes.
 struct SegChunk {      // a histogram CTA's rows: part of one segment
     uint64_t row_start;
     uint32_t rows;
@@ -142,7 +143,8 @@ struct SegChunk {      // a histogram CTA's rows: part of one segment
 };
 struct SegSortArgs {
     uint64_t n;                   // arena rows (< 2^30)
-    const uint64_t* keys;         // [n] ordered keys
+    const void* keys;             // [n] ordered key images
+    int key_width;                // 8, or 4 when every segment's keys are 4 bytes
     const SegDesc* segs;          // device [nsegs]
     uint32_t nsegs;
     const uint32_t* tile_seg;     // device [ntiles]; segments with more passes first
@@ -152,13 +154,14 @@ struct SegSortArgs {
     int max_passes;
     uint32_t tiles_in_pass[16];   // launch width of pass g: tiles of segments with passes > g
     int variant;                  // index into the segmented variant table
-    uint64_t* keys_out;           // [n] sorted ordered keys (each segment in place)
+    void* keys_out;               // [n] sorted key images (each segment in place)
     uint32_t* perm_out;           // [n] arena row ids in sorted order
     uint32_t* err;
 };
 int seg_sort_variant_count();
 bool seg_sort_variant_info(int v, int* bits, int* tile_rows);
-size_t seg_sort_workspace_bytes(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes, int variant);
+size_t seg_sort_workspace_bytes(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes, int variant,
+                                int key_width = 8);
 cudaError_t run_seg_sort(const SegSortArgs& a, unsigned char* ws, cudaStream_t s, Profiler* prof = nullptr);
 
 // ---- gather ----------------------------------------------------------------

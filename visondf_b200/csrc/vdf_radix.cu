@@ -115,7 +115,8 @@ __global__ void __launch_bounds__(256) k_hist_scan(ScanArgs a) {
 // segment's passes at once, flushed into the segment's own rows
 // [seg][pass][radix] of the global histogram.
 struct SegHistArgs {
-    const uint64_t* keys;
+    const void* keys;
+    int key_width;
     const SegChunk* chunks;
     const SegDesc* segs;
     uint32_t* hist;
@@ -135,7 +136,9 @@ __global__ void __launch_bounds__(512) k_seg_hist(SegHistArgs a) {
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) sh_hist[i] = 0;
     __syncthreads();
     for (uint32_t r = threadIdx.x; r < ch.rows; r += blockDim.x) {
-        const uint64_t k = ldg_stream(a.keys + ch.row_start + r);
+        const uint64_t k = a.key_width == 8
+                               ? ldg_stream(static_cast<const unsigned long long*>(a.keys) + ch.row_start + r)
+                               : (uint64_t)ldg_stream(static_cast<const uint32_t*>(a.keys) + ch.row_start + r);
         for (uint32_t p = 0; p < passes; ++p)
             atomicAdd(&sh_hist[p * radix + (uint32_t)((k >> (p * a.bits)) & mask)], 1u);
     }
@@ -612,22 +615,28 @@ const PassVariant kVariants[] = {
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
-// Segmented sorts run over ordered 8-byte keys; [0] = first pass (arena
-// rows), [1] = later passes (ping-pong buffers).
+// Segmented sorts run over ordered key images of 8 or 4 bytes; k[w][m]: w = 1
+// for 8-byte images, m = 0 for the first pass (arena rows), 1 for later
+// passes (ping-pong buffers).  Both widths of a variant share its digit width
+// and tile.
 struct SegVariant {
     int bits, tile;
-    size_t smem;
-    PassKernel k[2];
+    size_t smem[2];
+    PassKernel k[2][2];
 };
 template <int BITS, int THREADS, int ITEMS, int MATCH, int MINB>
 SegVariant make_seg_variant() {
-    using C = OnesweepCfg<uint64_t, BITS, THREADS, ITEMS>;
+    using C4 = OnesweepCfg<uint32_t, BITS, THREADS, ITEMS>;
+    using C8 = OnesweepCfg<uint64_t, BITS, THREADS, ITEMS>;
     SegVariant v{};
     v.bits = BITS;
     v.tile = THREADS * ITEMS;
-    v.smem = C::SMEM;
-    v.k[0] = k_onesweep<uint64_t, BITS, THREADS, ITEMS, IN_RAW, false, MATCH, MINB, true>;
-    v.k[1] = k_onesweep<uint64_t, BITS, THREADS, ITEMS, IN_BUF, false, MATCH, MINB, true>;
+    v.smem[0] = C4::SMEM;
+    v.smem[1] = C8::SMEM;
+    v.k[0][0] = k_onesweep<uint32_t, BITS, THREADS, ITEMS, IN_RAW, false, MATCH, MINB, true>;
+    v.k[0][1] = k_onesweep<uint32_t, BITS, THREADS, ITEMS, IN_BUF, false, MATCH, MINB, true>;
+    v.k[1][0] = k_onesweep<uint64_t, BITS, THREADS, ITEMS, IN_RAW, false, MATCH, MINB, true>;
+    v.k[1][1] = k_onesweep<uint64_t, BITS, THREADS, ITEMS, IN_BUF, false, MATCH, MINB, true>;
     return v;
 }
 const SegVariant kSegVariants[] = {
@@ -856,15 +865,15 @@ struct SegLayout {
     size_t keys[2], vals[2], offs, zero, hist, counters, status[2], zero_bytes, total;
     uint32_t stride, radix;
 };
-SegLayout seg_layout(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes, int variant) {
+SegLayout seg_layout(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes, int variant, int key_width) {
     SegLayout L{};
     const SegVariant& v = kSegVariants[variant];
     L.radix = 1u << v.bits;
     L.stride = (uint32_t)max_passes * L.radix;
     const size_t A = 256;
     size_t off = 0;
-    L.keys[0] = off; off = align_up(off + n * 8, A);
-    L.keys[1] = off; off = align_up(off + n * 8, A);
+    L.keys[0] = off; off = align_up(off + n * (size_t)key_width, A);
+    L.keys[1] = off; off = align_up(off + n * (size_t)key_width, A);
     L.vals[0] = off; off = align_up(off + n * 4, A);
     L.vals[1] = off; off = align_up(off + n * 4, A);
     L.offs = off; off = align_up(off + (size_t)nsegs * L.stride * 4, A);
@@ -879,17 +888,20 @@ SegLayout seg_layout(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes
 }
 }  // namespace
 
-size_t seg_sort_workspace_bytes(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes, int variant) {
+size_t seg_sort_workspace_bytes(uint64_t n, uint32_t nsegs, uint32_t ntiles, int max_passes, int variant,
+                                int key_width) {
     if (variant < 0 || variant >= kNumSegVariants) return 0;
-    return seg_layout(n, nsegs, ntiles, max_passes, variant).total;
+    return seg_layout(n, nsegs, ntiles, max_passes, variant, key_width).total;
 }
 
 cudaError_t run_seg_sort(const SegSortArgs& sa, unsigned char* ws, cudaStream_t s, Profiler* prof) {
     if (sa.n == 0 || sa.ntiles == 0) return cudaSuccess;
     if (sa.variant < 0 || sa.variant >= kNumSegVariants || sa.max_passes < 1 || sa.max_passes > 16)
         return cudaErrorInvalidValue;
+    if (sa.key_width != 4 && sa.key_width != 8) return cudaErrorInvalidValue;
     const SegVariant& var = kSegVariants[sa.variant];
-    const SegLayout L = seg_layout(sa.n, sa.nsegs, sa.ntiles, sa.max_passes, sa.variant);
+    const int wi = sa.key_width == 8 ? 1 : 0;
+    const SegLayout L = seg_layout(sa.n, sa.nsegs, sa.ntiles, sa.max_passes, sa.variant, sa.key_width);
     cudaError_t e = cudaMemsetAsync(ws + L.zero, 0, L.zero_bytes, s);
     if (e != cudaSuccess) return e;
     uint32_t* hist = reinterpret_cast<uint32_t*>(ws + L.hist);
@@ -897,10 +909,10 @@ cudaError_t run_seg_sort(const SegSortArgs& sa, unsigned char* ws, cudaStream_t 
     uint32_t* counters = reinterpret_cast<uint32_t*>(ws + L.counters);
     uint32_t* status[2] = {reinterpret_cast<uint32_t*>(ws + L.status[0]),
                            reinterpret_cast<uint32_t*>(ws + L.status[1])};
-    uint64_t* kbuf[2] = {reinterpret_cast<uint64_t*>(ws + L.keys[0]), reinterpret_cast<uint64_t*>(ws + L.keys[1])};
+    void* kbuf[2] = {ws + L.keys[0], ws + L.keys[1]};
     uint32_t* vbuf[2] = {reinterpret_cast<uint32_t*>(ws + L.vals[0]), reinterpret_cast<uint32_t*>(ws + L.vals[1])};
 
-    SegHistArgs h{sa.keys, sa.chunks, sa.segs, hist, L.stride, (uint32_t)var.bits, sa.nsegs, sa.n};
+    SegHistArgs h{sa.keys, sa.key_width, sa.chunks, sa.segs, hist, L.stride, (uint32_t)var.bits, sa.nsegs, sa.n};
     if (prof) prof->begin(KC_HIST, s);
     k_seg_hist<<<sa.nchunks, 512, (size_t)L.stride * 4, s>>>(h);
     if (prof) prof->end(KC_HIST, s);
@@ -916,7 +928,7 @@ cudaError_t run_seg_sort(const SegSortArgs& sa, unsigned char* ws, cudaStream_t 
         PassArgs a{};
         a.n = sa.n;
         a.shift = (uint32_t)(g * var.bits);
-        a.dtype = U64;
+        a.dtype = sa.key_width == 8 ? U64 : U32;
         a.status = status[g & 1];
         a.status_next = (g + 1 < sa.max_passes) ? status[(g + 1) & 1] : nullptr;
         a.status_rows = sa.ntiles;
@@ -928,16 +940,17 @@ cudaError_t run_seg_sort(const SegSortArgs& sa, unsigned char* ws, cudaStream_t 
         a.seg_offs = offs;
         a.seg_stride = L.stride;
         a.pass = (uint32_t)g;
-        a.keys_in = g == 0 ? static_cast<const void*>(sa.keys) : static_cast<const void*>(kbuf[(g - 1) & 1]);
+        a.keys_in = g == 0 ? sa.keys : static_cast<const void*>(kbuf[(g - 1) & 1]);
         a.vals_in = g == 0 ? nullptr : vbuf[(g - 1) & 1];
         a.keys_out = kbuf[g & 1];
         a.vals_out = vbuf[g & 1];
         a.keys_final = sa.keys_out;
         a.vals_final = sa.perm_out;
-        if (prof) prof->begin(KC_ONESWEEP64, s);
-        var.k[g == 0 ? 0 : 1]<<<grid, 256, var.smem, s>>>(a);
+        const int cls = wi ? KC_ONESWEEP64 : KC_ONESWEEP32;
+        if (prof) prof->begin(cls, s);
+        var.k[wi][g == 0 ? 0 : 1]<<<grid, 256, var.smem[wi], s>>>(a);
         e = cudaGetLastError();
-        if (prof) prof->end(KC_ONESWEEP64, s);
+        if (prof) prof->end(cls, s);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -983,10 +996,12 @@ cudaError_t prepare_sort_kernels() {
                 if (e != cudaSuccess) return e;
             }
     for (const SegVariant& v : kSegVariants)
-        for (int m = 0; m < 2; ++m) {
-            cudaError_t e = cudaFuncSetAttribute(v.k[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
-            if (e != cudaSuccess) return e;
-        }
+        for (int w = 0; w < 2; ++w)
+            for (int m = 0; m < 2; ++m) {
+                cudaError_t e =
+                    cudaFuncSetAttribute(v.k[w][m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem[w]);
+                if (e != cudaSuccess) return e;
+            }
     {
         cudaError_t e = cudaFuncSetAttribute(k_seg_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              8 * kMaxRadix * 4);

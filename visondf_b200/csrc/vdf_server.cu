@@ -349,9 +349,9 @@ vdf_status vdf_server_create(const vdf_server_config* cfg, vdf_server** out) {
                                                      : vdf::BatchTuning{cfg->small_rows, cfg->small_bits,
                                                                         cfg->seg_variant};
         if (vdf::plan_batch(P, a, t, why)) {
-            // queries with 4-byte keys pack no differently; the plan's tail is
-            // the largest need, plus descriptor tables for a full batch of
-            // queries
+            // 8-byte keys need the most (a batch whose large queries all have
+            // 4-byte keys packs 4-byte images); the plan's tail is the largest
+            // need, plus descriptor tables for a full batch of queries
             const size_t desc = (sizeof(vdf::BatchQuery) + sizeof(vdf::SegDesc) + sizeof(vdf::SegChunk) + 16) *
                                 (size_t)cfg->max_batch_queries + 4 * ((size_t)cfg->max_batch_rows / 1024 + 8);
             st = vdf_ctx_reserve(c, P.ws_bytes + desc + (P.ws_bytes >> 4));
