@@ -93,6 +93,30 @@ def test_long_segments_cross_many_tiles(ctx):
     np.testing.assert_allclose(host(gr.aggs[0].sum), og.sum[0], rtol=1e-12)
 
 
+@pytest.mark.parametrize("tail", [[1] * 300, [1] * 295 + [5]])
+def test_tiles_of_single_row_groups_beside_scanned_tiles(ctx, tail):
+    """Tiles (512 rows) where every row starts a group take a path without a
+    scan; this places them next to tiles that scan, with a group crossing
+    the first tile boundary, a group covering whole tiles, a whole-tile group
+    ending exactly at a boundary before a single-row tile, and a last tile
+    that is partial."""
+    runs = [1] * 511 + [2] + [1] * 511 + [1] * 512 + [1500] + [1] * 36 + [512] + [1] * 512 + tail
+    n = int(np.sum(runs))
+    key = np.repeat(np.arange(len(runs), dtype=np.int64) * 3 - 1000, runs)
+    rng = np.random.default_rng(21)
+    v1 = rng.standard_normal(n)
+    v2 = rng.integers(-2**62, 2**62, size=n, dtype=np.int64)
+    og = ob.groupby([key], [v1, v2])
+    gr = ctx.groupby_sorted([dev(key)], [dev(v1), dev(v2)], want_row_group=True, want_group_start=True)
+    compare(og, gr, [v1, v2], "sorted mix")
+    starts = np.concatenate([[0], np.cumsum(runs)[:-1]])
+    assert (host(gr.group_start).view(np.uint32) == starts).all()
+    assert (host(gr.row_group).view(np.uint32) == np.repeat(np.arange(len(runs)), runs)).all()
+    shuffled = rng.permutation(n)
+    gs = ctx.sort_groupby([dev(key[shuffled])], [dev(v1[shuffled]), dev(v2[shuffled])], agg_cols=[0, 1])
+    compare(og, gs, [v1, v2], "shuffled mix")
+
+
 def test_int64_sum_overflow_is_exact(ctx):
     n = 300_000
     key = np.zeros(n, np.int64)

@@ -260,18 +260,14 @@ __host__ __device__ constexpr size_t emit_smem_bytes() {
     return stage_offset<NK, NV>() + sizeof(WarpStage<NK, NV, kSegItems>) * (kSegThreads / 32);
 }
 
-// Head flags and the fold of this thread's rows into one aggregate.
-template <int NK, int NV>
-__device__ __forceinline__ Agg<NV> fold_rows(const SegArgs& a, uint64_t row0, int lane, const int* vc, const int* kw,
-                                             uint32_t& hmask) {
+// Head flags of this thread's rows (bit j: row row0 + j starts a group).
+template <int NK>
+__device__ __forceinline__ uint32_t row_heads(const SegArgs& a, uint64_t row0, int lane, const int* kw) {
     constexpr int ITEMS = kSegItems;
     const uint64_t n = a.n;
     uint64_t key[ITEMS][NK];
-    uint64_t val[ITEMS][NV > 0 ? NV : 1];
 #pragma unroll
     for (int k = 0; k < NK; ++k) load_rows<ITEMS>(a.key[k].src, kw[k], row0, n, key, k);
-#pragma unroll
-    for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
     uint64_t prev[NK];
 #pragma unroll
     for (int k = 0; k < NK; ++k) prev[k] = __shfl_up_sync(0xffffffffu, key[ITEMS - 1][k], 1);
@@ -279,7 +275,7 @@ __device__ __forceinline__ Agg<NV> fold_rows(const SegArgs& a, uint64_t row0, in
 #pragma unroll
         for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], row0 - 1);
     }
-    hmask = 0;
+    uint32_t hmask = 0;
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const uint64_t r = row0 + j;
@@ -288,6 +284,17 @@ __device__ __forceinline__ Agg<NV> fold_rows(const SegArgs& a, uint64_t row0, in
         for (int k = 0; k < NK; ++k) h |= (j == 0 ? prev[k] : key[j - 1][k]) != key[j][k];
         if (r < n && h) hmask |= 1u << j;
     }
+    return hmask;
+}
+
+// The fold of this thread's rows into one aggregate, given their head flags.
+template <int NV>
+__device__ __forceinline__ Agg<NV> fold_rows(const SegArgs& a, uint64_t row0, const int* vc, uint32_t hmask) {
+    constexpr int ITEMS = kSegItems;
+    const uint64_t n = a.n;
+    uint64_t val[ITEMS][NV > 0 ? NV : 1];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
     Agg<NV> t = agg_identity<NV>();
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
@@ -608,6 +615,59 @@ __global__ void __launch_bounds__(kScanTiles) k_seg_scan2(const SegArgs a, Agg<N
 }
 
 // ---- phase 3: scan each tile from its prefix and emit the groups -------------
+// A tile where every row starts a group (typical when most keys are
+// distinct) needs no scan: row r is group H + (r - first row), H = heads
+// before the tile, and the group ending at row r - 1 is emitted at row r as
+// everywhere else, so a row's own one-row record is written here when the
+// next row is in the tile (or r is the last row) and the tile's first row
+// emits the group carried in from earlier tiles.  Every column is written
+// by consecutive lanes.  Records are built with the same operations as the
+// scanning path, so results are bit-identical.
+template <int NK, int NV>
+__device__ __forceinline__ void emit_single_rows(const SegArgs& a, const Agg<NV>* tile_prefix,
+                                                 const Agg<NV>* block_prefix, uint32_t tile, uint32_t H,
+                                                 const int* vc, const int* kw) {
+    constexpr int ITEMS = kSegItems;
+    const int tid = threadIdx.x;
+    const uint64_t n = a.n;
+    const uint64_t first = (uint64_t)tile * kSegTile;
+    if (tid == 0 && H > 0) {
+        const Agg<NV> P = agg_combine(block_prefix[tile / kScanTiles], tile_prefix[tile], vc);
+        emit_group<NV>(a, H - 1, P.cnt, P.w, vc);
+    }
+    // every load before the first store (outputs may not be assumed apart
+    // from inputs, so the compiler would not reorder them)
+    uint64_t kx[ITEMS][NK];
+    uint64_t vx[ITEMS][NV > 0 ? NV : 1];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint64_t r = first + (uint64_t)j * kSegThreads + tid;
+#pragma unroll
+        for (int k = 0; k < NK; ++k) kx[j][k] = r < n ? load_raw(a.key[k].src, kw[k], r) : 0ull;
+#pragma unroll
+        for (int v = 0; v < NV; ++v) vx[j][v] = r < n ? load_val(a.val[v].src, a.val[v].dtype, r) : 0ull;
+    }
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t o = (uint32_t)j * kSegThreads + (uint32_t)tid;
+        const uint64_t r = first + o;
+        if (r >= n) break;
+        const uint32_t g = H + o;
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+            if (a.key_out[k]) store_raw(a.key_out[k], kw[k], g, kx[j][k]);
+        if (a.group_start) a.group_start[g] = (uint32_t)r;
+        if (a.row_group) a.row_group[r] = g;
+        if (o + 1 < (uint32_t)kSegTile || r == n - 1) {
+            uint64_t w[NV > 0 ? NV : 1][4];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) col_init(w[v], vx[j][v], vc[v]);
+            emit_group<NV>(a, g, 1, w, vc);
+        }
+        if (r == n - 1 && a.n_groups) *a.n_groups = g + 1;
+    }
+}
+
 template <int NK, int NV>
 __device__ __forceinline__ void seg_emit_body(const SegArgs& a, const Agg<NV>* tile_prefix, const Agg<NV>* block_prefix,
                                               uint32_t tile) {
@@ -618,8 +678,15 @@ __device__ __forceinline__ void seg_emit_body(const SegArgs& a, const Agg<NV>* t
     Agg<NV>* s_warp = reinterpret_cast<Agg<NV>*>(seg_smem);  // [8] warp totals, [8] tile prefix
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
-    uint32_t hmask;
-    const Agg<NV> t = fold_rows<NK, NV>(a, row0, lane, vc, kw, hmask);
+    // heads before the tile, loaded first so that its latency overlaps the key loads
+    const uint32_t H_tile = block_prefix[tile / kScanTiles].heads + tile_prefix[tile].heads;
+    const uint32_t hmask = row_heads<NK>(a, row0, lane, kw);
+    const uint32_t nvalid = row0 >= n ? 0u : (n - row0 >= (uint64_t)ITEMS ? (uint32_t)ITEMS : (uint32_t)(n - row0));
+    if (__syncthreads_and(hmask == (1u << nvalid) - 1u)) {
+        emit_single_rows<NK, NV>(a, tile_prefix, block_prefix, tile, H_tile, vc, kw);
+        return;
+    }
+    const Agg<NV> t = fold_rows<NV>(a, row0, vc, hmask);
     // Per warp: the aggregate of the lanes before each lane (lx) and the
     // warp's total.  When every lane's first row starts a group (typical with
     // many groups), no segment crosses into a lane, so a lane's carry is just
