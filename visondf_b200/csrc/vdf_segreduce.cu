@@ -253,7 +253,7 @@ extern __shared__ __align__(16) unsigned char seg_smem[];
 
 template <int NK, int NV>
 __host__ __device__ constexpr size_t stage_offset() {
-    return ((sizeof(Agg<NV>) * (kSegThreads / 32 + 1) + 15) / 16) * 16;
+    return ((sizeof(Agg<NV>) * 2 * (kSegThreads / 32 + 1) + 15) / 16) * 16;
 }
 template <int NK, int NV>
 __host__ __device__ constexpr size_t emit_smem_bytes() {
@@ -623,48 +623,52 @@ __global__ void __launch_bounds__(kScanTiles) k_seg_scan2(const SegArgs a, Agg<N
 // emits the group carried in from earlier tiles.  Every column is written
 // by consecutive lanes.  Records are built with the same operations as the
 // scanning path, so results are bit-identical.
-template <int NK, int NV>
+// TPT threads cover the tile, RPT rows each (row tile_first + j * TPT + tt),
+// loaded BATCH rows at a time before they are stored.
+template <int NK, int NV, int TPT, int RPT, int BATCH>
 __device__ __forceinline__ void emit_single_rows(const SegArgs& a, const Agg<NV>* tile_prefix,
                                                  const Agg<NV>* block_prefix, uint32_t tile, uint32_t H,
-                                                 const int* vc, const int* kw) {
-    constexpr int ITEMS = kSegItems;
-    const int tid = threadIdx.x;
+                                                 const int* vc, const int* kw, int tt) {
+    static_assert(TPT * RPT == kSegTile && RPT % BATCH == 0, "tile layout");
     const uint64_t n = a.n;
     const uint64_t first = (uint64_t)tile * kSegTile;
-    if (tid == 0 && H > 0) {
+    if (tt == 0 && H > 0) {
         const Agg<NV> P = agg_combine(block_prefix[tile / kScanTiles], tile_prefix[tile], vc);
         emit_group<NV>(a, H - 1, P.cnt, P.w, vc);
     }
-    // every load before the first store (outputs may not be assumed apart
-    // from inputs, so the compiler would not reorder them)
-    uint64_t kx[ITEMS][NK];
-    uint64_t vx[ITEMS][NV > 0 ? NV : 1];
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint64_t r = first + (uint64_t)j * kSegThreads + tid;
+    for (int j0 = 0; j0 < RPT; j0 += BATCH) {
+        // every load of the batch before its first store (outputs may not be
+        // assumed apart from inputs, so the compiler would not reorder them)
+        uint64_t kx[BATCH][NK];
+        uint64_t vx[BATCH][NV > 0 ? NV : 1];
 #pragma unroll
-        for (int k = 0; k < NK; ++k) kx[j][k] = r < n ? load_raw(a.key[k].src, kw[k], r) : 0ull;
+        for (int j = 0; j < BATCH; ++j) {
+            const uint64_t r = first + (uint64_t)(j0 + j) * TPT + tt;
 #pragma unroll
-        for (int v = 0; v < NV; ++v) vx[j][v] = r < n ? load_val(a.val[v].src, a.val[v].dtype, r) : 0ull;
-    }
+            for (int k = 0; k < NK; ++k) kx[j][k] = r < n ? load_raw(a.key[k].src, kw[k], r) : 0ull;
 #pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t o = (uint32_t)j * kSegThreads + (uint32_t)tid;
-        const uint64_t r = first + o;
-        if (r >= n) break;
-        const uint32_t g = H + o;
-#pragma unroll
-        for (int k = 0; k < NK; ++k)
-            if (a.key_out[k]) store_raw(a.key_out[k], kw[k], g, kx[j][k]);
-        if (a.group_start) a.group_start[g] = (uint32_t)r;
-        if (a.row_group) a.row_group[r] = g;
-        if (o + 1 < (uint32_t)kSegTile || r == n - 1) {
-            uint64_t w[NV > 0 ? NV : 1][4];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) col_init(w[v], vx[j][v], vc[v]);
-            emit_group<NV>(a, g, 1, w, vc);
+            for (int v = 0; v < NV; ++v) vx[j][v] = r < n ? load_val(a.val[v].src, a.val[v].dtype, r) : 0ull;
         }
-        if (r == n - 1 && a.n_groups) *a.n_groups = g + 1;
+#pragma unroll
+        for (int j = 0; j < BATCH; ++j) {
+            const uint32_t o = (uint32_t)(j0 + j) * TPT + (uint32_t)tt;
+            const uint64_t r = first + o;
+            if (r >= n) break;
+            const uint32_t g = H + o;
+#pragma unroll
+            for (int k = 0; k < NK; ++k)
+                if (a.key_out[k]) store_raw(a.key_out[k], kw[k], g, kx[j][k]);
+            if (a.group_start) a.group_start[g] = (uint32_t)r;
+            if (a.row_group) a.row_group[r] = g;
+            if (o + 1 < (uint32_t)kSegTile || r == n - 1) {
+                uint64_t w[NV > 0 ? NV : 1][4];
+#pragma unroll
+                for (int v = 0; v < NV; ++v) col_init(w[v], vx[j][v], vc[v]);
+                emit_group<NV>(a, g, 1, w, vc);
+            }
+            if (r == n - 1 && a.n_groups) *a.n_groups = g + 1;
+        }
     }
 }
 
@@ -675,7 +679,7 @@ __device__ __forceinline__ void seg_emit_body(const SegArgs& a, const Agg<NV>* t
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint64_t n = a.n;
     const uint64_t row0 = (uint64_t)tile * kSegTile + (uint64_t)tid * ITEMS;
-    Agg<NV>* s_warp = reinterpret_cast<Agg<NV>*>(seg_smem);  // [8] warp totals, [8] tile prefix
+    Agg<NV>* s_warp = reinterpret_cast<Agg<NV>*>(seg_smem);  // two buffers of [1 + 8] (see below)
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
     // heads before the tile, loaded first so that its latency overlaps the key loads
@@ -683,7 +687,8 @@ __device__ __forceinline__ void seg_emit_body(const SegArgs& a, const Agg<NV>* t
     const uint32_t hmask = row_heads<NK>(a, row0, lane, kw);
     const uint32_t nvalid = row0 >= n ? 0u : (n - row0 >= (uint64_t)ITEMS ? (uint32_t)ITEMS : (uint32_t)(n - row0));
     if (__syncthreads_and(hmask == (1u << nvalid) - 1u)) {
-        emit_single_rows<NK, NV>(a, tile_prefix, block_prefix, tile, H_tile, vc, kw);
+        emit_single_rows<NK, NV, kSegThreads, kSegItems, kSegItems>(a, tile_prefix, block_prefix, tile, H_tile, vc,
+                                                                     kw, tid);
         return;
     }
     const Agg<NV> t = fold_rows<NV>(a, row0, vc, hmask);
@@ -717,13 +722,27 @@ __device__ __forceinline__ void seg_emit_body(const SegArgs& a, const Agg<NV>* t
         if (lane == 0) lx = agg_identity<NV>();
         wtot = incl;
     }
-    if (lane == 31) s_warp[warp] = wtot;
-    if (tid == 0)
-        s_warp[kSegThreads / 32] = agg_combine(block_prefix[tile / kScanTiles], tile_prefix[tile], vc);
+    // [0] tile prefix, [1 + w] total of warp w; warp 0 scans these nine
+    // entries in shared memory (double-buffered, four steps) into each warp's
+    // exclusive prefix, so every thread then combines once
+    constexpr int WARPS = kSegThreads / 32;
+    if (lane == 31) s_warp[1 + warp] = wtot;
+    if (tid == 0) s_warp[0] = agg_combine(block_prefix[tile / kScanTiles], tile_prefix[tile], vc);
     __syncthreads();
-    Agg<NV> pre = s_warp[kSegThreads / 32];
-    for (int w2 = 0; w2 < warp; ++w2) pre = agg_combine(pre, s_warp[w2], vc);
-    pre = agg_combine(pre, lx, vc);
+    if (warp == 0) {
+        Agg<NV>* src = s_warp;
+        Agg<NV>* dst = s_warp + (WARPS + 1);
+#pragma unroll 1
+        for (int d = 1; d <= WARPS; d <<= 1) {
+            if (lane <= WARPS) dst[lane] = lane >= d ? agg_combine(src[lane - d], src[lane], vc) : src[lane];
+            __syncwarp();
+            Agg<NV>* t2 = src;
+            src = dst;
+            dst = t2;
+        }
+    }
+    __syncthreads();
+    const Agg<NV> pre = agg_combine(s_warp[warp], lx, vc);  // four steps: the result is back in s_warp
 
     // A segment is complete when the next head (or the last row) is reached;
     // the thread that reaches it produces the group's record.  The groups a
@@ -824,6 +843,189 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : (NV == 2 ? 4 : 3))
     }
 }
 
+// The emit pass with eight rows per thread: each 512-row tile is taken by
+// two warps (kSubTiles tiles per CTA, as in the reduce pass), so a warp scan
+// of aggregates and the cross-warp step are shared by eight rows instead of
+// two, and each row costs one merge in the final walk.  A thread's rows are
+// consecutive: its groups complete in order and are written as they
+// complete.  Tiles where every row starts a group take the one-row-record
+// path with coalesced writes.
+template <int NK, int NV>
+__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2))
+    k_seg_emit_wide(SegArgs a, const Agg<NV>* tile_prefix, const Agg<NV>* block_prefix, uint32_t tiles) {
+    constexpr int ITEMS = kWideItems, WARPS = kSegThreads / 32;
+    __shared__ Agg<NV> s_wtot[WARPS];
+    __shared__ Agg<NV> s_pre[kSubTiles];
+    __shared__ uint32_t s_all[WARPS];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int sub = warp / kWarpsPerSub, wsub = warp - sub * kWarpsPerSub;
+    const uint32_t tile = blockIdx.x * kSubTiles + sub;
+    const bool tvalid = tile < tiles;
+    const int sub_tid = tid - sub * kWarpsPerSub * 32;
+    const uint64_t n = a.n;
+    const uint64_t row0 = (uint64_t)tile * kSegTile + (uint64_t)sub_tid * ITEMS;
+    int vc[NV > 0 ? NV : 1], kw[NK];
+    seg_setup<NK, NV>(a, vc, kw);
+    // heads before the tile, loaded first so that its latency overlaps the key loads
+    const uint32_t H_tile = tvalid ? block_prefix[tile / kScanTiles].heads + tile_prefix[tile].heads : 0u;
+
+    uint32_t hmask = 0;
+    {
+        uint64_t key[ITEMS][NK];
+#pragma unroll
+        for (int k = 0; k < NK; ++k) load_rows<ITEMS>(a.key[k].src, kw[k], row0, n, key, k);
+        uint64_t prev[NK];
+#pragma unroll
+        for (int k = 0; k < NK; ++k) prev[k] = __shfl_up_sync(0xffffffffu, key[ITEMS - 1][k], 1);
+        if (lane == 0 && row0 > 0 && row0 < n) {
+#pragma unroll
+            for (int k = 0; k < NK; ++k) prev[k] = load_raw(a.key[k].src, kw[k], row0 - 1);
+        }
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint64_t r = row0 + j;
+            bool h = (r == 0);
+#pragma unroll
+            for (int k = 0; k < NK; ++k) h |= (j == 0 ? prev[k] : key[j - 1][k]) != key[j][k];
+            if (r < n && h) hmask |= 1u << j;
+        }
+    }
+    const uint32_t nvalid = row0 >= n ? 0u : (n - row0 >= (uint64_t)ITEMS ? (uint32_t)ITEMS : (uint32_t)(n - row0));
+    const bool wall = __all_sync(0xffffffffu, hmask == (1u << nvalid) - 1u);
+    if (lane == 0) s_all[warp] = wall ? 1u : 0u;
+    __syncthreads();
+    bool sub_all = true;
+#pragma unroll
+    for (int w = 0; w < kWarpsPerSub; ++w) sub_all = sub_all && s_all[sub * kWarpsPerSub + w] != 0u;
+
+    Agg<NV> lx = agg_identity<NV>();
+    if (!sub_all) {
+        // this thread's trailing segment: rows from its last head (all rows
+        // when it has none)
+        uint64_t val[ITEMS][NV > 0 ? NV : 1];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
+        const int from = hmask ? 31 - __clz(hmask) : 0;
+        Agg<NV> t = agg_identity<NV>();
+        t.heads = __popc(hmask);
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (j < from || row0 + j >= n) continue;
+            if (t.cnt == 0) {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) col_init(t.w[v], val[j][v], vc[v]);
+            } else {
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    uint64_t one[4];
+                    col_init(one, val[j][v], vc[v]);
+                    col_merge(t.w[v], one, vc[v]);
+                }
+            }
+            t.cnt++;
+        }
+        // per warp: the aggregate of the lanes before each lane, and the total
+        Agg<NV> wtot;
+        if (__all_sync(0xffffffffu, row0 >= n || (hmask & 1u))) {
+            // no segment crosses into a lane: carry = previous lane's trailing
+            // segment, plus a count of heads
+            const uint32_t h = __popc(hmask);
+            uint32_t ih = h;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t o = __shfl_up_sync(0xffffffffu, ih, d);
+                if (lane >= d) ih += o;
+            }
+            lx = agg_shfl_up(t, 1);
+            lx.heads = ih - h;
+            if (lane == 0) lx = agg_identity<NV>();
+            wtot = t;
+            wtot.heads = ih;
+        } else {
+            Agg<NV> incl = t;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const Agg<NV> o = agg_shfl_up(incl, d);
+                if (lane >= d) incl = agg_combine(o, incl, vc);
+            }
+            lx = agg_shfl_up(incl, 1);
+            if (lane == 0) lx = agg_identity<NV>();
+            wtot = incl;
+        }
+        if (lane == 31) s_wtot[warp] = wtot;
+        if (wsub == 0 && lane == 0 && tvalid)
+            s_pre[sub] = agg_combine(block_prefix[tile / kScanTiles], tile_prefix[tile], vc);
+    }
+    __syncthreads();
+
+    if (sub_all) {
+        if (tvalid)
+            emit_single_rows<NK, NV, kWarpsPerSub * 32, ITEMS, ITEMS / 2>(a, tile_prefix, block_prefix, tile, H_tile,
+                                                                          vc, kw, sub_tid);
+        return;
+    }
+    if (row0 >= n) return;
+    Agg<NV> pre = s_pre[sub];
+#pragma unroll
+    for (int w = 0; w < kWarpsPerSub; ++w)
+        if (w < wsub) pre = agg_combine(pre, s_wtot[sub * kWarpsPerSub + w], vc);
+    pre = agg_combine(pre, lx, vc);
+
+    // walk this thread's rows: a head completes the group before it
+    uint64_t val[ITEMS][NV > 0 ? NV : 1];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
+    uint32_t gid = pre.heads;
+    uint32_t cnt = pre.cnt;
+    uint64_t w[NV > 0 ? NV : 1][4];
+#pragma unroll
+    for (int v = 0; v < NV; ++v)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[v][q] = pre.w[v][q];
+    uint32_t rg[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint64_t r = row0 + j;
+        rg[j] = 0;
+        if (r >= n) continue;
+        if ((hmask >> j) & 1u) {
+            if (gid > 0) emit_group<NV>(a, gid - 1, cnt, w, vc);
+#pragma unroll
+            for (int k = 0; k < NK; ++k)
+                if (a.key_out[k]) store_raw(a.key_out[k], kw[k], gid, load_raw(a.key[k].src, kw[k], r));
+            if (a.group_start) a.group_start[gid] = (uint32_t)r;
+            ++gid;
+            cnt = 1;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) col_init(w[v], val[j][v], vc[v]);
+        } else {
+            ++cnt;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                uint64_t one[4];
+                col_init(one, val[j][v], vc[v]);
+                col_merge(w[v], one, vc[v]);
+            }
+        }
+        rg[j] = gid - 1;
+        if (r == n - 1) {
+            emit_group<NV>(a, gid - 1, cnt, w, vc);
+            if (a.n_groups) *a.n_groups = gid;
+        }
+    }
+    if (a.row_group) {
+        if (row0 + ITEMS <= n && (reinterpret_cast<uintptr_t>(a.row_group + row0) & 15) == 0) {
+            uint4* d = reinterpret_cast<uint4*>(a.row_group + row0);
+            d[0] = make_uint4(rg[0], rg[1], rg[2], rg[3]);
+            d[1] = make_uint4(rg[4], rg[5], rg[6], rg[7]);
+        } else {
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j)
+                if (row0 + j < n) a.row_group[row0 + j] = rg[j];
+        }
+    }
+}
+
 template <int NK, int NV>
 cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaStream_t s, Profiler* prof) {
     Agg<NV>* ta = reinterpret_cast<Agg<NV>*>(aggs);
@@ -841,7 +1043,10 @@ cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaS
     if (prof) prof->end(KC_SEGSCAN, s);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (prof) prof->begin(KC_SEGEMIT, s);
-    k_seg_emit<NK, NV><<<grid, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta, bt, tiles);
+    if constexpr (NV <= 2)
+        k_seg_emit_wide<NK, NV><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+    else
+        k_seg_emit<NK, NV><<<grid, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta, bt, tiles);
     if (prof) prof->end(KC_SEGEMIT, s);
     return cudaGetLastError();
 }
