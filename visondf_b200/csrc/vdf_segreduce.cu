@@ -851,7 +851,7 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : (NV == 2 ? 4 : 3))
 // complete.  Tiles where every row starts a group take the one-row-record
 // path with coalesced writes.
 template <int NK, int NV>
-__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2))
+__global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     k_seg_emit_wide(SegArgs a, const Agg<NV>* tile_prefix, const Agg<NV>* block_prefix, uint32_t tiles) {
     constexpr int ITEMS = kWideItems, WARPS = kSegThreads / 32;
     __shared__ Agg<NV> s_wtot[WARPS];
@@ -901,28 +901,36 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2))
     Agg<NV> lx = agg_identity<NV>();
     if (!sub_all) {
         // this thread's trailing segment: rows from its last head (all rows
-        // when it has none)
+        // when it has none).  Rows are consumed from the front of a shift
+        // register, so the loop stays rolled (one copy of the merge code)
+        // while the values stay in registers.
         uint64_t val[ITEMS][NV > 0 ? NV : 1];
 #pragma unroll
         for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
         const int from = hmask ? 31 - __clz(hmask) : 0;
+        const int upto = (int)nvalid;
         Agg<NV> t = agg_identity<NV>();
         t.heads = __popc(hmask);
+#pragma unroll 1
+        for (int j = 0; j < upto; ++j) {
+            if (j >= from) {
+                if (t.cnt == 0) {
 #pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            if (j < from || row0 + j >= n) continue;
-            if (t.cnt == 0) {
+                    for (int v = 0; v < NV; ++v) col_init(t.w[v], val[0][v], vc[v]);
+                } else {
 #pragma unroll
-                for (int v = 0; v < NV; ++v) col_init(t.w[v], val[j][v], vc[v]);
-            } else {
-#pragma unroll
-                for (int v = 0; v < NV; ++v) {
-                    uint64_t one[4];
-                    col_init(one, val[j][v], vc[v]);
-                    col_merge(t.w[v], one, vc[v]);
+                    for (int v = 0; v < NV; ++v) {
+                        uint64_t one[4];
+                        col_init(one, val[0][v], vc[v]);
+                        col_merge(t.w[v], one, vc[v]);
+                    }
                 }
+                t.cnt++;
             }
-            t.cnt++;
+#pragma unroll
+            for (int i = 0; i + 1 < ITEMS; ++i)
+#pragma unroll
+                for (int v = 0; v < NV; ++v) val[i][v] = val[i + 1][v];
         }
         // per warp: the aggregate of the lanes before each lane, and the total
         Agg<NV> wtot;
@@ -943,7 +951,7 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2))
             wtot.heads = ih;
         } else {
             Agg<NV> incl = t;
-#pragma unroll
+#pragma unroll 1
             for (int d = 1; d < 32; d <<= 1) {
                 const Agg<NV> o = agg_shfl_up(incl, d);
                 if (lane >= d) incl = agg_combine(o, incl, vc);
@@ -971,7 +979,8 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2))
         if (w < wsub) pre = agg_combine(pre, s_wtot[sub * kWarpsPerSub + w], vc);
     pre = agg_combine(pre, lx, vc);
 
-    // walk this thread's rows: a head completes the group before it
+    // walk this thread's rows (rolled, over a shift register): a head
+    // completes the group before it
     uint64_t val[ITEMS][NV > 0 ? NV : 1];
 #pragma unroll
     for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
@@ -983,11 +992,10 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2))
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[v][q] = pre.w[v][q];
     uint32_t rg[ITEMS];
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
+    const int upto = (int)nvalid;
+#pragma unroll 1
+    for (int j = 0; j < upto; ++j) {
         const uint64_t r = row0 + j;
-        rg[j] = 0;
-        if (r >= n) continue;
         if ((hmask >> j) & 1u) {
             if (gid > 0) emit_group<NV>(a, gid - 1, cnt, w, vc);
 #pragma unroll
@@ -997,31 +1005,38 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 2))
             ++gid;
             cnt = 1;
 #pragma unroll
-            for (int v = 0; v < NV; ++v) col_init(w[v], val[j][v], vc[v]);
+            for (int v = 0; v < NV; ++v) col_init(w[v], val[0][v], vc[v]);
         } else {
             ++cnt;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 uint64_t one[4];
-                col_init(one, val[j][v], vc[v]);
+                col_init(one, val[0][v], vc[v]);
                 col_merge(w[v], one, vc[v]);
             }
         }
-        rg[j] = gid - 1;
-        if (r == n - 1) {
-            emit_group<NV>(a, gid - 1, cnt, w, vc);
-            if (a.n_groups) *a.n_groups = gid;
+#pragma unroll
+        for (int i = 0; i + 1 < ITEMS; ++i) {
+            rg[i] = rg[i + 1];
+#pragma unroll
+            for (int v = 0; v < NV; ++v) val[i][v] = val[i + 1][v];
         }
+        rg[ITEMS - 1] = gid - 1;
+    }
+    if (row0 + upto == n) {  // this thread holds the last row: its group ends there
+        emit_group<NV>(a, gid - 1, cnt, w, vc);
+        if (a.n_groups) *a.n_groups = gid;
     }
     if (a.row_group) {
-        if (row0 + ITEMS <= n && (reinterpret_cast<uintptr_t>(a.row_group + row0) & 15) == 0) {
+        // after upto shifts the row groups sit in rg[ITEMS - upto ..]
+        if (upto == ITEMS && (reinterpret_cast<uintptr_t>(a.row_group + row0) & 15) == 0) {
             uint4* d = reinterpret_cast<uint4*>(a.row_group + row0);
             d[0] = make_uint4(rg[0], rg[1], rg[2], rg[3]);
             d[1] = make_uint4(rg[4], rg[5], rg[6], rg[7]);
         } else {
 #pragma unroll
             for (int j = 0; j < ITEMS; ++j)
-                if (row0 + j < n) a.row_group[row0 + j] = rg[j];
+                if (j >= ITEMS - upto) a.row_group[row0 + j - (ITEMS - upto)] = rg[j];
         }
     }
 }
