@@ -644,6 +644,7 @@ const SegVariant kSegVariants[] = {
     make_seg_variant<8, 256, 12, 2, 2>(),   // 1
     make_seg_variant<8, 256, 16, 0, 2>(),   // 2
     make_seg_variant<11, 256, 8, 1, 2>(),   // 3
+    make_seg_variant<8, 256, 12, 2, 4>(),   // 4
 };
 constexpr int kNumSegVariants = (int)(sizeof(kSegVariants) / sizeof(kSegVariants[0]));
 
