@@ -262,6 +262,17 @@ def batched_section(args, local_rank: int) -> dict:
     canonical = sum(c0_canonical_bytes(int(k.numel()), k.element_size(), int(g)) for (k, _), g in zip(queries, ng))
     peak, _ = measured_peaks()
     info = b.info()
+    # per-kernel-class split of one batch (plain launches with the library's
+    # event profiler; the one-CTA-per-query kernel runs on a side stream and
+    # is not in it), after the timed region
+    ctx.profile(True)
+    ctx.profile_reset()
+    prof_reps = 3
+    for _ in range(prof_reps):
+        b.launch(stream)
+    torch.cuda.synchronize()
+    split = {k: round(v[0] / prof_reps, 4) for k, v in ctx.profile_read().items() if v[1]}
+    ctx.profile(False)
     b.close()
 
     # one library call per query (vdf_sort_groupby, group count read back), one at a time
@@ -287,7 +298,7 @@ def batched_section(args, local_rank: int) -> dict:
         "queries": len(specs), "rows": rows, "value": value, "unit": UNIT, "ms_per_batch": ms,
         "launch": "one CUDA graph per batch (captured once, replayed)", "gpu_launches_per_batch": launches,
         "hbm_frac_canonical": canonical / (ms / 1e3) / 1e9 / peak, "canonical_bytes": canonical,
-        "split": info, "tuning": tuned["best"], "tuning_ms": tuned["table"],
+        "split": info, "kernel_ms": split, "tuning": tuned["best"], "tuning_ms": tuned["table"],
         "per_call": {"value": per_call, "unit": UNIT, "queries": len(per_call_q), "seconds": pc_sec,
                      "call": "vdf_sort_groupby per query, group count read back (host sync) after each"},
         "speedup_vs_per_call": value / per_call,

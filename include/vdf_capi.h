@@ -120,7 +120,8 @@ typedef enum vdf_kernel_class {
     VDF_KC_PACK = 7,        /* row-record packing for gathers */
     VDF_KC_SEGSCAN = 8,     /* group-by: tile prefix scan     */
     VDF_KC_SEGEMIT = 9,     /* group-by: scan + emit groups   */
-    VDF_KC_TIES = 10        /* equal-neighbour check (multi-key) */
+    VDF_KC_TIES = 10,       /* equal-neighbour check (multi-key) */
+    VDF_KC_BATCH = 11       /* batch bookkeeping: row ids per query, group ranges, group keys */
 } vdf_kernel_class;
 /* When enabled, every kernel the context launches is bracketed by CUDA
  * events on its stream (no reference counterpart: the reference has no

@@ -24,7 +24,7 @@ I32, I64, U32, U64, F64, F32 = range(6)
 ORDER_ASC, ORDER_DESC_STABLE, ORDER_DESC_REVERSE = range(3)
 
 KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast", "pack",
-                  "segscan", "segemit", "ties"]
+                  "segscan", "segemit", "ties", "batch"]
 # vdf_multikey_mode
 MULTIKEY_LSD, MULTIKEY_PRIMARY_FIRST = 0, 1
 

@@ -54,14 +54,17 @@ __global__ void __launch_bounds__(256) k_batch_pack(BatchDev b) {
         if (threadIdx.x == 0) atomicOr(b.err, ERR_BAD_INDEX);
         return;
     }
-    // four rows per thread per round, all loads issued before the stores
+    // four rows per thread per round (rows k * blockDim + thread, so every
+    // load and store instruction is coalesced), all loads issued before the
+    // stores
     constexpr int R = 4;
-    for (uint32_t r0 = threadIdx.x * R; r0 < ch.rows; r0 += blockDim.x * R) {
+    const uint32_t step = blockDim.x * R;
+    for (uint32_t r0 = 0; r0 < ch.rows; r0 += step) {
         uint64_t kimg[R];
         unsigned long long slot[R][VDF_BATCH_MAX_VALS];
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            const uint32_t r = r0 + k;
+            const uint32_t r = r0 + k * blockDim.x + threadIdx.x;
             kimg[k] = 0;
 #pragma unroll
             for (int j = 0; j < VDF_BATCH_MAX_VALS; ++j) slot[k][j] = 0;
@@ -77,7 +80,7 @@ __global__ void __launch_bounds__(256) k_batch_pack(BatchDev b) {
         }
 #pragma unroll
         for (int k = 0; k < R; ++k) {
-            const uint32_t r = r0 + k;
+            const uint32_t r = r0 + k * blockDim.x + threadIdx.x;
             if (r >= ch.rows) continue;
             const uint64_t i = ch.row_start + r;  // arena row
             if (b.key_width == 8) static_cast<uint64_t*>(b.arena_keys)[i] = kimg[k];
@@ -355,7 +358,9 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
     }
 
     if (P.n_large) {
+        if (prof) prof->begin(KC_PACK, s);
         k_batch_pack<<<(uint32_t)P.chunks.size(), 256, 0, s>>>(b);
+        if (prof) prof->end(KC_PACK, s);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         ++n;
         SegSortArgs sa{};
@@ -428,6 +433,7 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
         if ((e = run_segreduce(r, tail, s, prof, &rl)) != cudaSuccess) return e;
         n += rl;
 
+        if (prof) prof->begin(KC_BATCH, s);
         k_batch_localize<<<grid_for(P.n_large, sms), 256, 0, s>>>(b);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         k_batch_seg_groups<<<(b.nsegs + 255) / 256, 256, 0, s>>>(b);
@@ -438,6 +444,7 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
             if ((e = cudaGetLastError()) != cudaSuccess) return e;
             ++n;
         }
+        if (prof) prof->end(KC_BATCH, s);
     }
     if (have_small && (e = cudaStreamWaitEvent(s, join, 0)) != cudaSuccess) return e;
     if (launches) *launches += n;

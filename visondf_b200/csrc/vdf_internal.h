@@ -14,7 +14,8 @@ constexpr int kMaxGather = 8;   // columns per gather launch
 // Kernel classes for the optional per-launch timing (vdf_ctx_profile).
 enum KernelClass : int {
     KC_HIST = 0, KC_SCAN = 1, KC_ONESWEEP32 = 2, KC_ONESWEEP64 = 3, KC_GATHER = 4, KC_SEGREDUCE = 5,
-    KC_BROADCAST = 6, KC_PACK = 7, KC_SEGSCAN = 8, KC_SEGEMIT = 9, KC_TIES = 10, KC_COUNT = 11
+    KC_BROADCAST = 6, KC_PACK = 7, KC_SEGSCAN = 8, KC_SEGEMIT = 9, KC_TIES = 10, KC_BATCH = 11,
+    KC_COUNT = 12
 };
 
 // Brackets kernel launches with CUDA events when profiling is enabled.
