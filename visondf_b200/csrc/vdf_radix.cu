@@ -333,9 +333,19 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     uint32_t peers[ITEMS];
     uint32_t* my_cnt = wcnt + warp * RADIX;
     const uint32_t lt = lanemask_lt();
+    // 8-bit digits are computed once and kept four to a register
+    constexpr bool PACKED = (BITS == 8);
+    uint32_t dpk[(ITEMS + 3) / 4];
+#pragma unroll
+    for (int i = 0; i < (ITEMS + 3) / 4; ++i) dpk[i] = 0;
+    auto digit = [&](int j) -> uint32_t {
+        if constexpr (PACKED) return (dpk[j / 4] >> (8 * (j % 4))) & 0xffu;
+        else return digit_of<K, BITS>(key[j], a.shift);
+    };
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const uint32_t d = digit_of<K, BITS>(key[j], a.shift);
+        if constexpr (PACKED) dpk[j / 4] |= d << (8 * (j % 4));
         if (MATCH == 1 || (MATCH == 2 && (j & 1) == 0)) {
             peers[j] = __match_any_sync(0xffffffffu, d);
         } else {
@@ -348,13 +358,15 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
             peers[j] = pm;
         }
     }
+    // The leader's add returns before the full-warp shuffle that hands its
+    // result out, and the next item's add comes after that shuffle, so the
+    // items' adds on a counter happen in item order (stable ranks).
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t d = digit_of<K, BITS>(key[j], a.shift);
+        const uint32_t d = digit(j);
         const int leader = __ffs(peers[j]) - 1;
         uint32_t base = 0;
         if (lane == leader) base = atomicAdd(&my_cnt[d], (uint32_t)__popc(peers[j]));
-        __syncwarp();  // the next item's leaders see this item's counts
         base = __shfl_sync(0xffffffffu, base, leader);
         rank[j] = base + __popc(peers[j] & lt);
     }
@@ -411,7 +423,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     // (overlaps the look-back below: other warps' global writes wait on it)
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t d = digit_of<K, BITS>(key[j], a.shift);
+        const uint32_t d = digit(j);
         uint32_t r = rank[j] + wcnt[warp * RADIX + d];
         if (r >= (uint32_t)TILE) {  // never when the counts are consistent
             atomicOr(a.err, ERR_BAD_INDEX);
