@@ -28,7 +28,10 @@ int32 payloads.  One vdf_sort_groupby call per step through the C-ABI.
              (vdf_server_*: HBM-budget admission, continuous batching): capacity
              and p50/p99 latency at 50/70/90 % of batched capacity, against one
              vdf_sort_groupby call per request on the same traces.
-  (both single-GPU, after the headline measurement; --sections selects them)
+  unique_join  vdf_unique over 100M int64 keys and vdf_left_join_index of 100M
+             left rows against 10M right keys, with the oracle's hash walks
+             on a 10M-row sample as the CPU baseline.
+  (all single-GPU, after the headline measurement; --sections selects them)
 
 --gpus N (launched by torchrun for N > 1) runs N independent replicas, one per
 GPU ("replicas only": the single-GPU path has no exchange step); value is all
@@ -305,6 +308,70 @@ def batched_section(args, local_rank: int) -> dict:
     }
 
 
+def unique_join_section(args, local_rank: int) -> dict:
+    """De-duplication (vdf_unique) of a 100M-row int64 column and left-join
+    row matching (vdf_left_join_index) of 100M left rows against 10M right
+    rows, device-resident, CUDA events around each call (count read back);
+    the oracle's hash walks on a 10M / 1M-row sample as the CPU baseline (the
+    reference's own de-duplication and join cannot run: the first calls a
+    filter the reference does not define, the second does not compile)."""
+    import numpy as np
+    import torch
+
+    import visondf_b200 as vdf
+
+    dev = torch.device("cuda", local_rank)
+    rng = np.random.default_rng(0xB200 + 16 * 5)
+    n, n_right = args.rows, args.rows // 10
+    ukey = torch.from_numpy(rng.integers(0, n // 2, size=n, dtype=np.int64)).to(dev)  # ~86 % distinct
+    right = rng.integers(-(1 << 61), 1 << 61, size=n_right, dtype=np.int64) * 2  # even keys
+    left = right[rng.integers(0, n_right, size=n)]
+    left[rng.random(n) < 0.25] += 1  # odd: absent from the right side
+    left_d, right_d = torch.from_numpy(left).to(dev), torch.from_numpy(right).to(dev)
+    ctx = vdf.Context(local_rank)
+    stream = torch.cuda.current_stream()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, out
+
+    u_ms, (_, distinct) = timed(lambda: ctx.unique(ukey))
+    j_ms, (_, matched) = timed(lambda: ctx.left_join_index(left_d, right_d))
+    ctx.close()
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_bind as ob
+        s_n = min(n, 10_000_000)
+        k_host = ukey[:s_n].cpu().numpy()
+        t0 = time.perf_counter()
+        ob.unique(k_host)
+        u_cpu = s_n / (time.perf_counter() - t0)
+        s_r = max(1, s_n // 10)
+        t0 = time.perf_counter()
+        ob.left_join(left[:s_n], right[:s_r])
+        j_cpu = s_n / (time.perf_counter() - t0)
+        cpu = {"unique_rows_per_s": u_cpu, "left_join_rows_per_s": j_cpu, "cores": 1, "kind": "port",
+               "sample": f"{s_n:,} rows (left join: {s_n:,} x {s_r:,}); host CPU: {cpu_info()}"}
+    del ukey, left_d, right_d
+    torch.cuda.empty_cache()
+    return {
+        "workload": f"unique: {n:,} int64 keys drawn from [0, {n // 2:,}); left join: {n:,} left rows x "
+                    f"{n_right:,} distinct right int64 keys (75 % of left rows present), first match",
+        "unique": {"ms": u_ms, "rows_per_s": n / (u_ms / 1e3), "distinct": distinct},
+        "left_join": {"ms": j_ms, "rows_per_s": n / (j_ms / 1e3), "matched": matched},
+        "cpu_baseline": cpu,
+    }
+
+
 def served_section(args, local_rank: int) -> dict:
     """Poisson request stream over resident columns: continuous batching with
     HBM-budget admission, against one library call per request."""
@@ -551,11 +618,13 @@ def our_arm(args, rank: int, world: int, local_rank: int):
     del d, outs, packed, keys, payload
     torch.cuda.empty_cache()
     sections = set(args.sections.split(","))
-    batched = served = None
+    batched = served = unique_join = None
     if world == 1 and "batched" in sections:
         batched = batched_section(args, local_rank)
     if world == 1 and "served" in sections:
         served = served_section(args, local_rank)
+    if world == 1 and "unique_join" in sections:
+        unique_join = unique_join_section(args, local_rank)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -576,6 +645,7 @@ def our_arm(args, rank: int, world: int, local_rank: int):
             "cpu_baseline": cpu,
             "batched": batched,
             "served": served,
+            "unique_join": unique_join,
         }
         print(json.dumps(line), flush=True)
 
@@ -593,9 +663,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default kernel variants")
     ap.add_argument("--variants", type=int, nargs=2, metavar=("V32", "V64"),
                     help="with --no-autotune: radix-pass variant indices for 4- and 8-byte keys")
-    ap.add_argument("--sections", default="batched,served",
-                    help="extra single-GPU measurements after the headline one: batched, served (comma list, "
-                         "'none' for neither)")
+    ap.add_argument("--sections", default="batched,served,unique_join",
+                    help="extra single-GPU measurements after the headline one: batched, served, unique_join "
+                         "(comma list, 'none' for none)")
     ap.add_argument("--batch-queries", type=int, default=4096)
     ap.add_argument("--no-batch-autotune", action="store_true", help="batched section: the default tuning")
     ap.add_argument("--batch-bytes", type=int, default=2 << 30, help="batched section: key + value bytes of the batch")

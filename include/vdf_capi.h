@@ -334,6 +334,34 @@ vdf_status vdf_transform_groupby_host(vdf_ctx* ctx, uint64_t n, const vdf_col* k
 vdf_status vdf_broadcast(vdf_ctx* ctx, uint64_t n, const uint32_t* row_group, const void* group_vals,
                          uint64_t n_groups, int width, const uint32_t* perm, void* out, void* stream);
 
+/* ---- de-duplication and left-join row matching ------------------------------
+ * Both run on the sorted path: a stable ascending radix sort of the key
+ * column puts each key value's rows in one run in row order, so the run's
+ * first (last) row is the value's first (last) occurrence.  Keys compare by
+ * their raw bits (-0.0 and +0.0 differ; a NaN equals a NaN with the same
+ * bits), as the reference's byte-wise hash lookups do.  The counts go to
+ * *..._dev (device, async) and/or *..._host (host; the call then
+ * synchronises `stream`); both are optional. */
+
+/* keep_out[i] (u8) = 1 if row i is the first occurrence of its key
+ * (keep_last = 0) or the last (keep_last = 1), else 0; the number of distinct
+ * keys is the count.  Replaces the set walk of transform_unique_mt
+ * (V/transform/transform_unique/transform_unique_mt.hpp:105-140), which marks
+ * the same rows with mask[i] = 0 before its filter step (:173). */
+vdf_status vdf_unique(vdf_ctx* ctx, uint64_t n, vdf_col key, int keep_last, uint8_t* keep_out,
+                      uint64_t* n_unique_dev, uint64_t* n_unique_host, void* stream);
+
+/* match_out[i] (u32) = the row of the right column holding left row i's key
+ * -- its first such row (take_last = 0, LeftJoinMethods::First) or last
+ * (take_last = 1, LeftJoinMethods::Last) -- or UINT32_MAX when the key is
+ * absent; the number of matched left rows is the count.  Both columns have
+ * the same dtype.  Replaces the map build and probe of transform_left_join_mt
+ * (V/transform/transform_left_join/transform_left_join_mt.hpp:172-205),
+ * whose match_idx holds SIZE_MAX for absent keys. */
+vdf_status vdf_left_join_index(vdf_ctx* ctx, uint64_t n_left, vdf_col left_key, uint64_t n_right,
+                               vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched_dev,
+                               uint64_t* n_matched_host, void* stream);
+
 /* ---- batched queries ------------------------------------------------------
  * Many independent sort + group-by queries (each: stable ascending sort of
  * one key column, then count/sum/min/max/mean of every value column per

@@ -37,6 +37,9 @@
  *     are exact 128-bit, float sums are kept in long double with Neumaier
  *     compensation (so they are exact to ~1e-19 of sum|x|), and groups are
  *     returned in ascending key order (the hash order is kept separately).
+ *   - de-duplication and left-join row matching: the reference's set / map
+ *     walks over raw key bytes (orc_unique, orc_left_join, at the end of
+ *     this file, with their citations).
  */
 #include <stdint.h>
 #include <stdlib.h>
@@ -412,4 +415,107 @@ void orc_broadcast(const int64_t* row_group, size_t n, const void* group_vals, i
     for (size_t r = 0; r < n; ++r)
         memcpy((unsigned char*)out + r * (size_t)width,
                (const unsigned char*)group_vals + (size_t)row_group[r] * (size_t)width, (size_t)width);
+}
+
+/*
+ * Set and map over raw key bytes, the lookup structure of the reference's
+ * de-duplication and join (an ankerl set/map keyed by a string_view over the
+ * element's bytes).  Open addressing with linear probing; key = the raw bits
+ * zero-extended to 64, so two keys are equal exactly when their bytes are.
+ */
+typedef struct {
+    uint64_t* key;
+    int64_t* val;   /* -1: empty slot */
+    size_t mask;
+} orc_map;
+
+static int orc_map_init(orc_map* m, size_t n) {
+    size_t cap = 16;
+    while (cap < 2 * n + 16) cap <<= 1;
+    m->key = (uint64_t*)malloc(cap * sizeof(uint64_t));
+    m->val = (int64_t*)malloc(cap * sizeof(int64_t));
+    m->mask = cap - 1;
+    if (!m->key || !m->val) { free(m->key); free(m->val); return -1; }
+    for (size_t i = 0; i < cap; ++i) m->val[i] = -1;
+    return 0;
+}
+static void orc_map_free(orc_map* m) { free(m->key); free(m->val); }
+static uint64_t orc_raw_bits(const void* col, int width, size_t i) {
+    return width == 8 ? ((const uint64_t*)col)[i] : (uint64_t)((const uint32_t*)col)[i];
+}
+/* slot of key k: the slot holding it, or the empty slot where it would go */
+static size_t orc_map_slot(const orc_map* m, uint64_t k) {
+    size_t s = (size_t)orc_mix(k) & m->mask;
+    while (m->val[s] >= 0 && m->key[s] != k) s = (s + 1) & m->mask;
+    return s;
+}
+
+/*
+ * De-duplication (transform_unique_mt, V/transform/transform_unique/
+ * transform_unique_mt.hpp:105-140): rows are visited in order (Last = false)
+ * or in reverse (Last = true); a row whose key is not yet in the set is the
+ * kept occurrence of that key and its key is inserted.  The reference records
+ * the kept rows as mask[i] = 0 and then calls transform_filter_mt (:173),
+ * which the reference does not define; here keep[i] = 1 marks exactly those
+ * rows.
+ * Returns the number of distinct keys, or -1 on allocation failure.
+ */
+int64_t orc_unique(const void* col, int dt, size_t n, int last, uint8_t* keep) {
+    const int w = orc_dtype_width(dt);
+    orc_map m;
+    if (orc_map_init(&m, n)) return -1;
+    int64_t distinct = 0;
+    for (size_t t = 0; t < n; ++t) {
+        const size_t i = last ? n - 1 - t : t;
+        const uint64_t k = orc_raw_bits(col, w, i);
+        const size_t s = orc_map_slot(&m, k);
+        if (m.val[s] < 0) {
+            m.key[s] = k;
+            m.val[s] = (int64_t)i;
+            keep[i] = 1;
+            ++distinct;
+        } else {
+            keep[i] = 0;
+        }
+    }
+    orc_map_free(&m);
+    return distinct;
+}
+
+/*
+ * Left-join row matching, methods First and Last (transform_left_join_mt,
+ * V/transform/transform_left_join/transform_left_join_mt.hpp:172-205): the
+ * right key column is loaded into a map key -> row, keeping the first row of
+ * each key (try_emplace, First) or the last (assignment, Last); each left row
+ * then looks its key up (:201-205): match[i] = the right row, or UINT32_MAX where the
+ * key is absent (the reference's SIZE_MAX).  Keys compare by their raw bytes.
+ * Returns the number of matched left rows, or -1 on allocation failure.
+ */
+int64_t orc_left_join(const void* left, size_t n_left, const void* right, size_t n_right, int dt, int last,
+                      uint32_t* match) {
+    const int w = orc_dtype_width(dt);
+    orc_map m;
+    if (orc_map_init(&m, n_right)) return -1;
+    for (size_t j = 0; j < n_right; ++j) {
+        const uint64_t k = orc_raw_bits(right, w, j);
+        const size_t s = orc_map_slot(&m, k);
+        if (m.val[s] < 0) {
+            m.key[s] = k;
+            m.val[s] = (int64_t)j;
+        } else if (last) {
+            m.val[s] = (int64_t)j;
+        }
+    }
+    int64_t matched = 0;
+    for (size_t i = 0; i < n_left; ++i) {
+        const size_t s = orc_map_slot(&m, orc_raw_bits(left, w, i));
+        if (m.val[s] >= 0) {
+            match[i] = (uint32_t)m.val[s];
+            ++matched;
+        } else {
+            match[i] = 0xffffffffu;
+        }
+    }
+    orc_map_free(&m);
+    return matched;
 }

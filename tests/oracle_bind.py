@@ -39,6 +39,10 @@ def _load_oracle() -> C.CDLL:
     lib.orc_radix_u64.argtypes = [C.c_void_p, C.c_void_p, C.c_size_t]
     lib.orc_order_key.restype = C.c_uint64
     lib.orc_order_key.argtypes = [C.c_void_p, C.c_int, C.c_size_t]
+    lib.orc_unique.restype = C.c_int64
+    lib.orc_unique.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_int, C.c_void_p]
+    lib.orc_left_join.restype = C.c_int64
+    lib.orc_left_join.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p]
     return lib
 
 
@@ -152,3 +156,24 @@ def groupby(keys, vals, sorted_groups=True) -> OracleGroups:
     return OracleGroups(g, [a[:g] for a in ok], cnt[:g], [a[:g] for a in sums], [a[:g] for a in his],
                         [a[:g] for a in mins], [a[:g] for a in maxs], [a[:g] for a in means],
                         [a[:g] for a in abss], first[:g])
+
+
+def unique(key, keep_last=False):
+    """Oracle de-duplication: (keep mask uint8, number of distinct keys)."""
+    key = np.ascontiguousarray(key)
+    keep = np.zeros(key.size, np.uint8)
+    d = oracle().orc_unique(_vp(key), DT[key.dtype], key.size, 1 if keep_last else 0, _vp(keep))
+    assert d >= 0
+    return keep, int(d)
+
+
+def left_join(left, right, take_last=False):
+    """Oracle left-join matching: (match uint32, UINT32_MAX where absent; matched rows)."""
+    left = np.ascontiguousarray(left)
+    right = np.ascontiguousarray(right)
+    assert left.dtype == right.dtype
+    match = np.empty(left.size, np.uint32)
+    m = oracle().orc_left_join(_vp(left), left.size, _vp(right), right.size, DT[left.dtype],
+                               1 if take_last else 0, _vp(match))
+    assert m >= 0
+    return match, int(m)

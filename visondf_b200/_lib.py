@@ -122,6 +122,8 @@ def _load() -> C.CDLL:
         "vdf_sort_groupby": (st, [vp, C.POINTER(vdf_sort_groupby_args), vp]),
         "vdf_sort_groupby_host": (st, [vp, C.POINTER(vdf_sort_groupby_args), vp]),
         "vdf_broadcast": (st, [vp, u64, vp, vp, u64, i32, vp, vp, vp]),
+        "vdf_unique": (st, [vp, u64, vdf_col, i32, vp, vp, C.POINTER(C.c_uint64), vp]),
+        "vdf_left_join_index": (st, [vp, u64, vdf_col, u64, vdf_col, i32, vp, vp, C.POINTER(C.c_uint64), vp]),
         "vdf_gather_host": (st, [vp, u64, vp, C.POINTER(vdf_col), i32, C.POINTER(vp), vp]),
         "vdf_transform_groupby_host": (st, [vp, u64, C.POINTER(vdf_col), i32, vdf_col, C.c_int32, vp, vp,
                                             C.POINTER(C.c_uint64), vp]),
@@ -417,6 +419,29 @@ class Context:
                                       group_vals.element_size(), _ptr(perm), _ptr(out), _stream(stream)),
                     "vdf_broadcast")
         return out
+
+
+    def unique(self, key: torch.Tensor, keep_last: bool = False, stream=None):
+        """(keep, n_unique): keep[i] = 1 (uint8) where row i is the first
+        (or, with keep_last, the last) occurrence of its key."""
+        n = key.numel()
+        keep = torch.empty(n, dtype=torch.uint8, device=key.device)
+        cnt = C.c_uint64(0)
+        self._check(lib.vdf_unique(self.handle, n, _col(key), 1 if keep_last else 0, _ptr(keep), None,
+                                   C.byref(cnt), _stream(stream)), "vdf_unique")
+        return keep, int(cnt.value)
+
+    def left_join_index(self, left: torch.Tensor, right: torch.Tensor, take_last: bool = False, stream=None):
+        """(match, n_matched): match[i] = the first (or, with take_last, the
+        last) row of `right` holding left[i]'s key, or UINT32_MAX (int32 view:
+        -1) where none does."""
+        n = left.numel()
+        match = torch.empty(n, dtype=torch.int32, device=left.device)
+        cnt = C.c_uint64(0)
+        self._check(lib.vdf_left_join_index(self.handle, n, _col(left), right.numel(), _col(right),
+                                            1 if take_last else 0, _ptr(match), None, C.byref(cnt),
+                                            _stream(stream)), "vdf_left_join_index")
+        return match, int(cnt.value)
 
 
 def sort_variants() -> list:

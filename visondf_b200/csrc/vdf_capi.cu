@@ -908,4 +908,113 @@ vdf_status vdf_broadcast(vdf_ctx* c, uint64_t n, const uint32_t* row_group, cons
                      "broadcast");
 }
 
+// Reads a device count (u64) into *host after the stream's work.
+static vdf_status read_count(vdf_ctx* c, const uint64_t* dev, uint64_t* host, cudaStream_t s, const char* what) {
+    if (!host) return VDF_OK;
+    cudaError_t e = cudaMemcpyAsync(&c->host_pinned[0], dev, sizeof(uint64_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, what);
+    *host = c->host_pinned[0];
+    return drain_and_check(c, s);
+}
+
+vdf_status vdf_unique(vdf_ctx* c, uint64_t n, vdf_col key, int keep_last, uint8_t* keep_out,
+                      uint64_t* n_unique_dev, uint64_t* n_unique_host, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if ((st = check_keys(c, n, &key, 1)) != VDF_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DeviceGuard g(c->device);
+    if (n == 0) {
+        if (n_unique_dev && cudaMemsetAsync(n_unique_dev, 0, sizeof(uint64_t), s) != cudaSuccess)
+            return from_cuda(c, cudaGetLastError(), "clear count");
+        if (n_unique_host) *n_unique_host = 0;
+        return VDF_OK;
+    }
+    if (!keep_out) return fail(c, VDF_ERR_INVALID_ARG, "keep_out is NULL");
+    const int w = vdf::dtype_width(key.dtype);
+    // workspace: permutation | sorted keys | count | the sort's own
+    const size_t o_perm = 0, o_keys = align256(4 * n), o_cnt = o_keys + align256((size_t)w * n);
+    const size_t o_sort = o_cnt + 256;
+    const vdf::SortPlan plan = vdf::make_sort_plan(n, &key.dtype, 1, c->tuning);
+    if ((st = ws_ensure(c, o_sort + sort_ws_need(plan, n, 1, nullptr))) != VDF_OK) return st;
+    uint32_t* perm = reinterpret_cast<uint32_t*>(c->ws + o_perm);
+    void* skeys = c->ws + o_keys;
+    uint64_t* cnt = n_unique_dev ? n_unique_dev : reinterpret_cast<uint64_t*>(c->ws + o_cnt);
+    void* const souts[1] = {skeys};
+    if ((st = sort_impl(c, n, &key, 1, VDF_ORDER_ASC, perm, souts, c->ws + o_sort, c->ws_cap - o_sort, s)) != VDF_OK)
+        return st;
+    cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(uint64_t), s);
+    if (e == cudaSuccess)
+        e = vdf::run_unique_mark(skeys, w, perm, n, keep_last ? 1 : 0, keep_out,
+                                 reinterpret_cast<unsigned long long*>(cnt), err_word(c), s);
+    c->launches++;
+    if (e != cudaSuccess) return from_cuda(c, e, "unique");
+    return read_count(c, cnt, n_unique_host, s, "read unique count");
+}
+
+vdf_status vdf_left_join_index(vdf_ctx* c, uint64_t n_left, vdf_col left_key, uint64_t n_right,
+                               vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched_dev,
+                               uint64_t* n_matched_host, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n_left)) != VDF_OK) return st;
+    if ((st = check_rows(c, n_right)) != VDF_OK) return st;
+    if ((st = check_keys(c, n_left, &left_key, 1)) != VDF_OK) return st;
+    if ((st = check_keys(c, n_right, &right_key, 1)) != VDF_OK) return st;
+    if (left_key.dtype != right_key.dtype) return fail(c, VDF_ERR_INVALID_ARG, "left and right keys differ in dtype");
+    if (n_left && !match_out) return fail(c, VDF_ERR_INVALID_ARG, "match_out is NULL");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DeviceGuard g(c->device);
+    const int w = vdf::dtype_width(right_key.dtype);
+    const uint64_t nr = n_right;
+    // workspace: right permutation | right sorted keys | distinct keys | run
+    // starts | group count | matched count | the sort's or the reduction's own
+    const size_t o_perm = 0, o_sk = align256(4 * nr), o_uk = o_sk + align256((size_t)w * nr);
+    const size_t o_gs = o_uk + align256((size_t)w * nr), o_ng = o_gs + align256(4 * nr), o_cnt = o_ng + 256;
+    const size_t o_tail = o_cnt + 256;
+    size_t tail = 0;
+    if (nr) {
+        const vdf::SortPlan plan = vdf::make_sort_plan(nr, &right_key.dtype, 1, c->tuning);
+        tail = std::max(sort_ws_need(plan, nr, 1, nullptr), vdf::segreduce_workspace_bytes(nr, 0));
+    }
+    if ((st = ws_ensure(c, o_tail + tail)) != VDF_OK) return st;
+    uint64_t* cnt = n_matched_dev ? n_matched_dev : reinterpret_cast<uint64_t*>(c->ws + o_cnt);
+    cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(uint64_t), s);
+    if (e != cudaSuccess) return from_cuda(c, e, "clear count");
+    if (n_left == 0) return read_count(c, cnt, n_matched_host, s, "read match count");
+    if (nr == 0) {  // nothing to match
+        if ((e = cudaMemsetAsync(match_out, 0xff, 4 * n_left, s)) != cudaSuccess) return from_cuda(c, e, "no match");
+        return read_count(c, cnt, n_matched_host, s, "read match count");
+    }
+    uint32_t* perm = reinterpret_cast<uint32_t*>(c->ws + o_perm);
+    void* sk = c->ws + o_sk;
+    void* const souts[1] = {sk};
+    if ((st = sort_impl(c, nr, &right_key, 1, VDF_ORDER_ASC, perm, souts, c->ws + o_tail, c->ws_cap - o_tail, s)) !=
+        VDF_OK)
+        return st;
+    // distinct right keys and the sorted row where each one's run starts
+    vdf::SegArgs a{};
+    a.n = nr;
+    a.nkeys = 1;
+    a.nvals = 0;
+    a.key[0] = vdf::SegCol{sk, right_key.dtype};
+    a.key_out[0] = c->ws + o_uk;
+    a.group_start = reinterpret_cast<uint32_t*>(c->ws + o_gs);
+    a.n_groups = reinterpret_cast<uint64_t*>(c->ws + o_ng);
+    a.err = err_word(c);
+    int launched = 0;
+    if ((e = vdf::run_segreduce(a, c->ws + o_tail, s, prof_of(c), &launched)) != cudaSuccess)
+        return from_cuda(c, e, "distinct right keys");
+    c->launches += launched;
+    e = vdf::run_join_probe(left_key.data, n_left, left_key.dtype, c->ws + o_uk, a.group_start, a.n_groups, perm, nr,
+                            take_last ? 1 : 0, match_out, reinterpret_cast<unsigned long long*>(cnt), err_word(c), s);
+    c->launches++;
+    if (e != cudaSuccess) return from_cuda(c, e, "join probe");
+    return read_count(c, cnt, n_matched_host, s, "read match count");
+}
+
 }  // extern "C"
