@@ -362,6 +362,16 @@ vdf_status vdf_left_join_index(vdf_ctx* ctx, uint64_t n_left, vdf_col left_key, 
                                vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched_dev,
                                uint64_t* n_matched_host, void* stream);
 
+/* The same two operations on HOST columns and outputs (copied through the
+ * context's staging buffer; synchronise `stream`): the entry points of the
+ * C++ dataframe layer (transform_unique / transform_left_join in
+ * include/vison_b200/vison.hpp). */
+vdf_status vdf_unique_host(vdf_ctx* ctx, uint64_t n, vdf_col key, int keep_last, uint8_t* keep_out,
+                           uint64_t* n_unique, void* stream);
+vdf_status vdf_left_join_index_host(vdf_ctx* ctx, uint64_t n_left, vdf_col left_key, uint64_t n_right,
+                                    vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched,
+                                    void* stream);
+
 /* ---- batched queries ------------------------------------------------------
  * Many independent sort + group-by queries (each: stable ascending sort of
  * one key column, then count/sum/min/max/mean of every value column per

@@ -10,6 +10,9 @@
 //   materialize / materialize_mt  materialize/materialize_mt.hpp:3-55
 //   transform_group_by[_mt]       transform/transform_group_by/transform_group_by.hpp:3-113,
 //                                 transform_group_by_mt.hpp:3-114
+//   transform_unique[_mt]         transform/transform_unique/transform_unique_mt.hpp:3-11
+//   transform_left_join[_mt]      transform/transform_left_join/transform_left_join_mt.hpp:3-15
+//                                 (methods First and Last)
 //
 // Storage follows the reference: column-major type blocks (here int_v, uint_v,
 // dbl_v plus 64-bit integer blocks lint_v / luint_v, which the reference lacks:
@@ -54,6 +57,9 @@ enum class SortType { Standard, Radix };  // supported_sorting_methods.inl:1-4 (
 
 // supported_group_methods.inl:1-7, plus Min and Max
 enum class GroupFunction { Occurence, Sum, Mean, Gather, None, Min, Max };
+
+// types/supported_leftjoin_methods.inl:1-5 (Aligned: not on the GPU path)
+enum class LeftJoinMethods { First, Last, Aligned };
 
 struct DefaultTypes {  // types/inference_type.hpp:3-8 (CharT omitted: no char columns here)
     using IntT = int;
@@ -313,7 +319,131 @@ class Dataframe {
         }
     }
 
+    // ---- de-duplication ------------------------------------------------------------
+    // transform_unique_mt.hpp:3-11: keeps, in row order, the first (Last =
+    // false) or last occurrence of each value of column n, values compared by
+    // their bytes.  A frame in view is materialised first (Soft = true; with
+    // Soft = false a view is an error, as in the reference).
+    template <typename T = void, unsigned int CORES = 4, bool MemClean = false, bool Last = false,
+              bool MapCol = false, bool Soft = true, bool SimdHash = true>
+    void transform_unique_mt(unsigned int n) {
+        if (in_view && !Soft) {
+            std::cerr << "Can't perform this operation while in `view` mode, consider applying `.materialize()`\n";
+            return;
+        }
+        if (n >= ncol) {
+            std::cerr << "Column not found\n";
+            return;
+        }
+        if (in_view) materialize();
+        std::vector<uint8_t> keep(nrow);
+        uint64_t distinct = 0;
+        if (!detail::report(vdf_unique_host(context(), nrow, col_desc(n), Last ? 1 : 0, keep.data(), &distinct, nullptr),
+                            "transform_unique"))
+            return;
+        std::vector<uint32_t> rows;
+        rows.reserve(distinct);
+        for (unsigned int r = 0; r < nrow; ++r)
+            if (keep[r]) rows.push_back(r);
+        keep_rows(rows);
+    }
+    template <typename T = void, bool MemClean = false, bool Last = false, bool MapCol = false, bool Soft = true,
+              bool SimdHash = true>
+    void transform_unique(unsigned int n) {
+        transform_unique_mt<T, 1, MemClean, Last, MapCol, Soft, SimdHash>(n);
+    }
+
+    // ---- left join ---------------------------------------------------------------------
+    // transform_left_join_mt.hpp:3-15: appends obj's columns; row i takes the
+    // values of obj's first (First) or last (Last) row whose key2 equals this
+    // frame's key1 at row i, or the per-type default where none does.
+    template <typename T = void, unsigned int CORES = 4, bool SimdHash = true,
+              LeftJoinMethods Method = LeftJoinMethods::First>
+    void transform_left_join_mt(const Dataframe& obj, const unsigned int key1, const unsigned int key2,
+                                const char default_chr, const std::string default_str = "NA",
+                                const uint8_t default_bool = 0, const IntT default_int = 0,
+                                const UIntT default_uint = 0, const FloatT default_dbl = 0) {
+        (void)default_chr;
+        (void)default_str;
+        (void)default_bool;
+        if (in_view) {
+            std::cerr << "Can't perform this operation while in`view` mode, consider applying `.materialize()`\n";
+            return;
+        }
+        if constexpr (Method == LeftJoinMethods::Aligned) {
+            std::cerr << "transform_left_join: LeftJoinMethods::Aligned is not supported on the GPU path\n";
+            return;
+        } else {
+            if (key1 >= ncol || key2 >= obj.ncol) {
+                std::cerr << "Column not found\n";
+                return;
+            }
+            if (type_refv[key1] != obj.type_refv[key2]) {
+                std::cerr << "transform_left_join: key columns differ in type\n";
+                return;
+            }
+            Dataframe right = obj;  // obj as viewed
+            if (right.in_view) right.materialize();
+            std::vector<uint32_t> match(nrow);
+            uint64_t matched = 0;
+            if (!detail::report(vdf_left_join_index_host(context(), nrow, col_desc(key1), right.nrow,
+                                                         right.col_desc(key2),
+                                                         Method == LeftJoinMethods::Last ? 1 : 0, match.data(),
+                                                         &matched, nullptr),
+                                "transform_left_join"))
+                return;
+            for (unsigned int c = 0; c < right.ncol; ++c) {
+                const unsigned s = right.slot_v[c];
+                const std::string name = right.name_v[c];
+                auto join = [&](const auto& src, auto dflt) {
+                    using V = typename std::decay_t<decltype(src)>::value_type;
+                    std::vector<V> out(nrow);
+                    for (unsigned int r = 0; r < nrow; ++r) out[r] = match[r] == 0xffffffffu ? (V)dflt : src[match[r]];
+                    add_col(std::move(out), name);
+                };
+                switch (right.type_refv[c]) {
+                case 'i': join(right.int_v[s], default_int); break;
+                case 'u': join(right.uint_v[s], default_uint); break;
+                case 'd': join(right.dbl_v[s], default_dbl); break;
+                case 'l': join(right.lint_v[s], (LIntT)default_int); break;
+                default: join(right.luint_v[s], (LUIntT)default_uint); break;
+                }
+            }
+        }
+    }
+    template <typename T = void, bool SimdHash = true, LeftJoinMethods Method = LeftJoinMethods::First>
+    void transform_left_join(const Dataframe& obj, const unsigned int key1, const unsigned int key2,
+                             const char default_chr, const std::string default_str = "NA",
+                             const uint8_t default_bool = 0, const IntT default_int = 0, const UIntT default_uint = 0,
+                             const FloatT default_dbl = 0) {
+        transform_left_join_mt<T, 1, SimdHash, Method>(obj, key1, key2, default_chr, default_str, default_bool,
+                                                       default_int, default_uint, default_dbl);
+    }
+
   private:
+    // Keeps storage rows `rows` (ascending) of every column.
+    void keep_rows(const std::vector<uint32_t>& rows) {
+        for (unsigned int c = 0; c < ncol; ++c) {
+            const unsigned s = slot_v[c];
+            auto go = [&](auto& vec) {
+                using V = typename std::decay_t<decltype(vec)>::value_type;
+                std::vector<V> out(rows.size());
+                for (size_t i = 0; i < rows.size(); ++i) out[i] = vec[rows[i]];
+                vec.swap(out);
+            };
+            switch (type_refv[c]) {
+            case 'i': go(int_v[s]); break;
+            case 'u': go(uint_v[s]); break;
+            case 'd': go(dbl_v[s]); break;
+            case 'l': go(lint_v[s]); break;
+            default: go(luint_v[s]); break;
+            }
+        }
+        nrow = (unsigned int)rows.size();
+        row_view_idx.clear();
+        in_view = false;
+    }
+
     template <typename T>
     const std::vector<T>* col_ptr(unsigned int n) const {
         if (n >= ncol) return nullptr;

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <map>
+#include <set>
 #include <numeric>
 #include <random>
 #include <tuple>
@@ -13,6 +14,7 @@
 #include "vison_b200/vison.hpp"
 
 using DF = vison_b200::Dataframe<>;
+using vison_b200::LeftJoinMethods;
 using vison_b200::GroupFunction;
 
 static int failures = 0;
@@ -148,11 +150,85 @@ static void test_transform_group_by() {
     CHECK(ok);
 }
 
+// transform_unique: the rows kept are those a set walk keeps (first or last
+// occurrence per key value, in row order), for every column of the frame.
+static void test_transform_unique() {
+    std::mt19937_64 rng(23);
+    const unsigned N = 50000;
+    std::vector<int64_t> k(N);
+    std::vector<double> v(N);
+    for (unsigned i = 0; i < N; ++i) {
+        k[i] = (int64_t)(rng() % 7000) - 3500;
+        v[i] = (double)i;
+    }
+    for (int last = 0; last < 2; ++last) {
+        std::vector<unsigned> rows;
+        std::set<int64_t> seen;
+        if (!last) {
+            for (unsigned i = 0; i < N; ++i)
+                if (seen.insert(k[i]).second) rows.push_back(i);
+        } else {
+            for (unsigned i = N; i-- > 0;)
+                if (seen.insert(k[i]).second) rows.push_back(i);
+            std::sort(rows.begin(), rows.end());
+        }
+        DF df;
+        df.add_col(std::vector<int64_t>(k), "k");
+        df.add_col(std::vector<double>(v), "v");
+        if (last) df.transform_unique<void, false, true>(0);
+        else df.transform_unique(0);
+        CHECK(df.nrow == rows.size());
+        bool ok = df.nrow == rows.size();
+        for (unsigned i = 0; ok && i < rows.size(); ++i)
+            ok &= df.lint_v[0][i] == k[rows[i]] && df.dbl_v[0][i] == v[rows[i]];
+        CHECK(ok);
+    }
+}
+
+// transform_left_join: each left row takes the first (or last) right row with
+// its key, or the defaults; the right frame's columns are appended.
+static void test_transform_left_join() {
+    std::mt19937_64 rng(29);
+    const unsigned NL = 30000, NR = 8000;
+    std::vector<int> lk(NL), rk(NR), rv(NR);
+    std::vector<double> rd(NR);
+    for (unsigned i = 0; i < NL; ++i) lk[i] = (int)(rng() % 6000);
+    for (unsigned j = 0; j < NR; ++j) {
+        rk[j] = (int)(rng() % 4000) * 2;  // even: odd left keys never match
+        rv[j] = (int)j;
+        rd[j] = 0.5 * j;
+    }
+    for (int last = 0; last < 2; ++last) {
+        std::map<int, unsigned> m;
+        for (unsigned j = 0; j < NR; ++j)
+            if (last || !m.count(rk[j])) m[rk[j]] = j;
+        DF left, right;
+        left.add_col(std::vector<int>(lk), "lk");
+        right.add_col(std::vector<int>(rk), "rk");
+        right.add_col(std::vector<int>(rv), "rv");
+        right.add_col(std::vector<double>(rd), "rd");
+        if (last) left.transform_left_join<void, true, LeftJoinMethods::Last>(right, 0, 0, ' ', "NA", 0, -7, 0, -1.5);
+        else left.transform_left_join<void, true, LeftJoinMethods::First>(right, 0, 0, ' ', "NA", 0, -7, 0, -1.5);
+        CHECK(left.ncol == 4);
+        bool ok = left.ncol == 4;
+        for (unsigned i = 0; ok && i < NL; ++i) {
+            auto it = m.find(lk[i]);
+            const int ek = it == m.end() ? -7 : rk[it->second];
+            const int ev = it == m.end() ? -7 : rv[it->second];
+            const double ed = it == m.end() ? -1.5 : rd[it->second];
+            ok &= left.int_v[1][i] == ek && left.int_v[2][i] == ev && left.dbl_v[0][i] == ed;
+        }
+        CHECK(ok);
+    }
+}
+
 int main() {
     test_doc_example();
     test_hard_sort_and_view_composition();
     test_sort_by_external();
     test_transform_group_by();
+    test_transform_unique();
+    test_transform_left_join();
     if (failures) {
         std::fprintf(stderr, "%d checks failed\n", failures);
         return 1;

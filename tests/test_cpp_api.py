@@ -22,7 +22,9 @@ def test_header_compiles_as_vison_dropin(tmp_path):
     src.write_text('#define VISON_B200_AS_VISON\n#include "vison_b200/vison.hpp"\n'
                    "int main(){ vison::Dataframe<> df; unsigned n = 0; df.add_col(std::vector<int>{3,1,2});\n"
                    " df.sort_by_mt<1, 8, void, true, true, vison::SortType::Radix>(n); df.materialize_mt<8>();\n"
-                   " df.transform_group_by_mt<void, void, 4, vison::GroupFunction::Sum>({0}, 0, \"s\"); return 0; }\n")
+                   " df.transform_group_by_mt<void, void, 4, vison::GroupFunction::Sum>({0}, 0, \"s\");\n"
+                   " vison::Dataframe<> r = df; df.transform_unique_mt<void, 8>(0);\n"
+                   " df.transform_left_join_mt<void, 8, true, vison::LeftJoinMethods::Last>(r, 0, 0, ' '); return 0; }\n")
     r = subprocess.run(["g++", "-std=c++20", "-fsyntax-only", "-I", str(ROOT / "include"), str(src)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

@@ -918,10 +918,9 @@ static vdf_status read_count(vdf_ctx* c, const uint64_t* dev, uint64_t* host, cu
     return drain_and_check(c, s);
 }
 
-vdf_status vdf_unique(vdf_ctx* c, uint64_t n, vdf_col key, int keep_last, uint8_t* keep_out,
-                      uint64_t* n_unique_dev, uint64_t* n_unique_host, void* stream) {
-    if (!c) return VDF_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lk(c->mu);
+// vdf_unique with the context lock held
+static vdf_status unique_locked(vdf_ctx* c, uint64_t n, vdf_col key, int keep_last, uint8_t* keep_out,
+                                uint64_t* n_unique_dev, uint64_t* n_unique_host, void* stream) {
     vdf_status st;
     if ((st = check_rows(c, n)) != VDF_OK) return st;
     if ((st = check_keys(c, n, &key, 1)) != VDF_OK) return st;
@@ -955,11 +954,10 @@ vdf_status vdf_unique(vdf_ctx* c, uint64_t n, vdf_col key, int keep_last, uint8_
     return read_count(c, cnt, n_unique_host, s, "read unique count");
 }
 
-vdf_status vdf_left_join_index(vdf_ctx* c, uint64_t n_left, vdf_col left_key, uint64_t n_right,
-                               vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched_dev,
-                               uint64_t* n_matched_host, void* stream) {
-    if (!c) return VDF_ERR_INVALID_ARG;
-    std::lock_guard<std::mutex> lk(c->mu);
+// vdf_left_join_index with the context lock held
+static vdf_status left_join_locked(vdf_ctx* c, uint64_t n_left, vdf_col left_key, uint64_t n_right,
+                                   vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched_dev,
+                                   uint64_t* n_matched_host, void* stream) {
     vdf_status st;
     if ((st = check_rows(c, n_left)) != VDF_OK) return st;
     if ((st = check_rows(c, n_right)) != VDF_OK) return st;
@@ -1015,6 +1013,87 @@ vdf_status vdf_left_join_index(vdf_ctx* c, uint64_t n_left, vdf_col left_key, ui
     c->launches++;
     if (e != cudaSuccess) return from_cuda(c, e, "join probe");
     return read_count(c, cnt, n_matched_host, s, "read match count");
+}
+
+vdf_status vdf_unique(vdf_ctx* c, uint64_t n, vdf_col key, int keep_last, uint8_t* keep_out,
+                      uint64_t* n_unique_dev, uint64_t* n_unique_host, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    return unique_locked(c, n, key, keep_last, keep_out, n_unique_dev, n_unique_host, stream);
+}
+
+vdf_status vdf_left_join_index(vdf_ctx* c, uint64_t n_left, vdf_col left_key, uint64_t n_right,
+                               vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched_dev,
+                               uint64_t* n_matched_host, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    return left_join_locked(c, n_left, left_key, n_right, right_key, take_last, match_out, n_matched_dev,
+                            n_matched_host, stream);
+}
+
+vdf_status vdf_unique_host(vdf_ctx* c, uint64_t n, vdf_col key, int keep_last, uint8_t* keep_out,
+                           uint64_t* n_unique, void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n)) != VDF_OK) return st;
+    if (!valid_dtype(key.dtype)) return fail(c, VDF_ERR_INVALID_ARG, "bad key dtype");
+    if (n && (!key.data || !keep_out)) return fail(c, VDF_ERR_INVALID_ARG, "NULL key or keep_out");
+    if (n == 0) {
+        if (n_unique) *n_unique = 0;
+        return VDF_OK;
+    }
+    DeviceGuard g(c->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t w = (size_t)vdf::dtype_width(key.dtype);
+    const size_t o_key = 0, o_keep = align256(w * n);
+    if ((st = io_ensure(c, o_keep + align256(n))) != VDF_OK) return st;
+    cudaError_t e = cudaMemcpyAsync(c->io + o_key, key.data, w * n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return from_cuda(c, e, "copy key to the device");
+    uint64_t cnt = 0;
+    if ((st = unique_locked(c, n, vdf_col{c->io + o_key, key.dtype}, keep_last, c->io + o_keep, nullptr, &cnt,
+                            stream)) != VDF_OK)
+        return st;
+    e = cudaMemcpyAsync(keep_out, c->io + o_keep, n, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, "copy mask to the host");
+    if (n_unique) *n_unique = cnt;
+    return VDF_OK;
+}
+
+vdf_status vdf_left_join_index_host(vdf_ctx* c, uint64_t n_left, vdf_col left_key, uint64_t n_right,
+                                    vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched,
+                                    void* stream) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    vdf_status st;
+    if ((st = check_rows(c, n_left)) != VDF_OK) return st;
+    if ((st = check_rows(c, n_right)) != VDF_OK) return st;
+    if (!valid_dtype(left_key.dtype) || left_key.dtype != right_key.dtype)
+        return fail(c, VDF_ERR_INVALID_ARG, "bad or differing key dtypes");
+    if ((n_left && (!left_key.data || !match_out)) || (n_right && !right_key.data))
+        return fail(c, VDF_ERR_INVALID_ARG, "NULL key or match_out");
+    DeviceGuard g(c->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    const size_t w = (size_t)vdf::dtype_width(left_key.dtype);
+    const size_t o_l = 0, o_r = align256(w * n_left), o_m = o_r + align256(w * n_right);
+    if ((st = io_ensure(c, o_m + align256(4 * n_left))) != VDF_OK) return st;
+    cudaError_t e = cudaSuccess;
+    if (n_left) e = cudaMemcpyAsync(c->io + o_l, left_key.data, w * n_left, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && n_right)
+        e = cudaMemcpyAsync(c->io + o_r, right_key.data, w * n_right, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return from_cuda(c, e, "copy keys to the device");
+    uint64_t cnt = 0;
+    uint32_t* m_dev = reinterpret_cast<uint32_t*>(c->io + o_m);
+    if ((st = left_join_locked(c, n_left, vdf_col{c->io + o_l, left_key.dtype}, n_right,
+                               vdf_col{c->io + o_r, right_key.dtype}, take_last, m_dev, nullptr, &cnt, stream)) !=
+        VDF_OK)
+        return st;
+    if (n_left) e = cudaMemcpyAsync(match_out, m_dev, 4 * n_left, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, "copy matches to the host");
+    if (n_matched) *n_matched = cnt;
+    return VDF_OK;
 }
 
 }  // extern "C"
