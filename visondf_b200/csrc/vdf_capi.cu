@@ -934,9 +934,9 @@ static vdf_status unique_locked(vdf_ctx* c, uint64_t n, vdf_col key, int keep_la
     }
     if (!keep_out) return fail(c, VDF_ERR_INVALID_ARG, "keep_out is NULL");
     const int w = vdf::dtype_width(key.dtype);
-    // workspace: permutation | sorted keys | count | the sort's own
+    // workspace: permutation | sorted keys | count | mark bits | the sort's own
     const size_t o_perm = 0, o_keys = align256(4 * n), o_cnt = o_keys + align256((size_t)w * n);
-    const size_t o_sort = o_cnt + 256;
+    const size_t o_bits = o_cnt + 256, o_sort = o_bits + align256(vdf::unique_workspace_bytes(n));
     const vdf::SortPlan plan = vdf::make_sort_plan(n, &key.dtype, 1, c->tuning);
     if ((st = ws_ensure(c, o_sort + sort_ws_need(plan, n, 1, nullptr))) != VDF_OK) return st;
     uint32_t* perm = reinterpret_cast<uint32_t*>(c->ws + o_perm);
@@ -948,8 +948,9 @@ static vdf_status unique_locked(vdf_ctx* c, uint64_t n, vdf_col key, int keep_la
     cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(uint64_t), s);
     if (e == cudaSuccess)
         e = vdf::run_unique_mark(skeys, w, perm, n, keep_last ? 1 : 0, keep_out,
-                                 reinterpret_cast<unsigned long long*>(cnt), err_word(c), s);
-    c->launches++;
+                                 reinterpret_cast<unsigned long long*>(cnt), reinterpret_cast<uint32_t*>(c->ws + o_bits),
+                                 err_word(c), s);
+    c->launches += 2;
     if (e != cudaSuccess) return from_cuda(c, e, "unique");
     return read_count(c, cnt, n_unique_host, s, "read unique count");
 }
@@ -970,7 +971,8 @@ static vdf_status left_join_locked(vdf_ctx* c, uint64_t n_left, vdf_col left_key
     const int w = vdf::dtype_width(right_key.dtype);
     const uint64_t nr = n_right;
     // workspace: right permutation | right sorted keys | distinct keys | run
-    // starts | group count | matched count | the sort's or the reduction's own
+    // starts | group count | matched count | the sort's, the reduction's or
+    // the hash table's own
     const size_t o_perm = 0, o_sk = align256(4 * nr), o_uk = o_sk + align256((size_t)w * nr);
     const size_t o_gs = o_uk + align256((size_t)w * nr), o_ng = o_gs + align256(4 * nr), o_cnt = o_ng + 256;
     const size_t o_tail = o_cnt + 256;
@@ -978,6 +980,7 @@ static vdf_status left_join_locked(vdf_ctx* c, uint64_t n_left, vdf_col left_key
     if (nr) {
         const vdf::SortPlan plan = vdf::make_sort_plan(nr, &right_key.dtype, 1, c->tuning);
         tail = std::max(sort_ws_need(plan, nr, 1, nullptr), vdf::segreduce_workspace_bytes(nr, 0));
+        tail = std::max(tail, vdf::join_workspace_bytes(nr));
     }
     if ((st = ws_ensure(c, o_tail + tail)) != VDF_OK) return st;
     uint64_t* cnt = n_matched_dev ? n_matched_dev : reinterpret_cast<uint64_t*>(c->ws + o_cnt);
@@ -1009,8 +1012,9 @@ static vdf_status left_join_locked(vdf_ctx* c, uint64_t n_left, vdf_col left_key
         return from_cuda(c, e, "distinct right keys");
     c->launches += launched;
     e = vdf::run_join_probe(left_key.data, n_left, left_key.dtype, c->ws + o_uk, a.group_start, a.n_groups, perm, nr,
-                            take_last ? 1 : 0, match_out, reinterpret_cast<unsigned long long*>(cnt), err_word(c), s);
-    c->launches++;
+                            take_last ? 1 : 0, match_out, reinterpret_cast<unsigned long long*>(cnt), c->ws + o_tail,
+                            err_word(c), s);
+    c->launches += 2;
     if (e != cudaSuccess) return from_cuda(c, e, "join probe");
     return read_count(c, cnt, n_matched_host, s, "read match count");
 }

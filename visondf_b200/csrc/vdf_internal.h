@@ -232,14 +232,20 @@ cudaError_t run_broadcast(const uint32_t* row_group, uint64_t n, const void* gro
 // ---- de-duplication and left-join row matching (vdf_unique.cu) -------------
 // keep[perm[i]] = 1 where sorted row i is the first (last = 0) or last row of
 // its key's run in the stable ascending sort, else 0; *count += kept rows.
+// bits: unique_workspace_bytes(n) of scratch.
+size_t unique_workspace_bytes(uint64_t n);
 cudaError_t run_unique_mark(const void* sorted_keys, int width, const uint32_t* perm, uint64_t n, int last,
-                            uint8_t* keep, unsigned long long* count, uint32_t* err, cudaStream_t s);
+                            uint8_t* keep, unsigned long long* count, uint32_t* bits, uint32_t* err,
+                            cudaStream_t s);
 // match[i] = the right row of left row i's key (first or last of its run in
-// the right side's stable sort), or UINT32_MAX; found by binary search over
-// the right side's distinct sorted keys ukeys[0 .. *n_groups) whose runs
-// start at gstart[g]; *matched += matched rows.
+// the right side's stable sort), or UINT32_MAX: the right side's distinct
+// sorted keys ukeys[0 .. *n_groups), whose runs start at gstart[g], go into
+// a hash table (table_ws: join_workspace_bytes(n_right)) that each left key
+// is looked up in; *matched += matched rows.
+size_t join_workspace_bytes(uint64_t n_right);
 cudaError_t run_join_probe(const void* left, uint64_t n_left, int dtype, const void* ukeys, const uint32_t* gstart,
                            const uint64_t* n_groups, const uint32_t* perm_right, uint64_t n_right, int last,
-                           uint32_t* match, unsigned long long* matched, uint32_t* err, cudaStream_t s);
+                           uint32_t* match, unsigned long long* matched, void* table_ws, uint32_t* err,
+                           cudaStream_t s);
 
 }  // namespace vdf

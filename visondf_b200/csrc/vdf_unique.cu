@@ -4,9 +4,10 @@
 // row is the key's first occurrence and its last row the last occurrence.
 //   * k_unique_mark  marks those rows in a per-row keep mask (one pass over
 //                    the sorted keys, a scatter through the permutation);
-//   * k_join_probe   looks each left key up among the right side's distinct
-//                    sorted keys (binary search over the run starts the
-//                    group-by's segment pass produced).
+//   * k_join_build   puts the right side's distinct sorted keys (the
+//                    group-by's segment pass finds them) with the row of each
+//                    one's first or last occurrence into a hash table;
+//   * k_join_probe   looks each left key up in it.
 // Keys compare by their raw bits, so -0.0 and +0.0 are different keys and a
 // NaN equals a NaN with the same bits, as with the reference's byte-wise
 // hash lookups.
@@ -33,9 +34,12 @@ __device__ __forceinline__ void add_count(unsigned long long* total, uint32_t mi
     if ((threadIdx.x & 31) == 0 && w) atomicAdd(total, (unsigned long long)w);
 }
 
+// Marks go into a bit per row (atomicOr on 32-row words: the n/8-byte mask
+// stays in L2 while the permutation scatters into it), then one coalesced
+// pass expands the bits into the caller's byte mask.
 template <typename T>
 __global__ void __launch_bounds__(256) k_unique_mark(const T* __restrict__ sk, const uint32_t* __restrict__ perm,
-                                                      uint64_t n, int last, uint8_t* __restrict__ keep,
+                                                      uint64_t n, int last, uint32_t* __restrict__ bits,
                                                       unsigned long long* count, uint32_t* err) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     uint32_t kept = 0;
@@ -45,53 +49,117 @@ __global__ void __launch_bounds__(256) k_unique_mark(const T* __restrict__ sk, c
         if (i < n) {
             const T k = sk[i];
             const bool mark = last ? (i + 1 == n || sk[i + 1] != k) : (i == 0 || sk[i - 1] != k);
-            const uint32_t r = perm[i];
-            if (r >= n) {
-                atomicOr(err, ERR_BAD_INDEX);
-            } else {
-                keep[r] = mark ? 1 : 0;
-                kept += mark ? 1u : 0u;
+            if (mark) {
+                const uint32_t r = perm[i];
+                if (r >= n) {
+                    atomicOr(err, ERR_BAD_INDEX);
+                } else {
+                    atomicOr(&bits[r >> 5], 1u << (r & 31));
+                    ++kept;
+                }
             }
         }
     }
     add_count(count, kept);
 }
 
-template <typename T>
-__device__ __forceinline__ T order_of(T raw, int dt) {
-    if constexpr (sizeof(T) == 8) return (T)order64((uint64_t)raw, dt, false);
-    else return (T)order32((uint32_t)raw, dt, false);
+// keep[r] = bit r; one 32-row word per thread, 32 bytes written per thread.
+__global__ void __launch_bounds__(256) k_expand_bits(const uint32_t* __restrict__ bits, uint64_t n,
+                                                      uint8_t* __restrict__ keep) {
+    const uint64_t words = (n + 31) / 32;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    const bool vec = (reinterpret_cast<uintptr_t>(keep) & 15) == 0;
+    for (uint64_t w = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; w < words; w += stride) {
+        const uint32_t b = bits[w];
+        uint32_t q[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t nib = (b >> (4 * k)) & 0xfu;
+            q[k] = (nib & 1u) | ((nib & 2u) << 7) | ((nib & 4u) << 14) | ((nib & 8u) << 21);
+        }
+        const uint64_t r0 = w * 32;
+        if (vec && r0 + 32 <= n) {
+            uint4* d = reinterpret_cast<uint4*>(keep + r0);
+            d[0] = make_uint4(q[0], q[1], q[2], q[3]);
+            d[1] = make_uint4(q[4], q[5], q[6], q[7]);
+        } else {
+            for (uint32_t j = 0; j < 32 && r0 + j < n; ++j) keep[r0 + j] = (uint8_t)((b >> j) & 1u);
+        }
+    }
+}
+
+// Hash table of the right side's distinct keys: 16-byte slots {raw key,
+// row + 1 (0 = empty)}, open addressing with linear probing over a
+// power-of-two capacity of at least twice the right side's rows.  The keys
+// inserted are distinct, so a slot is claimed by a CAS of its row field and
+// its key written after; the probe kernel runs after the build completes.
+struct JoinSlot {
+    unsigned long long key;
+    uint32_t row1;
+    uint32_t pad;
+};
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    // 64-bit finaliser of MurmurHash3 (fmix64)
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    x ^= x >> 33;
+    return x;
 }
 
 template <typename T>
-__global__ void __launch_bounds__(256) k_join_probe(const T* __restrict__ left, uint64_t n_left, int dt,
-                                                     const T* __restrict__ ukeys, const uint32_t* __restrict__ gstart,
+__global__ void __launch_bounds__(256) k_join_build(const T* __restrict__ ukeys, const uint32_t* __restrict__ gstart,
                                                      const uint64_t* n_groups, const uint32_t* __restrict__ perm_r,
-                                                     uint64_t n_right, int last, uint32_t* __restrict__ match,
-                                                     unsigned long long* matched, uint32_t* err) {
+                                                     uint64_t n_right, int last, JoinSlot* table, uint64_t mask,
+                                                     uint32_t* err) {
     const uint64_t G = *n_groups;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G; g += stride) {
+        const uint64_t pos = last ? (g + 1 < G ? (uint64_t)gstart[g + 1] - 1 : n_right - 1) : gstart[g];
+        if (pos >= n_right) {
+            atomicOr(err, ERR_BAD_INDEX);
+            continue;
+        }
+        const uint32_t row1 = perm_r[pos] + 1u;
+        const unsigned long long key = (unsigned long long)ukeys[g];
+        uint64_t s = mix64(key) & mask;
+        bool placed = false;
+        for (uint64_t t = 0; t <= mask; ++t) {  // at most one lap of the table
+            if (atomicCAS(&table[s].row1, 0u, row1) == 0u) {
+                table[s].key = key;
+                placed = true;
+                break;
+            }
+            s = (s + 1) & mask;
+        }
+        if (!placed) atomicOr(err, ERR_BAD_INDEX);
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_join_probe(const T* __restrict__ left, uint64_t n_left,
+                                                     const JoinSlot* __restrict__ table, uint64_t mask,
+                                                     uint32_t* __restrict__ match, unsigned long long* matched) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     uint32_t found = 0;
     for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n_left; base += stride) {
         const uint64_t i = base + threadIdx.x;
         if (i >= n_left) continue;
-        const T raw = left[i];
-        const T x = order_of(raw, dt);
-        uint64_t lo = 0, hi = G;  // first distinct key whose image is >= x
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (order_of(ukeys[mid], dt) < x) lo = mid + 1;
-            else hi = mid;
-        }
+        const unsigned long long x = (unsigned long long)left[i];
+        uint64_t s = mix64(x) & mask;
         uint32_t m = 0xffffffffu;
-        if (lo < G && ukeys[lo] == raw) {
-            const uint64_t pos = last ? (lo + 1 < G ? (uint64_t)gstart[lo + 1] - 1 : n_right - 1) : gstart[lo];
-            if (pos >= n_right) {
-                atomicOr(err, ERR_BAD_INDEX);
-            } else {
-                m = perm_r[pos];
+        for (uint64_t t = 0; t <= mask; ++t) {  // an empty slot ends every chain (load <= 1/2)
+            const ulonglong2 v = ld_rand16(reinterpret_cast<const ulonglong2*>(table + s));
+            const uint32_t row1 = (uint32_t)v.y;
+            if (row1 == 0u) break;
+            if (v.x == x) {
+                m = row1 - 1u;
                 ++found;
+                break;
             }
+            s = (s + 1) & mask;
         }
         match[i] = m;
     }
@@ -100,33 +168,59 @@ __global__ void __launch_bounds__(256) k_join_probe(const T* __restrict__ left, 
 
 }  // namespace
 
+size_t unique_workspace_bytes(uint64_t n) { return ((n + 31) / 32) * 4; }
+
 cudaError_t run_unique_mark(const void* sorted_keys, int width, const uint32_t* perm, uint64_t n, int last,
-                            uint8_t* keep, unsigned long long* count, uint32_t* err, cudaStream_t s) {
+                            uint8_t* keep, unsigned long long* count, uint32_t* bits, uint32_t* err,
+                            cudaStream_t s) {
     if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(bits, 0, unique_workspace_bytes(n), s);
+    if (e != cudaSuccess) return e;
     const uint32_t grid = grid_size(n);
     if (width == 8)
         k_unique_mark<unsigned long long><<<grid, 256, 0, s>>>(
-            static_cast<const unsigned long long*>(sorted_keys), perm, n, last, keep, count, err);
+            static_cast<const unsigned long long*>(sorted_keys), perm, n, last, bits, count, err);
     else
-        k_unique_mark<uint32_t><<<grid, 256, 0, s>>>(static_cast<const uint32_t*>(sorted_keys), perm, n, last, keep,
+        k_unique_mark<uint32_t><<<grid, 256, 0, s>>>(static_cast<const uint32_t*>(sorted_keys), perm, n, last, bits,
                                                      count, err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    k_expand_bits<<<grid_size((n + 31) / 32), 256, 0, s>>>(bits, n, keep);
     return cudaGetLastError();
 }
 
+uint64_t join_table_slots(uint64_t n_right) {
+    uint64_t cap = 1024;
+    while (cap < 2 * n_right) cap <<= 1;
+    return cap;
+}
+size_t join_workspace_bytes(uint64_t n_right) { return join_table_slots(n_right) * sizeof(JoinSlot); }
+
 cudaError_t run_join_probe(const void* left, uint64_t n_left, int dtype, const void* ukeys, const uint32_t* gstart,
                            const uint64_t* n_groups, const uint32_t* perm_right, uint64_t n_right, int last,
-                           uint32_t* match, unsigned long long* matched, uint32_t* err, cudaStream_t s) {
+                           uint32_t* match, unsigned long long* matched, void* table_ws, uint32_t* err,
+                           cudaStream_t s) {
     if (n_left == 0) return cudaSuccess;
-    const uint32_t grid = grid_size(n_left);
-    if (dtype_width(dtype) == 8)
-        k_join_probe<unsigned long long><<<grid, 256, 0, s>>>(
-            static_cast<const unsigned long long*>(left), n_left, dtype,
-            static_cast<const unsigned long long*>(ukeys), gstart, n_groups, perm_right, n_right, last, match, matched,
-            err);
+    const uint64_t slots = join_table_slots(n_right);
+    JoinSlot* table = static_cast<JoinSlot*>(table_ws);
+    cudaError_t e = cudaMemsetAsync(table, 0, slots * sizeof(JoinSlot), s);
+    if (e != cudaSuccess) return e;
+    const bool w8 = dtype_width(dtype) == 8;
+    if (w8)
+        k_join_build<unsigned long long><<<grid_size(n_right), 256, 0, s>>>(
+            static_cast<const unsigned long long*>(ukeys), gstart, n_groups, perm_right, n_right, last, table,
+            slots - 1, err);
     else
-        k_join_probe<uint32_t><<<grid, 256, 0, s>>>(static_cast<const uint32_t*>(left), n_left, dtype,
-                                                     static_cast<const uint32_t*>(ukeys), gstart, n_groups, perm_right,
-                                                     n_right, last, match, matched, err);
+        k_join_build<uint32_t><<<grid_size(n_right), 256, 0, s>>>(static_cast<const uint32_t*>(ukeys), gstart,
+                                                                   n_groups, perm_right, n_right, last, table,
+                                                                   slots - 1, err);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    const uint32_t grid = grid_size(n_left);
+    if (w8)
+        k_join_probe<unsigned long long><<<grid, 256, 0, s>>>(static_cast<const unsigned long long*>(left), n_left,
+                                                              table, slots - 1, match, matched);
+    else
+        k_join_probe<uint32_t><<<grid, 256, 0, s>>>(static_cast<const uint32_t*>(left), n_left, table, slots - 1,
+                                                    match, matched);
     return cudaGetLastError();
 }
 
