@@ -11,7 +11,9 @@ int32 payloads.  One vdf_sort_groupby call per step through the C-ABI.
   value  rows/s with the inputs resident in HBM (device-timed, CUDA events).
   e2e    the same call fed from pinned HOST buffers: every step copies the five
          input columns host->device, runs the call, and copies the result
-         (permutation + the group table) device->host.
+         (permutation + the group table) device->host; issued from two host
+         threads with a context and stream each, so one step's uploads overlap
+         the other's downloads (e2e.single_stream: one call at a time).
   roofline   the dominant kernel's algorithmic bytes per launch / its average
              launch time (CUDA events around each launch, inside the timed
              region), against the measured HBM copy bandwidth.
@@ -563,48 +565,94 @@ def our_arm(args, rank: int, world: int, local_rank: int):
         from visondf_b200 import _lib
         h2d = sum(host[k].numel() * host[k].element_size() for k in names)
         pin = lambda dtype: torch.empty(n, dtype=dtype).pin_memory()  # noqa: E731
-        hp = {"perm": pin(torch.int32), "gk1": pin(torch.int64), "gk2": pin(torch.int32), "cnt": pin(torch.int64),
-              "f_sum": pin(torch.float64), "f_min": pin(torch.float64), "f_max": pin(torch.float64),
-              "f_mean": pin(torch.float64), "i_sum": pin(torch.int64), "i_hi": pin(torch.int64),
-              "i_min": pin(torch.int32), "i_max": pin(torch.int32), "i_mean": pin(torch.float64)}
-        hk = (_lib.vdf_col * 2)(_lib.vdf_col(host["key1"].data_ptr(), vdf.I64), _lib.vdf_col(host["key2"].data_ptr(), vdf.I32))
-        hpay = (_lib.vdf_col * 3)(_lib.vdf_col(host["f64"].data_ptr(), vdf.F64), _lib.vdf_col(host["i32"].data_ptr(), vdf.I32),
-                                  _lib.vdf_col(host["rowid"].data_ptr(), vdf.U64))
-        hagg = (_lib.vdf_agg_out * 2)(
-            _lib.vdf_agg_out(hp["f_sum"].data_ptr(), None, hp["f_min"].data_ptr(), hp["f_max"].data_ptr(), hp["f_mean"].data_ptr()),
-            _lib.vdf_agg_out(hp["i_sum"].data_ptr(), hp["i_hi"].data_ptr(), hp["i_min"].data_ptr(), hp["i_max"].data_ptr(),
-                             hp["i_mean"].data_ptr()))
-        hgk = (C.c_void_p * 2)(hp["gk1"].data_ptr(), hp["gk2"].data_ptr())
-        hac = (C.c_int32 * 2)(0, 1)
-        ng = C.c_uint64(0)
-        ha = _lib.vdf_sort_groupby_args()
-        ha.n, ha.keys, ha.nkeys, ha.order = n, hk, 2, vdf.ORDER_ASC
-        ha.payload, ha.npayload = hpay, 3
-        ha.perm_out = hp["perm"].data_ptr()
-        ha.groupby, ha.agg_cols, ha.nagg, ha.aggs = 1, hac, 2, hagg
-        ha.group_keys_out, ha.group_count_out = hgk, hp["cnt"].data_ptr()
-        ha.n_groups_host = C.pointer(ng)
 
-        def e2e_step():
-            ctx._check(vdf.lib.vdf_sort_groupby_host(ctx.handle, C.byref(ha), stream.cuda_stream), "vdf_sort_groupby_host")
+        def host_call(c, strm):
+            """One vdf_sort_groupby_host call's argument block with its own
+            pinned output buffers, on context c and stream strm."""
+            hp = {"perm": pin(torch.int32), "gk1": pin(torch.int64), "gk2": pin(torch.int32), "cnt": pin(torch.int64),
+                  "f_sum": pin(torch.float64), "f_min": pin(torch.float64), "f_max": pin(torch.float64),
+                  "f_mean": pin(torch.float64), "i_sum": pin(torch.int64), "i_hi": pin(torch.int64),
+                  "i_min": pin(torch.int32), "i_max": pin(torch.int32), "i_mean": pin(torch.float64)}
+            hk = (_lib.vdf_col * 2)(_lib.vdf_col(host["key1"].data_ptr(), vdf.I64),
+                                    _lib.vdf_col(host["key2"].data_ptr(), vdf.I32))
+            hpay = (_lib.vdf_col * 3)(_lib.vdf_col(host["f64"].data_ptr(), vdf.F64),
+                                      _lib.vdf_col(host["i32"].data_ptr(), vdf.I32),
+                                      _lib.vdf_col(host["rowid"].data_ptr(), vdf.U64))
+            hagg = (_lib.vdf_agg_out * 2)(
+                _lib.vdf_agg_out(hp["f_sum"].data_ptr(), None, hp["f_min"].data_ptr(), hp["f_max"].data_ptr(),
+                                 hp["f_mean"].data_ptr()),
+                _lib.vdf_agg_out(hp["i_sum"].data_ptr(), hp["i_hi"].data_ptr(), hp["i_min"].data_ptr(),
+                                 hp["i_max"].data_ptr(), hp["i_mean"].data_ptr()))
+            hgk = (C.c_void_p * 2)(hp["gk1"].data_ptr(), hp["gk2"].data_ptr())
+            hac = (C.c_int32 * 2)(0, 1)
+            ng = C.c_uint64(0)
+            ha = _lib.vdf_sort_groupby_args()
+            ha.n, ha.keys, ha.nkeys, ha.order = n, hk, 2, vdf.ORDER_ASC
+            ha.payload, ha.npayload = hpay, 3
+            ha.perm_out = hp["perm"].data_ptr()
+            ha.groupby, ha.agg_cols, ha.nagg, ha.aggs = 1, hac, 2, hagg
+            ha.group_keys_out, ha.group_count_out = hgk, hp["cnt"].data_ptr()
+            ha.n_groups_host = C.pointer(ng)
+            keep = (hp, hk, hpay, hagg, hgk, hac)  # the structs point into these
 
+            def step():
+                c._check(vdf.lib.vdf_sort_groupby_host(c.handle, C.byref(ha), strm.cuda_stream),
+                         "vdf_sort_groupby_host")
+            return step, ng, keep
+
+        # (1) one stream: each call's copies and kernels in turn
+        step_a, ng, keep_a = host_call(ctx, stream)
         for _ in range(max(1, args.warmup)):
-            e2e_step()
+            step_a()
         torch.cuda.synchronize()
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            e2e_step()
+            step_a()
         e1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ems = e0.elapsed_time(e1) / args.steps
+        ems_single = replicas.max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
         g = int(ng.value)
         d2h = 4 * n + g * (8 + 4 + 8 + 4 * 8 + (8 + 8 + 4 + 4 + 8))
-        ems = replicas.max_over_ranks(ems, world, dev)
-        e2e = {"value": replicas.whole_job_rate(n, world, ems), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-               "ms_per_step": ems, "call": "vdf_sort_groupby_host (pinned host buffers)"}
+
+        # (2) two host threads, each with its own context and stream (the
+        # library's rule for concurrent use), so one step's uploads run while
+        # the other's results come back over the full-duplex link; the events
+        # span both streams
+        import threading
+        ctx_b = vdf.Context(local_rank)
+        stream_b = torch.cuda.Stream(device=dev)
+        step_b, _, keep_b = host_call(ctx_b, stream_b)
+        for _ in range(max(1, args.warmup)):
+            step_b()
+        torch.cuda.synchronize()
+        barrier()
+        k_a = (args.steps + 1) // 2
+        k_b = args.steps - k_a
+        e0, e1, eb = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record(stream)
+        stream_b.wait_event(e0)
+        worker = threading.Thread(target=lambda: [step_b() for _ in range(k_b)])
+        worker.start()
+        for _ in range(k_a):
+            step_a()
+        worker.join()
+        eb.record(stream_b)
+        stream.wait_event(eb)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ems = replicas.max_over_ranks(e0.elapsed_time(e1) / args.steps, world, dev)
+        ctx_b.close()
+        del keep_a, keep_b
+        e2e = {"value": replicas.whole_job_rate(n, world, ems), "unit": UNIT, "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": d2h, "ms_per_step": ems,
+               "call": "vdf_sort_groupby_host (pinned host buffers) from two host threads, one context and stream "
+                       "each, consecutive steps overlapping",
+               "single_stream": {"value": replicas.whole_job_rate(n, world, ems_single), "ms_per_step": ems_single,
+                                 "call": "vdf_sort_groupby_host, one call at a time"}}
 
     # ---- CPU baseline (rank 0, one GPU only) -------------------------------------
     cpu = None
