@@ -351,15 +351,23 @@ vdf_status vdf_broadcast(vdf_ctx* ctx, uint64_t n, const uint32_t* row_group, co
 vdf_status vdf_unique(vdf_ctx* ctx, uint64_t n, vdf_col key, int keep_last, uint8_t* keep_out,
                       uint64_t* n_unique_dev, uint64_t* n_unique_host, void* stream);
 
-/* match_out[i] (u32) = the row of the right column holding left row i's key
- * -- its first such row (take_last = 0, LeftJoinMethods::First) or last
- * (take_last = 1, LeftJoinMethods::Last) -- or UINT32_MAX when the key is
- * absent; the number of matched left rows is the count.  Both columns have
- * the same dtype.  Replaces the map build and probe of transform_left_join_mt
- * (V/transform/transform_left_join/transform_left_join_mt.hpp:172-205),
- * whose match_idx holds SIZE_MAX for absent keys. */
+/* Left-join matching methods (LeftJoinMethods, V/types/supported_leftjoin_methods.inl:1-5). */
+typedef enum vdf_join_method {
+    VDF_JOIN_FIRST = 0,   /* the key's first right row                                  */
+    VDF_JOIN_LAST = 1,    /* the key's last right row                                   */
+    VDF_JOIN_ALIGNED = 2  /* the k-th left occurrence of a key takes its k-th right row */
+} vdf_join_method;
+
+/* match_out[i] (u32) = the row of the right column that left row i takes
+ * under `method`, or UINT32_MAX when there is none (the key is absent, or,
+ * for VDF_JOIN_ALIGNED, the right side has fewer rows of it); the number of
+ * matched left rows is the count.  Both columns have the same dtype.
+ * Replaces the map build and probe of transform_left_join_mt
+ * (V/transform/transform_left_join/transform_left_join_mt.hpp:172-238),
+ * whose match_idx holds SIZE_MAX for unmatched rows.  Aligned sorts the left
+ * side as well (its rows' occurrence ranks). */
 vdf_status vdf_left_join_index(vdf_ctx* ctx, uint64_t n_left, vdf_col left_key, uint64_t n_right,
-                               vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched_dev,
+                               vdf_col right_key, int method, uint32_t* match_out, uint64_t* n_matched_dev,
                                uint64_t* n_matched_host, void* stream);
 
 /* The same two operations on HOST columns and outputs (copied through the
@@ -369,7 +377,7 @@ vdf_status vdf_left_join_index(vdf_ctx* ctx, uint64_t n_left, vdf_col left_key, 
 vdf_status vdf_unique_host(vdf_ctx* ctx, uint64_t n, vdf_col key, int keep_last, uint8_t* keep_out,
                            uint64_t* n_unique, void* stream);
 vdf_status vdf_left_join_index_host(vdf_ctx* ctx, uint64_t n_left, vdf_col left_key, uint64_t n_right,
-                                    vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched,
+                                    vdf_col right_key, int method, uint32_t* match_out, uint64_t* n_matched,
                                     void* stream);
 
 /* ---- batched queries ------------------------------------------------------

@@ -12,7 +12,7 @@
 //                                 transform_group_by_mt.hpp:3-114
 //   transform_unique[_mt]         transform/transform_unique/transform_unique_mt.hpp:3-11
 //   transform_left_join[_mt]      transform/transform_left_join/transform_left_join_mt.hpp:3-15
-//                                 (methods First and Last)
+//                                 (methods First, Last and Aligned)
 //
 // Storage follows the reference: column-major type blocks (here int_v, uint_v,
 // dbl_v plus 64-bit integer blocks lint_v / luint_v, which the reference lacks:
@@ -58,7 +58,7 @@ enum class SortType { Standard, Radix };  // supported_sorting_methods.inl:1-4 (
 // supported_group_methods.inl:1-7, plus Min and Max
 enum class GroupFunction { Occurence, Sum, Mean, Gather, None, Min, Max };
 
-// types/supported_leftjoin_methods.inl:1-5 (Aligned: not on the GPU path)
+// types/supported_leftjoin_methods.inl:1-5
 enum class LeftJoinMethods { First, Last, Aligned };
 
 struct DefaultTypes {  // types/inference_type.hpp:3-8 (CharT omitted: no char columns here)
@@ -356,7 +356,8 @@ class Dataframe {
     // ---- left join ---------------------------------------------------------------------
     // transform_left_join_mt.hpp:3-15: appends obj's columns; row i takes the
     // values of obj's first (First) or last (Last) row whose key2 equals this
-    // frame's key1 at row i, or the per-type default where none does.
+    // frame's key1 at row i -- or, Aligned, the k-th such row for the key's
+    // k-th occurrence here -- or the per-type default where there is none.
     template <typename T = void, unsigned int CORES = 4, bool SimdHash = true,
               LeftJoinMethods Method = LeftJoinMethods::First>
     void transform_left_join_mt(const Dataframe& obj, const unsigned int key1, const unsigned int key2,
@@ -370,10 +371,7 @@ class Dataframe {
             std::cerr << "Can't perform this operation while in`view` mode, consider applying `.materialize()`\n";
             return;
         }
-        if constexpr (Method == LeftJoinMethods::Aligned) {
-            std::cerr << "transform_left_join: LeftJoinMethods::Aligned is not supported on the GPU path\n";
-            return;
-        } else {
+        {
             if (key1 >= ncol || key2 >= obj.ncol) {
                 std::cerr << "Column not found\n";
                 return;
@@ -388,7 +386,10 @@ class Dataframe {
             uint64_t matched = 0;
             if (!detail::report(vdf_left_join_index_host(context(), nrow, col_desc(key1), right.nrow,
                                                          right.col_desc(key2),
-                                                         Method == LeftJoinMethods::Last ? 1 : 0, match.data(),
+                                                         Method == LeftJoinMethods::First  ? VDF_JOIN_FIRST
+                                                         : Method == LeftJoinMethods::Last ? VDF_JOIN_LAST
+                                                                                           : VDF_JOIN_ALIGNED,
+                                                         match.data(),
                                                          &matched, nullptr),
                                 "transform_left_join"))
                 return;

@@ -489,11 +489,58 @@ int64_t orc_unique(const void* col, int dt, size_t n, int last, uint8_t* keep) {
  * each key (try_emplace, First) or the last (assignment, Last); each left row
  * then looks its key up (:201-205): match[i] = the right row, or UINT32_MAX where the
  * key is absent (the reference's SIZE_MAX).  Keys compare by their raw bytes.
+ * Method Aligned (method == 2, :206-238): the right rows of each key are kept
+ * in row order with a cursor; each left row, in row order, takes the row at
+ * its key's cursor and advances it, so the k-th left occurrence of a key
+ * matches the k-th right occurrence, and left rows beyond the right side's
+ * count of that key match nothing.
  * Returns the number of matched left rows, or -1 on allocation failure.
  */
+static int64_t orc_left_join_aligned(const void* left, size_t n_left, const void* right, size_t n_right, int w,
+                                     uint32_t* match) {
+    orc_map m;
+    if (orc_map_init(&m, n_right)) return -1;
+    /* key -> slot index, then per-key row lists (CSR) and cursors */
+    size_t* slot_of = (size_t*)malloc((n_right ? n_right : 1) * sizeof(size_t));
+    size_t nslots = m.mask + 1;
+    size_t* cnt = (size_t*)calloc(nslots + 1, sizeof(size_t));
+    size_t* cur = (size_t*)calloc(nslots, sizeof(size_t));
+    uint32_t* rows = (uint32_t*)malloc((n_right ? n_right : 1) * sizeof(uint32_t));
+    if (!slot_of || !cnt || !cur || !rows) {
+        free(slot_of); free(cnt); free(cur); free(rows); orc_map_free(&m);
+        return -1;
+    }
+    for (size_t j = 0; j < n_right; ++j) {
+        const uint64_t k = orc_raw_bits(right, w, j);
+        const size_t s = orc_map_slot(&m, k);
+        if (m.val[s] < 0) {
+            m.key[s] = k;
+            m.val[s] = (int64_t)s;
+        }
+        slot_of[j] = s;
+        cnt[s + 1]++;
+    }
+    for (size_t s = 0; s < nslots; ++s) cnt[s + 1] += cnt[s];  /* list of slot s: rows[cnt[s] .. cnt[s+1]) */
+    for (size_t j = 0; j < n_right; ++j) rows[cnt[slot_of[j]] + cur[slot_of[j]]++] = (uint32_t)j;
+    memset(cur, 0, nslots * sizeof(size_t));
+    int64_t matched = 0;
+    for (size_t i = 0; i < n_left; ++i) {
+        const size_t s = orc_map_slot(&m, orc_raw_bits(left, w, i));
+        match[i] = 0xffffffffu;
+        if (m.val[s] >= 0 && cnt[s] + cur[s] < cnt[s + 1]) {
+            match[i] = rows[cnt[s] + cur[s]++];
+            ++matched;
+        }
+    }
+    free(slot_of); free(cnt); free(cur); free(rows);
+    orc_map_free(&m);
+    return matched;
+}
+
 int64_t orc_left_join(const void* left, size_t n_left, const void* right, size_t n_right, int dt, int last,
                       uint32_t* match) {
     const int w = orc_dtype_width(dt);
+    if (last == 2) return orc_left_join_aligned(left, n_left, right, n_right, w, match);
     orc_map m;
     if (orc_map_init(&m, n_right)) return -1;
     for (size_t j = 0; j < n_right; ++j) {

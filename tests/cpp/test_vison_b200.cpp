@@ -198,24 +198,33 @@ static void test_transform_left_join() {
         rv[j] = (int)j;
         rd[j] = 0.5 * j;
     }
-    for (int last = 0; last < 2; ++last) {
-        std::map<int, unsigned> m;
-        for (unsigned j = 0; j < NR; ++j)
-            if (last || !m.count(rk[j])) m[rk[j]] = j;
+    for (int method = 0; method < 3; ++method) {
+        // expected right row per left row: first, last, or the k-th for the k-th occurrence
+        std::map<int, std::vector<unsigned>> rows;
+        for (unsigned j = 0; j < NR; ++j) rows[rk[j]].push_back(j);
+        std::map<int, unsigned> next;
+        std::vector<long> want(NL, -1);
+        for (unsigned i = 0; i < NL; ++i) {
+            auto it = rows.find(lk[i]);
+            if (it == rows.end()) continue;
+            if (method == 0) want[i] = it->second.front();
+            else if (method == 1) want[i] = it->second.back();
+            else if (next[lk[i]] < it->second.size()) want[i] = it->second[next[lk[i]]++];
+        }
         DF left, right;
         left.add_col(std::vector<int>(lk), "lk");
         right.add_col(std::vector<int>(rk), "rk");
         right.add_col(std::vector<int>(rv), "rv");
         right.add_col(std::vector<double>(rd), "rd");
-        if (last) left.transform_left_join<void, true, LeftJoinMethods::Last>(right, 0, 0, ' ', "NA", 0, -7, 0, -1.5);
-        else left.transform_left_join<void, true, LeftJoinMethods::First>(right, 0, 0, ' ', "NA", 0, -7, 0, -1.5);
+        if (method == 0) left.transform_left_join<void, true, LeftJoinMethods::First>(right, 0, 0, ' ', "NA", 0, -7, 0, -1.5);
+        else if (method == 1) left.transform_left_join<void, true, LeftJoinMethods::Last>(right, 0, 0, ' ', "NA", 0, -7, 0, -1.5);
+        else left.transform_left_join<void, true, LeftJoinMethods::Aligned>(right, 0, 0, ' ', "NA", 0, -7, 0, -1.5);
         CHECK(left.ncol == 4);
         bool ok = left.ncol == 4;
         for (unsigned i = 0; ok && i < NL; ++i) {
-            auto it = m.find(lk[i]);
-            const int ek = it == m.end() ? -7 : rk[it->second];
-            const int ev = it == m.end() ? -7 : rv[it->second];
-            const double ed = it == m.end() ? -1.5 : rd[it->second];
+            const int ek = want[i] < 0 ? -7 : rk[want[i]];
+            const int ev = want[i] < 0 ? -7 : rv[want[i]];
+            const double ed = want[i] < 0 ? -1.5 : rd[want[i]];
             ok &= left.int_v[1][i] == ek && left.int_v[2][i] == ev && left.dbl_v[0][i] == ed;
         }
         CHECK(ok);

@@ -167,13 +167,14 @@ def unique(key, keep_last=False):
     return keep, int(d)
 
 
-def left_join(left, right, take_last=False):
-    """Oracle left-join matching: (match uint32, UINT32_MAX where absent; matched rows)."""
+def left_join(left, right, method=0):
+    """Oracle left-join matching, method 0 First / 1 Last / 2 Aligned:
+    (match uint32, UINT32_MAX where absent; matched rows)."""
     left = np.ascontiguousarray(left)
     right = np.ascontiguousarray(right)
     assert left.dtype == right.dtype
     match = np.empty(left.size, np.uint32)
     m = oracle().orc_left_join(_vp(left), left.size, _vp(right), right.size, DT[left.dtype],
-                               1 if take_last else 0, _vp(match))
+                               int(method), _vp(match))
     assert m >= 0
     return match, int(m)

@@ -26,10 +26,24 @@ def py_unique(key, keep_last):
     return keep, len(seen)
 
 
-def py_left_join(left, right, take_last):
+def py_left_join(left, right, method):
+    if method == 2:  # Aligned: the k-th left occurrence takes the k-th right one
+        rows, nxt = {}, {}
+        for j, k in enumerate(raw(right)):
+            rows.setdefault(k, []).append(j)
+        out = []
+        for k in raw(left):
+            c = nxt.get(k, 0)
+            if k in rows and c < len(rows[k]):
+                out.append(rows[k][c])
+                nxt[k] = c + 1
+            else:
+                out.append(0xFFFFFFFF)
+        match = np.array(out, dtype=np.uint32)
+        return match, int((match != 0xFFFFFFFF).sum())
     m = {}
     for j, k in enumerate(raw(right)):
-        if take_last or k not in m:
+        if method == 1 or k not in m:
             m[k] = j
     match = np.array([m.get(k, 0xFFFFFFFF) for k in raw(left)], dtype=np.uint32)
     return match, int((match != 0xFFFFFFFF).sum())
@@ -56,15 +70,15 @@ def test_oracle_unique_matches_the_set_walk(dt, keep_last, n, card):
 
 
 @pytest.mark.parametrize("dt", DTYPES)
-@pytest.mark.parametrize("take_last", [False, True])
+@pytest.mark.parametrize("method", [0, 1, 2])
 @pytest.mark.parametrize("nl,nr,card", [(0, 5, 3), (7, 0, 3), (2000, 1500, 900), (100, 3000, 50)])
-def test_oracle_left_join_matches_the_map_walk(dt, take_last, nl, nr, card):
+def test_oracle_left_join_matches_the_map_walk(dt, method, nl, nr, card):
     rng = np.random.default_rng(nl * 7 + nr)
     pool = keys(dt, card, card, rng)
     left = np.concatenate([pool[rng.integers(0, card, size=nl)], keys(dt, 3, 3, rng)])[:nl]
     right = pool[rng.integers(0, card, size=nr)]
-    match, m = ob.left_join(left, right, take_last)
-    pm, pmm = py_left_join(left, right, take_last)
+    match, m = ob.left_join(left, right, method)
+    pm, pmm = py_left_join(left, right, method)
     assert m == pmm and (match == pm).all()
 
 

@@ -47,10 +47,10 @@ def test_unique_empty_and_large(ctx):
 
 
 @pytest.mark.parametrize("dt", DTYPES)
-@pytest.mark.parametrize("take_last", [False, True])
+@pytest.mark.parametrize("method", [0, 1, 2])
 @pytest.mark.parametrize("nl,nr,card", [(1, 1, 1), (5000, 1, 1), (20_000, 30_000, 7000), (100_000, 3, 3),
-                                        (250_000, 400_000, 300_000)])
-def test_left_join_matches_the_oracle(ctx, dt, take_last, nl, nr, card):
+                                        (250_000, 400_000, 300_000), (60_000, 90_000, 500)])
+def test_left_join_matches_the_oracle(ctx, dt, method, nl, nr, card):
     rng = np.random.default_rng(nl + 3 * nr + card)
     pool = keys(dt, card, card, rng)
     # about one left row in eight carries a key drawn outside the right side's pool
@@ -58,18 +58,25 @@ def test_left_join_matches_the_oracle(ctx, dt, take_last, nl, nr, card):
     miss = rng.random(nl) < 0.125
     left[miss] = keys(dt, int(miss.sum()), 11, np.random.default_rng(nl))
     right = pool[rng.integers(0, card, size=nr)]
-    match, m = ctx.left_join_index(dev(left), dev(right), take_last)
-    om, omm = ob.left_join(left, right, take_last)
+    match, m = ctx.left_join_index(dev(left), dev(right), method)
+    om, omm = ob.left_join(left, right, method)
     assert m == omm
     assert (host(match).view(np.uint32) == om).all()
 
 
-def test_left_join_empty_sides(ctx):
+@pytest.mark.parametrize("method", [0, 1, 2])
+def test_left_join_empty_sides(ctx, method):
     a = dev(np.array([3, 1, 3], np.int64))
-    match, m = ctx.left_join_index(a, torch.empty(0, dtype=torch.int64, device="cuda"))
+    match, m = ctx.left_join_index(a, torch.empty(0, dtype=torch.int64, device="cuda"), method)
     assert m == 0 and (host(match).view(np.uint32) == 0xFFFFFFFF).all()
-    match, m = ctx.left_join_index(torch.empty(0, dtype=torch.int64, device="cuda"), a)
+    match, m = ctx.left_join_index(torch.empty(0, dtype=torch.int64, device="cuda"), a, method)
     assert m == 0 and match.numel() == 0
+
+
+def test_bad_join_method_is_rejected(ctx):
+    import visondf_b200 as vdf
+    with pytest.raises(vdf.VdfError):
+        ctx.left_join_index(dev(np.arange(4, dtype=np.int64)), dev(np.arange(4, dtype=np.int64)), 3)
 
 
 def test_signed_zero_and_nan_bits(ctx):
@@ -78,8 +85,11 @@ def test_signed_zero_and_nan_bits(ctx):
     assert d == 4 and host(keep).tolist() == [1, 1, 1, 0, 0, 0, 1]
     keep, d = ctx.unique(dev(key), keep_last=True)
     assert d == 4 and host(keep).tolist() == [0, 0, 0, 1, 1, 1, 1]
-    match, m = ctx.left_join_index(dev(np.array([-0.0, 1.0, np.nan], np.float64)), dev(key), take_last=True)
+    match, m = ctx.left_join_index(dev(np.array([-0.0, 1.0, np.nan], np.float64)), dev(key), method=1)
     assert m == 2 and host(match).view(np.uint32).tolist() == [4, 0xFFFFFFFF, 5]
+    left = np.array([-0.0, np.nan, -0.0, -0.0, 0.0], np.float64)
+    match, m = ctx.left_join_index(dev(left), dev(key), method=2)  # k-th occurrence takes the k-th right row
+    assert m == 4 and host(match).view(np.uint32).tolist() == [1, 2, 4, 0xFFFFFFFF, 0]
 
 
 def test_mismatched_dtypes_are_rejected(ctx):

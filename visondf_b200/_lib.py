@@ -431,16 +431,16 @@ class Context:
                                    C.byref(cnt), _stream(stream)), "vdf_unique")
         return keep, int(cnt.value)
 
-    def left_join_index(self, left: torch.Tensor, right: torch.Tensor, take_last: bool = False, stream=None):
-        """(match, n_matched): match[i] = the first (or, with take_last, the
-        last) row of `right` holding left[i]'s key, or UINT32_MAX (int32 view:
-        -1) where none does."""
+    def left_join_index(self, left: torch.Tensor, right: torch.Tensor, method: int = 0, stream=None):
+        """(match, n_matched): match[i] = the row of `right` that left row i
+        takes -- method 0: the first row holding its key, 1: the last, 2
+        (aligned): the k-th one for the key's k-th left occurrence -- or
+        UINT32_MAX (int32 view: -1) where there is none."""
         n = left.numel()
         match = torch.empty(n, dtype=torch.int32, device=left.device)
         cnt = C.c_uint64(0)
-        self._check(lib.vdf_left_join_index(self.handle, n, _col(left), right.numel(), _col(right),
-                                            1 if take_last else 0, _ptr(match), None, C.byref(cnt),
-                                            _stream(stream)), "vdf_left_join_index")
+        self._check(lib.vdf_left_join_index(self.handle, n, _col(left), right.numel(), _col(right), int(method),
+                                            _ptr(match), None, C.byref(cnt), _stream(stream)), "vdf_left_join_index")
         return match, int(cnt.value)
 
 

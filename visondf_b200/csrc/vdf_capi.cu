@@ -957,7 +957,7 @@ static vdf_status unique_locked(vdf_ctx* c, uint64_t n, vdf_col key, int keep_la
 
 // vdf_left_join_index with the context lock held
 static vdf_status left_join_locked(vdf_ctx* c, uint64_t n_left, vdf_col left_key, uint64_t n_right,
-                                   vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched_dev,
+                                   vdf_col right_key, int method, uint32_t* match_out, uint64_t* n_matched_dev,
                                    uint64_t* n_matched_host, void* stream) {
     vdf_status st;
     if ((st = check_rows(c, n_left)) != VDF_OK) return st;
@@ -965,57 +965,89 @@ static vdf_status left_join_locked(vdf_ctx* c, uint64_t n_left, vdf_col left_key
     if ((st = check_keys(c, n_left, &left_key, 1)) != VDF_OK) return st;
     if ((st = check_keys(c, n_right, &right_key, 1)) != VDF_OK) return st;
     if (left_key.dtype != right_key.dtype) return fail(c, VDF_ERR_INVALID_ARG, "left and right keys differ in dtype");
+    if (method < VDF_JOIN_FIRST || method > VDF_JOIN_ALIGNED) return fail(c, VDF_ERR_INVALID_ARG, "bad method %d", method);
     if (n_left && !match_out) return fail(c, VDF_ERR_INVALID_ARG, "match_out is NULL");
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     DeviceGuard g(c->device);
     const int w = vdf::dtype_width(right_key.dtype);
-    const uint64_t nr = n_right;
+    const uint64_t nr = n_right, nl = n_left;
+    const bool aligned = method == VDF_JOIN_ALIGNED;
     // workspace: right permutation | right sorted keys | distinct keys | run
-    // starts | group count | matched count | the sort's, the reduction's or
-    // the hash table's own
+    // starts | group count | matched count | (aligned: left permutation, left
+    // sorted keys, run of each sorted left row, left run starts, left group
+    // count) | the sorts', the reductions' or the hash table's own
     const size_t o_perm = 0, o_sk = align256(4 * nr), o_uk = o_sk + align256((size_t)w * nr);
     const size_t o_gs = o_uk + align256((size_t)w * nr), o_ng = o_gs + align256(4 * nr), o_cnt = o_ng + 256;
-    const size_t o_tail = o_cnt + 256;
+    size_t o = o_cnt + 256;
+    size_t o_lperm = 0, o_lsk = 0, o_lrg = 0, o_lgs = 0, o_lng = 0;
+    if (aligned) {
+        o_lperm = o; o += align256(4 * nl);
+        o_lsk = o; o += align256((size_t)w * nl);
+        o_lrg = o; o += align256(4 * nl);
+        o_lgs = o; o += align256(4 * nl);
+        o_lng = o; o += 256;
+    }
+    const size_t o_tail = o;
     size_t tail = 0;
     if (nr) {
         const vdf::SortPlan plan = vdf::make_sort_plan(nr, &right_key.dtype, 1, c->tuning);
         tail = std::max(sort_ws_need(plan, nr, 1, nullptr), vdf::segreduce_workspace_bytes(nr, 0));
         tail = std::max(tail, vdf::join_workspace_bytes(nr));
     }
+    if (aligned && nl) {
+        const vdf::SortPlan plan = vdf::make_sort_plan(nl, &left_key.dtype, 1, c->tuning);
+        tail = std::max(tail, std::max(sort_ws_need(plan, nl, 1, nullptr), vdf::segreduce_workspace_bytes(nl, 0)));
+    }
     if ((st = ws_ensure(c, o_tail + tail)) != VDF_OK) return st;
     uint64_t* cnt = n_matched_dev ? n_matched_dev : reinterpret_cast<uint64_t*>(c->ws + o_cnt);
     cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(uint64_t), s);
     if (e != cudaSuccess) return from_cuda(c, e, "clear count");
-    if (n_left == 0) return read_count(c, cnt, n_matched_host, s, "read match count");
+    if (nl == 0) return read_count(c, cnt, n_matched_host, s, "read match count");
     if (nr == 0) {  // nothing to match
-        if ((e = cudaMemsetAsync(match_out, 0xff, 4 * n_left, s)) != cudaSuccess) return from_cuda(c, e, "no match");
+        if ((e = cudaMemsetAsync(match_out, 0xff, 4 * nl, s)) != cudaSuccess) return from_cuda(c, e, "no match");
         return read_count(c, cnt, n_matched_host, s, "read match count");
     }
-    uint32_t* perm = reinterpret_cast<uint32_t*>(c->ws + o_perm);
-    void* sk = c->ws + o_sk;
-    void* const souts[1] = {sk};
-    if ((st = sort_impl(c, nr, &right_key, 1, VDF_ORDER_ASC, perm, souts, c->ws + o_tail, c->ws_cap - o_tail, s)) !=
-        VDF_OK)
-        return st;
-    // distinct right keys and the sorted row where each one's run starts
-    vdf::SegArgs a{};
-    a.n = nr;
-    a.nkeys = 1;
-    a.nvals = 0;
-    a.key[0] = vdf::SegCol{sk, right_key.dtype};
-    a.key_out[0] = c->ws + o_uk;
-    a.group_start = reinterpret_cast<uint32_t*>(c->ws + o_gs);
-    a.n_groups = reinterpret_cast<uint64_t*>(c->ws + o_ng);
-    a.err = err_word(c);
-    int launched = 0;
-    if ((e = vdf::run_segreduce(a, c->ws + o_tail, s, prof_of(c), &launched)) != cudaSuccess)
-        return from_cuda(c, e, "distinct right keys");
-    c->launches += launched;
-    e = vdf::run_join_probe(left_key.data, n_left, left_key.dtype, c->ws + o_uk, a.group_start, a.n_groups, perm, nr,
-                            take_last ? 1 : 0, match_out, reinterpret_cast<unsigned long long*>(cnt), c->ws + o_tail,
-                            err_word(c), s);
+    // one side: stable sort, then its distinct keys and their run starts
+    auto sort_side = [&](uint64_t n, const vdf_col& key, size_t o_p, size_t o_s, size_t o_u, size_t o_g, size_t o_n,
+                         size_t o_rg) -> vdf_status {
+        void* const souts[1] = {c->ws + o_s};
+        vdf_status r = sort_impl(c, n, &key, 1, VDF_ORDER_ASC, reinterpret_cast<uint32_t*>(c->ws + o_p), souts,
+                                 c->ws + o_tail, c->ws_cap - o_tail, s);
+        if (r != VDF_OK) return r;
+        vdf::SegArgs a{};
+        a.n = n;
+        a.nkeys = 1;
+        a.nvals = 0;
+        a.key[0] = vdf::SegCol{c->ws + o_s, key.dtype};
+        a.key_out[0] = o_u ? c->ws + o_u : nullptr;
+        a.group_start = reinterpret_cast<uint32_t*>(c->ws + o_g);
+        a.row_group = o_rg ? reinterpret_cast<uint32_t*>(c->ws + o_rg) : nullptr;
+        a.n_groups = reinterpret_cast<uint64_t*>(c->ws + o_n);
+        a.err = err_word(c);
+        int launched = 0;
+        cudaError_t ee = vdf::run_segreduce(a, c->ws + o_tail, s, prof_of(c), &launched);
+        c->launches += launched;
+        return ee == cudaSuccess ? VDF_OK : from_cuda(c, ee, "distinct keys");
+    };
+    if ((st = sort_side(nr, right_key, o_perm, o_sk, o_uk, o_gs, o_ng, 0)) != VDF_OK) return st;
+    if (aligned && (st = sort_side(nl, left_key, o_lperm, o_lsk, 0, o_lgs, o_lng, o_lrg)) != VDF_OK) return st;
+    const uint32_t* perm_r = reinterpret_cast<const uint32_t*>(c->ws + o_perm);
+    const uint32_t* gs_r = reinterpret_cast<const uint32_t*>(c->ws + o_gs);
+    const uint64_t* ng_r = reinterpret_cast<const uint64_t*>(c->ws + o_ng);
+    e = vdf::run_join_build(c->ws + o_uk, w, gs_r, ng_r, perm_r, nr, method, c->ws + o_tail, err_word(c), s);
+    if (e == cudaSuccess) {
+        if (aligned)
+            e = vdf::run_join_probe_aligned(c->ws + o_lsk, w, reinterpret_cast<const uint32_t*>(c->ws + o_lperm),
+                                            reinterpret_cast<const uint32_t*>(c->ws + o_lrg),
+                                            reinterpret_cast<const uint32_t*>(c->ws + o_lgs), nl, c->ws + o_tail, gs_r,
+                                            ng_r, perm_r, nr, match_out, reinterpret_cast<unsigned long long*>(cnt),
+                                            err_word(c), s);
+        else
+            e = vdf::run_join_probe(left_key.data, nl, w, c->ws + o_tail, nr, match_out,
+                                    reinterpret_cast<unsigned long long*>(cnt), s);
+    }
     c->launches += 2;
-    if (e != cudaSuccess) return from_cuda(c, e, "join probe");
+    if (e != cudaSuccess) return from_cuda(c, e, "join");
     return read_count(c, cnt, n_matched_host, s, "read match count");
 }
 
@@ -1027,11 +1059,11 @@ vdf_status vdf_unique(vdf_ctx* c, uint64_t n, vdf_col key, int keep_last, uint8_
 }
 
 vdf_status vdf_left_join_index(vdf_ctx* c, uint64_t n_left, vdf_col left_key, uint64_t n_right,
-                               vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched_dev,
+                               vdf_col right_key, int method, uint32_t* match_out, uint64_t* n_matched_dev,
                                uint64_t* n_matched_host, void* stream) {
     if (!c) return VDF_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
-    return left_join_locked(c, n_left, left_key, n_right, right_key, take_last, match_out, n_matched_dev,
+    return left_join_locked(c, n_left, left_key, n_right, right_key, method, match_out, n_matched_dev,
                             n_matched_host, stream);
 }
 
@@ -1066,7 +1098,7 @@ vdf_status vdf_unique_host(vdf_ctx* c, uint64_t n, vdf_col key, int keep_last, u
 }
 
 vdf_status vdf_left_join_index_host(vdf_ctx* c, uint64_t n_left, vdf_col left_key, uint64_t n_right,
-                                    vdf_col right_key, int take_last, uint32_t* match_out, uint64_t* n_matched,
+                                    vdf_col right_key, int method, uint32_t* match_out, uint64_t* n_matched,
                                     void* stream) {
     if (!c) return VDF_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
@@ -1090,7 +1122,7 @@ vdf_status vdf_left_join_index_host(vdf_ctx* c, uint64_t n_left, vdf_col left_ke
     uint64_t cnt = 0;
     uint32_t* m_dev = reinterpret_cast<uint32_t*>(c->io + o_m);
     if ((st = left_join_locked(c, n_left, vdf_col{c->io + o_l, left_key.dtype}, n_right,
-                               vdf_col{c->io + o_r, right_key.dtype}, take_last, m_dev, nullptr, &cnt, stream)) !=
+                               vdf_col{c->io + o_r, right_key.dtype}, method, m_dev, nullptr, &cnt, stream)) !=
         VDF_OK)
         return st;
     if (n_left) e = cudaMemcpyAsync(match_out, m_dev, 4 * n_left, cudaMemcpyDeviceToHost, s);

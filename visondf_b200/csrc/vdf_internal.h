@@ -237,15 +237,23 @@ size_t unique_workspace_bytes(uint64_t n);
 cudaError_t run_unique_mark(const void* sorted_keys, int width, const uint32_t* perm, uint64_t n, int last,
                             uint8_t* keep, unsigned long long* count, uint32_t* bits, uint32_t* err,
                             cudaStream_t s);
-// match[i] = the right row of left row i's key (first or last of its run in
-// the right side's stable sort), or UINT32_MAX: the right side's distinct
-// sorted keys ukeys[0 .. *n_groups), whose runs start at gstart[g], go into
-// a hash table (table_ws: join_workspace_bytes(n_right)) that each left key
-// is looked up in; *matched += matched rows.
+// Left-join matching (method 0 First, 1 Last, 2 Aligned).  The right side's
+// distinct sorted keys ukeys[0 .. *n_groups), whose runs start at gstart[g],
+// go into a hash table (table_ws: join_workspace_bytes(n_right)) holding the
+// row of each key's first / last occurrence, or (Aligned) its run index.
 size_t join_workspace_bytes(uint64_t n_right);
-cudaError_t run_join_probe(const void* left, uint64_t n_left, int dtype, const void* ukeys, const uint32_t* gstart,
-                           const uint64_t* n_groups, const uint32_t* perm_right, uint64_t n_right, int last,
-                           uint32_t* match, unsigned long long* matched, void* table_ws, uint32_t* err,
+cudaError_t run_join_build(const void* ukeys, int width, const uint32_t* gstart, const uint64_t* n_groups,
+                           const uint32_t* perm_right, uint64_t n_right, int method, void* table_ws, uint32_t* err,
                            cudaStream_t s);
+// First / Last: match[i] = the table's row for left[i], or UINT32_MAX.
+cudaError_t run_join_probe(const void* left, uint64_t n_left, int width, const void* table_ws, uint64_t n_right,
+                           uint32_t* match, unsigned long long* matched, cudaStream_t s);
+// Aligned: over the left side's stable sort (permutation, run of each sorted
+// row, run starts), occurrence r of a key takes the right run's row r.
+cudaError_t run_join_probe_aligned(const void* sorted_left, int width, const uint32_t* perm_left,
+                                   const uint32_t* group_left, const uint32_t* gstart_left, uint64_t n_left,
+                                   const void* table_ws, const uint32_t* gstart_right, const uint64_t* n_groups_right,
+                                   const uint32_t* perm_right, uint64_t n_right, uint32_t* match,
+                                   unsigned long long* matched, uint32_t* err, cudaStream_t s);
 
 }  // namespace vdf

@@ -109,20 +109,22 @@ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
     return x;
 }
 
+// method 0 / 1: the slot holds the row of the key's first / last occurrence;
+// method 2 (aligned): it holds the key's run index g.
 template <typename T>
 __global__ void __launch_bounds__(256) k_join_build(const T* __restrict__ ukeys, const uint32_t* __restrict__ gstart,
                                                      const uint64_t* n_groups, const uint32_t* __restrict__ perm_r,
-                                                     uint64_t n_right, int last, JoinSlot* table, uint64_t mask,
+                                                     uint64_t n_right, int method, JoinSlot* table, uint64_t mask,
                                                      uint32_t* err) {
     const uint64_t G = *n_groups;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; g < G; g += stride) {
-        const uint64_t pos = last ? (g + 1 < G ? (uint64_t)gstart[g + 1] - 1 : n_right - 1) : gstart[g];
+        const uint64_t pos = method == 1 ? (g + 1 < G ? (uint64_t)gstart[g + 1] - 1 : n_right - 1) : gstart[g];
         if (pos >= n_right) {
             atomicOr(err, ERR_BAD_INDEX);
             continue;
         }
-        const uint32_t row1 = perm_r[pos] + 1u;
+        const uint32_t row1 = (method == 2 ? (uint32_t)g : perm_r[pos]) + 1u;
         const unsigned long long key = (unsigned long long)ukeys[g];
         uint64_t s = mix64(key) & mask;
         bool placed = false;
@@ -166,6 +168,49 @@ __global__ void __launch_bounds__(256) k_join_probe(const T* __restrict__ left, 
     add_count(matched, found);
 }
 
+// Aligned matching over the left side's stable sort: sorted left row i is
+// occurrence r = i - (start of its run) of its key; it takes the right row
+// at position r of that key's run in the right side's sort, if the run is
+// long enough.  Results are scattered back through the left permutation.
+template <typename T>
+__global__ void __launch_bounds__(256) k_join_probe_aligned(
+    const T* __restrict__ sorted_l, const uint32_t* __restrict__ perm_l, const uint32_t* __restrict__ group_l,
+    const uint32_t* __restrict__ gstart_l, uint64_t n_left, const JoinSlot* __restrict__ table, uint64_t mask,
+    const uint32_t* __restrict__ gstart_r, const uint64_t* n_groups_r, const uint32_t* __restrict__ perm_r,
+    uint64_t n_right, uint32_t* __restrict__ match, unsigned long long* matched, uint32_t* err) {
+    const uint64_t Gr = *n_groups_r;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    uint32_t found = 0;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n_left; base += stride) {
+        const uint64_t i = base + threadIdx.x;
+        if (i >= n_left) continue;
+        const unsigned long long x = (unsigned long long)sorted_l[i];
+        const uint32_t rank = (uint32_t)i - gstart_l[group_l[i]];
+        uint64_t s = mix64(x) & mask;
+        uint32_t m = 0xffffffffu;
+        for (uint64_t t = 0; t <= mask; ++t) {
+            const ulonglong2 v = ld_rand16(reinterpret_cast<const ulonglong2*>(table + s));
+            const uint32_t g1 = (uint32_t)v.y;
+            if (g1 == 0u) break;
+            if (v.x == x) {
+                const uint64_t g = g1 - 1u;
+                const uint64_t start = g < Gr ? gstart_r[g] : n_right;
+                const uint64_t end = g + 1 < Gr ? gstart_r[g + 1] : n_right;
+                if (start + rank < end) {
+                    m = perm_r[start + rank];
+                    ++found;
+                }
+                break;
+            }
+            s = (s + 1) & mask;
+        }
+        const uint32_t r = perm_l[i];
+        if (r >= n_left) atomicOr(err, ERR_BAD_INDEX);
+        else match[r] = m;
+    }
+    add_count(matched, found);
+}
+
 }  // namespace
 
 size_t unique_workspace_bytes(uint64_t n) { return ((n + 31) / 32) * 4; }
@@ -195,32 +240,56 @@ uint64_t join_table_slots(uint64_t n_right) {
 }
 size_t join_workspace_bytes(uint64_t n_right) { return join_table_slots(n_right) * sizeof(JoinSlot); }
 
-cudaError_t run_join_probe(const void* left, uint64_t n_left, int dtype, const void* ukeys, const uint32_t* gstart,
-                           const uint64_t* n_groups, const uint32_t* perm_right, uint64_t n_right, int last,
-                           uint32_t* match, unsigned long long* matched, void* table_ws, uint32_t* err,
+cudaError_t run_join_build(const void* ukeys, int width, const uint32_t* gstart, const uint64_t* n_groups,
+                           const uint32_t* perm_right, uint64_t n_right, int method, void* table_ws, uint32_t* err,
                            cudaStream_t s) {
-    if (n_left == 0) return cudaSuccess;
     const uint64_t slots = join_table_slots(n_right);
     JoinSlot* table = static_cast<JoinSlot*>(table_ws);
     cudaError_t e = cudaMemsetAsync(table, 0, slots * sizeof(JoinSlot), s);
-    if (e != cudaSuccess) return e;
-    const bool w8 = dtype_width(dtype) == 8;
-    if (w8)
+    if (e != cudaSuccess || n_right == 0) return e;
+    if (width == 8)
         k_join_build<unsigned long long><<<grid_size(n_right), 256, 0, s>>>(
-            static_cast<const unsigned long long*>(ukeys), gstart, n_groups, perm_right, n_right, last, table,
+            static_cast<const unsigned long long*>(ukeys), gstart, n_groups, perm_right, n_right, method, table,
             slots - 1, err);
     else
         k_join_build<uint32_t><<<grid_size(n_right), 256, 0, s>>>(static_cast<const uint32_t*>(ukeys), gstart,
-                                                                   n_groups, perm_right, n_right, last, table,
+                                                                   n_groups, perm_right, n_right, method, table,
                                                                    slots - 1, err);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaGetLastError();
+}
+
+cudaError_t run_join_probe(const void* left, uint64_t n_left, int width, const void* table_ws, uint64_t n_right,
+                           uint32_t* match, unsigned long long* matched, cudaStream_t s) {
+    if (n_left == 0) return cudaSuccess;
+    const uint64_t mask = join_table_slots(n_right) - 1;
+    const JoinSlot* table = static_cast<const JoinSlot*>(table_ws);
     const uint32_t grid = grid_size(n_left);
-    if (w8)
+    if (width == 8)
         k_join_probe<unsigned long long><<<grid, 256, 0, s>>>(static_cast<const unsigned long long*>(left), n_left,
-                                                              table, slots - 1, match, matched);
+                                                              table, mask, match, matched);
     else
-        k_join_probe<uint32_t><<<grid, 256, 0, s>>>(static_cast<const uint32_t*>(left), n_left, table, slots - 1,
-                                                    match, matched);
+        k_join_probe<uint32_t><<<grid, 256, 0, s>>>(static_cast<const uint32_t*>(left), n_left, table, mask, match,
+                                                    matched);
+    return cudaGetLastError();
+}
+
+cudaError_t run_join_probe_aligned(const void* sorted_left, int width, const uint32_t* perm_left,
+                                   const uint32_t* group_left, const uint32_t* gstart_left, uint64_t n_left,
+                                   const void* table_ws, const uint32_t* gstart_right, const uint64_t* n_groups_right,
+                                   const uint32_t* perm_right, uint64_t n_right, uint32_t* match,
+                                   unsigned long long* matched, uint32_t* err, cudaStream_t s) {
+    if (n_left == 0) return cudaSuccess;
+    const uint64_t mask = join_table_slots(n_right) - 1;
+    const JoinSlot* table = static_cast<const JoinSlot*>(table_ws);
+    const uint32_t grid = grid_size(n_left);
+    if (width == 8)
+        k_join_probe_aligned<unsigned long long><<<grid, 256, 0, s>>>(
+            static_cast<const unsigned long long*>(sorted_left), perm_left, group_left, gstart_left, n_left, table,
+            mask, gstart_right, n_groups_right, perm_right, n_right, match, matched, err);
+    else
+        k_join_probe_aligned<uint32_t><<<grid, 256, 0, s>>>(
+            static_cast<const uint32_t*>(sorted_left), perm_left, group_left, gstart_left, n_left, table, mask,
+            gstart_right, n_groups_right, perm_right, n_right, match, matched, err);
     return cudaGetLastError();
 }
 
