@@ -979,11 +979,9 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
         if (w < wsub) pre = agg_combine(pre, s_wtot[sub * kWarpsPerSub + w], vc);
     pre = agg_combine(pre, lx, vc);
 
-    // walk this thread's rows (rolled, over a shift register): a head
-    // completes the group before it
-    uint64_t val[ITEMS][NV > 0 ? NV : 1];
-#pragma unroll
-    for (int v = 0; v < NV; ++v) load_vals<ITEMS>(a.val[v].src, a.val[v].dtype, row0, n, val, v);
+    // walk this thread's rows (rolled; each row's values read again, from L1
+    // after the fold above brought them in): a head completes the group
+    // before it
     uint32_t gid = pre.heads;
     uint32_t cnt = pre.cnt;
     uint64_t w[NV > 0 ? NV : 1][4];
@@ -991,11 +989,13 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[v][q] = pre.w[v][q];
-    uint32_t rg[ITEMS];
     const int upto = (int)nvalid;
 #pragma unroll 1
     for (int j = 0; j < upto; ++j) {
         const uint64_t r = row0 + j;
+        uint64_t x[NV > 0 ? NV : 1];
+#pragma unroll
+        for (int v = 0; v < NV; ++v) x[v] = load_val(a.val[v].src, a.val[v].dtype, r);
         if ((hmask >> j) & 1u) {
             if (gid > 0) emit_group<NV>(a, gid - 1, cnt, w, vc);
 #pragma unroll
@@ -1005,39 +1005,21 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
             ++gid;
             cnt = 1;
 #pragma unroll
-            for (int v = 0; v < NV; ++v) col_init(w[v], val[0][v], vc[v]);
+            for (int v = 0; v < NV; ++v) col_init(w[v], x[v], vc[v]);
         } else {
             ++cnt;
 #pragma unroll
             for (int v = 0; v < NV; ++v) {
                 uint64_t one[4];
-                col_init(one, val[0][v], vc[v]);
+                col_init(one, x[v], vc[v]);
                 col_merge(w[v], one, vc[v]);
             }
         }
-#pragma unroll
-        for (int i = 0; i + 1 < ITEMS; ++i) {
-            rg[i] = rg[i + 1];
-#pragma unroll
-            for (int v = 0; v < NV; ++v) val[i][v] = val[i + 1][v];
-        }
-        rg[ITEMS - 1] = gid - 1;
+        if (a.row_group) a.row_group[r] = gid - 1;
     }
     if (row0 + upto == n) {  // this thread holds the last row: its group ends there
         emit_group<NV>(a, gid - 1, cnt, w, vc);
         if (a.n_groups) *a.n_groups = gid;
-    }
-    if (a.row_group) {
-        // after upto shifts the row groups sit in rg[ITEMS - upto ..]
-        if (upto == ITEMS && (reinterpret_cast<uintptr_t>(a.row_group + row0) & 15) == 0) {
-            uint4* d = reinterpret_cast<uint4*>(a.row_group + row0);
-            d[0] = make_uint4(rg[0], rg[1], rg[2], rg[3]);
-            d[1] = make_uint4(rg[4], rg[5], rg[6], rg[7]);
-        } else {
-#pragma unroll
-            for (int j = 0; j < ITEMS; ++j)
-                if (j >= ITEMS - upto) a.row_group[row0 + j - (ITEMS - upto)] = rg[j];
-        }
     }
 }
 
