@@ -135,7 +135,8 @@ vdf_status vdf_ctx_profile_reset(vdf_ctx* ctx);
 /* ---- tuning (the autotuner's search space) --------------------------------- */
 /* The radix pass is compiled in several variants (key width, threads per
  * CTA, keys per thread, digit bits, warp digit-match method: 0 = ballots,
- * 1 = match.any, 2 = both, alternating by item).  A context uses one variant per key width.  The reference
+ * 1 = match.any, 2 = both, alternating by item, 3 = shared-memory words
+ * the lanes OR their bits into).  A context uses one variant per key width.  The reference
  * fixes its digit width at 16 bits (RADIX_KI16, radix_sorts/details/
  * constants.inl:4) and has no tuning; the digit width, tile size and match
  * method here are chosen per size class by visondf_b200/autotune.py. */

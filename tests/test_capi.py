@@ -82,7 +82,7 @@ def test_variant_table_is_consistent():
     vs = _lib.sort_variants()
     assert vs and {v["key_width"] for v in vs} == {4, 8}
     for v in vs:
-        assert v["threads"] % 32 == 0 and v["items"] > 0 and v["digit_bits"] in (8, 11) and v["match"] in (0, 1, 2)
+        assert v["threads"] % 32 == 0 and v["items"] > 0 and v["digit_bits"] in (8, 11) and v["match"] in (0, 1, 2, 3)
     assert vdf.lib.vdf_sort_variant_info(len(vs), None, None, None, None, None) == _lib.ERR_INVALID_ARG
 
 

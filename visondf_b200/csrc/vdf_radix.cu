@@ -205,7 +205,7 @@ __device__ __forceinline__ uint32_t digit_of(K key, uint32_t shift) {
     }
 }
 
-template <typename K, int BITS, int THREADS, int ITEMS>
+template <typename K, int BITS, int THREADS, int ITEMS, int MATCH = 0>
 struct OnesweepCfg {
     static constexpr int RADIX = 1 << BITS;
     static constexpr int WARPS = THREADS / 32;
@@ -216,12 +216,17 @@ struct OnesweepCfg {
     static constexpr size_t VAL_BYTES = (size_t)TILE * 4;
     static constexpr size_t CNT_BYTES = (size_t)WARPS * RADIX * 4;
     static constexpr size_t GLOB_BYTES = (size_t)RADIX * 4;
-    static constexpr size_t SMEM = KEY_BYTES + VAL_BYTES + CNT_BYTES + GLOB_BYTES + 64 + WARPS * 4;
+    // match method 3: two per-warp words per digit, the lanes holding it
+    static constexpr size_t MASK_BYTES = MATCH == 3 ? (size_t)2 * WARPS * RADIX * 4 : 0;
+    static constexpr size_t SMEM = KEY_BYTES + VAL_BYTES + CNT_BYTES + GLOB_BYTES + 64 + WARPS * 4 + MASK_BYTES;
 };
 
 // MATCH selects how a warp finds the lanes holding the same digit:
 // 0 = one ballot per digit bit (ALU/vote pipes), 1 = match.any (XU pipe),
-// 2 = alternate the two by item, so both pipes work at once.
+// 2 = alternate the two by item, so both pipes work at once, 3 = each lane
+// ORs its bit into a per-warp shared-memory word of its digit and reads the
+// word back (two words per digit, alternating by item, so a word is cleared
+// well before it is used again).
 // MINB: CTAs per SM the register allocation is sized for.
 // SEG: segmented sort of many independent row ranges (the queries of a
 // batch) in one launch.  Tiles never straddle a segment; a tile's bin bases
@@ -231,7 +236,7 @@ struct OnesweepCfg {
 template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL, int MATCH, int MINB,
           bool SEG = false>
 __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
-    using C = OnesweepCfg<K, BITS, THREADS, ITEMS>;
+    using C = OnesweepCfg<K, BITS, THREADS, ITEMS, MATCH>;
     constexpr int RADIX = C::RADIX, WARPS = C::WARPS, TILE = C::TILE, BPT = C::BPT;
     extern __shared__ __align__(16) unsigned char smem[];
     K* ex_keys = reinterpret_cast<K*>(smem);
@@ -240,10 +245,13 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     uint32_t* bglob = wcnt + WARPS * RADIX;                                            // [RADIX]
     uint32_t* misc = bglob + RADIX;                                                    // [0]=tile
     uint32_t* wsum = misc + 16;                                                        // [WARPS]
+    uint32_t* wmask = wsum + WARPS;  // match method 3: [2][WARPS][RADIX]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) misc[0] = atomicAdd(a.tile_counter, 1u);
     for (int i = tid; i < WARPS * RADIX; i += THREADS) wcnt[i] = 0;
+    if constexpr (MATCH == 3)
+        for (int i = tid; i < 2 * WARPS * RADIX; i += THREADS) wmask[i] = 0;
     __syncthreads();
     const uint32_t tile = misc[0];
     const uint64_t n = a.n;
@@ -346,7 +354,15 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     for (int j = 0; j < ITEMS; ++j) {
         const uint32_t d = digit_of<K, BITS>(key[j], a.shift);
         if constexpr (PACKED) dpk[j / 4] |= d << (8 * (j % 4));
-        if (MATCH == 1 || (MATCH == 2 && (j & 1) == 0)) {
+        if constexpr (MATCH == 3) {
+            uint32_t* word = wmask + ((j & 1) * WARPS + warp) * RADIX + d;
+            atomicOr(word, 1u << lane);
+            __syncwarp();
+            const uint32_t pm = *word;
+            __syncwarp();  // every peer has read the word before its leader clears it
+            if (lane == __ffs(pm) - 1) *word = 0;
+            peers[j] = pm;
+        } else if (MATCH == 1 || (MATCH == 2 && (j & 1) == 0)) {
             peers[j] = __match_any_sync(0xffffffffu, d);
         } else {
             uint32_t pm = 0xffffffffu;
@@ -584,7 +600,7 @@ struct PassVariant {
 
 template <typename K, int BITS, int THREADS, int ITEMS, int MATCH, int MINB>
 PassVariant make_variant() {
-    using C = OnesweepCfg<K, BITS, THREADS, ITEMS>;
+    using C = OnesweepCfg<K, BITS, THREADS, ITEMS, MATCH>;
     static_assert(BITS <= kMaxBits, "digit wider than the histogram layout allows");
     PassVariant v{};
     v.width = (int)sizeof(K);
@@ -624,6 +640,10 @@ const PassVariant kVariants[] = {
     make_variant<uint64_t, 11, 256, 8, 1, 2>(),   // 15
     make_variant<uint32_t, 11, 256, 16, 2, 2>(),  // 16
     make_variant<uint64_t, 11, 256, 12, 2, 2>(),  // 17
+    // digit match through shared-memory words (match method 3); its cost
+    // grows when many lanes share a digit, so it is the autotuner's pick for
+    // a workload rather than the default
+    make_variant<uint64_t, 8, 256, 12, 3, 3>(),   // 18
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
 
@@ -638,8 +658,8 @@ struct SegVariant {
 };
 template <int BITS, int THREADS, int ITEMS, int MATCH, int MINB>
 SegVariant make_seg_variant() {
-    using C4 = OnesweepCfg<uint32_t, BITS, THREADS, ITEMS>;
-    using C8 = OnesweepCfg<uint64_t, BITS, THREADS, ITEMS>;
+    using C4 = OnesweepCfg<uint32_t, BITS, THREADS, ITEMS, MATCH>;
+    using C8 = OnesweepCfg<uint64_t, BITS, THREADS, ITEMS, MATCH>;
     SegVariant v{};
     v.bits = BITS;
     v.tile = THREADS * ITEMS;
