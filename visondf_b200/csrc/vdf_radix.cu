@@ -292,7 +292,9 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
         val[j] = (uint32_t)i;  // IN_RAW: the row itself
         if (pos < valid) {
             if (IN_MODE == IN_RAW) {
-                key[j] = KeyOps<K>::order(ldg_stream(static_cast<const K*>(a.keys_in) + i), a.dtype, a.invert);
+                const K raw = ldg_stream(static_cast<const K*>(a.keys_in) + i);
+                if constexpr (SEG) key[j] = raw;  // a batch arena already holds order images
+                else key[j] = KeyOps<K>::order(raw, a.dtype, a.invert);
             } else if (IN_MODE == IN_GATHER) {
                 uint32_t src = ldg_stream(a.vals_in + i);
                 if (src >= n) {  // never for a valid permutation
@@ -573,11 +575,17 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
                 atomicOr(a.err, ERR_BAD_INDEX);
                 continue;
             }
-            if (fin && a.reverse) p = (uint32_t)(n - 1) - p;
-            if (fin) {
-                if (kout) stg_stream(kout + p, KeyOps<K>::unorder(k, a.dtype, a.invert));
-            } else {
+            if constexpr (SEG) {
+                // a batch arena holds order images sorted ascending: the final
+                // pass differs from the others only in its output buffers
                 stg_stream(kout + p, k);
+            } else {
+                if (fin && a.reverse) p = (uint32_t)(n - 1) - p;
+                if (fin) {
+                    if (kout) stg_stream(kout + p, KeyOps<K>::unorder(k, a.dtype, a.invert));
+                } else {
+                    stg_stream(kout + p, k);
+                }
             }
             stg_stream(vout + p, v);
         }
