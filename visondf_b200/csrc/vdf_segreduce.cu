@@ -317,6 +317,22 @@ __device__ __forceinline__ Agg<NV> fold_rows(const SegArgs& a, uint64_t row0, co
     return t;
 }
 
+// Value-class patterns fixed at compile time (VCP): 0 = read from the column
+// dtypes at run time; 1 = two columns, float then signed integer (the
+// aggregation every workload here runs).  With the pattern fixed, the
+// per-row merges carry no branches on the class.
+template <int NV, int VCP>
+__device__ __forceinline__ void fix_classes(int* vc) {
+    if constexpr (VCP == 1 && NV == 2) {
+        vc[0] = VC_FLOAT;
+        vc[1] = VC_SINT;
+    }
+}
+inline int value_class_pattern(const SegArgs& a) {
+    auto cls = [](int dt) { return (dt == F64 || dt == F32) ? 0 : (dt == I32 || dt == I64) ? 1 : 2; };
+    return (a.nvals == 2 && cls(a.val[0].dtype) == 0 && cls(a.val[1].dtype) == 1) ? 1 : 0;
+}
+
 template <int NK, int NV>
 __device__ __forceinline__ void seg_setup(const SegArgs& a, int* vc, int* kw) {
 #pragma unroll
@@ -456,7 +472,7 @@ constexpr int kWideItems = 8;
 constexpr int kSubTiles = kSegThreads * kWideItems / kSegTile;  // 4
 constexpr int kWarpsPerSub = kSegThreads / 32 / kSubTiles;      // 2
 
-template <int NK, int NV>
+template <int NK, int NV, int VCP = 0>
 __global__ void __launch_bounds__(kSegThreads) k_seg_tiles_wide(SegArgs a, Agg<NV>* tile_agg, uint32_t tiles) {
     constexpr int ITEMS = kWideItems, WARPS = kSegThreads / 32;
     __shared__ Agg<NV> s_warp[WARPS];
@@ -470,6 +486,7 @@ __global__ void __launch_bounds__(kSegThreads) k_seg_tiles_wide(SegArgs a, Agg<N
     const uint64_t row0 = (uint64_t)tile * kSegTile + (uint64_t)sub_tid * ITEMS;
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
+    fix_classes<NV, VCP>(vc);
 
     uint64_t key[ITEMS][NK];
 #pragma unroll
@@ -850,7 +867,7 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : (NV == 2 ? 4 : 3))
 // consecutive: its groups complete in order and are written as they
 // complete.  Tiles where every row starts a group take the one-row-record
 // path with coalesced writes.
-template <int NK, int NV>
+template <int NK, int NV, int VCP = 0>
 __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     k_seg_emit_wide(SegArgs a, const Agg<NV>* tile_prefix, const Agg<NV>* block_prefix, uint32_t tiles) {
     constexpr int ITEMS = kWideItems, WARPS = kSegThreads / 32;
@@ -866,6 +883,7 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     const uint64_t row0 = (uint64_t)tile * kSegTile + (uint64_t)sub_tid * ITEMS;
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
+    fix_classes<NV, VCP>(vc);
     // heads before the tile, loaded first so that its latency overlaps the key loads
     const uint32_t H_tile = tvalid ? block_prefix[tile / kScanTiles].heads + tile_prefix[tile].heads : 0u;
 
@@ -1030,7 +1048,11 @@ cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaS
     Agg<NV>* bt = ta + tiles;
     if (prof) prof->begin(KC_SEGREDUCE, s);
     const uint32_t grid = (tiles + kSegTilesPerCta - 1) / kSegTilesPerCta;
-    k_seg_tiles_wide<NK, NV><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, tiles);
+    const bool fixed = value_class_pattern(a) == 1;
+    if (fixed)
+        k_seg_tiles_wide<NK, NV, 1><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, tiles);
+    else
+        k_seg_tiles_wide<NK, NV, 0><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, tiles);
     if (prof) prof->end(KC_SEGREDUCE, s);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1041,7 +1063,12 @@ cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaS
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (prof) prof->begin(KC_SEGEMIT, s);
     if constexpr (NV <= 2)
-        k_seg_emit_wide<NK, NV><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+    {
+        if (fixed)
+            k_seg_emit_wide<NK, NV, 1><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+        else
+            k_seg_emit_wide<NK, NV, 0><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+    }
     else
         k_seg_emit<NK, NV><<<grid, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta, bt, tiles);
     if (prof) prof->end(KC_SEGEMIT, s);
