@@ -328,6 +328,20 @@ __device__ __forceinline__ void fix_classes(int* vc) {
         vc[1] = VC_SINT;
     }
 }
+// Key-width patterns fixed at compile time (KWP): 0 = run time; otherwise
+// key k is (KWP >> 4k) & 15 bytes wide (two keys: 0x48 = 8 then 4 bytes).
+template <int NK, int KWP>
+__device__ __forceinline__ void fix_widths(int* kw) {
+    if constexpr (KWP != 0) {
+#pragma unroll
+        for (int k = 0; k < NK; ++k) kw[k] = (KWP >> (4 * k)) & 15;
+    }
+}
+inline int key_width_pattern(const SegArgs& a) {
+    int p = 0;
+    for (int k = 0; k < a.nkeys; ++k) p |= (dtype_width(a.key[k].dtype) & 15) << (4 * k);
+    return p;
+}
 inline int value_class_pattern(const SegArgs& a) {
     auto cls = [](int dt) { return (dt == F64 || dt == F32) ? 0 : (dt == I32 || dt == I64) ? 1 : 2; };
     return (a.nvals == 2 && cls(a.val[0].dtype) == 0 && cls(a.val[1].dtype) == 1) ? 1 : 0;
@@ -472,7 +486,7 @@ constexpr int kWideItems = 8;
 constexpr int kSubTiles = kSegThreads * kWideItems / kSegTile;  // 4
 constexpr int kWarpsPerSub = kSegThreads / 32 / kSubTiles;      // 2
 
-template <int NK, int NV, int VCP = 0>
+template <int NK, int NV, int VCP = 0, int KWP = 0>
 __global__ void __launch_bounds__(kSegThreads) k_seg_tiles_wide(SegArgs a, Agg<NV>* tile_agg, uint32_t tiles) {
     constexpr int ITEMS = kWideItems, WARPS = kSegThreads / 32;
     __shared__ Agg<NV> s_warp[WARPS];
@@ -487,6 +501,7 @@ __global__ void __launch_bounds__(kSegThreads) k_seg_tiles_wide(SegArgs a, Agg<N
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
     fix_classes<NV, VCP>(vc);
+    fix_widths<NK, KWP>(kw);
 
     uint64_t key[ITEMS][NK];
 #pragma unroll
@@ -867,7 +882,7 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : (NV == 2 ? 4 : 3))
 // consecutive: its groups complete in order and are written as they
 // complete.  Tiles where every row starts a group take the one-row-record
 // path with coalesced writes.
-template <int NK, int NV, int VCP = 0>
+template <int NK, int NV, int VCP = 0, int KWP = 0>
 __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     k_seg_emit_wide(SegArgs a, const Agg<NV>* tile_prefix, const Agg<NV>* block_prefix, uint32_t tiles) {
     constexpr int ITEMS = kWideItems, WARPS = kSegThreads / 32;
@@ -884,6 +899,7 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     int vc[NV > 0 ? NV : 1], kw[NK];
     seg_setup<NK, NV>(a, vc, kw);
     fix_classes<NV, VCP>(vc);
+    fix_widths<NK, KWP>(kw);
     // heads before the tile, loaded first so that its latency overlaps the key loads
     const uint32_t H_tile = tvalid ? block_prefix[tile / kScanTiles].heads + tile_prefix[tile].heads : 0u;
 
@@ -1048,11 +1064,31 @@ cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaS
     Agg<NV>* bt = ta + tiles;
     if (prof) prof->begin(KC_SEGREDUCE, s);
     const uint32_t grid = (tiles + kSegTilesPerCta - 1) / kSegTilesPerCta;
-    const bool fixed = value_class_pattern(a) == 1;
-    if (fixed)
-        k_seg_tiles_wide<NK, NV, 1><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, tiles);
-    else
-        k_seg_tiles_wide<NK, NV, 0><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, tiles);
+    // the float + signed-integer value pair with two keys of fixed widths
+    // (8+4, 4+8, 4+4 bytes) gets fully specialised kernels
+    const bool fixed = NV == 2 && value_class_pattern(a) == 1;
+    const int kwp = (fixed && NK == 2) ? key_width_pattern(a) : 0;
+    const uint32_t wide_grid = (tiles + kSubTiles - 1) / kSubTiles;
+    bool launched_tiles = false;
+    if constexpr (NK == 2 && NV == 2) {
+        launched_tiles = true;
+        if (kwp == 0x48)
+            k_seg_tiles_wide<NK, NV, 1, 0x48><<<wide_grid, kSegThreads, 0, s>>>(a, ta, tiles);
+        else if (kwp == 0x84)
+            k_seg_tiles_wide<NK, NV, 1, 0x84><<<wide_grid, kSegThreads, 0, s>>>(a, ta, tiles);
+        else if (kwp == 0x44)
+            k_seg_tiles_wide<NK, NV, 1, 0x44><<<wide_grid, kSegThreads, 0, s>>>(a, ta, tiles);
+        else
+            launched_tiles = false;
+    }
+    if (!launched_tiles) {
+        if constexpr (NV == 2) {
+            if (fixed) k_seg_tiles_wide<NK, NV, 1><<<wide_grid, kSegThreads, 0, s>>>(a, ta, tiles);
+            else k_seg_tiles_wide<NK, NV, 0><<<wide_grid, kSegThreads, 0, s>>>(a, ta, tiles);
+        } else {
+            k_seg_tiles_wide<NK, NV, 0><<<wide_grid, kSegThreads, 0, s>>>(a, ta, tiles);
+        }
+    }
     if (prof) prof->end(KC_SEGREDUCE, s);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
@@ -1064,10 +1100,26 @@ cudaError_t seg_run(const SegArgs& a, unsigned char* aggs, uint32_t tiles, cudaS
     if (prof) prof->begin(KC_SEGEMIT, s);
     if constexpr (NV <= 2)
     {
-        if (fixed)
-            k_seg_emit_wide<NK, NV, 1><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, bt, tiles);
-        else
-            k_seg_emit_wide<NK, NV, 0><<<(tiles + kSubTiles - 1) / kSubTiles, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+        bool launched_emit = false;
+        if constexpr (NK == 2 && NV == 2) {
+            launched_emit = true;
+            if (kwp == 0x48)
+                k_seg_emit_wide<NK, NV, 1, 0x48><<<wide_grid, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+            else if (kwp == 0x84)
+                k_seg_emit_wide<NK, NV, 1, 0x84><<<wide_grid, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+            else if (kwp == 0x44)
+                k_seg_emit_wide<NK, NV, 1, 0x44><<<wide_grid, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+            else
+                launched_emit = false;
+        }
+        if (!launched_emit) {
+            if constexpr (NV == 2) {
+                if (fixed) k_seg_emit_wide<NK, NV, 1><<<wide_grid, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+                else k_seg_emit_wide<NK, NV, 0><<<wide_grid, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+            } else {
+                k_seg_emit_wide<NK, NV, 0><<<wide_grid, kSegThreads, 0, s>>>(a, ta, bt, tiles);
+            }
+        }
     }
     else
         k_seg_emit<NK, NV><<<grid, kSegThreads, emit_smem_bytes<NK, NV>(), s>>>(a, ta, bt, tiles);
