@@ -281,6 +281,8 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
 
     // ---- load keys and row ids (warp-striped: item j of lane l is tile
     //      position warp*ITEMS*32 + j*32 + l, so positions follow row order) --
+    // Every load of the tile is issued before any key is transformed (a
+    // transform between loads keeps the compiler from overlapping them).
     K key[ITEMS];
     uint32_t val[ITEMS];
     const uint32_t wpos = (uint32_t)warp * ITEMS * 32;
@@ -292,9 +294,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
         val[j] = (uint32_t)i;  // IN_RAW: the row itself
         if (pos < valid) {
             if (IN_MODE == IN_RAW) {
-                const K raw = ldg_stream(static_cast<const K*>(a.keys_in) + i);
-                if constexpr (SEG) key[j] = raw;  // a batch arena already holds order images
-                else key[j] = KeyOps<K>::order(raw, a.dtype, a.invert);
+                key[j] = ldg_stream(static_cast<const K*>(a.keys_in) + i);
             } else if (IN_MODE == IN_GATHER) {
                 uint32_t src = ldg_stream(a.vals_in + i);
                 if (src >= n) {  // never for a valid permutation
@@ -302,16 +302,28 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
                     src = 0;
                 }
                 val[j] = src;
-                const K* kp = static_cast<const K*>(a.keys_in) + src;
-                K raw;
-                if constexpr (sizeof(K) == 8) raw = ld_rand8(kp);
-                else raw = ld_rand4(kp);
-                key[j] = KeyOps<K>::order(raw, a.dtype, a.invert);
             } else {
                 key[j] = ldg_stream(static_cast<const K*>(a.keys_in) + i);
                 val[j] = ldg_stream(a.vals_in + i);
             }
         }
+    }
+    if constexpr (IN_MODE == IN_GATHER) {
+        // keys through the current permutation: all random loads, then the transform
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (wpos + j * 32 + lane < valid) {
+                const K* kp = static_cast<const K*>(a.keys_in) + val[j];
+                if constexpr (sizeof(K) == 8) key[j] = ld_rand8(kp);
+                else key[j] = ld_rand4(kp);
+            }
+        }
+    }
+    if constexpr ((IN_MODE == IN_RAW && !SEG) || IN_MODE == IN_GATHER) {
+        // raw keys -> order images (a batch arena already holds images)
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j)
+            if (wpos + j * 32 + lane < valid) key[j] = KeyOps<K>::order(key[j], a.dtype, a.invert);
     }
 
     // Clear this tile's row of the other status buffer for the next pass
