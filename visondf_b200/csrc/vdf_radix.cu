@@ -50,20 +50,36 @@ __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
         const int w = dtype_width(col.dtype);
         const uint32_t bits = FIXED_BITS ? (uint32_t)FIXED_BITS : (uint32_t)col.bits;
         const uint32_t radix = 1u << bits, mask = radix - 1;
+        // four keys per thread per round, all loaded before any is used
+        constexpr int R = 4;
         if (w == 4) {
             const uint32_t* src = static_cast<const uint32_t*>(col.data);
-            for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-                uint32_t k = order32(ldg_stream(src + i), col.dtype, col.invert);
+            for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += R * stride) {
+                uint32_t k[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) k[r] = i0 + r * stride < n ? ldg_stream(src + i0 + r * stride) : 0u;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (i0 + r * stride >= n) break;
+                    const uint32_t x = order32(k[r], col.dtype, col.invert);
 #pragma unroll 4
-                for (int p = 0; p < col.passes; ++p) atomicAdd(&h[p * radix + ((k >> (p * bits)) & mask)], 1u);
+                    for (int p = 0; p < col.passes; ++p) atomicAdd(&h[p * radix + ((x >> (p * bits)) & mask)], 1u);
+                }
             }
         } else {
             const uint64_t* src = static_cast<const uint64_t*>(col.data);
-            for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-                uint64_t k = order64(ldg_stream(src + i), col.dtype, col.invert);
+            for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += R * stride) {
+                uint64_t k[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r) k[r] = i0 + r * stride < n ? ldg_stream(src + i0 + r * stride) : 0ull;
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    if (i0 + r * stride >= n) break;
+                    const uint64_t x = order64(k[r], col.dtype, col.invert);
 #pragma unroll 8
-                for (int p = 0; p < col.passes; ++p)
-                    atomicAdd(&h[p * radix + (uint32_t)((k >> (p * bits)) & mask)], 1u);
+                    for (int p = 0; p < col.passes; ++p)
+                        atomicAdd(&h[p * radix + (uint32_t)((x >> (p * bits)) & mask)], 1u);
+                }
             }
         }
     }
