@@ -151,12 +151,26 @@ __global__ void __launch_bounds__(512) k_seg_hist(SegHistArgs a) {
     if (words > a.stride) return;
     for (uint32_t i = threadIdx.x; i < words; i += blockDim.x) sh_hist[i] = 0;
     __syncthreads();
-    for (uint32_t r = threadIdx.x; r < ch.rows; r += blockDim.x) {
-        const uint64_t k = a.key_width == 8
-                               ? ldg_stream(static_cast<const unsigned long long*>(a.keys) + ch.row_start + r)
-                               : (uint64_t)ldg_stream(static_cast<const uint32_t*>(a.keys) + ch.row_start + r);
-        for (uint32_t p = 0; p < passes; ++p)
-            atomicAdd(&sh_hist[p * radix + (uint32_t)((k >> (p * a.bits)) & mask)], 1u);
+    // four rows per thread per round, all loaded before any is counted
+    constexpr int R = 4;
+    const uint32_t step = blockDim.x;
+    for (uint32_t r0 = threadIdx.x; r0 < ch.rows; r0 += R * step) {
+        uint64_t k[R];
+        if (a.key_width == 8) {
+            const unsigned long long* src = static_cast<const unsigned long long*>(a.keys) + ch.row_start;
+#pragma unroll
+            for (int q = 0; q < R; ++q) k[q] = r0 + q * step < ch.rows ? ldg_stream(src + r0 + q * step) : 0ull;
+        } else {
+            const uint32_t* src = static_cast<const uint32_t*>(a.keys) + ch.row_start;
+#pragma unroll
+            for (int q = 0; q < R; ++q) k[q] = r0 + q * step < ch.rows ? (uint64_t)ldg_stream(src + r0 + q * step) : 0ull;
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            if (r0 + q * step >= ch.rows) break;
+            for (uint32_t p = 0; p < passes; ++p)
+                atomicAdd(&sh_hist[p * radix + (uint32_t)((k[q] >> (p * a.bits)) & mask)], 1u);
+        }
     }
     __syncthreads();
     uint32_t* g = a.hist + (size_t)ch.seg * a.stride;
