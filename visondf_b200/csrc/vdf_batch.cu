@@ -106,16 +106,35 @@ __global__ void __launch_bounds__(256) k_batch_pack(BatchDev b) {
 // Sorted arena row ids -> row ids within each query (in place in perm_out).
 __global__ void __launch_bounds__(256) k_batch_localize(BatchDev b) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < b.n_large; i += stride) {
-        const uint32_t s = b.arena_seg[i];  // the sort keeps every segment in place
-        const uint64_t start = b.segs[s].row_start;
-        uint32_t* p = b.perm_out + b.large_base + i;
-        const uint32_t r = *p;
-        if (r < start || r - start >= b.segs[s].rows) {
-            atomicOr(b.err, ERR_BAD_INDEX);
-            continue;
+    // four rows per thread per round, every load issued before the first use
+    constexpr int R = 4;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < b.n_large; i0 += R * stride) {
+        uint32_t sg[R], rr[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const uint64_t i = i0 + q * stride;
+            sg[q] = 0;
+            rr[q] = 0;
+            if (i < b.n_large) {
+                sg[q] = b.arena_seg[i];  // the sort keeps every segment in place
+                rr[q] = b.perm_out[b.large_base + i];
+            }
         }
-        *p = (uint32_t)(r - start);
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const uint64_t i = i0 + q * stride;
+            if (i >= b.n_large) break;
+            if (sg[q] >= b.nsegs) {
+                atomicOr(b.err, ERR_BAD_INDEX);
+                continue;
+            }
+            const SegDesc d = b.segs[sg[q]];
+            if (rr[q] < d.row_start || rr[q] - d.row_start >= d.rows) {
+                atomicOr(b.err, ERR_BAD_INDEX);
+                continue;
+            }
+            b.perm_out[b.large_base + i] = (uint32_t)(rr[q] - d.row_start);
+        }
     }
 }
 
