@@ -1046,8 +1046,20 @@ template <typename T>
 __global__ void __launch_bounds__(256) k_adjacent_ties(const T* keys, uint64_t n, uint32_t* flag) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     bool eq = false;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i < n; i += stride)
-        eq = eq || (__ldg(keys + i) == __ldg(keys + i - 1));
+    // four rows per thread per round, all loads issued first (the previous
+    // row's key comes from the neighbouring lane's load, an L1 hit)
+    constexpr int R = 4;
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x + 1; i0 < n; i0 += R * stride) {
+        T cur[R], prev[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+            const uint64_t i = i0 + q * stride;
+            cur[q] = i < n ? __ldg(keys + i) : T(0);
+            prev[q] = i < n ? __ldg(keys + i - 1) : T(0);
+        }
+#pragma unroll
+        for (int q = 0; q < R; ++q) eq |= (i0 + q * stride < n) && cur[q] == prev[q];
+    }
     if (__any_sync(0xffffffffu, eq) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
 }
 
