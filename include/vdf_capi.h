@@ -121,7 +121,8 @@ typedef enum vdf_kernel_class {
     VDF_KC_SEGSCAN = 8,     /* group-by: tile prefix scan     */
     VDF_KC_SEGEMIT = 9,     /* group-by: scan + emit groups   */
     VDF_KC_TIES = 10,       /* equal-neighbour check (multi-key) */
-    VDF_KC_BATCH = 11       /* batch bookkeeping: row ids per query, group ranges, group keys */
+    VDF_KC_BATCH = 11,      /* batch bookkeeping: row ids per query, group ranges, group keys */
+    VDF_KC_CSV = 12         /* CSV ingest: record split, field parse, string columns */
 } vdf_kernel_class;
 /* When enabled, every kernel the context launches is bracketed by CUDA
  * events on its stream (no reference counterpart: the reference has no
@@ -380,6 +381,55 @@ vdf_status vdf_unique_host(vdf_ctx* ctx, uint64_t n, vdf_col key, int keep_last,
 vdf_status vdf_left_join_index_host(vdf_ctx* ctx, uint64_t n_left, vdf_col left_key, uint64_t n_right,
                                     vdf_col right_key, int method, uint32_t* match_out, uint64_t* n_matched,
                                     void* stream);
+
+/* ---- CSV ingest -------------------------------------------------------------
+ * Parses a CSV file's bytes into device-resident columns: the reference's
+ * read_csv (V/read/read_csv/read_csv.hpp:3-216, called as Dataframe::readf,
+ * benchmarks/readf.cpp:21) with its single-core parser
+ * (V/inlines/read/read_csv/parsers_core/parse_rows_chunk.inl:1-185) and type
+ * inference (V/inlines/classify_column.inl:13-133):
+ *   - the first line holds the names (header = 1) or the first data row; it
+ *     ends at the first CR or LF even inside quotes (read_csv.hpp:62-69);
+ *   - records end at a CR, LF or CR LF outside quotes; fields split at the
+ *     delimiter outside quotes; the quote byte toggles quoting and stays in
+ *     the field's text; an empty field reads "NA";
+ *   - a record with another field count than the first line is an error
+ *     (VDF_ERR_INVALID_ARG, "column number problem at row r"), where the
+ *     reference prints "column number problem" and stops;
+ *   - each column's type comes from its first 10 values: 'd' (double, the
+ *     first number with a '.' decides), 's' / 'c' (a value that is not digits
+ *     with at most one '.': 's' if it is longer than one byte), 'b' (all "0"
+ *     or "1"), 'u' (unsigned 32-bit);
+ *   - values: 'd' as fast_float::from_chars (correctly rounded; 0 when invalid
+ *     or out of range), 'u' as std::from_chars into unsigned int, 'b' as
+ *     std::from_chars into int != 0 (0 when invalid or out of range); strings
+ *     keep their bytes (offsets + bytes, "NA" for an empty field).
+ * Files must be below 4 GiB.  The table owns its device columns. */
+typedef struct vdf_csv vdf_csv;
+
+/* `bytes`: n bytes in device memory (16-byte aligned).  Synchronises `stream`. */
+vdf_status vdf_csv_read(vdf_ctx* ctx, const void* bytes, uint64_t n, char delim, int header, char quote,
+                        vdf_csv** out, void* stream);
+/* The same for a file's bytes in host memory (copied to the device first). */
+vdf_status vdf_csv_read_host(vdf_ctx* ctx, const void* bytes, uint64_t n, char delim, int header, char quote,
+                             vdf_csv** out, void* stream);
+uint64_t vdf_csv_nrow(const vdf_csv* t);
+uint32_t vdf_csv_ncol(const vdf_csv* t);
+/* Column name ("" without a header; "NA" for an empty header field). */
+const char* vdf_csv_name(const vdf_csv* t, uint32_t col);
+/* 'd' (f64), 'u' (u32), 'b' (u8 0/1), 's' or 'c' (string). */
+char vdf_csv_type(const vdf_csv* t, uint32_t col);
+/* Device pointer to the values (numbers) or the concatenated string bytes. */
+const void* vdf_csv_values(const vdf_csv* t, uint32_t col);
+/* Device pointer to nrow + 1 string offsets (NULL for numbers). */
+const uint64_t* vdf_csv_offsets(const vdf_csv* t, uint32_t col);
+uint64_t vdf_csv_string_bytes(const vdf_csv* t, uint32_t col);
+/* Copies one column into host or device memory: values (nrow elements, or
+ * the string bytes) and, for strings, the nrow + 1 offsets (either may be
+ * NULL).  Synchronises `stream`. */
+vdf_status vdf_csv_copy_column(vdf_ctx* ctx, const vdf_csv* t, uint32_t col, void* values, uint64_t* offsets,
+                               void* stream);
+void vdf_csv_free(vdf_csv* t);
 
 /* ---- batched queries ------------------------------------------------------
  * Many independent sort + group-by queries (each: stable ascending sort of

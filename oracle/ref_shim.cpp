@@ -15,6 +15,18 @@
 // and the vendored hash map / hash used by the reference group-by:
 //   external/ankerl/unordered_dense.h (v4.8.0), custom_simd_hash/simd_hash.hpp.
 //
+// The CSV entry point ref_csv_read() runs the reference's own record parser
+// (inlines/read/read_csv/parsers_core/parse_rows_chunk.inl, its AVX2 path),
+// simd_can_be_nb / has_dot and fast_float::from_chars / std::from_chars; the
+// parts of read_csv that are member code of the (uncompilable) Dataframe
+// class are restated: the first-line pass (read/read_csv/read_csv.hpp:58-135)
+// and classify_column's decision (inlines/classify_column.inl:13-133, whose
+// 'c' branch does not compile), with the per-column conversions run under
+// OpenMP over columns as type_classification does (type_classification.inl:
+// 15-19).  The reference's multi-core parser (standard_parser_mt.inl:30-37)
+// computes every chunk's end row from the first chunk's, so only its
+// single-core parser is usable.
+//
 // The reference group-by itself cannot compile (syntax errors in
 // transform/transform_group_by/*), so ref_groupby() restates its algorithm
 // (transform_group_by_onecol_mt.hpp:182-337: per-thread ankerl maps keyed by
@@ -51,6 +63,15 @@
 
 #include "external/ankerl/unordered_dense.h"
 #include "custom_simd_hash/simd_hash.hpp"
+
+// CSV ingest: the reference's record parser, numeric-shape tests and the
+// vendored fast_float (v8.1.0), compiled from the reference tree.
+#include <charconv>
+#include <chrono>
+#include "external/fast_float/fast_float.h"
+#include "inlines/simd_can_be_nb.inl"
+#include "inlines/has_dot.inl"
+#include "inlines/read/read_csv/parsers_core/parse_rows_chunk.inl"
 
 namespace {
 
@@ -284,5 +305,155 @@ int64_t ref_groupby(const void* const* keys, const int* kdt, int nkeys,
     }
     return int64_t(lookup.size());
 }
+
+
+// CSV: parse `n` bytes as read_csv does and write the oracle's blob layout
+// (see oracle/vdf_oracle_csv.c).  `seconds` (optional): time of the parse,
+// inference and conversions (not the blob).  Malformed records: the
+// reference stops at the first record with fewer fields (bad_row = that
+// record); a record with MORE fields indexes past its column vector, so
+// callers must not pass one.
+void* ref_csv_read(const char* b, size_t n, char delim, int header, char quote, int cores, size_t* blob_bytes,
+                   double* seconds) {
+    const auto t0 = std::chrono::steady_clock::now();
+    std::string_view csv(b, n);
+    std::vector<std::vector<std::string>> cols;
+    std::vector<std::string> names;
+    size_t i = 0, fs = 0;
+    bool inq = false;
+    for (; i < n; ++i) {
+        const char c = b[i];
+        if (c == '\n' || c == '\r') {
+            if (i + 1 < n && b[i + 1] == '\n') ++i;
+            break;
+        }
+        if (c == quote) inq = !inq;
+        else if (c == delim && !inq) {
+            std::string f(b + fs, i - fs);
+            if (header) names.push_back(f.empty() ? "NA" : f);
+            cols.emplace_back();
+            if (!header) cols.back().push_back(f);
+            fs = i + 1;
+        }
+    }
+    {
+        std::string f(b + fs, i - fs);
+        if (header) names.push_back(f.empty() ? "NA" : f);
+        cols.emplace_back();
+        if (!header) cols.back().push_back(f.empty() ? std::string("NA") : f);
+    }
+    const unsigned ncol = unsigned(cols.size());
+    const size_t start = i + 1 < n ? i + 1 : n;
+    if (start < n)
+        parse_rows_chunk<std::string, false>(std::string_view(b + start, n - start), cols, delim, quote, ncol, 0);
+    size_t nrow = cols[0].size();
+    int64_t bad = -1;
+    for (auto& c : cols) nrow = std::min(nrow, c.size());
+    for (auto& c : cols)
+        if (c.size() != nrow) bad = int64_t(nrow);
+    std::vector<char> types(ncol);
+    std::vector<std::vector<double>> dv(ncol);
+    std::vector<std::vector<unsigned>> uv(ncol);
+    std::vector<std::vector<uint8_t>> bv(ncol);
+    if (bad < 0) {
+#pragma omp parallel for num_threads(cores) schedule(dynamic, 1)
+        for (unsigned k = 0; k < ncol; ++k) {
+            const auto& v = cols[k];
+            bool is_bool = true, is_nb = true, is_bufchar = true;
+            char ty = 0;
+            const size_t chk = std::min<size_t>(v.size(), 10);
+            for (size_t r = 0; r < chk && !ty; ++r) {
+                const std::string_view s = v[r];
+                if (!simd_can_be_nb(s.data(), s.size())) {
+                    is_nb = false;
+                    if (s.size() > 1) {
+                        is_bufchar = false;
+                        break;
+                    }
+                    continue;
+                }
+                if (has_dot(s)) ty = 'd';
+                else if (s != "0" && s != "1") is_bool = false;
+            }
+            if (!ty) ty = !is_nb ? (is_bufchar ? 'c' : 's') : (is_bool ? 'b' : 'u');
+            types[k] = ty;
+            if (ty == 'd') {
+                dv[k].reserve(nrow);
+                for (const auto& el : v) {
+                    double x;
+                    auto [p, ec] = fast_float::from_chars(el.data(), el.data() + el.size(), x);
+                    dv[k].push_back(ec == std::errc() ? x : 0.0);
+                }
+            } else if (ty == 'u') {
+                uv[k].reserve(nrow);
+                for (const auto& el : v) {
+                    unsigned x;
+                    auto [p, ec] = std::from_chars(el.data(), el.data() + el.size(), x);
+                    uv[k].push_back(ec == std::errc() ? x : 0u);
+                }
+            } else if (ty == 'b') {
+                bv[k].reserve(nrow);
+                for (const auto& el : v) {
+                    int x;
+                    auto [p, ec] = std::from_chars(el.data(), el.data() + el.size(), x);
+                    bv[k].push_back(ec == std::errc() ? (x != 0) : 0);
+                }
+            }
+        }
+    }
+    if (seconds) seconds[0] = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::string blob;
+    auto put = [&](const void* p, size_t k) { blob.append(static_cast<const char*>(p), k); };
+    const uint64_t nrow_out = bad >= 0 ? 0 : nrow;
+    const uint32_t pad = 0;
+    put(&nrow_out, 8);
+    put(&ncol, 4);
+    put(&pad, 4);
+    put(&bad, 8);
+    for (unsigned k = 0; k < ncol; ++k) {
+        const uint8_t ty = uint8_t(types[k] ? types[k] : 's');
+        put(&ty, 1);
+        const std::string nm = header ? names[k] : std::string();
+        const uint32_t nl = uint32_t(nm.size());
+        put(&nl, 4);
+        put(nm.data(), nl);
+    }
+    if (nrow_out)
+        for (unsigned k = 0; k < ncol; ++k) {
+            const char ty = types[k];
+            if (ty == 'd') put(dv[k].data(), 8 * nrow);
+            else if (ty == 'u') put(uv[k].data(), 4 * nrow);
+            else if (ty == 'b') put(bv[k].data(), nrow);
+            else {
+                uint64_t off = 0;
+                put(&off, 8);
+                for (size_t r = 0; r < nrow; ++r) {
+                    off += cols[k][r].size();
+                    put(&off, 8);
+                }
+                for (size_t r = 0; r < nrow; ++r) put(cols[k][r].data(), cols[k][r].size());
+            }
+        }
+    void* out = malloc(blob.size() ? blob.size() : 1);
+    if (out) memcpy(out, blob.data(), blob.size());
+    if (blob_bytes) *blob_bytes = blob.size();
+    return out;
+}
+
+// One-call timing of the reference path on `reps` repetitions (for the CPU
+// baseline): returns the best parse + inference + conversion seconds.
+double ref_csv_time(const char* b, size_t n, char delim, int header, char quote, int cores, int reps) {
+    double best = 1e30;
+    for (int r = 0; r < reps; ++r) {
+        double s = 0;
+        size_t bytes = 0;
+        void* p = ref_csv_read(b, n, delim, header, quote, cores, &bytes, &s);
+        free(p);
+        best = std::min(best, s);
+    }
+    return best;
+}
+
+void ref_csv_free(void* p) { free(p); }
 
 }  // extern "C"

@@ -14,11 +14,19 @@
                           value column's group sums) of the restated reference
                           hash group-by (ankerl map + simd_hash from the
                           reference tree) on seeded frames.
+  ref_csv_cases.npz       CSV inputs (seeded synthetic files from
+                          tests/csv_gen.py plus hand-written edge cases) and the
+                          tables the REFERENCE'S OWN record parser and
+                          fast_float produce for them (oracle/_ref shim,
+                          ref_csv_read), in the oracle's blob layout; `meta`
+                          holds each case's delimiter, quote and header flag.
 
 Run here, where the reference tree exists:  python tests/golden/make_golden.py
+(`python tests/golden/make_golden.py csv` rewrites only ref_csv_cases.npz)
 """
 from __future__ import annotations
 
+import ctypes as C
 import json
 import sys
 from pathlib import Path
@@ -106,12 +114,96 @@ def make_groupby_cases() -> list:
     return cases
 
 
+def hard_decimals(seed: int, count: int) -> list:
+    """Decimal strings at and next to the exact halfway points between
+    adjacent doubles (exact rational arithmetic), plus out-of-range values."""
+    import math
+    import random
+    import struct
+    from fractions import Fraction
+
+    def exact(fr):
+        k = fr.denominator.bit_length() - 1
+        assert fr.denominator == 1 << k
+        digits = str(fr.numerator * 5 ** k)
+        if k == 0:
+            return digits
+        if len(digits) <= k:
+            digits = "0" * (k - len(digits) + 1) + digits
+        return digits[:-k] + "." + digits[-k:]
+
+    rnd = random.Random(seed)
+    out = ["0.5", "1e400", "-1e400", "1e-400", "2.4703282292062327e-324", "2.4703282292062328e-324",
+           "4.9e-324", "1.7976931348623158e308", "1.7976931348623159e308", "nan", "-inf", "Infinity", "NA",
+           "-0.0", "12abc", "1e", "1e+", ".5", "-.5", "5."]
+    while len(out) < count:
+        b = rnd.getrandbits(63) if rnd.random() < 0.8 else rnd.getrandbits(52)
+        x = struct.unpack("<d", struct.pack("<Q", b))[0]
+        y = math.nextafter(x, math.inf)
+        if not (0 < x and math.isfinite(y)):
+            continue
+        h = (Fraction(x) + Fraction(y)) / 2
+        s = exact(h)
+        out += [s, s + "000000000000000000001", exact(h - Fraction(1, 1 << 1100)) if h > Fraction(1, 1 << 1100) else s]
+    return out[:count]
+
+
+def make_csv_cases() -> dict:
+    import csv_gen
+    cases = []
+    for seed in range(10):
+        cases.append(dict(data=csv_gen.make_csv(100 + seed, 40 + 23 * seed, crlf=seed % 3 == 1,
+                                                empty_frac=0.05 * (seed % 2), header=seed % 4 != 3,
+                                                trailing_newline=seed % 5 != 4, quote="'" if seed % 2 else '"'),
+                          delim=",", quote="'" if seed % 2 else '"', header=seed % 4 != 3))
+    cases.append(dict(data=csv_gen.make_csv(7, 300, kinds=["d"] * 4, dec_style=2), delim=",", quote="'",
+                      header=True))
+    cases.append(dict(data=("x\n" + "\n".join(hard_decimals(11, 600)) + "\n").encode(), delim=",", quote="'",
+                      header=True))
+    edge = [
+        (b"a;b;c\n1;'x;y';2.5\n3;'multi\nline';4.0\n", ";", "'", True),   # quoted delimiter and LF
+        (b"a,b\r1,2\r3,4\r", ",", "'", True),                             # CR-only line ends
+        (b"1,2,x\r\n3,4,y\r\n", ",", "'", False),                           # no header, CR LF: first row keeps the CR
+        (b",2,\n3,,5\n", ",", "'", False),                                # no header, empty first-line fields
+        (b"h1,h2\n", ",", "'", True),                                      # header only
+        (b"h1,h2\n1,2\n3\n4,5\n", ",", "'", True),                         # a record with fewer fields
+        (b"n\n0\n1\n1\n0\n7\n-3\n", ",", "'", True),                         # 0/1 flags read as 'b'
+        (b"n\n4294967295\n4294967296\n0012\n7\n", ",", "'", True),          # u32 limits
+        (b"n\n1\n2\n3\n4\n5\n6\n7\n8\n9\n10\n12x\n\n-5\n+5\n", ",", "'", True),  # 'u' past the first 10
+        (b"c\nA\nB\nC", ",", "'", True),                                   # one-byte codes, no final LF
+        (b"c\nA\nB\n\nC", ",", "'", True),                                 # an empty record reads "NA" ('s')
+        (b"v\n1.5\nnan\n-nan\ninf\n-Infinity\n1e999\n1e-999\n+1\n 2\n", ",", "'", True),
+    ]
+    for data, d, q, h in edge:
+        cases.append(dict(data=data, delim=d, quote=q, header=h))
+    out, meta = {}, []
+    for i, c in enumerate(cases):
+        r = ob.ref_csv_read(c["data"], delim=c["delim"], header=c["header"], quote=c["quote"])
+        size = C.c_size_t(0)
+        lib = ob.ref()
+        blob = lib.ref_csv_read(c["data"], len(c["data"]), c["delim"].encode(), 1 if c["header"] else 0,
+                                c["quote"].encode(), 1, C.byref(size), None)
+        raw = C.string_at(blob, size.value)
+        lib.ref_csv_free(blob)
+        assert r.nrow == ob.CsvResult(raw).nrow
+        out[f"csv{i}"] = np.frombuffer(c["data"], dtype=np.uint8)
+        out[f"blob{i}"] = np.frombuffer(raw, dtype=np.uint8)
+        meta.append(dict(delim=c["delim"], quote=c["quote"], header=c["header"]))
+    out["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    return out
+
+
 def main():
+    if len(sys.argv) > 1 and sys.argv[1] == "csv":
+        np.savez_compressed(HERE / "ref_csv_cases.npz", **make_csv_cases())
+        print("written: ref_csv_cases.npz")
+        return
     if not ob.ref_available():
         sys.exit("oracle/_ref/libvdf_ref.so missing: run `make -C oracle ref` where the reference tree exists")
     (HERE / "internals_sort_by.json").write_text(json.dumps(INTERNALS, indent=1) + "\n")
     np.savez_compressed(HERE / "ref_sort_cases.npz", **make_sort_cases())
     (HERE / "ref_groupby_cases.json").write_text(json.dumps(make_groupby_cases(), indent=1) + "\n")
+    np.savez_compressed(HERE / "ref_csv_cases.npz", **make_csv_cases())
     print("written:", sorted(p.name for p in HERE.iterdir()))
 
 

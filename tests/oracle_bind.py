@@ -25,7 +25,8 @@ def _vp(a: np.ndarray):
 
 
 def _load_oracle() -> C.CDLL:
-    if not ORACLE_LIB.exists() or ORACLE_LIB.stat().st_mtime < (ORACLE_DIR / "vdf_oracle.c").stat().st_mtime:
+    srcs = [ORACLE_DIR / "vdf_oracle.c", ORACLE_DIR / "vdf_oracle_csv.c"]
+    if not ORACLE_LIB.exists() or any(ORACLE_LIB.stat().st_mtime < p.stat().st_mtime for p in srcs):
         subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "all"], check=True)
     lib = C.CDLL(str(ORACLE_LIB))
     lib.orc_argsort.restype = C.c_int
@@ -43,6 +44,15 @@ def _load_oracle() -> C.CDLL:
     lib.orc_unique.argtypes = [C.c_void_p, C.c_int, C.c_size_t, C.c_int, C.c_void_p]
     lib.orc_left_join.restype = C.c_int64
     lib.orc_left_join.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_int, C.c_int, C.c_void_p]
+    lib.orc_csv_read.restype = C.c_void_p
+    lib.orc_csv_read.argtypes = [C.c_char_p, C.c_size_t, C.c_char, C.c_int, C.c_char, C.POINTER(C.c_size_t)]
+    lib.orc_csv_free.argtypes = [C.c_void_p]
+    lib.orc_parse_double.restype = C.c_double
+    lib.orc_parse_double.argtypes = [C.c_char_p, C.c_size_t]
+    lib.orc_parse_u32.restype = C.c_uint32
+    lib.orc_parse_u32.argtypes = [C.c_char_p, C.c_size_t]
+    lib.orc_parse_i32.restype = C.c_int32
+    lib.orc_parse_i32.argtypes = [C.c_char_p, C.c_size_t]
     return lib
 
 
@@ -178,3 +188,88 @@ def left_join(left, right, method=0):
                                int(method), _vp(match))
     assert m >= 0
     return match, int(m)
+
+
+class CsvResult:
+    """A parsed CSV table in the oracle's blob layout: nrow, names, types,
+    bad_row (-1 when every record has the first line's field count) and
+    columns (numpy arrays, or lists of bytes for strings)."""
+
+    NP = {"d": np.float64, "u": np.uint32, "b": np.uint8}
+
+    def __init__(self, blob: bytes):
+        nrow, ncol, _pad, bad = np.frombuffer(blob[:24], dtype=np.dtype([("a", "<u8"), ("b", "<u4"), ("c", "<u4"),
+                                                                          ("d", "<i8")]))[0]
+        self.nrow, self.ncol, self.bad_row = int(nrow), int(ncol), int(bad)
+        p = 24
+        self.types, self.names = [], []
+        for _ in range(self.ncol):
+            self.types.append(chr(blob[p]))
+            nl = int(np.frombuffer(blob[p + 1:p + 5], dtype="<u4")[0])
+            self.names.append(blob[p + 5:p + 5 + nl].decode("latin-1"))
+            p += 5 + nl
+        self.columns = []
+        if self.nrow == 0 or self.bad_row >= 0:
+            self.columns = [np.zeros(0, self.NP.get(t, np.uint8)) if t in self.NP else [] for t in self.types]
+            return
+        for t in self.types:
+            if t in self.NP:
+                w = np.dtype(self.NP[t]).itemsize
+                self.columns.append(np.frombuffer(blob[p:p + w * self.nrow], dtype=self.NP[t]).copy())
+                p += w * self.nrow
+            else:
+                off = np.frombuffer(blob[p:p + 8 * (self.nrow + 1)], dtype="<u8")
+                p += 8 * (self.nrow + 1)
+                data = blob[p:p + int(off[-1])]
+                p += int(off[-1])
+                self.columns.append([data[int(off[i]):int(off[i + 1])] for i in range(self.nrow)])
+
+
+def csv_read(data: bytes, delim=",", header=True, quote="'") -> CsvResult:
+    """Oracle read_csv of `data` (the C restatement)."""
+    size = C.c_size_t(0)
+    blob = oracle().orc_csv_read(data, len(data), delim.encode("latin-1"), 1 if header else 0,
+                                 quote.encode("latin-1"), C.byref(size))
+    assert blob
+    try:
+        return CsvResult(C.string_at(blob, size.value))
+    finally:
+        oracle().orc_csv_free(blob)
+
+
+def parse_double(s: bytes) -> float:
+    return oracle().orc_parse_double(s, len(s))
+
+
+def parse_u32(s: bytes) -> int:
+    return int(oracle().orc_parse_u32(s, len(s)))
+
+
+def parse_i32(s: bytes) -> int:
+    return int(oracle().orc_parse_i32(s, len(s)))
+
+
+def ref_csv_read(data: bytes, delim=",", header=True, quote="'", cores=1) -> CsvResult:
+    """The reference's own parser (oracle/_ref shim) on `data`: the same blob layout."""
+    lib = ref()
+    lib.ref_csv_read.restype = C.c_void_p
+    lib.ref_csv_read.argtypes = [C.c_char_p, C.c_size_t, C.c_char, C.c_int, C.c_char, C.c_int,
+                                 C.POINTER(C.c_size_t), C.POINTER(C.c_double)]
+    lib.ref_csv_free.argtypes = [C.c_void_p]
+    size = C.c_size_t(0)
+    blob = lib.ref_csv_read(data, len(data), delim.encode("latin-1"), 1 if header else 0, quote.encode("latin-1"),
+                            int(cores), C.byref(size), None)
+    assert blob
+    try:
+        return CsvResult(C.string_at(blob, size.value))
+    finally:
+        lib.ref_csv_free(blob)
+
+
+def ref_csv_seconds(data: bytes, delim=",", header=True, quote="'", cores=1, reps=1) -> float:
+    """Best-of-`reps` seconds of the reference's parse + inference + conversions."""
+    lib = ref()
+    lib.ref_csv_time.restype = C.c_double
+    lib.ref_csv_time.argtypes = [C.c_char_p, C.c_size_t, C.c_char, C.c_int, C.c_char, C.c_int, C.c_int]
+    return float(lib.ref_csv_time(data, len(data), delim.encode("latin-1"), 1 if header else 0,
+                                  quote.encode("latin-1"), int(cores), int(reps)))

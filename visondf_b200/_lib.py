@@ -11,6 +11,7 @@ from dataclasses import dataclass, field
 from pathlib import Path
 from typing import Optional, Sequence
 
+import numpy as np
 import torch
 
 LIB_PATH = Path(__file__).resolve().parent / "libvdf_b200.so"
@@ -24,7 +25,7 @@ I32, I64, U32, U64, F64, F32 = range(6)
 ORDER_ASC, ORDER_DESC_STABLE, ORDER_DESC_REVERSE = range(3)
 
 KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast", "pack",
-                  "segscan", "segemit", "ties", "batch"]
+                  "segscan", "segemit", "ties", "batch", "csv"]
 # vdf_multikey_mode
 MULTIKEY_LSD, MULTIKEY_PRIMARY_FIRST = 0, 1
 
@@ -139,6 +140,17 @@ def _load() -> C.CDLL:
         "vdf_batch_launch": (st, [vp, vp]),
         "vdf_batch_launch_graph": (st, [vp, vp]),
         "vdf_batch_destroy": (None, [vp]),
+        "vdf_csv_read": (st, [vp, vp, u64, C.c_char, i32, C.c_char, C.POINTER(vp), vp]),
+        "vdf_csv_read_host": (st, [vp, vp, u64, C.c_char, i32, C.c_char, C.POINTER(vp), vp]),
+        "vdf_csv_nrow": (u64, [vp]),
+        "vdf_csv_ncol": (C.c_uint32, [vp]),
+        "vdf_csv_name": (C.c_char_p, [vp, C.c_uint32]),
+        "vdf_csv_type": (C.c_char, [vp, C.c_uint32]),
+        "vdf_csv_values": (vp, [vp, C.c_uint32]),
+        "vdf_csv_offsets": (vp, [vp, C.c_uint32]),
+        "vdf_csv_string_bytes": (u64, [vp, C.c_uint32]),
+        "vdf_csv_copy_column": (st, [vp, vp, C.c_uint32, vp, vp, vp]),
+        "vdf_csv_free": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -431,6 +443,25 @@ class Context:
                                    C.byref(cnt), _stream(stream)), "vdf_unique")
         return keep, int(cnt.value)
 
+    def read_csv(self, data, delim: str = ",", header: bool = True, quote: str = "'", stream=None) -> "CsvTable":
+        """Parses a CSV file's bytes (`bytes` / numpy uint8 in host memory, or
+        a contiguous CUDA uint8 tensor) into device columns (read_csv, with the
+        reference's defaults delim ',', header on, quote \\')."""
+        h = C.c_void_p()
+        d, q = delim.encode("latin-1"), quote.encode("latin-1")
+        if isinstance(data, torch.Tensor):
+            if not data.is_cuda or data.dtype != torch.uint8 or not data.is_contiguous():
+                raise ValueError("device input must be a contiguous CUDA uint8 tensor")
+            self._check(lib.vdf_csv_read(self.handle, data.data_ptr(), data.numel(), d, 1 if header else 0, q,
+                                         C.byref(h), _stream(stream)), "vdf_csv_read")
+        else:
+            buf = np.frombuffer(data, dtype=np.uint8) if isinstance(data, (bytes, bytearray)) else \
+                np.ascontiguousarray(data, dtype=np.uint8)
+            self._check(lib.vdf_csv_read_host(self.handle, buf.ctypes.data if buf.size else None, buf.size, d,
+                                              1 if header else 0, q, C.byref(h), _stream(stream)),
+                        "vdf_csv_read_host")
+        return CsvTable(self, h.value)
+
     def left_join_index(self, left: torch.Tensor, right: torch.Tensor, method: int = 0, stream=None):
         """(match, n_matched): match[i] = the row of `right` that left row i
         takes -- method 0: the first row holding its key, 1: the last, 2
@@ -442,6 +473,67 @@ class Context:
         self._check(lib.vdf_left_join_index(self.handle, n, _col(left), right.numel(), _col(right), int(method),
                                             _ptr(match), None, C.byref(cnt), _stream(stream)), "vdf_left_join_index")
         return match, int(cnt.value)
+
+
+class CsvTable:
+    """A parsed CSV file: device-resident columns owned by the table
+    (vdf_csv_read).  `types[k]` is 'd' (float64), 'u' (uint32), 'b' (uint8
+    0/1), 's' or 'c' (strings: offsets + bytes)."""
+
+    _NP = {"d": np.float64, "u": np.uint32, "b": np.uint8}
+
+    def __init__(self, ctx: "Context", handle: int):
+        self._ctx = ctx
+        self.handle = handle
+        self.nrow = int(lib.vdf_csv_nrow(handle))
+        self.ncol = int(lib.vdf_csv_ncol(handle))
+        self.names = [lib.vdf_csv_name(handle, k).decode("latin-1") for k in range(self.ncol)]
+        self.types = [lib.vdf_csv_type(handle, k).decode("latin-1") for k in range(self.ncol)]
+
+    def device_column(self, k: int) -> dict:
+        """{'values': device pointer, 'offsets': device pointer or None, 'bytes': string bytes}."""
+        return dict(values=lib.vdf_csv_values(self.handle, k), offsets=lib.vdf_csv_offsets(self.handle, k),
+                    bytes=int(lib.vdf_csv_string_bytes(self.handle, k)))
+
+    _TORCH = {"d": torch.float64, "u": torch.int32, "b": torch.uint8}
+
+    def tensor(self, k: int, stream=None) -> torch.Tensor:
+        """Numeric column k copied into a new CUDA tensor (uint32 columns as
+        int32 bit patterns)."""
+        ty = self.types[k]
+        if ty not in self._TORCH:
+            raise ValueError("string columns have no tensor form")
+        out = torch.empty(self.nrow, dtype=self._TORCH[ty], device=f"cuda:{self._ctx.device}")
+        self._ctx._check(lib.vdf_csv_copy_column(self._ctx.handle, self.handle, k, out.data_ptr(), None,
+                                                 _stream(stream)), "vdf_csv_copy_column")
+        return out
+
+    def column(self, k: int, stream=None):
+        """Column k on the host: a numpy array, or a list of bytes for strings."""
+        ty = self.types[k]
+        if ty in self._NP:
+            out = np.empty(self.nrow, dtype=self._NP[ty])
+            self._ctx._check(lib.vdf_csv_copy_column(self._ctx.handle, self.handle, k, out.ctypes.data, None,
+                                                        _stream(stream)), "vdf_csv_copy_column")
+            return out
+        nb = int(lib.vdf_csv_string_bytes(self.handle, k))
+        data = np.empty(max(nb, 1), dtype=np.uint8)
+        off = np.empty(self.nrow + 1, dtype=np.uint64)
+        self._ctx._check(lib.vdf_csv_copy_column(self._ctx.handle, self.handle, k, data.ctypes.data,
+                                                    off.ctypes.data, _stream(stream)), "vdf_csv_copy_column")
+        raw = data.tobytes()
+        return [raw[int(off[i]):int(off[i + 1])] for i in range(self.nrow)]
+
+    def close(self):
+        if self.handle:
+            lib.vdf_csv_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def sort_variants() -> list:

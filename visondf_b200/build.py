@@ -40,7 +40,8 @@ def sources() -> list[Path]:
 
 
 def headers() -> list[Path]:
-    return sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(INCLUDE.glob("*.h"))
+    return (sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inc"))
+            + sorted(INCLUDE.glob("*.h")))
 
 
 def _stale(target: Path, deps: list[Path]) -> bool:

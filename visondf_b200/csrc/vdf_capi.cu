@@ -610,21 +610,6 @@ struct HostStage {
     vdf_sort_groupby_args d;
 };
 
-vdf_status io_ensure(vdf_ctx* c, size_t bytes) {
-    if (bytes <= c->io_cap) return VDF_OK;
-    if (c->io) {
-        cudaFree(c->io);
-        c->io = nullptr;
-        c->io_cap = 0;
-    }
-    const size_t cap = align256(bytes + bytes / 8);
-    if (cudaMalloc(&c->io, cap) != cudaSuccess) {
-        cudaGetLastError();
-        return fail(c, VDF_ERR_OOM, "I/O staging allocation of %zu bytes failed", cap);
-    }
-    c->io_cap = cap;
-    return VDF_OK;
-}
 
 }  // namespace
 

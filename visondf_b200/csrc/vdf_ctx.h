@@ -146,6 +146,23 @@ inline vdf_status ws_ensure(vdf_ctx* c, size_t bytes) {
     return VDF_OK;
 }
 
+// Grow-only device staging for the host-memory entry points.
+inline vdf_status io_ensure(vdf_ctx* c, size_t bytes) {
+    if (bytes <= c->io_cap) return VDF_OK;
+    if (c->io) {
+        cudaFree(c->io);
+        c->io = nullptr;
+        c->io_cap = 0;
+    }
+    const size_t cap = align256(bytes + bytes / 8);
+    if (cudaMalloc(&c->io, cap) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, VDF_ERR_OOM, "I/O staging allocation of %zu bytes failed", cap);
+    }
+    c->io_cap = cap;
+    return VDF_OK;
+}
+
 // Reads and clears the device error bits after the stream has drained.
 inline vdf_status drain_and_check(vdf_ctx* c, cudaStream_t s) {
     cudaError_t e = cudaMemcpyAsync(&c->host_pinned[1], err_word(c), sizeof(uint32_t), cudaMemcpyDeviceToHost, s);

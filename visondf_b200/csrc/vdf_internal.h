@@ -15,7 +15,7 @@ constexpr int kMaxGather = 8;   // columns per gather launch
 enum KernelClass : int {
     KC_HIST = 0, KC_SCAN = 1, KC_ONESWEEP32 = 2, KC_ONESWEEP64 = 3, KC_GATHER = 4, KC_SEGREDUCE = 5,
     KC_BROADCAST = 6, KC_PACK = 7, KC_SEGSCAN = 8, KC_SEGEMIT = 9, KC_TIES = 10, KC_BATCH = 11,
-    KC_COUNT = 12
+    KC_CSV = 12, KC_COUNT = 13
 };
 
 // Brackets kernel launches with CUDA events when profiling is enabled.
