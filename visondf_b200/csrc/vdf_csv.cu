@@ -72,11 +72,12 @@ __device__ __forceinline__ uint64_t prefix_xor(uint64_t x) {
 struct Masks {
     uint64_t quote;  // quote bytes
     uint64_t term;   // record terminator candidates (CR, or LF not after CR)
+    uint64_t ev;     // field end candidates: terminators and delimiters
 };
 
 // Masks of the 64 bytes at `base` restricted to [start, n).
 __device__ __forceinline__ Masks chunk_masks(const uint8_t* __restrict__ buf, uint64_t n, uint64_t start,
-                                             uint64_t base, uint32_t quote4) {
+                                             uint64_t base, uint32_t quote4, uint32_t delim4) {
     uint32_t w[16];
     if (base + kChunk <= n) {
         const uint4* p = reinterpret_cast<const uint4*>(buf + base);
@@ -99,10 +100,11 @@ __device__ __forceinline__ Masks chunk_masks(const uint8_t* __restrict__ buf, ui
             w[k] = x;
         }
     }
-    uint64_t q = 0, cr = 0, lf = 0;
+    uint64_t q = 0, cr = 0, lf = 0, dl = 0;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
         q |= (uint64_t)nibble(__vcmpeq4(w[k], quote4)) << (4 * k);
+        dl |= (uint64_t)nibble(__vcmpeq4(w[k], delim4)) << (4 * k);
         cr |= (uint64_t)nibble(__vcmpeq4(w[k], 0x0d0d0d0du)) << (4 * k);
         lf |= (uint64_t)nibble(__vcmpeq4(w[k], 0x0a0a0a0au)) << (4 * k);
     }
@@ -117,6 +119,7 @@ __device__ __forceinline__ Masks chunk_masks(const uint8_t* __restrict__ buf, ui
     Masks m;
     m.quote = q;
     m.term = cr | (lf & ~after_cr);
+    m.ev = m.term | (dl & valid);
     return m;
 }
 
@@ -164,15 +167,16 @@ __device__ __forceinline__ uint32_t block_sum_excl(uint32_t v, uint32_t* s_w, ui
     return wp + x - v;
 }
 
-// Pass 1: per tile {quote parity, records if the tile starts outside quotes,
-// records if it starts inside}.
+// Pass 1: per tile {quote parity, field ends if the tile starts outside
+// quotes, field ends if it starts inside}.
 __global__ void __launch_bounds__(kThreads) k_csv_count(const uint8_t* __restrict__ buf, uint64_t n, uint64_t start,
-                                                        uint32_t quote4, uint32_t* __restrict__ tiles) {
+                                                        uint32_t quote4, uint32_t delim4,
+                                                        uint32_t* __restrict__ tiles) {
     __shared__ uint32_t s_w[kThreads / 32];
     const uint64_t base = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) * kChunk;
-    const Masks m = chunk_masks(buf, n, start, base, quote4);
+    const Masks m = chunk_masks(buf, n, start, base, quote4, delim4);
     const uint64_t px = prefix_xor(m.quote);  // bit i: quotes in [base, i] odd
-    const uint32_t c_out = __popcll(m.term & ~px), c_in = __popcll(m.term & px);
+    const uint32_t c_out = __popcll(m.ev & ~px), c_in = __popcll(m.ev & px);
     uint32_t par_total;
     const uint32_t pre = block_xor_excl(__popcll(m.quote) & 1u, s_w, par_total);
     uint32_t t0, t1;
@@ -209,21 +213,28 @@ __global__ void __launch_bounds__(1024) k_csv_scan(const uint32_t* __restrict__ 
     if (threadIdx.x == 0) *total = first;
 }
 
-// Pass 3: write each record terminator's position; the thread holding the
-// last one also records where the byte after it starts.
-__global__ void __launch_bounds__(kThreads) k_csv_records(const uint8_t* __restrict__ buf, uint64_t n, uint64_t start,
-                                                          uint32_t quote4, const uint32_t* __restrict__ tile_state,
-                                                          const uint32_t* __restrict__ tile_first,
-                                                          const uint32_t* __restrict__ total,
-                                                          uint32_t* __restrict__ pos, uint32_t* __restrict__ tail,
-                                                          uint32_t* __restrict__ err) {
+// Pass 3: write each field end's position (delimiter or record terminator
+// outside quotes).  Field f belongs to record f / ncol and must end in a
+// terminator exactly when f % ncol == ncol - 1; the first record that breaks
+// this is the "column number problem" row.  The thread holding the last
+// field end records where the bytes after it start (or ~0 after a
+// delimiter: the final record then has no terminator).
+__global__ void __launch_bounds__(kThreads) k_csv_fields(const uint8_t* __restrict__ buf, uint64_t n, uint64_t start,
+                                                         uint32_t quote4, uint32_t delim4,
+                                                         const uint32_t* __restrict__ tile_state,
+                                                         const uint32_t* __restrict__ tile_first,
+                                                         const uint32_t* __restrict__ total, uint32_t ncol,
+                                                         uint32_t row_base, uint32_t* __restrict__ pos,
+                                                         uint32_t* __restrict__ tail,
+                                                         unsigned long long* __restrict__ bad_row,
+                                                         uint32_t* __restrict__ err) {
     __shared__ uint32_t s_w[kThreads / 32];
     const uint64_t base = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) * kChunk;
-    const Masks m = chunk_masks(buf, n, start, base, quote4);
+    const Masks m = chunk_masks(buf, n, start, base, quote4, delim4);
     const uint64_t px = prefix_xor(m.quote);
     uint32_t par_total;
     const uint32_t st = tile_state[blockIdx.x] ^ block_xor_excl(__popcll(m.quote) & 1u, s_w, par_total);
-    uint64_t ev = m.term & (st ? px : ~px);
+    uint64_t ev = m.ev & (st ? px : ~px);
     uint32_t tot;
     uint32_t off = tile_first[blockIdx.x] + block_sum_excl(__popcll(ev), s_w, tot);
     const uint32_t last = *total - 1;
@@ -236,9 +247,14 @@ __global__ void __launch_bounds__(kThreads) k_csv_records(const uint8_t* __restr
             return;
         }
         pos[off] = p;
+        const bool is_term = (m.term >> b) & 1;
+        if (is_term != (off % ncol == ncol - 1)) atomicMin(bad_row, (unsigned long long)(off / ncol + row_base));
         if (off == last) {
-            uint32_t next = p + 1;
-            if (buf[p] == '\r' && (uint64_t)p + 1 < n && buf[p + 1] == '\n') ++next;
+            uint32_t next = 0xffffffffu;
+            if (is_term) {
+                next = p + 1;
+                if (buf[p] == '\r' && (uint64_t)p + 1 < n && buf[p + 1] == '\n') ++next;
+            }
             *tail = next;
         }
         ++off;
@@ -291,7 +307,7 @@ struct ParseArgs {
     const uint8_t* buf;
     uint64_t n;
     uint32_t data_start;
-    const uint32_t* pos;  // record terminator positions (the last may be n)
+    const uint32_t* pos;  // field end positions, ncol per record (the last may be n)
     uint32_t records;
     uint32_t row_base;    // 1 when the first line is a data row parsed separately
     uint32_t ncol;
@@ -332,39 +348,26 @@ __device__ __forceinline__ void emit_field(const ParseArgs& a, Reader& rd, uint3
     }
 }
 
+// One thread per record; the threads of a CTA convert column c of their
+// records together (the same type branch, coalesced column writes), taking
+// each field's bounds from the field-end positions.
 __global__ void __launch_bounds__(kThreads) k_csv_parse(ParseArgs a) {
     const uint32_t r = blockIdx.x * kThreads + threadIdx.x;
     if (r >= a.records) return;
-    uint32_t start = a.data_start;
-    if (r > 0) {
-        const uint32_t p = a.pos[r - 1];
-        start = p + 1;
-        if (a.buf[p] == '\r' && (uint64_t)p + 1 < a.n && a.buf[p + 1] == '\n') ++start;
-    }
-    const uint32_t end = a.pos[r];
     const uint32_t row = r + a.row_base;
+    const uint32_t* fp = a.pos + (uint64_t)r * a.ncol;
+    uint32_t fs = a.data_start;
+    if (r > 0) {
+        const uint32_t p = fp[-1];
+        fs = p + 1;
+        if (a.buf[p] == '\r' && (uint64_t)p + 1 < a.n && a.buf[p + 1] == '\n') ++fs;
+    }
     Reader rd(a.buf, a.n);
-    uint32_t col = 0, fs = start;
-    bool inq = false;
-    for (uint32_t i = start; i < end; ++i) {
-        const unsigned char c = rd.get(i);
-        if (c == a.quote) {
-            inq = !inq;
-        } else if (!inq && c == a.delim) {
-            if (col + 1 >= a.ncol) {
-                atomicMin(a.bad_row, (unsigned long long)row);
-                return;
-            }
-            emit_field(a, rd, fs, i, col, row, true);
-            ++col;
-            fs = i + 1;
-        }
+    for (uint32_t c = 0; c < a.ncol; ++c) {
+        const uint32_t fe = fp[c];
+        emit_field(a, rd, fs, fe, c, row, true);
+        fs = fe + 1;
     }
-    if (col + 1 != a.ncol) {
-        atomicMin(a.bad_row, (unsigned long long)row);
-        return;
-    }
-    emit_field(a, rd, fs, end, col, row, true);
 }
 
 // The first line as a data row (no header): field bounds from the host, an
@@ -469,20 +472,36 @@ struct StrCopy {
     uint8_t* bytes[64];
 };
 
+// One warp per 32 rows of one string column (blockIdx.y): the lanes walk the
+// rows' contiguous output span byte by byte (coalesced stores) and find each
+// byte's row by a binary search over the 32 row offsets held in lanes.
 __global__ void __launch_bounds__(kThreads) k_csv_strings(StrCopy sc) {
-    const uint64_t r = (uint64_t)blockIdx.x * kThreads + threadIdx.x;
-    if (r >= sc.nrow) return;
-    for (uint32_t k = 0; k < sc.nstr; ++k) {
-        const uint64_t o = sc.off[k][r];
-        const uint32_t len = (uint32_t)(sc.off[k][r + 1] - o);
-        const uint32_t s = sc.starts[k][r];
-        uint8_t* dst = sc.bytes[k] + o;
-        if (s == 0xffffffffu) {
-            dst[0] = 'N';
-            dst[1] = 'A';
-        } else {
-            for (uint32_t j = 0; j < len; ++j) dst[j] = __ldg(sc.buf + s + j);
+    const uint32_t k = blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    const uint64_t r0 = ((uint64_t)blockIdx.x * kThreads + threadIdx.x) & ~31ull;
+    if (r0 >= sc.nrow) return;
+    const uint64_t r = r0 + lane;
+    const uint64_t* off = sc.off[k];
+    const uint64_t o = r < sc.nrow ? off[r] : off[sc.nrow];
+    const uint32_t s = r < sc.nrow ? sc.starts[k][r] : 0u;
+    const uint64_t o0 = __shfl_sync(0xffffffffu, o, 0);
+    const uint64_t rend = r0 + 32 < sc.nrow ? r0 + 32 : sc.nrow;
+    const uint64_t span = off[rend] - o0;
+    uint8_t* dst = sc.bytes[k];
+    for (uint64_t b = 0; b < span; b += 32) {  // the same trip count in every lane
+        const uint64_t d = b + lane;
+        const uint64_t at = o0 + (d < span ? d : span - 1);
+        // largest j with off[r0 + j] <= at (lanes past the end hold the end offset)
+        int j = 0;
+#pragma unroll
+        for (int step = 16; step; step >>= 1) {
+            const uint64_t oj = __shfl_sync(0xffffffffu, o, j + step);
+            if (oj <= at) j += step;
         }
+        const uint64_t oj = __shfl_sync(0xffffffffu, o, j);
+        const uint32_t sj = __shfl_sync(0xffffffffu, s, j);
+        const uint32_t i = (uint32_t)(at - oj);
+        if (d < span) dst[at] = sj == 0xffffffffu ? (i == 0 ? 'N' : 'A') : __ldg(sc.buf + sj + i);
     }
 }
 
@@ -552,22 +571,6 @@ char classify(const std::vector<std::string>& v) {
     return is_bool ? 'b' : 'u';
 }
 
-// Splits one record [s, e) of host bytes into fields the way
-// parse_rows_chunk does; empty fields read "NA".
-void split_record(const unsigned char* b, size_t s, size_t e, char delim, char quote, std::vector<std::string>& out) {
-    size_t fs = s;
-    bool inq = false;
-    for (size_t i = s; i < e; ++i) {
-        const unsigned char c = b[i];
-        if (c == (unsigned char)quote) inq = !inq;
-        else if (!inq && c == (unsigned char)delim) {
-            out.push_back(i > fs ? std::string((const char*)b + fs, i - fs) : std::string("NA"));
-            fs = i + 1;
-        }
-    }
-    out.push_back(e > fs ? std::string((const char*)b + fs, e - fs) : std::string("NA"));
-}
-
 inline unsigned grid_of(uint64_t n, unsigned per) { return (unsigned)((n + per - 1) / per); }
 
 vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf, uint64_t n, char delim, int header,
@@ -614,7 +617,8 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
     }
     if (!header) names.assign(ncol, std::string());  // no header: the reference keeps no names
 
-    // ---- record split over [data_start, n)
+    // ---- field ends over [data_start, n)
+    const uint32_t row_base = header ? 0 : 1;
     const uint64_t nchunks = (n + kChunk - 1) / kChunk;
     const uint32_t ntiles = (uint32_t)((nchunks + kThreads - 1) / kThreads);
     const size_t o_tiles = 0, o_state = align256((size_t)12 * ntiles), o_first = o_state + align256((size_t)4 * ntiles);
@@ -624,69 +628,74 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
     uint32_t* tiles = reinterpret_cast<uint32_t*>(c->ws + o_tiles);
     uint32_t* tstate = reinterpret_cast<uint32_t*>(c->ws + o_state);
     uint32_t* tfirst = reinterpret_cast<uint32_t*>(c->ws + o_first);
-    uint32_t* misc = reinterpret_cast<uint32_t*>(c->ws + o_misc);  // [0] records, [1] tail
+    uint32_t* misc = reinterpret_cast<uint32_t*>(c->ws + o_misc);  // [0] field ends, [1] tail
     unsigned long long* bad = reinterpret_cast<unsigned long long*>(c->ws + o_misc + 8);
     const uint32_t quote4 = 0x01010101u * (unsigned char)quote;
-    uint32_t records = 0, tail = (uint32_t)data_start;
-    if (ntiles && data_start < n) {
+    const uint32_t delim4 = 0x01010101u * (unsigned char)delim;
+    uint32_t nfields = 0, tail = (uint32_t)data_start;
+    auto count_pass = [&]() -> vdf_status {
         begin();
-        k_csv_count<<<ntiles, kThreads, 0, s>>>(dbuf, n, data_start, quote4, tiles);
+        k_csv_count<<<ntiles, kThreads, 0, s>>>(dbuf, n, data_start, quote4, delim4, tiles);
         if ((e = cudaGetLastError()) != cudaSuccess) return from_cuda(c, e, "launch k_csv_count");
         k_csv_scan<<<1, 1024, 0, s>>>(tiles, ntiles, tstate, tfirst, misc);
         if ((e = cudaGetLastError()) != cudaSuccess) return from_cuda(c, e, "launch k_csv_scan");
         end();
         c->launches += 2;
+        return VDF_OK;
+    };
+    if (ntiles && data_start < n) {
+        if ((st = count_pass()) != VDF_OK) return st;
         e = cudaMemcpyAsync(&c->host_pinned[0], misc, 4, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) return from_cuda(c, e, "record count");
-        records = (uint32_t)(c->host_pinned[0] & 0xffffffffu);
-        if (records > n - data_start)
-            return fail(c, VDF_ERR_DEVICE, "record count %u exceeds the %llu data bytes", records,
+        if (e != cudaSuccess) return from_cuda(c, e, "field count");
+        nfields = (uint32_t)(c->host_pinned[0] & 0xffffffffu);
+        if (nfields > n - data_start)
+            return fail(c, VDF_ERR_DEVICE, "field count %u exceeds the %llu data bytes", nfields,
                         (unsigned long long)(n - data_start));
     }
-    // room for the record positions (+1: a final record without terminator).
+    // room for the positions (+1: a final record without terminator).
     // Growing the workspace replaces the buffer and loses the tile states and
     // offsets just computed, so the two passes run again on the new one.
-    const size_t need = o_pos + align256((size_t)4 * (records + 1));
-    if (need > c->ws_cap) {
-        if ((st = ws_ensure(c, need)) != VDF_OK) return st;
+    const size_t ws_need = o_pos + align256((size_t)4 * (nfields + 1));
+    if (ws_need > c->ws_cap) {
+        if ((st = ws_ensure(c, ws_need)) != VDF_OK) return st;
         tiles = reinterpret_cast<uint32_t*>(c->ws + o_tiles);
         tstate = reinterpret_cast<uint32_t*>(c->ws + o_state);
         tfirst = reinterpret_cast<uint32_t*>(c->ws + o_first);
         misc = reinterpret_cast<uint32_t*>(c->ws + o_misc);
         bad = reinterpret_cast<unsigned long long*>(c->ws + o_misc + 8);
-        if (records) {
-            begin();
-            k_csv_count<<<ntiles, kThreads, 0, s>>>(dbuf, n, data_start, quote4, tiles);
-            if ((e = cudaGetLastError()) != cudaSuccess) return from_cuda(c, e, "launch k_csv_count");
-            k_csv_scan<<<1, 1024, 0, s>>>(tiles, ntiles, tstate, tfirst, misc);
-            if ((e = cudaGetLastError()) != cudaSuccess) return from_cuda(c, e, "launch k_csv_scan");
-            end();
-            c->launches += 2;
-        }
+        if (nfields && (st = count_pass()) != VDF_OK) return st;
     }
     uint32_t* pos = reinterpret_cast<uint32_t*>(c->ws + o_pos);
-    if (records) {
+    e = cudaMemsetAsync(bad, 0xff, 8, s);
+    if (e != cudaSuccess) return from_cuda(c, e, "clear the error row");
+    unsigned long long bad_row = ~0ull;
+    if (nfields) {
         begin();
-        k_csv_records<<<ntiles, kThreads, 0, s>>>(dbuf, n, data_start, quote4, tstate, tfirst, misc, pos, misc + 1,
-                                                  err_word(c));
-        if ((e = cudaGetLastError()) != cudaSuccess) return from_cuda(c, e, "launch k_csv_records");
+        k_csv_fields<<<ntiles, kThreads, 0, s>>>(dbuf, n, data_start, quote4, delim4, tstate, tfirst, misc, ncol,
+                                                 row_base, pos, misc + 1, bad, err_word(c));
+        if ((e = cudaGetLastError()) != cudaSuccess) return from_cuda(c, e, "launch k_csv_fields");
         end();
         c->launches += 1;
         e = cudaMemcpyAsync(&c->host_pinned[0], misc + 1, 4, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&c->host_pinned[2], bad, 8, cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-        if (e != cudaSuccess) return from_cuda(c, e, "record tail");
+        if (e != cudaSuccess) return from_cuda(c, e, "field tail");
         tail = (uint32_t)(c->host_pinned[0] & 0xffffffffu);
+        bad_row = c->host_pinned[2];
     }
-    if (tail < n) {
-        // bytes after the last terminator form one more record
+    if (tail == 0xffffffffu || tail < n) {
+        // the bytes after the last terminator form one more record: its end is n
+        if (nfields % ncol != ncol - 1) bad_row = std::min<unsigned long long>(bad_row, nfields / ncol + row_base);
         c->host_pinned[0] = n;
-        e = cudaMemcpyAsync(pos + records, &c->host_pinned[0], 4, cudaMemcpyHostToDevice, s);
+        e = cudaMemcpyAsync(pos + nfields, &c->host_pinned[0], 4, cudaMemcpyHostToDevice, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return from_cuda(c, e, "final record");
-        ++records;
+        ++nfields;
     }
-    const uint32_t row_base = header ? 0 : 1;
+    if (bad_row != ~0ull)
+        return fail(c, VDF_ERR_INVALID_ARG, "column number problem at row %llu (%u fields expected)", bad_row, ncol);
+    const uint32_t records = nfields / ncol;
     const uint64_t nrow = (uint64_t)records + row_base;
 
     // ---- classify on the first 10 values of each column
@@ -695,31 +704,29 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
         for (uint32_t k = 0; k < ncol; ++k) vals[k].push_back(first[k]);
     const uint32_t nfirst = records < 10 ? records : 10;
     if (nfirst) {
-        std::vector<uint32_t> p(nfirst);
-        e = cudaMemcpyAsync(p.data(), pos, 4 * nfirst, cudaMemcpyDeviceToHost, s);
+        std::vector<uint32_t> p((size_t)nfirst * ncol);
+        e = cudaMemcpyAsync(p.data(), pos, 4 * p.size(), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return from_cuda(c, e, "first records");
-        const uint64_t span_end = (uint64_t)p[nfirst - 1] + 2 < n ? (uint64_t)p[nfirst - 1] + 2 : n;
+        const uint64_t span_end = (uint64_t)p.back() + 2 < n ? (uint64_t)p.back() + 2 : n;
         std::vector<unsigned char> tmp;
-        const unsigned char* b = hbuf;
+        const unsigned char* hb2 = hbuf;
         if (!hbuf) {
             tmp.resize(span_end);
             e = cudaMemcpyAsync(tmp.data(), dbuf, span_end, cudaMemcpyDeviceToHost, s);
             if (e == cudaSuccess) e = cudaStreamSynchronize(s);
             if (e != cudaSuccess) return from_cuda(c, e, "first records' bytes");
-            b = tmp.data();
+            hb2 = tmp.data();
         }
-        uint64_t rs = data_start;
-        for (uint32_t r = 0; r < nfirst; ++r) {
-            std::vector<std::string> fv;
-            split_record(b, rs, p[r], delim, quote, fv);
-            if (fv.size() != ncol)
-                return fail(c, VDF_ERR_INVALID_ARG, "column number problem at row %llu: %zu fields, %u expected",
-                            (unsigned long long)(r + row_base), fv.size(), ncol);
-            for (uint32_t k = 0; k < ncol && vals[k].size() < 10; ++k) vals[k].push_back(fv[k]);
-            rs = (uint64_t)p[r] + 1;
-            if (p[r] < n && b[p[r]] == '\r' && (uint64_t)p[r] + 1 < n && b[p[r] + 1] == '\n') ++rs;
-        }
+        uint64_t fs = data_start;
+        for (uint32_t r = 0; r < nfirst; ++r)
+            for (uint32_t k = 0; k < ncol; ++k) {
+                const uint64_t fe = p[(size_t)r * ncol + k];
+                if (vals[k].size() < 10)
+                    vals[k].push_back(fe > fs ? std::string((const char*)hb2 + fs, fe - fs) : std::string("NA"));
+                fs = fe + 1;
+                if (k + 1 == ncol && fe < n && hb2[fe] == '\r' && fe + 1 < n && hb2[fe + 1] == '\n') ++fs;
+            }
     }
     std::unique_ptr<vdf_csv> t(new vdf_csv());
     t->device = c->device;
@@ -790,7 +797,6 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
     uint32_t* dbounds = reinterpret_cast<uint32_t*>(t->block + o_bounds);
     e = cudaMemcpyAsync(ddesc, desc.data(), sizeof(CsvColDev) * ncol, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dbounds, bounds.data(), 8 * ncol, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0xff, 8, s);
     if (e != cudaSuccess) {
         cudaFree(t->block);
         t->block = nullptr;
@@ -841,12 +847,6 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
         t->block = nullptr;
         return from_cuda(c, e, "parse");
     }
-    if (sums[0] != ~0ull) {
-        cudaFree(t->block);
-        t->block = nullptr;
-        return fail(c, VDF_ERR_INVALID_ARG, "column number problem at row %llu (%u fields expected)",
-                    (unsigned long long)sums[0], ncol);
-    }
     if (!str_cols.empty()) {
         size_t stotal = 0;
         std::vector<size_t> o_str(str_cols.size());
@@ -875,7 +875,7 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
         }
         if (nrow) {
             begin();
-            k_csv_strings<<<grid_of(nrow, kThreads), kThreads, 0, s>>>(cp);
+            k_csv_strings<<<dim3(grid_of(nrow, kThreads), cp.nstr), kThreads, 0, s>>>(cp);
             end();
             c->launches += 1;
         }
