@@ -33,6 +33,9 @@ int32 payloads.  One vdf_sort_groupby call per step through the C-ABI.
   unique_join  vdf_unique over 100M int64 keys and vdf_left_join_index of 100M
              left rows against 10M right keys, with the oracle's hash walks
              on a 10M-row sample as the CPU baseline.
+  csv        read_csv of a ~1 GiB synthetic airline delay-cause table (the
+             reference's read benchmark shape) from HBM and end to end from
+             pinned host memory, against the reference's own parser.
   (all single-GPU, after the headline measurement; --sections selects them)
 
 --gpus N (launched by torchrun for N > 1) runs N independent replicas, one per
@@ -374,6 +377,115 @@ def unique_join_section(args, local_rank: int) -> dict:
     }
 
 
+def csv_section(args, local_rank: int) -> dict:
+    """CSV ingest (vdf_csv_read) of a ~1 GiB synthetic file shaped like the
+    reference's read benchmark input (benchmarks/readf.cpp:9-21: readf of an
+    airline delay-cause table, delimiter ',', quote '"', header on; its
+    metric is MB/s of file bytes).  `device`: file bytes resident in HBM,
+    CUDA events around each call (outputs allocated inside the call);
+    `e2e`: file bytes in pinned host memory -> vdf_csv_read_host -> every
+    column copied back to pinned host memory; CPU baseline: the reference's
+    own record parser and fast_float (oracle/_ref) on a bounded sample, its
+    per-column conversions on 4 threads as readf<0, 0, 4> asks (its
+    multi-core record parser computes every chunk's end from the first
+    chunk's, standard_parser_mt.inl:30-37, so only the single-core one runs)."""
+    import numpy as np
+    import torch
+
+    import visondf_b200 as vdf
+    from visondf_b200 import datagen
+
+    dev = torch.device("cuda", local_rank)
+    data = datagen.airline_csv(args.csv_bytes)
+    nbytes = len(data)
+    host = torch.from_numpy(np.frombuffer(data, dtype=np.uint8).copy()).pin_memory()
+    dbuf = host.to(dev)
+    ctx = vdf.Context(local_rank)
+    stream = torch.cuda.current_stream()
+    t = ctx.read_csv(dbuf, quote='"')
+    nrow, types = t.nrow, "".join(t.types)
+    out_bytes = sum((8 * nrow if ty == "d" else 4 * nrow if ty == "u" else nrow if ty == "b" else
+                     8 * (nrow + 1) + t.device_column(k)["bytes"]) for k, ty in enumerate(t.types))
+    t.close()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for _ in range(args.warmup):
+        ctx.read_csv(dbuf, quote='"').close()
+    launches0 = ctx.kernel_launches
+    dev_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        tt = ctx.read_csv(dbuf, quote='"')
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dev_ms.append(e0.elapsed_time(e1))
+        tt.close()
+    launches = (ctx.kernel_launches - launches0) / max(1, args.steps)
+    # end to end: pinned host bytes in, every column back in pinned host memory
+    sink = torch.empty(out_bytes + 4096 * (t.ncol + 1), dtype=torch.uint8).pin_memory()
+
+    def e2e_once():
+        tt = ctx.read_csv(host.numpy(), quote='"')
+        o = sink.data_ptr()
+        for k, ty in enumerate(tt.types):
+            dc = tt.device_column(k)
+            if ty in "dub":
+                w = {"d": 8, "u": 4, "b": 1}[ty]
+                tt.copy_column(k, o)
+                o += (w * nrow + 255) // 256 * 256
+            else:
+                tt.copy_column(k, o, o + (dc["bytes"] + 255) // 256 * 256)
+                o += (dc["bytes"] + 255) // 256 * 256 + (8 * (nrow + 1) + 255) // 256 * 256
+        tt.close()
+
+    for _ in range(args.warmup):
+        e2e_once()
+    e2e_ms = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        e0.record(stream)
+        e2e_once()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms.append(e0.elapsed_time(e1))
+    ctx.close()
+    del dbuf
+    torch.cuda.empty_cache()
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, str(ROOT / "tests"))
+        import oracle_bind as ob
+        sample = data[: min(nbytes, 64 << 20)]
+        sample = sample[: sample.rfind(b"\n") + 1]
+        if ob.ref_available():
+            sec = ob.ref_csv_seconds(sample, quote='"', cores=4, reps=2)
+            kind = "reference"
+        else:
+            t0 = time.perf_counter()
+            ob.csv_read(sample, quote='"')
+            sec, kind = time.perf_counter() - t0, "port"
+        cpu = {"value": len(sample) / sec / 1e9, "unit": "GB/s", "cores": 4 if kind == "reference" else 1,
+               "kind": kind, "sample": f"first {len(sample) / 1e6:.1f} MB of the same file; host CPU: {cpu_info()}"}
+    d_best, e_best = min(dev_ms), min(e2e_ms)
+    algo = nbytes + out_bytes
+    peak, peak_kind = measured_peaks()
+    return {
+        "workload": f"read_csv of a {nbytes / 1e6:.0f} MB synthetic airline delay-cause table "
+                    f"({nrow:,} rows, 21 columns: 2 unsigned, 4 strings, 15 two-decimal numbers), ',' / '\"' / header",
+        "bytes": nbytes, "rows": nrow, "types": types, "unit": "GB/s",
+        "device": {"ms": d_best, "ms_median": float(np.median(dev_ms)), "value": nbytes / (d_best / 1e3) / 1e9,
+                   "gpu_launches": launches},
+        "e2e": {"ms": e_best, "value": nbytes / (e_best / 1e3) / 1e9, "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": out_bytes},
+        "roofline": {"bound": "hbm", "algorithmic_bytes": algo, "achieved": algo / (d_best / 1e3) / 1e9,
+                     "peak": peak, "peak_kind": peak_kind, "frac": algo / (d_best / 1e3) / 1e9 / peak,
+                     "note": "file read once + columns written once; the parse is instruction-bound"},
+        "cpu_baseline": cpu,
+        "speedup_vs_cpu": (nbytes / (d_best / 1e3) / 1e9) / cpu["value"] if cpu else None,
+        "e2e_speedup_vs_cpu": (nbytes / (e_best / 1e3) / 1e9) / cpu["value"] if cpu else None,
+    }
+
+
 def served_section(args, local_rank: int) -> dict:
     """Poisson request stream over resident columns: continuous batching with
     HBM-budget admission, against one library call per request."""
@@ -666,13 +778,15 @@ def our_arm(args, rank: int, world: int, local_rank: int):
     del d, outs, packed, keys, payload
     torch.cuda.empty_cache()
     sections = set(args.sections.split(","))
-    batched = served = unique_join = None
+    batched = served = unique_join = csv_res = None
     if world == 1 and "batched" in sections:
         batched = batched_section(args, local_rank)
     if world == 1 and "served" in sections:
         served = served_section(args, local_rank)
     if world == 1 and "unique_join" in sections:
         unique_join = unique_join_section(args, local_rank)
+    if world == 1 and "csv" in sections:
+        csv_res = csv_section(args, local_rank)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -694,6 +808,7 @@ def our_arm(args, rank: int, world: int, local_rank: int):
             "batched": batched,
             "served": served,
             "unique_join": unique_join,
+            "csv": csv_res,
         }
         print(json.dumps(line), flush=True)
 
@@ -711,7 +826,8 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the library's default kernel variants")
     ap.add_argument("--variants", type=int, nargs=2, metavar=("V32", "V64"),
                     help="with --no-autotune: radix-pass variant indices for 4- and 8-byte keys")
-    ap.add_argument("--sections", default="batched,served,unique_join",
+    ap.add_argument("--csv-bytes", type=int, default=1 << 30, help="size of the synthetic CSV file (csv section)")
+    ap.add_argument("--sections", default="batched,served,unique_join,csv",
                     help="extra single-GPU measurements after the headline one: batched, served, unique_join "
                          "(comma list, 'none' for none)")
     ap.add_argument("--batch-queries", type=int, default=4096)

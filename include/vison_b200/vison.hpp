@@ -13,13 +13,17 @@
 //   transform_unique[_mt]         transform/transform_unique/transform_unique_mt.hpp:3-11
 //   transform_left_join[_mt]      transform/transform_left_join/transform_left_join_mt.hpp:3-15
 //                                 (methods First, Last and Aligned)
+//   readf                         read/read_csv/read_csv.hpp:3-216 (called as readf in
+//                                 benchmarks/readf.cpp:21): the file is parsed on the GPU
+//                                 (vdf_csv_read_host) into the frame's type blocks
 //
 // Storage follows the reference: column-major type blocks (here int_v, uint_v,
 // dbl_v plus 64-bit integer blocks lint_v / luint_v, which the reference lacks:
 // it has one signed width per frame, so an int32 key and an int64 value cannot
 // share a frame), a per-column type char, and a lazy row view (row_view_idx +
-// in_view) that Soft sorts set and materialize() applies.  String, char and
-// bool columns are not part of this path.
+// in_view) that Soft sorts set and materialize() applies.  String ('s'),
+// one-byte string ('c') and bool ('b') columns come from readf; they are kept,
+// viewed and permuted with the frame but are not sort or group-by keys here.
 //
 // Template parameters that tune the reference's CPU code (CORES, Simd,
 // SortType, comparator factories, SimdHash, MapCol, NPerGroup) are accepted
@@ -133,6 +137,8 @@ class Dataframe {
     std::vector<std::vector<FloatT>> dbl_v;    // 'd'
     std::vector<std::vector<LIntT>> lint_v;    // 'l' (extension)
     std::vector<std::vector<LUIntT>> luint_v;  // 'L' (extension)
+    std::vector<std::vector<std::string>> str_v;  // 's' and 'c'
+    std::vector<std::vector<uint8_t>> bool_v;     // 'b'
     std::vector<char> type_refv;               // type char of each column
     std::vector<unsigned int> slot_v;          // index of each column inside its type block
     std::vector<std::string> name_v;
@@ -153,12 +159,87 @@ class Dataframe {
         else if constexpr (std::is_same_v<T, FloatT>) { t = 'd'; slot = (unsigned)dbl_v.size(); dbl_v.push_back(std::move(v)); }
         else if constexpr (std::is_same_v<T, LIntT>) { t = 'l'; slot = (unsigned)lint_v.size(); lint_v.push_back(std::move(v)); }
         else if constexpr (std::is_same_v<T, LUIntT>) { t = 'L'; slot = (unsigned)luint_v.size(); luint_v.push_back(std::move(v)); }
+        else if constexpr (std::is_same_v<T, std::string>) { t = 's'; slot = (unsigned)str_v.size(); str_v.push_back(std::move(v)); }
+        else if constexpr (std::is_same_v<T, uint8_t>) { t = 'b'; slot = (unsigned)bool_v.size(); bool_v.push_back(std::move(v)); }
         else { static_assert(!sizeof(T), "unsupported column type"); }
         type_refv.push_back(t);
         slot_v.push_back(slot);
         name_v.push_back(name.empty() ? "col" + std::to_string(ncol + 1) : std::move(name));
         ++ncol;
     }
+
+    // ---- CSV ingest --------------------------------------------------------------
+    // read_csv / readf: replaces the frame with the file's columns, parsed on
+    // the GPU.  strt_row / end_row other than 0 keep records [strt_row, end_row)
+    // (end_row 0: to the end); CORES, WARMING, MEM_CLEAN and TrailingChar tune
+    // the reference's CPU parser and are accepted and ignored.  Errors (file
+    // not found, a record with another field count) go to std::cerr and leave
+    // the frame empty.
+    template <unsigned int strt_row = 0, unsigned int end_row = 0, unsigned int CORES = 1, bool WARMING = 0,
+              bool MEM_CLEAN = 0, char TrailingChar = '0'>
+    void readf(std::string& file_name, char delim = ',', bool header_name = 1, char str_context = '\'') {
+        *this = Dataframe();
+        std::FILE* f = std::fopen(file_name.c_str(), "rb");
+        if (!f) {
+            std::cerr << "Failed to open file: " << file_name << "\n";
+            return;
+        }
+        std::vector<char> bytes;
+        char chunk[1 << 16];
+        size_t got;
+        while ((got = std::fread(chunk, 1, sizeof chunk, f)) > 0) bytes.insert(bytes.end(), chunk, chunk + got);
+        std::fclose(f);
+        vdf_csv* t = nullptr;
+        if (!detail::report(vdf_csv_read_host(context(), bytes.data(), bytes.size(), delim, header_name ? 1 : 0,
+                                              str_context, &t, nullptr),
+                            "readf"))
+            return;
+        const uint64_t n = vdf_csv_nrow(t);
+        const uint64_t r0 = strt_row < n ? strt_row : n;
+        const uint64_t r1 = (end_row == 0 || end_row > n) ? n : (end_row < r0 ? r0 : end_row);
+        bool ok = true;
+        for (uint32_t c = 0; c < vdf_csv_ncol(t) && ok; ++c) {
+            const char ty = vdf_csv_type(t, c);
+            std::string name = vdf_csv_name(t, c);
+            if (ty == 'd' || ty == 'u' || ty == 'b') {
+                const size_t w = ty == 'd' ? 8 : ty == 'u' ? 4 : 1;
+                std::vector<unsigned char> raw(w * n);
+                ok = detail::report(vdf_csv_copy_column(context(), t, c, raw.data(), nullptr, nullptr), "readf");
+                auto cut = [&](auto* p, auto& block) {
+                    block.emplace_back(p + r0, p + r1);
+                };
+                if (ty == 'd') cut(reinterpret_cast<const double*>(raw.data()), dbl_v);
+                else if (ty == 'u') cut(reinterpret_cast<const uint32_t*>(raw.data()), uint_v);
+                else cut(raw.data(), bool_v);
+                slot_v.push_back(ty == 'd' ? (unsigned)dbl_v.size() - 1 : ty == 'u' ? (unsigned)uint_v.size() - 1
+                                                                                     : (unsigned)bool_v.size() - 1);
+            } else {
+                std::vector<unsigned char> data(vdf_csv_string_bytes(t, c) + 1);
+                std::vector<uint64_t> off(n + 1);
+                ok = detail::report(vdf_csv_copy_column(context(), t, c, data.data(), off.data(), nullptr), "readf");
+                std::vector<std::string> col;
+                col.reserve(r1 - r0);
+                for (uint64_t r = r0; r < r1; ++r)
+                    col.emplace_back(reinterpret_cast<const char*>(data.data()) + off[r], off[r + 1] - off[r]);
+                str_v.push_back(std::move(col));
+                slot_v.push_back((unsigned)str_v.size() - 1);
+            }
+            type_refv.push_back(ty);
+            name_v.push_back(std::move(name));
+        }
+        vdf_csv_free(t);
+        if (!ok) {
+            *this = Dataframe();
+            return;
+        }
+        ncol = (unsigned int)type_refv.size();
+        nrow = (unsigned int)(r1 - r0);
+    }
+
+    const std::vector<char>& get_typecol() const { return type_refv; }
+    void reinitiate() { *this = Dataframe(); }  // vison.hpp: back to an empty frame
+    unsigned int get_nrow() const { return nrow; }
+    unsigned int get_ncol() const { return ncol; }
 
     // Column n as currently viewed (through row_view_idx when in view).
     template <typename T>
@@ -187,6 +268,10 @@ class Dataframe {
         }
         if (n >= ncol) {
             std::cerr << "Column not found\n";
+            return;
+        }
+        if (!numeric(n)) {
+            std::cerr << "sort_by: string and bool columns are not sort keys on the GPU path\n";
             return;
         }
         vdf_col key = col_desc(n);
@@ -280,7 +365,15 @@ class Dataframe {
                     std::cerr << "Column not found\n";
                     return;
                 }
+                if (!numeric(c)) {
+                    std::cerr << "transform_group_by: string and bool columns are not keys on the GPU path\n";
+                    return;
+                }
                 keys.push_back(col_desc(c));
+            }
+            if (!numeric(n_col)) {
+                std::cerr << "transform_group_by: string and bool columns are not value columns on the GPU path\n";
+                return;
             }
             const vdf_col val = col_desc(n_col);
             int32_t fn = VDF_AGG_COUNT;
@@ -335,6 +428,10 @@ class Dataframe {
             std::cerr << "Column not found\n";
             return;
         }
+        if (!numeric(n)) {
+            std::cerr << "transform_unique: string and bool columns are not keys on the GPU path\n";
+            return;
+        }
         if (in_view) materialize();
         std::vector<uint8_t> keep(nrow);
         uint64_t distinct = 0;
@@ -365,8 +462,6 @@ class Dataframe {
                                 const uint8_t default_bool = 0, const IntT default_int = 0,
                                 const UIntT default_uint = 0, const FloatT default_dbl = 0) {
         (void)default_chr;
-        (void)default_str;
-        (void)default_bool;
         if (in_view) {
             std::cerr << "Can't perform this operation while in`view` mode, consider applying `.materialize()`\n";
             return;
@@ -374,6 +469,10 @@ class Dataframe {
         {
             if (key1 >= ncol || key2 >= obj.ncol) {
                 std::cerr << "Column not found\n";
+                return;
+            }
+            if (!numeric(key1) || !obj.numeric(key2)) {
+                std::cerr << "transform_left_join: string and bool columns are not keys on the GPU path\n";
                 return;
             }
             if (type_refv[key1] != obj.type_refv[key2]) {
@@ -407,6 +506,8 @@ class Dataframe {
                 case 'u': join(right.uint_v[s], default_uint); break;
                 case 'd': join(right.dbl_v[s], default_dbl); break;
                 case 'l': join(right.lint_v[s], (LIntT)default_int); break;
+                case 's': case 'c': join(right.str_v[s], default_str); break;
+                case 'b': join(right.bool_v[s], default_bool); break;
                 default: join(right.luint_v[s], (LUIntT)default_uint); break;
                 }
             }
@@ -437,6 +538,8 @@ class Dataframe {
             case 'u': go(uint_v[s]); break;
             case 'd': go(dbl_v[s]); break;
             case 'l': go(lint_v[s]); break;
+            case 's': case 'c': go(str_v[s]); break;
+            case 'b': go(bool_v[s]); break;
             default: go(luint_v[s]); break;
             }
         }
@@ -455,8 +558,15 @@ class Dataframe {
         case 'd': if constexpr (std::is_same_v<T, FloatT>) return &dbl_v[s]; break;
         case 'l': if constexpr (std::is_same_v<T, LIntT>) return &lint_v[s]; break;
         case 'L': if constexpr (std::is_same_v<T, LUIntT>) return &luint_v[s]; break;
+        case 's': case 'c': if constexpr (std::is_same_v<T, std::string>) return &str_v[s]; break;
+        case 'b': if constexpr (std::is_same_v<T, uint8_t>) return &bool_v[s]; break;
         }
         return nullptr;
+    }
+
+    bool numeric(unsigned int n) const {
+        const char t = type_refv[n];
+        return t == 'i' || t == 'u' || t == 'd' || t == 'l' || t == 'L';
     }
 
     vdf_col col_desc(unsigned int n) const {
@@ -492,8 +602,19 @@ class Dataframe {
     }
 
     void permute_col(unsigned int c, const std::vector<uint32_t>& perm) {
-        vdf_col in = col_desc(c);
         const unsigned s = slot_v[c];
+        if (!numeric(c)) {  // strings and bools: permuted on the host
+            auto host = [&](auto& vec) {
+                using V = typename std::decay_t<decltype(vec)>::value_type;
+                std::vector<V> out(nrow);
+                for (unsigned int r = 0; r < nrow; ++r) out[r] = vec[perm[r]];
+                vec.swap(out);
+            };
+            if (type_refv[c] == 'b') host(bool_v[s]);
+            else host(str_v[s]);
+            return;
+        }
+        vdf_col in = col_desc(c);
         auto go = [&](auto& vec) {
             using V = typename std::decay_t<decltype(vec)>::value_type;
             std::vector<V> out(nrow);

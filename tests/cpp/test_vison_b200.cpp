@@ -231,6 +231,39 @@ static void test_transform_left_join() {
     }
 }
 
+static void test_readf() {
+    // a small file with every inferred kind: 'u', 'd', 's' (quoted delimiter),
+    // 'c', 'b'; CR LF line ends; an empty string field reads "NA"
+    const char* text =
+        "year,delay,name,code,flag\r\n"
+        "2003,1.50,alpha,A,0\r\n"
+        "2004,2.25,\"b, c\",B,1\r\n"
+        "2005,1e3,,C,1\r\n";
+    std::string path = "/tmp/vison_b200_readf_test.csv";
+    std::FILE* f = std::fopen(path.c_str(), "wb");
+    std::fputs(text, f);
+    std::fclose(f);
+    vison_b200::Dataframe df;
+    df.readf<0, 0, 4, 0, 0>(path, ',', true, '"');
+    CHECK(df.get_nrow() == 3 && df.get_ncol() == 5);
+    CHECK((df.get_typecol() == std::vector<char>{'u', 'd', 's', 'c', 'b'}));
+    CHECK((df.name_v == std::vector<std::string>{"year", "delay", "name", "code", "flag"}));
+    CHECK((df.get_col<unsigned>(0) == std::vector<unsigned>{2003, 2004, 2005}));
+    CHECK((df.get_col<double>(1) == std::vector<double>{1.5, 2.25, 1000.0}));
+    CHECK((df.get_col<std::string>(2) == std::vector<std::string>{"alpha", "\"b, c\"", "NA"}));
+    CHECK((df.get_col<std::string>(3) == std::vector<std::string>{"A", "B", "C"}));
+    CHECK((df.get_col<uint8_t>(4) == std::vector<uint8_t>{0, 1, 1}));
+    // a Hard sort by the double column permutes the string columns with it
+    unsigned int k = 1;
+    df.sort_by<0, void, true, false>(k);
+    CHECK((df.get_col<std::string>(2) == std::vector<std::string>{"NA", "\"b, c\"", "alpha"}));
+    // rows [1, 2) only
+    vison_b200::Dataframe part;
+    part.readf<1, 2>(path, ',', true, '"');
+    CHECK(part.get_nrow() == 1 && part.get_col<unsigned>(0) == std::vector<unsigned>{2004});
+    std::remove(path.c_str());
+}
+
 int main() {
     test_doc_example();
     test_hard_sort_and_view_composition();
@@ -238,6 +271,7 @@ int main() {
     test_transform_group_by();
     test_transform_unique();
     test_transform_left_join();
+    test_readf();
     if (failures) {
         std::fprintf(stderr, "%d checks failed\n", failures);
         return 1;

@@ -11,7 +11,8 @@ The library is loaded on first use of any binding name (so `build` and
 there is no CPU fallback.
 """
 _EXPORTS = {"Context", "GroupResult", "VdfError", "lib", "LIB_PATH", "I32", "I64", "U32", "U64", "F64", "F32",
-            "ORDER_ASC", "ORDER_DESC_STABLE", "ORDER_DESC_REVERSE", "KERNEL_CLASSES", "Batch", "QueryResult"}
+            "ORDER_ASC", "ORDER_DESC_STABLE", "ORDER_DESC_REVERSE", "KERNEL_CLASSES", "Batch", "QueryResult",
+            "CsvTable"}
 
 __all__ = sorted(_EXPORTS)
 

@@ -497,6 +497,12 @@ class CsvTable:
 
     _TORCH = {"d": torch.float64, "u": torch.int32, "b": torch.uint8}
 
+    def copy_column(self, k: int, values: int, offsets: Optional[int] = None, stream=None):
+        """Copies column k into caller memory (host or device addresses):
+        the values (or string bytes) and, for strings, nrow + 1 offsets."""
+        self._ctx._check(lib.vdf_csv_copy_column(self._ctx.handle, self.handle, k, values, offsets,
+                                                 _stream(stream)), "vdf_csv_copy_column")
+
     def tensor(self, k: int, stream=None) -> torch.Tensor:
         """Numeric column k copied into a new CUDA tensor (uint32 columns as
         int32 bit patterns)."""

@@ -170,3 +170,31 @@ def stream_specs(n_requests: int, rate_per_s: float, median_rows: float = 1e6, s
     n = np.minimum(cap_rows, np.maximum(1, np.floor(rng.lognormal(np.log(median_rows), sigma, size=n_requests))))
     return [dict(t=float(t[i]), n=int(n[i]), dtype=np.int32, card=int(min(10_000, n[i])),
                  seed=int(rng.integers(0, 2**62))) for i in range(n_requests)]
+
+
+def airline_csv(target_bytes: int = 1 << 30, seed_: int = 1, block_rows: int = 200_000) -> bytes:
+    """A CSV file shaped like the reference's read benchmark input
+    (benchmarks/readf.cpp:9, an airline delay-cause table: 21 columns -- year
+    and month, a carrier code and name, an airport code and name, 15 counts
+    and delay minutes with two decimals), synthetic and seeded: names with a
+    comma come quoted with '"'.  One block of `block_rows` rows is generated
+    and repeated up to about `target_bytes`; the header comes first."""
+    rng = np.random.default_rng(seed_)
+    n = block_rows
+    carriers = np.array(["AA", "DL", "UA", "WN", "B6", "AS", "NK", "F9"])
+    cnames = np.array(["Alpha Air Inc.", "Beta Air Lines Inc.", '"Gamma Air, Inc."', "Delta Wings Co."])
+    airports = np.array(["AAA", "BBB", "CCC", "DDD", "EEE", "FFF", "GGG", "HHH"])
+    anames = np.array(['"Aton, GA: Aton Municipal"', '"Bexley, IL: Bexley International"',
+                       '"Corin, TX: Corin Regional"', '"Dover, CO: Dover Field"'])
+    cols = [rng.integers(2003, 2025, n).astype(str), rng.integers(1, 13, n).astype(str),
+            carriers[rng.integers(0, 8, n)], cnames[rng.integers(0, 4, n)],
+            airports[rng.integers(0, 8, n)], anames[rng.integers(0, 4, n)]]
+    for k in range(15):
+        cols.append(np.char.mod("%.2f", np.round(rng.exponential(50.0 * (k + 1), n), 2)))
+    rows = cols[0]
+    for c in cols[1:]:
+        rows = np.char.add(np.char.add(rows, ","), c)
+    block = ("\n".join(rows.tolist()) + "\n").encode()
+    header = ("year,month,carrier,carrier_name,airport,airport_name,"
+              + ",".join(f"delay_{k}" for k in range(15)) + "\n").encode()
+    return header + block * max(1, target_bytes // len(block))
