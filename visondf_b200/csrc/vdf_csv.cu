@@ -45,6 +45,7 @@ struct vdf_csv {
     std::vector<uint64_t> str_bytes;  // string bytes per column
     unsigned char* block = nullptr;   // numeric values + offsets + start arrays
     unsigned char* sblock = nullptr;  // string bytes
+    bool pooled = false, spooled = false;  // from the stream-ordered pool (else cudaMalloc)
 };
 
 namespace {
@@ -238,6 +239,7 @@ __global__ void __launch_bounds__(kThreads) k_csv_fields(const uint8_t* __restri
     uint32_t tot;
     uint32_t off = tile_first[blockIdx.x] + block_sum_excl(__popcll(ev), s_w, tot);
     const uint32_t last = *total - 1;
+    uint32_t col = ev ? off % ncol : 0;  // column of field `off`, advanced without dividing
     while (ev) {
         const int b = __ffsll((long long)ev) - 1;
         ev &= ev - 1;
@@ -248,7 +250,8 @@ __global__ void __launch_bounds__(kThreads) k_csv_fields(const uint8_t* __restri
         }
         pos[off] = p;
         const bool is_term = (m.term >> b) & 1;
-        if (is_term != (off % ncol == ncol - 1)) atomicMin(bad_row, (unsigned long long)(off / ncol + row_base));
+        if (is_term != (col == ncol - 1)) atomicMin(bad_row, (unsigned long long)(off / ncol + row_base));
+        col = col + 1 == ncol ? 0 : col + 1;
         if (off == last) {
             uint32_t next = 0xffffffffu;
             if (is_term) {
@@ -488,24 +491,84 @@ __global__ void __launch_bounds__(kThreads) k_csv_strings(StrCopy sc) {
     const uint64_t rend = r0 + 32 < sc.nrow ? r0 + 32 : sc.nrow;
     const uint64_t span = off[rend] - o0;
     uint8_t* dst = sc.bytes[k];
-    for (uint64_t b = 0; b < span; b += 32) {  // the same trip count in every lane
-        const uint64_t d = b + lane;
-        const uint64_t at = o0 + (d < span ? d : span - 1);
-        // largest j with off[r0 + j] <= at (lanes past the end hold the end offset)
-        int j = 0;
+    constexpr int U = 4;  // output bytes per lane per round: all U sources located, then loaded, then stored
+    for (uint64_t b = 0; b < span; b += 32 * U) {  // the same trip count in every lane
+        uint32_t src[U];
+        bool na[U];
+        uint8_t val[U];
 #pragma unroll
-        for (int step = 16; step; step >>= 1) {
-            const uint64_t oj = __shfl_sync(0xffffffffu, o, j + step);
-            if (oj <= at) j += step;
+        for (int u = 0; u < U; ++u) {
+            const uint64_t d = b + (uint64_t)u * 32 + lane;
+            const uint64_t at = o0 + (d < span ? d : span - 1);
+            // largest j with off[r0 + j] <= at (lanes past the end hold the end offset)
+            int j = 0;
+#pragma unroll
+            for (int step = 16; step; step >>= 1) {
+                const uint64_t oj = __shfl_sync(0xffffffffu, o, j + step);
+                if (oj <= at) j += step;
+            }
+            const uint64_t oj = __shfl_sync(0xffffffffu, o, j);
+            const uint32_t sj = __shfl_sync(0xffffffffu, s, j);
+            const uint32_t i = (uint32_t)(at - oj);
+            na[u] = sj == 0xffffffffu;
+            src[u] = na[u] ? i : sj + i;  // for "NA": the byte's index in "NA"
         }
-        const uint64_t oj = __shfl_sync(0xffffffffu, o, j);
-        const uint32_t sj = __shfl_sync(0xffffffffu, s, j);
-        const uint32_t i = (uint32_t)(at - oj);
-        if (d < span) dst[at] = sj == 0xffffffffu ? (i == 0 ? 'N' : 'A') : __ldg(sc.buf + sj + i);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            val[u] = na[u] ? (src[u] ? 'A' : 'N') : __ldg(sc.buf + src[u]);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint64_t d = b + (uint64_t)u * 32 + lane;
+            if (d < span) dst[o0 + d] = val[u];
+        }
     }
 }
 
 // ---------------------------------------------------------------- host side
+// Table blocks come from a stream-ordered pool per device that keeps up to
+// 8 GiB cached between reads (a fresh cudaMalloc of the ~1.5 GB a 1 GB file
+// needs costs about a millisecond).
+cudaMemPool_t table_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    std::lock_guard<std::mutex> lk(mu);
+    if (device < 0 || device >= 64) return nullptr;
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = 8ull << 30;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = p;
+    }
+    return pools[device];
+}
+
+cudaError_t table_alloc(int device, unsigned char** p, size_t bytes, cudaStream_t s, bool& pooled) {
+    cudaMemPool_t pool = table_pool(device);
+    pooled = pool != nullptr;
+    if (!pool) return cudaMalloc(p, bytes);
+    return cudaMallocFromPoolAsync(reinterpret_cast<void**>(p), bytes, pool, s);
+}
+
+// Frees a table block once no work can still use it (cudaFree's guarantee).
+void table_free(unsigned char*& p, bool pooled) {
+    if (!p) return;
+    if (pooled) {
+        cudaDeviceSynchronize();
+        cudaFreeAsync(p, 0);
+    } else {
+        cudaFree(p);
+    }
+    p = nullptr;
+}
+
 // The reference's first-line pass (read_csv.hpp:58-135): splits at the
 // delimiter outside quotes and stops at the first CR or LF even inside
 // quotes; a CR or LF followed by LF moves the stop onto that LF, so the last
@@ -766,7 +829,7 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
     size_t o_part = total;
     const uint32_t nblk = (uint32_t)((nrow + kScanRows - 1) / kScanRows);
     total += align256(8 * (size_t)nblk * (str_cols.empty() ? 1 : str_cols.size()) + 8);
-    e = cudaMalloc(&t->block, total);
+    e = table_alloc(c->device, &t->block, total, s, t->pooled);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(c, VDF_ERR_OOM, "column allocation of %zu bytes failed", total);
@@ -798,8 +861,7 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
     e = cudaMemcpyAsync(ddesc, desc.data(), sizeof(CsvColDev) * ncol, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dbounds, bounds.data(), 8 * ncol, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) {
-        cudaFree(t->block);
-        t->block = nullptr;
+        table_free(t->block, t->pooled);
         return from_cuda(c, e, "column descriptors");
     }
     // ---- parse
@@ -843,8 +905,7 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
         e = cudaMemcpyAsync(&sums[k + 1], t->offsets[str_cols[k]] + nrow, 8, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
-        cudaFree(t->block);
-        t->block = nullptr;
+        table_free(t->block, t->pooled);
         return from_cuda(c, e, "parse");
     }
     if (!str_cols.empty()) {
@@ -855,11 +916,10 @@ vdf_status csv_read_locked(vdf_ctx* c, const uint8_t* dbuf, const uint8_t* hbuf,
             stotal += align256(sums[k + 1] ? sums[k + 1] : 1);
             t->str_bytes[str_cols[k]] = sums[k + 1];
         }
-        e = cudaMalloc(&t->sblock, stotal);
+        e = table_alloc(c->device, &t->sblock, stotal, s, t->spooled);
         if (e != cudaSuccess) {
             cudaGetLastError();
-            cudaFree(t->block);
-            t->block = nullptr;
+            table_free(t->block, t->pooled);
             return fail(c, VDF_ERR_OOM, "string allocation of %zu bytes failed", stotal);
         }
         StrCopy cp;
@@ -968,8 +1028,8 @@ void vdf_csv_free(vdf_csv* t) {
     if (!t) return;
     {
         DeviceGuard g(t->device);
-        if (t->block) cudaFree(t->block);
-        if (t->sblock) cudaFree(t->sblock);
+        table_free(t->block, t->pooled);
+        table_free(t->sblock, t->spooled);
     }
     delete t;
 }
