@@ -7,7 +7,7 @@
 // Device pipeline over the file bytes in HBM (positions are 32-bit, files
 // below 4 GiB):
 //   1. k_csv_count: each thread takes 64 bytes, builds bit masks of quote,
-//      CR and LF bytes (SWAR compares), the in-quote state as a prefix XOR of
+//      CR and LF bytes (SWAR zero-byte tests), the in-quote state as a prefix XOR of
 //      the quote mask, and counts record terminators outside quotes (a CR, or
 //      an LF not right after a CR) for both possible starting states; per
 //      16 KB tile: quote parity and the two counts;
@@ -54,10 +54,19 @@ constexpr int kThreads = 256;
 constexpr int kChunk = 64;                     // bytes per thread in the split passes
 constexpr int kTileBytes = kThreads * kChunk;  // 16 KB
 
-__device__ __forceinline__ uint32_t nibble(uint32_t eq) {
-    // the top bit of each of the four bytes -> four bits (products land on
-    // distinct bit positions, so no carries)
-    return ((eq & 0x80808080u) * 0x00204081u) >> 28;
+// Top bit of each byte of w set exactly where that byte equals the byte of
+// `pat` (x = w ^ pat is zero there): adding 0x7f to the low seven bits sets
+// the top bit of every byte whose low bits are nonzero and never carries
+// into the next byte.
+__device__ __forceinline__ uint32_t eq_bytes(uint32_t w, uint32_t pat) {
+    const uint32_t x = w ^ pat;
+    return ~(((x & 0x7f7f7f7fu) + 0x7f7f7f7fu) | x | 0x7f7f7f7fu);
+}
+
+__device__ __forceinline__ uint32_t nibble(uint32_t top) {
+    // the top bits of the four bytes (only those set) -> four bits; the
+    // products land on distinct bit positions, so no carries
+    return (top * 0x00204081u) >> 28;
 }
 
 __device__ __forceinline__ uint64_t prefix_xor(uint64_t x) {
@@ -104,10 +113,10 @@ __device__ __forceinline__ Masks chunk_masks(const uint8_t* __restrict__ buf, ui
     uint64_t q = 0, cr = 0, lf = 0, dl = 0;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-        q |= (uint64_t)nibble(__vcmpeq4(w[k], quote4)) << (4 * k);
-        dl |= (uint64_t)nibble(__vcmpeq4(w[k], delim4)) << (4 * k);
-        cr |= (uint64_t)nibble(__vcmpeq4(w[k], 0x0d0d0d0du)) << (4 * k);
-        lf |= (uint64_t)nibble(__vcmpeq4(w[k], 0x0a0a0a0au)) << (4 * k);
+        q |= (uint64_t)nibble(eq_bytes(w[k], quote4)) << (4 * k);
+        dl |= (uint64_t)nibble(eq_bytes(w[k], delim4)) << (4 * k);
+        cr |= (uint64_t)nibble(eq_bytes(w[k], 0x0d0d0d0du)) << (4 * k);
+        lf |= (uint64_t)nibble(eq_bytes(w[k], 0x0a0a0a0au)) << (4 * k);
     }
     uint64_t valid = ~0ull;
     if (start > base) valid = (start - base >= 64) ? 0 : (~0ull << (start - base));
