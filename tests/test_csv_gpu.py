@@ -140,3 +140,20 @@ def test_columns_feed_the_sort(ctx):
     exp = np.argsort(r.columns[0].astype(np.int64), kind="stable")
     assert (perm.cpu().numpy().astype(np.int64) == exp).all()
     assert t.tensor(1).cpu().numpy().tobytes() == r.columns[1].tobytes()
+
+
+def test_zero_copy_views_feed_the_group_by(ctx):
+    """read_csv -> sort + group-by on the parsed columns in place (no copies)."""
+    data = csv_gen.make_csv(11, 30_000, kinds=["u", "d", "d"], quote='"')
+    t = read(ctx, data, True, quote='"')
+    r = ob.csv_read(data, quote='"')
+    key, val = t.view(0), t.view(1)
+    assert key.dtype == torch.uint32 and val.dtype == torch.float64
+    assert key.data_ptr() == t.device_column(0)["values"]
+    gr = ctx.sort_groupby([key], [val], agg_cols=[0])
+    og = ob.groupby([r.columns[0]], [r.columns[1]])
+    assert gr.n_groups == og.n_groups
+    assert (gr.keys[0].cpu().numpy() == og.keys[0]).all()
+    assert (gr.count.cpu().numpy() == og.count).all()
+    del t   # the views keep the table's memory alive
+    assert (key.cpu().numpy() == r.columns[0]).all()

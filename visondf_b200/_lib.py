@@ -497,6 +497,29 @@ class CsvTable:
 
     _TORCH = {"d": torch.float64, "u": torch.int32, "b": torch.uint8}
 
+    _TYPESTR = {"d": "<f8", "u": "<u4", "b": "|u1"}
+
+    def view(self, k: int) -> torch.Tensor:
+        """Numeric column k as a CUDA tensor over the table's own memory (no
+        copy; the tensor keeps the table alive): parsed columns go straight
+        into the sort and group-by; writes through it change the table.
+        uint32 columns come back as torch.uint32."""
+        ty = self.types[k]
+        if ty not in self._TYPESTR:
+            raise ValueError("string columns have no tensor view")
+        table = self
+
+        class _Col:
+            __cuda_array_interface__ = {"shape": (self.nrow,), "typestr": self._TYPESTR[ty],
+                                        "data": (int(lib.vdf_csv_values(self.handle, k) or 0), False),
+                                        "version": 3, "strides": None}
+            owner = table
+
+        holder = _Col()
+        t = torch.as_tensor(holder, device=f"cuda:{self._ctx.device}")
+        t._vdf_owner = holder  # the table outlives the view
+        return t
+
     def copy_column(self, k: int, values: int, offsets: Optional[int] = None, stream=None):
         """Copies column k into caller memory (host or device addresses):
         the values (or string bytes) and, for strings, nrow + 1 offsets."""
