@@ -117,7 +117,14 @@ def random_strings(seed: int, count: int) -> list[str]:
     alpha = "0123456789.-+eEnaifNAIF x"
     out = []
     for _ in range(count):
-        k = rng.randrange(6)
+        k = rng.randrange(7)
+        if k == 6:   # short decimals, the CSV-typical shape, with odd tails
+            s = "".join(rng.choice("0123456789") for _ in range(rng.randrange(0, 10)))
+            if rng.random() < 0.7:
+                s += "." + "".join(rng.choice("0123456789") for _ in range(rng.randrange(0, 10)))
+            s += rng.choice(["", "", "", "x", "e5", "E-2", ".", "-", " "])
+            out.append(("-" if rng.random() < 0.2 else "") + s)
+            continue
         if k == 0:
             s = "".join(rng.choice("0123456789") for _ in range(rng.randrange(1, 25)))
             if rng.random() < 0.5:
@@ -165,15 +172,19 @@ def oracle_bits(s: str) -> str:
 def test_device_decimal_code_matches_oracle(decimal_check, kind):
     strings = random_strings(3, 20000) if kind == "random" else hard_strings(5, 2000)
     rows = run_check(decimal_check, strings)
-    slow = 0
-    for s, (bits, u, i, path) in zip(strings, rows):
+    slow = fast = 0
+    for s, (bits, u, i, path, scan) in zip(strings, rows):
         assert path != "2", s
+        assert scan != "2", s   # the eight-byte scan gives the general scan's result
         slow += path == "1"
+        fast += scan == "1"
         assert bits == oracle_bits(s), s
         assert int(u) == ob.parse_u32(s.encode()), s
         assert int(i) == ob.parse_i32(s.encode()), s
     if kind == "halfway":
         assert slow > len(strings) // 2   # the exact decision is exercised
+    else:
+        assert fast > len(strings) // 10  # the eight-byte scan is exercised
 
 
 @pytest.mark.skipif(not ob.ref_available(), reason="reference shim not built")

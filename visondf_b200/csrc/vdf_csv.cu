@@ -304,6 +304,26 @@ struct Reader {
         const uint32_t word = k < 8 ? (k < 4 ? w0 : w1) : (k < 12 ? w2 : w3);
         return (unsigned char)(word >> ((k & 3) * 8));
     }
+    // The 8 bytes at i (byte i lowest), those at and past i + avail zeroed.
+    __device__ __forceinline__ uint64_t get8(uint64_t i, uint32_t avail) {
+        get(i);  // window holding byte i
+        const uint32_t k = (uint32_t)(i & 15);
+        const uint64_t lo = (uint64_t)w0 | ((uint64_t)w1 << 32), hi = (uint64_t)w2 | ((uint64_t)w3 << 32);
+        uint64_t v;
+        if (k == 0) v = lo;
+        else if (k < 8) v = (lo >> (8 * k)) | (hi << (64 - 8 * k));
+        else if (k == 8) v = hi;
+        else {
+            v = hi >> (8 * (k - 8));
+            if (avail > 16 - k) {  // the rest is in the next window
+                get(i + (16 - k));
+                const uint64_t nlo = (uint64_t)w0 | ((uint64_t)w1 << 32);
+                v |= nlo << (8 * (16 - k));
+            }
+        }
+        if (avail < 8) v &= (1ull << (8 * avail)) - 1;
+        return v;
+    }
 };
 
 // Per-column output descriptor.
@@ -344,7 +364,9 @@ __device__ __forceinline__ void emit_field(const ParseArgs& a, Reader& rd, uint3
     const uint32_t len = fe - fs;
     auto at = [&](uint32_t j) { return rd.get((uint64_t)fs + j); };
     if (type == 'd') {
-        const vdfdec::Conv cv = vdfdec::convert(vdfdec::scan_number(at, len));
+        vdfdec::Number num;
+        if (!vdfdec::scan_number_fast(rd, fs, len, num)) num = vdfdec::scan_number(at, len);
+        const vdfdec::Conv cv = vdfdec::convert(num);
         double v = cv.v;
         if (cv.ambiguous) v = slow_field(a.buf, fs, len, a.err);
         static_cast<double*>(d->values)[row] = v;

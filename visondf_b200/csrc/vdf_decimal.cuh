@@ -210,6 +210,95 @@ VDF_HD Number scan_number(At at, uint32_t len) {
     return r;
 }
 
+// ------------------------------------------------------ eight at a time
+// Top bit of each byte set exactly where the byte is an ASCII digit: for a
+// byte b below 0x80, (b & 0x7f) + 0x50 reaches 0x80 iff b >= '0' and
+// (b & 0x7f) + 0x46 reaches 0x80 iff b > '9'; neither sum carries into the
+// next byte.
+VDF_HD uint64_t digit_bytes(uint64_t v) {
+    const uint64_t low = v & 0x7f7f7f7f7f7f7f7full;
+    const uint64_t ge0 = low + 0x5050505050505050ull;
+    const uint64_t gt9 = low + 0x4646464646464646ull;
+    return ge0 & ~gt9 & ~v & 0x8080808080808080ull;
+}
+
+// Number of leading digit bytes (byte 0 first) of v, 0..8.
+VDF_HD int digit_run(uint64_t v) {
+    const uint64_t stop = ~digit_bytes(v) & 0x8080808080808080ull;
+    if (!stop) return 8;
+#ifdef __CUDA_ARCH__
+    return (__ffsll((long long)stop) - 1) >> 3;
+#else
+    return __builtin_ctzll(stop) >> 3;
+#endif
+}
+
+// The value of the k leading digit bytes of v (k <= 8): the digits are moved
+// to the top k bytes (zeros before them read as leading zeros), then adjacent
+// digits combine pairwise three times -- x*10 + y per byte pair, per 16-bit
+// pair (x*100 + y) and per 32-bit pair (x*10^4 + y) -- each by one multiply
+// whose cross terms land outside the kept lanes.
+VDF_HD uint64_t digits_value(uint64_t v, int k) {
+    if (k == 0) return 0;
+    const uint64_t mask = k == 8 ? ~0ull : ((1ull << (8 * k)) - 1);
+    uint64_t d = (v & mask) - (0x3030303030303030ull & mask);
+    d <<= 8 * (8 - k);
+    d = ((d * (1 + (10ull << 8))) >> 8) & 0x00ff00ff00ff00ffull;
+    d = ((d * (1 + (100ull << 16))) >> 16) & 0x0000ffff0000ffffull;
+    return (d * (1 + (10000ull << 32))) >> 32;
+}
+
+VDF_HD uint64_t pow10_small(int k) {  // 10^k, k <= 8
+    uint64_t p = 1;
+    for (int i = 0; i < k; ++i) p *= 10;
+    return p;
+}
+
+// The common field shape [-]d{0,7}[.d{0,7}] (at least one digit, then the
+// end of the field or a byte other than 'e' / 'E') read eight bytes at a
+// time; any other shape returns false and goes through scan_number, which
+// gives the same Number for the shapes accepted here.  `src.get8(i, avail)`
+// returns the 8 bytes at i with the bytes at and past `avail` zeroed.
+template <typename Src>
+VDF_HD bool scan_number_fast(Src& src, uint64_t fs, uint32_t len, Number& out) {
+    if (len == 0) return false;
+    uint32_t i = 0;
+    const bool neg = src.get(fs) == '-';
+    if (neg) i = 1;
+    const uint64_t v1 = src.get8(fs + i, len - i);
+    const int k1 = digit_run(v1);
+    if (k1 == 8) return false;
+    uint64_t w = digits_value(v1, k1);
+    int64_t q = 0;
+    i += k1;
+    if (i < len) {
+        const unsigned char c = (unsigned char)(v1 >> (8 * k1));
+        if (c == '.') {
+            ++i;
+            const uint64_t v2 = i < len ? src.get8(fs + i, len - i) : 0;
+            const int k2 = digit_run(v2);
+            if (k2 == 8 || k1 + k2 == 0) return false;
+            w = w * pow10_small(k2) + digits_value(v2, k2);
+            q = -k2;
+            i += k2;
+            if (i < len) {
+                const unsigned char e = (unsigned char)(v2 >> (8 * k2));
+                if (e == 'e' || e == 'E') return false;
+            }
+        } else if (c == 'e' || c == 'E' || k1 == 0) {
+            return false;
+        }
+    } else if (k1 == 0) {
+        return false;
+    }
+    out.w = w;
+    out.q = q;
+    out.kind = kFinite;
+    out.neg = neg;
+    out.many = false;
+    return true;
+}
+
 // ---------------------------------------------------------- conversion
 struct U192 {
     uint64_t p0, p1, p2;
