@@ -404,7 +404,10 @@ vdf_status vdf_left_join_index_host(vdf_ctx* ctx, uint64_t n_left, vdf_col left_
  *     or out of range), 'u' as std::from_chars into unsigned int, 'b' as
  *     std::from_chars into int != 0 (0 when invalid or out of range); strings
  *     keep their bytes (offsets + bytes, "NA" for an empty field).
- * Files must be below 4 GiB.  The table owns its device columns. */
+ * Limits: files below 4 GiB, at most 4096 columns of which at most 64 are
+ * strings (VDF_ERR_UNSUPPORTED beyond).  The table owns its device columns;
+ * they come from a stream-ordered pool per device that keeps up to 8 GiB
+ * cached between reads. */
 typedef struct vdf_csv vdf_csv;
 
 /* `bytes`: n bytes in device memory (16-byte aligned).  Synchronises `stream`. */
@@ -429,6 +432,8 @@ uint64_t vdf_csv_string_bytes(const vdf_csv* t, uint32_t col);
  * NULL).  Synchronises `stream`. */
 vdf_status vdf_csv_copy_column(vdf_ctx* ctx, const vdf_csv* t, uint32_t col, void* values, uint64_t* offsets,
                                void* stream);
+/* Frees the table's columns once no work can still use them (it waits for
+ * the device, as cudaFree does). */
 void vdf_csv_free(vdf_csv* t);
 
 /* ---- batched queries ------------------------------------------------------

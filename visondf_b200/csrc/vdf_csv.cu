@@ -1040,6 +1040,7 @@ uint64_t vdf_csv_string_bytes(const vdf_csv* t, uint32_t col) { return (t && col
 vdf_status vdf_csv_copy_column(vdf_ctx* c, const vdf_csv* t, uint32_t col, void* values, uint64_t* offsets,
                                void* stream) {
     if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
     if (!t || col >= t->ncol) return fail(c, VDF_ERR_INVALID_ARG, "bad table or column");
     DeviceGuard g(t->device);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
