@@ -61,3 +61,37 @@ def make_csv(seed: int, nrow: int, kinds=None, crlf=False, empty_frac=0.0, quote
     if trailing_newline and lines:
         text += eol
     return text.encode("latin-1")
+
+
+def soup_csv(seed: int, nrow: int, ncol: int, quote="'", delim=",", short_row: int = -1) -> bytes:
+    """Records whose fields mix plain text, fully quoted text and quotes in
+    the middle of a field, with delimiters, CR, LF and CR LF inside the quoted
+    parts, empty fields, and LF / CR LF / CR line ends chosen per record.  A
+    header row of names comes first.  `short_row` >= 0 gives that record one
+    field too few (a "column number problem")."""
+    rng = np.random.default_rng(seed)
+    plain = list("abcxyz 0123456789.-")
+    inner = plain + [delim, "\n", "\r", "\r\n", delim + delim]
+
+    def text(pool, k):
+        return "".join(pool[int(i)] for i in rng.integers(0, len(pool), k))
+
+    def field():
+        kind = int(rng.integers(0, 5))
+        if kind == 0:
+            return ""
+        if kind == 1:
+            return text(plain, int(rng.integers(1, 8)))
+        if kind == 2:
+            return quote + text(inner, int(rng.integers(0, 10))) + quote
+        if kind == 3:   # a quoted part in the middle of the field
+            return text(plain, int(rng.integers(0, 3))) + quote + text(inner, int(rng.integers(0, 6))) + quote + \
+                text(plain, int(rng.integers(0, 3)))
+        return str(int(rng.integers(0, 100000)))
+
+    eols = ["\n", "\r\n", "\r"]
+    out = [delim.join(f"h{j}" for j in range(ncol)) + "\n"]
+    for r in range(nrow):
+        k = ncol - 1 if r == short_row else ncol
+        out.append(delim.join(field() for _ in range(k)) + eols[int(rng.integers(0, 3))])
+    return "".join(out).encode("latin-1")

@@ -196,3 +196,22 @@ def test_oracle_doubles_match_reference_fast_float():
     assert ref.types == ["d"]
     got = np.array([ob.parse_double(s.encode()) for s in strings])
     assert got.tobytes() == ref.columns[0][1:].tobytes()
+
+
+@pytest.mark.skipif(not ob.ref_available(), reason="reference shim not built")
+def test_oracle_matches_reference_parser_on_quoting_soup():
+    """Quotes mid-field, quoted delimiters and line ends, mixed line ends:
+    the oracle's split equals the reference parser's (and a short record
+    is the same error row)."""
+    checked = 0
+    for seed in range(60):
+        q = "'" if seed % 2 else '"'
+        short = 7 if seed % 10 == 3 else -1
+        data = csv_gen.soup_csv(seed, 40 + seed, 2 + seed % 5, quote=q, short_row=short)
+        o = ob.csv_read(data, quote=q)
+        r = ob.ref_csv_read(data, quote=q)
+        assert same_table(o, r), seed
+        if short >= 0:
+            assert o.bad_row == short
+        checked += 1
+    assert checked == 60

@@ -157,3 +157,19 @@ def test_zero_copy_views_feed_the_group_by(ctx):
     assert (gr.count.cpu().numpy() == og.count).all()
     del t   # the views keep the table's memory alive
     assert (key.cpu().numpy() == r.columns[0]).all()
+
+
+@pytest.mark.parametrize("device", [False, True])
+def test_quoting_soup_matches_the_oracle(ctx, device):
+    for seed in range(40):
+        q = "'" if seed % 2 else '"'
+        short = 5 + seed if seed % 8 == 3 else -1
+        data = csv_gen.soup_csv(100 + seed, 200 + 37 * seed, 2 + seed % 6, quote=q, short_row=short)
+        r = ob.csv_read(data, quote=q)
+        if r.bad_row >= 0:
+            with pytest.raises(vdf.VdfError, match=f"column number problem at row {r.bad_row} "):
+                read(ctx, data, device, quote=q)
+            continue
+        t = read(ctx, data, device, quote=q)
+        assert_same(t, r)
+        t.close()
