@@ -2,9 +2,10 @@
 
 The product is libvdf_b200.so (C-ABI in include/vdf_capi.h) and the
 header-only C++ dataframe layer in include/vison_b200/vison.hpp.  This
-package is the Python view of the same library: a ctypes binding
-(`_lib`), the dataframe mirror (`frame`) used by the tests and the
-benchmark, and the seeded workload generators (`datagen`).
+package is the Python view of the same library: a ctypes binding (`_lib`:
+Context, Batch, CsvTable), the request loop (`serve`), the autotuner
+(`autotune`), replica plumbing (`replicas`) and the seeded workload
+generators (`datagen`) used by the tests and the benchmark.
 
 The library is loaded on first use of any binding name (so `build` and
 `datagen` import without it); a missing library raises ImportError there --

@@ -51,8 +51,7 @@ struct vdf_csv {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kChunk = 64;                     // bytes per thread in the split passes
-constexpr int kTileBytes = kThreads * kChunk;  // 16 KB
+constexpr int kChunk = 64;  // bytes per thread in the split passes: 16 KB tiles of kThreads threads
 
 // Top bit of each byte of w set exactly where that byte equals the byte of
 // `pat` (x = w ^ pat is zero there): adding 0x7f to the low seven bits sets
