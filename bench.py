@@ -212,6 +212,266 @@ def c0_canonical_bytes(n: int, key_width: int, n_groups: int) -> int:
     return n * (w + w * 2 * (w + 4) + 4 + 32 + w + 16) + n_groups * (w + 8 + 32 + 40)
 
 
+def kernel_bytes(cls: str, n: int, key_w, gather_w, val_w, n_groups: int, val_float):
+    """Algorithmic bytes of ONE launch of a kernel class (the canonical model's
+    per-kernel terms): a radix pass reads and writes (key, u32 row id); the
+    shared-memory finish reads key images + row ids and writes raw keys + the
+    permutation; the payload gather reads the permutation once and each
+    gathered column once and writes it once; the group-by emit reads the sorted
+    keys and values and writes each group's record (keys, count 8, per float
+    column sum/min/max/mean 32, per integer column sum128 16 + min/max 2w +
+    mean 8); the reduce pass reads the sorted keys and values.  None: no
+    model (histograms, scans, the pack)."""
+    out = sum(key_w) + 8 + sum(32 if f else 16 + 2 * w + 8 for w, f in zip(val_w, val_float))
+    return {"onesweep64": 2 * (8 + 4) * n, "onesweep32": 2 * (4 + 4) * n,
+            "localsort": 2 * (key_w[0] + 4) * n,
+            "gather": (4 + 2 * sum(gather_w)) * n if gather_w else None,
+            "segemit": (sum(key_w) + sum(val_w)) * n + n_groups * out,
+            "segreduce": (sum(key_w) + sum(val_w)) * n}.get(cls)
+
+
+def roofline_from_profile(prof: dict, steps: int, n: int, key_w, gather_w, val_w, n_groups: int, val_float,
+                          peak: float, peak_kind: str) -> dict:
+    """The dominant kernel (most device time among the classes with a byte
+    model): its algorithmic bytes per launch / average launch time (library
+    CUDA events inside the timed region) against the HBM peak."""
+    best = None
+    for cls, (ms, cnt) in prof.items():
+        b = kernel_bytes(cls, n, key_w, gather_w, val_w, n_groups, val_float)
+        if b is None or not cnt or ms <= 0:
+            continue
+        if best is None or ms > best[1]:
+            best = (cls, ms, cnt, b)
+    if best is None:
+        return None
+    cls, ms, cnt, b = best
+    avg = ms / cnt
+    achieved = b / (avg / 1e3) / 1e9
+    return {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b,
+            "avg_launch_ms": avg, "launches_per_step": cnt / steps}
+
+
+def group_parity_sample(gr, keys_h, vals_h, n_sample: int, seed: int) -> dict:
+    """Exact per-group check of a random sample of groups of a device result
+    (size-independent: any row count): the group's rows come from the group
+    starts and the permutation; keys, counts and integer sum/min/max must be
+    bit-exact, float sums within 1e-12 of the exact value (math.fsum), and the
+    groups that pass only the condition-aware bound 1e-12 * sum|x| (cancelling
+    sums) are counted apart."""
+    import math
+
+    import torch
+    G = int(gr.n_groups)
+    rng = np.random.default_rng(seed)
+    gi = np.unique(rng.integers(0, G, size=n_sample)) if G > n_sample else np.arange(G)
+    dgi = torch.from_numpy(gi).to(gr.count.device)
+    pick = lambda t: t[dgi].cpu().numpy()  # noqa: E731
+    starts = pick(gr.group_start).view(np.uint32).astype(np.int64)
+    counts = pick(gr.count)
+    idx = np.concatenate([np.arange(s0, s0 + c) for s0, c in zip(starts, counts)])
+    rows = gr.perm[torch.from_numpy(idx).to(gr.perm.device)].cpu().numpy().view(np.uint32)
+    gkeys = [pick(k) for k in gr.keys]
+    aggs = []
+    for v, vh in enumerate(vals_h):
+        a = gr.aggs[v]
+        if vh.dtype.kind == "f":
+            aggs.append((pick(a.sum), None, pick(a.min), pick(a.max)))
+        else:
+            aggs.append((pick(a.sum), pick(a.sum_hi), pick(a.min), pick(a.max)))
+    bad = {"keys": 0, "counts": int((counts <= 0).sum()), "int": 0, "float_min_max": 0, "float_cond": 0}
+    plain_fail, worst = 0, 0.0
+    o = 0
+    for j in range(gi.size):
+        r = rows[o:o + counts[j]]
+        o += counts[j]
+        for kh, gk in zip(keys_h, gkeys):
+            if not (kh[r] == gk[j]).all():
+                bad["keys"] += 1
+        for vh, (sm, hi, mn, mx) in zip(vals_h, aggs):
+            x = vh[r]
+            if vh.dtype.kind == "f":
+                exact = math.fsum(x.tolist())
+                absum = math.fsum(np.abs(x).tolist())
+                err = abs(float(sm[j]) - exact)
+                if err > 1e-12 * max(absum, abs(exact)) + 1e-300:
+                    bad["float_cond"] += 1
+                if err > 1e-12 * abs(exact):
+                    plain_fail += 1
+                if exact:
+                    worst = max(worst, err / abs(exact))
+                if mn[j] != x.min() or mx[j] != x.max():
+                    bad["float_min_max"] += 1
+            else:
+                exact = int(sum(int(t) for t in x))
+                got = ((int(hi[j]) << 64) | (int(sm[j]) & ((1 << 64) - 1)))
+                if got >= 1 << 127:
+                    got -= 1 << 128
+                if got != exact or int(mn[j]) != int(x.min()) or int(mx[j]) != int(x.max()):
+                    bad["int"] += 1
+    return {"groups_checked": int(gi.size), "rows_checked": int(idx.size), "bit_exact_failures": bad,
+            "f64_plain_relative_failures": plain_fail, "f64_worst_relative_error": worst,
+            "rule": "keys, counts, integer sum/min/max and f64 min/max bit-exact; f64 sums within 1e-12 of "
+                    "math.fsum, groups passing only 1e-12 * sum|x| counted as plain-relative failures"}
+
+
+def config_section(args, local_rank: int, name: str) -> dict:
+    """One more configuration of the sort + gather + group-by pipeline, device-
+    resident and timed like the headline (CUDA events around args.steps calls,
+    library events per kernel class), with its canonical %HBM, the dominant
+    kernel's roofline, a parity summary and the reference CPU path on the
+    first rows of the same seeded inputs:
+      c1_ties  the two-key frame with key1 drawn from 50M values (about two
+               rows per key1 value, so key2 orders them)
+      c0       1M rows, int32 key over 10,000 values, f64 + int64 values
+      c2a      200M rows, int64 key over 50M values, lognormal f64 + int64 values
+      c2b      200M rows, int32 key over 16 values, 90/10 skew, same values"""
+    import torch
+
+    import visondf_b200 as vdf
+    from visondf_b200 import datagen
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_bind as ob
+
+    dev = torch.device("cuda", local_rank)
+    t0 = time.time()
+    if name == "c1_ties":
+        n = args.rows
+        f = datagen.frame_w1(n, key1_pool=n // 2)
+        knames, pnames, agg = ["key1", "key2"], ["f64", "i32", "rowid"], [0, 1]
+        workload = (f"{n:,} rows: the two-key frame with key1 drawn from {n // 2:,} distinct full-range int64 "
+                    f"values (about two rows per value, ordered by key2), same payload and group-by")
+    elif name == "c0":
+        n = 1_000_000
+        f = datagen.frame_w0(n)
+        knames, pnames, agg = ["key"], ["v1", "v2"], [0, 1]
+        workload = ("1,000,000 rows, int32 key over 10,000 distinct values, f64 N(0,1) + int64 U[-1e9, 1e9]; "
+                    "sort by key, group-by count/sum/min/max/mean of both")
+    elif name == "c2a":
+        n = 200_000_000
+        f = datagen.frame_w2a(n)
+        knames, pnames, agg = ["key"], ["v1", "v2"], [0, 1]
+        workload = ("200,000,000 rows, int64 key over 50,000,000 distinct values, f64 lognormal(0,1) + int64 "
+                    "U[0, 2^40); sort, gather, group-by count/sum/min/max/mean")
+    elif name == "c2b":
+        n = 200_000_000
+        f = datagen.frame_w2b(n)
+        knames, pnames, agg = ["key"], ["v1", "v2"], [0, 1]
+        workload = ("200,000,000 rows, int32 key over 16 distinct values (two take 45 % each, 14 share 10 %), "
+                    "f64 lognormal(0,1) + int64 U[0, 2^40); sort, gather, group-by")
+    else:
+        raise ValueError(name)
+    log(f"[{name}] generated {n:,} rows in {time.time() - t0:.1f}s")
+    keys = [torch.from_numpy(f[k]).to(dev) for k in knames]
+    payload = [torch.from_numpy(f[k]).to(dev) for k in pnames]
+    ctx = vdf.Context(local_rank)
+    stream = torch.cuda.current_stream()
+    outs = ctx.alloc_sort_groupby_outputs(keys, payload, agg, want_group_start=True)
+    packed = ctx.pack_sort_groupby(keys, payload, agg, vdf.ORDER_ASC, True, outs, host_count=False)
+    steps = args.steps * (10 if n <= 1_000_000 else 1)
+    for _ in range(args.warmup):
+        ctx.sort_groupby_packed(packed, stream)
+    ctx.check(stream)
+    st0 = ctx.sort_stats(stream)
+    ctx.profile(True)
+    ctx.profile_reset()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.kernel_launches
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.sort_groupby_packed(packed, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    launches = (ctx.kernel_launches - l0) / steps
+    prof = ctx.profile_read()
+    ctx.profile(False)
+    ctx.check(stream)
+    st1 = ctx.sort_stats(stream)
+    G = int(outs["ngroups_dev"].item())
+    peak, peak_kind = measured_peaks()
+    key_w = [k.element_size() for k in keys]
+    gather_w = key_w[1:] + [p.element_size() for p in payload]
+    val_w = [payload[i].element_size() for i in agg]
+    val_float = [payload[i].dtype.is_floating_point for i in agg]
+    if name == "c1_ties":
+        canonical = (SORT_BYTES_PER_ROW + 24) * n + G * 84
+    else:
+        canonical = c0_canonical_bytes(n, key_w[0], G)
+    roof = roofline_from_profile(prof, steps, n, key_w, gather_w, val_w, G, val_float, peak, peak_kind)
+    res = {"workload": workload, "rows": n, "n_groups": G, "unit": UNIT, "steps": steps,
+           "ms_per_step": ms, "value": n / (ms / 1e3), "hbm_frac_canonical": canonical / (ms / 1e3) / 1e9 / peak,
+           "canonical_bytes": canonical, "gpu_launches_per_step": launches,
+           "sort_plan": {**vdf._lib.sort_plan_info(n, [vdf._lib.TORCH_TO_VDF[k.dtype] for k in keys]),
+                         "msd_sorts": st1["msd_sorts"] - st0["msd_sorts"],
+                         "msd_fallbacks": st1["msd_fallbacks"] - st0["msd_fallbacks"]},
+           "kernels": {k: {"ms_per_step": v[0] / steps, "launches_per_step": v[1] / steps}
+                       for k, v in prof.items() if v[1]},
+           "roofline": roof}
+    if name == "c2b":
+        res["hbm_frac_sort_free_20B"] = 20 * n / (ms / 1e3) / 1e9 / peak
+    # parity: the whole group table against the oracle where that is quick
+    # (c0: 1M rows; c2b: 16 groups), an exact check of sampled groups otherwise
+    gr = vdf.GroupResult(G, outs["gkeys"], outs["count"], outs["aggs"], outs["gstart"], None, outs["perm"],
+                         outs["skeys"], outs["pay"]).trimmed()
+    keys_h = [f[k] for k in knames]
+    vals_h = [f[pnames[i]] for i in agg]
+    if name in ("c0", "c2b"):
+        og = ob.groupby(keys_h, vals_h)
+        ok = {"n_groups": og.n_groups == G,
+              "keys": all((k.cpu().numpy() == o).all() for k, o in zip(gr.keys, og.keys)),
+              "counts": bool((gr.count.cpu().numpy() == og.count).all())}
+        plain = 0
+        for v in range(len(vals_h)):
+            a = gr.aggs[v]
+            if vals_h[v].dtype.kind == "f":
+                got = a.sum.cpu().numpy()
+                err = np.abs(got - og.sum[v])
+                ok[f"v{v}_sum_cond"] = bool((err <= 1e-12 * np.maximum(og.abs[v], np.abs(og.sum[v])) + 1e-300).all())
+                plain += int(np.count_nonzero(err > 1e-12 * np.abs(og.sum[v])))
+                ok[f"v{v}_min_max"] = bool((a.min.cpu().numpy() == og.min[v]).all() and
+                                           (a.max.cpu().numpy() == og.max[v]).all())
+            else:
+                ok[f"v{v}_sum"] = bool((a.sum.cpu().numpy() == og.sum[v]).all() and
+                                       (a.sum_hi.cpu().numpy() == og.sum_hi[v]).all())
+                ok[f"v{v}_min_max"] = bool((a.min.cpu().numpy() == og.min[v]).all() and
+                                           (a.max.cpu().numpy() == og.max[v]).all())
+        res["parity"] = {"against": "oracle group-by of every row (exact 128-bit integer sums, long double "
+                                    "Neumaier float sums)", "checks": ok, "all_ok": all(ok.values()),
+                         "f64_plain_relative_failures": plain}
+    else:
+        res["parity"] = {"against": "exact sums of sampled groups", **group_parity_sample(
+            gr, keys_h, vals_h, 2000, seed=17)}
+    ctx.close()
+    del keys, payload, outs, packed, gr
+    torch.cuda.empty_cache()
+    # the reference CPU path on the first rows of the same inputs
+    if not args.no_cpu_baseline:
+        m = min(n, args.ref_sample)
+        ks = [np.ascontiguousarray(f[k][:m]) for k in knames]
+        ps = [np.ascontiguousarray(f[k][:m]) for k in pnames]
+        cores = cpu_threads()
+        if ob.ref_available():
+            cores = max(1, min(cores, 32))
+            c0 = time.perf_counter()
+            ob.ref_sort(ks, ob.ASC, cores=cores, payload=ps)
+            ob.ref_groupby(ks, [ps[i] for i in agg], cores=cores)
+            sec, kind = time.perf_counter() - c0, "reference"
+        else:
+            c0 = time.perf_counter()
+            perm = ob.argsort(ks)
+            for q in ps:
+                q[perm]
+            ob.groupby(ks, [ps[i] for i in agg], sorted_groups=False)
+            sec, kind, cores = time.perf_counter() - c0, "port", 1
+        res["cpu_baseline"] = {"value": m / sec, "unit": UNIT, "cores": cores, "kind": kind,
+                               "sample": f"first {m:,} rows of the same inputs; host CPU: {cpu_info()}"}
+    del f
+    return res
+
+
 def batched_section(args, local_rank: int) -> dict:
     """Many independent queries as one graph-launched batch, against the same
     queries run one library call each."""
@@ -618,6 +878,7 @@ def our_arm(args, rank: int, world: int, local_rank: int):
     for _ in range(args.warmup):
         ctx.sort_groupby_packed(packed, stream)
     ctx.check(stream)
+    sstats0 = ctx.sort_stats(stream)
     ctx.profile(True)
     ctx.profile_reset()
     barrier()
@@ -636,6 +897,7 @@ def our_arm(args, rank: int, world: int, local_rank: int):
     prof = ctx.profile_read()
     ctx.profile(False)
     ctx.check(stream)
+    sstats = ctx.sort_stats(stream)
     n_groups = int(outs["ngroups_dev"].item())
     clk = clocks.summary()
     ms = replicas.max_over_ranks(ms, world, dev)
@@ -643,25 +905,17 @@ def our_arm(args, rank: int, world: int, local_rank: int):
 
     # ---- roofline of the dominant kernel ------------------------------------------
     peak, peak_kind = measured_peaks()
-    bytes_per_launch = {"onesweep32": 2 * (4 + 4) * n, "onesweep64": 2 * (8 + 4) * n,
-                        "hist": 12 * n, "gather": None, "segreduce": None}
-    dom = max(prof, key=lambda k: prof[k][0])
-    dom_ms, dom_cnt = prof[dom]
-    if bytes_per_launch.get(dom) is None:
-        dom = "onesweep64"
-        dom_ms, dom_cnt = prof[dom]
-    avg_ms = dom_ms / max(dom_cnt, 1)
-    achieved = bytes_per_launch[dom] / (avg_ms / 1e3) / 1e9
-    traffic = None
+    roofline = roofline_from_profile(prof, args.steps, n, [8, 4], [4, 8, 4, 8], [8, 4], n_groups, [True, False],
+                                     peak, peak_kind)
     tfile = ROOT / "profiles" / "traffic.json"
+    roofline["traffic"] = None
     if tfile.exists():
         tj = json.loads(tfile.read_text())
-        ent = tj.get(dom)
+        ent = tj.get(roofline["kernel"])
         if ent and ent.get("rows"):
-            traffic = ent["bytes_per_launch"] * n / ent["rows"]
-    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                "algorithmic_bytes_per_launch": bytes_per_launch[dom], "avg_launch_ms": avg_ms}
+            roofline["traffic"] = ent["bytes_per_launch"] * n / ent["rows"]
+            roofline["traffic_source"] = (f"scaled from profiles/traffic.json: ncu dram__bytes_read.sum + "
+                                          f"dram__bytes_write.sum of one {ent['rows']:,}-row launch")
     kernels = {k: {"ms_per_step": v[0] / args.steps, "launches_per_step": v[1] / args.steps}
                for k, v in prof.items() if v[1]}
     canonical = (SORT_BYTES_PER_ROW + GROUPBY_BYTES_PER_ROW_G_EQ_N) * n
@@ -779,6 +1033,10 @@ def our_arm(args, rank: int, world: int, local_rank: int):
     torch.cuda.empty_cache()
     sections = set(args.sections.split(","))
     batched = served = unique_join = csv_res = None
+    configs = {}
+    for name in ("c1_ties", "c0", "c2a", "c2b"):
+        if world == 1 and name in sections:
+            configs[name] = config_section(args, local_rank, name)
     if world == 1 and "batched" in sections:
         batched = batched_section(args, local_rank)
     if world == 1 and "served" in sections:
@@ -799,12 +1057,16 @@ def our_arm(args, rank: int, world: int, local_rank: int):
             "hbm_frac_canonical": step_frac,
             "canonical_bytes_per_row": SORT_BYTES_PER_ROW + GROUPBY_BYTES_PER_ROW_G_EQ_N,
             "kernels": kernels,
+            "sort_plan": {**__import__("visondf_b200._lib", fromlist=["x"]).sort_plan_info(n, [1, 0]),
+                          "msd_sorts": sstats["msd_sorts"] - sstats0["msd_sorts"],
+                          "msd_fallbacks": sstats["msd_fallbacks"] - sstats0["msd_fallbacks"]},
             "tuning": {"variant32": tuned["variant32"], "variant64": tuned["variant64"],
                        "variants": __import__("visondf_b200._lib", fromlist=["x"]).sort_variants()},
             "gpu_launches": launches,
             "clocks": clk,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "configs": configs,
             "batched": batched,
             "served": served,
             "unique_join": unique_join,
@@ -827,7 +1089,7 @@ def main():
     ap.add_argument("--variants", type=int, nargs=2, metavar=("V32", "V64"),
                     help="with --no-autotune: radix-pass variant indices for 4- and 8-byte keys")
     ap.add_argument("--csv-bytes", type=int, default=1 << 30, help="size of the synthetic CSV file (csv section)")
-    ap.add_argument("--sections", default="batched,served,unique_join,csv",
+    ap.add_argument("--sections", default="c1_ties,c0,c2a,c2b,batched,served,unique_join,csv",
                     help="extra single-GPU measurements after the headline one: batched, served, unique_join "
                          "(comma list, 'none' for none)")
     ap.add_argument("--batch-queries", type=int, default=4096)

@@ -122,7 +122,9 @@ typedef enum vdf_kernel_class {
     VDF_KC_SEGEMIT = 9,     /* group-by: scan + emit groups   */
     VDF_KC_TIES = 10,       /* equal-neighbour check (multi-key) */
     VDF_KC_BATCH = 11,      /* batch bookkeeping: row ids per query, group ranges, group keys */
-    VDF_KC_CSV = 12         /* CSV ingest: record split, field parse, string columns */
+    VDF_KC_CSV = 12,        /* CSV ingest: record split, field parse, string columns */
+    VDF_KC_LOCALSORT = 13,  /* MSD-first sort: chunk search + shared-memory finish */
+    VDF_KC_FALLBACK = 14    /* MSD-first sort: the conditional LSD kernels (return at once unless taken) */
 } vdf_kernel_class;
 /* When enabled, every kernel the context launches is bracketed by CUDA
  * events on its stream (no reference counterpart: the reference has no
@@ -169,6 +171,32 @@ typedef enum vdf_multikey_mode {
 vdf_status vdf_ctx_set_multikey_mode(vdf_ctx* ctx, int mode);
 int vdf_ctx_get_multikey_mode(vdf_ctx* ctx); /* -1 for a NULL context */
 
+/* Sort strategy for sorts by one or two key columns.
+ * VDF_SORT_AUTO (default, with msd_min_rows = 2^20): sorts of at least
+ *   msd_min_rows rows first partition the rows by the top 1-3 bytes of key 0
+ *   with global radix passes (most significant digit first) and then sort
+ *   each chunk of whole partitions (<= 4096 rows) in shared memory by the
+ *   rest of key 0 and key 1; where the data defeats that plan (a partition
+ *   larger than a chunk, or more than 64 rows sharing key 0's high 32 bits
+ *   out of order) the LSD passes over all keys run instead, decided on the
+ *   device without a host round trip.  The result is the same stable order.
+ * VDF_SORT_LSD: always the LSD passes (as the reference's radix sorts do,
+ *   radix_sort_uint64_mt.inl:6-166). */
+typedef enum vdf_sort_strategy {
+    VDF_SORT_AUTO = 0,
+    VDF_SORT_LSD = 1
+} vdf_sort_strategy;
+vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* ctx, int strategy, uint64_t msd_min_rows);
+vdf_status vdf_ctx_get_sort_strategy(vdf_ctx* ctx, int32_t* strategy, uint64_t* msd_min_rows);
+/* Sorts this context planned MSD-first, and how many of them fell back to
+ * the LSD passes on the device (synchronises `stream`).  No counterpart in
+ * the reference. */
+vdf_status vdf_ctx_sort_stats(vdf_ctx* ctx, void* stream, uint64_t* msd_sorts, uint64_t* msd_fallbacks);
+/* The plan a sort of n rows with these key dtypes gets under a strategy
+ * (pure host function): global MSD passes (0 = LSD sort) and chunks. */
+vdf_status vdf_sort_plan_info(uint64_t n, const int32_t* key_dtypes, int nkeys, int strategy, uint64_t msd_min_rows,
+                              int32_t* msd_passes, uint32_t* chunks);
+
 /* ---- workspace sizing (pure host functions) ------------------------------ */
 /* Enough for every tuning; vdf_sort_argsort_ws also packs the other sorted
  * key columns into this buffer when it holds n * 16 * ceil((nkeys-1)/2)
@@ -213,11 +241,16 @@ vdf_status vdf_sort_argsort_ws(vdf_ctx* ctx, uint64_t n, const vdf_col* keys, in
  * n above VDF_NOALLOC_MAX_ROWS returns VDF_ERR_UNSUPPORTED.  All calls on a
  * device share the one array: calls that overlap on the GPU (other streams,
  * other host threads) race and corrupt each other's results; serialise them.
- * The call is asynchronous on `stream` and does not report device-side wait
- * timeouts.  No counterpart in the reference: the reference's radix sort
+ * The call is asynchronous on `stream`; device-side wait timeouts are read
+ * back with vdf_sort_noalloc_error.  No counterpart in the reference: the reference's radix sort
  * always allocates its buffers (radix_sort_uint64.inl:23-24). */
 vdf_status vdf_sort_argsort_noalloc(uint64_t n, const vdf_col* keys, int nkeys, int order, uint32_t* perm_out,
                                     void* const* sorted_keys_out, void* stream);
+/* The device error bits of the last vdf_sort_argsort_noalloc call on the
+ * current device (0 = none; bit 0: a bounded wait gave up, bit 1: an
+ * out-of-range row id), copied into *host_out after `stream` has drained.
+ * Allocates nothing.  No counterpart in the reference. */
+vdf_status vdf_sort_noalloc_error(uint32_t* host_out, void* stream);
 
 /* ---- gather ---------------------------------------------------------------- */
 /* out[c][r] = in[c].data[perm[r]] for ncols (<= 8) columns in one launch.

@@ -94,3 +94,18 @@ def test_autotune_size_classes():
     t = autotune.TuningTable({20: [1, 2, 0.1, 0.2]})
     assert t.lookup(1 << 20) == (1, 2)
     assert t.lookup(5) is None
+
+
+def test_sort_plan_choice():
+    info = _lib.sort_plan_info
+    # 100M rows, int64 + int32 keys: two top-digit passes, 2048-row chunks
+    assert info(100_000_000, [vdf.I64, vdf.I32]) == {"msd_passes": 2, "chunks": (100_000_000 + 2047) // 2048}
+    assert info(200_000_000, [vdf.I64])["msd_passes"] == 3
+    assert info(393_216, [vdf.I32], msd_min_rows=0)["msd_passes"] == 1
+    assert info(393_217, [vdf.I32], msd_min_rows=0)["msd_passes"] == 2
+    # below the row threshold, with three keys, or with the LSD strategy: LSD
+    assert info(1000, [vdf.I64])["msd_passes"] == 0
+    assert info(1000, [vdf.I64], msd_min_rows=0)["msd_passes"] == 1
+    assert info(10_000_000, [vdf.I64, vdf.I32, vdf.I32])["msd_passes"] == 0
+    assert info(10_000_000, [vdf.I64], strategy=_lib.SORT_LSD)["msd_passes"] == 0
+    assert info(1, [vdf.I64], msd_min_rows=0)["msd_passes"] == 0

@@ -135,9 +135,10 @@ def test_columns_feed_the_sort(ctx):
     data = csv_gen.make_csv(3, 50_000, kinds=["u", "d"], quote='"')
     t = read(ctx, data, True, quote='"')
     r = ob.csv_read(data, quote='"')
-    key = t.tensor(0).to(torch.int64) & 0xffffffff
+    key = t.tensor(0)
+    assert key.dtype == torch.uint32
     perm = ctx.argsort([key])
-    exp = np.argsort(r.columns[0].astype(np.int64), kind="stable")
+    exp = np.argsort(r.columns[0], kind="stable")
     assert (perm.cpu().numpy().astype(np.int64) == exp).all()
     assert t.tensor(1).cpu().numpy().tobytes() == r.columns[1].tobytes()
 
@@ -173,3 +174,43 @@ def test_quoting_soup_matches_the_oracle(ctx, device):
         t = read(ctx, data, device, quote=q)
         assert_same(t, r)
         t.close()
+
+
+def test_close_waits_for_live_views(ctx):
+    """close() while a view is alive must not hand the view's memory to the
+    next table: the free waits for the last view."""
+    data = csv_gen.make_csv(21, 40_000, kinds=["u", "d"], quote='"')
+    t = read(ctx, data, True, quote='"')
+    r = ob.csv_read(data, quote='"')
+    v = t.view(1)
+    t.close()
+    with pytest.raises(ValueError, match="closed"):
+        t.view(0)
+    others = [read(ctx, csv_gen.make_csv(22 + i, 40_000, kinds=["d", "d"], quote='"'), True, quote='"')
+              for i in range(3)]
+    assert v.cpu().numpy().tobytes() == r.columns[1].tobytes()
+    assert t.handle  # still held for the view
+    del v
+    import gc
+    gc.collect()
+    assert not t.handle  # the last view went: the table is freed
+    for o in others:
+        o.close()
+
+
+def test_unsigned_columns_sort_alike_through_view_and_tensor(ctx):
+    """uint32 values at and above 2^31 order the same whichever accessor
+    feeds the sort (both give torch.uint32)."""
+    rng = np.random.default_rng(9)
+    vals = rng.integers(0, 1 << 32, 5_000, dtype=np.uint64)
+    vals[:4] = [0, (1 << 31) - 1, 1 << 31, (1 << 32) - 1]
+    data = ("k\n" + "\n".join(str(int(x)) for x in vals) + "\n").encode()
+    t = read(ctx, data, True, quote='"')
+    assert t.types == ["u"]
+    a, b = t.view(0), t.tensor(0)
+    assert a.dtype == b.dtype == torch.uint32
+    exp = np.argsort(vals.astype(np.uint32), kind="stable").astype(np.uint32)
+    for col in (a, b):
+        assert (ctx.argsort([col]).cpu().numpy().view(np.uint32) == exp).all()
+    del a
+    t.close()

@@ -26,9 +26,14 @@ def noalloc_sort(keys, order):
     n = keys[0].numel()
     perm = torch.empty(n, dtype=torch.int32, device="cuda")
     skeys = [torch.empty_like(k) for k in keys]
+    stream = torch.cuda.current_stream().cuda_stream
     st = vdf.lib.vdf_sort_argsort_noalloc(n, _lib._cols(keys), len(keys), order, perm.data_ptr(),
-                                          _lib._ptrs(skeys), torch.cuda.current_stream().cuda_stream)
+                                          _lib._ptrs(skeys), stream)
     assert st == _lib.OK, vdf.lib.vdf_status_string(st)
+    # a normal call leaves no device error bits
+    err = C.c_uint32(0xFFFFFFFF)
+    assert vdf.lib.vdf_sort_noalloc_error(C.byref(err), stream) == _lib.OK
+    assert err.value == 0
     torch.cuda.synchronize()
     return perm, skeys
 
@@ -49,6 +54,10 @@ def test_noalloc_matches_context_sort_on_two_calls(ctx):
         assert (host(perm) == host(ref_perm)).all()
         for a, b in zip(skeys, ref_skeys):
             assert bits_equal(host(a), host(b))
+
+
+def test_noalloc_error_query_rejects_null():
+    assert vdf.lib.vdf_sort_noalloc_error(None, None) == _lib.ERR_INVALID_ARG
 
 
 def test_noalloc_rejects_more_rows_than_its_scratch_holds():

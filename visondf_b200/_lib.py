@@ -7,6 +7,7 @@ is missing the import fails loudly -- there is no CPU fallback.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass, field
 from pathlib import Path
 from typing import Optional, Sequence
@@ -25,9 +26,11 @@ I32, I64, U32, U64, F64, F32 = range(6)
 ORDER_ASC, ORDER_DESC_STABLE, ORDER_DESC_REVERSE = range(3)
 
 KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast", "pack",
-                  "segscan", "segemit", "ties", "batch", "csv"]
+                  "segscan", "segemit", "ties", "batch", "csv", "localsort", "fallback"]
 # vdf_multikey_mode
 MULTIKEY_LSD, MULTIKEY_PRIMARY_FIRST = 0, 1
+# vdf_sort_strategy
+SORT_AUTO, SORT_LSD = 0, 1
 
 TORCH_TO_VDF = {
     torch.int32: I32, torch.int64: I64, torch.uint32: U32, torch.uint64: U64,
@@ -117,6 +120,7 @@ def _load() -> C.CDLL:
         "vdf_sort_argsort": (st, [vp, u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp]),
         "vdf_sort_argsort_ws": (st, [vp, u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp, sz, vp]),
         "vdf_sort_argsort_noalloc": (st, [u64, C.POINTER(vdf_col), i32, i32, vp, C.POINTER(vp), vp]),
+        "vdf_sort_noalloc_error": (st, [C.POINTER(C.c_uint32), vp]),
         "vdf_gather": (st, [vp, u64, vp, C.POINTER(vdf_col), i32, C.POINTER(vp), vp]),
         "vdf_groupby_sorted": (st, [vp, u64, C.POINTER(vdf_col), i32, C.POINTER(vdf_col), i32, C.POINTER(vp), vp,
                                     C.POINTER(vdf_agg_out), vp, vp, vp, C.POINTER(C.c_uint64), vp]),
@@ -130,6 +134,11 @@ def _load() -> C.CDLL:
                                             C.POINTER(C.c_uint64), vp]),
         "vdf_ctx_set_multikey_mode": (st, [vp, i32]),
         "vdf_ctx_get_multikey_mode": (i32, [vp]),
+        "vdf_ctx_set_sort_strategy": (st, [vp, i32, u64]),
+        "vdf_ctx_sort_stats": (st, [vp, vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "vdf_ctx_get_sort_strategy": (st, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]),
+        "vdf_sort_plan_info": (st, [u64, C.POINTER(C.c_int32), i32, i32, u64, C.POINTER(C.c_int32),
+                                    C.POINTER(C.c_uint32)]),
         "vdf_batch_variant_count": (i32, []),
         "vdf_batch_variant_info": (st, [i32, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
         "vdf_batch_default_tuning": (st, [C.POINTER(vdf_batch_tuning)]),
@@ -298,6 +307,22 @@ class Context:
 
     def get_multikey_mode(self) -> int:
         return lib.vdf_ctx_get_multikey_mode(self.handle)
+
+    def set_sort_strategy(self, strategy: int, msd_min_rows: int = 1 << 20):
+        """SORT_AUTO: MSD-first sorts (one or two keys, >= msd_min_rows rows)
+        with the LSD passes as the on-device fallback; SORT_LSD: LSD only."""
+        self._check(lib.vdf_ctx_set_sort_strategy(self.handle, strategy, msd_min_rows), "vdf_ctx_set_sort_strategy")
+
+    def sort_stats(self, stream=None) -> dict:
+        """{"msd_sorts": sorts planned MSD-first, "msd_fallbacks": of those, LSD fallbacks on the device}"""
+        a, b = C.c_uint64(), C.c_uint64()
+        self._check(lib.vdf_ctx_sort_stats(self.handle, _stream(stream), C.byref(a), C.byref(b)), "sort_stats")
+        return {"msd_sorts": int(a.value), "msd_fallbacks": int(b.value)}
+
+    def get_sort_strategy(self) -> tuple:
+        st, mn = C.c_int32(), C.c_uint64()
+        self._check(lib.vdf_ctx_get_sort_strategy(self.handle, C.byref(st), C.byref(mn)), "get_sort_strategy")
+        return st.value, int(mn.value)
 
     def get_sort_tuning(self) -> tuple:
         t = vdf_sort_tuning()
@@ -485,6 +510,8 @@ class CsvTable:
     def __init__(self, ctx: "Context", handle: int):
         self._ctx = ctx
         self.handle = handle
+        self._live_views = 0    # view() tensors still alive
+        self._closing = False   # close() called: free once the last view is gone
         self.nrow = int(lib.vdf_csv_nrow(handle))
         self.ncol = int(lib.vdf_csv_ncol(handle))
         self.names = [lib.vdf_csv_name(handle, k).decode("latin-1") for k in range(self.ncol)]
@@ -495,18 +522,21 @@ class CsvTable:
         return dict(values=lib.vdf_csv_values(self.handle, k), offsets=lib.vdf_csv_offsets(self.handle, k),
                     bytes=int(lib.vdf_csv_string_bytes(self.handle, k)))
 
-    _TORCH = {"d": torch.float64, "u": torch.int32, "b": torch.uint8}
+    _TORCH = {"d": torch.float64, "u": torch.uint32, "b": torch.uint8}
 
     _TYPESTR = {"d": "<f8", "u": "<u4", "b": "|u1"}
 
     def view(self, k: int) -> torch.Tensor:
         """Numeric column k as a CUDA tensor over the table's own memory (no
-        copy; the tensor keeps the table alive): parsed columns go straight
-        into the sort and group-by; writes through it change the table.
-        uint32 columns come back as torch.uint32."""
+        copy): parsed columns go straight into the sort and group-by; writes
+        through it change the table.  The tensor keeps the table alive, and
+        close() while views are alive frees the table's memory only when the
+        last of them is gone.  uint32 columns come back as torch.uint32."""
         ty = self.types[k]
         if ty not in self._TYPESTR:
             raise ValueError("string columns have no tensor view")
+        if not self.handle or self._closing:
+            raise ValueError("the table is closed")
         table = self
 
         class _Col:
@@ -518,7 +548,15 @@ class CsvTable:
         holder = _Col()
         t = torch.as_tensor(holder, device=f"cuda:{self._ctx.device}")
         t._vdf_owner = holder  # the table outlives the view
+        self._live_views += 1
+        weakref.finalize(holder, CsvTable._view_gone, self)
         return t
+
+    @staticmethod
+    def _view_gone(table: "CsvTable"):
+        table._live_views -= 1
+        if table._closing and table._live_views == 0:
+            table._free()
 
     def copy_column(self, k: int, values: int, offsets: Optional[int] = None, stream=None):
         """Copies column k into caller memory (host or device addresses):
@@ -528,7 +566,7 @@ class CsvTable:
 
     def tensor(self, k: int, stream=None) -> torch.Tensor:
         """Numeric column k copied into a new CUDA tensor (uint32 columns as
-        int32 bit patterns)."""
+        torch.uint32, as view() gives them, so both sort the same way)."""
         ty = self.types[k]
         if ty not in self._TORCH:
             raise ValueError("string columns have no tensor form")
@@ -554,13 +592,21 @@ class CsvTable:
         return [raw[int(off[i]):int(off[i + 1])] for i in range(self.nrow)]
 
     def close(self):
+        """Frees the table's device memory, or, while view() tensors are
+        alive, as soon as the last of them is gone (their memory must not go
+        back to the pool under them)."""
+        self._closing = True
+        if self._live_views == 0:
+            self._free()
+
+    def _free(self):
         if self.handle:
             lib.vdf_csv_free(self.handle)
             self.handle = None
 
     def __del__(self):
         try:
-            self.close()
+            self._free()
         except Exception:
             pass
 
@@ -574,6 +620,16 @@ def sort_variants() -> list:
             out.append(dict(index=i, key_width=vals[0].value, threads=vals[1].value, items=vals[2].value,
                             digit_bits=vals[3].value, match=vals[4].value))
     return out
+
+
+def sort_plan_info(n: int, dtypes: Sequence[int], strategy: int = SORT_AUTO, msd_min_rows: int = 1 << 20) -> dict:
+    """The plan of a sort: {"msd_passes": global MSD passes (0 = LSD), "chunks": shared-memory chunks}."""
+    dts = (C.c_int32 * len(dtypes))(*dtypes)
+    p, c = C.c_int32(), C.c_uint32()
+    st = lib.vdf_sort_plan_info(n, dts, len(dtypes), strategy, msd_min_rows, C.byref(p), C.byref(c))
+    if st != OK:
+        raise VdfError(st, "vdf_sort_plan_info")
+    return {"msd_passes": p.value, "chunks": c.value}
 
 
 def header_functions() -> list[str]:

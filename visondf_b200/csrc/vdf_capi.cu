@@ -61,6 +61,7 @@ size_t sort_ws_need(const vdf::SortPlan& p, uint64_t n, int nkeys, void* const* 
 size_t primary_first_need(vdf_ctx* c, uint64_t n, const int32_t* dts, int nkeys, void* const* sorted_keys_out) {
     if (nkeys < 2 || c->multikey_mode != VDF_MULTIKEY_PRIMARY_FIRST || (sorted_keys_out && sorted_keys_out[0]))
         return 0;
+    if (vdf::make_sort_plan(n, dts, nkeys, c->tuning).msd) return 0;
     const vdf::SortPlan p0 = vdf::make_sort_plan(n, dts, 1, c->tuning);
     return align256(p0.ws_bytes) + (size_t)n * vdf::dtype_width(dts[0]);
 }
@@ -79,6 +80,8 @@ vdf_status primary_first(vdf_ctx* c, uint64_t n, const int32_t* dts, const void*
                          const uint32_t* perm_in, bool* done) {
     *done = false;
     if (nkeys < 2 || c->multikey_mode != VDF_MULTIKEY_PRIMARY_FIRST || n < 2) return VDF_OK;
+    // the MSD-first plan sorts by both keys at once without a host round trip
+    if (vdf::make_sort_plan(n, dts, nkeys, c->tuning).msd) return VDF_OK;
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) {
         cudaGetLastError();
@@ -92,8 +95,7 @@ vdf_status primary_first(vdf_ctx* c, uint64_t n, const int32_t* dts, const void*
         need = align256(p0.ws_bytes) + (size_t)n * vdf::dtype_width(dts[0]);
     }
     if (need > ws_bytes) return VDF_OK;  // no room: the LSD sort over all keys
-    cudaError_t e = vdf::run_sort(p0, cols, order, perm, k0, ws, err_word(c), s, prof_of(c), perm_in);
-    c->launches += 2 + (uint64_t)p0.total_passes;
+    cudaError_t e = ctx_run_sort(c, p0, cols, order, perm, k0, ws, s, perm_in);
     if (e == cudaSuccess) e = cudaMemsetAsync(tie_word(c), 0, sizeof(uint32_t), s);
     if (e == cudaSuccess) e = vdf::flag_adjacent_ties(k0, vdf::dtype_width(dts[0]), n, tie_word(c), s, prof_of(c));
     c->launches += 1;
@@ -121,8 +123,7 @@ vdf_status sort_impl(vdf_ctx* c, uint64_t n, const vdf_col* keys, int nkeys, int
     vdf_status pst = primary_first(c, n, dts, cols, nkeys, order, perm_out, key0_out, ws, ws_bytes, s, nullptr, &done);
     if (pst != VDF_OK) return pst;
     if (!done) {
-        cudaError_t e = vdf::run_sort(p, cols, order, perm_out, key0_out, ws, err_word(c), s, prof_of(c));
-        c->launches += 2 + (uint64_t)p.total_passes;
+        cudaError_t e = ctx_run_sort(c, p, cols, order, perm_out, key0_out, ws, s);
         if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
     }
     return emit_other_keys(c, n, keys, nkeys, perm_out, sorted_keys_out, ws, ws_bytes, s);
@@ -171,10 +172,12 @@ size_t vdf_sort_workspace_bytes(uint64_t n, const int32_t* key_dtypes, int nkeys
     size_t best = 0;
     const int nv = vdf::sort_variant_count();
     for (int a = 0; a < nv; ++a)
-        for (int b = 0; b < nv; ++b) {
-            vdf::SortTuning t{a, b};
-            if (vdf::sort_tuning_valid(t)) best = std::max(best, vdf::make_sort_plan(n, key_dtypes, nkeys, t).ws_bytes);
-        }
+        for (int b = 0; b < nv; ++b)
+            for (int msd = 0; msd < 2; ++msd) {
+                vdf::SortTuning t{a, b, msd, 0};
+                if (vdf::sort_tuning_valid(t))
+                    best = std::max(best, vdf::make_sort_plan(n, key_dtypes, nkeys, t).ws_bytes);
+            }
     return best;
 }
 
@@ -194,9 +197,11 @@ vdf_status vdf_sort_variant_info(int index, int32_t* key_width, int32_t* threads
 
 vdf_status vdf_ctx_set_sort_tuning(vdf_ctx* c, const vdf_sort_tuning* t) {
     if (!c || !t) return VDF_ERR_INVALID_ARG;
-    vdf::SortTuning st{t->pass_variant32, t->pass_variant64};
-    if (!vdf::sort_tuning_valid(st)) return fail(c, VDF_ERR_INVALID_ARG, "invalid sort tuning %d/%d", st.variant32, st.variant64);
     std::lock_guard<std::mutex> lk(c->mu);
+    vdf::SortTuning st = c->tuning;
+    st.variant32 = t->pass_variant32;
+    st.variant64 = t->pass_variant64;
+    if (!vdf::sort_tuning_valid(st)) return fail(c, VDF_ERR_INVALID_ARG, "invalid sort tuning %d/%d", st.variant32, st.variant64);
     c->tuning = st;
     return VDF_OK;
 }
@@ -222,6 +227,51 @@ int vdf_ctx_get_multikey_mode(vdf_ctx* c) {
     if (!c) return -1;
     std::lock_guard<std::mutex> lk(c->mu);
     return c->multikey_mode;
+}
+
+vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* c, int strategy, uint64_t msd_min_rows) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    if (strategy != VDF_SORT_AUTO && strategy != VDF_SORT_LSD)
+        return fail(c, VDF_ERR_INVALID_ARG, "bad sort strategy %d", strategy);
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->tuning.msd = strategy == VDF_SORT_AUTO ? 1 : 0;
+    c->tuning.msd_min_rows = msd_min_rows;
+    return VDF_OK;
+}
+
+vdf_status vdf_ctx_sort_stats(vdf_ctx* c, void* stream, uint64_t* msd_sorts, uint64_t* msd_fallbacks) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(&c->host_pinned[3], fallback_word(c), sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, "read sort statistics");
+    if (msd_sorts) *msd_sorts = c->msd_sorts;
+    if (msd_fallbacks) *msd_fallbacks = (uint32_t)c->host_pinned[3];
+    return VDF_OK;
+}
+
+vdf_status vdf_ctx_get_sort_strategy(vdf_ctx* c, int32_t* strategy, uint64_t* msd_min_rows) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (strategy) *strategy = c->tuning.msd ? VDF_SORT_AUTO : VDF_SORT_LSD;
+    if (msd_min_rows) *msd_min_rows = c->tuning.msd_min_rows;
+    return VDF_OK;
+}
+
+vdf_status vdf_sort_plan_info(uint64_t n, const int32_t* key_dtypes, int nkeys, int strategy, uint64_t msd_min_rows,
+                              int32_t* msd_passes, uint32_t* chunks) {
+    if (!key_dtypes || nkeys < 1 || nkeys > vdf::kMaxKeys) return VDF_ERR_INVALID_ARG;
+    for (int k = 0; k < nkeys; ++k)
+        if (!valid_dtype(key_dtypes[k])) return VDF_ERR_INVALID_ARG;
+    vdf::SortTuning t = vdf::default_sort_tuning();
+    t.msd = strategy == VDF_SORT_AUTO ? 1 : 0;
+    t.msd_min_rows = msd_min_rows;
+    const vdf::SortPlan p = vdf::make_sort_plan(n, key_dtypes, nkeys, t);
+    if (msd_passes) *msd_passes = p.msd ? p.msd_passes : 0;
+    if (chunks) *chunks = p.msd ? p.msd_chunks : 0;
+    return VDF_OK;
 }
 
 size_t vdf_groupby_workspace_bytes(uint64_t n, int nvals) {
@@ -515,7 +565,7 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
     const size_t rec_bytes = (size_t)n * vdf::gather_record_bytes(std::min(ngather, vdf::kMaxGather));
     const size_t seg_bytes = x->groupby ? vdf::segreduce_workspace_bytes(n, x->nagg) : 0;
     size_t tail = std::max(std::max(plan.ws_bytes, seg_bytes), rec_bytes);
-    if (x->nkeys >= 2 && c->multikey_mode == VDF_MULTIKEY_PRIMARY_FIRST && !skey[0]) {
+    if (x->nkeys >= 2 && c->multikey_mode == VDF_MULTIKEY_PRIMARY_FIRST && !skey[0] && !plan.msd) {
         // room for the primary key's sorted copy next to its sort's workspace
         const vdf::SortPlan p0 = vdf::make_sort_plan(n, dts, 1, c->tuning);
         tail = std::max(tail, align256(p0.ws_bytes) + (size_t)n * vdf::dtype_width(dts[0]));
@@ -541,8 +591,7 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
         return st;
     cudaError_t e = cudaSuccess;
     if (!done) {
-        e = vdf::run_sort(plan, cols, x->order, perm, skey[0], tws, err_word(c), s, prof_of(c), x->perm_in);
-        c->launches += 2 + (uint64_t)plan.total_passes;
+        e = ctx_run_sort(c, plan, cols, x->order, perm, skey[0], tws, s, x->perm_in);
         if (e != cudaSuccess) return from_cuda(c, e, "radix sort");
     }
 

@@ -77,8 +77,10 @@ struct vdf_ctx {
     std::mutex mu;
     unsigned char* ws = nullptr;
     size_t ws_cap = 0;
-    unsigned char* dev_small = nullptr;  // [0,4): error bits; [8,16): group count scratch
-    uint64_t* host_pinned = nullptr;     // [0]: group count, [1]: error bits, [2]: tie flag
+    unsigned char* dev_small = nullptr;  // [0,4): error bits; [8,16): group count scratch;
+                                         // [16,20): tie flag; [24,28): MSD fallbacks
+    uint64_t* host_pinned = nullptr;     // [0]: group count, [1]: error bits, [2]: tie flag, [3]: fallbacks
+    uint64_t msd_sorts = 0;              // sorts planned MSD-first
     int multikey_mode = VDF_MULTIKEY_PRIMARY_FIRST;
     std::atomic<uint64_t> launches{0};
     std::string last_error;
@@ -126,6 +128,17 @@ inline vdf::Profiler* prof_of(vdf_ctx* c) { return c->profiling ? &c->prof : nul
 inline uint32_t* err_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->dev_small); }
 inline uint64_t* count_word(vdf_ctx* c) { return reinterpret_cast<uint64_t*>(c->dev_small + 8); }
 inline uint32_t* tie_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->dev_small + 16); }
+inline uint32_t* fallback_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->dev_small + 24); }
+
+// run_sort with the context's error word, profiler and MSD bookkeeping.
+inline cudaError_t ctx_run_sort(vdf_ctx* c, const vdf::SortPlan& p, const void* const* cols, int order,
+                                uint32_t* perm_out, void* key0_out, unsigned char* ws, cudaStream_t s,
+                                const uint32_t* perm_in = nullptr) {
+    if (p.msd && p.n) c->msd_sorts++;
+    c->launches += (uint64_t)vdf::sort_launches(p);
+    return vdf::run_sort(p, cols, order, perm_out, key0_out, ws, err_word(c), s, prof_of(c), perm_in,
+                         fallback_word(c));
+}
 
 inline vdf_status ws_ensure(vdf_ctx* c, size_t bytes) {
     if (bytes <= c->ws_cap) return VDF_OK;

@@ -15,7 +15,7 @@ constexpr int kMaxGather = 8;   // columns per gather launch
 enum KernelClass : int {
     KC_HIST = 0, KC_SCAN = 1, KC_ONESWEEP32 = 2, KC_ONESWEEP64 = 3, KC_GATHER = 4, KC_SEGREDUCE = 5,
     KC_BROADCAST = 6, KC_PACK = 7, KC_SEGSCAN = 8, KC_SEGEMIT = 9, KC_TIES = 10, KC_BATCH = 11,
-    KC_CSV = 12, KC_COUNT = 13
+    KC_CSV = 12, KC_LOCALSORT = 13, KC_FALLBACK = 14, KC_COUNT = 15
 };
 
 // Brackets kernel launches with CUDA events when profiling is enabled.
@@ -46,6 +46,8 @@ struct HistArgs {
     int hist_words;
     uint64_t n;
     uint32_t* hist;
+    const uint32_t* run_flag;  // non-null: the kernel runs only if *run_flag != 0
+    uint32_t* run_count;       // non-null: incremented once when a conditional launch runs
 };
 // Histograms of every pass laid out back to back: pass g has radix[g] bins
 // starting at word off[g]; the scan writes exclusive starts at the same words.
@@ -54,6 +56,7 @@ struct ScanArgs {
     uint32_t* offs;
     uint32_t off[kMaxPasses];
     uint32_t radix[kMaxPasses];
+    const uint32_t* run_flag;  // non-null: the kernel runs only if *run_flag != 0
 };
 
 // One segment of a segmented sort: rows [row_start, row_start + rows) of the
@@ -92,6 +95,10 @@ struct PassArgs {
     uint32_t pass;              // digit pass index
     void* keys_final;           // where a segment's last pass writes its keys
     uint32_t* vals_final;       // ... and its row ids
+    // conditional passes: with run_flag set the pass runs only when
+    // (*run_flag != 0) == (run_when != 0), and otherwise returns at once
+    const uint32_t* run_flag;
+    uint32_t run_when;
 };
 
 
@@ -100,6 +107,10 @@ struct PassArgs {
 struct SortTuning {
     int variant32;
     int variant64;
+    // MSD-first sort (vdf_msd.cu): 1 = used for sorts of one or two key
+    // columns with at least msd_min_rows rows, 0 = never
+    int msd = 0;
+    uint64_t msd_min_rows = 0;
 };
 SortTuning default_sort_tuning();
 bool sort_tuning_valid(const SortTuning& t);
@@ -117,17 +128,70 @@ struct SortPlan {
     size_t off_keys[2], off_vals[2], off_offs, off_zero, off_hist, off_counters, off_status[2];
     size_t zero_bytes;
     size_t ws_bytes;
+    // MSD-first sort: msd_passes global passes over the top 8-bit digits of
+    // key 0, then one CTA per chunk of whole buckets sorts the rest in shared
+    // memory; the LSD passes above run only if that fails (a flag on the
+    // device decides, no host round trip).
+    bool msd;
+    int msd_passes;
+    uint32_t msd_chunk_rows;   // nominal rows per chunk
+    uint32_t msd_chunks;       // ceil(n / msd_chunk_rows)
+    size_t off_msd_hist, off_msd_offs, off_msd_flag, off_chunks;
 };
+// MSD-first sort limits: rows one CTA sorts in shared memory, the longest
+// run of equal high key bits the shared-memory finish ranks directly, and the
+// most top digits that go through global passes.
+constexpr uint32_t kMsdCap = 4096;
+constexpr uint32_t kMsdRunMax = 64;
+constexpr int kMsdMaxPasses = 3;
+constexpr uint32_t kMsdBucketRows = 1536;           // planned average bucket
+constexpr uint64_t kMsdDefaultMinRows = 1u << 20;   // smaller sorts: LSD passes
+struct MsdHistArgs {
+    const void* keys;  // raw key 0 column
+    int dtype, invert, first_digit, ndig;
+    uint64_t n;
+    uint32_t* hist;    // [ndig][256]
+};
+struct MsdChunkArgs {
+    const void* keys;  // order images sorted by their top bits
+    uint64_t n;
+    uint32_t chunk_rows, nchunks, pshift;
+    uint32_t* chunk_start;  // [nchunks + 1]
+    uint32_t* flag;
+};
+struct MsdLocalArgs {
+    const void* keys;        // order images of key 0 sorted by their top bits
+    const uint32_t* vals;    // their row ids
+    const uint32_t* chunk_start;
+    uint64_t n;
+    const void* sec;         // raw key 1 column (null for one key)
+    int sec_dtype, dtype, invert, reverse;
+    uint32_t lo_bits;        // key 0 bits below the shared-memory passes
+    uint32_t* flag;
+    uint32_t* err;
+    void* keys_out;          // raw sorted key 0 (may be null)
+    uint32_t* perm_out;
+};
+cudaError_t msd_hist(const MsdHistArgs& a, int width, cudaStream_t s);
+cudaError_t msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t top_limit, uint32_t* flag,
+                     cudaStream_t s);
+cudaError_t msd_chunks(const MsdChunkArgs& a, int width, cudaStream_t s);
+cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, cudaStream_t s);
+// Kernel launches run_sort makes for a plan (conditional ones included).
+int sort_launches(const SortPlan& p);
 
 SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const SortTuning& tuning);
 // Sorts; writes perm_out (and key0_out = raw sorted most-significant key, may
 // be null).  Bounded waits that give up OR their ErrBits into *err.  With
 // perm_in (a permutation of [0, n)) the rows are sorted as seen through it
 // and perm_out is the composed permutation.
+// msd_fallbacks (optional, device word): incremented each time an MSD-first
+// plan falls back to the LSD passes.
 cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
                      void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof = nullptr,
-                     const uint32_t* perm_in = nullptr);
+                     const uint32_t* perm_in = nullptr, uint32_t* msd_fallbacks = nullptr);
 cudaError_t prepare_sort_kernels();
+cudaError_t prepare_msd_kernels();
 // *flag |= 1 when two neighbouring elements of a sorted key column (4- or
 // 8-byte elements) have the same bits.
 cudaError_t flag_adjacent_ties(const void* sorted_keys, int width, uint64_t n, uint32_t* flag, cudaStream_t s,

@@ -1,0 +1,488 @@
+// vdf_msd.cu -- most-significant-digit-first radix sort with a shared-memory
+// finish, for sorts by one or two key columns.
+//
+// The reference sorts with LSD radix passes over every 16-bit digit of the
+// key (radix_sort_uint64_mt.inl:6-166: four passes for an 8-byte key, each a
+// histogram and a scatter of (key, size_t idx)), and composes a second key by
+// a second sort through the in/out idx.  The LSD onesweep passes of
+// vdf_radix.cu follow that shape with 8-bit digits: eight passes over HBM for
+// an 8-byte key.  Here only the top P digits of key 0 go through HBM-wide
+// passes, so that rows sharing the top 8P bits ("buckets") end up
+// contiguous; the rest is finished per chunk of whole buckets in shared
+// memory:
+//
+//   1. k_msd_hist    histograms of the top P digits of key 0 (one read)
+//   2. k_msd_scan    their exclusive scans; a top-digit bin holding more rows
+//                    than its buckets could possibly fit in chunks flags the
+//                    MSD path as failed up front
+//   3. P onesweep passes (vdf_radix.cu kernels), stable, over digits
+//      W-P .. W-1 of key 0, least significant first: afterwards the rows
+//      are stably sorted by their top 8P bits
+//   4. k_msd_chunks  chunk c holds the whole buckets that start in
+//                    [c*T, (c+1)*T); found by a two-level warp search for
+//                    the first bucket boundary at or after c*T
+//   5. k_msd_local   one CTA per chunk (<= kMsdCap rows): stable 8-bit LSD
+//                    passes in shared memory over the digits of key 0 above
+//                    its low 32 bits (8-byte keys; all digits for 4-byte
+//                    keys) that vary inside the chunk, then each run of rows
+//                    with equal high bits is ranked directly by (low 32
+//                    bits, key 1's order image, position) -- key 1 read
+//                    through the row id only for rows in such runs -- and
+//                    the raw sorted key 0 and the permutation are written.
+//
+// Every pass is stable and ties keep their row order, so the result is
+// exactly the stable order over all keys.  Where the data defeats the plan
+// (a chunk above kMsdCap rows, or an unsorted run longer than kMsdRunMax),
+// a device flag is set and the LSD passes that follow in the same stream run
+// from the raw columns instead (they return at once while the flag is
+// clear); no host round trip either way.
+#include "vdf_common.cuh"
+#include "vdf_internal.h"
+
+namespace vdf {
+
+// ---------------------------------------------------------------------------
+// 1. histograms of the top digits of key 0
+// ---------------------------------------------------------------------------
+template <typename K>
+__global__ void __launch_bounds__(512) k_msd_hist(MsdHistArgs a) {
+    __shared__ uint32_t h[kMsdMaxPasses * 256];
+    for (int i = threadIdx.x; i < a.ndig * 256; i += blockDim.x) h[i] = 0;
+    __syncthreads();
+    const K* src = static_cast<const K*>(a.keys);
+    const uint64_t n = a.n;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    constexpr int R = 4;  // four keys per thread per round, all loaded first
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += R * stride) {
+        K k[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) k[r] = i0 + r * stride < n ? ldg_stream(src + i0 + r * stride) : K(0);
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (i0 + r * stride >= n) break;
+            const K x = KeyOps<K>::order(k[r], a.dtype, a.invert);
+            for (int p = 0; p < a.ndig; ++p)
+                atomicAdd(&h[p * 256 + (uint32_t)((x >> (8 * (a.first_digit + p))) & 0xff)], 1u);
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < a.ndig * 256; i += blockDim.x)
+        if (h[i]) atomicAdd(&a.hist[i], h[i]);
+}
+
+// ---------------------------------------------------------------------------
+// 2. exclusive scans (one CTA of 256 threads per digit) + the up-front check
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_msd_scan(const uint32_t* hist, uint32_t* offs, int ndig,
+                                                  uint32_t top_limit, uint32_t* flag) {
+    __shared__ uint32_t wsum[8];
+    const int p = blockIdx.x, b = threadIdx.x, lane = b & 31, warp = b >> 5;
+    const uint32_t v = hist[p * 256 + b];
+    uint32_t incl = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t base = 0;
+    for (int w = 0; w < warp; ++w) base += wsum[w];
+    offs[p * 256 + b] = base + incl - v;
+    // a top digit shared by more rows than 256^(P-1) full chunks hold: some
+    // bucket under it cannot fit one chunk
+    if (p == ndig - 1 && v > top_limit) atomicOr(flag, 1u);
+}
+
+// ---------------------------------------------------------------------------
+// 4. chunk starts: one warp per chunk
+// ---------------------------------------------------------------------------
+template <typename K>
+__global__ void __launch_bounds__(256) k_msd_chunks(MsdChunkArgs a) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t c = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (c > a.nchunks) return;
+    uint32_t failed = 0;  // read once per warp: the ballots below need the whole warp
+    if (lane == 0) failed = *static_cast<volatile uint32_t*>(a.flag);
+    if (__shfl_sync(0xffffffffu, failed, 0)) return;
+    const K* keys = static_cast<const K*>(a.keys);
+    const uint64_t n = a.n;
+    uint64_t out;
+    if (c == 0) {
+        out = 0;
+    } else if (c == a.nchunks) {
+        out = n;
+    } else {
+        // first i >= x whose top bits differ from row x-1's; rows are sorted
+        // by their top bits, so "differs" is false up to the boundary and
+        // true after it, and a probe tells on which side it lies
+        const uint64_t x = (uint64_t)c * a.chunk_rows;  // < n
+        const K p0 = keys[x - 1] >> a.pshift;
+        constexpr uint32_t S = kMsdCap / 32;  // level-1 probe spacing
+        const uint64_t q = min(x + (uint64_t)(lane + 1) * S - 1, n - 1);
+        const uint32_t hit = __ballot_sync(0xffffffffu, (keys[q] >> a.pshift) != p0);
+        if (!hit) {
+            // kMsdCap rows after x still share row x-1's top bits: that bucket
+            // is larger than a chunk can hold (or runs to the end)
+            out = n;
+            if (x + (uint64_t)32 * S - 1 < n - 1 && lane == 0) atomicOr(a.flag, 1u);
+        } else {
+            const uint32_t L = __ffs(hit) - 1;
+            const uint64_t lo = x + (uint64_t)L * S;  // every row before lo shares p0
+            const uint64_t hi = min(x + (uint64_t)(L + 1) * S - 1, n - 1);  // differs at hi
+            out = hi;
+#pragma unroll
+            for (uint32_t r = 0; r < S / 32; ++r) {
+                const uint64_t pos = lo + r * 32 + lane;
+                const bool d = pos >= hi || (keys[pos] >> a.pshift) != p0;
+                const uint32_t b = __ballot_sync(0xffffffffu, d);
+                if (b) {
+                    out = lo + r * 32 + (__ffs(b) - 1);
+                    break;
+                }
+            }
+        }
+    }
+    if (lane == 0) a.chunk_start[c] = (uint32_t)out;
+}
+
+// ---------------------------------------------------------------------------
+// 5. shared-memory finish, one CTA per chunk
+// ---------------------------------------------------------------------------
+template <typename K, int THREADS, int ITEMS>
+struct LocalCfg {
+    static constexpr int WARPS = THREADS / 32;
+    static constexpr int CAP = THREADS * ITEMS;
+    static constexpr size_t KEYS = (size_t)CAP * sizeof(K);
+    static constexpr size_t VALS = (size_t)CAP * 4;
+    static constexpr size_t SEC = (size_t)CAP * 8;  // key 1 images of rows in runs
+    static constexpr size_t CNT = (size_t)WARPS * 256 * 4;
+    static constexpr size_t MISC = 16 * 4 + (size_t)WARPS * 4 + (size_t)2 * WARPS * 8;
+    static constexpr size_t SMEM = KEYS + VALS + SEC + CNT + MISC;
+};
+
+template <int THREADS>
+__device__ __forceinline__ uint32_t local_excl_scan(uint32_t v, uint32_t* wsum, uint32_t* total) {
+    constexpr int WARPS = THREADS / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += t;
+    }
+    if (lane == 31) wsum[warp] = incl;
+    __syncthreads();
+    uint32_t base = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+        const uint32_t x = wsum[w];
+        base += (w < warp) ? x : 0u;
+        all += x;
+    }
+    *total = all;
+    return base + incl - v;
+}
+
+__device__ __forceinline__ uint64_t sec_image(const void* col, int dt, uint32_t row, bool invert) {
+    if (dtype_width(dt) == 8) return order64(ld_rand8(static_cast<const unsigned long long*>(col) + row), dt, invert);
+    return (uint64_t)order32(ld_rand4(static_cast<const uint32_t*>(col) + row), dt, invert);
+}
+
+// MATCH: 0 = one ballot per digit bit, 1 = match.any.
+template <typename K, int THREADS, int ITEMS, int MATCH>
+__global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
+    using C = LocalCfg<K, THREADS, ITEMS>;
+    constexpr int WARPS = C::WARPS, RADIX = 256;
+    constexpr uint32_t CAP = (uint32_t)C::CAP;
+    constexpr int KBITS = 8 * (int)sizeof(K);
+    extern __shared__ __align__(16) unsigned char smem[];
+    K* sk = reinterpret_cast<K*>(smem);
+    uint32_t* sv = reinterpret_cast<uint32_t*>(smem + C::KEYS);
+    uint64_t* ssec = reinterpret_cast<uint64_t*>(smem + C::KEYS + C::VALS);
+    uint32_t* wcnt = reinterpret_cast<uint32_t*>(smem + C::KEYS + C::VALS + C::SEC);  // [WARPS][RADIX]
+    uint32_t* misc = wcnt + WARPS * RADIX;                                            // [0]: failure seen
+    uint32_t* wsum = misc + 16;                                                       // [WARPS]
+    K* wor = reinterpret_cast<K*>(smem + C::KEYS + C::VALS + C::SEC + C::CNT + 16 * 4 + WARPS * 4);
+    K* wand = wor + WARPS;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // One thread reads the flag and the chunk bounds for the whole CTA (the
+    // flag may be raised by another CTA meanwhile; every thread must take
+    // the same branch around the barriers below).
+    if (tid == 0) {
+        misc[1] = *static_cast<volatile uint32_t*>(a.flag);
+        misc[2] = a.chunk_start[blockIdx.x];
+        misc[3] = a.chunk_start[blockIdx.x + 1];
+        misc[0] = 0;
+    }
+    __syncthreads();
+    if (misc[1]) return;  // the plan failed earlier: the LSD passes take over
+    const uint32_t s0 = misc[2], s1 = misc[3];
+    if (s1 <= s0) return;
+    const uint32_t m = s1 - s0;
+    if (m > CAP || s1 > a.n) {
+        if (tid == 0) atomicOr(a.flag, 1u);
+        return;
+    }
+    const uint32_t ia = (m + THREADS - 1) / THREADS;  // items per thread in use
+    const uint32_t lt = lanemask_lt();
+
+    // ---- load: item j of a thread sits at position (warp * ia + j) * 32 + lane;
+    //      slots past m hold all-ones keys, which every pass ranks last
+    K key[ITEMS];
+    uint32_t val[ITEMS];
+    const K* kin = static_cast<const K*>(a.keys) + s0;
+    const uint32_t* vin = a.vals + s0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+        key[j] = ~K(0);
+        val[j] = 0;
+        if (j < (int)ia && pos < m) {
+            key[j] = ldg_stream(kin + pos);
+            val[j] = ldg_stream(vin + pos);
+        }
+    }
+
+    // ---- which digits vary inside the chunk
+    K vor = 0, vand = ~K(0);
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+        if (j < (int)ia && pos < m) {
+            vor |= key[j];
+            vand &= key[j];
+        }
+    }
+#pragma unroll
+    for (int d = 16; d >= 1; d >>= 1) {
+        vor |= __shfl_xor_sync(0xffffffffu, vor, d);
+        vand &= __shfl_xor_sync(0xffffffffu, vand, d);
+    }
+    if (lane == 0) {
+        wor[warp] = vor;
+        wand[warp] = vand;
+    }
+    __syncthreads();
+    vor = 0;
+    vand = ~K(0);
+#pragma unroll
+    for (int w = 0; w < WARPS; ++w) {
+        vor |= wor[w];
+        vand &= wand[w];
+    }
+    const K vary = vor ^ vand;
+
+    // ---- stable 8-bit LSD passes in shared memory over the varying digits
+    //      of key 0 from digit lo_bits / 8 up
+    bool sorted_in_smem = false;
+    uint32_t* my = wcnt + warp * RADIX;
+    for (int dg = (int)(a.lo_bits / 8); dg < KBITS / 8; ++dg) {
+        const uint32_t shift = 8u * dg;
+        if (((vary >> shift) & 0xff) == 0) continue;
+        for (int i = tid; i < WARPS * RADIX; i += THREADS) wcnt[i] = 0;
+        __syncthreads();
+        uint32_t rank[ITEMS];
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            rank[j] = 0;
+            if (j < (int)ia) {
+                const uint32_t d = (uint32_t)(key[j] >> shift) & 0xffu;
+                uint32_t peers;
+                if constexpr (MATCH == 1) {
+                    peers = __match_any_sync(0xffffffffu, d);
+                } else {
+                    peers = 0xffffffffu;
+#pragma unroll
+                    for (int bt = 0; bt < 8; ++bt) {
+                        const uint32_t bal = __ballot_sync(0xffffffffu, (d >> bt) & 1u);
+                        peers &= ((d >> bt) & 1u) ? bal : ~bal;
+                    }
+                }
+                const int leader = __ffs(peers) - 1;
+                uint32_t base = 0;
+                if (lane == leader) {
+                    base = my[d];
+                    my[d] = base + __popc(peers);
+                }
+                __syncwarp();
+                base = __shfl_sync(0xffffffffu, base, leader);
+                rank[j] = base + __popc(peers & lt);
+            }
+        }
+        __syncthreads();
+        // bin-major exclusive prefix over (bin, warp)
+        uint32_t tot = 0;
+        if (tid < RADIX) {
+#pragma unroll
+            for (int w = 0; w < WARPS; ++w) {
+                const uint32_t c = wcnt[w * RADIX + tid];
+                wcnt[w * RADIX + tid] = tot;
+                tot += c;
+            }
+        }
+        uint32_t all;
+        const uint32_t start = local_excl_scan<THREADS>(tot, wsum, &all);
+        if (tid < RADIX)
+#pragma unroll
+            for (int w = 0; w < WARPS; ++w) wcnt[w * RADIX + tid] += start;
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (j < (int)ia) {
+                const uint32_t d = (uint32_t)(key[j] >> shift) & 0xffu;
+                uint32_t r = rank[j] + my[d];
+                if (r >= CAP) {  // never when the counts are consistent
+                    atomicOr(a.err, ERR_BAD_INDEX);
+                    r = ((uint32_t)warp * ia + j) * 32 + lane;
+                }
+                sk[r] = key[j];
+                sv[r] = val[j];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (j < (int)ia) {
+                const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+                key[j] = sk[pos];
+                val[j] = sv[pos];
+            }
+        }
+        sorted_in_smem = true;
+    }
+    if (!sorted_in_smem) {
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (j < (int)ia) {
+                const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+                sk[pos] = key[j];
+                sv[pos] = val[j];
+            }
+        }
+        __syncthreads();
+    }
+
+    // ---- runs of equal high bits, ranked by (low bits, key 1, position)
+    const bool fix = a.lo_bits > 0 || a.sec != nullptr;
+    const uint32_t hs = a.lo_bits;  // high part = key >> hs
+    const K lo_mask = hs ? (K)((((K)1) << hs) - 1) : K(0);
+    uint32_t newpos[ITEMS];
+    bool inrun[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+        newpos[j] = pos;
+        inrun[j] = false;
+        if (fix && j < (int)ia && pos < m) {
+            const K h = key[j] >> hs;
+            inrun[j] = (pos > 0 && (sk[pos - 1] >> hs) == h) || (pos + 1 < m && (sk[pos + 1] >> hs) == h);
+            if (inrun[j] && a.sec) ssec[pos] = sec_image(a.sec, a.sec_dtype, val[j], a.invert != 0);
+        }
+    }
+    if (fix) {
+        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            if (!inrun[j]) continue;
+            const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+            const K h = key[j] >> hs;
+            const K lo = key[j] & lo_mask;
+            const uint64_t sc = a.sec ? ssec[pos] : 0;
+            uint32_t s = pos, e = pos + 1;
+            while (s > 0 && pos - s < kMsdRunMax && (sk[s - 1] >> hs) == h) --s;
+            while (e < m && e - pos <= kMsdRunMax && (sk[e] >> hs) == h) ++e;
+            if (e - s > kMsdRunMax) {
+                // a long run: fine if it already is in order (e.g. equal
+                // keys), otherwise the plan fails
+                if (pos > s) {
+                    const K plo = sk[pos - 1] & lo_mask;
+                    const uint64_t psc = a.sec ? ssec[pos - 1] : 0;
+                    if (plo > lo || (plo == lo && psc > sc)) misc[0] = 1;
+                }
+                continue;
+            }
+            uint32_t r = 0;
+            for (uint32_t t = s; t < e; ++t) {
+                const K tlo = sk[t] & lo_mask;
+                const uint64_t tsc = a.sec ? ssec[t] : 0;
+                r += (tlo < lo || (tlo == lo && (tsc < sc || (tsc == sc && t < pos)))) ? 1u : 0u;
+            }
+            newpos[j] = s + r;
+        }
+        __syncthreads();
+        if (misc[0]) {
+            if (tid == 0) atomicOr(a.flag, 1u);
+            return;
+        }
+    }
+
+    // ---- output: raw sorted key 0 and the permutation
+    K* kout = static_cast<K*>(a.keys_out);
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+        if (j < (int)ia && pos < m) {
+            uint64_t gp = (uint64_t)s0 + newpos[j];
+            if (a.reverse) gp = a.n - 1 - gp;
+            stg_stream(a.perm_out + gp, val[j]);
+            if (kout) stg_stream(kout + gp, KeyOps<K>::unorder(key[j], a.dtype, a.invert != 0));
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kLocalThreads = 512, kLocalItems = 8;
+static_assert(kLocalThreads * kLocalItems == (int)kMsdCap, "chunk capacity");
+using Local64 = LocalCfg<uint64_t, kLocalThreads, kLocalItems>;
+using Local32 = LocalCfg<uint32_t, kLocalThreads, kLocalItems>;
+#define VDF_LOCAL64 k_msd_local<uint64_t, kLocalThreads, kLocalItems, 1>
+#define VDF_LOCAL32 k_msd_local<uint32_t, kLocalThreads, kLocalItems, 1>
+
+int sm_count() {
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms;
+}
+}  // namespace
+
+cudaError_t prepare_msd_kernels() {
+    cudaError_t e = cudaFuncSetAttribute(VDF_LOCAL64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Local64::SMEM);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(VDF_LOCAL32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Local32::SMEM);
+}
+
+cudaError_t msd_hist(const MsdHistArgs& a, int width, cudaStream_t s) {
+    const uint64_t want = (a.n + 511) / 512;
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sm_count() * 4));
+    if (width == 8) k_msd_hist<uint64_t><<<grid, 512, 0, s>>>(a);
+    else k_msd_hist<uint32_t><<<grid, 512, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t top_limit, uint32_t* flag,
+                     cudaStream_t s) {
+    k_msd_scan<<<ndig, 256, 0, s>>>(hist, offs, ndig, top_limit, flag);
+    return cudaGetLastError();
+}
+
+cudaError_t msd_chunks(const MsdChunkArgs& a, int width, cudaStream_t s) {
+    const uint32_t grid = (a.nchunks + 1 + 7) / 8;
+    if (width == 8) k_msd_chunks<uint64_t><<<grid, 256, 0, s>>>(a);
+    else k_msd_chunks<uint32_t><<<grid, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, cudaStream_t s) {
+    if (nchunks == 0) return cudaSuccess;
+    if (width == 8) VDF_LOCAL64<<<nchunks, kLocalThreads, Local64::SMEM, s>>>(a);
+    else VDF_LOCAL32<<<nchunks, kLocalThreads, Local32::SMEM, s>>>(a);
+    return cudaGetLastError();
+}
+
+}  // namespace vdf

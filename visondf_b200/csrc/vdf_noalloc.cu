@@ -85,8 +85,8 @@ extern "C" vdf_status vdf_sort_argsort_noalloc(uint64_t n, const vdf_col* keys, 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     uint32_t* err = reinterpret_cast<uint32_t*>(base);
     // The array keeps the previous call's contents: the error word is cleared
-    // here and run_sort clears its histograms, tile counters and first status
-    // buffer itself.
+    // here and run_sort clears its histograms, tile counters, look-back status
+    // and plan flag itself.
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(uint32_t), s);
     if (e == cudaSuccess) {
         void* key0 = sorted_keys_out ? sorted_keys_out[0] : nullptr;
@@ -109,6 +109,30 @@ extern "C" vdf_status vdf_sort_argsort_noalloc(uint64_t n, const vdf_col* keys, 
     if (e != cudaSuccess) {
         cudaGetLastError();
         return e == cudaErrorMemoryAllocation ? VDF_ERR_OOM : VDF_ERR_DEVICE;
+    }
+    return VDF_OK;
+}
+
+// The error word of the last call on the current device: bounded waits that
+// gave up and out-of-range row ids set bits in it (the same bits
+// vdf_ctx_check reports for a context).  A 4-byte device-to-host copy into
+// the caller's memory, then a wait for `stream`; nothing is allocated.
+extern "C" vdf_status vdf_sort_noalloc_error(uint32_t* host_out, void* stream) {
+    if (!host_out) return VDF_ERR_INVALID_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return VDF_ERR_DEVICE;
+    }
+    unsigned char* base = nullptr;
+    vdf_status st = scratch_on(dev, &base);
+    if (st != VDF_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(host_out, base, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return VDF_ERR_DEVICE;
     }
     return VDF_OK;
 }

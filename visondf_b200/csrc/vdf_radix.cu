@@ -39,6 +39,8 @@ namespace vdf {
 template <int FIXED_BITS>
 __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
     extern __shared__ uint32_t sh_hist[];  // [hist_words]
+    if (a.run_flag && *a.run_flag == 0) return;  // conditional launch not taken
+    if (a.run_count && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.run_count, 1u);
     for (int i = threadIdx.x; i < a.hist_words; i += blockDim.x) sh_hist[i] = 0;
     __syncthreads();
 
@@ -96,6 +98,7 @@ __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
 __global__ void __launch_bounds__(256) k_hist_scan(ScanArgs a) {
     constexpr int PER = kMaxRadix / 256;
     __shared__ uint32_t warp_tot[8];
+    if (a.run_flag && *a.run_flag == 0) return;  // conditional launch not taken
     const uint32_t radix = a.radix[blockIdx.x];
     const uint32_t* h = a.hist + a.off[blockIdx.x];
     uint32_t* o = a.offs + a.off[blockIdx.x];
@@ -278,6 +281,9 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     uint32_t* wmask = wsum + WARPS;  // match method 3: [2][WARPS][RADIX]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // A conditional pass not taken returns before touching anything; the
+    // flag was written by an earlier launch, so every thread reads the same.
+    if (a.run_flag && ((*a.run_flag != 0) != (a.run_when != 0))) return;
     if (tid == 0) misc[0] = atomicAdd(a.tile_counter, 1u);
     for (int i = tid; i < WARPS * RADIX; i += THREADS) wcnt[i] = 0;
     if constexpr (MATCH == 3)
@@ -756,11 +762,22 @@ bool sort_tuning_valid(const SortTuning& t) {
            t.variant64 >= 0 && t.variant64 < kNumVariants && kVariants[t.variant64].width == 8;
 }
 
-SortTuning default_sort_tuning() { return SortTuning{1, 2}; }
+SortTuning default_sort_tuning() { return SortTuning{1, 2, 1, kMsdDefaultMinRows}; }
 
 static int tile_rows(const SortTuning& t, int width) {
     const PassVariant& v = variant_for(t, width);
     return v.threads * v.items;
+}
+
+// Global MSD passes for n rows: the fewest top digits after which a bucket
+// averages at most kMsdBucketRows rows, so that with chunks of nominal
+// kMsdCap / 2 rows a chunk of whole buckets stays within kMsdCap for
+// uniformly spread keys (the average bucket plus six standard deviations).
+static int msd_passes_for(uint64_t n, int width) {
+    const int maxp = std::min(kMsdMaxPasses, width - 1);
+    for (int p = 1; p <= maxp; ++p)
+        if (n <= (uint64_t)kMsdBucketRows << (8 * p)) return p;
+    return 0;
 }
 
 SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const SortTuning& tuning) {
@@ -783,6 +800,11 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
         uint32_t t = (uint32_t)((n + rows - 1) / rows);
         if (t > max_tiles) max_tiles = t;
     }
+    // MSD-first for one or two keys when the key-0 passes use 8-bit digits
+    if (tuning.msd && nkeys <= 2 && n >= 2 && n >= tuning.msd_min_rows && p.bits[0] == 8) {
+        p.msd_passes = msd_passes_for(n, p.width[0]);
+        p.msd = p.msd_passes > 0;
+    }
     // passes are numbered in processing order (least-significant key first);
     // their histograms follow one another in that order
     int total = 0, words = 0;
@@ -798,29 +820,53 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
     size_t off = 0;
     const size_t A = 256;
     const size_t status_bytes = (size_t)max_tiles * p.max_radix * 4;
+    const int msd_p = p.msd ? p.msd_passes : 0;
     p.off_keys[0] = off; off = align_up(off + n * (size_t)maxw, A);
     p.off_keys[1] = off; off = align_up(off + n * (size_t)maxw, A);
     p.off_vals[0] = off; off = align_up(off + n * 4, A);
     p.off_vals[1] = off; off = align_up(off + n * 4, A);
     p.off_offs = off; off = align_up(off + (size_t)words * 4, A);
-    // zeroed region: hist | counters+err | status[0]
+    if (p.msd) {
+        p.msd_chunk_rows = kMsdCap / 2;
+        p.msd_chunks = (uint32_t)((n + p.msd_chunk_rows - 1) / p.msd_chunk_rows);
+        p.off_msd_offs = off; off = align_up(off + (size_t)msd_p * 256 * 4, A);
+        p.off_chunks = off; off = align_up(off + ((size_t)p.msd_chunks + 1) * 4, A);
+    }
+    // zeroed region: hist | counters+err | status[0] (| status[1] | MSD
+    // histograms | MSD flag: with the MSD plan the LSD passes may start after
+    // passes that never ran, so both status buffers start clear)
     p.off_zero = off;
     p.off_hist = off; off = align_up(off + (size_t)words * 4, A);
-    p.off_counters = off; off = align_up(off + (size_t)(total + 1) * 4, A);
+    p.off_counters = off; off = align_up(off + (size_t)(total + msd_p + 1) * 4, A);
     p.off_status[0] = off; off = align_up(off + status_bytes, A);
-    p.zero_bytes = off - p.off_zero;
-    p.off_status[1] = off; off = align_up(off + status_bytes, A);
+    if (p.msd) {
+        p.off_status[1] = off; off = align_up(off + status_bytes, A);
+        p.off_msd_hist = off; off = align_up(off + (size_t)msd_p * 256 * 4, A);
+        p.off_msd_flag = off; off = align_up(off + 4, A);
+        p.zero_bytes = off - p.off_zero;
+    } else {
+        p.zero_bytes = off - p.off_zero;
+        p.off_status[1] = off; off = align_up(off + status_bytes, A);
+    }
     p.ws_bytes = off;
     return p;
 }
 
-cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
-                     void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof,
-                     const uint32_t* perm_in) {
+int sort_launches(const SortPlan& p) {
+    // histogram + scan + passes, plus for the MSD plan its histogram, scan,
+    // passes, chunk search and shared-memory finish (the LSD kernels are
+    // launched in either case and return at once when not needed)
+    return 2 + p.total_passes + (p.msd ? 4 + p.msd_passes : 0);
+}
+
+namespace {
+// The LSD passes over all keys (first_g: global index of the first pass, for
+// tile counters and status parity; run_flag: conditional launches).
+cudaError_t run_lsd(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out, void* key0_out,
+                    unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof, const uint32_t* perm_in,
+                    int first_g, const uint32_t* run_flag, uint32_t* run_count) {
     const uint64_t n = p.n;
-    if (n == 0) return cudaSuccess;
-    cudaError_t e = cudaMemsetAsync(ws + p.off_zero, 0, p.zero_bytes, s);
-    if (e != cudaSuccess) return e;
+    cudaError_t e;
     uint32_t* hist = reinterpret_cast<uint32_t*>(ws + p.off_hist);
     uint32_t* offs = reinterpret_cast<uint32_t*>(ws + p.off_offs);
     uint32_t* counters = reinterpret_cast<uint32_t*>(ws + p.off_counters);
@@ -837,9 +883,12 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
     h.hist = hist;
     h.ncols = p.nkeys;
     h.hist_words = p.hist_words;
+    h.run_flag = run_flag;
+    h.run_count = run_count;
     ScanArgs sc{};
     sc.hist = hist;
     sc.offs = offs;
+    sc.run_flag = run_flag;
     for (int k = 0; k < p.nkeys; ++k) {
         h.col[k].data = key_cols[k];
         h.col[k].dtype = p.dtype[k];
@@ -860,21 +909,22 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
         uint64_t want = (n + 511) / 512;
         uint32_t grid = (uint32_t)(want < (uint64_t)sms * 4 ? want : (uint64_t)sms * 4);
         if (grid == 0) grid = 1;
-        if (prof) prof->begin(KC_HIST, s);
+        if (prof) prof->begin(run_flag ? KC_FALLBACK : KC_HIST, s);
         bool all8 = true;
         for (int k = 0; k < p.nkeys; ++k) all8 = all8 && p.bits[k] == 8;
         if (all8) k_digit_hist<8><<<grid, 512, smem, s>>>(h);
         else k_digit_hist<0><<<grid, 512, smem, s>>>(h);
-        if (prof) prof->end(KC_HIST, s);
+        if (prof) prof->end(run_flag ? KC_FALLBACK : KC_HIST, s);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
-        if (prof) prof->begin(KC_SCAN, s);
+        if (prof) prof->begin(run_flag ? KC_FALLBACK : KC_SCAN, s);
         k_hist_scan<<<p.total_passes, 256, 0, s>>>(sc);
-        if (prof) prof->end(KC_SCAN, s);
+        if (prof) prof->end(run_flag ? KC_FALLBACK : KC_SCAN, s);
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
 
+    const int last_g = first_g + p.total_passes - 1;
     int kcur = -1, vcur = -1;
-    int g = 0;  // global pass counter (processing order)
+    int g = first_g;  // global pass counter (processing order)
     for (int k = p.nkeys - 1; k >= 0; --k) {
         const int w = p.width[k];
         const PassVariant& var = variant_for(p.tuning, w);
@@ -888,11 +938,13 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
             a.reverse = reverse;
             a.bin_offsets = offs + p.hist_off[k] + (size_t)q * p.radix[k];
             a.status = status[g & 1];
-            a.status_next = (g + 1 < p.total_passes) ? status[(g + 1) & 1] : nullptr;
+            a.status_next = (g < last_g) ? status[(g + 1) & 1] : nullptr;
             a.status_rows = p.max_tiles;
             a.status_row_words = (uint32_t)p.max_radix;
             a.tile_counter = counters + g;
             a.err = err;
+            a.run_flag = run_flag;
+            a.run_when = 1;
             int mode;
             if (q == 0 && k == p.nkeys - 1) {
                 // first pass: the rows themselves, or the rows as seen through
@@ -919,16 +971,136 @@ cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, 
                 a.keys_out = kbuf[kn];
                 a.vals_out = vbuf[vn];
             }
-            if (prof) prof->begin(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
+            // conditional passes (the MSD plan's fallback) are timed apart
+            // from the passes that always run
+            const int cls = run_flag ? KC_FALLBACK : (w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64);
+            if (prof) prof->begin(cls, s);
             var.k[mode][fin ? 1 : 0]<<<tiles, var.threads, var.smem, s>>>(a);
             e = cudaGetLastError();
-            if (prof) prof->end(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
+            if (prof) prof->end(cls, s);
             if (e != cudaSuccess) return e;
             kcur = kn;
             vcur = vn;
         }
     }
     return cudaSuccess;
+}
+
+// MSD-first front half: top-digit histograms and scans, the global passes
+// over the top digits of key 0, the chunk search and the shared-memory
+// finish.  Leaves the flag at ws + off_msd_flag set if the plan failed.
+cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out, void* key0_out,
+                    unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof, const uint32_t* perm_in) {
+    const uint64_t n = p.n;
+    const int w = p.width[0];
+    const int P = p.msd_passes;
+    const int ndigits = w;  // 8-bit digits
+    const int first = ndigits - P;
+    cudaError_t e;
+    uint32_t* mhist = reinterpret_cast<uint32_t*>(ws + p.off_msd_hist);
+    uint32_t* moffs = reinterpret_cast<uint32_t*>(ws + p.off_msd_offs);
+    uint32_t* flag = reinterpret_cast<uint32_t*>(ws + p.off_msd_flag);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(ws + p.off_counters);
+    uint32_t* status[2] = {reinterpret_cast<uint32_t*>(ws + p.off_status[0]),
+                           reinterpret_cast<uint32_t*>(ws + p.off_status[1])};
+    void* kbuf[2] = {ws + p.off_keys[0], ws + p.off_keys[1]};
+    uint32_t* vbuf[2] = {reinterpret_cast<uint32_t*>(ws + p.off_vals[0]),
+                         reinterpret_cast<uint32_t*>(ws + p.off_vals[1])};
+    const bool invert = (order == 1);
+
+    MsdHistArgs mh{key_cols[0], p.dtype[0], invert ? 1 : 0, first, P, n, mhist};
+    if (prof) prof->begin(KC_HIST, s);
+    e = msd_hist(mh, w, s);
+    if (prof) prof->end(KC_HIST, s);
+    if (e != cudaSuccess) return e;
+    // a top-digit bin with more rows than chunks of kMsdCap rows could hold
+    // for all 256^(P-1) buckets under it
+    const uint64_t lim = (uint64_t)kMsdCap << (8 * (P - 1));
+    const uint32_t top_limit = (uint32_t)std::min<uint64_t>(lim, 0xffffffffull);
+    if (prof) prof->begin(KC_SCAN, s);
+    e = msd_scan(mhist, moffs, P, top_limit, flag, s);
+    if (prof) prof->end(KC_SCAN, s);
+    if (e != cudaSuccess) return e;
+
+    const PassVariant& var = variant_for(p.tuning, w);
+    const uint32_t tiles = (uint32_t)((n + var.threads * var.items - 1) / (var.threads * var.items));
+    for (int q = 0; q < P; ++q) {
+        PassArgs a{};
+        a.n = n;
+        a.shift = (uint32_t)(8 * (first + q));
+        a.dtype = p.dtype[0];
+        a.invert = invert;
+        a.reverse = 0;
+        a.bin_offsets = moffs + (size_t)q * 256;
+        a.status = status[q & 1];
+        a.status_next = status[(q + 1) & 1];
+        a.status_rows = p.max_tiles;
+        a.status_row_words = (uint32_t)p.max_radix;
+        a.tile_counter = counters + q;
+        a.err = err;
+        a.run_flag = flag;
+        a.run_when = 0;
+        int mode;
+        if (q == 0) {
+            mode = perm_in ? IN_GATHER : IN_RAW;
+            a.keys_in = key_cols[0];
+            a.vals_in = perm_in;
+        } else {
+            mode = IN_BUF;
+            a.keys_in = kbuf[(q - 1) & 1];
+            a.vals_in = vbuf[(q - 1) & 1];
+        }
+        a.keys_out = kbuf[q & 1];
+        a.vals_out = vbuf[q & 1];
+        if (prof) prof->begin(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
+        var.k[mode][0]<<<tiles, var.threads, var.smem, s>>>(a);
+        e = cudaGetLastError();
+        if (prof) prof->end(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
+        if (e != cudaSuccess) return e;
+    }
+    const void* skeys = kbuf[(P - 1) & 1];
+    const uint32_t* svals = vbuf[(P - 1) & 1];
+    uint32_t* chunk_start = reinterpret_cast<uint32_t*>(ws + p.off_chunks);
+    MsdChunkArgs ca{skeys, n, p.msd_chunk_rows, p.msd_chunks, (uint32_t)(8 * (ndigits - P)), chunk_start, flag};
+    if (prof) prof->begin(KC_LOCALSORT, s);
+    e = msd_chunks(ca, w, s);
+    if (e == cudaSuccess) {
+        MsdLocalArgs la{};
+        la.keys = skeys;
+        la.vals = svals;
+        la.chunk_start = chunk_start;
+        la.n = n;
+        la.sec = p.nkeys > 1 ? key_cols[1] : nullptr;
+        la.sec_dtype = p.nkeys > 1 ? p.dtype[1] : 0;
+        la.dtype = p.dtype[0];
+        la.invert = invert ? 1 : 0;
+        la.reverse = order == 2 ? 1 : 0;
+        la.lo_bits = w == 8 ? 32 : 0;
+        la.flag = flag;
+        la.err = err;
+        la.keys_out = key0_out;
+        la.perm_out = perm_out;
+        e = msd_local(la, w, p.msd_chunks, s);
+    }
+    if (prof) prof->end(KC_LOCALSORT, s);
+    return e;
+}
+}  // namespace
+
+cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
+                     void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof,
+                     const uint32_t* perm_in, uint32_t* msd_fallbacks) {
+    if (p.n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(ws + p.off_zero, 0, p.zero_bytes, s);
+    if (e != cudaSuccess) return e;
+    if (!p.msd)
+        return run_lsd(p, key_cols, order, perm_out, key0_out, ws, err, s, prof, perm_in, 0, nullptr, nullptr);
+    e = run_msd(p, key_cols, order, perm_out, key0_out, ws, err, s, prof, perm_in);
+    if (e != cudaSuccess) return e;
+    // the LSD sort over all keys, taken only if the MSD plan failed
+    const uint32_t* flag = reinterpret_cast<const uint32_t*>(ws + p.off_msd_flag);
+    return run_lsd(p, key_cols, order, perm_out, key0_out, ws, err, s, prof, perm_in, p.msd_passes, flag,
+                   msd_fallbacks);
 }
 
 // ---------------------------------------------------------------------------
@@ -1100,6 +1272,10 @@ cudaError_t prepare_sort_kernels() {
     {
         cudaError_t e = cudaFuncSetAttribute(k_seg_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              8 * kMaxRadix * 4);
+        if (e != cudaSuccess) return e;
+    }
+    {
+        cudaError_t e = prepare_msd_kernels();
         if (e != cudaSuccess) return e;
     }
     // all histograms of a sort in shared memory: at most 4 keys x 6 passes x

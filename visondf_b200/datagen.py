@@ -66,9 +66,16 @@ def frame_w0(n: int = 1_000_000, distinct: int = 10_000):
     return {"key": key, "v1": v1, "v2": v2}
 
 
-def frame_w1(n: int = 100_000_000, ranks: int = 1_000_000, s: float = 1.1):
-    k1 = np.random.default_rng(seed(1, 0)).integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, size=n,
-                                                    dtype=np.int64, endpoint=True)
+def frame_w1(n: int = 100_000_000, ranks: int = 1_000_000, s: float = 1.1, key1_pool: int = 0):
+    """The two-key frame; key1_pool > 0 draws key1 from that many distinct
+    full-range values instead (the tie-heavy variant: key2 then decides the
+    order of rows sharing key1)."""
+    if key1_pool:
+        r1 = np.random.default_rng(seed(1, 5))
+        k1 = distinct_pool(r1, key1_pool, np.int64)[r1.integers(0, key1_pool, size=n)]
+    else:
+        k1 = np.random.default_rng(seed(1, 0)).integers(np.iinfo(np.int64).min, np.iinfo(np.int64).max, size=n,
+                                                        dtype=np.int64, endpoint=True)
     rng2 = np.random.default_rng(seed(1, 1))
     pool = distinct_pool(rng2, ranks, np.int32)
     k2 = pool[zipf_ranks(rng2, n, ranks, s)]
