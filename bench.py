@@ -366,6 +366,9 @@ def config_section(args, local_rank: int, name: str) -> dict:
     keys = [torch.from_numpy(f[k]).to(dev) for k in knames]
     payload = [torch.from_numpy(f[k]).to(dev) for k in pnames]
     ctx = vdf.Context(local_rank)
+    if args.section_tuning:
+        ctx.set_sort_tuning(*args.section_tuning[:2])
+        ctx.set_local_sort_variant(args.section_tuning[2])
     stream = torch.cuda.current_stream()
     outs = ctx.alloc_sort_groupby_outputs(keys, payload, agg, want_group_start=True)
     packed = ctx.pack_sort_groupby(keys, payload, agg, vdf.ORDER_ASC, True, outs, host_count=False)
@@ -1031,6 +1034,7 @@ def our_arm(args, rank: int, world: int, local_rank: int):
     ctx.close()
     del d, outs, packed, keys, payload
     torch.cuda.empty_cache()
+    args.section_tuning = (tuned["variant32"], tuned["variant64"], tuned.get("local", 0))
     sections = set(args.sections.split(","))
     batched = served = unique_join = csv_res = None
     configs = {}
@@ -1061,6 +1065,7 @@ def our_arm(args, rank: int, world: int, local_rank: int):
                           "msd_sorts": sstats["msd_sorts"] - sstats0["msd_sorts"],
                           "msd_fallbacks": sstats["msd_fallbacks"] - sstats0["msd_fallbacks"]},
             "tuning": {"variant32": tuned["variant32"], "variant64": tuned["variant64"],
+                       "local_sort_variant": tuned.get("local"), "ms_local": tuned.get("ms_local"),
                        "variants": __import__("visondf_b200._lib", fromlist=["x"]).sort_variants()},
             "gpu_launches": launches,
             "clocks": clk,
@@ -1089,6 +1094,7 @@ def main():
     ap.add_argument("--variants", type=int, nargs=2, metavar=("V32", "V64"),
                     help="with --no-autotune: radix-pass variant indices for 4- and 8-byte keys")
     ap.add_argument("--csv-bytes", type=int, default=1 << 30, help="size of the synthetic CSV file (csv section)")
+    ap.set_defaults(section_tuning=None)
     ap.add_argument("--sections", default="c1_ties,c0,c2a,c2b,batched,served,unique_join,csv",
                     help="extra single-GPU measurements after the headline one: batched, served, unique_join "
                          "(comma list, 'none' for none)")

@@ -188,6 +188,22 @@ typedef enum vdf_sort_strategy {
 } vdf_sort_strategy;
 vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* ctx, int strategy, uint64_t msd_min_rows);
 vdf_status vdf_ctx_get_sort_strategy(vdf_ctx* ctx, int32_t* strategy, uint64_t* msd_min_rows);
+/* Digit matching of the MSD-first sort's shared-memory passes: 0 = one warp
+ * ballot per digit bit (default), 1 = match.any; the autotuner's choice. */
+vdf_status vdf_ctx_set_local_sort_variant(vdf_ctx* ctx, int variant);
+int vdf_ctx_get_local_sort_variant(vdf_ctx* ctx); /* -1 for a NULL context */
+/* Failure injection for tests; nothing here faults the device.
+ *   spin_limit : polls a look-back wait makes before it gives up, records
+ *                VDF_ERR_TIMEOUT in the error bits and carries on (0: the
+ *                default, about 2^20 polls, ~0.1 s)
+ *   stall_tile : in the first radix pass of each later sort, the CTA that
+ *                draws this tile leaves without publishing its counts, so the
+ *                waits on it run out (UINT32_MAX: none); vdf_ctx_check then
+ *                returns VDF_ERR_TIMEOUT and the sort's results are undefined
+ *   fail_allocs: the next that many workspace allocations fail as a failed
+ *                cudaMalloc would (VDF_ERR_OOM); the context stays usable
+ * No counterpart in the reference. */
+vdf_status vdf_ctx_set_test_hooks(vdf_ctx* ctx, uint32_t spin_limit, uint32_t stall_tile, uint32_t fail_allocs);
 /* Sorts this context planned MSD-first, and how many of them fell back to
  * the LSD passes on the device (synchronises `stream`).  No counterpart in
  * the reference. */
@@ -614,6 +630,12 @@ vdf_status vdf_server_wait(vdf_server* srv, uint64_t request_id, double timeout_
  * is released, the batch's outputs return to the allocator). */
 vdf_status vdf_server_release(vdf_server* srv, uint64_t request_id);
 vdf_status vdf_server_read_stats(vdf_server* srv, vdf_server_stats* out);
+/* Failure injection for tests: the next `count` batches fail with `status`
+ * when they start (where = 0: planning and launch) or when they finish
+ * (where = 1: reading back the results), as a real failure there would; the
+ * batch's requests end VDF_REQ_FAILED with that status and later requests
+ * are served as usual. */
+vdf_status vdf_server_inject_failure(vdf_server* srv, int where, uint32_t count, vdf_status status);
 const char* vdf_server_last_error(vdf_server* srv);
 /* Stops the scheduler after the batches in flight and frees everything. */
 void vdf_server_destroy(vdf_server* srv);

@@ -117,6 +117,40 @@ def test_tiles_of_single_row_groups_beside_scanned_tiles(ctx, tail):
     compare(og, gs, [v1, v2], "shuffled mix")
 
 
+@pytest.mark.parametrize("nkeys", [1, 2])
+def test_tiles_of_mostly_single_row_groups(ctx, nkeys):
+    """Tiles (512 rows) where at most 32 rows continue a group take a striped
+    path: one-row groups written by consecutive lanes, the head row of a
+    longer group walks it.  Runs of 2-3 rows, a 33-row group inside a tile, a
+    group running over a tile boundary, one ending exactly at a boundary, one
+    covering the first row of a tile, and a partial last tile."""
+    rng = np.random.default_rng(31)
+    runs = []
+    while sum(runs) < 40_000:
+        r = int(rng.choice([1, 2, 3], p=[0.97, 0.02, 0.01]))
+        runs.append(r)
+    runs += [1] * 100 + [33] + [1] * 500 + [7] + [1] * 300 + [2] * 3 + [1] * 77
+    # a group spanning a tile boundary and one ending exactly at one
+    csum = np.cumsum(runs)
+    runs[int(np.searchsorted(csum, 30 * 512))] += 4
+    n = int(np.sum(runs))
+    gid = np.repeat(np.arange(len(runs), dtype=np.int64), runs)
+    keys = [gid * 5 - 7] if nkeys == 1 else [(gid // 3).astype(np.int32), (gid % 3) * 11 - 4]
+    v1 = rng.standard_normal(n)
+    v2 = rng.integers(-2**40, 2**40, size=n, dtype=np.int64)
+    og = ob.groupby(keys, [v1, v2])
+    gr = ctx.groupby_sorted([dev(k) for k in keys], [dev(v1), dev(v2)], want_row_group=True,
+                            want_group_start=True)
+    compare(og, gr, [v1, v2], "mostly single rows")
+    starts = np.concatenate([[0], np.cumsum(runs)[:-1]])
+    assert (host(gr.group_start).view(np.uint32) == starts).all()
+    assert (host(gr.row_group).view(np.uint32) == np.repeat(np.arange(len(runs)), runs)).all()
+    shuffled = rng.permutation(n)
+    gs = ctx.sort_groupby([dev(k[shuffled]) for k in keys], [dev(v1[shuffled]), dev(v2[shuffled])],
+                          agg_cols=[0, 1])
+    compare(og, gs, [v1, v2], "shuffled mostly single rows")
+
+
 def test_int64_sum_overflow_is_exact(ctx):
     n = 300_000
     key = np.zeros(n, np.int64)

@@ -123,15 +123,19 @@ def test_fallback_when_one_bucket_overflows_a_chunk(mctx):
     assert (used, fell) == (1, 1)
 
 
-def test_fallback_when_a_long_run_is_out_of_order(mctx):
-    # ~250 rows share each high 32-bit half, in random low-half order
+def test_long_unsorted_runs(mctx):
+    # ~250 rows share each high 32-bit half, in random low-half order: a
+    # one-key chunk finishes with more shared-memory passes ...
     rng = np.random.default_rng(2)
     n = 500_000
     hi = rng.integers(0, 1 << 32, 2000, dtype=np.uint64)[rng.integers(0, 2000, n)]
     k = (hi << np.uint64(32)) | rng.integers(0, 1 << 32, n, dtype=np.uint64)
     used, fell = run_sort(mctx, [k])
-    assert (used, fell) == (1, 1)
-    # the same with a second key deciding: equal primaries, random key 1
+    assert (used, fell) == (1, 0)
+    for order in ORDERS[1:]:
+        assert run_sort(mctx, [k.view(np.int64)], order) == (1, 0)
+    # ... and with a second key deciding (equal primaries, random key 1) the
+    # plan falls back to the LSD passes
     k0 = pool_keys(rng, n, 2000, np.int64)
     k1 = datagen.keys_for("uniform", np.int32, n, rng)
     used, fell = run_sort(mctx, [k0, k1])

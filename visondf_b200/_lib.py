@@ -136,6 +136,9 @@ def _load() -> C.CDLL:
         "vdf_ctx_get_multikey_mode": (i32, [vp]),
         "vdf_ctx_set_sort_strategy": (st, [vp, i32, u64]),
         "vdf_ctx_sort_stats": (st, [vp, vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "vdf_ctx_set_local_sort_variant": (st, [vp, i32]),
+        "vdf_ctx_set_test_hooks": (st, [vp, C.c_uint32, C.c_uint32, C.c_uint32]),
+        "vdf_ctx_get_local_sort_variant": (i32, [vp]),
         "vdf_ctx_get_sort_strategy": (st, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]),
         "vdf_sort_plan_info": (st, [u64, C.POINTER(C.c_int32), i32, i32, u64, C.POINTER(C.c_int32),
                                     C.POINTER(C.c_uint32)]),
@@ -318,6 +321,16 @@ class Context:
         a, b = C.c_uint64(), C.c_uint64()
         self._check(lib.vdf_ctx_sort_stats(self.handle, _stream(stream), C.byref(a), C.byref(b)), "sort_stats")
         return {"msd_sorts": int(a.value), "msd_fallbacks": int(b.value)}
+
+    def set_test_hooks(self, spin_limit: int = 0, stall_tile: int = 0xFFFFFFFF, fail_allocs: int = 0):
+        """Failure injection for tests (see vdf_ctx_set_test_hooks)."""
+        self._check(lib.vdf_ctx_set_test_hooks(self.handle, spin_limit, stall_tile, fail_allocs), "set_test_hooks")
+
+    def set_local_sort_variant(self, variant: int):
+        self._check(lib.vdf_ctx_set_local_sort_variant(self.handle, variant), "vdf_ctx_set_local_sort_variant")
+
+    def get_local_sort_variant(self) -> int:
+        return lib.vdf_ctx_get_local_sort_variant(self.handle)
 
     def get_sort_strategy(self) -> tuple:
         st, mn = C.c_int32(), C.c_uint64()

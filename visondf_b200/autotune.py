@@ -51,18 +51,21 @@ class TuningTable:
 def tune(ctx: "_lib.Context", run: Callable[[], None], reps: int = 2) -> dict:
     """Times `run` (one sort or sort + group-by on the context) under every
     variant assignment and returns {"variant32": i, "variant64": j,
-    "ms32": {i: ms per run}, "ms64": {j: ms per run}} (time of all radix
-    passes over keys of that width in one run); leaves the best tuning set on
-    the context."""
+    "ms32": {i: ms per run}, "ms64": {j: ms per run}, "local": k,
+    "ms_local": {k: ms per run}} (time of all radix passes over keys of that
+    width in one run, and of the MSD-first sort's shared-memory finish);
+    leaves the best tuning set on the context."""
     variants = _lib.sort_variants()
     v32 = [v["index"] for v in variants if v["key_width"] == 4]
     v64 = [v["index"] for v in variants if v["key_width"] == 8]
     ms32, ms64 = {}, {}
     saved = ctx.get_sort_tuning()
-    # every key's passes run in the LSD mode, so both widths get timed (the
-    # primary-key-first mode may skip the other keys' passes)
+    # every key's passes run in the LSD mode and strategy, so both widths get
+    # timed (the primary-key-first mode and the MSD-first plan skip passes)
     mode = ctx.get_multikey_mode()
+    strategy = ctx.get_sort_strategy()
     ctx.set_multikey_mode(_lib.MULTIKEY_LSD)
+    ctx.set_sort_strategy(_lib.SORT_LSD, strategy[1])
     try:
         run()  # warm the workspace and the kernels
         for i in range(max(len(v32), len(v64))):
@@ -83,10 +86,27 @@ def tune(ctx: "_lib.Context", run: Callable[[], None], reps: int = 2) -> dict:
                 ms64[b] = min(ms64.get(b, math.inf), t64 / reps)
     finally:
         ctx.set_multikey_mode(mode)
+        ctx.set_sort_strategy(*strategy)
     best32 = min(ms32, key=ms32.get) if ms32 else saved[0]  # a width not timed keeps its choice
     best64 = min(ms64, key=ms64.get) if ms64 else saved[1]
     ctx.set_sort_tuning(best32, best64)
-    return {"variant32": best32, "variant64": best64, "ms32": ms32, "ms64": ms64}
+    # the shared-memory finish of the MSD-first plan (where the plan applies)
+    ms_local = {}
+    for k in (0, 1):
+        ctx.set_local_sort_variant(k)
+        run()
+        ctx.profile(True)
+        ctx.profile_reset()
+        for _ in range(reps):
+            run()
+        t, c = ctx.profile_read()["localsort"]
+        ctx.profile(False)
+        if c:
+            ms_local[k] = t / reps
+    best_local = min(ms_local, key=ms_local.get) if ms_local else 0
+    ctx.set_local_sort_variant(best_local)
+    return {"variant32": best32, "variant64": best64, "ms32": ms32, "ms64": ms64, "local": best_local,
+            "ms_local": ms_local}
 
 
 def batch_candidates() -> list:

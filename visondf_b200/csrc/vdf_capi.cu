@@ -239,6 +239,29 @@ vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* c, int strategy, uint64_t msd_min_
     return VDF_OK;
 }
 
+vdf_status vdf_ctx_set_local_sort_variant(vdf_ctx* c, int variant) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    if (variant < 0 || variant > 1) return fail(c, VDF_ERR_INVALID_ARG, "bad local sort variant %d", variant);
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->tuning.msd_match = variant;
+    return VDF_OK;
+}
+
+int vdf_ctx_get_local_sort_variant(vdf_ctx* c) {
+    if (!c) return -1;
+    std::lock_guard<std::mutex> lk(c->mu);
+    return c->tuning.msd_match;
+}
+
+vdf_status vdf_ctx_set_test_hooks(vdf_ctx* c, uint32_t spin_limit, uint32_t stall_tile, uint32_t fail_allocs) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->tuning.spin_limit = spin_limit;
+    c->tuning.stall_tile = stall_tile;
+    c->fail_allocs = fail_allocs;
+    return VDF_OK;
+}
+
 vdf_status vdf_ctx_sort_stats(vdf_ctx* c, void* stream, uint64_t* msd_sorts, uint64_t* msd_fallbacks) {
     if (!c) return VDF_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);

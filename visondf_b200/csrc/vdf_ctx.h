@@ -81,6 +81,7 @@ struct vdf_ctx {
                                          // [16,20): tie flag; [24,28): MSD fallbacks
     uint64_t* host_pinned = nullptr;     // [0]: group count, [1]: error bits, [2]: tie flag, [3]: fallbacks
     uint64_t msd_sorts = 0;              // sorts planned MSD-first
+    uint32_t fail_allocs = 0;            // test hook: workspace allocations to fail
     int multikey_mode = VDF_MULTIKEY_PRIMARY_FIRST;
     std::atomic<uint64_t> launches{0};
     std::string last_error;
@@ -149,6 +150,10 @@ inline vdf_status ws_ensure(vdf_ctx* c, size_t bytes) {
         if (e != cudaSuccess) return from_cuda(c, e, "cudaFree(workspace)");
     }
     size_t cap = align256(bytes + bytes / 8);
+    if (c->fail_allocs) {  // failure injection (vdf_ctx_set_test_hooks)
+        c->fail_allocs--;
+        return fail(c, VDF_ERR_OOM, "workspace allocation of %zu bytes failed (injected by a test hook)", cap);
+    }
     cudaError_t e = cudaMalloc(&c->ws, cap);
     if (e != cudaSuccess) {
         c->ws = nullptr;

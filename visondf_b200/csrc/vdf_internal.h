@@ -99,6 +99,10 @@ struct PassArgs {
     // (*run_flag != 0) == (run_when != 0), and otherwise returns at once
     const uint32_t* run_flag;
     uint32_t run_when;
+    // failure injection for tests: polls before a look-back wait gives up (0:
+    // the default kSpinLimit), and a tile whose CTA publishes nothing
+    uint32_t spin_limit = 0;
+    uint32_t stall_tile = 0xffffffffu;
 };
 
 
@@ -111,6 +115,11 @@ struct SortTuning {
     // columns with at least msd_min_rows rows, 0 = never
     int msd = 0;
     uint64_t msd_min_rows = 0;
+    int msd_match = 0;  // shared-memory passes: 0 = ballots, 1 = match.any
+    // failure injection for tests (vdf_ctx_set_test_hooks): look-back poll
+    // limit (0 = default) and a tile of the first pass that never publishes
+    uint32_t spin_limit = 0;
+    uint32_t stall_tile = 0xffffffffu;
 };
 SortTuning default_sort_tuning();
 bool sort_tuning_valid(const SortTuning& t);
@@ -134,6 +143,7 @@ struct SortPlan {
     // device decides, no host round trip).
     bool msd;
     int msd_passes;
+    int msd_lo_bits;           // key 0 bits ranked directly in runs (below the shared-memory passes)
     uint32_t msd_chunk_rows;   // nominal rows per chunk
     uint32_t msd_chunks;       // ceil(n / msd_chunk_rows)
     size_t off_msd_hist, off_msd_offs, off_msd_flag, off_chunks;
@@ -173,10 +183,9 @@ struct MsdLocalArgs {
     uint32_t* perm_out;
 };
 cudaError_t msd_hist(const MsdHistArgs& a, int width, cudaStream_t s);
-cudaError_t msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t top_limit, uint32_t* flag,
-                     cudaStream_t s);
+cudaError_t msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t cap, uint32_t* flag, cudaStream_t s);
 cudaError_t msd_chunks(const MsdChunkArgs& a, int width, cudaStream_t s);
-cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, cudaStream_t s);
+cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, int match, cudaStream_t s);
 // Kernel launches run_sort makes for a plan (conditional ones included).
 int sort_launches(const SortPlan& p);
 

@@ -13,7 +13,8 @@
 //
 //   1. k_msd_hist    histograms of the top P digits of key 0 (one read)
 //   2. k_msd_scan    their exclusive scans; a top-digit bin holding more rows
-//                    than its buckets could possibly fit in chunks flags the
+//                    than chunks could take for every bucket possible under it
+//                    (bounded by the lower digits' non-empty bins) flags the
 //                    MSD path as failed up front
 //   3. P onesweep passes (vdf_radix.cu kernels), stable, over digits
 //      W-P .. W-1 of key 0, least significant first: afterwards the rows
@@ -23,16 +24,19 @@
 //                    the first bucket boundary at or after c*T
 //   5. k_msd_local   one CTA per chunk (<= kMsdCap rows): stable 8-bit LSD
 //                    passes in shared memory over the digits of key 0 above
-//                    its low 32 bits (8-byte keys; all digits for 4-byte
-//                    keys) that vary inside the chunk, then each run of rows
-//                    with equal high bits is ranked directly by (low 32
-//                    bits, key 1's order image, position) -- key 1 read
-//                    through the row id only for rows in such runs -- and
-//                    the raw sorted key 0 and the permutation are written.
+//                    its low F bits that vary inside the chunk, then each
+//                    run of rows with equal high bits is ranked directly by
+//                    (low F bits, key 1's order image, position) -- key 1 is
+//                    read through the row id only for rows whose key 0 ties
+//                    with another row's -- and the raw sorted key 0 and the
+//                    permutation are written.  F is 32 for 8-byte keys
+//                    (runs are rare for spread keys) and 0 for 4-byte keys.
 //
 // Every pass is stable and ties keep their row order, so the result is
-// exactly the stable order over all keys.  Where the data defeats the plan
-// (a chunk above kMsdCap rows, or an unsorted run longer than kMsdRunMax),
+// exactly the stable order over all keys.  A one-key chunk with a run longer
+// than kMsdRunMax out of order is finished with more shared-memory passes.
+// Where the data defeats the plan (a chunk above kMsdCap rows, or with two
+// keys a long run whose key 0 ties or is out of order),
 // a device flag is set and the LSD passes that follow in the same stream run
 // from the raw columns instead (they return at once while the flag is
 // clear); no host round trip either way.
@@ -71,27 +75,42 @@ __global__ void __launch_bounds__(512) k_msd_hist(MsdHistArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// 2. exclusive scans (one CTA of 256 threads per digit) + the up-front check
+// 2. exclusive scans (one CTA of 256 threads, one bin per thread) + the
+//    up-front check
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_msd_scan(const uint32_t* hist, uint32_t* offs, int ndig,
-                                                  uint32_t top_limit, uint32_t* flag) {
+__global__ void __launch_bounds__(256) k_msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t cap,
+                                                  uint32_t* flag) {
     __shared__ uint32_t wsum[8];
-    const int p = blockIdx.x, b = threadIdx.x, lane = b & 31, warp = b >> 5;
-    const uint32_t v = hist[p * 256 + b];
-    uint32_t incl = v;
+    __shared__ uint32_t nonempty[kMsdMaxPasses];
+    const int b = threadIdx.x, lane = b & 31, warp = b >> 5;
+    if (b < kMsdMaxPasses) nonempty[b] = 0;
+    uint32_t top = 0;
+    for (int p = 0; p < ndig; ++p) {
+        __syncthreads();  // wsum of the previous digit has been read
+        const uint32_t v = hist[p * 256 + b];
+        uint32_t incl = v;
 #pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= d) incl += t;
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += t;
+        }
+        if (lane == 31) wsum[warp] = incl;
+        const uint32_t ne = __popc(__ballot_sync(0xffffffffu, v != 0));
+        if (lane == 0) atomicAdd(&nonempty[p], ne);
+        __syncthreads();
+        uint32_t base = 0;
+        for (int w = 0; w < warp; ++w) base += wsum[w];
+        offs[p * 256 + b] = base + incl - v;
+        if (p == ndig - 1) top = v;
     }
-    if (lane == 31) wsum[warp] = incl;
     __syncthreads();
-    uint32_t base = 0;
-    for (int w = 0; w < warp; ++w) base += wsum[w];
-    offs[p * 256 + b] = base + incl - v;
-    // a top digit shared by more rows than 256^(P-1) full chunks hold: some
-    // bucket under it cannot fit one chunk
-    if (p == ndig - 1 && v > top_limit) atomicOr(flag, 1u);
+    // Rows under one top-digit value can form at most as many buckets as the
+    // lower digits have distinct values (the product of their non-empty
+    // bins); more rows than that many full chunks hold means some bucket
+    // cannot fit a chunk.
+    uint64_t under = 1;
+    for (int p = 0; p + 1 < ndig; ++p) under *= nonempty[p];
+    if ((uint64_t)top > (uint64_t)cap * under) atomicOr(flag, 1u);
 }
 
 // ---------------------------------------------------------------------------
@@ -189,6 +208,89 @@ __device__ __forceinline__ uint64_t sec_image(const void* col, int dt, uint32_t 
     return (uint64_t)order32(ld_rand4(static_cast<const uint32_t*>(col) + row), dt, invert);
 }
 
+// One stable 8-bit LSD pass in shared memory over the digit at `shift` of
+// the CTA's rows (item j of a thread at position (warp * ia + j) * 32 + lane;
+// slots past the chunk hold all-ones keys and rank last).  Afterwards the
+// rows are in sk / sv in the new order and back in key / val by position.
+template <typename K, int THREADS, int ITEMS, int MATCH>
+__device__ __forceinline__ void local_pass(K (&key)[ITEMS], uint32_t (&val)[ITEMS], uint32_t shift, uint32_t ia,
+                                           K* sk, uint32_t* sv, uint32_t* wcnt, uint32_t* wsum, uint32_t* err) {
+    constexpr int WARPS = THREADS / 32, RADIX = 256;
+    constexpr uint32_t CAP = (uint32_t)(THREADS * ITEMS);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t lt = lanemask_lt();
+    uint32_t* my = wcnt + warp * RADIX;
+    for (int i = tid; i < WARPS * RADIX; i += THREADS) wcnt[i] = 0;
+    __syncthreads();
+    uint32_t rank[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        rank[j] = 0;
+        if (j < (int)ia) {
+            const uint32_t d = (uint32_t)(key[j] >> shift) & 0xffu;
+            uint32_t peers;
+            if constexpr (MATCH == 1) {
+                peers = __match_any_sync(0xffffffffu, d);
+            } else {
+                peers = 0xffffffffu;
+#pragma unroll
+                for (int bt = 0; bt < 8; ++bt) {
+                    const uint32_t bal = __ballot_sync(0xffffffffu, (d >> bt) & 1u);
+                    peers &= ((d >> bt) & 1u) ? bal : ~bal;
+                }
+            }
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if (lane == leader) {
+                base = my[d];
+                my[d] = base + __popc(peers);
+            }
+            __syncwarp();
+            base = __shfl_sync(0xffffffffu, base, leader);
+            rank[j] = base + __popc(peers & lt);
+        }
+    }
+    __syncthreads();
+    // bin-major exclusive prefix over (bin, warp)
+    uint32_t tot = 0;
+    if (tid < RADIX) {
+#pragma unroll
+        for (int w = 0; w < WARPS; ++w) {
+            const uint32_t c = wcnt[w * RADIX + tid];
+            wcnt[w * RADIX + tid] = tot;
+            tot += c;
+        }
+    }
+    uint32_t all;
+    const uint32_t start = local_excl_scan<THREADS>(tot, wsum, &all);
+    if (tid < RADIX)
+#pragma unroll
+        for (int w = 0; w < WARPS; ++w) wcnt[w * RADIX + tid] += start;
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        if (j < (int)ia) {
+            const uint32_t d = (uint32_t)(key[j] >> shift) & 0xffu;
+            uint32_t r = rank[j] + my[d];
+            if (r >= CAP) {  // never when the counts are consistent
+                atomicOr(err, ERR_BAD_INDEX);
+                r = ((uint32_t)warp * ia + j) * 32 + lane;
+            }
+            sk[r] = key[j];
+            sv[r] = val[j];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        if (j < (int)ia) {
+            const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+            key[j] = sk[pos];
+            val[j] = sv[pos];
+        }
+    }
+}
+
 // MATCH: 0 = one ballot per digit bit, 1 = match.any.
 template <typename K, int THREADS, int ITEMS, int MATCH>
 __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
@@ -226,7 +328,6 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
         return;
     }
     const uint32_t ia = (m + THREADS - 1) / THREADS;  // items per thread in use
-    const uint32_t lt = lanemask_lt();
 
     // ---- load: item j of a thread sits at position (warp * ia + j) * 32 + lane;
     //      slots past m hold all-ones keys, which every pass ranks last
@@ -277,79 +378,10 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
     // ---- stable 8-bit LSD passes in shared memory over the varying digits
     //      of key 0 from digit lo_bits / 8 up
     bool sorted_in_smem = false;
-    uint32_t* my = wcnt + warp * RADIX;
     for (int dg = (int)(a.lo_bits / 8); dg < KBITS / 8; ++dg) {
         const uint32_t shift = 8u * dg;
         if (((vary >> shift) & 0xff) == 0) continue;
-        for (int i = tid; i < WARPS * RADIX; i += THREADS) wcnt[i] = 0;
-        __syncthreads();
-        uint32_t rank[ITEMS];
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            rank[j] = 0;
-            if (j < (int)ia) {
-                const uint32_t d = (uint32_t)(key[j] >> shift) & 0xffu;
-                uint32_t peers;
-                if constexpr (MATCH == 1) {
-                    peers = __match_any_sync(0xffffffffu, d);
-                } else {
-                    peers = 0xffffffffu;
-#pragma unroll
-                    for (int bt = 0; bt < 8; ++bt) {
-                        const uint32_t bal = __ballot_sync(0xffffffffu, (d >> bt) & 1u);
-                        peers &= ((d >> bt) & 1u) ? bal : ~bal;
-                    }
-                }
-                const int leader = __ffs(peers) - 1;
-                uint32_t base = 0;
-                if (lane == leader) {
-                    base = my[d];
-                    my[d] = base + __popc(peers);
-                }
-                __syncwarp();
-                base = __shfl_sync(0xffffffffu, base, leader);
-                rank[j] = base + __popc(peers & lt);
-            }
-        }
-        __syncthreads();
-        // bin-major exclusive prefix over (bin, warp)
-        uint32_t tot = 0;
-        if (tid < RADIX) {
-#pragma unroll
-            for (int w = 0; w < WARPS; ++w) {
-                const uint32_t c = wcnt[w * RADIX + tid];
-                wcnt[w * RADIX + tid] = tot;
-                tot += c;
-            }
-        }
-        uint32_t all;
-        const uint32_t start = local_excl_scan<THREADS>(tot, wsum, &all);
-        if (tid < RADIX)
-#pragma unroll
-            for (int w = 0; w < WARPS; ++w) wcnt[w * RADIX + tid] += start;
-        __syncthreads();
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            if (j < (int)ia) {
-                const uint32_t d = (uint32_t)(key[j] >> shift) & 0xffu;
-                uint32_t r = rank[j] + my[d];
-                if (r >= CAP) {  // never when the counts are consistent
-                    atomicOr(a.err, ERR_BAD_INDEX);
-                    r = ((uint32_t)warp * ia + j) * 32 + lane;
-                }
-                sk[r] = key[j];
-                sv[r] = val[j];
-            }
-        }
-        __syncthreads();
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            if (j < (int)ia) {
-                const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
-                key[j] = sk[pos];
-                val[j] = sv[pos];
-            }
-        }
+        local_pass<K, THREADS, ITEMS, MATCH>(key, val, shift, ia, sk, sv, wcnt, wsum, a.err);
         sorted_in_smem = true;
     }
     if (!sorted_in_smem) {
@@ -364,57 +396,99 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
         __syncthreads();
     }
 
-    // ---- runs of equal high bits, ranked by (low bits, key 1, position)
+    // ---- runs of equal high bits, ranked by (low bits, key 1, position).
+    //      Key 1 is read (through the row id) only for rows whose low bits
+    //      tie with another row of their run, i.e. rows whose key 0 ties.
     const bool fix = a.lo_bits > 0 || a.sec != nullptr;
     const uint32_t hs = a.lo_bits;  // high part = key >> hs
     const K lo_mask = hs ? (K)((((K)1) << hs) - 1) : K(0);
     uint32_t newpos[ITEMS];
-    bool inrun[ITEMS];
+    uint32_t run[ITEMS];  // run bounds s | e << 16 (positions < 2^16); 0: not in a run
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
         newpos[j] = pos;
-        inrun[j] = false;
+        run[j] = 0;
         if (fix && j < (int)ia && pos < m) {
             const K h = key[j] >> hs;
-            inrun[j] = (pos > 0 && (sk[pos - 1] >> hs) == h) || (pos + 1 < m && (sk[pos + 1] >> hs) == h);
-            if (inrun[j] && a.sec) ssec[pos] = sec_image(a.sec, a.sec_dtype, val[j], a.invert != 0);
+            if ((pos > 0 && (sk[pos - 1] >> hs) == h) || (pos + 1 < m && (sk[pos + 1] >> hs) == h)) {
+                uint32_t s = pos, e = pos + 1;
+                while (s > 0 && pos - s < kMsdRunMax && (sk[s - 1] >> hs) == h) --s;
+                while (e < m && e - pos <= kMsdRunMax && (sk[e] >> hs) == h) ++e;
+                run[j] = s | (e << 16);
+                if (a.sec && e - s <= kMsdRunMax) {
+                    const K lo = key[j] & lo_mask;
+                    bool tie = false;
+                    for (uint32_t t = s; t < e; ++t) tie |= (t != pos) && ((sk[t] & lo_mask) == lo);
+                    if (tie) {
+                        uint32_t row = val[j];
+                        if (row >= a.n) {  // never for a permutation of [0, n)
+                            atomicOr(a.err, ERR_BAD_INDEX);
+                            row = 0;
+                        }
+                        ssec[pos] = sec_image(a.sec, a.sec_dtype, row, a.invert != 0);
+                    }
+                }
+            }
         }
     }
     if (fix) {
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
-            if (!inrun[j]) continue;
+            if (run[j] == 0) continue;
             const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
-            const K h = key[j] >> hs;
+            const uint32_t s = run[j] & 0xffffu, e = run[j] >> 16;
             const K lo = key[j] & lo_mask;
-            const uint64_t sc = a.sec ? ssec[pos] : 0;
-            uint32_t s = pos, e = pos + 1;
-            while (s > 0 && pos - s < kMsdRunMax && (sk[s - 1] >> hs) == h) --s;
-            while (e < m && e - pos <= kMsdRunMax && (sk[e] >> hs) == h) ++e;
             if (e - s > kMsdRunMax) {
                 // a long run: fine if it already is in order (e.g. equal
-                // keys), otherwise the plan fails
+                // keys of a one-key sort); otherwise see below
                 if (pos > s) {
                     const K plo = sk[pos - 1] & lo_mask;
-                    const uint64_t psc = a.sec ? ssec[pos - 1] : 0;
-                    if (plo > lo || (plo == lo && psc > sc)) misc[0] = 1;
+                    if (plo > lo || (plo == lo && a.sec)) misc[0] = 1;
                 }
                 continue;
             }
             uint32_t r = 0;
+            bool have_sec = false;
+            uint64_t sc = 0;
             for (uint32_t t = s; t < e; ++t) {
                 const K tlo = sk[t] & lo_mask;
-                const uint64_t tsc = a.sec ? ssec[t] : 0;
-                r += (tlo < lo || (tlo == lo && (tsc < sc || (tsc == sc && t < pos)))) ? 1u : 0u;
+                bool less = tlo < lo;
+                if (tlo == lo && t != pos) {
+                    if (a.sec) {
+                        if (!have_sec) {
+                            sc = ssec[pos];
+                            have_sec = true;
+                        }
+                        const uint64_t tsc = ssec[t];
+                        less = tsc < sc || (tsc == sc && t < pos);
+                    } else {
+                        less = t < pos;
+                    }
+                }
+                r += less ? 1u : 0u;
             }
             newpos[j] = s + r;
         }
         __syncthreads();
         if (misc[0]) {
-            if (tid == 0) atomicOr(a.flag, 1u);
-            return;
+            // A run longer than the direct ranking handles is out of order.
+            // With a second key that needs key 1 for every row: the plan
+            // fails.  With one key the chunk is finished in shared memory:
+            // LSD passes over the varying low digits, then the high ones
+            // again (every pass is stable, so ties keep their row order).
+            if (a.sec) {
+                if (tid == 0) atomicOr(a.flag, 1u);
+                return;
+            }
+            for (int dg = 0; dg < KBITS / 8; ++dg) {
+                const uint32_t shift = 8u * dg;
+                if (((vary >> shift) & 0xff) == 0) continue;
+                local_pass<K, THREADS, ITEMS, MATCH>(key, val, shift, ia, sk, sv, wcnt, wsum, a.err);
+            }
+#pragma unroll
+            for (int j = 0; j < ITEMS; ++j) newpos[j] = ((uint32_t)warp * ia + j) * 32 + lane;
         }
     }
 
@@ -438,10 +512,14 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
 namespace {
 constexpr int kLocalThreads = 512, kLocalItems = 8;
 static_assert(kLocalThreads * kLocalItems == (int)kMsdCap, "chunk capacity");
+static_assert(kMsdCap < (1u << 16), "run bounds are packed in 16 bits");
 using Local64 = LocalCfg<uint64_t, kLocalThreads, kLocalItems>;
 using Local32 = LocalCfg<uint32_t, kLocalThreads, kLocalItems>;
-#define VDF_LOCAL64 k_msd_local<uint64_t, kLocalThreads, kLocalItems, 1>
-#define VDF_LOCAL32 k_msd_local<uint32_t, kLocalThreads, kLocalItems, 1>
+template <int MATCH>
+struct LocalKernels {
+    static constexpr auto k64 = k_msd_local<uint64_t, kLocalThreads, kLocalItems, MATCH>;
+    static constexpr auto k32 = k_msd_local<uint32_t, kLocalThreads, kLocalItems, MATCH>;
+};
 
 int sm_count() {
     int dev = 0, sms = 148;
@@ -452,9 +530,15 @@ int sm_count() {
 }  // namespace
 
 cudaError_t prepare_msd_kernels() {
-    cudaError_t e = cudaFuncSetAttribute(VDF_LOCAL64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Local64::SMEM);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(VDF_LOCAL32, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Local32::SMEM);
+    const void* k64[2] = {(const void*)LocalKernels<0>::k64, (const void*)LocalKernels<1>::k64};
+    const void* k32[2] = {(const void*)LocalKernels<0>::k32, (const void*)LocalKernels<1>::k32};
+    for (int m = 0; m < 2; ++m) {
+        cudaError_t e = cudaFuncSetAttribute(k64[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Local64::SMEM);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k32[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Local32::SMEM);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 cudaError_t msd_hist(const MsdHistArgs& a, int width, cudaStream_t s) {
@@ -465,9 +549,8 @@ cudaError_t msd_hist(const MsdHistArgs& a, int width, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t top_limit, uint32_t* flag,
-                     cudaStream_t s) {
-    k_msd_scan<<<ndig, 256, 0, s>>>(hist, offs, ndig, top_limit, flag);
+cudaError_t msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t cap, uint32_t* flag, cudaStream_t s) {
+    k_msd_scan<<<1, 256, 0, s>>>(hist, offs, ndig, cap, flag);
     return cudaGetLastError();
 }
 
@@ -478,10 +561,15 @@ cudaError_t msd_chunks(const MsdChunkArgs& a, int width, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, cudaStream_t s) {
+cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, int match, cudaStream_t s) {
     if (nchunks == 0) return cudaSuccess;
-    if (width == 8) VDF_LOCAL64<<<nchunks, kLocalThreads, Local64::SMEM, s>>>(a);
-    else VDF_LOCAL32<<<nchunks, kLocalThreads, Local32::SMEM, s>>>(a);
+    if (width == 8) {
+        if (match) LocalKernels<1>::k64<<<nchunks, kLocalThreads, Local64::SMEM, s>>>(a);
+        else LocalKernels<0>::k64<<<nchunks, kLocalThreads, Local64::SMEM, s>>>(a);
+    } else {
+        if (match) LocalKernels<1>::k32<<<nchunks, kLocalThreads, Local32::SMEM, s>>>(a);
+        else LocalKernels<0>::k32<<<nchunks, kLocalThreads, Local32::SMEM, s>>>(a);
+    }
     return cudaGetLastError();
 }
 

@@ -290,6 +290,10 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
         for (int i = tid; i < 2 * WARPS * RADIX; i += THREADS) wmask[i] = 0;
     __syncthreads();
     const uint32_t tile = misc[0];
+    // failure injection for tests: this tile's CTA leaves before publishing
+    // anything, so the look-back waits on it run out (bounded, reported)
+    if (tile == a.stall_tile) return;
+    const uint32_t spin_limit = a.spin_limit ? a.spin_limit : kSpinLimit;
     const uint64_t n = a.n;
     uint64_t tile_base = (uint64_t)tile * TILE;
     uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tile_base);
@@ -524,7 +528,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
                         if (done) break;
                         uint32_t st = sw[w];
                         while ((st & ~ST_CNT) == 0) {  // not yet published: wait for this one
-                            if (++spins > kSpinLimit) {
+                            if (++spins > spin_limit) {
                                 atomicOr(a.err, ERR_LOOKBACK_TIMEOUT);
                                 st = ST_INC;
                                 break;
@@ -577,7 +581,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
                     if (done[k]) break;
                     uint32_t st = sw[k][w];
                     while ((st & ~ST_CNT) == 0) {  // not yet published: wait for this one
-                        if (++spins > kSpinLimit) {
+                        if (++spins > spin_limit) {
                             atomicOr(a.err, ERR_LOOKBACK_TIMEOUT);
                             st = ST_INC;
                             break;
@@ -804,6 +808,11 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
     if (tuning.msd && nkeys <= 2 && n >= 2 && n >= tuning.msd_min_rows && p.bits[0] == 8) {
         p.msd_passes = msd_passes_for(n, p.width[0]);
         p.msd = p.msd_passes > 0;
+        // low bits ranked directly in runs of equal high bits: the low half of
+        // an 8-byte key (such runs are rare for spread keys, and ranking
+        // every row of frequent short runs measured slower than the shared-
+        // memory passes it saves); none for 4-byte keys
+        p.msd_lo_bits = p.width[0] == 8 ? 32 : 0;
     }
     // passes are numbered in processing order (least-significant key first);
     // their histograms follow one another in that order
@@ -945,6 +954,8 @@ cudaError_t run_lsd(const SortPlan& p, const void* const* key_cols, int order, u
             a.err = err;
             a.run_flag = run_flag;
             a.run_when = 1;
+            a.spin_limit = p.tuning.spin_limit;
+            a.stall_tile = g == first_g ? p.tuning.stall_tile : 0xffffffffu;
             int mode;
             if (q == 0 && k == p.nkeys - 1) {
                 // first pass: the rows themselves, or the rows as seen through
@@ -1013,12 +1024,8 @@ cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, u
     e = msd_hist(mh, w, s);
     if (prof) prof->end(KC_HIST, s);
     if (e != cudaSuccess) return e;
-    // a top-digit bin with more rows than chunks of kMsdCap rows could hold
-    // for all 256^(P-1) buckets under it
-    const uint64_t lim = (uint64_t)kMsdCap << (8 * (P - 1));
-    const uint32_t top_limit = (uint32_t)std::min<uint64_t>(lim, 0xffffffffull);
     if (prof) prof->begin(KC_SCAN, s);
-    e = msd_scan(mhist, moffs, P, top_limit, flag, s);
+    e = msd_scan(mhist, moffs, P, kMsdCap, flag, s);
     if (prof) prof->end(KC_SCAN, s);
     if (e != cudaSuccess) return e;
 
@@ -1040,6 +1047,8 @@ cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, u
         a.err = err;
         a.run_flag = flag;
         a.run_when = 0;
+        a.spin_limit = p.tuning.spin_limit;
+        a.stall_tile = q == 0 ? p.tuning.stall_tile : 0xffffffffu;
         int mode;
         if (q == 0) {
             mode = perm_in ? IN_GATHER : IN_RAW;
@@ -1075,12 +1084,12 @@ cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, u
         la.dtype = p.dtype[0];
         la.invert = invert ? 1 : 0;
         la.reverse = order == 2 ? 1 : 0;
-        la.lo_bits = w == 8 ? 32 : 0;
+        la.lo_bits = (uint32_t)p.msd_lo_bits;
         la.flag = flag;
         la.err = err;
         la.keys_out = key0_out;
         la.perm_out = perm_out;
-        e = msd_local(la, w, p.msd_chunks, s);
+        e = msd_local(la, w, p.msd_chunks, p.tuning.msd_match, s);
     }
     if (prof) prof->end(KC_LOCALSORT, s);
     return e;

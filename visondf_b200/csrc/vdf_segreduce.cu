@@ -704,6 +704,116 @@ __device__ __forceinline__ void emit_single_rows(const SegArgs& a, const Agg<NV>
     }
 }
 
+// Tiles where nearly every row starts a group (few groups of two or more
+// rows): rows are striped over the TPT threads (row first + j * TPT + tt),
+// so that records of one-row groups go out with consecutive lanes at
+// (nearly) consecutive group ids; the head row of a longer group walks that
+// group's few rows itself.  A group is emitted by the tile holding its last
+// row: one that runs past the tile's end is left to the next tile, whose
+// prefix carries it.  hm[t] / hp[t]: head mask of the sub-tile's 8-row block
+// t (consecutive rows 8t .. 8t+7) and the number of heads in blocks before
+// it within its warp of blocks (32 blocks), wh[w]: heads in warp w's blocks.
+template <int NK, int NV, int TPT, int RPT>
+__device__ __forceinline__ void emit_mostly_single(const SegArgs& a, const Agg<NV>* tile_prefix,
+                                                   const Agg<NV>* block_prefix, uint32_t tile, uint32_t H,
+                                                   const uint32_t* hm, const uint32_t* hp, const uint32_t* wh,
+                                                   const int* vc, const int* kw, int tt) {
+    constexpr int B = 8;  // rows per head-mask block
+    static_assert(TPT * RPT == kSegTile && kSegTile / B <= TPT * RPT, "tile layout");
+    const uint64_t n = a.n;
+    const uint64_t first = (uint64_t)tile * kSegTile;
+    const uint32_t rows = (uint32_t)min((uint64_t)kSegTile, n - first);
+    // is tile row o a head? (o == rows: the row after the tile)
+    auto is_head = [&](uint32_t o) -> bool {
+        if (o >= rows) {
+            if (first + o >= n) return true;
+            bool d = false;
+#pragma unroll
+            for (int k = 0; k < NK; ++k)
+                d |= load_raw(a.key[k].src, kw[k], first + o) != load_raw(a.key[k].src, kw[k], first + o - 1);
+            return d;
+        }
+        return (hm[o / B] >> (o % B)) & 1u;
+    };
+    auto heads_before = [&](uint32_t o) -> uint32_t {  // heads among tile rows < o
+        const uint32_t t = o / B;
+        uint32_t c = hp[t] + __popc(hm[t] & ((1u << (o % B)) - 1u));
+        for (uint32_t w = 0; w < t / 32; ++w) c += wh[w];
+        return c;
+    };
+    // Aggregate of tile rows [o, end) up to the next head; returns the end.
+    auto walk = [&](uint32_t o, uint64_t (*w)[4], uint32_t& cnt) -> uint32_t {
+        uint32_t e = o;
+        while (e < rows && (e == o || !is_head(e))) {
+            const uint64_t r = first + e;
+#pragma unroll
+            for (int v = 0; v < NV; ++v) {
+                const uint64_t x = load_val(a.val[v].src, a.val[v].dtype, r);
+                if (cnt == 0) {
+                    col_init(w[v], x, vc[v]);
+                } else {
+                    uint64_t one[4];
+                    col_init(one, x, vc[v]);
+                    col_merge(w[v], one, vc[v]);
+                }
+            }
+            ++cnt;
+            ++e;
+        }
+        return e;
+    };
+    // the group carried in from earlier tiles (id H - 1): it ends before the
+    // first row if that is a head, else at the tile's first head after it
+    if (tt == 0 && H > 0) {
+        const Agg<NV> P = agg_combine(block_prefix[tile / kScanTiles], tile_prefix[tile], vc);
+        uint64_t w[NV > 0 ? NV : 1][4];
+#pragma unroll
+        for (int v = 0; v < NV; ++v)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) w[v][q] = P.w[v][q];
+        uint32_t cnt = P.cnt;
+        bool ends = true;
+        if (!is_head(0)) {
+            uint32_t e = 0;
+            while (e < rows && !is_head(e)) {
+                const uint64_t r = first + e;
+#pragma unroll
+                for (int v = 0; v < NV; ++v) {
+                    uint64_t one[4];
+                    col_init(one, load_val(a.val[v].src, a.val[v].dtype, r), vc[v]);
+                    col_merge(w[v], one, vc[v]);
+                }
+                ++cnt;
+                ++e;
+            }
+            ends = e < rows || first + e == n || is_head(e);
+        }
+        if (ends) emit_group<NV>(a, H - 1, cnt, w, vc);
+    }
+#pragma unroll 1
+    for (int j = 0; j < RPT; ++j) {
+        const uint32_t o = (uint32_t)j * TPT + (uint32_t)tt;
+        if (o >= rows) break;
+        const uint64_t r = first + o;
+        const bool h = is_head(o);
+        const uint32_t hb = heads_before(o);
+        const uint32_t grow = h ? H + hb : H + hb - 1;  // the group of row r
+        if (a.row_group) a.row_group[r] = grow;
+        if (r == n - 1 && a.n_groups) *a.n_groups = grow + 1;
+        if (!h) continue;
+        const uint32_t g = H + hb;
+#pragma unroll
+        for (int k = 0; k < NK; ++k)
+            if (a.key_out[k]) store_raw(a.key_out[k], kw[k], g, load_raw(a.key[k].src, kw[k], r));
+        if (a.group_start) a.group_start[g] = (uint32_t)r;
+        uint64_t w[NV > 0 ? NV : 1][4];
+        uint32_t cnt = 0;
+        const uint32_t e = walk(o, w, cnt);
+        // complete when the next head (or the last row) is inside this tile
+        if (e < rows || first + e == n || is_head(e)) emit_group<NV>(a, g, cnt, w, vc);
+    }
+}
+
 template <int NK, int NV>
 __device__ __forceinline__ void seg_emit_body(const SegArgs& a, const Agg<NV>* tile_prefix, const Agg<NV>* block_prefix,
                                               uint32_t tile) {
@@ -889,6 +999,9 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     __shared__ Agg<NV> s_wtot[WARPS];
     __shared__ Agg<NV> s_pre[kSubTiles];
     __shared__ uint32_t s_all[WARPS];
+    __shared__ uint32_t s_hm[kSegThreads];  // head mask of each thread's rows
+    __shared__ uint32_t s_hp[kSegThreads];  // heads before them in the warp
+    __shared__ uint32_t s_wh[WARPS];        // heads in each warp's rows
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int sub = warp / kWarpsPerSub, wsub = warp - sub * kWarpsPerSub;
     const uint32_t tile = blockIdx.x * kSubTiles + sub;
@@ -927,13 +1040,31 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     const uint32_t nvalid = row0 >= n ? 0u : (n - row0 >= (uint64_t)ITEMS ? (uint32_t)ITEMS : (uint32_t)(n - row0));
     const bool wall = __all_sync(0xffffffffu, hmask == (1u << nvalid) - 1u);
     if (lane == 0) s_all[warp] = wall ? 1u : 0u;
+    {
+        const uint32_t h = __popc(hmask);
+        uint32_t ih = h;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, ih, d);
+            if (lane >= d) ih += o;
+        }
+        s_hm[tid] = hmask;
+        s_hp[tid] = ih - h;
+        if (lane == 31) s_wh[warp] = ih;
+    }
     __syncthreads();
     bool sub_all = true;
+    uint32_t sub_heads = 0;
 #pragma unroll
-    for (int w = 0; w < kWarpsPerSub; ++w) sub_all = sub_all && s_all[sub * kWarpsPerSub + w] != 0u;
+    for (int w = 0; w < kWarpsPerSub; ++w) {
+        sub_all = sub_all && s_all[sub * kWarpsPerSub + w] != 0u;
+        sub_heads += s_wh[sub * kWarpsPerSub + w];
+    }
+    // nearly every row starts a group: at most 32 rows continue one
+    const bool sub_most = !sub_all && sub_heads + 32 >= (uint32_t)kSegTile;
 
     Agg<NV> lx = agg_identity<NV>();
-    if (!sub_all) {
+    if (!sub_all && !sub_most) {
         // this thread's trailing segment: rows from its last head (all rows
         // when it has none).  Rows are consumed from the front of a shift
         // register, so the loop stays rolled (one copy of the merge code)
@@ -1004,6 +1135,15 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
         if (tvalid)
             emit_single_rows<NK, NV, kWarpsPerSub * 32, ITEMS, ITEMS / 2>(a, tile_prefix, block_prefix, tile, H_tile,
                                                                           vc, kw, sub_tid);
+        return;
+    }
+    if (sub_most) {
+        if (tvalid) {
+            const int base = sub * kWarpsPerSub * 32;
+            emit_mostly_single<NK, NV, kWarpsPerSub * 32, ITEMS>(a, tile_prefix, block_prefix, tile, H_tile,
+                                                                s_hm + base, s_hp + base, s_wh + sub * kWarpsPerSub,
+                                                                vc, kw, sub_tid);
+        }
         return;
     }
     if (row0 >= n) return;

@@ -16,6 +16,7 @@
 // transform_group_by_onecol_mt pair per query (sort_by_mt.hpp:3-180,
 // transform_group_by_onecol_mt.hpp:14-373).
 #include <chrono>
+#include <atomic>
 #include <condition_variable>
 #include <deque>
 #include <memory>
@@ -94,6 +95,9 @@ struct vdf_server {
     uint64_t fixed = 0, in_use = 0, max_in_use = 0;
     uint64_t batches = 0, completed = 0;
     bool stop = false;
+    // failure injection for tests: batches left to fail at start / finish
+    std::atomic<uint32_t> inject_start{0}, inject_finish{0};
+    vdf_status inject_status = VDF_ERR_DEVICE;
     std::thread th;
     std::chrono::steady_clock::time_point t0;
     std::string last_error;
@@ -114,6 +118,12 @@ void free_batch_outputs(vdf_server* S, ServerBatch& B) {
 // Builds and launches one batch on a free slot; called without the lock.
 vdf_status start_batch(vdf_server* S, ServerBatch& B, std::string& why) {
     const vdf_server_config& c = S->cfg;
+    for (uint32_t k = S->inject_start.load(); k > 0;) {
+        if (S->inject_start.compare_exchange_weak(k, k - 1)) {
+            why = "batch start failed (injected by a test hook)";
+            return S->inject_status;
+        }
+    }
     cudaStream_t s = S->stream[B.slot];
     uint64_t rows = 0;
     for (const vdf_batch_query& q : B.queries) rows += q.n;
@@ -177,6 +187,12 @@ vdf_status finish_batch(vdf_server* S, ServerBatch& B, std::string& why) {
     }
     vdf_status st = vdf_ctx_check(S->ctx[B.slot], s);  // device wait timeouts / bad indices
     if (st != VDF_OK) why = vdf_ctx_last_error(S->ctx[B.slot]);
+    for (uint32_t k = S->inject_finish.load(); st == VDF_OK && k > 0;) {
+        if (S->inject_finish.compare_exchange_weak(k, k - 1)) {
+            why = "batch finish failed (injected by a test hook)";
+            return S->inject_status;
+        }
+    }
     return st;
 }
 
@@ -509,6 +525,14 @@ vdf_status vdf_server_release(vdf_server* S, uint64_t id) {
         if (S->holding[B->slot] == B) S->holding[B->slot] = nullptr;  // the slot's arenas are free again
         S->cv.notify_one();
     }
+    return VDF_OK;
+}
+
+vdf_status vdf_server_inject_failure(vdf_server* S, int where, uint32_t count, vdf_status status) {
+    if (!S || (where != 0 && where != 1) || status == VDF_OK) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->inject_status = status;
+    (where == 0 ? S->inject_start : S->inject_finish).store(count);
     return VDF_OK;
 }
 

@@ -326,6 +326,7 @@ def _server_lib():
         ("vdf_server_wait", st, [vp, C.c_uint64, C.c_double, C.POINTER(Result)]),
         ("vdf_server_release", st, [vp, C.c_uint64]),
         ("vdf_server_read_stats", st, [vp, C.POINTER(Stats)]),
+        ("vdf_server_inject_failure", st, [vp, C.c_int, C.c_uint32, C.c_int]),
         ("vdf_server_last_error", C.c_char_p, [vp]),
         ("vdf_server_destroy", None, [vp]),
     ]:
@@ -459,6 +460,13 @@ class Server:
         st = self.lib.vdf_server_release(self.handle, rid)
         if st != self._lib.OK:
             raise self._lib.VdfError(st, "vdf_server_release")
+
+    def inject_failure(self, where: str, count: int = 1, status: int = 4):
+        """Test hook: the next `count` batches fail with `status` when they
+        start ("start") or when their results are read back ("finish")."""
+        st = self.lib.vdf_server_inject_failure(self.handle, {"start": 0, "finish": 1}[where], count, status)
+        if st != self._lib.OK:
+            raise self._lib.VdfError(st, "vdf_server_inject_failure")
 
     def stats(self) -> dict:
         _, _, Stats = self.lib._server_types
