@@ -22,15 +22,19 @@
 //   4. k_msd_chunks  chunk c holds the whole buckets that start in
 //                    [c*T, (c+1)*T); found by a two-level warp search for
 //                    the first bucket boundary at or after c*T
-//   5. k_msd_local   one CTA per chunk (<= kMsdCap rows): stable 8-bit LSD
-//                    passes in shared memory over the digits of key 0 above
-//                    its low F bits that vary inside the chunk, then each
-//                    run of rows with equal high bits is ranked directly by
-//                    (low F bits, key 1's order image, position) -- key 1 is
-//                    read through the row id only for rows whose key 0 ties
-//                    with another row's -- and the raw sorted key 0 and the
-//                    permutation are written.  F is 32 for 8-byte keys
-//                    (runs are rare for spread keys) and 0 for 4-byte keys.
+//   5. k_msd_local   one CTA per chunk (<= kMsdCap rows): one counting pass
+//                    over 8192 bins of (key - chunk minimum) >> S puts the
+//                    rows of spread keys about one per bin; the rows sharing
+//                    a bin are ranked by (key 0, key 1's order image,
+//                    position in the chunk) -- key 1 is read through the row
+//                    id only where key 0 ties -- and the raw sorted key 0 and
+//                    the permutation are written.  A chunk where a bin holds
+//                    a run longer than kMsdRunMax (many equal or clustered
+//                    keys) is sorted instead by stable 8-bit LSD passes in
+//                    shared memory over the digits of key 0 above its low F
+//                    bits that vary inside it, with runs of equal high bits
+//                    ranked the same way (F = 32 for 8-byte keys, 0 for
+//                    4-byte keys).
 //
 // Every pass is stable and ties keep their row order, so the result is
 // exactly the stable order over all keys.  A one-key chunk with a run longer
@@ -174,10 +178,14 @@ struct LocalCfg {
     static constexpr int CAP = THREADS * ITEMS;
     static constexpr size_t KEYS = (size_t)CAP * sizeof(K);
     static constexpr size_t VALS = (size_t)CAP * 4;
-    static constexpr size_t SEC = (size_t)CAP * 8;  // key 1 images of rows in runs
-    static constexpr size_t CNT = (size_t)WARPS * 256 * 4;
+    static constexpr size_t SEC = (size_t)CAP * 8;  // key 1 images of rows in runs; the counting pass's bins
     static constexpr size_t MISC = 16 * 4 + (size_t)WARPS * 4 + (size_t)2 * WARPS * 8;
-    static constexpr size_t SMEM = KEYS + VALS + SEC + CNT + MISC;
+    static constexpr size_t ORIG = (size_t)CAP * 2;  // chunk position of each slot's row
+    static constexpr size_t SBIN = (size_t)CAP * 2;  // bin of each slot's row
+    static constexpr size_t SMEM = KEYS + VALS + SEC + MISC + ORIG + SBIN;
+    // the counting pass's 8192 bins and the LSD passes' per-warp counters
+    // live in the key-1 buffer, which is only needed after either is done
+    static_assert(SEC >= 8192 * 4 && SEC >= (size_t)WARPS * 256 * 4, "key-1 buffer doubles as counters");
 };
 
 template <int THREADS>
@@ -291,6 +299,198 @@ __device__ __forceinline__ void local_pass(K (&key)[ITEMS], uint32_t (&val)[ITEM
     }
 }
 
+// The chunk's rows in one counting pass: bin = (key - min) >> S with S the
+// smallest shift that brings the chunk's key range below 8192 bins, so rows
+// of spread keys fall about one per bin or fewer.  Rows land in their bin in no
+// particular order (shared-memory atomics); then each run of rows sharing a
+// bin is ranked by (key, key 1's order image, position in the chunk) --
+// positions are the rows' stable order so far -- which restores the exact
+// stable order.  Returns false, with nothing written to global memory, when
+// some run is longer than kMsdRunMax (many equal or clustered keys): the
+// caller then sorts the chunk with LSD passes instead.  On success item j of
+// a thread holds the row of slot (warp * ia + j) * 32 + lane and its final
+// position in the chunk is newpos[j].
+// Warp-wide minimum / maximum with the 32-bit reduce instructions: 8-byte
+// keys reduce their high halves first, then the low halves of the lanes that
+// hold the extreme high half.
+__device__ __forceinline__ uint32_t warp_min(uint32_t x) { return __reduce_min_sync(0xffffffffu, x); }
+__device__ __forceinline__ uint32_t warp_max(uint32_t x) { return __reduce_max_sync(0xffffffffu, x); }
+__device__ __forceinline__ uint64_t warp_min(uint64_t x) {
+    const uint32_t hi = __reduce_min_sync(0xffffffffu, (uint32_t)(x >> 32));
+    const uint32_t lo = __reduce_min_sync(0xffffffffu, (uint32_t)(x >> 32) == hi ? (uint32_t)x : 0xffffffffu);
+    return ((uint64_t)hi << 32) | lo;
+}
+__device__ __forceinline__ uint64_t warp_max(uint64_t x) {
+    const uint32_t hi = __reduce_max_sync(0xffffffffu, (uint32_t)(x >> 32));
+    const uint32_t lo = __reduce_max_sync(0xffffffffu, (uint32_t)(x >> 32) == hi ? (uint32_t)x : 0u);
+    return ((uint64_t)hi << 32) | lo;
+}
+
+template <typename K, int THREADS, int ITEMS>
+__device__ __forceinline__ bool counting_finish(K (&key)[ITEMS], uint32_t (&val)[ITEMS], uint32_t (&newpos)[ITEMS],
+                                                uint32_t m, uint32_t ia, const MsdLocalArgs& a, K* sk, uint32_t* sv,
+                                                uint16_t* so, uint16_t* sbin, uint64_t* ssec, uint32_t* misc,
+                                                uint32_t* wsum, K* wmin, K* wmax) {
+    // the bins live in the key-1 buffer, which is not needed before the
+    // scatter is done
+    uint32_t* bins = reinterpret_cast<uint32_t*>(ssec);
+    constexpr int WARPS = THREADS / 32;
+    constexpr int NB = 8192, BPT = NB / THREADS;  // bins, bins per thread
+    static_assert(NB % THREADS == 0 && BPT % 4 == 0, "bin layout");
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // ---- key range of the chunk
+    K kmin = ~K(0), kmax = 0;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+        if (j < (int)ia && pos < m) {
+            kmin = min(kmin, key[j]);
+            kmax = max(kmax, key[j]);
+        }
+    }
+    kmin = warp_min(kmin);
+    kmax = warp_max(kmax);
+    if (lane == 0) {
+        wmin[warp] = kmin;
+        wmax[warp] = kmax;
+    }
+#pragma unroll
+    for (int i = 0; i < BPT; i += 4) *reinterpret_cast<uint4*>(bins + tid * BPT + i) = make_uint4(0, 0, 0, 0);
+    __syncthreads();
+    kmin = warp_min(lane < WARPS ? wmin[lane] : ~K(0));
+    kmax = warp_max(lane < WARPS ? wmax[lane] : K(0));
+    const K range = kmax - kmin;
+    int bl = 0;  // bit length of the range
+    if constexpr (sizeof(K) == 8) bl = range ? 64 - __clzll((long long)range) : 0;
+    else bl = range ? 32 - __clz((int)range) : 0;
+    const uint32_t S = bl > 13 ? (uint32_t)(bl - 13) : 0u;
+    auto bin_of = [&](K k) -> uint32_t { return (uint32_t)((k - kmin) >> S); };
+    // ---- histogram, exclusive scan, scatter
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+        if (j < (int)ia && pos < m) atomicAdd(&bins[bin_of(key[j])], 1u);
+    }
+    __syncthreads();
+    uint32_t b[BPT];
+    uint32_t tsum = 0;
+#pragma unroll
+    for (int i = 0; i < BPT; i += 4) {
+        const uint4 q = *reinterpret_cast<const uint4*>(bins + tid * BPT + i);
+        b[i] = q.x;
+        b[i + 1] = q.y;
+        b[i + 2] = q.z;
+        b[i + 3] = q.w;
+    }
+#pragma unroll
+    for (int i = 0; i < BPT; ++i) {
+        const uint32_t c = b[i];
+        b[i] = tsum;
+        tsum += c;
+    }
+    uint32_t all;
+    const uint32_t start = local_excl_scan<THREADS>(tsum, wsum, &all);
+#pragma unroll
+    for (int i = 0; i < BPT; i += 4)
+        *reinterpret_cast<uint4*>(bins + tid * BPT + i) =
+            make_uint4(start + b[i], start + b[i + 1], start + b[i + 2], start + b[i + 3]);
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+        if (j < (int)ia && pos < m) {
+            const uint32_t bn = bin_of(key[j]);
+            uint32_t slot = atomicAdd(&bins[bn], 1u);
+            if (slot >= m) {  // never when the counts are consistent
+                atomicOr(a.err, ERR_BAD_INDEX);
+                slot = pos;
+            }
+            sk[slot] = key[j];
+            sv[slot] = val[j];
+            so[slot] = (uint16_t)pos;
+            sbin[slot] = (uint16_t)bn;
+        }
+    }
+    __syncthreads();
+    // ---- rows by slot; runs of one bin (bounds from ballots over each
+    //      32-slot group, loops only for runs that cross a group), and key 1
+    //      where key 0 ties inside a run
+    uint32_t run[ITEMS];  // s | e << 16; 0: alone in its bin
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t base = ((uint32_t)warp * ia + j) * 32;
+        const uint32_t p = base + lane;
+        newpos[j] = p;
+        run[j] = 0;
+        if (j < (int)ia) {
+            bool first = true, last = true;
+            uint32_t h = 0;
+            if (p < m) {
+                key[j] = sk[p];
+                val[j] = sv[p];
+                h = sbin[p];
+                first = p == 0 || sbin[p - 1] != h;
+                last = p + 1 >= m || sbin[p + 1] != h;
+            }
+            const uint32_t starts = __ballot_sync(0xffffffffu, first);
+            const uint32_t ends = __ballot_sync(0xffffffffu, last);
+            if (!(first && last)) {
+                const uint32_t sm = starts & (lt | (1u << lane));  // starts at lanes <= this one
+                const uint32_t em = ends & ~lt;                    // ends at lanes >= this one
+                uint32_t s = sm ? base + 31 - __clz(sm) : base;
+                uint32_t e = em ? base + __ffs(em) : base + 32;
+                if (!sm)
+                    while (s > 0 && p - s < kMsdRunMax && sbin[s - 1] == h) --s;
+                if (!em)
+                    while (e < m && e - p <= kMsdRunMax && sbin[e] == h) ++e;
+                run[j] = s | (e << 16);
+                if (e - s > kMsdRunMax) {
+                    misc[4] = 1;
+                } else if (a.sec) {
+                    bool tie = false;
+                    for (uint32_t t = s; t < e; ++t) tie |= (t != p) && sk[t] == key[j];
+                    if (tie) {
+                        uint32_t row = val[j];
+                        if (row >= a.n) {  // never for a permutation of [0, n)
+                            atomicOr(a.err, ERR_BAD_INDEX);
+                            row = 0;
+                        }
+                        ssec[p] = sec_image(a.sec, a.sec_dtype, row, a.invert != 0);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (misc[4]) return false;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        if (run[j] == 0) continue;
+        const uint32_t p = ((uint32_t)warp * ia + j) * 32 + lane;
+        const uint32_t s = run[j] & 0xffffu, e = run[j] >> 16;
+        const K k = key[j];
+        const uint32_t o = so[p];
+        uint32_t r = 0;
+        for (uint32_t t = s; t < e; ++t) {
+            const K tk = sk[t];
+            bool less = tk < k;
+            if (tk == k && t != p) {
+                const uint32_t to = so[t];
+                if (a.sec) {
+                    const uint64_t sc = ssec[p], tsc = ssec[t];
+                    less = tsc < sc || (tsc == sc && to < o);
+                } else {
+                    less = to < o;
+                }
+            }
+            r += less ? 1u : 0u;
+        }
+        newpos[j] = s + r;
+    }
+    return true;
+}
+
 // MATCH: 0 = one ballot per digit bit, 1 = match.any.
 template <typename K, int THREADS, int ITEMS, int MATCH>
 __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
@@ -302,11 +502,13 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
     K* sk = reinterpret_cast<K*>(smem);
     uint32_t* sv = reinterpret_cast<uint32_t*>(smem + C::KEYS);
     uint64_t* ssec = reinterpret_cast<uint64_t*>(smem + C::KEYS + C::VALS);
-    uint32_t* wcnt = reinterpret_cast<uint32_t*>(smem + C::KEYS + C::VALS + C::SEC);  // [WARPS][RADIX]
-    uint32_t* misc = wcnt + WARPS * RADIX;                                            // [0]: failure seen
+    uint32_t* wcnt = reinterpret_cast<uint32_t*>(ssec);                                 // [WARPS][RADIX]
+    uint32_t* misc = reinterpret_cast<uint32_t*>(smem + C::KEYS + C::VALS + C::SEC);  // [0], [4]: long runs
     uint32_t* wsum = misc + 16;                                                       // [WARPS]
-    K* wor = reinterpret_cast<K*>(smem + C::KEYS + C::VALS + C::SEC + C::CNT + 16 * 4 + WARPS * 4);
+    K* wor = reinterpret_cast<K*>(smem + C::KEYS + C::VALS + C::SEC + 16 * 4 + WARPS * 4);
     K* wand = wor + WARPS;
+    uint16_t* so = reinterpret_cast<uint16_t*>(smem + C::KEYS + C::VALS + C::SEC + C::MISC);
+    uint16_t* sbin = so + CAP;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // One thread reads the flag and the chunk bounds for the whole CTA (the
@@ -317,6 +519,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
         misc[2] = a.chunk_start[blockIdx.x];
         misc[3] = a.chunk_start[blockIdx.x + 1];
         misc[0] = 0;
+        misc[4] = 0;
     }
     __syncthreads();
     if (misc[1]) return;  // the plan failed earlier: the LSD passes take over
@@ -346,149 +549,166 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
         }
     }
 
-    // ---- which digits vary inside the chunk
-    K vor = 0, vand = ~K(0);
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
-        if (j < (int)ia && pos < m) {
-            vor |= key[j];
-            vand &= key[j];
-        }
-    }
-#pragma unroll
-    for (int d = 16; d >= 1; d >>= 1) {
-        vor |= __shfl_xor_sync(0xffffffffu, vor, d);
-        vand &= __shfl_xor_sync(0xffffffffu, vand, d);
-    }
-    if (lane == 0) {
-        wor[warp] = vor;
-        wand[warp] = vand;
-    }
-    __syncthreads();
-    vor = 0;
-    vand = ~K(0);
-#pragma unroll
-    for (int w = 0; w < WARPS; ++w) {
-        vor |= wor[w];
-        vand &= wand[w];
-    }
-    const K vary = vor ^ vand;
-
-    // ---- stable 8-bit LSD passes in shared memory over the varying digits
-    //      of key 0 from digit lo_bits / 8 up
-    bool sorted_in_smem = false;
-    for (int dg = (int)(a.lo_bits / 8); dg < KBITS / 8; ++dg) {
-        const uint32_t shift = 8u * dg;
-        if (((vary >> shift) & 0xff) == 0) continue;
-        local_pass<K, THREADS, ITEMS, MATCH>(key, val, shift, ia, sk, sv, wcnt, wsum, a.err);
-        sorted_in_smem = true;
-    }
-    if (!sorted_in_smem) {
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            if (j < (int)ia) {
-                const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
-                sk[pos] = key[j];
-                sv[pos] = val[j];
-            }
-        }
-        __syncthreads();
-    }
-
-    // ---- runs of equal high bits, ranked by (low bits, key 1, position).
-    //      Key 1 is read (through the row id) only for rows whose low bits
-    //      tie with another row of their run, i.e. rows whose key 0 ties.
-    const bool fix = a.lo_bits > 0 || a.sec != nullptr;
-    const uint32_t hs = a.lo_bits;  // high part = key >> hs
-    const K lo_mask = hs ? (K)((((K)1) << hs) - 1) : K(0);
+    // ---- one counting pass over the chunk's key range; where that leaves a
+    //      long run (many equal or clustered keys), stable LSD passes instead
     uint32_t newpos[ITEMS];
-    uint32_t run[ITEMS];  // run bounds s | e << 16 (positions < 2^16); 0: not in a run
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
-        newpos[j] = pos;
-        run[j] = 0;
-        if (fix && j < (int)ia && pos < m) {
-            const K h = key[j] >> hs;
-            if ((pos > 0 && (sk[pos - 1] >> hs) == h) || (pos + 1 < m && (sk[pos + 1] >> hs) == h)) {
-                uint32_t s = pos, e = pos + 1;
-                while (s > 0 && pos - s < kMsdRunMax && (sk[s - 1] >> hs) == h) --s;
-                while (e < m && e - pos <= kMsdRunMax && (sk[e] >> hs) == h) ++e;
-                run[j] = s | (e << 16);
-                if (a.sec && e - s <= kMsdRunMax) {
-                    const K lo = key[j] & lo_mask;
-                    bool tie = false;
-                    for (uint32_t t = s; t < e; ++t) tie |= (t != pos) && ((sk[t] & lo_mask) == lo);
-                    if (tie) {
-                        uint32_t row = val[j];
-                        if (row >= a.n) {  // never for a permutation of [0, n)
-                            atomicOr(a.err, ERR_BAD_INDEX);
-                            row = 0;
-                        }
-                        ssec[pos] = sec_image(a.sec, a.sec_dtype, row, a.invert != 0);
-                    }
-                }
-            }
-        }
-    }
-    if (fix) {
+    const bool counted = counting_finish<K, THREADS, ITEMS>(key, val, newpos, m, ia, a, sk, sv, so, sbin, ssec,
+                                                            misc, wsum, wor, wand);
+    if (!counted) {
         __syncthreads();
 #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
-            if (run[j] == 0) continue;
             const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
-            const uint32_t s = run[j] & 0xffffu, e = run[j] >> 16;
-            const K lo = key[j] & lo_mask;
-            if (e - s > kMsdRunMax) {
-                // a long run: fine if it already is in order (e.g. equal
-                // keys of a one-key sort); otherwise see below
-                if (pos > s) {
-                    const K plo = sk[pos - 1] & lo_mask;
-                    if (plo > lo || (plo == lo && a.sec)) misc[0] = 1;
-                }
-                continue;
+            key[j] = ~K(0);
+            val[j] = 0;
+            if (j < (int)ia && pos < m) {
+                key[j] = ldg_stream(kin + pos);
+                val[j] = ldg_stream(vin + pos);
             }
-            uint32_t r = 0;
-            bool have_sec = false;
-            uint64_t sc = 0;
-            for (uint32_t t = s; t < e; ++t) {
-                const K tlo = sk[t] & lo_mask;
-                bool less = tlo < lo;
-                if (tlo == lo && t != pos) {
-                    if (a.sec) {
-                        if (!have_sec) {
-                            sc = ssec[pos];
-                            have_sec = true;
-                        }
-                        const uint64_t tsc = ssec[t];
-                        less = tsc < sc || (tsc == sc && t < pos);
-                    } else {
-                        less = t < pos;
-                    }
-                }
-                r += less ? 1u : 0u;
+        }
+        // ---- which digits vary inside the chunk
+        K vor = 0, vand = ~K(0);
+    #pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+            if (j < (int)ia && pos < m) {
+                vor |= key[j];
+                vand &= key[j];
             }
-            newpos[j] = s + r;
+        }
+    #pragma unroll
+        for (int d = 16; d >= 1; d >>= 1) {
+            vor |= __shfl_xor_sync(0xffffffffu, vor, d);
+            vand &= __shfl_xor_sync(0xffffffffu, vand, d);
+        }
+        if (lane == 0) {
+            wor[warp] = vor;
+            wand[warp] = vand;
         }
         __syncthreads();
-        if (misc[0]) {
-            // A run longer than the direct ranking handles is out of order.
-            // With a second key that needs key 1 for every row: the plan
-            // fails.  With one key the chunk is finished in shared memory:
-            // LSD passes over the varying low digits, then the high ones
-            // again (every pass is stable, so ties keep their row order).
-            if (a.sec) {
-                if (tid == 0) atomicOr(a.flag, 1u);
-                return;
+        vor = 0;
+        vand = ~K(0);
+    #pragma unroll
+        for (int w = 0; w < WARPS; ++w) {
+            vor |= wor[w];
+            vand &= wand[w];
+        }
+        const K vary = vor ^ vand;
+
+        // ---- stable 8-bit LSD passes in shared memory over the varying digits
+        //      of key 0 from digit lo_bits / 8 up
+        bool sorted_in_smem = false;
+        for (int dg = (int)(a.lo_bits / 8); dg < KBITS / 8; ++dg) {
+            const uint32_t shift = 8u * dg;
+            if (((vary >> shift) & 0xff) == 0) continue;
+            local_pass<K, THREADS, ITEMS, MATCH>(key, val, shift, ia, sk, sv, wcnt, wsum, a.err);
+            sorted_in_smem = true;
+        }
+        if (!sorted_in_smem) {
+    #pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                if (j < (int)ia) {
+                    const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+                    sk[pos] = key[j];
+                    sv[pos] = val[j];
+                }
             }
-            for (int dg = 0; dg < KBITS / 8; ++dg) {
-                const uint32_t shift = 8u * dg;
-                if (((vary >> shift) & 0xff) == 0) continue;
-                local_pass<K, THREADS, ITEMS, MATCH>(key, val, shift, ia, sk, sv, wcnt, wsum, a.err);
+            __syncthreads();
+        }
+
+        // ---- runs of equal high bits, ranked by (low bits, key 1, position).
+        //      Key 1 is read (through the row id) only for rows whose low bits
+        //      tie with another row of their run, i.e. rows whose key 0 ties.
+        const bool fix = a.lo_bits > 0 || a.sec != nullptr;
+        const uint32_t hs = a.lo_bits;  // high part = key >> hs
+        const K lo_mask = hs ? (K)((((K)1) << hs) - 1) : K(0);
+        uint32_t run[ITEMS];  // run bounds s | e << 16 (positions < 2^16); 0: not in a run
+    #pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+            newpos[j] = pos;
+            run[j] = 0;
+            if (fix && j < (int)ia && pos < m) {
+                const K h = key[j] >> hs;
+                if ((pos > 0 && (sk[pos - 1] >> hs) == h) || (pos + 1 < m && (sk[pos + 1] >> hs) == h)) {
+                    uint32_t s = pos, e = pos + 1;
+                    while (s > 0 && pos - s < kMsdRunMax && (sk[s - 1] >> hs) == h) --s;
+                    while (e < m && e - pos <= kMsdRunMax && (sk[e] >> hs) == h) ++e;
+                    run[j] = s | (e << 16);
+                    if (a.sec && e - s <= kMsdRunMax) {
+                        const K lo = key[j] & lo_mask;
+                        bool tie = false;
+                        for (uint32_t t = s; t < e; ++t) tie |= (t != pos) && ((sk[t] & lo_mask) == lo);
+                        if (tie) {
+                            uint32_t row = val[j];
+                            if (row >= a.n) {  // never for a permutation of [0, n)
+                                atomicOr(a.err, ERR_BAD_INDEX);
+                                row = 0;
+                            }
+                            ssec[pos] = sec_image(a.sec, a.sec_dtype, row, a.invert != 0);
+                        }
+                    }
+                }
             }
-#pragma unroll
-            for (int j = 0; j < ITEMS; ++j) newpos[j] = ((uint32_t)warp * ia + j) * 32 + lane;
+        }
+        if (fix) {
+            __syncthreads();
+    #pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                if (run[j] == 0) continue;
+                const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+                const uint32_t s = run[j] & 0xffffu, e = run[j] >> 16;
+                const K lo = key[j] & lo_mask;
+                if (e - s > kMsdRunMax) {
+                    // a long run: fine if it already is in order (e.g. equal
+                    // keys of a one-key sort); otherwise see below
+                    if (pos > s) {
+                        const K plo = sk[pos - 1] & lo_mask;
+                        if (plo > lo || (plo == lo && a.sec)) misc[0] = 1;
+                    }
+                    continue;
+                }
+                uint32_t r = 0;
+                bool have_sec = false;
+                uint64_t sc = 0;
+                for (uint32_t t = s; t < e; ++t) {
+                    const K tlo = sk[t] & lo_mask;
+                    bool less = tlo < lo;
+                    if (tlo == lo && t != pos) {
+                        if (a.sec) {
+                            if (!have_sec) {
+                                sc = ssec[pos];
+                                have_sec = true;
+                            }
+                            const uint64_t tsc = ssec[t];
+                            less = tsc < sc || (tsc == sc && t < pos);
+                        } else {
+                            less = t < pos;
+                        }
+                    }
+                    r += less ? 1u : 0u;
+                }
+                newpos[j] = s + r;
+            }
+            __syncthreads();
+            if (misc[0]) {
+                // A run longer than the direct ranking handles is out of order.
+                // With a second key that needs key 1 for every row: the plan
+                // fails.  With one key the chunk is finished in shared memory:
+                // LSD passes over the varying low digits, then the high ones
+                // again (every pass is stable, so ties keep their row order).
+                if (a.sec) {
+                    if (tid == 0) atomicOr(a.flag, 1u);
+                    return;
+                }
+                for (int dg = 0; dg < KBITS / 8; ++dg) {
+                    const uint32_t shift = 8u * dg;
+                    if (((vary >> shift) & 0xff) == 0) continue;
+                    local_pass<K, THREADS, ITEMS, MATCH>(key, val, shift, ia, sk, sv, wcnt, wsum, a.err);
+                }
+    #pragma unroll
+                for (int j = 0; j < ITEMS; ++j) newpos[j] = ((uint32_t)warp * ia + j) * 32 + lane;
+            }
         }
     }
 
