@@ -549,11 +549,28 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
         }
     }
 
+    // ---- rows already in order (with one key: non-decreasing; with two:
+    //      increasing, so key 1 decides nothing) stay where they are; this is
+    //      the common case when each bucket holds one key value
+    bool in_order = true;
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) {
+        const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+        if (j < (int)ia) {
+            K prev = __shfl_up_sync(0xffffffffu, key[j], 1);
+            if (lane == 0 && pos > 0 && pos < m) prev = kin[pos - 1];
+            if (pos > 0 && pos < m) in_order = in_order && (a.sec ? prev < key[j] : prev <= key[j]);
+        }
+    }
+    in_order = __syncthreads_and(in_order) != 0;
+    uint32_t newpos[ITEMS];
+#pragma unroll
+    for (int j = 0; j < ITEMS; ++j) newpos[j] = ((uint32_t)warp * ia + j) * 32 + lane;
+
     // ---- one counting pass over the chunk's key range; where that leaves a
     //      long run (many equal or clustered keys), stable LSD passes instead
-    uint32_t newpos[ITEMS];
-    const bool counted = counting_finish<K, THREADS, ITEMS>(key, val, newpos, m, ia, a, sk, sv, so, sbin, ssec,
-                                                            misc, wsum, wor, wand);
+    const bool counted = in_order || counting_finish<K, THREADS, ITEMS>(key, val, newpos, m, ia, a, sk, sv, so, sbin,
+                                                                        ssec, misc, wsum, wor, wand);
     if (!counted) {
         __syncthreads();
 #pragma unroll

@@ -1155,7 +1155,9 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
 
     // walk this thread's rows (rolled; each row's values read again, from L1
     // after the fold above brought them in): a head completes the group
-    // before it
+    // before it.  Rows after the last head belong to a group that ends in a
+    // later thread, so the walk stops at the last head unless the rows' groups
+    // are wanted (row_group) or the thread holds the table's last row.
     uint32_t gid = pre.heads;
     uint32_t cnt = pre.cnt;
     uint64_t w[NV > 0 ? NV : 1][4];
@@ -1163,7 +1165,8 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     for (int v = 0; v < NV; ++v)
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[v][q] = pre.w[v][q];
-    const int upto = (int)nvalid;
+    const bool holds_last = row0 + nvalid == n;
+    const int upto = (a.row_group || holds_last) ? (int)nvalid : (hmask ? 32 - __clz(hmask) : 0);
 #pragma unroll 1
     for (int j = 0; j < upto; ++j) {
         const uint64_t r = row0 + j;
@@ -1191,7 +1194,7 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
         }
         if (a.row_group) a.row_group[r] = gid - 1;
     }
-    if (row0 + upto == n) {  // this thread holds the last row: its group ends there
+    if (holds_last) {  // this thread holds the last row: its group ends there
         emit_group<NV>(a, gid - 1, cnt, w, vc);
         if (a.n_groups) *a.n_groups = gid;
     }
