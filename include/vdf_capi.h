@@ -555,6 +555,14 @@ uint64_t vdf_batch_rows(const vdf_batch* batch);
 /* How the plan split the queries (any pointer may be NULL). */
 vdf_status vdf_batch_info(const vdf_batch* batch, uint32_t* small_queries, uint64_t* small_rows,
                           uint32_t* large_queries, uint64_t* large_rows);
+/* How the sort treats the large queries: msd_queries take the MSD-first
+ * sort (top-digit passes, then chunks finished in shared memory), the other
+ * lsd_queries the LSD passes.  With fallbacks non-NULL it waits for the
+ * device and counts the MSD queries of the last launch whose chunks defeated
+ * the plan, so that the LSD passes sorted them instead (any pointer may be
+ * NULL). */
+vdf_status vdf_batch_sort_info(vdf_batch* batch, uint32_t* msd_queries, uint32_t* lsd_queries,
+                               uint32_t* fallbacks);
 /* Enqueues the batch on `stream`: no allocation, no host synchronisation,
  * no host memory read, so it can be stream-captured.  Device-side wait
  * timeouts are reported by vdf_ctx_check. */

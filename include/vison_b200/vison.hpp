@@ -39,8 +39,14 @@
 //     reference re-sorts the raw column, sort_by_mt.hpp:99,111,169-176);
 //   * GroupFunction::Mean is sum / group count (the reference divides by the
 //     frame's row count, create_value_col.inl:46); Min and Max are added;
-//     Gather (a user lambda over the group's values) is not supported on the
-//     GPU path and reports an error.
+//   * GroupFunction::Gather calls the user function f once per group on the
+//     group's values in row order (transform_group_by_alrd_mt.hpp:245-260:
+//     value_col[i] = f(val_grp[grp_by[i]].v)); the groups and their values
+//     come from the GPU sort + group-by with the value column as payload, f
+//     runs on the host.  The element type of f's vector argument is taken
+//     from a function pointer's signature (group_function_assertion.inl:3-13),
+//     else it is the value column's own type.  GroupFunction::None takes the
+//     same path.
 #pragma once
 
 #include <cstdint>
@@ -73,7 +79,8 @@ struct DefaultTypes {  // types/inference_type.hpp:3-8 (CharT omitted: no char c
 
 struct DefaultComparatorFactory {};  // types/comparator.inl:1-11; accepted, unused
 
-inline void default_groupfn_impl() {}
+// group_function_assertion.inl:22-25: the first value of the group (0 for none)
+inline int default_groupfn_impl(std::vector<int>& v) { return v.empty() ? 0 : v[0]; }
 
 // One library context per device, created on first use (the reference's
 // init_openmp, vison.hpp:57-74, is likewise process-wide state).
@@ -108,6 +115,16 @@ inline bool report(vdf_status s, const char* what) {
     std::cerr << "\n";
     return false;
 }
+// element type of a group function's vector argument: from a function
+// pointer's or a (non-generic) lambda's signature; void when neither tells
+template <typename M> struct member_arg { using type = void; };
+template <typename C, typename R, typename T> struct member_arg<R (C::*)(std::vector<T>&) const> { using type = T; };
+template <typename C, typename R, typename T> struct member_arg<R (C::*)(std::vector<T>&)> { using type = T; };
+template <typename F, typename = void> struct group_arg { using type = void; };
+template <typename R, typename T> struct group_arg<R (*)(std::vector<T>&), void> { using type = T; };
+template <typename F>
+struct group_arg<F, std::void_t<decltype(&F::operator())>> : member_arg<decltype(&F::operator())> {};
+
 template <bool ASC>
 constexpr int32_t order() {
 #ifdef VISON_B200_STABLE_DESCENDING
@@ -352,8 +369,7 @@ class Dataframe {
                                const std::string colname = "n", const F f = &default_groupfn_impl) {
         (void)f;
         if constexpr (Function == GroupFunction::Gather || Function == GroupFunction::None) {
-            std::cerr << "transform_group_by: GroupFunction::Gather/None is not supported on the GPU path\n";
-            return;
+            gather_group_by(x, n_col, colname, f);
         } else {
             if (x.empty() || x.size() > 4 || n_col >= ncol) {
                 std::cerr << "transform_group_by: bad key or value column\n";
@@ -578,6 +594,97 @@ class Dataframe {
         case 'l': return vdf_col{lint_v[s].data(), VDF_I64};
         default: return vdf_col{luint_v[s].data(), VDF_U64};
         }
+    }
+
+    // Gather: groups of the key columns (rows seen through the view), the
+    // user function over each group's values, its result broadcast to every
+    // row of the group (the new column is in storage order).
+    template <typename F>
+    void gather_group_by(const std::vector<unsigned int>& x, unsigned int n_col, const std::string& colname,
+                         const F& f) {
+        if (x.empty() || x.size() > 4 || n_col >= ncol) {
+            std::cerr << "transform_group_by: bad key or value column\n";
+            return;
+        }
+        std::vector<vdf_col> keys;
+        for (unsigned int c : x) {
+            if (c >= ncol) {
+                std::cerr << "Column not found\n";
+                return;
+            }
+            if (!numeric(c)) {
+                std::cerr << "transform_group_by: string and bool columns are not keys on the GPU path\n";
+                return;
+            }
+            keys.push_back(col_desc(c));
+        }
+        if (!numeric(n_col)) {
+            std::cerr << "transform_group_by: string and bool columns are not value columns on the GPU path\n";
+            return;
+        }
+        const unsigned s = slot_v[n_col];
+        switch (type_refv[n_col]) {
+        case 'i': gather_typed(keys, int_v[s], n_col, colname, f); break;
+        case 'u': gather_typed(keys, uint_v[s], n_col, colname, f); break;
+        case 'd': gather_typed(keys, dbl_v[s], n_col, colname, f); break;
+        case 'l': gather_typed(keys, lint_v[s], n_col, colname, f); break;
+        default: gather_typed(keys, luint_v[s], n_col, colname, f); break;
+        }
+    }
+
+    template <typename V, typename F>
+    void gather_typed(const std::vector<vdf_col>& keys, const std::vector<V>& col, unsigned int n_col,
+                      const std::string& colname, const F& f) {
+        using GA = typename detail::group_arg<F>::type;
+        using T = std::conditional_t<std::is_void_v<GA>, V, GA>;
+        if constexpr (!std::is_invocable_v<const F&, std::vector<T>&>) {
+            std::cerr << "transform_group_by: the group function does not take this column's values\n";
+        } else {
+            gather_apply<T>(keys, col, n_col, colname, f);
+        }
+    }
+
+    template <typename T, typename V, typename F>
+    void gather_apply(const std::vector<vdf_col>& keys, const std::vector<V>& col, unsigned int n_col,
+                      const std::string& colname, const F& f) {
+        using R = std::decay_t<std::invoke_result_t<const F&, std::vector<T>&>>;
+        static_assert(std::is_arithmetic_v<R>, "a group function returns a number");
+        using Out = std::conditional_t<
+            std::is_floating_point_v<R>, FloatT,
+            std::conditional_t<std::is_signed_v<R>, std::conditional_t<(sizeof(R) > sizeof(IntT)), LIntT, IntT>,
+                               std::conditional_t<(sizeof(R) > sizeof(UIntT)), LUIntT, UIntT>>>;
+        std::vector<uint32_t> perm(nrow), gstart(nrow + 1);
+        std::vector<V> sorted(nrow);
+        std::vector<uint32_t> view;
+        if (in_view) view.assign(row_view_idx.begin(), row_view_idx.end());
+        const vdf_col val = col_desc(n_col);
+        void* po = sorted.data();
+        uint64_t groups = 0;
+        vdf_sort_groupby_args a{};
+        a.n = nrow;
+        a.keys = keys.data();
+        a.nkeys = (int32_t)keys.size();
+        a.order = VDF_ORDER_ASC;
+        a.payload = &val;
+        a.npayload = 1;
+        a.perm_out = perm.data();
+        a.payload_out = &po;
+        a.groupby = 1;
+        a.group_start_out = gstart.data();
+        a.n_groups_host = &groups;
+        a.perm_in = in_view ? view.data() : nullptr;
+        if (!detail::report(vdf_sort_groupby_host(context(), &a, nullptr), "transform_group_by")) return;
+        (void)col;
+        std::vector<Out> out(nrow);
+        std::vector<T> vals;
+        for (uint64_t g = 0; g < groups; ++g) {
+            const uint32_t b = gstart[g], e = g + 1 < groups ? gstart[g + 1] : nrow;
+            vals.clear();
+            for (uint32_t p = b; p < e; ++p) vals.push_back(static_cast<T>(sorted[p]));
+            const Out r = static_cast<Out>(f(vals));
+            for (uint32_t p = b; p < e; ++p) out[perm[p]] = r;
+        }
+        add_raw(std::move(out), colname);
     }
 
     template <bool ASC, bool Soft>

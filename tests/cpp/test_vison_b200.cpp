@@ -1,7 +1,7 @@
 // Exercises the header-only dataframe layer (include/vison_b200/vison.hpp) on
 // the GPU: the reference documentation's sort_by example, Soft/Hard sorts,
 // sorts while in view, materialize, sort_by_external, multi-key sorts and
-// the transform group-by, checked against plain CPU computations here.
+// the transform group-by (Gather with user functions included), checked against plain CPU computations here.
 #include <algorithm>
 #include <cstdio>
 #include <map>
@@ -150,6 +150,75 @@ static void test_transform_group_by() {
     CHECK(ok);
 }
 
+// GroupFunction::Gather: the user function over each group's values in row
+// order (the rows as viewed, when the frame is in view), broadcast per row;
+// checked against a std::map walk over the rows here.
+static double sum_sq(std::vector<double>& v) {
+    double s = 0;
+    for (double x : v) s += x * x;
+    return s;
+}
+
+static void test_transform_group_by_gather() {
+    std::mt19937_64 rng(12);
+    const unsigned N = 50000;
+    std::vector<int> k(N), iv(N);
+    std::vector<double> dv(N);
+    for (unsigned i = 0; i < N; ++i) {
+        k[i] = (int)(rng() % 97) - 40;
+        iv[i] = (int)(rng() % 2000001) - 1000000;
+        dv[i] = (double)((int64_t)(rng() % 4001) - 2000) / 7.0;
+    }
+    std::map<int, std::vector<unsigned>> rows;  // key -> rows in row order
+    for (unsigned i = 0; i < N; ++i) rows[k[i]].push_back(i);
+    DF df;
+    df.add_col(k, "k");
+    df.add_col(iv, "iv");
+    df.add_col(dv, "dv");
+    // the default group function (the first value) and None take the same path
+    df.transform_group_by<void, void, GroupFunction::Gather>({0}, 1, "first");
+    df.transform_group_by<void, void, GroupFunction::None>({0}, 1, "first2");
+    df.transform_group_by<void, void, GroupFunction::Gather>({0}, 2, "ss", &sum_sq);
+    df.transform_group_by<void, void, GroupFunction::Gather>(
+        {0}, 1, "last", [](std::vector<int>& v) { return v.empty() ? 0 : v.back(); });
+    df.transform_group_by<void, void, GroupFunction::Gather>(
+        {0}, 2, "n", [](std::vector<double>& v) { return (unsigned)v.size(); });
+    CHECK(df.ncol == 8);
+    bool ok = true;
+    for (const auto& [key, rs] : rows) {
+        double ss = 0;
+        for (unsigned r : rs) ss += dv[r] * dv[r];
+        for (unsigned r : rs) {
+            ok &= df.int_v[2][r] == iv[rs.front()];  // int_v: k, iv, first, first2, last
+            ok &= df.int_v[3][r] == iv[rs.front()];
+            ok &= df.dbl_v[1][r] == ss;
+            ok &= df.int_v[4][r] == iv[rs.back()];
+            ok &= df.uint_v[0][r] == (unsigned)rs.size();
+        }
+    }
+    CHECK(ok);
+
+    // in view (a Soft sort by dv): groups see their rows in view order
+    DF dw;
+    dw.add_col(k, "k");
+    dw.add_col(iv, "iv");
+    dw.add_col(dv, "dv");
+    unsigned by = 2;
+    dw.sort_by(by);
+    CHECK(dw.in_view);
+    std::vector<unsigned> view(N);
+    std::iota(view.begin(), view.end(), 0u);
+    std::stable_sort(view.begin(), view.end(), [&](unsigned a, unsigned b) { return dv[a] < dv[b]; });
+    std::map<int, int> first_in_view;
+    for (unsigned r : view) first_in_view.emplace(k[r], iv[r]);
+    dw.transform_group_by<void, void, GroupFunction::Gather>({0}, 1, "first");
+    CHECK(dw.in_view && dw.ncol == 4);
+    dw.materialize();
+    bool okv = true;
+    for (unsigned p = 0; p < N; ++p) okv &= dw.int_v[2][p] == first_in_view[k[view[p]]];
+    CHECK(okv);
+}
+
 // transform_unique: the rows kept are those a set walk keeps (first or last
 // occurrence per key value, in row order), for every column of the frame.
 static void test_transform_unique() {
@@ -270,6 +339,7 @@ int main() {
     test_hard_sort_and_view_composition();
     test_sort_by_external();
     test_transform_group_by();
+    test_transform_group_by_gather();
     test_transform_unique();
     test_transform_left_join();
     test_readf();

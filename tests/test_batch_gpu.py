@@ -248,3 +248,125 @@ def test_value_column_sets(ctx, vals):
                 else:
                     assert (host(a.sum) == og.sum[j]).all() and (host(a.sum_hi) == og.sum_hi[j]).all(), (q, j)
         b.close()
+
+
+# queries of the MSD-first plan: spread keys (one and two top digits, 8- and
+# 4-byte), few distinct values (a bucket larger than a chunk: that query falls
+# back to the LSD passes), one key for all rows (likewise), 8-byte keys whose
+# high halves repeat (long runs finished by shared-memory passes)
+SPECS_MSD = [(300_000, np.int64, 300_000), (4097, np.int32, 4097), (50_000, np.int64, 3), (393_217, np.uint32, 10**6),
+             (9000, np.float64, 9000), (60_000, np.int32, 1), (2000, np.int64, 5), (120_000, np.uint64, 60_000),
+             (25_000, np.float32, 25_000)]
+
+
+def msd_queries():
+    queries = make_queries(SPECS_MSD)
+    rng = np.random.default_rng(41)
+    n = 100_000
+    hi = rng.integers(0, 1 << 31, 1000, dtype=np.int64)[rng.integers(0, 1000, n)]
+    k = (hi << 32) | rng.integers(0, 1 << 32, n, dtype=np.int64)
+    queries.append((k, rng.standard_normal(n), rng.integers(-10**15, 10**15, size=n, dtype=np.int64)))
+    return queries
+
+
+def order_image(key):
+    """Unsigned image whose order is the key's (ints: sign bit flipped;
+    floats: sign-magnitude to two's order)."""
+    w = key.itemsize
+    u = key.view(np.uint64 if w == 8 else np.uint32).astype(np.uint64)
+    top = np.uint64(1 << (8 * w - 1))
+    if key.dtype.kind == "i":
+        return u ^ top
+    if key.dtype.kind == "f":
+        full = np.uint64((1 << (8 * w)) - 1)
+        return np.where(u & top, ~u & full, u | top)
+    return u
+
+
+def msd_top_passes(key):
+    """Top-digit passes of a large query's MSD-first plan in a batch (0: the
+    LSD passes): the fewest that leave about 1536 rows per bucket, at most
+    three and fewer than the key's digits; 4-byte keys only with one."""
+    n, w = key.size, key.itemsize
+    passes = [p for p in range(1, min(3, w - 1) + 1) if n <= 1536 << (8 * p)]
+    if not passes or (w == 4 and passes[0] > 1):
+        return 0
+    return passes[0]
+
+
+def msd_plan_fails(key):
+    """Whether the MSD-first plan of one large query falls back to the LSD
+    passes: chunks start every 2048 rows, moved forward to the next change of
+    the top-digit bucket if one lies within 4096 rows, and no chunk may hold
+    more than 4096 rows."""
+    n, w = key.size, key.itemsize
+    p = msd_top_passes(key)
+    if not p:
+        return False
+    b = np.sort(order_image(key) >> np.uint64(8 * (w - p)))
+    starts = [0]
+    for x in range(2048, n, 2048):
+        i = int(np.searchsorted(b, b[x - 1], side="right"))
+        if i <= min(x + 4095, n - 1):
+            starts.append(i)
+        else:
+            if x + 4095 < n - 1:
+                return True
+            starts.append(n)
+    starts.append(n)
+    return any(e - s > 4096 for s, e in zip(starts, starts[1:]))
+
+
+@pytest.mark.parametrize("seg_variant", [0, 4])
+def test_msd_plan_with_per_query_fallback_matches_lsd_plan(ctx, seg_variant):
+    queries = msd_queries()
+    tuning = dict(small_rows=4096, small_bits=8, seg_variant=seg_variant)
+    m = vdf.Context(0)
+    l = vdf.Context(0)
+    try:
+        m.set_sort_strategy(_lib.SORT_AUTO, 0)
+        l.set_sort_strategy(_lib.SORT_LSD, 0)
+        bm, _ = to_batch(m, queries, tuning)
+        bl, _ = to_batch(l, queries, tuning)
+        large = bm.info()["large_queries"]
+        msd = sum(msd_top_passes(k) > 0 for k, _, _ in queries if k.size > 4096)
+        assert 0 < msd < large  # the 393,217-row 4-byte query takes the LSD passes
+        assert bm.sort_info() == dict(msd_queries=msd, lsd_queries=large - msd)
+        assert bl.sort_info() == dict(msd_queries=0, lsd_queries=large)
+        bm.launch()
+        m.check()
+        # the three-value and the one-value queries defeat the plan, and the
+        # normal floats (most share a top byte); the others do not
+        fails = [msd_plan_fails(k) for k, _, _ in queries if k.size > 4096]
+        assert fails[2] and fails[5] and not fails[0] and not fails[-1]
+        assert bm.sort_info(fallbacks=True)["fallbacks"] == sum(fails)
+        check_against_oracle(bm, queries)
+        bl.launch()
+        l.check()
+        ref = snapshot(bl, len(queries))
+        for rep in range(2):  # replays re-arm the per-query flags
+            bm.perm.fill_(-1)
+            bm.launch_graph() if rep else bm.launch()
+            m.check()
+            got = snapshot(bm, len(queries))
+            for q, (x, y) in enumerate(zip(ref, got)):
+                assert (x[0] == y[0]).all() and x[1] == y[1], q
+                assert bits_equal(x[2], y[2]) and (x[3] == y[3]).all(), q
+        bm.close()
+        bl.close()
+    finally:
+        m.close()
+        l.close()
+
+
+def test_four_byte_arena_takes_the_msd_plan(ctx):
+    queries = make_queries(SPECS_4BYTE_LARGE)
+    b, _ = to_batch(ctx, queries, dict(small_rows=8192, small_bits=8, seg_variant=4))
+    assert b.sort_info()["msd_queries"] == 4
+    b.launch()
+    ctx.check()
+    fails = sum(msd_plan_fails(k) for k, _, _ in queries if k.size > 8192)
+    assert fails >= 1  # the two-value query at least
+    assert b.sort_info(fallbacks=True)["fallbacks"] == fails
+    check_against_oracle(b, queries)
+    b.close()

@@ -149,6 +149,7 @@ def _load() -> C.CDLL:
         "vdf_batch_rows": (u64, [vp]),
         "vdf_batch_info": (st, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
                                 C.POINTER(C.c_uint64)]),
+        "vdf_batch_sort_info": (st, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),
         "vdf_batch_launch": (st, [vp, vp]),
         "vdf_batch_launch_graph": (st, [vp, vp]),
         "vdf_batch_destroy": (None, [vp]),
@@ -764,6 +765,18 @@ class Batch:
         lib.vdf_batch_info(self.handle, C.byref(sq), C.byref(sr), C.byref(lq), C.byref(lr))
         return dict(small_queries=sq.value, small_rows=sr.value, large_queries=lq.value, large_rows=lr.value,
                     rows=lib.vdf_batch_rows(self.handle))
+
+    def sort_info(self, fallbacks: bool = False) -> dict:
+        """Queries on the MSD-first sort and on the LSD passes; with
+        fallbacks=True also (after waiting for the device) the MSD queries of
+        the last launch that fell back to the LSD passes."""
+        mq, lq, fb = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        st = lib.vdf_batch_sort_info(self.handle, C.byref(mq), C.byref(lq), C.byref(fb) if fallbacks else None)
+        self.ctx._check(st, "vdf_batch_sort_info")
+        out = dict(msd_queries=mq.value, lsd_queries=lq.value)
+        if fallbacks:
+            out["fallbacks"] = fb.value
+        return out
 
     def launch(self, stream=None):
         self._host = None

@@ -23,6 +23,7 @@
 // n_q) of perm_out and group slots [group_offset[q], group_offset[q] +
 // n_groups[q]) of the group arrays; its group keys are packed in its own key
 // width starting at byte 8 * group_offset[q] of group_keys_out.
+#include <algorithm>
 #include <cstring>
 
 #include "vdf_ctx.h"
@@ -207,9 +208,11 @@ bool batch_tuning_valid(const BatchTuning& t) {
 
 // Host-side plan: classifies the queries, lays out the arena and the tables,
 // and sizes the workspace.  Everything device-side is relative to `ws`.
-bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std::string& why) {
+bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std::string& why, bool msd,
+                int msd_match) {
     P = BatchPlan{};
     P.tuning = t;
+    P.msd_match = msd_match;
     P.nq = a.nqueries;
     P.nvals = a.nvals;
     int bits = 8, tile = 2048;
@@ -280,6 +283,70 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
         return false;
     }
 
+    // MSD-first tables: segment s with D digits and P = msd_passes_for top
+    // digits sorts by digits D-P .. D-1 first; its chunks start every
+    // kMsdCap / 2 rows (moved forward to a bucket boundary on the device).
+    // Taken where it saves passes over HBM: 8-byte keys (P of 8 passes, then
+    // the shared-memory finish), and 4-byte keys with one top digit; two top
+    // digits of a 4-byte key plus the finish measured slower than its four
+    // LSD passes on served batches.
+    P.seg_flag_init.assign(P.segs.size(), 1);
+    if (msd && bits == 8) {
+        std::vector<uint32_t> order;
+        std::vector<int> mp(P.segs.size(), 0);
+        for (uint32_t s = 0; s < P.segs.size(); ++s) {
+            const int w = dtype_width(a.queries[P.seg_query[s]].key.dtype);
+            mp[s] = msd_passes_for(P.segs[s].rows, w);
+            if (w == 4 && mp[s] > 1) mp[s] = 0;
+            if (mp[s] > 0) order.push_back(s);
+        }
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return mp[x] > mp[y]; });
+        uint32_t mt = 0;
+        for (uint32_t i = 0; i < order.size(); ++i) {
+            const uint32_t s = order[i];
+            const SegDesc& d0 = P.segs[s];
+            SegDesc d = d0;
+            d.first_tile = mt;
+            d.passes = (uint32_t)mp[s];
+            d.first_digit = d0.passes - (uint32_t)mp[s];
+            const uint32_t nt = (uint32_t)((d.rows + tile - 1) / tile);
+            for (uint32_t k = 0; k < nt; ++k) P.msd_tile_seg.push_back(i);
+            mt += nt;
+            for (uint64_t r = 0; r < d.rows; r += kChunkRows) {
+                SegChunk c{};
+                c.row_start = d.row_start + r;
+                c.rows = (uint32_t)std::min<uint64_t>(kChunkRows, d.rows - r);
+                c.seg = i;
+                P.msd_hist_chunks.push_back(c);
+            }
+            P.msd_segs.push_back(d);
+            P.msd_seg_of.push_back(s);
+            P.msd_max_passes = std::max(P.msd_max_passes, mp[s]);
+            P.seg_flag_init[s] = 0;
+        }
+        for (uint32_t s = 0; s < P.segs.size(); ++s) {  // chunks in arena order
+            if (mp[s] == 0) continue;
+            const SegDesc& d = P.segs[s];
+            for (uint64_t r = 0; r < d.rows; r += kMsdCap / 2) {
+                MsdSegChunk c{};
+                c.x = (uint32_t)(d.row_start + r);
+                c.seg_start = (uint32_t)d.row_start;
+                c.seg_end = (uint32_t)(d.row_start + d.rows);
+                c.pshift = 8u * (d.passes - (uint32_t)mp[s]);
+                c.seg = s;
+                P.msd_chunks.push_back(c);
+            }
+        }
+        for (int g = 0; g < 16; ++g) {
+            uint32_t c = 0;
+            for (const SegDesc& d : P.msd_segs)
+                if ((int)d.passes > g) c += (uint32_t)((d.rows + tile - 1) / tile);
+            P.msd_tiles_in_pass[g] = c;
+        }
+        P.msd_queries = (uint32_t)order.size();
+        P.msd = !order.empty();
+    }
+
     // workspace layout
     const size_t A = 256;
     size_t o = 0;
@@ -290,8 +357,15 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
     P.o_tile_seg = o; o = align_up(o + 4 * std::max<size_t>(1, P.tile_seg.size()), A);
     P.o_chunks = o; o = align_up(o + sizeof(SegChunk) * std::max<size_t>(1, P.chunks.size()), A);
     P.o_small = o; o = align_up(o + 4 * std::max<size_t>(1, small.size()), A);
+    P.o_msd_segs = o; o = align_up(o + sizeof(SegDesc) * std::max<size_t>(1, P.msd_segs.size()), A);
+    P.o_msd_tile_seg = o; o = align_up(o + 4 * std::max<size_t>(1, P.msd_tile_seg.size()), A);
+    P.o_msd_hist_chunks = o; o = align_up(o + sizeof(SegChunk) * std::max<size_t>(1, P.msd_hist_chunks.size()), A);
+    P.o_msd_chunks = o; o = align_up(o + sizeof(MsdSegChunk) * std::max<size_t>(1, P.msd_chunks.size()), A);
+    P.o_flag_init = o; o = align_up(o + 4 * std::max<size_t>(1, P.segs.size()), A);
     P.desc_bytes = o;
     P.o_counters = o; o = align_up(o + 64, A);  // [0]: small-kernel work counter, [8]: large group count
+    P.o_seg_flag = o; o = align_up(o + 4 * std::max<size_t>(1, P.segs.size()), A);
+    P.o_chunk_start = o; o = align_up(o + 4 * (P.msd_chunks.size() + 1), A);
     P.o_seg_first = o; o = align_up(o + 4 * std::max<size_t>(1, P.segs.size()), A);
     const size_t kw = (size_t)P.key_width;
     P.o_arena_keys = o; o = align_up(o + kw * nl, A);
@@ -310,6 +384,9 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
     P.o_tail = o;
     size_t tail = seg_sort_workspace_bytes(nl, (uint32_t)P.segs.size(), (uint32_t)P.tile_seg.size(),
                                            std::max(1, maxp), t.seg_variant, P.key_width);
+    if (P.msd)
+        tail = std::max(tail, seg_sort_workspace_bytes(nl, (uint32_t)P.msd_segs.size(), (uint32_t)P.msd_tile_seg.size(),
+                                                       P.msd_max_passes, t.seg_variant, P.key_width));
     tail = std::max(tail, segreduce_workspace_bytes(nl, a.nvals));
     P.ws_bytes = o + tail;
     return true;
@@ -399,6 +476,57 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
         sa.perm_out = a.perm_out + P.large_base;
         sa.err = err;
         unsigned char* tail = ws + P.o_tail;
+        if (P.msd) {
+            // top-digit passes of the MSD segments straight into the sorted
+            // buffers, then each chunk of whole buckets is finished in place
+            // (a CTA reads its rows before it writes them)
+            uint32_t* flags = reinterpret_cast<uint32_t*>(ws + P.o_seg_flag);
+            if ((e = cudaMemcpyAsync(flags, ws + P.o_flag_init, 4 * P.segs.size(), cudaMemcpyDeviceToDevice, s)) !=
+                cudaSuccess)
+                return e;
+            SegSortArgs ma = sa;
+            ma.segs = reinterpret_cast<const SegDesc*>(ws + P.o_msd_segs);
+            ma.nsegs = (uint32_t)P.msd_segs.size();
+            ma.tile_seg = reinterpret_cast<const uint32_t*>(ws + P.o_msd_tile_seg);
+            ma.ntiles = (uint32_t)P.msd_tile_seg.size();
+            ma.chunks = reinterpret_cast<const SegChunk*>(ws + P.o_msd_hist_chunks);
+            ma.nchunks = (uint32_t)P.msd_hist_chunks.size();
+            ma.max_passes = P.msd_max_passes;
+            for (int g = 0; g < 16; ++g) ma.tiles_in_pass[g] = P.msd_tiles_in_pass[g];
+            if ((e = run_seg_sort(ma, tail, s, prof)) != cudaSuccess) return e;
+            n += 2;
+            for (int g = 0; g < P.msd_max_passes; ++g) n += P.msd_tiles_in_pass[g] ? 1 : 0;
+            uint32_t* chunk_start = reinterpret_cast<uint32_t*>(ws + P.o_chunk_start);
+            const uint32_t nch = (uint32_t)P.msd_chunks.size();
+            const MsdSegChunk* sc = reinterpret_cast<const MsdSegChunk*>(ws + P.o_msd_chunks);
+            MsdChunkArgs ca{};
+            ca.keys = sa.keys_out;
+            ca.n = P.n_large;
+            ca.nchunks = nch;
+            ca.chunk_start = chunk_start;
+            ca.seg_chunks = sc;
+            ca.seg_flag = flags;
+            if (prof) prof->begin(KC_LOCALSORT, s);
+            e = msd_chunks(ca, P.key_width, s);
+            if (e == cudaSuccess) {
+                MsdLocalArgs la{};
+                la.keys = sa.keys_out;
+                la.vals = sa.perm_out;
+                la.chunk_start = chunk_start;
+                la.n = P.n_large;
+                la.dtype = P.key_width == 8 ? U64 : U32;  // the arena holds order images
+                la.err = err;
+                la.keys_out = sa.keys_out;
+                la.perm_out = sa.perm_out;
+                la.seg_chunks = sc;
+                la.seg_flag = flags;
+                e = msd_local(la, P.key_width, nch, P.msd_match, s);
+            }
+            if (prof) prof->end(KC_LOCALSORT, s);
+            if (e != cudaSuccess) return e;
+            n += 2;
+            sa.seg_flag = flags;  // the LSD passes: planned and failed segments only
+        }
         if ((e = run_seg_sort(sa, tail, s, prof)) != cudaSuccess) return e;
         n += 2;
         for (int g = 0; g < P.max_passes; ++g) n += P.tiles_in_pass[g] ? 1 : 0;
@@ -558,7 +686,7 @@ vdf_status vdf_batch_create(vdf_ctx* c, const vdf_batch_args* a, const vdf_batch
     b->queries.assign(a->queries, a->queries + a->nqueries);
     b->args.queries = b->queries.data();
     std::string why;
-    if (!vdf::plan_batch(b->plan, b->args, t, why)) {
+    if (!vdf::plan_batch(b->plan, b->args, t, why, c->tuning.msd != 0, c->tuning.msd_match)) {
         delete b;
         return fail(c, VDF_ERR_UNSUPPORTED, "%s", why.c_str());
     }
@@ -586,6 +714,14 @@ vdf_status vdf_batch_create(vdf_ctx* c, const vdf_batch_args* a, const vdf_batch
         std::memcpy(host.data() + P.o_chunks, P.chunks.data(), sizeof(vdf::SegChunk) * P.chunks.size());
     if (!P.small_queries.empty())
         std::memcpy(host.data() + P.o_small, P.small_queries.data(), 4 * P.small_queries.size());
+    if (P.msd) {
+        std::memcpy(host.data() + P.o_msd_segs, P.msd_segs.data(), sizeof(vdf::SegDesc) * P.msd_segs.size());
+        std::memcpy(host.data() + P.o_msd_tile_seg, P.msd_tile_seg.data(), 4 * P.msd_tile_seg.size());
+        std::memcpy(host.data() + P.o_msd_hist_chunks, P.msd_hist_chunks.data(),
+                    sizeof(vdf::SegChunk) * P.msd_hist_chunks.size());
+        std::memcpy(host.data() + P.o_msd_chunks, P.msd_chunks.data(), sizeof(vdf::MsdSegChunk) * P.msd_chunks.size());
+        std::memcpy(host.data() + P.o_flag_init, P.seg_flag_init.data(), 4 * P.seg_flag_init.size());
+    }
     // per-query outputs known on the host: row offsets; empty queries' ranges.
     // Uploaded on the batch's own non-blocking stream, so creating a batch
     // does not wait for other work on the device (only for these copies).
@@ -620,6 +756,27 @@ vdf_status vdf_batch_info(const vdf_batch* b, uint32_t* small_queries, uint64_t*
     if (small_rows) *small_rows = b->plan.n_small;
     if (large_queries) *large_queries = (uint32_t)b->plan.segs.size();
     if (large_rows) *large_rows = b->plan.n_large;
+    return VDF_OK;
+}
+
+vdf_status vdf_batch_sort_info(vdf_batch* b, uint32_t* msd_queries, uint32_t* lsd_queries, uint32_t* fallbacks) {
+    if (!b) return VDF_ERR_INVALID_ARG;
+    const vdf::BatchPlan& P = b->plan;
+    if (msd_queries) *msd_queries = P.msd_queries;
+    if (lsd_queries) *lsd_queries = (uint32_t)P.segs.size() - P.msd_queries;
+    if (!fallbacks) return VDF_OK;
+    *fallbacks = 0;
+    if (!P.msd) return VDF_OK;
+    vdf_ctx* c = b->ctx;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if (c->ws != b->ws) return fail(c, VDF_ERR_WORKSPACE, "the context workspace moved since vdf_batch_create");
+    DeviceGuard g(c->device);
+    std::vector<uint32_t> flags(P.segs.size());
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess)
+        e = cudaMemcpy(flags.data(), b->ws + P.o_seg_flag, 4 * flags.size(), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return from_cuda(c, e, "batch sort info");
+    for (size_t s = 0; s < flags.size(); ++s) *fallbacks += (P.seg_flag_init[s] == 0 && flags[s] != 0) ? 1u : 0u;
     return VDF_OK;
 }
 

@@ -84,8 +84,27 @@ struct BatchPlan {
     uint64_t n_small = 0, n_large = 0, n_total = 0, large_base = 0;
     int max_passes = 0;
     uint32_t tiles_in_pass[16] = {};
+    // MSD-first plan for the large queries: the segments that take it sort
+    // by their top digits (msd_segs: passes over those digits only), then
+    // chunks of whole buckets are finished in shared memory; afterwards the
+    // LSD passes run only for segments whose flag is set (those planned for
+    // them, and those whose chunks defeated the plan)
+    bool msd = false;
+    int msd_match = 0;
+    uint32_t msd_queries = 0;
+    std::vector<SegDesc> msd_segs;         // more passes first
+    std::vector<uint32_t> msd_seg_of;      // [msd segs] segment index in segs
+    std::vector<uint32_t> msd_tile_seg;
+    std::vector<SegChunk> msd_hist_chunks;
+    std::vector<MsdSegChunk> msd_chunks;   // in arena order
+    std::vector<uint32_t> seg_flag_init;   // [segs] 1: LSD passes, 0: MSD-first
+    int msd_max_passes = 0;
+    uint32_t msd_tiles_in_pass[16] = {};
     // workspace layout (byte offsets)
-    size_t o_queries = 0, o_segs = 0, o_seg_query = 0, o_tile_seg = 0, o_chunks = 0, o_small = 0, desc_bytes = 0;
+    size_t o_queries = 0, o_segs = 0, o_seg_query = 0, o_tile_seg = 0, o_chunks = 0, o_small = 0;
+    size_t o_msd_segs = 0, o_msd_tile_seg = 0, o_msd_hist_chunks = 0, o_msd_chunks = 0, o_flag_init = 0;
+    size_t desc_bytes = 0;
+    size_t o_seg_flag = 0, o_chunk_start = 0;
     size_t o_counters = 0, o_seg_first = 0, o_arena_keys = 0, o_arena_seg = 0, o_arena_vals[VDF_BATCH_MAX_VALS] = {};
     size_t o_arena_recs = 0, rec_bytes = 0;
     size_t o_sorted_keys = 0, o_sorted_vals[VDF_BATCH_MAX_VALS] = {}, o_group_seg = 0, o_group_key = 0, o_tail = 0;
@@ -93,7 +112,10 @@ struct BatchPlan {
     int graph_launches = 0;
 };
 
-bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std::string& why);
+// msd: plan the MSD-first sort for the large queries it fits (8-bit digit
+// variants only); msd_match: the shared-memory finish's digit-match method.
+bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std::string& why, bool msd = false,
+                int msd_match = 0);
 BatchDev batch_dev_view(const BatchPlan& P, const vdf_batch_args& a, unsigned char* ws, uint32_t* err);
 cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned char* ws, uint32_t* err,
                          cudaStream_t s, cudaStream_t side, cudaEvent_t fork, cudaEvent_t join, Profiler* prof,

@@ -61,13 +61,15 @@ struct ScanArgs {
 
 // One segment of a segmented sort: rows [row_start, row_start + rows) of the
 // arena, tiles [first_tile, first_tile + ceil(rows / tile)), sorted in
-// `passes` digit passes.
+// `passes` digit passes over digits first_digit .. first_digit + passes - 1
+// (0 and the key's digit count for an LSD sort; the top digits for the
+// MSD-first plan).
 struct SegDesc {
     uint64_t row_start;
     uint32_t rows;
     uint32_t first_tile;
     uint32_t passes;
-    uint32_t pad;
+    uint32_t first_digit;
 };
 
 struct PassArgs {
@@ -103,6 +105,10 @@ struct PassArgs {
     // the default kSpinLimit), and a tile whose CTA publishes nothing
     uint32_t spin_limit = 0;
     uint32_t stall_tile = 0xffffffffu;
+    // segmented passes only: with seg_flag set, a tile runs only when
+    // (seg_flag[segment] != 0) == (seg_flag_when != 0)
+    const uint32_t* seg_flag = nullptr;
+    uint32_t seg_flag_when = 0;
 };
 
 
@@ -120,6 +126,10 @@ struct SortTuning {
     // limit (0 = default) and a tile of the first pass that never publishes
     uint32_t spin_limit = 0;
     uint32_t stall_tile = 0xffffffffu;
+    // segmented passes only: with seg_flag set, a tile runs only when
+    // (seg_flag[segment] != 0) == (seg_flag_when != 0)
+    const uint32_t* seg_flag = nullptr;
+    uint32_t seg_flag_when = 0;
 };
 SortTuning default_sort_tuning();
 bool sort_tuning_valid(const SortTuning& t);
@@ -162,12 +172,21 @@ struct MsdHistArgs {
     uint64_t n;
     uint32_t* hist;    // [ndig][256]
 };
+// A chunk of a segmented MSD-first sort: nominal first row x (the segment's
+// first row for its first chunk), the segment's rows [seg_start, seg_end),
+// the shift that leaves its keys' top (bucket) bits, and its segment.
+struct MsdSegChunk {
+    uint32_t x, seg_start, seg_end, pshift, seg, pad[3];
+};
 struct MsdChunkArgs {
     const void* keys;  // order images sorted by their top bits
     uint64_t n;
     uint32_t chunk_rows, nchunks, pshift;
     uint32_t* chunk_start;  // [nchunks + 1]
     uint32_t* flag;
+    // segmented sorts: per-chunk descriptors, and a failure flag per segment
+    const MsdSegChunk* seg_chunks = nullptr;
+    uint32_t* seg_flag = nullptr;
 };
 struct MsdLocalArgs {
     const void* keys;        // order images of key 0 sorted by their top bits
@@ -181,6 +200,10 @@ struct MsdLocalArgs {
     uint32_t* err;
     void* keys_out;          // raw sorted key 0 (may be null)
     uint32_t* perm_out;
+    // segmented sorts: each chunk's segment; a failing chunk sets its
+    // segment's flag instead of the global one
+    const MsdSegChunk* seg_chunks = nullptr;
+    uint32_t* seg_flag = nullptr;
 };
 cudaError_t msd_hist(const MsdHistArgs& a, int width, cudaStream_t s);
 cudaError_t msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t cap, uint32_t* flag, cudaStream_t s);
@@ -188,6 +211,9 @@ cudaError_t msd_chunks(const MsdChunkArgs& a, int width, cudaStream_t s);
 cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, int match, cudaStream_t s);
 // Kernel launches run_sort makes for a plan (conditional ones included).
 int sort_launches(const SortPlan& p);
+// Global top-digit passes of the MSD-first plan for n rows of width-byte keys
+// (0: none fits).
+int msd_passes_for(uint64_t n, int width);
 
 SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const SortTuning& tuning);
 // Sorts; writes perm_out (and key0_out = raw sorted most-significant key, may
@@ -231,6 +257,9 @@ struct SegSortArgs {
     void* keys_out;               // [n] sorted key images (each segment in place)
     uint32_t* perm_out;           // [n] arena row ids in sorted order
     uint32_t* err;
+    // conditional per segment: with seg_flag set, only the segments whose
+    // flag is non-zero are sorted (their histograms, passes and outputs)
+    const uint32_t* seg_flag = nullptr;
 };
 int seg_sort_variant_count();
 bool seg_sort_variant_info(int v, int* bits, int* tile_rows);

@@ -125,39 +125,57 @@ __global__ void __launch_bounds__(256) k_msd_chunks(MsdChunkArgs a) {
     const int lane = threadIdx.x & 31;
     const uint32_t c = blockIdx.x * 8 + (threadIdx.x >> 5);
     if (c > a.nchunks) return;
-    uint32_t failed = 0;  // read once per warp: the ballots below need the whole warp
-    if (lane == 0) failed = *static_cast<volatile uint32_t*>(a.flag);
-    if (__shfl_sync(0xffffffffu, failed, 0)) return;
     const K* keys = static_cast<const K*>(a.keys);
-    const uint64_t n = a.n;
+    // chunk c starts at or after row x of rows [start, end) sorted by their
+    // top bits (key >> pshift); a segmented sort gives each chunk its
+    // segment's bounds, shift and failure flag
+    uint64_t x = 0, start = 0, end = a.n;
+    uint32_t pshift = a.pshift;
+    uint32_t* flag = a.flag;
+    if (c < a.nchunks) {
+        if (a.seg_chunks) {
+            const MsdSegChunk d = a.seg_chunks[c];
+            x = d.x;
+            start = d.seg_start;
+            end = min((uint64_t)d.seg_end, a.n);
+            pshift = d.pshift;
+            flag = a.seg_flag + d.seg;
+        } else {
+            x = (uint64_t)c * a.chunk_rows;
+        }
+    }
     uint64_t out;
-    if (c == 0) {
-        out = 0;
-    } else if (c == a.nchunks) {
-        out = n;
+    if (c == a.nchunks) {
+        out = a.n;
+    } else if (x <= start || x >= end) {
+        // a segment's first chunk starts with it (written even when the
+        // segment has failed: the chunk before it may end another segment)
+        out = min(max(x, start), end);
     } else {
+        uint32_t failed = 0;  // read once per warp: the ballots below need the whole warp
+        if (lane == 0) failed = *static_cast<volatile uint32_t*>(flag);
+        if (__shfl_sync(0xffffffffu, failed, 0)) return;
         // first i >= x whose top bits differ from row x-1's; rows are sorted
         // by their top bits, so "differs" is false up to the boundary and
         // true after it, and a probe tells on which side it lies
-        const uint64_t x = (uint64_t)c * a.chunk_rows;  // < n
-        const K p0 = keys[x - 1] >> a.pshift;
+        const K p0 = keys[x - 1] >> pshift;
         constexpr uint32_t S = kMsdCap / 32;  // level-1 probe spacing
-        const uint64_t q = min(x + (uint64_t)(lane + 1) * S - 1, n - 1);
-        const uint32_t hit = __ballot_sync(0xffffffffu, (keys[q] >> a.pshift) != p0);
+        const uint64_t q = min(x + (uint64_t)(lane + 1) * S - 1, end - 1);
+        const uint32_t hit = __ballot_sync(0xffffffffu, (keys[q] >> pshift) != p0);
         if (!hit) {
             // kMsdCap rows after x still share row x-1's top bits: that bucket
             // is larger than a chunk can hold (or runs to the end)
-            out = n;
-            if (x + (uint64_t)32 * S - 1 < n - 1 && lane == 0) atomicOr(a.flag, 1u);
+            out = end;
+            if (x + (uint64_t)32 * S - 1 < end - 1 && lane == 0) atomicOr(flag, 1u);
         } else {
             const uint32_t L = __ffs(hit) - 1;
             const uint64_t lo = x + (uint64_t)L * S;  // every row before lo shares p0
-            const uint64_t hi = min(x + (uint64_t)(L + 1) * S - 1, n - 1);  // differs at hi
+            const uint64_t hi = min(x + (uint64_t)(L + 1) * S - 1, end - 1);  // differs at hi
             out = hi;
 #pragma unroll
             for (uint32_t r = 0; r < S / 32; ++r) {
                 const uint64_t pos = lo + r * 32 + lane;
-                const bool d = pos >= hi || (keys[pos] >> a.pshift) != p0;
+                const bool d = pos >= hi || (keys[pos] >> pshift) != p0;
                 const uint32_t b = __ballot_sync(0xffffffffu, d);
                 if (b) {
                     out = lo + r * 32 + (__ffs(b) - 1);
@@ -216,12 +234,13 @@ __device__ __forceinline__ uint64_t sec_image(const void* col, int dt, uint32_t 
     return (uint64_t)order32(ld_rand4(static_cast<const uint32_t*>(col) + row), dt, invert);
 }
 
-// One stable 8-bit LSD pass in shared memory over the digit at `shift` of
+// One stable 8-bit LSD pass in shared memory over the digit digit(key) of
 // the CTA's rows (item j of a thread at position (warp * ia + j) * 32 + lane;
-// slots past the chunk hold all-ones keys and rank last).  Afterwards the
-// rows are in sk / sv in the new order and back in key / val by position.
-template <typename K, int THREADS, int ITEMS, int MATCH>
-__device__ __forceinline__ void local_pass(K (&key)[ITEMS], uint32_t (&val)[ITEMS], uint32_t shift, uint32_t ia,
+// slots past the chunk hold all-ones keys, whose digit must be the largest,
+// and rank last).  Afterwards the rows are in sk / sv in the new order and
+// back in key / val by position.
+template <typename K, int THREADS, int ITEMS, int MATCH, typename DigitF>
+__device__ __forceinline__ void local_pass(K (&key)[ITEMS], uint32_t (&val)[ITEMS], DigitF digit, uint32_t ia,
                                            K* sk, uint32_t* sv, uint32_t* wcnt, uint32_t* wsum, uint32_t* err) {
     constexpr int WARPS = THREADS / 32, RADIX = 256;
     constexpr uint32_t CAP = (uint32_t)(THREADS * ITEMS);
@@ -235,7 +254,7 @@ __device__ __forceinline__ void local_pass(K (&key)[ITEMS], uint32_t (&val)[ITEM
     for (int j = 0; j < ITEMS; ++j) {
         rank[j] = 0;
         if (j < (int)ia) {
-            const uint32_t d = (uint32_t)(key[j] >> shift) & 0xffu;
+            const uint32_t d = digit(key[j]);
             uint32_t peers;
             if constexpr (MATCH == 1) {
                 peers = __match_any_sync(0xffffffffu, d);
@@ -278,7 +297,7 @@ __device__ __forceinline__ void local_pass(K (&key)[ITEMS], uint32_t (&val)[ITEM
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
         if (j < (int)ia) {
-            const uint32_t d = (uint32_t)(key[j] >> shift) & 0xffu;
+            const uint32_t d = digit(key[j]);
             uint32_t r = rank[j] + my[d];
             if (r >= CAP) {  // never when the counts are consistent
                 atomicOr(err, ERR_BAD_INDEX);
@@ -326,7 +345,7 @@ __device__ __forceinline__ uint64_t warp_max(uint64_t x) {
     return ((uint64_t)hi << 32) | lo;
 }
 
-template <typename K, int THREADS, int ITEMS>
+template <typename K, int THREADS, int ITEMS, int MATCH>
 __device__ __forceinline__ bool counting_finish(K (&key)[ITEMS], uint32_t (&val)[ITEMS], uint32_t (&newpos)[ITEMS],
                                                 uint32_t m, uint32_t ia, const MsdLocalArgs& a, K* sk, uint32_t* sv,
                                                 uint16_t* so, uint16_t* sbin, uint64_t* ssec, uint32_t* misc,
@@ -372,8 +391,10 @@ __device__ __forceinline__ bool counting_finish(K (&key)[ITEMS], uint32_t (&val)
         if (j < (int)ia && pos < m) atomicAdd(&bins[bin_of(key[j])], 1u);
     }
     __syncthreads();
+    // one scan of packed words: rows before the bin (low 16 bits) and
+    // occupied bins before it (high 16 bits: the bin's dense index)
     uint32_t b[BPT];
-    uint32_t tsum = 0;
+    uint32_t tsum = 0, tmax = 0;
 #pragma unroll
     for (int i = 0; i < BPT; i += 4) {
         const uint4 q = *reinterpret_cast<const uint4*>(bins + tid * BPT + i);
@@ -385,15 +406,57 @@ __device__ __forceinline__ bool counting_finish(K (&key)[ITEMS], uint32_t (&val)
 #pragma unroll
     for (int i = 0; i < BPT; ++i) {
         const uint32_t c = b[i];
+        tmax = max(tmax, c);
         b[i] = tsum;
-        tsum += c;
+        tsum += c + (c ? (1u << 16) : 0u);
     }
     uint32_t all;
     const uint32_t start = local_excl_scan<THREADS>(tsum, wsum, &all);
+    if (__syncthreads_or(tmax > kMsdRunMax)) {
+        // A bin holds a run longer than the direct ranking takes (many equal
+        // or clustered keys): stable passes over the dense bin index instead
+        // of the scatter -- one when at most 256 bins are occupied, else two
+        // -- keep each bin's rows in their stable order, which is the final
+        // order wherever a bin holds one key value.  The dense index table
+        // takes the position and bin buffers (unused on this path).
+        static_assert(2 * (size_t)THREADS * ITEMS >= NB, "dense table fits the position and bin buffers");
+        uint16_t* dt = so;
+#pragma unroll
+        for (int i = 0; i < BPT; ++i) dt[tid * BPT + i] = (uint16_t)((start + b[i]) >> 16);
+        __syncthreads();
+        // slots past the chunk (all-ones keys) take the largest index, so they stay last
+        auto dense = [&](K k) -> uint32_t {
+            const K off = (k - kmin) >> S;
+            return off < (K)NB ? (uint32_t)dt[(uint32_t)off] : 0xffffu;
+        };
+        uint32_t* wcnt = bins;  // the bin counts are no longer needed
+        if ((all >> 16) <= 256) {
+            local_pass<K, THREADS, ITEMS, MATCH>(
+                key, val, [&](K k) { return min(dense(k), 255u); }, ia, sk, sv, wcnt, wsum, a.err);
+        } else {
+            local_pass<K, THREADS, ITEMS, MATCH>(
+                key, val, [&](K k) { return dense(k) & 0xffu; }, ia, sk, sv, wcnt, wsum, a.err);
+            local_pass<K, THREADS, ITEMS, MATCH>(
+                key, val, [&](K k) { return dense(k) >> 8; }, ia, sk, sv, wcnt, wsum, a.err);
+        }
+        // in order now unless some bin holds several key values (or, with a
+        // second key, key 0 ties): then the caller's LSD passes take over
+        bool bad = false;
+#pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t pos = ((uint32_t)warp * ia + j) * 32 + lane;
+            if (j < (int)ia && pos > 0 && pos < m) {
+                const K prev = sk[pos - 1];
+                bad |= a.sec ? !(prev < key[j]) : (prev > key[j]);
+            }
+        }
+        return __syncthreads_or(bad) == 0;
+    }
 #pragma unroll
     for (int i = 0; i < BPT; i += 4)
         *reinterpret_cast<uint4*>(bins + tid * BPT + i) =
-            make_uint4(start + b[i], start + b[i + 1], start + b[i + 2], start + b[i + 3]);
+            make_uint4((start + b[i]) & 0xffffu, (start + b[i + 1]) & 0xffffu, (start + b[i + 2]) & 0xffffu,
+                       (start + b[i + 3]) & 0xffffu);
     __syncthreads();
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
@@ -511,13 +574,17 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
     uint16_t* sbin = so + CAP;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // the flag a failing chunk raises: the sort's, or its segment's
+    uint32_t* const fail_word = a.seg_chunks ? a.seg_flag + a.seg_chunks[blockIdx.x].seg : a.flag;
     // One thread reads the flag and the chunk bounds for the whole CTA (the
     // flag may be raised by another CTA meanwhile; every thread must take
     // the same branch around the barriers below).
     if (tid == 0) {
-        misc[1] = *static_cast<volatile uint32_t*>(a.flag);
+        misc[1] = *static_cast<volatile uint32_t*>(fail_word);
         misc[2] = a.chunk_start[blockIdx.x];
-        misc[3] = a.chunk_start[blockIdx.x + 1];
+        uint32_t e = a.chunk_start[blockIdx.x + 1];
+        if (a.seg_chunks) e = min(e, a.seg_chunks[blockIdx.x].seg_end);  // the segment's last chunk
+        misc[3] = e;
         misc[0] = 0;
         misc[4] = 0;
     }
@@ -527,7 +594,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
     if (s1 <= s0) return;
     const uint32_t m = s1 - s0;
     if (m > CAP || s1 > a.n) {
-        if (tid == 0) atomicOr(a.flag, 1u);
+        if (tid == 0) atomicOr(fail_word, 1u);
         return;
     }
     const uint32_t ia = (m + THREADS - 1) / THREADS;  // items per thread in use
@@ -569,8 +636,8 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
 
     // ---- one counting pass over the chunk's key range; where that leaves a
     //      long run (many equal or clustered keys), stable LSD passes instead
-    const bool counted = in_order || counting_finish<K, THREADS, ITEMS>(key, val, newpos, m, ia, a, sk, sv, so, sbin,
-                                                                        ssec, misc, wsum, wor, wand);
+    const bool counted = in_order || counting_finish<K, THREADS, ITEMS, MATCH>(key, val, newpos, m, ia, a, sk, sv, so,
+                                                                               sbin, ssec, misc, wsum, wor, wand);
     if (!counted) {
         __syncthreads();
 #pragma unroll
@@ -618,7 +685,8 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
         for (int dg = (int)(a.lo_bits / 8); dg < KBITS / 8; ++dg) {
             const uint32_t shift = 8u * dg;
             if (((vary >> shift) & 0xff) == 0) continue;
-            local_pass<K, THREADS, ITEMS, MATCH>(key, val, shift, ia, sk, sv, wcnt, wsum, a.err);
+            local_pass<K, THREADS, ITEMS, MATCH>(
+                key, val, [shift](K k) { return (uint32_t)(k >> shift) & 0xffu; }, ia, sk, sv, wcnt, wsum, a.err);
             sorted_in_smem = true;
         }
         if (!sorted_in_smem) {
@@ -715,13 +783,15 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
                 // LSD passes over the varying low digits, then the high ones
                 // again (every pass is stable, so ties keep their row order).
                 if (a.sec) {
-                    if (tid == 0) atomicOr(a.flag, 1u);
+                    if (tid == 0) atomicOr(fail_word, 1u);
                     return;
                 }
                 for (int dg = 0; dg < KBITS / 8; ++dg) {
                     const uint32_t shift = 8u * dg;
                     if (((vary >> shift) & 0xff) == 0) continue;
-                    local_pass<K, THREADS, ITEMS, MATCH>(key, val, shift, ia, sk, sv, wcnt, wsum, a.err);
+                    local_pass<K, THREADS, ITEMS, MATCH>(
+                        key, val, [shift](K k) { return (uint32_t)(k >> shift) & 0xffu; }, ia, sk, sv, wcnt, wsum,
+                        a.err);
                 }
     #pragma unroll
                 for (int j = 0; j < ITEMS; ++j) newpos[j] = ((uint32_t)warp * ia + j) * 32 + lane;

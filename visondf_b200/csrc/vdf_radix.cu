@@ -131,8 +131,10 @@ __global__ void __launch_bounds__(256) k_hist_scan(ScanArgs a) {
 }
 
 // Segmented histograms: one CTA per chunk of one segment, all of that
-// segment's passes at once, flushed into the segment's own rows
-// [seg][pass][radix] of the global histogram.
+// segment's passes at once (digits first_digit .. first_digit + passes - 1),
+// flushed into the segment's own rows [seg][pass][radix] of the global
+// histogram.  With seg_flag set, chunks of segments whose flag is clear
+// return at once.
 struct SegHistArgs {
     const void* keys;
     int key_width;
@@ -143,12 +145,15 @@ struct SegHistArgs {
     uint32_t bits;
     uint32_t nsegs;
     uint64_t n;
+    const uint32_t* seg_flag;
 };
 __global__ void __launch_bounds__(512) k_seg_hist(SegHistArgs a) {
     extern __shared__ uint32_t sh_hist[];
     const SegChunk ch = a.chunks[blockIdx.x];
     if (ch.seg >= a.nsegs || ch.row_start + ch.rows > a.n) return;  // host-built tables are consistent
+    if (a.seg_flag && a.seg_flag[ch.seg] == 0) return;  // flag written by an earlier launch
     const uint32_t passes = a.segs[ch.seg].passes;
+    const uint32_t shift0 = a.segs[ch.seg].first_digit * a.bits;
     const uint32_t radix = 1u << a.bits, mask = radix - 1;
     const uint32_t words = passes * radix;
     if (words > a.stride) return;
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(512) k_seg_hist(SegHistArgs a) {
         for (int q = 0; q < R; ++q) {
             if (r0 + q * step >= ch.rows) break;
             for (uint32_t p = 0; p < passes; ++p)
-                atomicAdd(&sh_hist[p * radix + (uint32_t)((k[q] >> (p * a.bits)) & mask)], 1u);
+                atomicAdd(&sh_hist[p * radix + (uint32_t)((k[q] >> (shift0 + p * a.bits)) & mask)], 1u);
         }
     }
     __syncthreads();
@@ -299,17 +304,22 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tile_base);
     uint32_t first_tile = 0;   // look-back stops here
     uint32_t seg = 0;
+    uint32_t shift = a.shift;
     bool fin = FINAL;
     if constexpr (SEG) {
         valid = 0;
         if (tile < a.status_rows) {
             seg = a.tile_seg[tile];
             const SegDesc sd = a.segs[seg];
+            // a segment left out by its flag (written by an earlier launch,
+            // so every tile of the segment sees the same) only clears status
+            const bool skip = a.seg_flag && ((a.seg_flag[seg] != 0) != (a.seg_flag_when != 0));
             if (tile < sd.first_tile || sd.row_start + sd.rows > n ||
                 (uint64_t)(tile - sd.first_tile) * TILE >= sd.rows) {
                 if (tid == 0) atomicOr(a.err, ERR_BAD_INDEX);  // inconsistent tile table
-            } else if (a.pass < sd.passes) {
+            } else if (a.pass < sd.passes && !skip) {
                 first_tile = sd.first_tile;
+                shift = (sd.first_digit + a.pass) * BITS;
                 tile_base = sd.row_start + (uint64_t)(tile - sd.first_tile) * TILE;
                 valid = (uint32_t)min((uint64_t)TILE, sd.row_start + sd.rows - tile_base);
                 fin = (a.pass + 1 == sd.passes);
@@ -402,11 +412,11 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     for (int i = 0; i < (ITEMS + 3) / 4; ++i) dpk[i] = 0;
     auto digit = [&](int j) -> uint32_t {
         if constexpr (PACKED) return (dpk[j / 4] >> (8 * (j % 4))) & 0xffu;
-        else return digit_of<K, BITS>(key[j], a.shift);
+        else return digit_of<K, BITS>(key[j], shift);
     };
 #pragma unroll
     for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t d = digit_of<K, BITS>(key[j], a.shift);
+        const uint32_t d = digit_of<K, BITS>(key[j], shift);
         if constexpr (PACKED) dpk[j / 4] |= d << (8 * (j % 4));
         if constexpr (MATCH == 3) {
             uint32_t* word = wmask + ((j & 1) * WARPS + warp) * RADIX + d;
@@ -621,7 +631,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
         if (i < valid) {
             const K k = ex_keys[i];
             const uint32_t v = ex_vals[i];
-            const uint32_t d = digit_of<K, BITS>(k, a.shift);
+            const uint32_t d = digit_of<K, BITS>(k, shift);
             uint32_t p = bglob[d] + i;
             if (p >= n) {  // only after a look-back timeout: never write out of bounds
                 atomicOr(a.err, ERR_BAD_INDEX);
@@ -777,7 +787,7 @@ static int tile_rows(const SortTuning& t, int width) {
 // averages at most kMsdBucketRows rows, so that with chunks of nominal
 // kMsdCap / 2 rows a chunk of whole buckets stays within kMsdCap for
 // uniformly spread keys (the average bucket plus six standard deviations).
-static int msd_passes_for(uint64_t n, int width) {
+int msd_passes_for(uint64_t n, int width) {
     const int maxp = std::min(kMsdMaxPasses, width - 1);
     for (int p = 1; p <= maxp; ++p)
         if (n <= (uint64_t)kMsdBucketRows << (8 * p)) return p;
@@ -1176,7 +1186,8 @@ cudaError_t run_seg_sort(const SegSortArgs& sa, unsigned char* ws, cudaStream_t 
     void* kbuf[2] = {ws + L.keys[0], ws + L.keys[1]};
     uint32_t* vbuf[2] = {reinterpret_cast<uint32_t*>(ws + L.vals[0]), reinterpret_cast<uint32_t*>(ws + L.vals[1])};
 
-    SegHistArgs h{sa.keys, sa.key_width, sa.chunks, sa.segs, hist, L.stride, (uint32_t)var.bits, sa.nsegs, sa.n};
+    SegHistArgs h{sa.keys, sa.key_width, sa.chunks, sa.segs, hist, L.stride, (uint32_t)var.bits, sa.nsegs, sa.n,
+                  sa.seg_flag};
     if (prof) prof->begin(KC_HIST, s);
     k_seg_hist<<<sa.nchunks, 512, (size_t)L.stride * 4, s>>>(h);
     if (prof) prof->end(KC_HIST, s);
@@ -1210,6 +1221,8 @@ cudaError_t run_seg_sort(const SegSortArgs& sa, unsigned char* ws, cudaStream_t 
         a.vals_out = vbuf[g & 1];
         a.keys_final = sa.keys_out;
         a.vals_final = sa.perm_out;
+        a.seg_flag = sa.seg_flag;
+        a.seg_flag_when = 1;
         const int cls = wi ? KC_ONESWEEP64 : KC_ONESWEEP32;
         if (prof) prof->begin(cls, s);
         var.k[wi][g == 0 ? 0 : 1]<<<grid, 256, var.smem[wi], s>>>(a);

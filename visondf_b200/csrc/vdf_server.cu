@@ -364,12 +364,17 @@ vdf_status vdf_server_create(const vdf_server_config* cfg, vdf_server** out) {
         vdf::BatchTuning t = cfg->use_default_tuning ? vdf::default_batch_tuning()
                                                      : vdf::BatchTuning{cfg->small_rows, cfg->small_bits,
                                                                         cfg->seg_variant};
-        if (vdf::plan_batch(P, a, t, why)) {
+        if (vdf::plan_batch(P, a, t, why, c->tuning.msd != 0, c->tuning.msd_match)) {
             // 8-byte keys need the most (a batch whose large queries all have
             // 4-byte keys packs 4-byte images); the plan's tail is the largest
-            // need, plus descriptor tables for a full batch of queries
-            const size_t desc = (sizeof(vdf::BatchQuery) + sizeof(vdf::SegDesc) + sizeof(vdf::SegChunk) + 16) *
-                                (size_t)cfg->max_batch_queries + 4 * ((size_t)cfg->max_batch_rows / 1024 + 8);
+            // need, plus descriptor tables for a full batch of queries: per
+            // query a descriptor, its segment (twice with the MSD-first
+            // tables), chunks and flags; per 1024 rows a tile entry (twice),
+            // per kMsdCap / 2 rows an MSD chunk and its start
+            const size_t Q = (size_t)cfg->max_batch_queries, R = (size_t)cfg->max_batch_rows;
+            const size_t desc = (sizeof(vdf::BatchQuery) + 2 * sizeof(vdf::SegDesc) + 2 * sizeof(vdf::SegChunk) +
+                                 sizeof(vdf::MsdSegChunk) + 32) * Q + 8 * (R / 1024 + 8) +
+                                (sizeof(vdf::MsdSegChunk) + 4) * (R / (vdf::kMsdCap / 2) + 8) + 16 * 256;
             st = vdf_ctx_reserve(c, P.ws_bytes + desc + (P.ws_bytes >> 4));
             if (st != VDF_OK) {
                 for (vdf_ctx* x : S->ctx) vdf_ctx_destroy(x);
