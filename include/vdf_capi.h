@@ -173,18 +173,25 @@ int vdf_ctx_get_multikey_mode(vdf_ctx* ctx); /* -1 for a NULL context */
 
 /* Sort strategy for sorts by one or two key columns.
  * VDF_SORT_AUTO (default, with msd_min_rows = 2^20): sorts of at least
- *   msd_min_rows rows first partition the rows by the top 1-3 bytes of key 0
- *   with global radix passes (most significant digit first) and then sort
- *   each chunk of whole partitions (<= 4096 rows) in shared memory by the
- *   rest of key 0 and key 1; where the data defeats that plan (a partition
- *   larger than a chunk, or more than 64 rows sharing key 0's high 32 bits
- *   out of order) the LSD passes over all keys run instead, decided on the
- *   device without a host round trip.  The result is the same stable order.
+ *   msd_min_rows rows whose key 0 is 8 bytes wide first partition the rows
+ *   by the top 1-3 bytes of key 0 with global radix passes (most
+ *   significant digit first) and then sort each chunk of whole partitions
+ *   (<= 4096 rows) in shared memory by the rest of key 0 and key 1; where
+ *   the data defeats that plan (a partition larger than a chunk, or with two
+ *   keys more than 64 rows sharing key 0's high bits out of order) the LSD
+ *   passes over all keys run instead, decided on the device without a host
+ *   round trip.  The result is the same stable order.  Batches (vdf_batch_*)
+ *   choose per query the same way (queries of 8-byte keys).  4-byte keys
+ *   take the LSD passes: their four passes measured faster than the
+ *   partition passes plus the shared-memory finish.
  * VDF_SORT_LSD: always the LSD passes (as the reference's radix sorts do,
- *   radix_sort_uint64_mt.inl:6-166). */
+ *   radix_sort_uint64_mt.inl:6-166).
+ * VDF_SORT_MSD: the MSD-first plan for every key width where it fits (for
+ *   tests and measurements). */
 typedef enum vdf_sort_strategy {
     VDF_SORT_AUTO = 0,
-    VDF_SORT_LSD = 1
+    VDF_SORT_LSD = 1,
+    VDF_SORT_MSD = 2
 } vdf_sort_strategy;
 vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* ctx, int strategy, uint64_t msd_min_rows);
 vdf_status vdf_ctx_get_sort_strategy(vdf_ctx* ctx, int32_t* strategy, uint64_t* msd_min_rows);

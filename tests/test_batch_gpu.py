@@ -283,24 +283,25 @@ def order_image(key):
     return u
 
 
-def msd_top_passes(key):
+def msd_top_passes(key, strategy=_lib.SORT_AUTO):
     """Top-digit passes of a large query's MSD-first plan in a batch (0: the
     LSD passes): the fewest that leave about 1536 rows per bucket, at most
-    three and fewer than the key's digits; 4-byte keys only with one."""
+    three and fewer than the key's digits; 4-byte keys only when the MSD
+    strategy is forced."""
     n, w = key.size, key.itemsize
     passes = [p for p in range(1, min(3, w - 1) + 1) if n <= 1536 << (8 * p)]
-    if not passes or (w == 4 and passes[0] > 1):
+    if not passes or (w == 4 and strategy != _lib.SORT_MSD):
         return 0
     return passes[0]
 
 
-def msd_plan_fails(key):
+def msd_plan_fails(key, strategy=_lib.SORT_AUTO):
     """Whether the MSD-first plan of one large query falls back to the LSD
     passes: chunks start every 2048 rows, moved forward to the next change of
     the top-digit bucket if one lies within 4096 rows, and no chunk may hold
     more than 4096 rows."""
     n, w = key.size, key.itemsize
-    p = msd_top_passes(key)
+    p = msd_top_passes(key, strategy)
     if not p:
         return False
     b = np.sort(order_image(key) >> np.uint64(8 * (w - p)))
@@ -317,28 +318,29 @@ def msd_plan_fails(key):
     return any(e - s > 4096 for s, e in zip(starts, starts[1:]))
 
 
+@pytest.mark.parametrize("strategy", [_lib.SORT_AUTO, _lib.SORT_MSD])
 @pytest.mark.parametrize("seg_variant", [0, 4])
-def test_msd_plan_with_per_query_fallback_matches_lsd_plan(ctx, seg_variant):
+def test_msd_plan_with_per_query_fallback_matches_lsd_plan(ctx, seg_variant, strategy):
     queries = msd_queries()
     tuning = dict(small_rows=4096, small_bits=8, seg_variant=seg_variant)
     m = vdf.Context(0)
     l = vdf.Context(0)
     try:
-        m.set_sort_strategy(_lib.SORT_AUTO, 0)
+        m.set_sort_strategy(strategy, 0)
         l.set_sort_strategy(_lib.SORT_LSD, 0)
         bm, _ = to_batch(m, queries, tuning)
         bl, _ = to_batch(l, queries, tuning)
         large = bm.info()["large_queries"]
-        msd = sum(msd_top_passes(k) > 0 for k, _, _ in queries if k.size > 4096)
-        assert 0 < msd < large  # the 393,217-row 4-byte query takes the LSD passes
+        msd = sum(msd_top_passes(k, strategy) > 0 for k, _, _ in queries if k.size > 4096)
+        assert 0 < msd and (msd < large) == (strategy == _lib.SORT_AUTO)  # 4-byte queries: LSD under AUTO
         assert bm.sort_info() == dict(msd_queries=msd, lsd_queries=large - msd)
         assert bl.sort_info() == dict(msd_queries=0, lsd_queries=large)
         bm.launch()
         m.check()
         # the three-value and the one-value queries defeat the plan, and the
         # normal floats (most share a top byte); the others do not
-        fails = [msd_plan_fails(k) for k, _, _ in queries if k.size > 4096]
-        assert fails[2] and fails[5] and not fails[0] and not fails[-1]
+        fails = [msd_plan_fails(k, strategy) for k, _, _ in queries if k.size > 4096]
+        assert fails[2] and not fails[0] and not fails[-1]
         assert bm.sort_info(fallbacks=True)["fallbacks"] == sum(fails)
         check_against_oracle(bm, queries)
         bl.launch()
@@ -359,14 +361,23 @@ def test_msd_plan_with_per_query_fallback_matches_lsd_plan(ctx, seg_variant):
         l.close()
 
 
-def test_four_byte_arena_takes_the_msd_plan(ctx):
+def test_four_byte_arena_takes_the_msd_plan_when_forced(ctx):
     queries = make_queries(SPECS_4BYTE_LARGE)
-    b, _ = to_batch(ctx, queries, dict(small_rows=8192, small_bits=8, seg_variant=4))
-    assert b.sort_info()["msd_queries"] == 4
-    b.launch()
-    ctx.check()
-    fails = sum(msd_plan_fails(k) for k, _, _ in queries if k.size > 8192)
-    assert fails >= 1  # the two-value query at least
-    assert b.sort_info(fallbacks=True)["fallbacks"] == fails
-    check_against_oracle(b, queries)
-    b.close()
+    tuning = dict(small_rows=8192, small_bits=8, seg_variant=4)
+    auto, _ = to_batch(ctx, queries, tuning)
+    assert auto.sort_info()["msd_queries"] == 0  # AUTO: 4-byte keys take the LSD passes
+    auto.close()
+    m = vdf.Context(0)
+    try:
+        m.set_sort_strategy(_lib.SORT_MSD, 0)
+        b, _ = to_batch(m, queries, tuning)
+        assert b.sort_info()["msd_queries"] == 4
+        b.launch()
+        m.check()
+        fails = sum(msd_plan_fails(k, _lib.SORT_MSD) for k, _, _ in queries if k.size > 8192)
+        assert fails >= 1  # the two-value query at least
+        assert b.sort_info(fallbacks=True)["fallbacks"] == fails
+        check_against_oracle(b, queries)
+        b.close()
+    finally:
+        m.close()

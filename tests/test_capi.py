@@ -101,8 +101,11 @@ def test_sort_plan_choice():
     # 100M rows, int64 + int32 keys: two top-digit passes, 2048-row chunks
     assert info(100_000_000, [vdf.I64, vdf.I32]) == {"msd_passes": 2, "chunks": (100_000_000 + 2047) // 2048}
     assert info(200_000_000, [vdf.I64])["msd_passes"] == 3
-    assert info(393_216, [vdf.I32], msd_min_rows=0)["msd_passes"] == 1
-    assert info(393_217, [vdf.I32], msd_min_rows=0)["msd_passes"] == 2
+    # 4-byte key 0: the LSD passes unless the MSD strategy is forced
+    assert info(393_216, [vdf.I32], msd_min_rows=0)["msd_passes"] == 0
+    assert info(10_000_000, [vdf.U32, vdf.I64])["msd_passes"] == 0
+    assert info(393_216, [vdf.I32], strategy=_lib.SORT_MSD, msd_min_rows=0)["msd_passes"] == 1
+    assert info(393_217, [vdf.I32], strategy=_lib.SORT_MSD, msd_min_rows=0)["msd_passes"] == 2
     # below the row threshold, with three keys, or with the LSD strategy: LSD
     assert info(1000, [vdf.I64])["msd_passes"] == 0
     assert info(1000, [vdf.I64], msd_min_rows=0)["msd_passes"] == 1

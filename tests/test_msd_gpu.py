@@ -2,7 +2,8 @@
 in shared memory, runs of equal high key bits ranked by the rest of the key)
 against the CPU oracle, bit for bit, and its on-device fallback to the LSD
 passes wherever the data defeats the plan.  A context with the MSD-first plan
-at every size makes small inputs take the same path as the 100M-row ones."""
+forced at every size and key width makes small inputs take the same path as
+the 100M-row ones."""
 import ctypes as C
 
 import numpy as np
@@ -22,7 +23,7 @@ ORDERS = [vdf.ORDER_ASC, vdf.ORDER_DESC_STABLE, vdf.ORDER_DESC_REVERSE]
 @pytest.fixture(scope="module")
 def mctx():
     c = vdf.Context(0)
-    c.set_sort_strategy(_lib.SORT_AUTO, 0)
+    c.set_sort_strategy(_lib.SORT_MSD, 0)
     yield c
     c.close()
 
@@ -168,6 +169,13 @@ def test_lsd_strategy_and_min_rows(ctx):
         used, _ = run_sort(c, [datagen.keys_for("uniform", np.int64, 300_000, rng)])
         assert used == 1
         assert c.get_sort_strategy() == (_lib.SORT_AUTO, 300_000)
+        # the automatic choice leaves 4-byte key 0 to the LSD passes
+        used, _ = run_sort(c, [datagen.keys_for("uniform", np.int32, 300_000, rng)])
+        assert used == 0
+        c.set_sort_strategy(_lib.SORT_MSD, 300_000)
+        used, _ = run_sort(c, [datagen.keys_for("uniform", np.int32, 300_000, rng)])
+        assert used == 1
+        assert c.get_sort_strategy() == (_lib.SORT_MSD, 300_000)
     finally:
         c.close()
 
@@ -201,3 +209,35 @@ def test_sort_groupby_two_keys_matches_oracle(mctx):
         assert (host(g) == o).all()
     assert (host(gr.count) == og.count).all()
     assert (host(gr.aggs[1].sum) == og.sum[1]).all()
+
+
+@pytest.mark.parametrize("dt", [np.int32, np.int64, np.uint64])
+@pytest.mark.parametrize("n,pool", [(300_000, 3), (300_000, 40), (300_000, 5000), (1_000_000, 2000),
+                                    (1_000_000, 12_000)])
+def test_long_runs_of_few_values_take_the_dense_bin_finish(mctx, dt, n, pool):
+    # chunks where a bin holds more than 64 rows: stable passes over the
+    # dense bin index (one for <= 256 occupied bins, two above), no fallback
+    # unless a top-digit bucket overflows a chunk
+    from test_batch_gpu import msd_plan_fails  # the chunk rules, emulated on the host
+    rng = np.random.default_rng(pool * 7 + np.dtype(dt).itemsize)
+    k = pool_keys(rng, n, pool, dt)
+    used, fell = run_sort(mctx, [k])
+    assert used == 1
+    assert fell == int(msd_plan_fails(k, _lib.SORT_MSD))
+    if pool >= 2000:
+        assert fell == 0
+
+
+def test_dense_bin_finish_with_mixed_runs(mctx):
+    # long runs of one value next to spread keys in the same chunks (more
+    # than 256 occupied bins), and bins holding two values of a long run
+    rng = np.random.default_rng(8)
+    n = 400_000
+    k = datagen.keys_for("uniform", np.int64, n, rng)
+    hot = datagen.distinct_pool(rng, 2000, np.int64)
+    pick = rng.random(n) < 0.3
+    k[pick] = hot[rng.integers(0, 2000, int(pick.sum()))]
+    k[rng.random(n) < 0.01] += 1  # neighbours of hot values share their bins
+    for order in ORDERS:
+        used, fell = run_sort(mctx, [k], order)
+        assert used == 1 and fell == 0

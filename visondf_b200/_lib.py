@@ -30,7 +30,7 @@ KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segredu
 # vdf_multikey_mode
 MULTIKEY_LSD, MULTIKEY_PRIMARY_FIRST = 0, 1
 # vdf_sort_strategy
-SORT_AUTO, SORT_LSD = 0, 1
+SORT_AUTO, SORT_LSD, SORT_MSD = 0, 1, 2
 
 TORCH_TO_VDF = {
     torch.int32: I32, torch.int64: I64, torch.uint32: U32, torch.uint64: U64,
@@ -313,8 +313,9 @@ class Context:
         return lib.vdf_ctx_get_multikey_mode(self.handle)
 
     def set_sort_strategy(self, strategy: int, msd_min_rows: int = 1 << 20):
-        """SORT_AUTO: MSD-first sorts (one or two keys, >= msd_min_rows rows)
-        with the LSD passes as the on-device fallback; SORT_LSD: LSD only."""
+        """SORT_AUTO: MSD-first sorts (one or two keys, >= msd_min_rows rows,
+        8-byte key 0) with the LSD passes as the on-device fallback;
+        SORT_LSD: LSD only; SORT_MSD: MSD-first for every key width."""
         self._check(lib.vdf_ctx_set_sort_strategy(self.handle, strategy, msd_min_rows), "vdf_ctx_set_sort_strategy")
 
     def sort_stats(self, stream=None) -> dict:

@@ -208,7 +208,7 @@ bool batch_tuning_valid(const BatchTuning& t) {
 
 // Host-side plan: classifies the queries, lays out the arena and the tables,
 // and sizes the workspace.  Everything device-side is relative to `ws`.
-bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std::string& why, bool msd,
+bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std::string& why, int msd,
                 int msd_match) {
     P = BatchPlan{};
     P.tuning = t;
@@ -286,10 +286,10 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
     // MSD-first tables: segment s with D digits and P = msd_passes_for top
     // digits sorts by digits D-P .. D-1 first; its chunks start every
     // kMsdCap / 2 rows (moved forward to a bucket boundary on the device).
-    // Taken where it saves passes over HBM: 8-byte keys (P of 8 passes, then
-    // the shared-memory finish), and 4-byte keys with one top digit; two top
-    // digits of a 4-byte key plus the finish measured slower than its four
-    // LSD passes on served batches.
+    // Taken (msd 1) where it saves time: 8-byte keys (P of 8 passes, then
+    // the shared-memory finish); the top digits of a 4-byte key plus the
+    // finish measured slower than its four LSD passes on served batches.
+    // msd 2 takes it for every width.
     P.seg_flag_init.assign(P.segs.size(), 1);
     if (msd && bits == 8) {
         std::vector<uint32_t> order;
@@ -297,7 +297,7 @@ bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std
         for (uint32_t s = 0; s < P.segs.size(); ++s) {
             const int w = dtype_width(a.queries[P.seg_query[s]].key.dtype);
             mp[s] = msd_passes_for(P.segs[s].rows, w);
-            if (w == 4 && mp[s] > 1) mp[s] = 0;
+            if (w == 4 && msd != 2) mp[s] = 0;
             if (mp[s] > 0) order.push_back(s);
         }
         std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return mp[x] > mp[y]; });
@@ -686,7 +686,7 @@ vdf_status vdf_batch_create(vdf_ctx* c, const vdf_batch_args* a, const vdf_batch
     b->queries.assign(a->queries, a->queries + a->nqueries);
     b->args.queries = b->queries.data();
     std::string why;
-    if (!vdf::plan_batch(b->plan, b->args, t, why, c->tuning.msd != 0, c->tuning.msd_match)) {
+    if (!vdf::plan_batch(b->plan, b->args, t, why, c->tuning.msd, c->tuning.msd_match)) {
         delete b;
         return fail(c, VDF_ERR_UNSUPPORTED, "%s", why.c_str());
     }

@@ -112,9 +112,10 @@ struct BatchPlan {
     int graph_launches = 0;
 };
 
-// msd: plan the MSD-first sort for the large queries it fits (8-bit digit
-// variants only); msd_match: the shared-memory finish's digit-match method.
-bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std::string& why, bool msd = false,
+// msd: 0 the LSD passes; 1 the MSD-first sort for large queries of 8-byte
+// keys, 2 for every width (8-bit digit variants only); msd_match: the
+// shared-memory finish's digit-match method.
+bool plan_batch(BatchPlan& P, const vdf_batch_args& a, const BatchTuning& t, std::string& why, int msd = 0,
                 int msd_match = 0);
 BatchDev batch_dev_view(const BatchPlan& P, const vdf_batch_args& a, unsigned char* ws, uint32_t* err);
 cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned char* ws, uint32_t* err,

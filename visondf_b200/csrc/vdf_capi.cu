@@ -229,12 +229,17 @@ int vdf_ctx_get_multikey_mode(vdf_ctx* c) {
     return c->multikey_mode;
 }
 
+// SortTuning::msd of a strategy: 0 LSD, 1 MSD-first for 8-byte key 0, 2 for every width
+static int msd_mode_of(int strategy) {
+    return strategy == VDF_SORT_MSD ? 2 : (strategy == VDF_SORT_AUTO ? 1 : 0);
+}
+
 vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* c, int strategy, uint64_t msd_min_rows) {
     if (!c) return VDF_ERR_INVALID_ARG;
-    if (strategy != VDF_SORT_AUTO && strategy != VDF_SORT_LSD)
+    if (strategy != VDF_SORT_AUTO && strategy != VDF_SORT_LSD && strategy != VDF_SORT_MSD)
         return fail(c, VDF_ERR_INVALID_ARG, "bad sort strategy %d", strategy);
     std::lock_guard<std::mutex> lk(c->mu);
-    c->tuning.msd = strategy == VDF_SORT_AUTO ? 1 : 0;
+    c->tuning.msd = msd_mode_of(strategy);
     c->tuning.msd_min_rows = msd_min_rows;
     return VDF_OK;
 }
@@ -278,7 +283,7 @@ vdf_status vdf_ctx_sort_stats(vdf_ctx* c, void* stream, uint64_t* msd_sorts, uin
 vdf_status vdf_ctx_get_sort_strategy(vdf_ctx* c, int32_t* strategy, uint64_t* msd_min_rows) {
     if (!c) return VDF_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
-    if (strategy) *strategy = c->tuning.msd ? VDF_SORT_AUTO : VDF_SORT_LSD;
+    if (strategy) *strategy = c->tuning.msd == 2 ? VDF_SORT_MSD : (c->tuning.msd ? VDF_SORT_AUTO : VDF_SORT_LSD);
     if (msd_min_rows) *msd_min_rows = c->tuning.msd_min_rows;
     return VDF_OK;
 }
@@ -289,7 +294,8 @@ vdf_status vdf_sort_plan_info(uint64_t n, const int32_t* key_dtypes, int nkeys, 
     for (int k = 0; k < nkeys; ++k)
         if (!valid_dtype(key_dtypes[k])) return VDF_ERR_INVALID_ARG;
     vdf::SortTuning t = vdf::default_sort_tuning();
-    t.msd = strategy == VDF_SORT_AUTO ? 1 : 0;
+    if (strategy != VDF_SORT_AUTO && strategy != VDF_SORT_LSD && strategy != VDF_SORT_MSD) return VDF_ERR_INVALID_ARG;
+    t.msd = msd_mode_of(strategy);
     t.msd_min_rows = msd_min_rows;
     const vdf::SortPlan p = vdf::make_sort_plan(n, key_dtypes, nkeys, t);
     if (msd_passes) *msd_passes = p.msd ? p.msd_passes : 0;

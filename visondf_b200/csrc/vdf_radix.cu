@@ -815,7 +815,8 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
         if (t > max_tiles) max_tiles = t;
     }
     // MSD-first for one or two keys when the key-0 passes use 8-bit digits
-    if (tuning.msd && nkeys <= 2 && n >= 2 && n >= tuning.msd_min_rows && p.bits[0] == 8) {
+    if (tuning.msd && nkeys <= 2 && n >= 2 && n >= tuning.msd_min_rows && p.bits[0] == 8 &&
+        (tuning.msd == 2 || p.width[0] == 8)) {
         p.msd_passes = msd_passes_for(n, p.width[0]);
         p.msd = p.msd_passes > 0;
         // low bits ranked directly in runs of equal high bits: the low half of

@@ -364,7 +364,7 @@ vdf_status vdf_server_create(const vdf_server_config* cfg, vdf_server** out) {
         vdf::BatchTuning t = cfg->use_default_tuning ? vdf::default_batch_tuning()
                                                      : vdf::BatchTuning{cfg->small_rows, cfg->small_bits,
                                                                         cfg->seg_variant};
-        if (vdf::plan_batch(P, a, t, why, c->tuning.msd != 0, c->tuning.msd_match)) {
+        if (vdf::plan_batch(P, a, t, why, c->tuning.msd, c->tuning.msd_match)) {
             // 8-byte keys need the most (a batch whose large queries all have
             // 4-byte keys packs 4-byte images); the plan's tail is the largest
             // need, plus descriptor tables for a full batch of queries: per
