@@ -150,6 +150,11 @@ typedef struct vdf_sort_tuning {
 int vdf_sort_variant_count(void);
 vdf_status vdf_sort_variant_info(int index, int32_t* key_width, int32_t* threads, int32_t* items_per_thread,
                                  int32_t* digit_bits, int32_t* match);
+/* Feature bits of a variant (0 for an invalid index): bit 0 = its tiles are
+ * staged in shared memory by bulk copies (cp.async.bulk behind an mbarrier,
+ * the next tile's copy overlapping the current tile's ranking), on a
+ * persistent grid. */
+uint32_t vdf_sort_variant_flags(int index);
 vdf_status vdf_ctx_set_sort_tuning(vdf_ctx* ctx, const vdf_sort_tuning* tuning);
 vdf_status vdf_ctx_get_sort_tuning(vdf_ctx* ctx, vdf_sort_tuning* tuning);
 

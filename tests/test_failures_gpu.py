@@ -22,11 +22,17 @@ def sorts_correctly(c, k):
     assert (host(perm).view(np.uint32) == ob.argsort([k])).all()
 
 
-@pytest.mark.parametrize("strategy", [_lib.SORT_LSD, _lib.SORT_AUTO])
-def test_lookback_wait_runs_out_and_is_reported(strategy):
+def _bulk64():
+    return [v["index"] for v in _lib.sort_variants() if v["tma"] and v["key_width"] == 8][0]
+
+
+@pytest.mark.parametrize("strategy,bulk", [(_lib.SORT_LSD, False), (_lib.SORT_AUTO, False), (_lib.SORT_LSD, True)])
+def test_lookback_wait_runs_out_and_is_reported(strategy, bulk):
     c = vdf.Context(0)
     try:
         c.set_sort_strategy(strategy, 0)
+        if bulk:  # the persistent bulk-load variant: the stalled tile's CTA goes on to later tiles
+            c.set_sort_tuning(c.get_sort_tuning()[0], _bulk64())
         rng = np.random.default_rng(1)
         k = datagen.keys_for("uniform", np.int64, 2_000_000, rng)
         c.set_test_hooks(spin_limit=256, stall_tile=0)

@@ -266,3 +266,70 @@ def test_multikey_sort_under_graph_capture(ctx):
     ctx.check()
     assert (host(perm).view(np.uint32) == exp).all()
     del g
+
+
+def _bulk_variants(width):
+    return [v["index"] for v in vdf._lib.sort_variants() if v["tma"] and v["key_width"] == width]
+
+
+@pytest.mark.parametrize("order", ORDERS)
+def test_bulk_load_variants_match_the_oracle(ctx, order):
+    """Variants whose tiles are staged by bulk copies (persistent grid, the
+    next tile's copy overlapping the current one): full and partial last
+    tiles, every pass input (raw column, buffers, keys read through the
+    permutation) and a column that starts off the 16-byte grid, where the
+    tiles load without bulk copies."""
+    from visondf_b200 import _lib
+    t32, t64 = _bulk_variants(4), _bulk_variants(8)
+    assert t32 and t64
+    rng = np.random.default_rng(300 + order)
+    saved = ctx.get_sort_tuning()
+    strategy = ctx.get_sort_strategy()
+    try:
+        ctx.set_sort_strategy(_lib.SORT_LSD, 0)
+        for n in (1, 3071, 3072, 3073, 4096 * 3, 1_000_003):
+            keys = [datagen.keys_for("uniform", np.uint64, n, rng), datagen.keys_for("zipf", np.int32, n, rng)]
+            exp = ob.argsort(keys, order)
+            for a, b in [(t32[0], t64[0]), (t32[-1], t64[-1]), (t32[0], 2), (1, t64[-1])]:
+                ctx.set_sort_tuning(a, b)
+                perm = ctx.argsort([dev(k) for k in keys], order=order)
+                ctx.check()
+                assert (host(perm).view(np.uint32) == exp).all(), (n, a, b)
+        # a column viewed one element in: its tiles are not 16-byte aligned
+        n = 500_001
+        base = datagen.keys_for("uniform", np.int64, n + 1, rng)
+        k = dev(base)[1:]
+        assert k.data_ptr() % 16 != 0
+        ctx.set_sort_tuning(t32[0], t64[0])
+        perm = ctx.argsort([k], order=order)
+        ctx.check()
+        assert (host(perm).view(np.uint32) == ob.argsort([base[1:]], order)).all()
+    finally:
+        ctx.set_sort_tuning(*saved)
+        ctx.set_sort_strategy(*strategy)
+
+
+def test_bulk_load_variants_through_a_row_view_and_the_msd_plan(ctx):
+    import ctypes as C
+
+    from test_groupby_gpu import _host_args
+    from visondf_b200 import _lib
+    t32, t64 = _bulk_variants(4), _bulk_variants(8)
+    rng = np.random.default_rng(31)
+    n = 700_001
+    saved = ctx.get_sort_tuning()
+    strategy = ctx.get_sort_strategy()
+    try:
+        for st in (_lib.SORT_LSD, _lib.SORT_AUTO):
+            ctx.set_sort_strategy(st, 0)
+            for b in t64:
+                ctx.set_sort_tuning(t32[0], b)
+                k = datagen.keys_for("uniform", np.int64, n, rng)
+                view = rng.permutation(n).astype(np.uint32)
+                a, out = _host_args([k], [], [], n, perm_in=view)
+                a.groupby = 0
+                assert vdf.lib.vdf_sort_groupby_host(ctx.handle, C.byref(a), None) == 0
+                assert (out["perm"] == view[np.argsort(k[view], kind="stable")]).all(), (st, b)
+    finally:
+        ctx.set_sort_tuning(*saved)
+        ctx.set_sort_strategy(*strategy)

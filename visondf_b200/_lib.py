@@ -114,6 +114,7 @@ def _load() -> C.CDLL:
         "vdf_sort_workspace_bytes": (sz, [u64, C.POINTER(C.c_int32), i32]),
         "vdf_sort_variant_count": (i32, []),
         "vdf_sort_variant_info": (st, [i32] + [C.POINTER(C.c_int32)] * 5),
+        "vdf_sort_variant_flags": (C.c_uint32, [i32]),
         "vdf_ctx_set_sort_tuning": (st, [vp, C.POINTER(vdf_sort_tuning)]),
         "vdf_ctx_get_sort_tuning": (st, [vp, C.POINTER(vdf_sort_tuning)]),
         "vdf_groupby_workspace_bytes": (sz, [u64, i32]),
@@ -627,13 +628,15 @@ class CsvTable:
 
 
 def sort_variants() -> list:
-    """[{index, key_width, threads, items, digit_bits, match}] of the compiled radix-pass variants."""
+    """[{index, key_width, threads, items, digit_bits, match, tma}] of the compiled radix-pass variants
+    (tma: tiles staged by bulk copies on a persistent grid)."""
     out = []
     for i in range(lib.vdf_sort_variant_count()):
         vals = [C.c_int32() for _ in range(5)]
         if lib.vdf_sort_variant_info(i, *[C.byref(v) for v in vals]) == OK:
             out.append(dict(index=i, key_width=vals[0].value, threads=vals[1].value, items=vals[2].value,
-                            digit_bits=vals[3].value, match=vals[4].value))
+                            digit_bits=vals[3].value, match=vals[4].value,
+                            tma=bool(lib.vdf_sort_variant_flags(i) & 1)))
     return out
 
 

@@ -195,6 +195,8 @@ vdf_status vdf_sort_variant_info(int index, int32_t* key_width, int32_t* threads
     return VDF_OK;
 }
 
+uint32_t vdf_sort_variant_flags(int index) { return vdf::sort_variant_uses_tma(index) ? 1u : 0u; }
+
 vdf_status vdf_ctx_set_sort_tuning(vdf_ctx* c, const vdf_sort_tuning* t) {
     if (!c || !t) return VDF_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);

@@ -109,6 +109,9 @@ struct PassArgs {
     // (seg_flag[segment] != 0) == (seg_flag_when != 0)
     const uint32_t* seg_flag = nullptr;
     uint32_t seg_flag_when = 0;
+    // tiles of the pass (0: one per CTA of the grid); a grid smaller than
+    // that loops, each CTA taking the next tile id until none is left
+    uint32_t ntiles = 0;
 };
 
 
@@ -135,6 +138,7 @@ SortTuning default_sort_tuning();
 bool sort_tuning_valid(const SortTuning& t);
 int sort_variant_count();
 bool sort_variant_info(int i, int* width, int* threads, int* items, int* bits, int* match);
+bool sort_variant_uses_tma(int i);
 
 struct SortPlan {
     uint64_t n;

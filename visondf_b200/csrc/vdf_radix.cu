@@ -257,6 +257,9 @@ struct OnesweepCfg {
     // match method 3: two per-warp words per digit, the lanes holding it
     static constexpr size_t MASK_BYTES = MATCH == 3 ? (size_t)2 * WARPS * RADIX * 4 : 0;
     static constexpr size_t SMEM = KEY_BYTES + VAL_BYTES + CNT_BYTES + GLOB_BYTES + 64 + WARPS * 4 + MASK_BYTES;
+    // the bulk-load variant stages the next tile in a second key / row-id buffer
+    static constexpr size_t SMEM_BULK = SMEM + KEY_BYTES + VAL_BYTES;
+    static_assert(SMEM % 16 == 0 && KEY_BYTES % 16 == 0 && VAL_BYTES % 16 == 0, "bulk copies need 16-byte alignment");
 };
 
 // MATCH selects how a warp finds the lanes holding the same digit:
@@ -271,272 +274,410 @@ struct OnesweepCfg {
 // come from its segment's own histogram, its look-back stops at the
 // segment's first tile, and each segment has its own number of passes (the
 // last one writes to the final buffers, later passes skip its tiles).
+// Each CTA takes tile ids from the pass's counter until none is left, so a
+// grid smaller than the tile count works (a conditional pass not taken then
+// costs one short wave).  Tiles are taken in counter order, so the tile a
+// look-back waits on always belongs to a running CTA.
+// TMA: while a tile is ranked, one thread stages the next tile's keys and
+// row ids into a second shared-memory buffer with a bulk copy behind an
+// mbarrier (full, 16-byte aligned tiles; others load as usual); meant for a
+// persistent grid of a few CTAs per SM.
 template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL, int MATCH, int MINB,
-          bool SEG = false>
+          bool SEG = false, bool TMA = false>
 __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     using C = OnesweepCfg<K, BITS, THREADS, ITEMS, MATCH>;
     constexpr int RADIX = C::RADIX, WARPS = C::WARPS, TILE = C::TILE, BPT = C::BPT;
+    constexpr bool BULK = TMA && !SEG;
     extern __shared__ __align__(16) unsigned char smem[];
-    K* ex_keys = reinterpret_cast<K*>(smem);
-    uint32_t* ex_vals = reinterpret_cast<uint32_t*>(smem + C::KEY_BYTES);
+    K* const kbuf0 = reinterpret_cast<K*>(smem);
+    uint32_t* const vbuf0 = reinterpret_cast<uint32_t*>(smem + C::KEY_BYTES);
     uint32_t* wcnt = reinterpret_cast<uint32_t*>(smem + C::KEY_BYTES + C::VAL_BYTES);  // [WARPS][RADIX]
     uint32_t* bglob = wcnt + WARPS * RADIX;                                            // [RADIX]
-    uint32_t* misc = bglob + RADIX;                                                    // [0]=tile
+    // misc: [2 + (it & 1)] the tile of iteration it, [4 + b] buffer b holds a
+    // bulk-loaded tile, [8..11] the two buffers' mbarriers
+    uint32_t* misc = bglob + RADIX;
     uint32_t* wsum = misc + 16;                                                        // [WARPS]
     uint32_t* wmask = wsum + WARPS;  // match method 3: [2][WARPS][RADIX]
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(misc + 8);
+    K* const kbuf1 = reinterpret_cast<K*>(smem + C::SMEM);
+    uint32_t* const vbuf1 = reinterpret_cast<uint32_t*>(smem + C::SMEM + C::KEY_BYTES);
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // A conditional pass not taken returns before touching anything; the
     // flag was written by an earlier launch, so every thread reads the same.
     if (a.run_flag && ((*a.run_flag != 0) != (a.run_when != 0))) return;
-    if (tid == 0) misc[0] = atomicAdd(a.tile_counter, 1u);
-    for (int i = tid; i < WARPS * RADIX; i += THREADS) wcnt[i] = 0;
-    if constexpr (MATCH == 3)
-        for (int i = tid; i < 2 * WARPS * RADIX; i += THREADS) wmask[i] = 0;
-    __syncthreads();
-    const uint32_t tile = misc[0];
-    // failure injection for tests: this tile's CTA leaves before publishing
-    // anything, so the look-back waits on it run out (bounded, reported)
-    if (tile == a.stall_tile) return;
+    const uint32_t ntiles = a.ntiles ? a.ntiles : gridDim.x;
     const uint32_t spin_limit = a.spin_limit ? a.spin_limit : kSpinLimit;
     const uint64_t n = a.n;
-    uint64_t tile_base = (uint64_t)tile * TILE;
-    uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tile_base);
-    uint32_t first_tile = 0;   // look-back stops here
-    uint32_t seg = 0;
-    uint32_t shift = a.shift;
-    bool fin = FINAL;
-    if constexpr (SEG) {
-        valid = 0;
-        if (tile < a.status_rows) {
-            seg = a.tile_seg[tile];
-            const SegDesc sd = a.segs[seg];
-            // a segment left out by its flag (written by an earlier launch,
-            // so every tile of the segment sees the same) only clears status
-            const bool skip = a.seg_flag && ((a.seg_flag[seg] != 0) != (a.seg_flag_when != 0));
-            if (tile < sd.first_tile || sd.row_start + sd.rows > n ||
-                (uint64_t)(tile - sd.first_tile) * TILE >= sd.rows) {
-                if (tid == 0) atomicOr(a.err, ERR_BAD_INDEX);  // inconsistent tile table
-            } else if (a.pass < sd.passes && !skip) {
-                first_tile = sd.first_tile;
-                shift = (sd.first_digit + a.pass) * BITS;
-                tile_base = sd.row_start + (uint64_t)(tile - sd.first_tile) * TILE;
-                valid = (uint32_t)min((uint64_t)TILE, sd.row_start + sd.rows - tile_base);
-                fin = (a.pass + 1 == sd.passes);
-            }
-        } else if (tid == 0) {
-            atomicOr(a.err, ERR_BAD_INDEX);
-        }
-    }
-
-    // ---- load keys and row ids (warp-striped: item j of lane l is tile
-    //      position warp*ITEMS*32 + j*32 + l, so positions follow row order) --
-    // Every load of the tile is issued before any key is transformed (a
-    // transform between loads keeps the compiler from overlapping them).
-    K key[ITEMS];
-    uint32_t val[ITEMS];
-    const uint32_t wpos = (uint32_t)warp * ITEMS * 32;
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t pos = wpos + j * 32 + lane;
-        const uint64_t i = tile_base + pos;
-        key[j] = ~K(0);
-        val[j] = (uint32_t)i;  // IN_RAW: the row itself
-        if (pos < valid) {
-            if (IN_MODE == IN_RAW) {
-                key[j] = ldg_stream(static_cast<const K*>(a.keys_in) + i);
-            } else if (IN_MODE == IN_GATHER) {
-                uint32_t src = ldg_stream(a.vals_in + i);
-                if (src >= n) {  // never for a valid permutation
-                    atomicOr(a.err, ERR_BAD_INDEX);
-                    src = 0;
-                }
-                val[j] = src;
-            } else {
-                key[j] = ldg_stream(static_cast<const K*>(a.keys_in) + i);
-                val[j] = ldg_stream(a.vals_in + i);
+    // bulk loads (thread 0): the keys (unless read through the permutation)
+    // and row ids (unless the rows themselves) of a full, aligned tile t
+    constexpr bool LOAD_K = IN_MODE != IN_GATHER, LOAD_V = IN_MODE != IN_RAW;
+    auto issue = [&](uint32_t t, int b) {
+        bool ok = false;
+        if (t < ntiles && (uint64_t)(t + 1) * TILE <= n) {
+            const K* ks = LOAD_K ? static_cast<const K*>(a.keys_in) + (uint64_t)t * TILE : nullptr;
+            const uint32_t* vs = LOAD_V ? a.vals_in + (uint64_t)t * TILE : nullptr;
+            ok = (!LOAD_K || (reinterpret_cast<uintptr_t>(ks) & 15) == 0) &&
+                 (!LOAD_V || (reinterpret_cast<uintptr_t>(vs) & 15) == 0);
+            if (ok) {
+                fence_async_smem();  // the buffer's earlier reads come first
+                mbar_expect(&mbar[b], (LOAD_K ? (uint32_t)C::KEY_BYTES : 0u) + (LOAD_V ? (uint32_t)C::VAL_BYTES : 0u));
+                if (LOAD_K) bulk_load(b ? kbuf1 : kbuf0, ks, (uint32_t)C::KEY_BYTES, &mbar[b]);
+                if (LOAD_V) bulk_load(b ? vbuf1 : vbuf0, vs, (uint32_t)C::VAL_BYTES, &mbar[b]);
             }
         }
-    }
-    if constexpr (IN_MODE == IN_GATHER) {
-        // keys through the current permutation: all random loads, then the transform
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j) {
-            if (wpos + j * 32 + lane < valid) {
-                const K* kp = static_cast<const K*>(a.keys_in) + val[j];
-                if constexpr (sizeof(K) == 8) key[j] = ld_rand8(kp);
-                else key[j] = ld_rand4(kp);
-            }
-        }
-    }
-    if constexpr ((IN_MODE == IN_RAW && !SEG) || IN_MODE == IN_GATHER) {
-        // raw keys -> order images (a batch arena already holds images)
-#pragma unroll
-        for (int j = 0; j < ITEMS; ++j)
-            if (wpos + j * 32 + lane < valid) key[j] = KeyOps<K>::order(key[j], a.dtype, a.invert);
-    }
-
-    // Clear this tile's row of the other status buffer for the next pass
-    // (that buffer's previous user, the pass before this one, has finished).
-    // Rows tile, tile + gridDim.x, ... so that every row a later pass with
-    // more tiles could read is cleared too.
-    if (a.status_next) {
-        if (a.status_row_words == RADIX) {  // every pass of the plan has this radix
-            for (uint32_t r = tile; r < a.status_rows; r += gridDim.x)
-                for (int b = tid; b < RADIX; b += THREADS) a.status_next[(size_t)r * RADIX + b] = 0;
-        } else {
-            for (uint32_t r = tile; r < a.status_rows; r += gridDim.x)
-                for (uint32_t b = tid; b < a.status_row_words; b += THREADS)
-                    a.status_next[(size_t)r * a.status_row_words + b] = 0;
-        }
-    }
-    if (SEG && valid == 0) return;  // segment finished in an earlier pass
-
-    // ---- warp-local ranks and per-warp digit counts --------------------------
-    // First the lanes holding the same digit are found for every item (one
-    // ballot per digit bit, or match.any); these are independent and
-    // overlap.  Then the warp's per-digit counters advance item by item (the
-    // lowest lane of each peer group adds the group's size), which is the
-    // only serial part.  Slots past the end of the last tile hold all-ones
-    // keys, whose digit is the largest in every pass: ranked like any key,
-    // they come after every real key of that digit (their positions are
-    // last), so they fill the tile's last slots and are never written out.
-    uint32_t rank[ITEMS];
-    uint32_t peers[ITEMS];
-    uint32_t* my_cnt = wcnt + warp * RADIX;
-    const uint32_t lt = lanemask_lt();
-    // 8-bit digits are computed once and kept four to a register
-    constexpr bool PACKED = (BITS == 8);
-    uint32_t dpk[(ITEMS + 3) / 4];
-#pragma unroll
-    for (int i = 0; i < (ITEMS + 3) / 4; ++i) dpk[i] = 0;
-    auto digit = [&](int j) -> uint32_t {
-        if constexpr (PACKED) return (dpk[j / 4] >> (8 * (j % 4))) & 0xffu;
-        else return digit_of<K, BITS>(key[j], shift);
+        misc[4 + b] = ok ? 1u : 0u;
     };
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t d = digit_of<K, BITS>(key[j], shift);
-        if constexpr (PACKED) dpk[j / 4] |= d << (8 * (j % 4));
-        if constexpr (MATCH == 3) {
-            uint32_t* word = wmask + ((j & 1) * WARPS + warp) * RADIX + d;
-            atomicOr(word, 1u << lane);
-            __syncwarp();
-            const uint32_t pm = *word;
-            __syncwarp();  // every peer has read the word before its leader clears it
-            if (lane == __ffs(pm) - 1) *word = 0;
-            peers[j] = pm;
-        } else if (MATCH == 1 || (MATCH == 2 && (j & 1) == 0)) {
-            peers[j] = __match_any_sync(0xffffffffu, d);
-        } else {
-            uint32_t pm = 0xffffffffu;
-#pragma unroll
-            for (int b = 0; b < BITS; ++b) {
-                const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
-                pm &= ((d >> b) & 1u) ? bal : ~bal;
-            }
-            peers[j] = pm;
+    if (tid == 0) {
+        if constexpr (BULK) {
+            mbar_init(&mbar[0], 1);
+            mbar_init(&mbar[1], 1);
+            mbar_init_fence();
         }
+        misc[2] = atomicAdd(a.tile_counter, 1u);
+        if constexpr (BULK) issue(misc[2], 0);
     }
-    // The leader's add returns before the full-warp shuffle that hands its
-    // result out, and the next item's add comes after that shuffle, so the
-    // items' adds on a counter happen in item order (stable ranks).
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t d = digit(j);
-        const int leader = __ffs(peers[j]) - 1;
-        uint32_t base = 0;
-        if (lane == leader) base = atomicAdd(&my_cnt[d], (uint32_t)__popc(peers[j]));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        rank[j] = base + __popc(peers[j] & lt);
-    }
-    __syncthreads();
+    uint32_t phase = 0;  // bit b: parity of buffer b's next completed load
+    uint32_t lost = 0;   // bit b: a load into buffer b that a wait gave up on
+    for (uint32_t it = 0;; ++it) {
+        const int cb = BULK ? (int)(it & 1) : 0;  // this tile's buffer
+        K* const ex_keys = cb ? kbuf1 : kbuf0;
+        uint32_t* const ex_vals = cb ? vbuf1 : vbuf0;
+        uint32_t* const next_slot = misc + 2 + ((it + 1) & 1);
+        // this thread's accesses to the buffers come before the bulk copies
+        // into them that follow the barrier below
+        if constexpr (BULK) fence_async_smem();
+        for (int i = tid; i < WARPS * RADIX; i += THREADS) wcnt[i] = 0;
+        if constexpr (MATCH == 3)
+            for (int i = tid; i < 2 * WARPS * RADIX; i += THREADS) wmask[i] = 0;
+        __syncthreads();
+        const uint32_t tile = misc[2 + (it & 1)];
+        if (tile >= ntiles) break;
+        const bool bulk = BULK && misc[4 + cb] != 0;
+        if constexpr (BULK) {
+            if (tid == 0) {  // the next tile, so that its load overlaps this one
+                *next_slot = atomicAdd(a.tile_counter, 1u);
+                issue(*next_slot, cb ^ 1);
+            }
+            if (bulk) {
+                if (!mbar_wait(&mbar[cb], (phase >> cb) & 1u, spin_limit)) {
+                    lost |= 1u << cb;
+                    if (tid == 0) atomicOr(a.err, ERR_LOOKBACK_TIMEOUT);
+                }
+                phase ^= 1u << cb;
+            }
+        }
+        // failure injection for tests: this tile publishes nothing, so the
+        // look-back waits on it run out (bounded, reported)
+        if (tile == a.stall_tile) {
+            if (!BULK && tid == 0) *next_slot = atomicAdd(a.tile_counter, 1u);
+            continue;
+        }
+        uint64_t tile_base = (uint64_t)tile * TILE;
+        uint32_t valid = (uint32_t)min((uint64_t)TILE, n - tile_base);
+        uint32_t first_tile = 0;   // look-back stops here
+        uint32_t seg = 0;
+        uint32_t shift = a.shift;
+        bool fin = FINAL;
+        if constexpr (SEG) {
+            valid = 0;
+            if (tile < a.status_rows) {
+                seg = a.tile_seg[tile];
+                const SegDesc sd = a.segs[seg];
+                // a segment left out by its flag (written by an earlier launch,
+                // so every tile of the segment sees the same) only clears status
+                const bool skip = a.seg_flag && ((a.seg_flag[seg] != 0) != (a.seg_flag_when != 0));
+                if (tile < sd.first_tile || sd.row_start + sd.rows > n ||
+                    (uint64_t)(tile - sd.first_tile) * TILE >= sd.rows) {
+                    if (tid == 0) atomicOr(a.err, ERR_BAD_INDEX);  // inconsistent tile table
+                } else if (a.pass < sd.passes && !skip) {
+                    first_tile = sd.first_tile;
+                    shift = (sd.first_digit + a.pass) * BITS;
+                    tile_base = sd.row_start + (uint64_t)(tile - sd.first_tile) * TILE;
+                    valid = (uint32_t)min((uint64_t)TILE, sd.row_start + sd.rows - tile_base);
+                    fin = (a.pass + 1 == sd.passes);
+                }
+            } else if (tid == 0) {
+                atomicOr(a.err, ERR_BAD_INDEX);
+            }
+        }
 
-    // ---- per-bin totals, early publish, tile-local bin starts --------------
-    uint32_t tot[BPT];
-    uint32_t tsum = 0;
-#pragma unroll
-    for (int k = 0; k < BPT; ++k) {
-        const int b = tid * BPT + k;
-        uint32_t run = 0;
-        if (b < RADIX) {
-#pragma unroll
-            for (int w = 0; w < WARPS; ++w) {
-                uint32_t c = wcnt[w * RADIX + b];
-                wcnt[w * RADIX + b] = run;
-                run += c;
+        // ---- load keys and row ids (warp-striped: item j of lane l is tile
+        //      position warp*ITEMS*32 + j*32 + l, so positions follow row order) --
+        // Every load of the tile is issued before any key is transformed (a
+        // transform between loads keeps the compiler from overlapping them).
+        K key[ITEMS];
+        uint32_t val[ITEMS];
+        const uint32_t wpos = (uint32_t)warp * ITEMS * 32;
+        if (bulk) {  // a full tile, staged in shared memory
+    #pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                const uint32_t pos = wpos + j * 32 + lane;
+                key[j] = LOAD_K ? ex_keys[pos] : ~K(0);
+                val[j] = LOAD_V ? ex_vals[pos] : (uint32_t)(tile_base + pos);
+                if (IN_MODE == IN_GATHER && val[j] >= n) {  // never for a valid permutation
+                    atomicOr(a.err, ERR_BAD_INDEX);
+                    val[j] = 0;
+                }
             }
-            uint32_t* st = a.status + (size_t)tile * RADIX + b;
-            st_relaxed_u32(st, (tile == first_tile ? ST_INC : ST_AGG) | run);
+        } else
+    #pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t pos = wpos + j * 32 + lane;
+            const uint64_t i = tile_base + pos;
+            key[j] = ~K(0);
+            val[j] = (uint32_t)i;  // IN_RAW: the row itself
+            if (pos < valid) {
+                if (IN_MODE == IN_RAW) {
+                    key[j] = ldg_stream(static_cast<const K*>(a.keys_in) + i);
+                } else if (IN_MODE == IN_GATHER) {
+                    uint32_t src = ldg_stream(a.vals_in + i);
+                    if (src >= n) {  // never for a valid permutation
+                        atomicOr(a.err, ERR_BAD_INDEX);
+                        src = 0;
+                    }
+                    val[j] = src;
+                } else {
+                    key[j] = ldg_stream(static_cast<const K*>(a.keys_in) + i);
+                    val[j] = ldg_stream(a.vals_in + i);
+                }
+            }
         }
-        tot[k] = run;
-        tsum += run;
-    }
-    // block exclusive scan of tsum over threads (bins are blocked per thread)
-    uint32_t incl = tsum;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
-        if (lane >= d) incl += t;
-    }
-    if (lane == 31) wsum[warp] = incl;
-    __syncthreads();
-    uint32_t wb = 0;
-#pragma unroll
-    for (int w = 0; w < WARPS; ++w) wb += (w < warp) ? wsum[w] : 0u;
-    uint32_t bstart[BPT];
-    {
-        uint32_t run = wb + incl - tsum;
-#pragma unroll
+        if constexpr (IN_MODE == IN_GATHER) {
+            // keys through the current permutation: all random loads, then the transform
+    #pragma unroll
+            for (int j = 0; j < ITEMS; ++j) {
+                if (wpos + j * 32 + lane < valid) {
+                    const K* kp = static_cast<const K*>(a.keys_in) + val[j];
+                    if constexpr (sizeof(K) == 8) key[j] = ld_rand8(kp);
+                    else key[j] = ld_rand4(kp);
+                }
+            }
+        }
+        if constexpr ((IN_MODE == IN_RAW && !SEG) || IN_MODE == IN_GATHER) {
+            // raw keys -> order images (a batch arena already holds images)
+    #pragma unroll
+            for (int j = 0; j < ITEMS; ++j)
+                if (wpos + j * 32 + lane < valid) key[j] = KeyOps<K>::order(key[j], a.dtype, a.invert);
+        }
+
+        // Clear this tile's row of the other status buffer for the next pass
+        // (that buffer's previous user, the pass before this one, has finished).
+        // Rows tile, tile + gridDim.x, ... so that every row a later pass with
+        // more tiles could read is cleared too.
+        if (a.status_next) {
+            if (a.status_row_words == RADIX) {  // every pass of the plan has this radix
+                for (uint32_t r = tile; r < a.status_rows; r += ntiles)
+                    for (int b = tid; b < RADIX; b += THREADS) a.status_next[(size_t)r * RADIX + b] = 0;
+            } else {
+                for (uint32_t r = tile; r < a.status_rows; r += ntiles)
+                    for (uint32_t b = tid; b < a.status_row_words; b += THREADS)
+                        a.status_next[(size_t)r * a.status_row_words + b] = 0;
+            }
+        }
+        if (SEG && valid == 0) {  // segment finished in an earlier pass, or left out
+            if (!BULK && tid == 0) *next_slot = atomicAdd(a.tile_counter, 1u);
+            continue;
+        }
+
+        // ---- warp-local ranks and per-warp digit counts --------------------------
+        // First the lanes holding the same digit are found for every item (one
+        // ballot per digit bit, or match.any); these are independent and
+        // overlap.  Then the warp's per-digit counters advance item by item (the
+        // lowest lane of each peer group adds the group's size), which is the
+        // only serial part.  Slots past the end of the last tile hold all-ones
+        // keys, whose digit is the largest in every pass: ranked like any key,
+        // they come after every real key of that digit (their positions are
+        // last), so they fill the tile's last slots and are never written out.
+        uint32_t rank[ITEMS];
+        uint32_t peers[ITEMS];
+        uint32_t* my_cnt = wcnt + warp * RADIX;
+        const uint32_t lt = lanemask_lt();
+        // 8-bit digits are computed once and kept four to a register
+        constexpr bool PACKED = (BITS == 8);
+        uint32_t dpk[(ITEMS + 3) / 4];
+    #pragma unroll
+        for (int i = 0; i < (ITEMS + 3) / 4; ++i) dpk[i] = 0;
+        auto digit = [&](int j) -> uint32_t {
+            if constexpr (PACKED) return (dpk[j / 4] >> (8 * (j % 4))) & 0xffu;
+            else return digit_of<K, BITS>(key[j], shift);
+        };
+    #pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t d = digit_of<K, BITS>(key[j], shift);
+            if constexpr (PACKED) dpk[j / 4] |= d << (8 * (j % 4));
+            if constexpr (MATCH == 3) {
+                uint32_t* word = wmask + ((j & 1) * WARPS + warp) * RADIX + d;
+                atomicOr(word, 1u << lane);
+                __syncwarp();
+                const uint32_t pm = *word;
+                __syncwarp();  // every peer has read the word before its leader clears it
+                if (lane == __ffs(pm) - 1) *word = 0;
+                peers[j] = pm;
+            } else if (MATCH == 1 || (MATCH == 2 && (j & 1) == 0)) {
+                peers[j] = __match_any_sync(0xffffffffu, d);
+            } else {
+                uint32_t pm = 0xffffffffu;
+    #pragma unroll
+                for (int b = 0; b < BITS; ++b) {
+                    const uint32_t bal = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+                    pm &= ((d >> b) & 1u) ? bal : ~bal;
+                }
+                peers[j] = pm;
+            }
+        }
+        // The leader's add returns before the full-warp shuffle that hands its
+        // result out, and the next item's add comes after that shuffle, so the
+        // items' adds on a counter happen in item order (stable ranks).
+    #pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t d = digit(j);
+            const int leader = __ffs(peers[j]) - 1;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(&my_cnt[d], (uint32_t)__popc(peers[j]));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            rank[j] = base + __popc(peers[j] & lt);
+        }
+        __syncthreads();
+
+        // ---- per-bin totals, early publish, tile-local bin starts --------------
+        uint32_t tot[BPT];
+        uint32_t tsum = 0;
+    #pragma unroll
         for (int k = 0; k < BPT; ++k) {
-            bstart[k] = run;
-            run += tot[k];
             const int b = tid * BPT + k;
-            if (b < RADIX)
-#pragma unroll
-                for (int w = 0; w < WARPS; ++w) wcnt[w * RADIX + b] += bstart[k];
+            uint32_t run = 0;
+            if (b < RADIX) {
+    #pragma unroll
+                for (int w = 0; w < WARPS; ++w) {
+                    uint32_t c = wcnt[w * RADIX + b];
+                    wcnt[w * RADIX + b] = run;
+                    run += c;
+                }
+                uint32_t* st = a.status + (size_t)tile * RADIX + b;
+                st_relaxed_u32(st, (tile == first_tile ? ST_INC : ST_AGG) | run);
+            }
+            tot[k] = run;
+            tsum += run;
         }
-    }
-    __syncthreads();
-
-    // ---- tile-local ranks; keys and row ids into shared memory --------------
-    // (overlaps the look-back below: other warps' global writes wait on it)
-#pragma unroll
-    for (int j = 0; j < ITEMS; ++j) {
-        const uint32_t d = digit(j);
-        uint32_t r = rank[j] + wcnt[warp * RADIX + d];
-        if (r >= (uint32_t)TILE) {  // never when the counts are consistent
-            atomicOr(a.err, ERR_BAD_INDEX);
-            r = wpos + j * 32 + lane;
+        // block exclusive scan of tsum over threads (bins are blocked per thread)
+        uint32_t incl = tsum;
+    #pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            uint32_t t = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= d) incl += t;
         }
-        ex_keys[r] = key[j];
-        ex_vals[r] = val[j];
-    }
+        if (lane == 31) wsum[warp] = incl;
+        __syncthreads();
+        uint32_t wb = 0;
+    #pragma unroll
+        for (int w = 0; w < WARPS; ++w) wb += (w < warp) ? wsum[w] : 0u;
+        uint32_t bstart[BPT];
+        {
+            uint32_t run = wb + incl - tsum;
+    #pragma unroll
+            for (int k = 0; k < BPT; ++k) {
+                bstart[k] = run;
+                run += tot[k];
+                const int b = tid * BPT + k;
+                if (b < RADIX)
+    #pragma unroll
+                    for (int w = 0; w < WARPS; ++w) wcnt[w * RADIX + b] += bstart[k];
+            }
+        }
+        __syncthreads();
 
-    // ---- decoupled look-back per bin ---------------------------------------
-    // Each bin's thread reads the status words of LB predecessors at once (one
-    // round trip per window), adds counts from the nearest one backwards and
-    // stops at the first inclusive prefix.  A thread owning several bins (wide
-    // digits) issues the windows of all its unfinished bins together.
-    const int64_t lo = first_tile;
-    if constexpr (BPT == 1) {
-        constexpr int LB = 8;
-        const int b = tid;
-        if (b < RADIX) {
-            uint32_t excl = 0;
-            if (tile > first_tile) {
-                int64_t p = (int64_t)tile - 1;
-                uint32_t spins = 0;
-                bool done = false;
-                while (!done) {
-                    uint32_t sw[LB];
-#pragma unroll
+        // ---- tile-local ranks; keys and row ids into shared memory --------------
+        // (overlaps the look-back below: other warps' global writes wait on it)
+    #pragma unroll
+        for (int j = 0; j < ITEMS; ++j) {
+            const uint32_t d = digit(j);
+            uint32_t r = rank[j] + wcnt[warp * RADIX + d];
+            if (r >= (uint32_t)TILE) {  // never when the counts are consistent
+                atomicOr(a.err, ERR_BAD_INDEX);
+                r = wpos + j * 32 + lane;
+            }
+            ex_keys[r] = key[j];
+            ex_vals[r] = val[j];
+        }
+
+        // ---- decoupled look-back per bin ---------------------------------------
+        // Each bin's thread reads the status words of LB predecessors at once (one
+        // round trip per window), adds counts from the nearest one backwards and
+        // stops at the first inclusive prefix.  A thread owning several bins (wide
+        // digits) issues the windows of all its unfinished bins together.
+        const int64_t lo = first_tile;
+        if constexpr (BPT == 1) {
+            constexpr int LB = 8;
+            const int b = tid;
+            if (b < RADIX) {
+                uint32_t excl = 0;
+                if (tile > first_tile) {
+                    int64_t p = (int64_t)tile - 1;
+                    uint32_t spins = 0;
+                    bool done = false;
+                    while (!done) {
+                        uint32_t sw[LB];
+    #pragma unroll
+                        for (int w = 0; w < LB; ++w)
+                            sw[w] = (p - w >= lo) ? ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b) : ST_INC;
+    #pragma unroll
+                        for (int w = 0; w < LB; ++w) {
+                            if (done) break;
+                            uint32_t st = sw[w];
+                            while ((st & ~ST_CNT) == 0) {  // not yet published: wait for this one
+                                if (++spins > spin_limit) {
+                                    atomicOr(a.err, ERR_LOOKBACK_TIMEOUT);
+                                    st = ST_INC;
+                                    break;
+                                }
+                                backoff(spins);
+                                st = ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b);
+                            }
+                            excl += st & ST_CNT;
+                            if (st & ST_INC) done = true;
+                        }
+                        p -= LB;
+                        if (p < lo) done = true;
+                    }
+                    st_relaxed_u32(a.status + (size_t)tile * RADIX + b, ST_INC | (excl + tot[0]));
+                }
+                uint32_t base;
+                if constexpr (SEG)
+                    base = (uint32_t)a.segs[seg].row_start + a.seg_offs[(size_t)seg * a.seg_stride + a.pass * RADIX + b];
+                else
+                    base = a.bin_offsets[b];
+                bglob[b] = base + excl - bstart[0];
+            }
+        } else {
+            constexpr int LB = (BPT >= 8) ? 2 : 4;
+            uint32_t excl[BPT];
+            bool done[BPT];
+    #pragma unroll
+            for (int k = 0; k < BPT; ++k) {
+                excl[k] = 0;
+                done[k] = (tile == first_tile) || (tid * BPT + k >= RADIX);
+            }
+            int64_t p = (int64_t)tile - 1;
+            uint32_t spins = 0;
+            bool all_done = false;
+            while (!all_done) {
+                uint32_t sw[BPT][LB];
+    #pragma unroll
+                for (int k = 0; k < BPT; ++k)
+    #pragma unroll
                     for (int w = 0; w < LB; ++w)
-                        sw[w] = (p - w >= lo) ? ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b) : ST_INC;
-#pragma unroll
+                        sw[k][w] = (!done[k] && p - w >= lo)
+                                       ? ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + tid * BPT + k)
+                                       : ST_INC;
+                all_done = true;
+    #pragma unroll
+                for (int k = 0; k < BPT; ++k) {
+                    if (done[k]) continue;
+    #pragma unroll
                     for (int w = 0; w < LB; ++w) {
-                        if (done) break;
-                        uint32_t st = sw[w];
+                        if (done[k]) break;
+                        uint32_t st = sw[k][w];
                         while ((st & ~ST_CNT) == 0) {  // not yet published: wait for this one
                             if (++spins > spin_limit) {
                                 atomicOr(a.err, ERR_LOOKBACK_TIMEOUT);
@@ -544,113 +685,68 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
                                 break;
                             }
                             backoff(spins);
-                            st = ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + b);
+                            st = ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + tid * BPT + k);
                         }
-                        excl += st & ST_CNT;
-                        if (st & ST_INC) done = true;
+                        excl[k] += st & ST_CNT;
+                        if (st & ST_INC) done[k] = true;
                     }
-                    p -= LB;
-                    if (p < lo) done = true;
+                    if (p - LB < lo) done[k] = true;
+                    all_done = all_done && done[k];
                 }
-                st_relaxed_u32(a.status + (size_t)tile * RADIX + b, ST_INC | (excl + tot[0]));
+                p -= LB;
             }
-            uint32_t base;
-            if constexpr (SEG)
-                base = (uint32_t)a.segs[seg].row_start + a.seg_offs[(size_t)seg * a.seg_stride + a.pass * RADIX + b];
-            else
-                base = a.bin_offsets[b];
-            bglob[b] = base + excl - bstart[0];
-        }
-    } else {
-        constexpr int LB = (BPT >= 8) ? 2 : 4;
-        uint32_t excl[BPT];
-        bool done[BPT];
-#pragma unroll
-        for (int k = 0; k < BPT; ++k) {
-            excl[k] = 0;
-            done[k] = (tile == first_tile) || (tid * BPT + k >= RADIX);
-        }
-        int64_t p = (int64_t)tile - 1;
-        uint32_t spins = 0;
-        bool all_done = false;
-        while (!all_done) {
-            uint32_t sw[BPT][LB];
-#pragma unroll
-            for (int k = 0; k < BPT; ++k)
-#pragma unroll
-                for (int w = 0; w < LB; ++w)
-                    sw[k][w] = (!done[k] && p - w >= lo)
-                                   ? ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + tid * BPT + k)
-                                   : ST_INC;
-            all_done = true;
-#pragma unroll
+    #pragma unroll
             for (int k = 0; k < BPT; ++k) {
-                if (done[k]) continue;
-#pragma unroll
-                for (int w = 0; w < LB; ++w) {
-                    if (done[k]) break;
-                    uint32_t st = sw[k][w];
-                    while ((st & ~ST_CNT) == 0) {  // not yet published: wait for this one
-                        if (++spins > spin_limit) {
-                            atomicOr(a.err, ERR_LOOKBACK_TIMEOUT);
-                            st = ST_INC;
-                            break;
-                        }
-                        backoff(spins);
-                        st = ld_relaxed_u32(a.status + (size_t)(p - w) * RADIX + tid * BPT + k);
-                    }
-                    excl[k] += st & ST_CNT;
-                    if (st & ST_INC) done[k] = true;
-                }
-                if (p - LB < lo) done[k] = true;
-                all_done = all_done && done[k];
+                const int b = tid * BPT + k;
+                if (b >= RADIX) break;
+                if (tile > first_tile) st_relaxed_u32(a.status + (size_t)tile * RADIX + b, ST_INC | (excl[k] + tot[k]));
+                uint32_t base;
+                if constexpr (SEG)
+                    base = (uint32_t)a.segs[seg].row_start + a.seg_offs[(size_t)seg * a.seg_stride + a.pass * RADIX + b];
+                else
+                    base = a.bin_offsets[b];
+                bglob[b] = base + excl[k] - bstart[k];
             }
-            p -= LB;
         }
-#pragma unroll
-        for (int k = 0; k < BPT; ++k) {
-            const int b = tid * BPT + k;
-            if (b >= RADIX) break;
-            if (tile > first_tile) st_relaxed_u32(a.status + (size_t)tile * RADIX + b, ST_INC | (excl[k] + tot[k]));
-            uint32_t base;
-            if constexpr (SEG)
-                base = (uint32_t)a.segs[seg].row_start + a.seg_offs[(size_t)seg * a.seg_stride + a.pass * RADIX + b];
-            else
-                base = a.bin_offsets[b];
-            bglob[b] = base + excl[k] - bstart[k];
-        }
-    }
-    __syncthreads();
+        __syncthreads();
 
-    // ---- run-coalesced writes of keys and row ids ----------------------------
-    K* kout = static_cast<K*>((SEG && fin) ? a.keys_final : a.keys_out);
-    uint32_t* vout = (SEG && fin) ? a.vals_final : a.vals_out;
-#pragma unroll
-    for (int r = 0; r < ITEMS; ++r) {
-        const uint32_t i = r * THREADS + tid;
-        if (i < valid) {
-            const K k = ex_keys[i];
-            const uint32_t v = ex_vals[i];
-            const uint32_t d = digit_of<K, BITS>(k, shift);
-            uint32_t p = bglob[d] + i;
-            if (p >= n) {  // only after a look-back timeout: never write out of bounds
-                atomicOr(a.err, ERR_BAD_INDEX);
-                continue;
-            }
-            if constexpr (SEG) {
-                // a batch arena holds order images sorted ascending: the final
-                // pass differs from the others only in its output buffers
-                stg_stream(kout + p, k);
-            } else {
-                if (fin && a.reverse) p = (uint32_t)(n - 1) - p;
-                if (fin) {
-                    if (kout) stg_stream(kout + p, KeyOps<K>::unorder(k, a.dtype, a.invert));
-                } else {
-                    stg_stream(kout + p, k);
+        // ---- run-coalesced writes of keys and row ids ----------------------------
+        K* kout = static_cast<K*>((SEG && fin) ? a.keys_final : a.keys_out);
+        uint32_t* vout = (SEG && fin) ? a.vals_final : a.vals_out;
+    #pragma unroll
+        for (int r = 0; r < ITEMS; ++r) {
+            const uint32_t i = r * THREADS + tid;
+            if (i < valid) {
+                const K k = ex_keys[i];
+                const uint32_t v = ex_vals[i];
+                const uint32_t d = digit_of<K, BITS>(k, shift);
+                uint32_t p = bglob[d] + i;
+                if (p >= n) {  // only after a look-back timeout: never write out of bounds
+                    atomicOr(a.err, ERR_BAD_INDEX);
+                    continue;
                 }
+                if constexpr (SEG) {
+                    // a batch arena holds order images sorted ascending: the final
+                    // pass differs from the others only in its output buffers
+                    stg_stream(kout + p, k);
+                } else {
+                    if (fin && a.reverse) p = (uint32_t)(n - 1) - p;
+                    if (fin) {
+                        if (kout) stg_stream(kout + p, KeyOps<K>::unorder(k, a.dtype, a.invert));
+                    } else {
+                        stg_stream(kout + p, k);
+                    }
+                }
+                stg_stream(vout + p, v);
             }
-            stg_stream(vout + p, v);
         }
+        if (!BULK && tid == 0) *next_slot = atomicAdd(a.tile_counter, 1u);
+    }  // tiles
+    if constexpr (BULK) {
+        // a load a wait gave up on must land before the CTA's shared memory
+        // is handed on (bounded again; an error is already recorded)
+        for (int b = 0; b < 2; ++b)
+            if (lost & (1u << b)) mbar_wait(&mbar[b], ((phase >> b) & 1u) ^ 1u, spin_limit);
     }
 }
 
@@ -662,13 +758,15 @@ using PassKernel = void (*)(PassArgs);
 
 // One compiled configuration of the radix pass.  The variant table is the
 // autotuner's search space; a context selects one variant per key width.
+// tma: tiles staged by bulk copies, on a persistent grid of `resident` CTAs
+// per SM (found with the occupancy calculator when the kernels are prepared).
 struct PassVariant {
-    int width, threads, items, bits, match, minb;
+    int width, threads, items, bits, match, minb, tma;
     size_t smem;
     PassKernel k[3][2];  // [IN_MODE][FINAL]
 };
 
-template <typename K, int BITS, int THREADS, int ITEMS, int MATCH, int MINB>
+template <typename K, int BITS, int THREADS, int ITEMS, int MATCH, int MINB, bool TMA = false>
 PassVariant make_variant() {
     using C = OnesweepCfg<K, BITS, THREADS, ITEMS, MATCH>;
     static_assert(BITS <= kMaxBits, "digit wider than the histogram layout allows");
@@ -679,13 +777,14 @@ PassVariant make_variant() {
     v.bits = BITS;
     v.match = MATCH;
     v.minb = MINB;
-    v.smem = C::SMEM;
-    v.k[IN_RAW][0] = k_onesweep<K, BITS, THREADS, ITEMS, IN_RAW, false, MATCH, MINB>;
-    v.k[IN_GATHER][0] = k_onesweep<K, BITS, THREADS, ITEMS, IN_GATHER, false, MATCH, MINB>;
-    v.k[IN_BUF][0] = k_onesweep<K, BITS, THREADS, ITEMS, IN_BUF, false, MATCH, MINB>;
-    v.k[IN_RAW][1] = k_onesweep<K, BITS, THREADS, ITEMS, IN_RAW, true, MATCH, MINB>;
-    v.k[IN_GATHER][1] = k_onesweep<K, BITS, THREADS, ITEMS, IN_GATHER, true, MATCH, MINB>;
-    v.k[IN_BUF][1] = k_onesweep<K, BITS, THREADS, ITEMS, IN_BUF, true, MATCH, MINB>;
+    v.tma = TMA ? 1 : 0;
+    v.smem = TMA ? C::SMEM_BULK : C::SMEM;
+    v.k[IN_RAW][0] = k_onesweep<K, BITS, THREADS, ITEMS, IN_RAW, false, MATCH, MINB, false, TMA>;
+    v.k[IN_GATHER][0] = k_onesweep<K, BITS, THREADS, ITEMS, IN_GATHER, false, MATCH, MINB, false, TMA>;
+    v.k[IN_BUF][0] = k_onesweep<K, BITS, THREADS, ITEMS, IN_BUF, false, MATCH, MINB, false, TMA>;
+    v.k[IN_RAW][1] = k_onesweep<K, BITS, THREADS, ITEMS, IN_RAW, true, MATCH, MINB, false, TMA>;
+    v.k[IN_GATHER][1] = k_onesweep<K, BITS, THREADS, ITEMS, IN_GATHER, true, MATCH, MINB, false, TMA>;
+    v.k[IN_BUF][1] = k_onesweep<K, BITS, THREADS, ITEMS, IN_BUF, true, MATCH, MINB, false, TMA>;
     return v;
 }
 
@@ -714,8 +813,26 @@ const PassVariant kVariants[] = {
     // grows when many lanes share a digit, so it is the autotuner's pick for
     // a workload rather than the default
     make_variant<uint64_t, 8, 256, 12, 3, 3>(),   // 18
+    // tiles staged in shared memory by bulk copies, the next tile's copy
+    // overlapping the current tile's ranking (persistent grid)
+    make_variant<uint64_t, 8, 256, 12, 0, 2, true>(),  // 19
+    make_variant<uint64_t, 8, 256, 12, 2, 2, true>(),  // 20
+    make_variant<uint32_t, 8, 256, 16, 1, 2, true>(),  // 21
+    make_variant<uint32_t, 8, 256, 16, 2, 2, true>(),  // 22
 };
 constexpr int kNumVariants = (int)(sizeof(kVariants) / sizeof(kVariants[0]));
+// resident CTAs per SM of each variant's kernels (the fewest over its six)
+int g_resident[kNumVariants];
+int g_seg_resident[16][2];
+int g_sms = 0;
+
+// Grid of a radix pass over `tiles` tiles: one CTA per tile, or (persistent:
+// bulk-load variants, and conditional passes, which usually return at once)
+// as many CTAs as fit on the GPU, each looping over tiles.
+uint32_t pass_grid(uint32_t tiles, int resident, bool persistent) {
+    if (!persistent || g_sms <= 0 || resident <= 0) return tiles;
+    return (uint32_t)std::min<uint64_t>(tiles, (uint64_t)g_sms * (uint64_t)resident);
+}
 
 // Segmented sorts run over ordered key images of 8 or 4 bytes; k[w][m]: w = 1
 // for 8-byte images, m = 0 for the first pass (arena rows), 1 for later
@@ -754,11 +871,14 @@ const PassVariant& variant_for(const SortTuning& t, int width) {
     const int v = (width == 4) ? t.variant32 : t.variant64;
     return kVariants[v];
 }
+int resident_of(const PassVariant& v) { return g_resident[&v - kVariants]; }
 
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 }  // namespace
 
 int sort_variant_count() { return kNumVariants; }
+
+bool sort_variant_uses_tma(int i) { return i >= 0 && i < kNumVariants && kVariants[i].tma != 0; }
 
 bool sort_variant_info(int i, int* width, int* threads, int* items, int* bits, int* match) {
     if (i < 0 || i >= kNumVariants) return false;
@@ -996,8 +1116,12 @@ cudaError_t run_lsd(const SortPlan& p, const void* const* key_cols, int order, u
             // conditional passes (the MSD plan's fallback) are timed apart
             // from the passes that always run
             const int cls = run_flag ? KC_FALLBACK : (w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64);
+            // a fallback pass usually returns at once: a persistent grid
+            // makes that one short wave
+            a.ntiles = tiles;
+            const uint32_t grid = pass_grid(tiles, resident_of(var), var.tma || run_flag != nullptr);
             if (prof) prof->begin(cls, s);
-            var.k[mode][fin ? 1 : 0]<<<tiles, var.threads, var.smem, s>>>(a);
+            var.k[mode][fin ? 1 : 0]<<<grid, var.threads, var.smem, s>>>(a);
             e = cudaGetLastError();
             if (prof) prof->end(cls, s);
             if (e != cudaSuccess) return e;
@@ -1072,8 +1196,9 @@ cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, u
         }
         a.keys_out = kbuf[q & 1];
         a.vals_out = vbuf[q & 1];
+        a.ntiles = tiles;
         if (prof) prof->begin(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
-        var.k[mode][0]<<<tiles, var.threads, var.smem, s>>>(a);
+        var.k[mode][0]<<<pass_grid(tiles, resident_of(var), var.tma != 0), var.threads, var.smem, s>>>(a);
         e = cudaGetLastError();
         if (prof) prof->end(w == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64, s);
         if (e != cudaSuccess) return e;
@@ -1224,9 +1349,12 @@ cudaError_t run_seg_sort(const SegSortArgs& sa, unsigned char* ws, cudaStream_t 
         a.vals_final = sa.perm_out;
         a.seg_flag = sa.seg_flag;
         a.seg_flag_when = 1;
+        // passes over flagged segments only (usually a few): a persistent grid
+        a.ntiles = grid;
+        const uint32_t launch = pass_grid(grid, g_seg_resident[sa.variant][wi], sa.seg_flag != nullptr);
         const int cls = wi ? KC_ONESWEEP64 : KC_ONESWEEP32;
         if (prof) prof->begin(cls, s);
-        var.k[wi][g == 0 ? 0 : 1]<<<grid, 256, var.smem[wi], s>>>(a);
+        var.k[wi][g == 0 ? 0 : 1]<<<launch, 256, var.smem[wi], s>>>(a);
         e = cudaGetLastError();
         if (prof) prof->end(cls, s);
         if (e != cudaSuccess) return e;
@@ -1279,19 +1407,41 @@ cudaError_t flag_adjacent_ties(const void* sorted_keys, int width, uint64_t n, u
 // Raises the dynamic shared-memory limit of every sort kernel on the current
 // device; called once per device before the first sort.
 cudaError_t prepare_sort_kernels() {
-    for (const PassVariant& v : kVariants)
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaError_t e0 = cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e0 != cudaSuccess) return e0;
+    for (int i = 0; i < kNumVariants; ++i) {
+        const PassVariant& v = kVariants[i];
+        int res = 1 << 30;
         for (int m = 0; m < 3; ++m)
             for (int f = 0; f < 2; ++f) {
                 cudaError_t e = cudaFuncSetAttribute(v.k[m][f], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
                 if (e != cudaSuccess) return e;
+                int nb = 0;
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, v.k[m][f], v.threads, v.smem);
+                if (e != cudaSuccess) return e;
+                res = std::min(res, nb);
             }
-    for (const SegVariant& v : kSegVariants)
-        for (int w = 0; w < 2; ++w)
+        g_resident[i] = std::max(res, 1);
+    }
+    static_assert(kNumSegVariants <= 16, "residency table");
+    for (int i = 0; i < kNumSegVariants; ++i) {
+        const SegVariant& v = kSegVariants[i];
+        for (int w = 0; w < 2; ++w) {
+            int res = 1 << 30;
             for (int m = 0; m < 2; ++m) {
                 cudaError_t e =
                     cudaFuncSetAttribute(v.k[w][m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem[w]);
                 if (e != cudaSuccess) return e;
+                int nb = 0;
+                e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, v.k[w][m], 256, v.smem[w]);
+                if (e != cudaSuccess) return e;
+                res = std::min(res, nb);
             }
+            g_seg_resident[i][w] = std::max(res, 1);
+        }
+    }
     {
         cudaError_t e = cudaFuncSetAttribute(k_seg_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              8 * kMaxRadix * 4);
