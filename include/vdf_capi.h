@@ -308,6 +308,33 @@ vdf_status vdf_groupby_sorted(vdf_ctx* ctx, uint64_t n, const vdf_col* keys, int
                               uint32_t* row_group_out, uint64_t* n_groups_dev, uint64_t* n_groups_host,
                               void* stream);
 
+/* ---- pivot ------------------------------------------------------------------ */
+/* A string column: bytes, and n + 1 offsets (row r = bytes[offsets[r] ..
+ * offsets[r + 1]), offsets[0] = 0). */
+typedef struct vdf_strcol {
+    const char* bytes;
+    const uint64_t* offsets;
+} vdf_strcol;
+/* Pivot (replaces V/pivots/pivot.hpp:5-128): the sum of `value` over the
+ * rows of each (col key, row key) pair, as a matrix with one column per
+ * distinct col key and one row per distinct row key, both in order of first
+ * appearance; a pair that never occurs is 0.  Keys compare by their bytes.
+ * value: VDF_I32 / VDF_U32 / VDF_F64 (the reference's IntT, UIntT, FloatT)
+ * or VDF_I64 / VDF_U64; integer sums wrap in the value type as the
+ * reference's "+=" does, f64 sums are compensated (within 1e-12 relative of
+ * the row-order sum).  Host memory, synchronous.  Writes *n_colkeys,
+ * *n_rowkeys and each key's first row (colkey_row / rowkey_row, capacity n
+ * each); then the matrix, n_colkeys x n_rowkeys values of the value dtype,
+ * one output column after another (cell (c, r) at c * n_rowkeys + r), when
+ * it fits in matrix_cap values, else VDF_ERR_WORKSPACE with the counts and
+ * first rows written (call again with a matrix that fits).  The keys are
+ * dictionary-encoded on the device (a hash table of the strings, first rows
+ * by atomic minimum, ranks by a scan) and the pairs summed on the sorted
+ * path (vdf_sort_groupby). */
+vdf_status vdf_pivot_host(vdf_ctx* ctx, uint64_t n, vdf_strcol col_key, vdf_strcol row_key, vdf_col value,
+                          uint32_t* n_colkeys, uint32_t* n_rowkeys, uint32_t* colkey_row, uint32_t* rowkey_row,
+                          void* matrix, uint64_t matrix_cap);
+
 /* ---- fused sort + payload gather + group-by --------------------------------- */
 typedef struct vdf_sort_groupby_args {
     uint64_t n;

@@ -13,6 +13,7 @@
 //   transform_unique[_mt]         transform/transform_unique/transform_unique_mt.hpp:3-11
 //   transform_left_join[_mt]      transform/transform_left_join/transform_left_join_mt.hpp:3-15
 //                                 (methods First, Last and Aligned)
+//   pivot                         pivots/pivot.hpp:5-128 (vdf_pivot_host)
 //   readf                         read/read_csv/read_csv.hpp:3-216 (called as readf in
 //                                 benchmarks/readf.cpp:21): the file is parsed on the GPU
 //                                 (vdf_csv_read_host) into the frame's type blocks
@@ -49,6 +50,7 @@
 //     same path.
 #pragma once
 
+#include <charconv>
 #include <cstdint>
 #include <iostream>
 #include <map>
@@ -159,6 +161,7 @@ class Dataframe {
     std::vector<char> type_refv;               // type char of each column
     std::vector<unsigned int> slot_v;          // index of each column inside its type block
     std::vector<std::string> name_v;
+    std::vector<std::string> name_v_row;       // row names (set by pivot, as in the reference)
 
     // ---- building and reading ------------------------------------------------
     template <typename T>
@@ -426,6 +429,95 @@ class Dataframe {
                 dispatch_minmax(vt, run, colname);
             }
         }
+    }
+
+    // ---- pivot --------------------------------------------------------------------
+    // pivots/pivot.hpp:5-128: this frame becomes the pivot of obj -- one column
+    // (named by the key) per distinct value of column n1, one row (name_v_row)
+    // per distinct value of column n2, both in order of first appearance, and
+    // in each cell the sum of column n3 over the rows of that pair (0 for a
+    // pair that never occurs).  Keys compare as the text of their cells: the
+    // strings of 's' / 'c' columns, the decimal text of numbers (the reference
+    // keys on each cell's text as read).  Column n3 holds T (IntT, UIntT or
+    // FloatT as in the reference, or the 64-bit integer types); integer sums
+    // wrap in T like the reference's "+=", f64 sums are compensated.  The
+    // rows of obj are read as viewed.
+    template <typename T, bool SimdHash = true>
+    void pivot(Dataframe& obj, unsigned int& n1, unsigned int& n2, unsigned int& n3) {
+        (void)SimdHash;
+        if (n1 >= obj.ncol || n2 >= obj.ncol || n3 >= obj.ncol) {
+            std::cerr << "Column not found\n";
+            return;
+        }
+        const std::vector<T>* vals = obj.template col_ptr<T>(n3);
+        if (!vals) {
+            std::cerr << "Unsupported type for pivots\n";
+            return;
+        }
+        const unsigned int n = obj.nrow;
+        auto row_of = [&](unsigned int i) -> unsigned int { return obj.in_view ? (unsigned)obj.row_view_idx[i] : i; };
+        std::vector<std::string> ck = obj.cell_text(n1), rk = obj.cell_text(n2);
+        std::vector<char> cb, rb;
+        std::vector<uint64_t> co(n + 1, 0), ro(n + 1, 0);
+        std::vector<T> v(n);
+        for (unsigned int i = 0; i < n; ++i) {
+            const unsigned int r = row_of(i);
+            cb.insert(cb.end(), ck[r].begin(), ck[r].end());
+            rb.insert(rb.end(), rk[r].begin(), rk[r].end());
+            co[i + 1] = cb.size();
+            ro[i + 1] = rb.size();
+            v[i] = (*vals)[r];
+        }
+        cb.push_back(0);
+        rb.push_back(0);
+        uint32_t nc = 0, nr = 0;
+        std::vector<uint32_t> cfirst(std::max(1u, n)), rfirst(std::max(1u, n));
+        const vdf_col vc{v.data(), detail::dtype_of<T>()};
+        const vdf_strcol cs{cb.data(), co.data()}, rs{rb.data(), ro.data()};
+        vdf_status st = vdf_pivot_host(context(), n, cs, rs, vc, &nc, &nr, cfirst.data(), rfirst.data(), nullptr, 0);
+        if (st != VDF_OK && st != VDF_ERR_WORKSPACE) {
+            detail::report(st, "pivot");
+            return;
+        }
+        std::vector<T> cells((size_t)nc * nr);
+        st = vdf_pivot_host(context(), n, cs, rs, vc, &nc, &nr, cfirst.data(), rfirst.data(), cells.data(),
+                            cells.size());
+        if (!detail::report(st, "pivot")) return;
+        Dataframe out;
+        for (uint32_t c = 0; c < nc; ++c)
+            out.add_col(std::vector<T>(cells.begin() + (size_t)c * nr, cells.begin() + (size_t)(c + 1) * nr),
+                        ck[row_of(cfirst[c])]);
+        out.nrow = nr;
+        out.name_v_row.resize(nr);
+        for (uint32_t r = 0; r < nr; ++r) out.name_v_row[r] = rk[row_of(rfirst[r])];
+        *this = std::move(out);
+    }
+
+    // Text of every cell of column n in storage order (strings as they are,
+    // integers in decimal, doubles in their shortest round-trip form, bools
+    // as 0 / 1).
+    std::vector<std::string> cell_text(unsigned int n) const {
+        const unsigned s = slot_v[n];
+        std::vector<std::string> out(nrow);
+        auto num = [&](const auto& vec) {
+            char buf[64];
+            for (unsigned int r = 0; r < nrow; ++r) {
+                auto res = std::to_chars(buf, buf + sizeof(buf), vec[r]);
+                out[r].assign(buf, res.ptr);
+            }
+        };
+        switch (type_refv[n]) {
+        case 'i': num(int_v[s]); break;
+        case 'u': num(uint_v[s]); break;
+        case 'd': num(dbl_v[s]); break;
+        case 'l': num(lint_v[s]); break;
+        case 'L': num(luint_v[s]); break;
+        case 'b':
+            for (unsigned int r = 0; r < nrow; ++r) out[r] = bool_v[s][r] ? "1" : "0";
+            break;
+        default: out = str_v[s]; break;
+        }
+        return out;
     }
 
     // ---- de-duplication ------------------------------------------------------------

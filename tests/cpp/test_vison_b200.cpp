@@ -1,7 +1,8 @@
 // Exercises the header-only dataframe layer (include/vison_b200/vison.hpp) on
 // the GPU: the reference documentation's sort_by example, Soft/Hard sorts,
 // sorts while in view, materialize, sort_by_external, multi-key sorts and
-// the transform group-by (Gather with user functions included), checked against plain CPU computations here.
+// the transform group-by (Gather with user functions included) and the
+// pivot, checked against plain CPU computations here.
 #include <algorithm>
 #include <cstdio>
 #include <map>
@@ -219,6 +220,60 @@ static void test_transform_group_by_gather() {
     CHECK(okv);
 }
 
+// pivot: the documented example (INTERNALS.doc:1251-1296), then a random
+// frame against a std::map walk in row order (first-appearance indices).
+static void test_pivot() {
+    DF df;
+    df.add_col(std::vector<std::string>{"A", "A", "A", "B", "B", "A", "B", "B", "B", "A", "A", "B", "B", "B", "B"},
+               "col5");
+    df.add_col(std::vector<std::string>{"D", "D", "C", "C", "C", "D", "C", "D", "D", "C", "D", "C", "D", "C", "D"},
+               "col1");
+    df.add_col(std::vector<double>{3, 8, 0, 8, 3, 8, 3, 3, 8, 0, 8, 8, 0, 8, 3}, "col3");
+    unsigned n1 = 0, n2 = 1, n3 = 2;
+    DF p;
+    p.pivot<double>(df, n1, n2, n3);
+    CHECK(p.ncol == 2 && p.nrow == 2);
+    CHECK((p.name_v == std::vector<std::string>{"A", "B"}));
+    CHECK((p.name_v_row == std::vector<std::string>{"D", "C"}));
+    CHECK((p.dbl_v[0] == std::vector<double>{27, 0}) && (p.dbl_v[1] == std::vector<double>{14, 30}));
+
+    std::mt19937_64 rng(13);
+    const unsigned N = 40000;
+    std::vector<std::string> ck(N);
+    std::vector<unsigned> rk(N);
+    std::vector<int> v(N);
+    for (unsigned i = 0; i < N; ++i) {
+        ck[i] = "k" + std::string(rng() % 4, 'x') + std::to_string(rng() % 61);
+        rk[i] = (unsigned)(rng() % 257);
+        v[i] = (int)(rng() % 2000000001u) - 1000000000;  // sums wrap in int
+    }
+    DF q;
+    q.add_col(ck, "ck");
+    q.add_col(rk, "rk");
+    q.add_col(v, "v");
+    std::map<std::string, unsigned> ci, ri;
+    std::vector<std::string> corder, rorder;
+    std::map<std::pair<unsigned, unsigned>, uint32_t> acc;
+    for (unsigned i = 0; i < N; ++i) {
+        const std::string r = std::to_string(rk[i]);
+        if (ci.emplace(ck[i], (unsigned)ci.size()).second) corder.push_back(ck[i]);
+        if (ri.emplace(r, (unsigned)ri.size()).second) rorder.push_back(r);
+        acc[{ci[ck[i]], ri[r]}] += (uint32_t)v[i];
+    }
+    DF pq;
+    unsigned a = 0, b = 1, c = 2;
+    pq.pivot<int>(q, a, b, c);
+    CHECK(pq.ncol == corder.size() && pq.nrow == rorder.size());
+    CHECK(pq.name_v == corder && pq.name_v_row == rorder);
+    bool ok = pq.int_v.size() == corder.size();
+    for (unsigned x = 0; ok && x < corder.size(); ++x)
+        for (unsigned y = 0; y < rorder.size(); ++y) {
+            auto it = acc.find({x, y});
+            ok &= pq.int_v[x][y] == (int)(it == acc.end() ? 0u : it->second);
+        }
+    CHECK(ok);
+}
+
 // transform_unique: the rows kept are those a set walk keeps (first or last
 // occurrence per key value, in row order), for every column of the frame.
 static void test_transform_unique() {
@@ -340,6 +395,7 @@ int main() {
     test_sort_by_external();
     test_transform_group_by();
     test_transform_group_by_gather();
+    test_pivot();
     test_transform_unique();
     test_transform_left_join();
     test_readf();

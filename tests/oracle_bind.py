@@ -25,7 +25,7 @@ def _vp(a: np.ndarray):
 
 
 def _load_oracle() -> C.CDLL:
-    srcs = [ORACLE_DIR / "vdf_oracle.c", ORACLE_DIR / "vdf_oracle_csv.c"]
+    srcs = [ORACLE_DIR / "vdf_oracle.c", ORACLE_DIR / "vdf_oracle_csv.c", ORACLE_DIR / "vdf_oracle_pivot.c"]
     if not ORACLE_LIB.exists() or any(ORACLE_LIB.stat().st_mtime < p.stat().st_mtime for p in srcs):
         subprocess.run(["make", "-s", "-C", str(ORACLE_DIR), "all"], check=True)
     lib = C.CDLL(str(ORACLE_LIB))
@@ -53,6 +53,10 @@ def _load_oracle() -> C.CDLL:
     lib.orc_parse_u32.argtypes = [C.c_char_p, C.c_size_t]
     lib.orc_parse_i32.restype = C.c_int32
     lib.orc_parse_i32.argtypes = [C.c_char_p, C.c_size_t]
+    lib.orc_pivot.restype = C.c_int
+    lib.orc_pivot.argtypes = [C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                              C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.c_void_p, C.c_void_p, C.c_void_p,
+                              C.c_size_t]
     return lib
 
 
@@ -273,3 +277,41 @@ def ref_csv_seconds(data: bytes, delim=",", header=True, quote="'", cores=1, rep
     lib.ref_csv_time.argtypes = [C.c_char_p, C.c_size_t, C.c_char, C.c_int, C.c_char, C.c_int, C.c_int]
     return float(lib.ref_csv_time(data, len(data), delim.encode("latin-1"), 1 if header else 0,
                                   quote.encode("latin-1"), int(cores), int(reps)))
+
+
+def string_column(strings) -> tuple:
+    """(bytes uint8, offsets uint64 of len + 1) of a list of str / bytes."""
+    enc = [x.encode() if isinstance(x, str) else bytes(x) for x in strings]
+    offs = np.zeros(len(enc) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(x) for x in enc], dtype=np.uint64)
+    data = np.frombuffer(b"".join(enc) or b"\0", np.uint8).copy()
+    return data, offs
+
+
+class OraclePivot:
+    def __init__(self, colkey_row, rowkey_row, matrix):
+        self.colkey_row = colkey_row  # first row of each col key, in first-appearance order
+        self.rowkey_row = rowkey_row
+        self.matrix = matrix          # [n_colkeys, n_rowkeys]
+
+
+def pivot(col_strings, row_strings, values) -> OraclePivot:
+    """Oracle pivot (V/pivots/pivot.hpp:5-128): sum of values per (col key,
+    row key), col and row keys in first-appearance order."""
+    n = len(values)
+    cb, co = string_column(col_strings)
+    rb, ro = string_column(row_strings)
+    values = np.ascontiguousarray(values)
+    code = {np.dtype(np.int32): 0, np.dtype(np.int64): 1, np.dtype(np.uint32): 2, np.dtype(np.uint64): 3,
+            np.dtype(np.float64): 4}[values.dtype]
+    ckr = np.zeros(max(1, n), np.uint32)
+    rkr = np.zeros(max(1, n), np.uint32)
+    nc, nr = C.c_uint32(), C.c_uint32()
+    lib = oracle()
+    assert lib.orc_pivot(n, _vp(cb), _vp(co), _vp(rb), _vp(ro), _vp(values), code, C.byref(nc), C.byref(nr),
+                         _vp(ckr), _vp(rkr), None, 0) in (0, -1)
+    m = np.zeros(max(1, nc.value * nr.value), values.dtype)
+    assert lib.orc_pivot(n, _vp(cb), _vp(co), _vp(rb), _vp(ro), _vp(values), code, C.byref(nc), C.byref(nr),
+                         _vp(ckr), _vp(rkr), _vp(m), m.size) == 0
+    return OraclePivot(ckr[:nc.value].copy(), rkr[:nr.value].copy(),
+                       m[:nc.value * nr.value].reshape(nc.value, nr.value))

@@ -177,3 +177,37 @@ def test_live_reference_groupby_multikey_checksums(cores):
     assert chk[0] == og.count.sum()
     assert chk[1] == pytest.approx(og.sum[0].sum(), rel=1e-12)
     assert chk[2] == float(og.sum[1].sum())
+
+
+def test_pivot_matches_the_documented_example():
+    """INTERNALS.doc:1251-1296 (pivot of the 15-row frame): col key col5
+    (A/B), row key the second col1 (D/C), values the second col3; the
+    documented result is A: D=27, C=0 and B: D=14, C=30."""
+    col5 = list("AAABBABBBAABBBB")
+    col1b = list("DDCCCDCDDCDCDCD")
+    col3b = np.array([3, 8, 0, 8, 3, 8, 3, 3, 8, 0, 8, 8, 0, 8, 3], np.float64)
+    p = ob.pivot(col5, col1b, col3b)
+    assert [col5[r] for r in p.colkey_row] == ["A", "B"]
+    assert [col1b[r] for r in p.rowkey_row] == ["D", "C"]
+    assert p.matrix.tolist() == [[27.0, 0.0], [14.0, 30.0]]
+
+
+def test_pivot_oracle_against_a_dict_walk():
+    rng = np.random.default_rng(5)
+    n = 5000
+    cols = [f"c{x}" for x in rng.integers(0, 37, n)]
+    rows = ["r" * int(x % 3) + str(x) for x in rng.integers(0, 101, n)]
+    for dt in (np.int32, np.uint32, np.int64, np.float64):
+        vals = rng.integers(-1000, 1000, n).astype(dt) if dt != np.float64 else rng.standard_normal(n)
+        p = ob.pivot(cols, rows, vals)
+        ci, ri, acc = {}, {}, {}
+        for c, r, v in zip(cols, rows, vals):
+            ci.setdefault(c, len(ci))
+            ri.setdefault(r, len(ri))
+            acc[(c, r)] = acc.get((c, r), dt(0)) + v
+        assert [cols[r] for r in p.colkey_row] == list(ci)
+        assert [rows[r] for r in p.rowkey_row] == list(ri)
+        exp = np.zeros((len(ci), len(ri)), vals.dtype)
+        for (c, r), v in acc.items():
+            exp[ci[c], ri[r]] = v
+        assert (p.matrix == exp).all()

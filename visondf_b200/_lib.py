@@ -50,6 +50,10 @@ class vdf_col(C.Structure):
     _fields_ = [("data", C.c_void_p), ("dtype", C.c_int32)]
 
 
+class vdf_strcol(C.Structure):
+    _fields_ = [("bytes", C.c_void_p), ("offsets", C.c_void_p)]
+
+
 class vdf_agg_out(C.Structure):
     _fields_ = [("sum", C.c_void_p), ("sum_hi", C.c_void_p), ("min", C.c_void_p), ("max", C.c_void_p),
                 ("mean", C.c_void_p)]
@@ -129,6 +133,8 @@ def _load() -> C.CDLL:
         "vdf_sort_groupby_host": (st, [vp, C.POINTER(vdf_sort_groupby_args), vp]),
         "vdf_broadcast": (st, [vp, u64, vp, vp, u64, i32, vp, vp, vp]),
         "vdf_unique": (st, [vp, u64, vdf_col, i32, vp, vp, C.POINTER(C.c_uint64), vp]),
+        "vdf_pivot_host": (st, [vp, u64, vdf_strcol, vdf_strcol, vdf_col, C.POINTER(C.c_uint32),
+                                C.POINTER(C.c_uint32), vp, vp, vp, u64]),
         "vdf_left_join_index": (st, [vp, u64, vdf_col, u64, vdf_col, i32, vp, vp, C.POINTER(C.c_uint64), vp]),
         "vdf_gather_host": (st, [vp, u64, vp, C.POINTER(vdf_col), i32, C.POINTER(vp), vp]),
         "vdf_transform_groupby_host": (st, [vp, u64, C.POINTER(vdf_col), i32, vdf_col, C.c_int32, vp, vp,
@@ -483,6 +489,39 @@ class Context:
         self._check(lib.vdf_unique(self.handle, n, _col(key), 1 if keep_last else 0, _ptr(keep), None,
                                    C.byref(cnt), _stream(stream)), "vdf_unique")
         return keep, int(cnt.value)
+
+    def pivot_host(self, col_key, row_key, values) -> dict:
+        """Pivot (the reference's pivot, pivots/pivot.hpp:5-128) of host
+        columns: col_key / row_key are string columns given as (bytes uint8,
+        offsets uint64 of n + 1) numpy arrays, values a numpy int32 / uint32 /
+        int64 / uint64 / float64 column.  Returns {"colkey_row": first row of
+        each col key, "rowkey_row": likewise, "matrix": [n_colkeys,
+        n_rowkeys] sums}, keys in first-appearance order."""
+        import numpy as np
+        values = np.ascontiguousarray(values)
+        code = {np.dtype(np.int32): I32, np.dtype(np.uint32): U32, np.dtype(np.int64): I64,
+                np.dtype(np.uint64): U64, np.dtype(np.float64): F64, np.dtype(np.float32): F32}[values.dtype]
+        n = values.size
+        cols = []
+        for b, o in (col_key, row_key):
+            b = np.ascontiguousarray(b, np.uint8)
+            o = np.ascontiguousarray(o, np.uint64)
+            assert o.size == n + 1
+            cols.append((b, o, vdf_strcol(b.ctypes.data if b.size else None, o.ctypes.data)))
+        ckr = np.zeros(max(1, n), np.uint32)
+        rkr = np.zeros(max(1, n), np.uint32)
+        nc, nr = C.c_uint32(), C.c_uint32()
+        vc = vdf_col(values.ctypes.data if n else None, code)
+        st = lib.vdf_pivot_host(self.handle, n, cols[0][2], cols[1][2], vc, C.byref(nc), C.byref(nr),
+                                ckr.ctypes.data, rkr.ctypes.data, None, 0)
+        if st not in (OK, ERR_WORKSPACE):
+            self._check(st, "vdf_pivot_host")
+        m = np.zeros(max(1, nc.value * nr.value), values.dtype)
+        st = lib.vdf_pivot_host(self.handle, n, cols[0][2], cols[1][2], vc, C.byref(nc), C.byref(nr),
+                                ckr.ctypes.data, rkr.ctypes.data, m.ctypes.data, m.size)
+        self._check(st, "vdf_pivot_host")
+        return {"colkey_row": ckr[:nc.value].copy(), "rowkey_row": rkr[:nr.value].copy(),
+                "matrix": m[:nc.value * nr.value].reshape(nc.value, nr.value)}
 
     def read_csv(self, data, delim: str = ",", header: bool = True, quote: str = "'", stream=None) -> "CsvTable":
         """Parses a CSV file's bytes (`bytes` / numpy uint8 in host memory, or

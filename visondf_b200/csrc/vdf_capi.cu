@@ -337,7 +337,7 @@ vdf_status vdf_ctx_create(int device, vdf_ctx** out) {
         }
     }
     if (cudaMalloc(&c->dev_small, 256) != cudaSuccess || cudaMemset(c->dev_small, 0, 256) != cudaSuccess ||
-        cudaMallocHost(&c->host_pinned, 4 * sizeof(uint64_t)) != cudaSuccess) {
+        cudaMallocHost(&c->host_pinned, 8 * sizeof(uint64_t)) != cudaSuccess) {
         cudaGetLastError();
         if (c->dev_small) cudaFree(c->dev_small);
         delete c;
@@ -692,6 +692,10 @@ struct HostStage {
 
 
 }  // namespace
+
+vdf_status vdfc::sort_groupby_device(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaStream_t s) {
+    return sort_groupby_locked(c, x, s);
+}
 
 extern "C" {
 

@@ -79,7 +79,8 @@ struct vdf_ctx {
     size_t ws_cap = 0;
     unsigned char* dev_small = nullptr;  // [0,4): error bits; [8,16): group count scratch;
                                          // [16,20): tie flag; [24,28): MSD fallbacks
-    uint64_t* host_pinned = nullptr;     // [0]: group count, [1]: error bits, [2]: tie flag, [3]: fallbacks
+    uint64_t* host_pinned = nullptr;     // [0]: group count, [1]: error bits, [2]: tie flag, [3]: fallbacks,
+                                         // [4]: pivot key counts (two words), [5..7] spare
     uint64_t msd_sorts = 0;              // sorts planned MSD-first
     uint32_t fail_allocs = 0;            // test hook: workspace allocations to fail
     int multikey_mode = VDF_MULTIKEY_PRIMARY_FIRST;
@@ -180,6 +181,9 @@ inline vdf_status io_ensure(vdf_ctx* c, size_t bytes) {
     c->io_cap = cap;
     return VDF_OK;
 }
+
+// vdf_sort_groupby on device pointers with the context lock already held.
+vdf_status sort_groupby_device(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaStream_t s);
 
 // Reads and clears the device error bits after the stream has drained.
 inline vdf_status drain_and_check(vdf_ctx* c, cudaStream_t s) {
