@@ -34,4 +34,6 @@ def assert_f64_close(got: np.ndarray, exact: np.ndarray, abs_sum: np.ndarray, wh
     assert cond_ok.all(), f"{what}: {np.count_nonzero(~cond_ok)} groups beyond 1e-12 * sum|x|, " \
                           f"worst {err[~cond_ok][:5]} vs {exact[~cond_ok][:5]}"
     rel_ok = err <= F64_REL * np.abs(exact)
-    return int(np.count_nonzero(~rel_ok))
+    plain = int(np.count_nonzero(~rel_ok))
+    print(f"{what}: {got.size} groups within 1e-12 * sum|x|; plain-relative failures: {plain}")
+    return plain
