@@ -124,7 +124,8 @@ typedef enum vdf_kernel_class {
     VDF_KC_BATCH = 11,      /* batch bookkeeping: row ids per query, group ranges, group keys */
     VDF_KC_CSV = 12,        /* CSV ingest: record split, field parse, string columns */
     VDF_KC_LOCALSORT = 13,  /* MSD-first sort: chunk search + shared-memory finish */
-    VDF_KC_FALLBACK = 14    /* MSD-first sort: the conditional LSD kernels (return at once unless taken) */
+    VDF_KC_FALLBACK = 14,   /* MSD-first / dictionary sort: the conditional LSD kernels (return at once unless taken) */
+    VDF_KC_DICT = 15        /* dictionary sort: collection of the distinct keys and their ranks */
 } vdf_kernel_class;
 /* When enabled, every kernel the context launches is bracketed by CUDA
  * events on its stream (no reference counterpart: the reference has no
@@ -199,6 +200,17 @@ typedef enum vdf_sort_strategy {
     VDF_SORT_MSD = 2
 } vdf_sort_strategy;
 vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* ctx, int strategy, uint64_t msd_min_rows);
+/* The dictionary plan (VDF_SORT_AUTO, sorts by ONE key column of at least
+ * msd_min_rows rows): the key column's distinct values are collected on the
+ * device first; with at most 256 of them the sort is one stable radix pass
+ * over each key's rank among them (a category column: 1 pass instead of 4 or
+ * 8), otherwise the MSD-first plan (8-byte keys) or the LSD passes run, as
+ * decided on the device.  vdf_sort_plan_tries_dict: 1 when a sort of that
+ * shape tries it (-1 for bad arguments); vdf_ctx_dict_stats: sorts of the
+ * context that tried it and (reading the device counter, synchronising
+ * `stream`) those that took it. */
+int vdf_sort_plan_tries_dict(uint64_t n, const int32_t* key_dtypes, int nkeys, int strategy, uint64_t min_rows);
+vdf_status vdf_ctx_dict_stats(vdf_ctx* ctx, void* stream, uint64_t* tried, uint64_t* taken);
 vdf_status vdf_ctx_get_sort_strategy(vdf_ctx* ctx, int32_t* strategy, uint64_t* msd_min_rows);
 /* Digit matching of the MSD-first sort's shared-memory passes: 0 = one warp
  * ballot per digit bit (default), 1 = match.any; the autotuner's choice. */

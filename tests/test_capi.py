@@ -99,7 +99,8 @@ def test_autotune_size_classes():
 def test_sort_plan_choice():
     info = _lib.sort_plan_info
     # 100M rows, int64 + int32 keys: two top-digit passes, 2048-row chunks
-    assert info(100_000_000, [vdf.I64, vdf.I32]) == {"msd_passes": 2, "chunks": (100_000_000 + 2047) // 2048}
+    assert info(100_000_000, [vdf.I64, vdf.I32]) == {"msd_passes": 2, "chunks": (100_000_000 + 2047) // 2048,
+                                                       "dict": False}
     assert info(200_000_000, [vdf.I64])["msd_passes"] == 3
     # 4-byte key 0: the LSD passes unless the MSD strategy is forced
     assert info(393_216, [vdf.I32], msd_min_rows=0)["msd_passes"] == 0
@@ -112,3 +113,16 @@ def test_sort_plan_choice():
     assert info(10_000_000, [vdf.I64, vdf.I32, vdf.I32])["msd_passes"] == 0
     assert info(10_000_000, [vdf.I64], strategy=_lib.SORT_LSD)["msd_passes"] == 0
     assert info(1, [vdf.I64], msd_min_rows=0)["msd_passes"] == 0
+
+
+def test_dictionary_plan_choice():
+    info = _lib.sort_plan_info
+    # one key, at least the row threshold, the automatic strategy: tried first
+    assert info(200_000_000, [vdf.I32])["dict"] and info(2_000_000, [vdf.F64])["dict"]
+    assert info(200_000_000, [vdf.I64])["msd_passes"] == 3  # its fallback when the values are many
+    assert not info(1000, [vdf.I32])["dict"]
+    assert info(1000, [vdf.I32], msd_min_rows=0)["dict"]
+    assert not info(2_000_000, [vdf.I32, vdf.I32])["dict"]
+    assert not info(2_000_000, [vdf.I32], strategy=_lib.SORT_LSD)["dict"]
+    assert not info(2_000_000, [vdf.I32], strategy=_lib.SORT_MSD)["dict"]
+    assert vdf.lib.vdf_sort_plan_tries_dict(10, None, 1, 0, 0) == -1

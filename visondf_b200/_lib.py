@@ -26,7 +26,7 @@ I32, I64, U32, U64, F64, F32 = range(6)
 ORDER_ASC, ORDER_DESC_STABLE, ORDER_DESC_REVERSE = range(3)
 
 KERNEL_CLASSES = ["hist", "scan", "onesweep32", "onesweep64", "gather", "segreduce", "broadcast", "pack",
-                  "segscan", "segemit", "ties", "batch", "csv", "localsort", "fallback"]
+                  "segscan", "segemit", "ties", "batch", "csv", "localsort", "fallback", "dict"]
 # vdf_multikey_mode
 MULTIKEY_LSD, MULTIKEY_PRIMARY_FIRST = 0, 1
 # vdf_sort_strategy
@@ -143,6 +143,8 @@ def _load() -> C.CDLL:
         "vdf_ctx_get_multikey_mode": (i32, [vp]),
         "vdf_ctx_set_sort_strategy": (st, [vp, i32, u64]),
         "vdf_ctx_sort_stats": (st, [vp, vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "vdf_ctx_dict_stats": (st, [vp, vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "vdf_sort_plan_tries_dict": (i32, [u64, C.POINTER(C.c_int32), i32, i32, u64]),
         "vdf_ctx_set_local_sort_variant": (st, [vp, i32]),
         "vdf_ctx_set_test_hooks": (st, [vp, C.c_uint32, C.c_uint32, C.c_uint32]),
         "vdf_ctx_get_local_sort_variant": (i32, [vp]),
@@ -326,10 +328,13 @@ class Context:
         self._check(lib.vdf_ctx_set_sort_strategy(self.handle, strategy, msd_min_rows), "vdf_ctx_set_sort_strategy")
 
     def sort_stats(self, stream=None) -> dict:
-        """{"msd_sorts": sorts planned MSD-first, "msd_fallbacks": of those, LSD fallbacks on the device}"""
-        a, b = C.c_uint64(), C.c_uint64()
+        """{"msd_sorts": sorts planned MSD-first, "msd_fallbacks": of those, LSD fallbacks on the device,
+        "dict_sorts": sorts that tried the dictionary plan, "dict_taken": of those, the ones it sorted}"""
+        a, b, c, d = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_uint64()
         self._check(lib.vdf_ctx_sort_stats(self.handle, _stream(stream), C.byref(a), C.byref(b)), "sort_stats")
-        return {"msd_sorts": int(a.value), "msd_fallbacks": int(b.value)}
+        self._check(lib.vdf_ctx_dict_stats(self.handle, _stream(stream), C.byref(c), C.byref(d)), "sort_stats")
+        return {"msd_sorts": int(a.value), "msd_fallbacks": int(b.value), "dict_sorts": int(c.value),
+                "dict_taken": int(d.value)}
 
     def set_test_hooks(self, spin_limit: int = 0, stall_tile: int = 0xFFFFFFFF, fail_allocs: int = 0):
         """Failure injection for tests (see vdf_ctx_set_test_hooks)."""
@@ -680,13 +685,15 @@ def sort_variants() -> list:
 
 
 def sort_plan_info(n: int, dtypes: Sequence[int], strategy: int = SORT_AUTO, msd_min_rows: int = 1 << 20) -> dict:
-    """The plan of a sort: {"msd_passes": global MSD passes (0 = LSD), "chunks": shared-memory chunks}."""
+    """The plan of a sort: {"msd_passes": global MSD passes (0 = LSD), "chunks": shared-memory chunks,
+    "dict": whether the dictionary plan is tried first}."""
     dts = (C.c_int32 * len(dtypes))(*dtypes)
     p, c = C.c_int32(), C.c_uint32()
+    tries = lib.vdf_sort_plan_tries_dict(n, dts, len(dtypes), strategy, msd_min_rows)
     st = lib.vdf_sort_plan_info(n, dts, len(dtypes), strategy, msd_min_rows, C.byref(p), C.byref(c))
     if st != OK:
         raise VdfError(st, "vdf_sort_plan_info")
-    return {"msd_passes": p.value, "chunks": c.value}
+    return {"msd_passes": p.value, "chunks": c.value, "dict": tries == 1}
 
 
 def header_functions() -> list[str]:

@@ -173,11 +173,13 @@ size_t vdf_sort_workspace_bytes(uint64_t n, const int32_t* key_dtypes, int nkeys
     const int nv = vdf::sort_variant_count();
     for (int a = 0; a < nv; ++a)
         for (int b = 0; b < nv; ++b)
-            for (int msd = 0; msd < 2; ++msd) {
-                vdf::SortTuning t{a, b, msd, 0};
-                if (vdf::sort_tuning_valid(t))
-                    best = std::max(best, vdf::make_sort_plan(n, key_dtypes, nkeys, t).ws_bytes);
-            }
+            for (int msd = 0; msd < 2; ++msd)
+                for (int dict = 0; dict < 2; ++dict) {
+                    vdf::SortTuning t{a, b, msd, 0};
+                    t.dict = dict;
+                    if (vdf::sort_tuning_valid(t))
+                        best = std::max(best, vdf::make_sort_plan(n, key_dtypes, nkeys, t).ws_bytes);
+                }
     return best;
 }
 
@@ -242,6 +244,7 @@ vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* c, int strategy, uint64_t msd_min_
         return fail(c, VDF_ERR_INVALID_ARG, "bad sort strategy %d", strategy);
     std::lock_guard<std::mutex> lk(c->mu);
     c->tuning.msd = msd_mode_of(strategy);
+    c->tuning.dict = strategy == VDF_SORT_AUTO ? 1 : 0;
     c->tuning.msd_min_rows = msd_min_rows;
     return VDF_OK;
 }
@@ -298,10 +301,36 @@ vdf_status vdf_sort_plan_info(uint64_t n, const int32_t* key_dtypes, int nkeys, 
     vdf::SortTuning t = vdf::default_sort_tuning();
     if (strategy != VDF_SORT_AUTO && strategy != VDF_SORT_LSD && strategy != VDF_SORT_MSD) return VDF_ERR_INVALID_ARG;
     t.msd = msd_mode_of(strategy);
+    t.dict = strategy == VDF_SORT_AUTO ? 1 : 0;
     t.msd_min_rows = msd_min_rows;
     const vdf::SortPlan p = vdf::make_sort_plan(n, key_dtypes, nkeys, t);
     if (msd_passes) *msd_passes = p.msd ? p.msd_passes : 0;
     if (chunks) *chunks = p.msd ? p.msd_chunks : 0;
+    return VDF_OK;
+}
+
+int vdf_sort_plan_tries_dict(uint64_t n, const int32_t* key_dtypes, int nkeys, int strategy, uint64_t min_rows) {
+    if (!key_dtypes || nkeys < 1 || nkeys > vdf::kMaxKeys) return -1;
+    for (int k = 0; k < nkeys; ++k)
+        if (!valid_dtype(key_dtypes[k])) return -1;
+    if (strategy != VDF_SORT_AUTO && strategy != VDF_SORT_LSD && strategy != VDF_SORT_MSD) return -1;
+    vdf::SortTuning t = vdf::default_sort_tuning();
+    t.msd = msd_mode_of(strategy);
+    t.dict = strategy == VDF_SORT_AUTO ? 1 : 0;
+    t.msd_min_rows = min_rows;
+    return vdf::make_sort_plan(n, key_dtypes, nkeys, t).dict ? 1 : 0;
+}
+
+vdf_status vdf_ctx_dict_stats(vdf_ctx* c, void* stream, uint64_t* tried, uint64_t* taken) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(c->mu);
+    DeviceGuard g(c->device);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(&c->host_pinned[5], dict_word(c), sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return from_cuda(c, e, "read sort statistics");
+    if (tried) *tried = c->dict_sorts;
+    if (taken) *taken = (uint32_t)c->host_pinned[5];
     return VDF_OK;
 }
 

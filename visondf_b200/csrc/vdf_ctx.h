@@ -78,10 +78,13 @@ struct vdf_ctx {
     unsigned char* ws = nullptr;
     size_t ws_cap = 0;
     unsigned char* dev_small = nullptr;  // [0,4): error bits; [8,16): group count scratch;
-                                         // [16,20): tie flag; [24,28): MSD fallbacks
+                                         // [16,20): tie flag; [24,28): MSD fallbacks;
+                                         // [28,32): dictionary passes taken
     uint64_t* host_pinned = nullptr;     // [0]: group count, [1]: error bits, [2]: tie flag, [3]: fallbacks,
-                                         // [4]: pivot key counts (two words), [5..7] spare
+                                         // [4]: pivot key counts (two words), [5]: dictionary passes
+                                         // taken, [6..7] spare
     uint64_t msd_sorts = 0;              // sorts planned MSD-first
+    uint64_t dict_sorts = 0;             // sorts that tried the dictionary plan
     uint32_t fail_allocs = 0;            // test hook: workspace allocations to fail
     int multikey_mode = VDF_MULTIKEY_PRIMARY_FIRST;
     std::atomic<uint64_t> launches{0};
@@ -131,15 +134,17 @@ inline uint32_t* err_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->de
 inline uint64_t* count_word(vdf_ctx* c) { return reinterpret_cast<uint64_t*>(c->dev_small + 8); }
 inline uint32_t* tie_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->dev_small + 16); }
 inline uint32_t* fallback_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->dev_small + 24); }
+inline uint32_t* dict_word(vdf_ctx* c) { return reinterpret_cast<uint32_t*>(c->dev_small + 28); }
 
 // run_sort with the context's error word, profiler and MSD bookkeeping.
 inline cudaError_t ctx_run_sort(vdf_ctx* c, const vdf::SortPlan& p, const void* const* cols, int order,
                                 uint32_t* perm_out, void* key0_out, unsigned char* ws, cudaStream_t s,
                                 const uint32_t* perm_in = nullptr) {
     if (p.msd && p.n) c->msd_sorts++;
+    if (p.dict && p.n) c->dict_sorts++;
     c->launches += (uint64_t)vdf::sort_launches(p);
     return vdf::run_sort(p, cols, order, perm_out, key0_out, ws, err_word(c), s, prof_of(c), perm_in,
-                         fallback_word(c));
+                         fallback_word(c), dict_word(c));
 }
 
 inline vdf_status ws_ensure(vdf_ctx* c, size_t bytes) {

@@ -15,7 +15,7 @@ constexpr int kMaxGather = 8;   // columns per gather launch
 enum KernelClass : int {
     KC_HIST = 0, KC_SCAN = 1, KC_ONESWEEP32 = 2, KC_ONESWEEP64 = 3, KC_GATHER = 4, KC_SEGREDUCE = 5,
     KC_BROADCAST = 6, KC_PACK = 7, KC_SEGSCAN = 8, KC_SEGEMIT = 9, KC_TIES = 10, KC_BATCH = 11,
-    KC_CSV = 12, KC_LOCALSORT = 13, KC_FALLBACK = 14, KC_COUNT = 15
+    KC_CSV = 12, KC_LOCALSORT = 13, KC_FALLBACK = 14, KC_DICT = 15, KC_COUNT = 16
 };
 
 // Brackets kernel launches with CUDA events when profiling is enabled.
@@ -46,7 +46,7 @@ struct HistArgs {
     int hist_words;
     uint64_t n;
     uint32_t* hist;
-    const uint32_t* run_flag;  // non-null: the kernel runs only if *run_flag != 0
+    const uint32_t* run_flag;  // non-null: the kernel runs only if *run_flag == 1 (the LSD fallback)
     uint32_t* run_count;       // non-null: incremented once when a conditional launch runs
 };
 // Histograms of every pass laid out back to back: pass g has radix[g] bins
@@ -56,7 +56,7 @@ struct ScanArgs {
     uint32_t* offs;
     uint32_t off[kMaxPasses];
     uint32_t radix[kMaxPasses];
-    const uint32_t* run_flag;  // non-null: the kernel runs only if *run_flag != 0
+    const uint32_t* run_flag;  // non-null: the kernel runs only if *run_flag == 1 (the LSD fallback)
 };
 
 // One segment of a segmented sort: rows [row_start, row_start + rows) of the
@@ -71,6 +71,49 @@ struct SegDesc {
     uint32_t passes;
     uint32_t first_digit;
 };
+
+// Dictionary plan limits: distinct keys it takes, slots of the collection
+// table (global; each CTA has a table of kDictCtaSlots in shared memory) and
+// of the lookup table the pass reads.
+constexpr uint32_t kDictMax = 256;
+constexpr uint32_t kDictSlots = 1024;
+constexpr uint32_t kDictCtaSlots = 512;
+constexpr uint32_t kDictLutSlots = 512;
+// One slot of a collection table: state 0 empty, 1 being written, 2 ready.
+struct DictSlot {
+    unsigned long long key;
+    uint32_t count;
+    uint32_t state;
+};
+// Order image -> rank among the distinct keys (rank kDictEmpty: free slot).
+constexpr uint32_t kDictEmpty = 0xffffffffu;
+struct DictLut {
+    unsigned long long key[kDictLutSlots];
+    uint32_t rank[kDictLutSlots];
+};
+__host__ __device__ inline uint32_t dict_hash(unsigned long long x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    return (uint32_t)x;
+}
+struct DictArgs {
+    const void* keys;         // raw key column (any row order: only the key multiset matters)
+    int dtype, invert, width;
+    uint64_t n;
+    DictSlot* table;          // [kDictSlots], zeroed
+    uint32_t* distinct;       // distinct keys merged so far
+    uint32_t* overflow;       // set when there are more than kDictMax (or a wait gave up)
+    uint32_t* state;          // the sort's plan word
+    uint32_t fail_state;      // plan word when the dictionary does not apply (0 MSD-first, 1 LSD)
+    DictLut* lut;
+    uint32_t* bin_offsets;    // [256] exclusive starts of the ranks
+    uint32_t* taken;          // non-null: incremented when the dictionary pass is taken
+    uint32_t spin_limit;
+    uint32_t* err;
+};
+cudaError_t dict_collect(const DictArgs& a, cudaStream_t s);
+cudaError_t dict_rank(const DictArgs& a, cudaStream_t s);
 
 struct PassArgs {
     const void* keys_in;        // raw column (IN_RAW / IN_GATHER) or ordered-key buffer
@@ -98,9 +141,13 @@ struct PassArgs {
     void* keys_final;           // where a segment's last pass writes its keys
     uint32_t* vals_final;       // ... and its row ids
     // conditional passes: with run_flag set the pass runs only when
-    // (*run_flag != 0) == (run_when != 0), and otherwise returns at once
+    // *run_flag == run_when, and otherwise returns at once (the sort's plan
+    // word: 0 MSD-first passes, 1 LSD passes, 2 done by the dictionary pass)
     const uint32_t* run_flag;
     uint32_t run_when;
+    // dictionary pass: the digit of a key is its rank among the sort's
+    // distinct keys, looked up in this table
+    const DictLut* dict_lut = nullptr;
     // failure injection for tests: polls before a look-back wait gives up (0:
     // the default kSpinLimit), and a tile whose CTA publishes nothing
     uint32_t spin_limit = 0;
@@ -129,10 +176,9 @@ struct SortTuning {
     // limit (0 = default) and a tile of the first pass that never publishes
     uint32_t spin_limit = 0;
     uint32_t stall_tile = 0xffffffffu;
-    // segmented passes only: with seg_flag set, a tile runs only when
-    // (seg_flag[segment] != 0) == (seg_flag_when != 0)
-    const uint32_t* seg_flag = nullptr;
-    uint32_t seg_flag_when = 0;
+    // dictionary plan (vdf_dict.cu): 1 = tried for one-key sorts with at
+    // least msd_min_rows rows, 0 = never
+    int dict = 0;
 };
 SortTuning default_sort_tuning();
 bool sort_tuning_valid(const SortTuning& t);
@@ -161,6 +207,14 @@ struct SortPlan {
     uint32_t msd_chunk_rows;   // nominal rows per chunk
     uint32_t msd_chunks;       // ceil(n / msd_chunk_rows)
     size_t off_msd_hist, off_msd_offs, off_msd_flag, off_chunks;
+    // dictionary plan: a one-key sort whose key takes at most kDictMax
+    // distinct values is one stable pass over each key's rank; the values
+    // are collected on the device first, and with more of them the MSD-first
+    // or LSD passes run instead (the plan word at off_msd_flag decides)
+    bool dict;
+    int dict_variant;          // index into the dictionary-pass kernels
+    uint32_t dict_tiles;
+    size_t off_dict_table, off_dict_lut, off_dict_offs, off_dict_words;
 };
 // MSD-first sort limits: rows one CTA sorts in shared memory, the longest
 // run of equal high key bits the shared-memory finish ranks directly, and the
@@ -175,6 +229,7 @@ struct MsdHistArgs {
     int dtype, invert, first_digit, ndig;
     uint64_t n;
     uint32_t* hist;    // [ndig][256]
+    const uint32_t* flag = nullptr;  // the plan word: the histograms run only while it is 0
 };
 // A chunk of a segmented MSD-first sort: nominal first row x (the segment's
 // first row for its first chunk), the segment's rows [seg_start, seg_end),
@@ -228,7 +283,8 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
 // plan falls back to the LSD passes.
 cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
                      void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof = nullptr,
-                     const uint32_t* perm_in = nullptr, uint32_t* msd_fallbacks = nullptr);
+                     const uint32_t* perm_in = nullptr, uint32_t* msd_fallbacks = nullptr,
+                     uint32_t* dict_taken = nullptr);
 cudaError_t prepare_sort_kernels();
 cudaError_t prepare_msd_kernels();
 // *flag |= 1 when two neighbouring elements of a sorted key column (4- or

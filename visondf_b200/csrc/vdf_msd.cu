@@ -54,6 +54,8 @@ namespace vdf {
 // ---------------------------------------------------------------------------
 template <typename K>
 __global__ void __launch_bounds__(512) k_msd_hist(MsdHistArgs a) {
+    // the plan word (written by an earlier launch): this plan runs only at 0
+    if (a.flag && *a.flag != 0) return;
     __shared__ uint32_t h[kMsdMaxPasses * 256];
     for (int i = threadIdx.x; i < a.ndig * 256; i += blockDim.x) h[i] = 0;
     __syncthreads();
@@ -86,6 +88,7 @@ __global__ void __launch_bounds__(256) k_msd_scan(const uint32_t* hist, uint32_t
                                                   uint32_t* flag) {
     __shared__ uint32_t wsum[8];
     __shared__ uint32_t nonempty[kMsdMaxPasses];
+    if (*static_cast<volatile uint32_t*>(flag) != 0) return;  // another plan sorts (written by an earlier launch)
     const int b = threadIdx.x, lane = b & 31, warp = b >> 5;
     if (b < kMsdMaxPasses) nonempty[b] = 0;
     uint32_t top = 0;

@@ -39,7 +39,7 @@ namespace vdf {
 template <int FIXED_BITS>
 __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
     extern __shared__ uint32_t sh_hist[];  // [hist_words]
-    if (a.run_flag && *a.run_flag == 0) return;  // conditional launch not taken
+    if (a.run_flag && *a.run_flag != 1) return;  // conditional launch (the LSD fallback) not taken
     if (a.run_count && blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(a.run_count, 1u);
     for (int i = threadIdx.x; i < a.hist_words; i += blockDim.x) sh_hist[i] = 0;
     __syncthreads();
@@ -98,7 +98,7 @@ __global__ void __launch_bounds__(512) k_digit_hist(HistArgs a) {
 __global__ void __launch_bounds__(256) k_hist_scan(ScanArgs a) {
     constexpr int PER = kMaxRadix / 256;
     __shared__ uint32_t warp_tot[8];
-    if (a.run_flag && *a.run_flag == 0) return;  // conditional launch not taken
+    if (a.run_flag && *a.run_flag != 1) return;  // conditional launch (the LSD fallback) not taken
     const uint32_t radix = a.radix[blockIdx.x];
     const uint32_t* h = a.hist + a.off[blockIdx.x];
     uint32_t* o = a.offs + a.off[blockIdx.x];
@@ -282,9 +282,24 @@ struct OnesweepCfg {
 // row ids into a second shared-memory buffer with a bulk copy behind an
 // mbarrier (full, 16-byte aligned tiles; others load as usual); meant for a
 // persistent grid of a few CTAs per SM.
+// DICT: the dictionary pass of a one-key sort: a key's digit is its rank
+// among the sort's distinct keys, looked up (open addressing) in a table
+// staged in shared memory once per CTA.
+__device__ __forceinline__ uint32_t dict_digit(const unsigned long long* lk, const uint32_t* lr, unsigned long long x) {
+    uint32_t h = dict_hash(x) & (kDictLutSlots - 1);
+    for (uint32_t probe = 0; probe < kDictLutSlots; ++probe) {
+        const uint32_t r = lr[h];
+        if (r == kDictEmpty) break;
+        if (lk[h] == x) return r;
+        h = (h + 1) & (kDictLutSlots - 1);
+    }
+    return 255;  // slots past the chunk: their all-ones keys rank last
+}
+
 template <typename K, int BITS, int THREADS, int ITEMS, int IN_MODE, bool FINAL, int MATCH, int MINB,
-          bool SEG = false, bool TMA = false>
+          bool SEG = false, bool TMA = false, bool DICT = false>
 __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
+    static_assert(!DICT || (BITS == 8 && !SEG && !TMA), "the dictionary pass is a plain 8-bit pass");
     using C = OnesweepCfg<K, BITS, THREADS, ITEMS, MATCH>;
     constexpr int RADIX = C::RADIX, WARPS = C::WARPS, TILE = C::TILE, BPT = C::BPT;
     constexpr bool BULK = TMA && !SEG;
@@ -301,11 +316,20 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
     uint64_t* mbar = reinterpret_cast<uint64_t*>(misc + 8);
     K* const kbuf1 = reinterpret_cast<K*>(smem + C::SMEM);
     uint32_t* const vbuf1 = reinterpret_cast<uint32_t*>(smem + C::SMEM + C::KEY_BYTES);
+    unsigned long long* const dlk = reinterpret_cast<unsigned long long*>(smem + C::SMEM);  // DICT: the table
+    uint32_t* const dlr = reinterpret_cast<uint32_t*>(smem + C::SMEM + kDictLutSlots * 8);
+    uint8_t* const ex_dig = smem + C::SMEM + sizeof(DictLut);  // DICT: digits beside the exchanged keys
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // A conditional pass not taken returns before touching anything; the
     // flag was written by an earlier launch, so every thread reads the same.
-    if (a.run_flag && ((*a.run_flag != 0) != (a.run_when != 0))) return;
+    if (a.run_flag && *a.run_flag != a.run_when) return;
+    if constexpr (DICT) {  // the lookup table, used after the first barrier below
+        for (uint32_t i = threadIdx.x; i < kDictLutSlots; i += THREADS) {
+            dlk[i] = a.dict_lut->key[i];
+            dlr[i] = a.dict_lut->rank[i];
+        }
+    }
     const uint32_t ntiles = a.ntiles ? a.ntiles : gridDim.x;
     const uint32_t spin_limit = a.spin_limit ? a.spin_limit : kSpinLimit;
     const uint64_t n = a.n;
@@ -500,11 +524,14 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
         for (int i = 0; i < (ITEMS + 3) / 4; ++i) dpk[i] = 0;
         auto digit = [&](int j) -> uint32_t {
             if constexpr (PACKED) return (dpk[j / 4] >> (8 * (j % 4))) & 0xffu;
+            else if constexpr (DICT) return dict_digit(dlk, dlr, (unsigned long long)key[j]);
             else return digit_of<K, BITS>(key[j], shift);
         };
     #pragma unroll
         for (int j = 0; j < ITEMS; ++j) {
-            const uint32_t d = digit_of<K, BITS>(key[j], shift);
+            uint32_t d;
+            if constexpr (DICT) d = dict_digit(dlk, dlr, (unsigned long long)key[j]);
+            else d = digit_of<K, BITS>(key[j], shift);
             if constexpr (PACKED) dpk[j / 4] |= d << (8 * (j % 4));
             if constexpr (MATCH == 3) {
                 uint32_t* word = wmask + ((j & 1) * WARPS + warp) * RADIX + d;
@@ -599,6 +626,7 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
             }
             ex_keys[r] = key[j];
             ex_vals[r] = val[j];
+            if constexpr (DICT) ex_dig[r] = (uint8_t)d;  // spares a second table lookup
         }
 
         // ---- decoupled look-back per bin ---------------------------------------
@@ -719,7 +747,9 @@ __global__ void __launch_bounds__(THREADS, MINB) k_onesweep(PassArgs a) {
             if (i < valid) {
                 const K k = ex_keys[i];
                 const uint32_t v = ex_vals[i];
-                const uint32_t d = digit_of<K, BITS>(k, shift);
+                uint32_t d;
+                if constexpr (DICT) d = ex_dig[i];
+                else d = digit_of<K, BITS>(k, shift);
                 uint32_t p = bglob[d] + i;
                 if (p >= n) {  // only after a look-back timeout: never write out of bounds
                     atomicOr(a.err, ERR_BAD_INDEX);
@@ -867,6 +897,32 @@ const SegVariant kSegVariants[] = {
 };
 constexpr int kNumSegVariants = (int)(sizeof(kSegVariants) / sizeof(kSegVariants[0]));
 
+// Dictionary-pass kernels (one final 8-bit pass over each key's rank), for
+// 4- and 8-byte keys; k[0] reads the raw column, k[1] the keys through the
+// input permutation.
+struct DictVariant {
+    int width, threads, items;
+    size_t smem;
+    PassKernel k[2];
+};
+template <typename K, int THREADS, int ITEMS, int MATCH, int MINB>
+DictVariant make_dict_variant() {
+    using C = OnesweepCfg<K, 8, THREADS, ITEMS, MATCH>;
+    DictVariant v{};
+    v.width = (int)sizeof(K);
+    v.threads = THREADS;
+    v.items = ITEMS;
+    v.smem = C::SMEM + sizeof(DictLut) + (size_t)C::TILE;
+    v.k[0] = k_onesweep<K, 8, THREADS, ITEMS, IN_RAW, true, MATCH, MINB, false, false, true>;
+    v.k[1] = k_onesweep<K, 8, THREADS, ITEMS, IN_GATHER, true, MATCH, MINB, false, false, true>;
+    return v;
+}
+const DictVariant kDictVariants[] = {
+    make_dict_variant<uint32_t, 256, 16, 1, 3>(),  // 0: 4-byte keys
+    make_dict_variant<uint64_t, 256, 12, 1, 3>(),  // 1: 8-byte keys
+};
+int g_dict_resident[2];
+
 const PassVariant& variant_for(const SortTuning& t, int width) {
     const int v = (width == 4) ? t.variant32 : t.variant64;
     return kVariants[v];
@@ -896,7 +952,11 @@ bool sort_tuning_valid(const SortTuning& t) {
            t.variant64 >= 0 && t.variant64 < kNumVariants && kVariants[t.variant64].width == 8;
 }
 
-SortTuning default_sort_tuning() { return SortTuning{1, 2, 1, kMsdDefaultMinRows}; }
+SortTuning default_sort_tuning() {
+    SortTuning t{1, 2, 1, kMsdDefaultMinRows};
+    t.dict = 1;
+    return t;
+}
 
 static int tile_rows(const SortTuning& t, int width) {
     const PassVariant& v = variant_for(t, width);
@@ -945,6 +1005,15 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
         // memory passes it saves); none for 4-byte keys
         p.msd_lo_bits = p.width[0] == 8 ? 32 : 0;
     }
+    // dictionary plan for one key (tried first; the device decides)
+    if (tuning.dict && nkeys == 1 && n >= 2 && n >= tuning.msd_min_rows) {
+        p.dict = true;
+        p.dict_variant = p.width[0] == 8 ? 1 : 0;
+        const DictVariant& dv = kDictVariants[p.dict_variant];
+        const uint32_t rows = (uint32_t)(dv.threads * dv.items);
+        p.dict_tiles = (uint32_t)((n + rows - 1) / rows);
+        if (p.dict_tiles > max_tiles) max_tiles = p.dict_tiles;
+    }
     // passes are numbered in processing order (least-significant key first);
     // their histograms follow one another in that order
     int total = 0, words = 0;
@@ -972,17 +1041,26 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
         p.off_msd_offs = off; off = align_up(off + (size_t)msd_p * 256 * 4, A);
         p.off_chunks = off; off = align_up(off + ((size_t)p.msd_chunks + 1) * 4, A);
     }
+    if (p.dict) {
+        p.off_dict_lut = off; off = align_up(off + sizeof(DictLut), A);
+        p.off_dict_offs = off; off = align_up(off + 256 * 4, A);
+    }
     // zeroed region: hist | counters+err | status[0] (| status[1] | MSD
-    // histograms | MSD flag: with the MSD plan the LSD passes may start after
-    // passes that never ran, so both status buffers start clear)
+    // histograms | plan word | dictionary table and words: with the MSD-first
+    // or dictionary plan the LSD passes may start after passes that never
+    // ran, so both status buffers start clear)
     p.off_zero = off;
     p.off_hist = off; off = align_up(off + (size_t)words * 4, A);
-    p.off_counters = off; off = align_up(off + (size_t)(total + msd_p + 1) * 4, A);
+    p.off_counters = off; off = align_up(off + (size_t)(total + msd_p + 2) * 4, A);
     p.off_status[0] = off; off = align_up(off + status_bytes, A);
-    if (p.msd) {
+    if (p.msd || p.dict) {
         p.off_status[1] = off; off = align_up(off + status_bytes, A);
-        p.off_msd_hist = off; off = align_up(off + (size_t)msd_p * 256 * 4, A);
+        if (p.msd) { p.off_msd_hist = off; off = align_up(off + (size_t)msd_p * 256 * 4, A); }
         p.off_msd_flag = off; off = align_up(off + 4, A);
+        if (p.dict) {
+            p.off_dict_table = off; off = align_up(off + sizeof(DictSlot) * kDictSlots, A);
+            p.off_dict_words = off; off = align_up(off + 16, A);
+        }
         p.zero_bytes = off - p.off_zero;
     } else {
         p.zero_bytes = off - p.off_zero;
@@ -996,7 +1074,7 @@ int sort_launches(const SortPlan& p) {
     // histogram + scan + passes, plus for the MSD plan its histogram, scan,
     // passes, chunk search and shared-memory finish (the LSD kernels are
     // launched in either case and return at once when not needed)
-    return 2 + p.total_passes + (p.msd ? 4 + p.msd_passes : 0);
+    return 2 + p.total_passes + (p.msd ? 4 + p.msd_passes : 0) + (p.dict ? 3 : 0);
 }
 
 namespace {
@@ -1154,7 +1232,7 @@ cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, u
                          reinterpret_cast<uint32_t*>(ws + p.off_vals[1])};
     const bool invert = (order == 1);
 
-    MsdHistArgs mh{key_cols[0], p.dtype[0], invert ? 1 : 0, first, P, n, mhist};
+    MsdHistArgs mh{key_cols[0], p.dtype[0], invert ? 1 : 0, first, P, n, mhist, flag};
     if (prof) prof->begin(KC_HIST, s);
     e = msd_hist(mh, w, s);
     if (prof) prof->end(KC_HIST, s);
@@ -1230,22 +1308,91 @@ cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, u
     if (prof) prof->end(KC_LOCALSORT, s);
     return e;
 }
+
+// The dictionary plan: the distinct keys and their ranks, then the one pass
+// (taken only when the plan word says 2).
+cudaError_t run_dict(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out, void* key0_out,
+                     unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof, const uint32_t* perm_in,
+                     uint32_t* taken) {
+    uint32_t* word = reinterpret_cast<uint32_t*>(ws + p.off_msd_flag);
+    uint32_t* words = reinterpret_cast<uint32_t*>(ws + p.off_dict_words);
+    DictLut* lut = reinterpret_cast<DictLut*>(ws + p.off_dict_lut);
+    uint32_t* offs = reinterpret_cast<uint32_t*>(ws + p.off_dict_offs);
+    uint32_t* counters = reinterpret_cast<uint32_t*>(ws + p.off_counters);
+    const bool invert = (order == 1);
+    DictArgs da{};
+    da.keys = key_cols[0];
+    da.dtype = p.dtype[0];
+    da.invert = invert ? 1 : 0;
+    da.width = p.width[0];
+    da.n = p.n;
+    da.table = reinterpret_cast<DictSlot*>(ws + p.off_dict_table);
+    da.distinct = words;
+    da.overflow = words + 1;
+    da.state = word;
+    da.fail_state = p.msd ? 0u : 1u;  // next: the MSD-first plan, or the LSD passes
+    da.lut = lut;
+    da.bin_offsets = offs;
+    da.taken = taken;
+    da.spin_limit = p.tuning.spin_limit;
+    da.err = err;
+    if (prof) prof->begin(KC_DICT, s);
+    cudaError_t e = dict_collect(da, s);
+    if (e == cudaSuccess) e = dict_rank(da, s);
+    if (prof) prof->end(KC_DICT, s);
+    if (e != cudaSuccess) return e;
+    const DictVariant& dv = kDictVariants[p.dict_variant];
+    PassArgs a{};
+    a.n = p.n;
+    a.shift = 0;
+    a.dtype = p.dtype[0];
+    a.invert = invert;
+    a.reverse = order == 2 ? 1 : 0;
+    a.bin_offsets = offs;
+    a.status = reinterpret_cast<uint32_t*>(ws + p.off_status[0]);
+    a.status_next = nullptr;  // nothing runs after this pass when it runs
+    a.status_rows = p.max_tiles;
+    a.status_row_words = (uint32_t)p.max_radix;
+    a.tile_counter = counters + p.total_passes + (p.msd ? p.msd_passes : 0);
+    a.err = err;
+    a.run_flag = word;
+    a.run_when = 2;
+    a.spin_limit = p.tuning.spin_limit;
+    a.stall_tile = p.tuning.stall_tile;
+    a.keys_in = key_cols[0];
+    a.vals_in = perm_in;
+    a.keys_out = key0_out;
+    a.vals_out = perm_out;
+    a.dict_lut = lut;
+    a.ntiles = p.dict_tiles;
+    const int cls = dv.width == 4 ? KC_ONESWEEP32 : KC_ONESWEEP64;
+    if (prof) prof->begin(cls, s);
+    dv.k[perm_in ? 1 : 0]<<<pass_grid(p.dict_tiles, g_dict_resident[p.dict_variant], true), dv.threads, dv.smem, s>>>(a);
+    e = cudaGetLastError();
+    if (prof) prof->end(cls, s);
+    return e;
+}
 }  // namespace
 
 cudaError_t run_sort(const SortPlan& p, const void* const* key_cols, int order, uint32_t* perm_out,
                      void* key0_out, unsigned char* ws, uint32_t* err, cudaStream_t s, Profiler* prof,
-                     const uint32_t* perm_in, uint32_t* msd_fallbacks) {
+                     const uint32_t* perm_in, uint32_t* msd_fallbacks, uint32_t* dict_taken) {
     if (p.n == 0) return cudaSuccess;
     cudaError_t e = cudaMemsetAsync(ws + p.off_zero, 0, p.zero_bytes, s);
     if (e != cudaSuccess) return e;
-    if (!p.msd)
+    if (!p.msd && !p.dict)
         return run_lsd(p, key_cols, order, perm_out, key0_out, ws, err, s, prof, perm_in, 0, nullptr, nullptr);
-    e = run_msd(p, key_cols, order, perm_out, key0_out, ws, err, s, prof, perm_in);
-    if (e != cudaSuccess) return e;
-    // the LSD sort over all keys, taken only if the MSD plan failed
+    // the plan word picks what runs: 2 the dictionary pass, 0 the MSD-first
+    // plan, 1 the LSD passes over all keys (each launch returns at once
+    // unless the word selects it)
+    if (p.dict && (e = run_dict(p, key_cols, order, perm_out, key0_out, ws, err, s, prof, perm_in, dict_taken)) !=
+                      cudaSuccess)
+        return e;
+    if (p.msd && (e = run_msd(p, key_cols, order, perm_out, key0_out, ws, err, s, prof, perm_in)) != cudaSuccess)
+        return e;
     const uint32_t* flag = reinterpret_cast<const uint32_t*>(ws + p.off_msd_flag);
-    return run_lsd(p, key_cols, order, perm_out, key0_out, ws, err, s, prof, perm_in, p.msd_passes, flag,
-                   msd_fallbacks);
+    return run_lsd(p, key_cols, order, perm_out, key0_out, ws, err, s, prof, perm_in, p.msd ? p.msd_passes : 0, flag,
+                   p.msd ? msd_fallbacks : nullptr);
 }
 
 // ---------------------------------------------------------------------------
@@ -1424,6 +1571,19 @@ cudaError_t prepare_sort_kernels() {
                 res = std::min(res, nb);
             }
         g_resident[i] = std::max(res, 1);
+    }
+    for (int i = 0; i < 2; ++i) {
+        const DictVariant& v = kDictVariants[i];
+        int res = 1 << 30;
+        for (int m = 0; m < 2; ++m) {
+            cudaError_t e = cudaFuncSetAttribute(v.k[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
+            if (e != cudaSuccess) return e;
+            int nb = 0;
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, v.k[m], v.threads, v.smem);
+            if (e != cudaSuccess) return e;
+            res = std::min(res, nb);
+        }
+        g_dict_resident[i] = std::max(res, 1);
     }
     static_assert(kNumSegVariants <= 16, "residency table");
     for (int i = 0; i < kNumSegVariants; ++i) {
