@@ -156,6 +156,13 @@ vdf_status vdf_sort_variant_info(int index, int32_t* key_width, int32_t* threads
  * the next tile's copy overlapping the current tile's ranking), on a
  * persistent grid. */
 uint32_t vdf_sort_variant_flags(int index);
+/* Group-by emit tuning: a 512-row tile with at least striped_min_heads group
+ * starts is written by the striped path (the thread of each group's first
+ * row walks and writes the group, consecutive threads writing consecutive
+ * groups); others by the per-thread walk after a warp scan of aggregates.
+ * 0 restores the default (480); get returns the value in use. */
+vdf_status vdf_ctx_set_group_tuning(vdf_ctx* ctx, uint32_t striped_min_heads);
+uint32_t vdf_ctx_get_group_tuning(vdf_ctx* ctx);
 vdf_status vdf_ctx_set_sort_tuning(vdf_ctx* ctx, const vdf_sort_tuning* tuning);
 vdf_status vdf_ctx_get_sort_tuning(vdf_ctx* ctx, vdf_sort_tuning* tuning);
 
@@ -212,8 +219,11 @@ vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* ctx, int strategy, uint64_t msd_mi
 int vdf_sort_plan_tries_dict(uint64_t n, const int32_t* key_dtypes, int nkeys, int strategy, uint64_t min_rows);
 vdf_status vdf_ctx_dict_stats(vdf_ctx* ctx, void* stream, uint64_t* tried, uint64_t* taken);
 vdf_status vdf_ctx_get_sort_strategy(vdf_ctx* ctx, int32_t* strategy, uint64_t* msd_min_rows);
-/* Digit matching of the MSD-first sort's shared-memory passes: 0 = one warp
- * ballot per digit bit (default), 1 = match.any; the autotuner's choice. */
+/* The MSD-first sort's shared-memory finish.  Bit 0, digit matching of its
+ * passes: 0 = one warp ballot per digit bit (default), 1 = match.any (the
+ * autotuner's choice).  Bit 1: wide chunks (up to 8192 rows, one CTA of 1024
+ * threads per SM) for every such sort; without it they are used only where
+ * they save the third top-digit pass (between 100.7M and 201M rows). */
 vdf_status vdf_ctx_set_local_sort_variant(vdf_ctx* ctx, int variant);
 int vdf_ctx_get_local_sort_variant(vdf_ctx* ctx); /* -1 for a NULL context */
 /* Failure injection for tests; nothing here faults the device.

@@ -101,7 +101,10 @@ def test_sort_plan_choice():
     # 100M rows, int64 + int32 keys: two top-digit passes, 2048-row chunks
     assert info(100_000_000, [vdf.I64, vdf.I32]) == {"msd_passes": 2, "chunks": (100_000_000 + 2047) // 2048,
                                                        "dict": False}
-    assert info(200_000_000, [vdf.I64])["msd_passes"] == 3
+    # wide chunks (8,192 rows) save the third top digit up to 201M rows
+    assert info(200_000_000, [vdf.I64]) == {"msd_passes": 2, "chunks": (200_000_000 + 4095) // 4096, "dict": True}
+    assert info(100_000_000, [vdf.I64])["chunks"] == (100_000_000 + 2047) // 2048
+    assert info(300_000_000, [vdf.I64])["msd_passes"] == 3
     # 4-byte key 0: the LSD passes unless the MSD strategy is forced
     assert info(393_216, [vdf.I32], msd_min_rows=0)["msd_passes"] == 0
     assert info(10_000_000, [vdf.U32, vdf.I64])["msd_passes"] == 0
@@ -119,10 +122,15 @@ def test_dictionary_plan_choice():
     info = _lib.sort_plan_info
     # one key, at least the row threshold, the automatic strategy: tried first
     assert info(200_000_000, [vdf.I32])["dict"] and info(2_000_000, [vdf.F64])["dict"]
-    assert info(200_000_000, [vdf.I64])["msd_passes"] == 3  # its fallback when the values are many
+    assert info(200_000_000, [vdf.I64])["msd_passes"] == 2  # its fallback when the values are many
     assert not info(1000, [vdf.I32])["dict"]
     assert info(1000, [vdf.I32], msd_min_rows=0)["dict"]
     assert not info(2_000_000, [vdf.I32, vdf.I32])["dict"]
     assert not info(2_000_000, [vdf.I32], strategy=_lib.SORT_LSD)["dict"]
     assert not info(2_000_000, [vdf.I32], strategy=_lib.SORT_MSD)["dict"]
     assert vdf.lib.vdf_sort_plan_tries_dict(10, None, 1, 0, 0) == -1
+
+
+def test_group_tuning_bounds_without_a_context():
+    assert vdf.lib.vdf_ctx_set_group_tuning(None, 10) == _lib.ERR_INVALID_ARG
+    assert vdf.lib.vdf_ctx_get_group_tuning(None) == 0

@@ -309,3 +309,34 @@ def test_gather_host_and_transform_groupby_host(ctx):
             np.testing.assert_allclose(out, exp, rtol=1e-12)
         else:
             assert (out == exp).all(), fn
+
+
+@pytest.mark.parametrize("threshold", [1, 64, 200, 480, 512])
+def test_striped_emit_threshold_gives_the_same_groups(threshold):
+    """Every tile whose group starts reach the threshold takes the striped
+    emit path (down to 1: groups of any length); the result is the oracle's
+    either way."""
+    c = vdf.Context(0)
+    try:
+        c.set_group_tuning(threshold)
+        assert c.get_group_tuning() == threshold
+        rng = np.random.default_rng(threshold)
+        n = 300_001
+        for pool in (n // 2, n // 4, 3000, 7):  # ~2, ~4, ~100, ~43,000 rows per group
+            key = rng.integers(0, pool, n).astype(np.int64)
+            v1 = rng.standard_normal(n)
+            v2 = rng.integers(-10**12, 10**12, n)
+            gr = c.sort_groupby([dev(key)], [dev(v1), dev(v2)], agg_cols=[0, 1])
+            c.check()
+            og = ob.groupby([key], [v1, v2])
+            assert gr.n_groups == og.n_groups
+            assert (host(gr.keys[0]) == og.keys[0]).all() and (host(gr.count) == og.count).all()
+            a1, a2 = gr.aggs
+            assert (host(a2.sum) == og.sum[1]).all() and (host(a2.sum_hi) == og.sum_hi[1]).all()
+            assert (host(a2.min) == og.min[1]).all() and (host(a2.max) == og.max[1]).all()
+            assert bits_equal(host(a1.min), og.min[0]) and bits_equal(host(a1.max), og.max[0])
+            assert_f64_close(host(a1.sum), og.sum[0], og.abs[0], f"threshold {threshold} pool {pool} f64 sum")
+        c.set_group_tuning(0)
+        assert c.get_group_tuning() == 480
+    finally:
+        c.close()

@@ -241,3 +241,32 @@ def test_dense_bin_finish_with_mixed_runs(mctx):
     for order in ORDERS:
         used, fell = run_sort(mctx, [k], order)
         assert used == 1 and fell == 0
+
+
+@pytest.mark.parametrize("dt", [np.int64, np.uint32, np.float64])
+@pytest.mark.parametrize("dist", ["uniform", "ties", "few-long-runs"])
+def test_wide_chunks(dt, dist):
+    """Chunks of up to 8,192 rows (one CTA of 1024 threads) -- forced here at
+    small sizes; planned by default where they save a top-digit pass."""
+    c = vdf.Context(0)
+    try:
+        c.set_sort_strategy(_lib.SORT_MSD, 0)
+        c.set_local_sort_variant(2)
+        assert c.get_local_sort_variant() == 2
+        rng = np.random.default_rng(hash((np.dtype(dt).name, dist)) & 0xFFFF)
+        for n in (5000, 8193, 400_001, 2_000_003):
+            if dist == "uniform":
+                keys = [datagen.keys_for("uniform", dt, n, rng)]
+            elif dist == "ties":
+                keys = [pool_keys(rng, n, max(2, n // 2), dt), datagen.keys_for("zipf", np.int32, n, rng)]
+            else:
+                keys = [pool_keys(rng, n, max(2, n // 150), dt)]
+            for order in ORDERS:
+                used, fell = run_sort(c, keys, order)
+                assert used == 1
+                if dist == "uniform" and np.dtype(dt).kind != "f":
+                    assert fell == 0
+        c.set_local_sort_variant(3)  # with match.any
+        run_sort(c, [datagen.keys_for("uniform", np.int64, 1_000_003, rng)])
+    finally:
+        c.close()

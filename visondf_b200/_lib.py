@@ -119,6 +119,8 @@ def _load() -> C.CDLL:
         "vdf_sort_variant_count": (i32, []),
         "vdf_sort_variant_info": (st, [i32] + [C.POINTER(C.c_int32)] * 5),
         "vdf_sort_variant_flags": (C.c_uint32, [i32]),
+        "vdf_ctx_set_group_tuning": (st, [vp, C.c_uint32]),
+        "vdf_ctx_get_group_tuning": (C.c_uint32, [vp]),
         "vdf_ctx_set_sort_tuning": (st, [vp, C.POINTER(vdf_sort_tuning)]),
         "vdf_ctx_get_sort_tuning": (st, [vp, C.POINTER(vdf_sort_tuning)]),
         "vdf_groupby_workspace_bytes": (sz, [u64, i32]),
@@ -335,6 +337,13 @@ class Context:
         self._check(lib.vdf_ctx_dict_stats(self.handle, _stream(stream), C.byref(c), C.byref(d)), "sort_stats")
         return {"msd_sorts": int(a.value), "msd_fallbacks": int(b.value), "dict_sorts": int(c.value),
                 "dict_taken": int(d.value)}
+
+    def set_group_tuning(self, striped_min_heads: int = 0):
+        """Group starts per 512-row tile from which the emit takes its striped path (0: the default)."""
+        self._check(lib.vdf_ctx_set_group_tuning(self.handle, striped_min_heads), "vdf_ctx_set_group_tuning")
+
+    def get_group_tuning(self) -> int:
+        return int(lib.vdf_ctx_get_group_tuning(self.handle))
 
     def set_test_hooks(self, spin_limit: int = 0, stall_tile: int = 0xFFFFFFFF, fail_allocs: int = 0):
         """Failure injection for tests (see vdf_ctx_set_test_hooks)."""

@@ -520,7 +520,7 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
                 la.perm_out = sa.perm_out;
                 la.seg_chunks = sc;
                 la.seg_flag = flags;
-                e = msd_local(la, P.key_width, nch, P.msd_match, s);
+                e = msd_local(la, P.key_width, nch, P.msd_match & 1, s);
             }
             if (prof) prof->end(KC_LOCALSORT, s);
             if (e != cudaSuccess) return e;
@@ -556,6 +556,7 @@ cudaError_t launch_batch(const BatchPlan& P, const vdf_batch_args& a, unsigned c
         // sorted one, since the sort keeps every segment in place
         SegArgs r{};
         r.n = P.n_large;
+        r.striped_min_heads = P.emit_min_heads;
         r.nkeys = 2;
         r.nvals = P.nvals;
         r.key[0] = SegCol{b.arena_seg, U32};
@@ -690,6 +691,7 @@ vdf_status vdf_batch_create(vdf_ctx* c, const vdf_batch_args* a, const vdf_batch
         delete b;
         return fail(c, VDF_ERR_UNSUPPORTED, "%s", why.c_str());
     }
+    b->plan.emit_min_heads = c->emit_min_heads;
     st = ws_ensure(c, b->plan.ws_bytes);
     if (st != VDF_OK) {
         delete b;

@@ -91,6 +91,7 @@ struct BatchPlan {
     // them, and those whose chunks defeated the plan)
     bool msd = false;
     int msd_match = 0;
+    uint32_t emit_min_heads = 0;  // the group-by emit's striped-path threshold (0 = default)
     uint32_t msd_queries = 0;
     std::vector<SegDesc> msd_segs;         // more passes first
     std::vector<uint32_t> msd_seg_of;      // [msd segs] segment index in segs

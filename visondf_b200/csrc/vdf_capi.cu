@@ -199,6 +199,20 @@ vdf_status vdf_sort_variant_info(int index, int32_t* key_width, int32_t* threads
 
 uint32_t vdf_sort_variant_flags(int index) { return vdf::sort_variant_uses_tma(index) ? 1u : 0u; }
 
+vdf_status vdf_ctx_set_group_tuning(vdf_ctx* c, uint32_t striped_min_heads) {
+    if (!c) return VDF_ERR_INVALID_ARG;
+    if (striped_min_heads > 512) return fail(c, VDF_ERR_INVALID_ARG, "striped_min_heads must be 0..512");
+    std::lock_guard<std::mutex> lk(c->mu);
+    c->emit_min_heads = striped_min_heads;
+    return VDF_OK;
+}
+
+uint32_t vdf_ctx_get_group_tuning(vdf_ctx* c) {
+    if (!c) return 0;
+    std::lock_guard<std::mutex> lk(c->mu);
+    return c->emit_min_heads ? c->emit_min_heads : vdf::kStripedMinHeads;
+}
+
 vdf_status vdf_ctx_set_sort_tuning(vdf_ctx* c, const vdf_sort_tuning* t) {
     if (!c || !t) return VDF_ERR_INVALID_ARG;
     std::lock_guard<std::mutex> lk(c->mu);
@@ -251,7 +265,7 @@ vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* c, int strategy, uint64_t msd_min_
 
 vdf_status vdf_ctx_set_local_sort_variant(vdf_ctx* c, int variant) {
     if (!c) return VDF_ERR_INVALID_ARG;
-    if (variant < 0 || variant > 1) return fail(c, VDF_ERR_INVALID_ARG, "bad local sort variant %d", variant);
+    if (variant < 0 || variant > 3) return fail(c, VDF_ERR_INVALID_ARG, "bad local sort variant %d", variant);
     std::lock_guard<std::mutex> lk(c->mu);
     c->tuning.msd_match = variant;
     return VDF_OK;
@@ -525,6 +539,7 @@ vdf_status vdf_groupby_sorted(vdf_ctx* c, uint64_t n, const vdf_col* keys, int n
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     vdf::SegArgs a{};
     a.n = n;
+    a.striped_min_heads = c->emit_min_heads;
     a.nkeys = nkeys;
     a.nvals = nvals;
     for (int k = 0; k < nkeys; ++k) {
@@ -683,6 +698,7 @@ vdf_status sort_groupby_locked(vdf_ctx* c, const vdf_sort_groupby_args* x, cudaS
 
     vdf::SegArgs a{};
     a.n = n;
+    a.striped_min_heads = c->emit_min_heads;
     a.nkeys = x->nkeys;
     a.nvals = x->nagg;
     for (int k = 0; k < x->nkeys; ++k) {
@@ -1114,6 +1130,7 @@ static vdf_status left_join_locked(vdf_ctx* c, uint64_t n_left, vdf_col left_key
         if (r != VDF_OK) return r;
         vdf::SegArgs a{};
         a.n = n;
+        a.striped_min_heads = c->emit_min_heads;
         a.nkeys = 1;
         a.nvals = 0;
         a.key[0] = vdf::SegCol{c->ws + o_s, key.dtype};

@@ -85,6 +85,7 @@ struct vdf_ctx {
                                          // taken, [6..7] spare
     uint64_t msd_sorts = 0;              // sorts planned MSD-first
     uint64_t dict_sorts = 0;             // sorts that tried the dictionary plan
+    uint32_t emit_min_heads = 0;         // group-by emit: striped-path threshold (0 = default)
     uint32_t fail_allocs = 0;            // test hook: workspace allocations to fail
     int multikey_mode = VDF_MULTIKEY_PRIMARY_FIRST;
     std::atomic<uint64_t> launches{0};

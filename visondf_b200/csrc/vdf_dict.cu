@@ -42,6 +42,7 @@ __device__ __forceinline__ unsigned long long ld_volatile(const unsigned long lo
 // set *over.  Returns false when the value was not recorded.
 __device__ bool dict_add(unsigned long long* keys, uint32_t* cnt, uint32_t* st, uint32_t mask, unsigned long long x,
                          uint32_t add, uint32_t limit, uint32_t* distinct, uint32_t* over, uint32_t* err) {
+    if (ld_volatile(over)) return false;  // too many values already: the table is not filled further
     uint32_t s = dict_hash(x) & mask;
     for (uint32_t probe = 0; probe <= mask; ++probe) {
         uint32_t state = ld_volatile(st + s);
@@ -102,15 +103,20 @@ __global__ void __launch_bounds__(512) k_dict_collect(DictArgs a) {
     // bound depends on the warp's first row only), so the warp-wide match
     // below always has all 32 lanes
     const uint64_t warp_first = (uint64_t)blockIdx.x * blockDim.x + (threadIdx.x & ~31u);
+    // every early exit is decided for the whole warp at once (__any_sync): a
+    // lane leaving alone would leave its warp-mates waiting in the warp-wide
+    // ballot below
     for (uint64_t w0 = warp_first; w0 < n; w0 += R * stride, ++round) {
-        if (ld_volatile(&sover)) break;
-        if ((round & 7) == 7 && ld_volatile(a.overflow)) break;  // another CTA has seen too many values
+        if (__any_sync(0xffffffffu, ld_volatile(&sover) != 0)) break;
+        // another CTA has seen too many values
+        if ((round & 7) == 7 && __any_sync(0xffffffffu, ld_volatile(a.overflow) != 0)) break;
         const uint64_t i0 = w0 + lane;
         K k[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) k[r] = i0 + r * stride < n ? ldg_stream(src + i0 + r * stride) : K(0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
+            if (__any_sync(0xffffffffu, ld_volatile(&sover) != 0)) break;
             const bool valid = i0 + r * stride < n;
             const unsigned long long x = (unsigned long long)KeyOps<K>::order(k[r], a.dtype, a.invert != 0);
             const uint32_t vb = __ballot_sync(0xffffffffu, valid);

@@ -204,6 +204,7 @@ struct SortPlan {
     bool msd;
     int msd_passes;
     int msd_lo_bits;           // key 0 bits ranked directly in runs (below the shared-memory passes)
+    uint32_t msd_cap;          // rows a chunk may hold (kMsdCap, or kMsdWideCap)
     uint32_t msd_chunk_rows;   // nominal rows per chunk
     uint32_t msd_chunks;       // ceil(n / msd_chunk_rows)
     size_t off_msd_hist, off_msd_offs, off_msd_flag, off_chunks;
@@ -220,6 +221,8 @@ struct SortPlan {
 // run of equal high key bits the shared-memory finish ranks directly, and the
 // most top digits that go through global passes.
 constexpr uint32_t kMsdCap = 4096;
+// wide chunks (one CTA of 1024 threads per SM) where they save a top digit
+constexpr uint32_t kMsdWideCap = 8192;
 constexpr uint32_t kMsdRunMax = 64;
 constexpr int kMsdMaxPasses = 3;
 constexpr uint32_t kMsdBucketRows = 1536;           // planned average bucket
@@ -266,13 +269,14 @@ struct MsdLocalArgs {
 };
 cudaError_t msd_hist(const MsdHistArgs& a, int width, cudaStream_t s);
 cudaError_t msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t cap, uint32_t* flag, cudaStream_t s);
-cudaError_t msd_chunks(const MsdChunkArgs& a, int width, cudaStream_t s);
-cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, int match, cudaStream_t s);
+cudaError_t msd_chunks(const MsdChunkArgs& a, int width, cudaStream_t s, uint32_t cap = kMsdCap);
+cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, int match, cudaStream_t s,
+                      uint32_t cap = kMsdCap);
 // Kernel launches run_sort makes for a plan (conditional ones included).
 int sort_launches(const SortPlan& p);
 // Global top-digit passes of the MSD-first plan for n rows of width-byte keys
 // (0: none fits).
-int msd_passes_for(uint64_t n, int width);
+int msd_passes_for(uint64_t n, int width, uint32_t bucket_rows = kMsdBucketRows);
 
 SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const SortTuning& tuning);
 // Sorts; writes perm_out (and key0_out = raw sorted most-significant key, may
@@ -378,7 +382,12 @@ struct SegArgs {
     uint32_t* row_group;       // group index of each sorted row (may be null)
     uint64_t* n_groups;        // device word: number of groups (may be null)
     uint32_t* err;             // error word
+    // tiles of the emit pass with at least this many heads (of 512 rows)
+    // take the striped path, each group written by the thread of its first
+    // row; 0 = kStripedMinHeads
+    uint32_t striped_min_heads = 0;
 };
+constexpr uint32_t kStripedMinHeads = 480;
 size_t segreduce_workspace_bytes(uint64_t n, int nvals);
 cudaError_t prepare_segreduce_kernels();
 // Three launches: tile aggregates, their scan (one CTA), then the emit pass.

@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(256) k_msd_scan(const uint32_t* hist, uint32_t
 // ---------------------------------------------------------------------------
 // 4. chunk starts: one warp per chunk
 // ---------------------------------------------------------------------------
-template <typename K>
+template <typename K, uint32_t CAP>
 __global__ void __launch_bounds__(256) k_msd_chunks(MsdChunkArgs a) {
     const int lane = threadIdx.x & 31;
     const uint32_t c = blockIdx.x * 8 + (threadIdx.x >> 5);
@@ -162,11 +162,11 @@ __global__ void __launch_bounds__(256) k_msd_chunks(MsdChunkArgs a) {
         // by their top bits, so "differs" is false up to the boundary and
         // true after it, and a probe tells on which side it lies
         const K p0 = keys[x - 1] >> pshift;
-        constexpr uint32_t S = kMsdCap / 32;  // level-1 probe spacing
+        constexpr uint32_t S = CAP / 32;  // level-1 probe spacing
         const uint64_t q = min(x + (uint64_t)(lane + 1) * S - 1, end - 1);
         const uint32_t hit = __ballot_sync(0xffffffffu, (keys[q] >> pshift) != p0);
         if (!hit) {
-            // kMsdCap rows after x still share row x-1's top bits: that bucket
+            // CAP rows after x still share row x-1's top bits: that bucket
             // is larger than a chunk can hold (or runs to the end)
             out = end;
             if (x + (uint64_t)32 * S - 1 < end - 1 && lane == 0) atomicOr(flag, 1u);
@@ -206,7 +206,7 @@ struct LocalCfg {
     static constexpr size_t SMEM = KEYS + VALS + SEC + MISC + ORIG + SBIN;
     // the counting pass's 8192 bins and the LSD passes' per-warp counters
     // live in the key-1 buffer, which is only needed after either is done
-    static_assert(SEC >= 8192 * 4 && SEC >= (size_t)WARPS * 256 * 4, "key-1 buffer doubles as counters");
+    static_assert(SEC >= (size_t)2 * CAP * 4 && SEC >= (size_t)WARPS * 256 * 4, "key-1 buffer doubles as counters");
 };
 
 template <int THREADS>
@@ -357,8 +357,10 @@ __device__ __forceinline__ bool counting_finish(K (&key)[ITEMS], uint32_t (&val)
     // scatter is done
     uint32_t* bins = reinterpret_cast<uint32_t*>(ssec);
     constexpr int WARPS = THREADS / 32;
-    constexpr int NB = 8192, BPT = NB / THREADS;  // bins, bins per thread
-    static_assert(NB % THREADS == 0 && BPT % 4 == 0, "bin layout");
+    // bins (two per slot: 8192 for 4096-row chunks), bins per thread
+    constexpr int NB = 2 * THREADS * ITEMS, BPT = NB / THREADS;
+    constexpr int LNB = NB == 16384 ? 14 : 13;
+    static_assert((1 << LNB) == NB && BPT % 4 == 0, "bin layout");
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // ---- key range of the chunk
     K kmin = ~K(0), kmax = 0;
@@ -559,7 +561,7 @@ __device__ __forceinline__ bool counting_finish(K (&key)[ITEMS], uint32_t (&val)
 
 // MATCH: 0 = one ballot per digit bit, 1 = match.any.
 template <typename K, int THREADS, int ITEMS, int MATCH>
-__global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
+__global__ void __launch_bounds__(THREADS, THREADS >= 1024 ? 1 : 2) k_msd_local(MsdLocalArgs a) {
     using C = LocalCfg<K, THREADS, ITEMS>;
     constexpr int WARPS = C::WARPS, RADIX = 256;
     constexpr uint32_t CAP = (uint32_t)C::CAP;
@@ -822,13 +824,19 @@ __global__ void __launch_bounds__(THREADS, 2) k_msd_local(MsdLocalArgs a) {
 namespace {
 constexpr int kLocalThreads = 512, kLocalItems = 8;
 static_assert(kLocalThreads * kLocalItems == (int)kMsdCap, "chunk capacity");
-static_assert(kMsdCap < (1u << 16), "run bounds are packed in 16 bits");
+static_assert(2 * kLocalThreads * kLocalItems == (int)kMsdWideCap, "wide chunk capacity");
+static_assert(kMsdWideCap < (1u << 16), "run bounds are packed in 16 bits");
 using Local64 = LocalCfg<uint64_t, kLocalThreads, kLocalItems>;
 using Local32 = LocalCfg<uint32_t, kLocalThreads, kLocalItems>;
+using Wide64 = LocalCfg<uint64_t, 2 * kLocalThreads, kLocalItems>;
+using Wide32 = LocalCfg<uint32_t, 2 * kLocalThreads, kLocalItems>;
 template <int MATCH>
 struct LocalKernels {
     static constexpr auto k64 = k_msd_local<uint64_t, kLocalThreads, kLocalItems, MATCH>;
     static constexpr auto k32 = k_msd_local<uint32_t, kLocalThreads, kLocalItems, MATCH>;
+    // wide chunks (<= 8192 rows): one CTA of 1024 threads per SM
+    static constexpr auto w64 = k_msd_local<uint64_t, 2 * kLocalThreads, kLocalItems, MATCH>;
+    static constexpr auto w32 = k_msd_local<uint32_t, 2 * kLocalThreads, kLocalItems, MATCH>;
 };
 
 int sm_count() {
@@ -842,10 +850,16 @@ int sm_count() {
 cudaError_t prepare_msd_kernels() {
     const void* k64[2] = {(const void*)LocalKernels<0>::k64, (const void*)LocalKernels<1>::k64};
     const void* k32[2] = {(const void*)LocalKernels<0>::k32, (const void*)LocalKernels<1>::k32};
+    const void* w64[2] = {(const void*)LocalKernels<0>::w64, (const void*)LocalKernels<1>::w64};
+    const void* w32[2] = {(const void*)LocalKernels<0>::w32, (const void*)LocalKernels<1>::w32};
     for (int m = 0; m < 2; ++m) {
         cudaError_t e = cudaFuncSetAttribute(k64[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Local64::SMEM);
         if (e != cudaSuccess) return e;
         e = cudaFuncSetAttribute(k32[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Local32::SMEM);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(w64[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Wide64::SMEM);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(w32[m], cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Wide32::SMEM);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
@@ -864,16 +878,30 @@ cudaError_t msd_scan(const uint32_t* hist, uint32_t* offs, int ndig, uint32_t ca
     return cudaGetLastError();
 }
 
-cudaError_t msd_chunks(const MsdChunkArgs& a, int width, cudaStream_t s) {
+cudaError_t msd_chunks(const MsdChunkArgs& a, int width, cudaStream_t s, uint32_t cap) {
     const uint32_t grid = (a.nchunks + 1 + 7) / 8;
-    if (width == 8) k_msd_chunks<uint64_t><<<grid, 256, 0, s>>>(a);
-    else k_msd_chunks<uint32_t><<<grid, 256, 0, s>>>(a);
+    if (cap == kMsdWideCap) {
+        if (width == 8) k_msd_chunks<uint64_t, kMsdWideCap><<<grid, 256, 0, s>>>(a);
+        else k_msd_chunks<uint32_t, kMsdWideCap><<<grid, 256, 0, s>>>(a);
+    } else {
+        if (width == 8) k_msd_chunks<uint64_t, kMsdCap><<<grid, 256, 0, s>>>(a);
+        else k_msd_chunks<uint32_t, kMsdCap><<<grid, 256, 0, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
-cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, int match, cudaStream_t s) {
+cudaError_t msd_local(const MsdLocalArgs& a, int width, uint32_t nchunks, int match, cudaStream_t s, uint32_t cap) {
     if (nchunks == 0) return cudaSuccess;
-    if (width == 8) {
+    constexpr int WT = 2 * kLocalThreads;
+    if (cap == kMsdWideCap) {
+        if (width == 8) {
+            if (match) LocalKernels<1>::w64<<<nchunks, WT, Wide64::SMEM, s>>>(a);
+            else LocalKernels<0>::w64<<<nchunks, WT, Wide64::SMEM, s>>>(a);
+        } else {
+            if (match) LocalKernels<1>::w32<<<nchunks, WT, Wide32::SMEM, s>>>(a);
+            else LocalKernels<0>::w32<<<nchunks, WT, Wide32::SMEM, s>>>(a);
+        }
+    } else if (width == 8) {
         if (match) LocalKernels<1>::k64<<<nchunks, kLocalThreads, Local64::SMEM, s>>>(a);
         else LocalKernels<0>::k64<<<nchunks, kLocalThreads, Local64::SMEM, s>>>(a);
     } else {

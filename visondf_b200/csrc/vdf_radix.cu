@@ -964,13 +964,14 @@ static int tile_rows(const SortTuning& t, int width) {
 }
 
 // Global MSD passes for n rows: the fewest top digits after which a bucket
-// averages at most kMsdBucketRows rows, so that with chunks of nominal
-// kMsdCap / 2 rows a chunk of whole buckets stays within kMsdCap for
-// uniformly spread keys (the average bucket plus six standard deviations).
-int msd_passes_for(uint64_t n, int width) {
+// averages at most bucket_rows rows (kMsdBucketRows for chunks of nominal
+// kMsdCap / 2 rows, twice that for wide chunks), so that a chunk of whole
+// buckets stays within its capacity for uniformly spread keys (the average
+// bucket plus six standard deviations).
+int msd_passes_for(uint64_t n, int width, uint32_t bucket_rows) {
     const int maxp = std::min(kMsdMaxPasses, width - 1);
     for (int p = 1; p <= maxp; ++p)
-        if (n <= (uint64_t)kMsdBucketRows << (8 * p)) return p;
+        if (n <= (uint64_t)bucket_rows << (8 * p)) return p;
     return 0;
 }
 
@@ -998,6 +999,16 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
     if (tuning.msd && nkeys <= 2 && n >= 2 && n >= tuning.msd_min_rows && p.bits[0] == 8 &&
         (tuning.msd == 2 || p.width[0] == 8)) {
         p.msd_passes = msd_passes_for(n, p.width[0]);
+        p.msd_cap = kMsdCap;
+        // wide chunks where they save the third top-digit pass (100.7M-201M
+        // rows: two digits instead of three; measured 0.3 ms faster on 200M
+        // rows, the finish of twice the rows per CTA costing most of the pass
+        // it saves)
+        const int wide = msd_passes_for(n, p.width[0], 2 * kMsdBucketRows);
+        if (wide > 0 && ((wide < p.msd_passes && p.msd_passes == 3) || (tuning.msd_match & 2))) {  // bit 1: always
+            p.msd_passes = wide;
+            p.msd_cap = kMsdWideCap;
+        }
         p.msd = p.msd_passes > 0;
         // low bits ranked directly in runs of equal high bits: the low half of
         // an 8-byte key (such runs are rare for spread keys, and ranking
@@ -1036,7 +1047,7 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
     p.off_vals[1] = off; off = align_up(off + n * 4, A);
     p.off_offs = off; off = align_up(off + (size_t)words * 4, A);
     if (p.msd) {
-        p.msd_chunk_rows = kMsdCap / 2;
+        p.msd_chunk_rows = p.msd_cap / 2;
         p.msd_chunks = (uint32_t)((n + p.msd_chunk_rows - 1) / p.msd_chunk_rows);
         p.off_msd_offs = off; off = align_up(off + (size_t)msd_p * 256 * 4, A);
         p.off_chunks = off; off = align_up(off + ((size_t)p.msd_chunks + 1) * 4, A);
@@ -1238,7 +1249,7 @@ cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, u
     if (prof) prof->end(KC_HIST, s);
     if (e != cudaSuccess) return e;
     if (prof) prof->begin(KC_SCAN, s);
-    e = msd_scan(mhist, moffs, P, kMsdCap, flag, s);
+    e = msd_scan(mhist, moffs, P, p.msd_cap, flag, s);
     if (prof) prof->end(KC_SCAN, s);
     if (e != cudaSuccess) return e;
 
@@ -1286,7 +1297,7 @@ cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, u
     uint32_t* chunk_start = reinterpret_cast<uint32_t*>(ws + p.off_chunks);
     MsdChunkArgs ca{skeys, n, p.msd_chunk_rows, p.msd_chunks, (uint32_t)(8 * (ndigits - P)), chunk_start, flag};
     if (prof) prof->begin(KC_LOCALSORT, s);
-    e = msd_chunks(ca, w, s);
+    e = msd_chunks(ca, w, s, p.msd_cap);
     if (e == cudaSuccess) {
         MsdLocalArgs la{};
         la.keys = skeys;
@@ -1303,7 +1314,7 @@ cudaError_t run_msd(const SortPlan& p, const void* const* key_cols, int order, u
         la.err = err;
         la.keys_out = key0_out;
         la.perm_out = perm_out;
-        e = msd_local(la, w, p.msd_chunks, p.tuning.msd_match, s);
+        e = msd_local(la, w, p.msd_chunks, p.tuning.msd_match & 1, s, p.msd_cap);
     }
     if (prof) prof->end(KC_LOCALSORT, s);
     return e;

@@ -1060,8 +1060,10 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
         sub_all = sub_all && s_all[sub * kWarpsPerSub + w] != 0u;
         sub_heads += s_wh[sub * kWarpsPerSub + w];
     }
-    // nearly every row starts a group: at most 32 rows continue one
-    const bool sub_most = !sub_all && sub_heads + 32 >= (uint32_t)kSegTile;
+    // many rows start a group (by default at most 32 rows continue one): the
+    // striped path
+    const uint32_t min_heads = a.striped_min_heads ? a.striped_min_heads : kStripedMinHeads;
+    const bool sub_most = !sub_all && sub_heads >= min_heads;
 
     Agg<NV> lx = agg_identity<NV>();
     if (!sub_all && !sub_most) {
