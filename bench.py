@@ -818,6 +818,21 @@ def served_section(args, local_rank: int) -> dict:
                       "offered_rows_per_s": rate * mean_rows, "batched": sb.as_dict(), "per_call": sp.as_dict()})
     server_stats = server.stats()
     server.close()
+    # the same server with three slots (three batches in flight): capacity
+    # and the 90 % load point
+    slots_more = None
+    if args.served_slots_more > 2:
+        more = serve.Server(local_rank, budget_bytes=budget, resident_bytes=resident, slots=args.served_slots_more,
+                            max_batch_rows=max_rows, val_dtypes=vdts)
+        server = more
+        run("batched", make_trace(1e9, 64, 7))
+        cap_m = run("batched", make_trace(1e12, nreq, 0))
+        rate = 0.9 * cap_b.rows_per_s / mean_rows
+        sm = run("batched", make_trace(rate, nreq, 1))
+        slots_more = {"slots": args.served_slots_more, "capacity_rows_per_s": cap_m.rows_per_s,
+                      "speedup": cap_m.rows_per_s / cap_p.rows_per_s, "at_0.9_of_two_slot_capacity": sm.as_dict(),
+                      "fixed_bytes": more.stats()["fixed_bytes"]}
+        more.close()
     del key, v1, v2
     torch.cuda.empty_cache()
     return {
@@ -833,6 +848,7 @@ def served_section(args, local_rank: int) -> dict:
                      "speedup": cap_b.rows_per_s / cap_p.rows_per_s,
                      "batched": cap_b.as_dict(), "per_call": cap_p.as_dict()},
         "rates": rates,
+        "more_slots": slots_more,
     }
 
 
@@ -1105,6 +1121,8 @@ def main():
     ap.add_argument("--served-requests", type=int, default=400)
     ap.add_argument("--served-table-rows", type=int, default=100_000_000)
     ap.add_argument("--served-fractions", type=float, nargs="+", default=[0.5, 0.7, 0.9])
+    ap.add_argument("--served-slots-more", type=int, default=3,
+                    help="served section: also measure a server with this many slots (<= 2: skip)")
     ap.add_argument("--hbm-budget-gb", type=float, default=150.0)
     args = ap.parse_args()
     if args.warmup < 3:
