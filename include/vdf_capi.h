@@ -208,7 +208,7 @@ typedef enum vdf_sort_strategy {
 } vdf_sort_strategy;
 vdf_status vdf_ctx_set_sort_strategy(vdf_ctx* ctx, int strategy, uint64_t msd_min_rows);
 /* The dictionary plan (VDF_SORT_AUTO, sorts by ONE key column of at least
- * msd_min_rows rows): the key column's distinct values are collected on the
+ * 4 x msd_min_rows rows): the key column's distinct values are collected on the
  * device first; with at most 256 of them the sort is one stable radix pass
  * over each key's rank among them (a category column: 1 pass instead of 4 or
  * 8), otherwise the MSD-first plan (8-byte keys) or the LSD passes run, as

@@ -121,7 +121,9 @@ def test_sort_plan_choice():
 def test_dictionary_plan_choice():
     info = _lib.sort_plan_info
     # one key, at least the row threshold, the automatic strategy: tried first
-    assert info(200_000_000, [vdf.I32])["dict"] and info(2_000_000, [vdf.F64])["dict"]
+    # from four times the row threshold (4 x 2^20 by default)
+    assert info(200_000_000, [vdf.I32])["dict"] and info(4_194_304, [vdf.F64])["dict"]
+    assert not info(4_194_303, [vdf.F64])["dict"]
     assert info(200_000_000, [vdf.I64])["msd_passes"] == 2  # its fallback when the values are many
     assert not info(1000, [vdf.I32])["dict"]
     assert info(1000, [vdf.I32], msd_min_rows=0)["dict"]

@@ -106,7 +106,7 @@ def test_hand_over_to_the_msd_and_lsd_plans(dctx):
 
 def test_strategies_that_skip_it(ctx):
     rng = np.random.default_rng(6)
-    key = pool_of(rng, 8, np.int32)[rng.integers(0, 8, 2_000_000)]
+    key = pool_of(rng, 8, np.int32)[rng.integers(0, 8, 5_000_000)]
     for strat in (_lib.SORT_LSD, _lib.SORT_MSD):
         c = vdf.Context(0)
         try:
@@ -114,7 +114,7 @@ def test_strategies_that_skip_it(ctx):
             assert run_sort(c, key, vdf.ORDER_ASC)[:2] == (0, 0)
         finally:
             c.close()
-    # the default context: 2M rows are above its row threshold
+    # the default context: 5M rows are above its row threshold (4 x 2^20)
     c = vdf.Context(0)
     try:
         assert run_sort(c, key, vdf.ORDER_ASC)[:2] == (1, 1)

@@ -36,10 +36,11 @@ __device__ __forceinline__ unsigned long long ld_volatile(const unsigned long lo
     return *static_cast<const volatile unsigned long long*>(p);
 }
 
-// Adds `add` rows of value x to an open-addressing table (keys / counts /
-// states, any address space).  A new value takes the next index of
+// Adds `add` rows of value x to a CTA's open-addressing table in shared
+// memory (keys / counts / states).  A new value takes the next index of
 // *distinct; more than kDictMax of them, a full table or a wait that gives up
-// set *over.  Returns false when the value was not recorded.
+// set *over.  Returns false when the value was not recorded.  The fences are
+// CTA-scoped: only the CTA's own threads read the table.
 __device__ bool dict_add(unsigned long long* keys, uint32_t* cnt, uint32_t* st, uint32_t mask, unsigned long long x,
                          uint32_t add, uint32_t limit, uint32_t* distinct, uint32_t* over, uint32_t* err) {
     if (ld_volatile(over)) return false;  // too many values already: the table is not filled further
@@ -51,7 +52,7 @@ __device__ bool dict_add(unsigned long long* keys, uint32_t* cnt, uint32_t* st, 
             if (state == 0) {  // this thread owns the slot: key, then count, then publish
                 keys[s] = x;
                 atomicAdd(cnt + s, add);
-                __threadfence();
+                __threadfence_block();
                 atomicExch(st + s, 2u);
                 if (atomicAdd(distinct, 1u) >= kDictMax) atomicOr(over, 1u);
                 return true;
@@ -67,7 +68,7 @@ __device__ bool dict_add(unsigned long long* keys, uint32_t* cnt, uint32_t* st, 
             if (spins > 16) __nanosleep(32);
             state = ld_volatile(st + s);
         }
-        __threadfence();
+        __threadfence_block();
         if (ld_volatile(keys + s) == x) {
             atomicAdd(cnt + s, add);
             return true;

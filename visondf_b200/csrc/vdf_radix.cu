@@ -1016,8 +1016,11 @@ SortPlan make_sort_plan(uint64_t n, const int32_t* dtypes, int nkeys, const Sort
         // memory passes it saves); none for 4-byte keys
         p.msd_lo_bits = p.width[0] == 8 ? 32 : 0;
     }
-    // dictionary plan for one key (tried first; the device decides)
-    if (tuning.dict && nkeys == 1 && n >= 2 && n >= tuning.msd_min_rows) {
+    // dictionary plan for one key (tried first; the device decides), from
+    // four times the MSD-first plan's row threshold: where the keys take
+    // many values the attempt costs a few short launches, which at 1M-4M
+    // rows is several percent of the sort
+    if (tuning.dict && nkeys == 1 && n >= 2 && n >= 4 * tuning.msd_min_rows) {
         p.dict = true;
         p.dict_variant = p.width[0] == 8 ? 1 : 0;
         const DictVariant& dv = kDictVariants[p.dict_variant];
