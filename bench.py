@@ -21,6 +21,11 @@ int32 payloads.  One vdf_sort_groupby call per step through the C-ABI.
                  on the reference's map and hash) on the host cores, on a
                  10,000,000-row sample of the same workload.
 
+  configs    the other configurations, timed like the headline with parity
+             checks and the reference CPU path beside each: c1_ties (key1 from
+             a 50M pool), c0 (1M rows, int32 key over 10,000 values), c2a
+             (200M rows, 50M distinct int64 keys), c2b (200M rows, 16 int32
+             keys: the dictionary plan).
   batched    4,096 independent sort + group-by queries (rows log-uniform
              1e3..1e7 scaled to a 2 GiB batch, int32/int64 keys, f64 + int64
              values) as one CUDA graph launch per batch (vdf_batch_*), autotuned,
@@ -29,7 +34,8 @@ int32 payloads.  One vdf_sort_groupby call per step through the C-ABI.
              resident 100M-row table through the library's request loop
              (vdf_server_*: HBM-budget admission, continuous batching): capacity
              and p50/p99 latency at 50/70/90 % of batched capacity, against one
-             vdf_sort_groupby call per request on the same traces.
+             vdf_sort_groupby call per request on the same traces; more_slots:
+             the same server with three slots (capacity, 90 % load).
   unique_join  vdf_unique over 100M int64 keys and vdf_left_join_index of 100M
              left rows against 10M right keys, with the oracle's hash walks
              on a 10M-row sample as the CPU baseline.
