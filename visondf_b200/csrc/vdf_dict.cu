@@ -117,24 +117,21 @@ __global__ void __launch_bounds__(512) k_dict_collect(DictArgs a) {
         for (int r = 0; r < R; ++r) k[r] = i0 + r * stride < n ? ldg_stream(src + i0 + r * stride) : K(0);
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            if (__any_sync(0xffffffffu, ld_volatile(&sover) != 0)) break;
             const bool valid = i0 + r * stride < n;
-            const unsigned long long x = (unsigned long long)KeyOps<K>::order(k[r], a.dtype, a.invert != 0);
+            const K kx = KeyOps<K>::order(k[r], a.dtype, a.invert != 0);
+            const unsigned long long x = (unsigned long long)kx;
             const uint32_t vb = __ballot_sync(0xffffffffu, valid);
-            const uint32_t peers = __match_any_sync(0xffffffffu, x) & vb;
-            // every lane looks its value up at once (read only; the common
-            // case); the group's leader then adds the group's rows, or takes
-            // the insertion path for a value not yet in the table
-            uint32_t h = dict_hash(x) & (kDictCtaSlots - 1), found = kDictEmpty;
-            for (uint32_t probe = 0; probe < kDictCtaSlots; ++probe) {
-                const uint32_t st = ld_volatile(&sst[h]);
-                if (st == 0) break;
-                if (st == 2 && ld_volatile(&skey[h]) == x) {
-                    found = h;
-                    break;
-                }
-                h = (h + 1) & (kDictCtaSlots - 1);
-            }
+            const uint32_t peers = __match_any_sync(0xffffffffu, kx) & vb;
+            // every lane looks its value up at once in its first two slots
+            // (read only; with at most 256 values in 512 slots nearly every
+            // value is there); the group's leader then adds the group's rows,
+            // or takes the insertion path (a new value, or one further on)
+            const uint32_t h0 = dict_hash(x) & (kDictCtaSlots - 1), h1 = (h0 + 1) & (kDictCtaSlots - 1);
+            const uint32_t st0 = ld_volatile(&sst[h0]), st1 = ld_volatile(&sst[h1]);
+            const unsigned long long k0 = ld_volatile(&skey[h0]), k1 = ld_volatile(&skey[h1]);
+            uint32_t found = kDictEmpty;
+            if (st0 == 2 && k0 == x) found = h0;
+            else if (st0 != 0 && st1 == 2 && k1 == x) found = h1;
             if (valid && lane == __ffs(peers) - 1) {
                 if (found != kDictEmpty)
                     atomicAdd(&scnt[found], (uint32_t)__popc(peers));
@@ -279,7 +276,7 @@ cudaError_t dict_collect(const DictArgs& a, cudaStream_t s) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint64_t want = (a.n + 2047) / 2048;
-    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sms * 2));
+    const uint32_t grid = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(want, (uint64_t)sms * 4));
     if (a.width == 8) k_dict_collect<uint64_t><<<grid, 512, 0, s>>>(a);
     else k_dict_collect<uint32_t><<<grid, 512, 0, s>>>(a);
     return cudaGetLastError();
