@@ -331,7 +331,9 @@ def config_section(args, local_rank: int, name: str) -> dict:
                rows per key1 value, so key2 orders them)
       c0       1M rows, int32 key over 10,000 values, f64 + int64 values
       c2a      200M rows, int64 key over 50M values, lognormal f64 + int64 values
-      c2b      200M rows, int32 key over 16 values, 90/10 skew, same values"""
+      c2b      200M rows, int32 key over 16 values, 90/10 skew, same values
+    (--c2-rows sets the c2a / c2b row count, e.g. for a profiler capture of a
+    smaller case)"""
     import torch
 
     import visondf_b200 as vdf
@@ -355,16 +357,16 @@ def config_section(args, local_rank: int, name: str) -> dict:
         workload = ("1,000,000 rows, int32 key over 10,000 distinct values, f64 N(0,1) + int64 U[-1e9, 1e9]; "
                     "sort by key, group-by count/sum/min/max/mean of both")
     elif name == "c2a":
-        n = 200_000_000
+        n = args.c2_rows
         f = datagen.frame_w2a(n)
         knames, pnames, agg = ["key"], ["v1", "v2"], [0, 1]
-        workload = ("200,000,000 rows, int64 key over 50,000,000 distinct values, f64 lognormal(0,1) + int64 "
+        workload = (f"{n:,} rows, int64 key over 50,000,000 distinct values, f64 lognormal(0,1) + int64 "
                     "U[0, 2^40); sort, gather, group-by count/sum/min/max/mean")
     elif name == "c2b":
-        n = 200_000_000
+        n = args.c2_rows
         f = datagen.frame_w2b(n)
         knames, pnames, agg = ["key"], ["v1", "v2"], [0, 1]
-        workload = ("200,000,000 rows, int32 key over 16 distinct values (two take 45 % each, 14 share 10 %), "
+        workload = (f"{n:,} rows, int32 key over 16 distinct values (two take 45 % each, 14 share 10 %), "
                     "f64 lognormal(0,1) + int64 U[0, 2^40); sort, gather, group-by")
     else:
         raise ValueError(name)
@@ -1117,6 +1119,8 @@ def main():
                     help="with --no-autotune: radix-pass variant indices for 4- and 8-byte keys")
     ap.add_argument("--csv-bytes", type=int, default=1 << 30, help="size of the synthetic CSV file (csv section)")
     ap.set_defaults(section_tuning=None)
+    ap.add_argument("--c2-rows", type=int, default=200_000_000,
+                    help="rows of the c2a / c2b sections (200M: the configurations as stated)")
     ap.add_argument("--sections", default="c1_ties,c0,c2a,c2b,batched,served,unique_join,csv",
                     help="extra single-GPU measurements after the headline one: batched, served, unique_join "
                          "(comma list, 'none' for none)")
