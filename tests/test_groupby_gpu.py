@@ -340,3 +340,39 @@ def test_striped_emit_threshold_gives_the_same_groups(threshold):
         assert c.get_group_tuning() == 480
     finally:
         c.close()
+
+
+# Tiles of the emit pass are 512 rows, four to a CTA of the two-value kernel;
+# a tile range without a group head is skipped there, so boundaries at and
+# beside those edges (and next to the last row) are the cases to pin.
+EDGE_N = [2048 * 5, 2048 * 5 + 1, 2048 * 5 - 1, 2048 * 3 + 512, 1_000_003]
+
+
+def edge_bounds(n, rng):
+    cand = [1, 511, 512, 513, 1535, 2047, 2048, 2049, 4096, 4608, 6143, 200_000, 204_800, 204_801,
+            n - 2049, n - 2048, n - 2047, n - 513, n - 512, n - 511, n - 2, n - 1]
+    cand += list(rng.integers(1, n, 3))
+    return sorted({int(b) for b in cand if 0 < b < n})
+
+
+@pytest.mark.parametrize("n", EDGE_N)
+@pytest.mark.parametrize("nvals", [2, 3])  # two values: the wide emit kernel; three: the per-tile one
+@pytest.mark.parametrize("bounds", ["none", "last", "first", "edges"])
+def test_few_groups_with_heads_at_tile_edges(ctx, n, nvals, bounds):
+    rng = np.random.default_rng(n + nvals)
+    b = {"none": [], "last": [n - 1], "first": [1], "edges": edge_bounds(n, rng)}[bounds]
+    b = [x for x in b if 0 < x < n]
+    key = np.zeros(n, np.int64)
+    for x in b:
+        key[x:] += 1
+    key = key * 1_000_003 - 7  # sorted, distinct per group
+    vals = [rng.standard_normal(n), rng.integers(-10**15, 10**15, n), rng.integers(-2**31, 2**31, n).astype(np.int32)]
+    vals = vals[:nvals]
+    og = ob.groupby([key], vals)
+    for want_rg in (False, True):  # row_group wanted: every tile is emitted
+        gr = ctx.groupby_sorted([dev(key)], [dev(v) for v in vals], want_row_group=want_rg, want_group_start=True)
+        ctx.check()
+        compare(og, gr, vals, f"n={n} bounds={bounds} row_group={want_rg}")
+        assert (host(gr.group_start).view(np.uint32) == np.array([0] + b, np.uint32)).all()
+        if want_rg:
+            assert (host(gr.row_group).view(np.uint32) == (key + 7) // 1_000_003).all()

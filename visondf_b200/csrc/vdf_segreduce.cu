@@ -21,9 +21,11 @@
 //   * k_seg_emit re-reads each tile, block-scans it seeded with its prefix,
 //     and writes every segment that ends inside it (keys, count, sum, min,
 //     max, mean), staged per warp in shared memory so that each output
-//     column is written by consecutive lanes at consecutive group ids.
+//     column is written by consecutive lanes at consecutive group ids; a
+//     tile without a segment head (known from the prefixes) is skipped.
 // Nothing spins on another CTA, so there is no look-back latency chain: the
-// price is one extra sequential read of the key and value columns.
+// price is one extra sequential read of the key and value columns (of the
+// tiles that hold a head).
 //
 // Exactness: integer sums are 128-bit (lo, hi words); float sums are carried
 // as (sum, compensation) with an error-free TwoSum at every combine, so a
@@ -976,10 +978,30 @@ __device__ __forceinline__ void seg_emit_body(const SegArgs& a, const Agg<NV>* t
     }
 }
 
+// Tiles t0 .. t1-1 write nothing in the emit pass when no segment head lies
+// in their rows and no row's group is wanted (row_group): a tile writes the
+// group that ends before each head in it (with the new group's key and first
+// row), and the group running through head-less tiles is written where the
+// next head is.  The tile holding the last row (which writes the last group
+// and the group count) is never quiet; nor is t1 past the last tile, whose
+// prefix is not stored.  Heads before tile t are the exclusive prefix of the
+// tile pass's head counts, so the heads in the range are H(t1) - H(t0).  With
+// few groups over many rows (a low-cardinality key) nearly every tile is
+// quiet, and its rows are not read a second time.
+template <int NV>
+__device__ __forceinline__ bool quiet_tiles(const SegArgs& a, const Agg<NV>* tile_prefix, const Agg<NV>* block_prefix,
+                                            uint32_t t0, uint32_t t1, uint32_t tiles) {
+    if (a.row_group || t1 >= tiles) return false;
+    const uint32_t h0 = block_prefix[t0 / kScanTiles].heads + tile_prefix[t0].heads;
+    const uint32_t h1 = block_prefix[t1 / kScanTiles].heads + tile_prefix[t1].heads;
+    return h1 == h0;
+}
+
 template <int NK, int NV>
 __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : (NV == 2 ? 4 : 3))) k_seg_emit(SegArgs a, const Agg<NV>* tile_prefix,
                                                                           const Agg<NV>* block_prefix, uint32_t tiles) {
     for (uint32_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        if (quiet_tiles(a, tile_prefix, block_prefix, t, t + 1, tiles)) continue;  // the same for the whole CTA
         seg_emit_body<NK, NV>(a, tile_prefix, block_prefix, t);
         __syncthreads();  // the warp totals and staging are reused by the next tile
     }
@@ -1002,6 +1024,10 @@ __global__ void __launch_bounds__(kSegThreads, (NV >= 3 ? 1 : 3))
     __shared__ uint32_t s_hm[kSegThreads];  // head mask of each thread's rows
     __shared__ uint32_t s_hp[kSegThreads];  // heads before them in the warp
     __shared__ uint32_t s_wh[WARPS];        // heads in each warp's rows
+    // tiles without a segment head write nothing (uniform over the CTA, so
+    // before any barrier)
+    if (quiet_tiles(a, tile_prefix, block_prefix, blockIdx.x * kSubTiles, (blockIdx.x + 1) * kSubTiles, tiles))
+        return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int sub = warp / kWarpsPerSub, wsub = warp - sub * kWarpsPerSub;
     const uint32_t tile = blockIdx.x * kSubTiles + sub;
