@@ -43,9 +43,13 @@ __device__ __forceinline__ unsigned long long ld_volatile(const unsigned long lo
 // CTA-scoped: only the CTA's own threads read the table.
 __device__ bool dict_add(unsigned long long* keys, uint32_t* cnt, uint32_t* st, uint32_t mask, unsigned long long x,
                          uint32_t add, uint32_t limit, uint32_t* distinct, uint32_t* over, uint32_t* err) {
-    if (ld_volatile(over)) return false;  // too many values already: the table is not filled further
     uint32_t s = dict_hash(x) & mask;
     for (uint32_t probe = 0; probe <= mask; ++probe) {
+        // too many values already: the table is not filled further.  Checked
+        // at every step, before a slot is claimed: with many distinct keys all
+        // the CTA's threads insert at once, and without it they would fill
+        // the table and probe it end to end after the plan has failed.
+        if (ld_volatile(over)) return false;
         uint32_t state = ld_volatile(st + s);
         if (state == 0) {
             state = atomicCAS(st + s, 0u, 1u);
@@ -60,6 +64,7 @@ __device__ bool dict_add(unsigned long long* keys, uint32_t* cnt, uint32_t* st, 
         }
         uint32_t spins = 0;
         while (state != 2) {  // another thread is writing the slot's key
+            if (ld_volatile(over)) return false;
             if (++spins > limit) {
                 atomicOr(err, ERR_LOOKBACK_TIMEOUT);
                 atomicOr(over, 1u);
