@@ -253,9 +253,14 @@ def roofline_from_profile(prof: dict, steps: int, n: int, key_w, gather_w, val_w
     cls, ms, cnt, b = best
     avg = ms / cnt
     achieved = b / (avg / 1e3) / 1e9
-    return {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": peak, "unit": "GB/s",
+    roof = {"bound": "hbm", "kernel": cls, "achieved": achieved, "peak": peak, "unit": "GB/s",
             "frac": achieved / peak, "peak_kind": peak_kind, "algorithmic_bytes_per_launch": b,
             "avg_launch_ms": avg, "launches_per_step": cnt / steps}
+    if cls == "localsort":
+        roof["note"] = ("the shared-memory finish moves only about its algorithmic bytes and is issue- and "
+                        "latency-bound (ncu: about 49 % issue active, two CTAs per SM by shared memory and "
+                        "registers), so HBM bandwidth is not what limits it")
+    return roof
 
 
 def group_parity_sample(gr, keys_h, vals_h, n_sample: int, seed: int) -> dict:
